@@ -1,1 +1,344 @@
-"""ctpwa_b200 package (API is added below)."""
+"""ctpwa_b200 — B200-native event-parallel likelihood engine for partial-wave analysis.
+
+Drop-in for the reference module ``ctpwa`` (pybind11 class ``analysis``,
+src/main.cu:91-131)::
+
+    import ctpwa_b200 as ctpwa
+    ana = ctpwa.analysis("config.yml")
+    p = torch.tensor(..., dtype=torch.float64, device="cuda")  # [2*nV + nT]
+    p.requires_grad_(True)
+    nll = ana.getNLL(p)            # 0-d float64 CUDA tensor, differentiable
+    g, = torch.autograd.grad(nll, p)
+    H = ana.getHessian(p)          # [(2nV+nT), (2nV+nT)] float64 CUDA
+
+Parameter layout, names and defaults follow the reference
+(``getNVector``, ``getNFreeTheta``, ``getParamNames``, ``getFreeResParams``).
+Everything runs through the C ABI of ``libctpwa_b200.so`` (include/ctpwa_b200.h);
+there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import warnings
+
+import torch
+
+from . import _lib
+
+__all__ = ["analysis", "DecayInfo", "describe", "precompile", "version"]
+
+_PRECISIONS = {"fp64": 0, "double": 0, "plain": 0, "mixed": 1, "fp32": 1, "float": 1}
+
+
+def version() -> str:
+    return _lib.load().ctpwa_version().decode()
+
+
+def precompile(config_file: str) -> float:
+    """Compile the fused kernel of a config's model into the kernel cache (no GPU needed)."""
+    lib = _lib.load()
+    sec = ctypes.c_double(0.0)
+    err = ctypes.create_string_buffer(4096)
+    rc = lib.ctpwa_precompile(str(config_file).encode(), ctypes.byref(sec), err, 4096)
+    if rc != 0:
+        raise RuntimeError(err.value.decode("utf-8", "replace"))
+    return sec.value
+
+
+def describe(config_file: str) -> dict:
+    """Lowered model of a config (no GPU needed): amplitude columns, groups,
+    resonance blocks, theta slots, coupling map and parameter names."""
+    lib = _lib.load()
+    err = ctypes.create_string_buffer(4096)
+    n = lib.ctpwa_describe(str(config_file).encode(), None, 0, err, 4096)
+    if n < 0:
+        raise RuntimeError(err.value.decode("utf-8", "replace"))
+    buf = ctypes.create_string_buffer(n)
+    lib.ctpwa_describe(str(config_file).encode(), buf, n, err, 4096)
+    return json.loads(buf.value.decode("utf-8"))
+
+
+class DecayInfo:
+    """Host-side model information of a config (reference ``ctpwa.DecayInfo``)."""
+
+    def __init__(self, config_file: str = "config.yml"):
+        try:
+            self._m = describe(config_file)
+        except RuntimeError as e:
+            if "analysis not initialized" not in str(e):
+                raise
+            self._m = None
+
+    def isValid(self) -> bool:
+        return self._m is not None
+
+    def nAmplitudes(self) -> int:
+        return len(self._m["amplitude_names"])
+
+    def amplitudeNames(self):
+        return list(self._m["amplitude_names"])
+
+    def resonanceParamNames(self):
+        return [s["name"] for s in self._m["slots"]]
+
+    def resonanceNames(self):
+        names = []
+        for b in self._m["blocks"]:
+            g = self._m["groups"][b["group"]]
+            rep = {r["tag"]: r["name"] for r in b["res"]}
+            names.append("_".join(
+                f"{rep.get(g['particles'][n['mother']], g['particles'][n['mother']])}\u2192"
+                f"{rep.get(g['particles'][n['d1']], g['particles'][n['d1']])}+"
+                f"{rep.get(g['particles'][n['d2']], g['particles'][n['d2']])}" for n in g["nodes"]))
+        return names
+
+    def hasCouplingMatrix(self) -> bool:
+        return True
+
+    def print(self):
+        print("=== DecayInfo ===")
+        print(f"Amplitudes: {self.nAmplitudes()}")
+        for i, n in enumerate(self.amplitudeNames()):
+            print(f"  [{i}] {n}")
+        print(f"Resonance theta params ({len(self._m['slots'])}):")
+        for i, n in enumerate(self.resonanceParamNames()):
+            print(f"  [{i}] {n}")
+
+
+class _NLLFunction(torch.autograd.Function):
+    """Forward evaluates the NLL and its gradient in one device pass; backward
+    returns the stored gradient times the incoming grad (reference
+    NLLFunction, src/Analysis.cu:625-1261)."""
+
+    @staticmethod
+    def forward(ctx, params, ana):
+        nll, grad = ana._eval(params)
+        ctx.save_for_backward(grad)
+        return nll
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (grad,) = ctx.saved_tensors
+        return grad * grad_out, None
+
+
+class analysis:
+    """Likelihood of one config.yml model over its phase-space, data and
+    background samples (reference ``ctpwa.analysis``)."""
+
+    def __init__(self, config_file: str = "config.yml", device=None, precision: str = "fp64"):
+        self._h = None
+        self._lib = _lib.load()
+        if device is None:
+            device = torch.cuda.current_device() if torch.cuda.is_available() else 0
+        self._device = int(device)
+        self._precision = self._parse_precision(precision)
+        self._fit_mode = 1
+        status = ctypes.c_int(0)
+        err = ctypes.create_string_buffer(4096)
+        h = self._lib.ctpwa_create(str(config_file).encode(), self._device, ctypes.byref(status), err, 4096)
+        if not h:
+            msg = err.value.decode("utf-8", "replace")
+            if status.value == -1 and msg.startswith("analysis not initialized"):
+                # reference: warning + isValid() == False, later calls raise
+                warnings.warn(f'Config file "{config_file}" is empty or not found. Analysis not initialized. ({msg})')
+                return
+            raise RuntimeError(msg)
+        self._h = ctypes.c_void_p(h)
+        self._np = self._lib.ctpwa_n_params(self._h)
+
+    # ------------------------------------------------------------ lifecycle
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h is not None:
+            try:
+                self._lib.ctpwa_destroy(h)
+            except Exception:
+                pass
+
+    def isValid(self) -> bool:
+        return self._h is not None
+
+    def _check(self):
+        if self._h is None:
+            raise RuntimeError("analysis not initialized: invalid or missing config file")
+
+    @staticmethod
+    def _parse_precision(p):
+        if isinstance(p, int):
+            if p not in (0, 1):
+                raise ValueError("precision must be 'fp64' or 'mixed'")
+            return p
+        try:
+            return _PRECISIONS[str(p).lower()]
+        except KeyError:
+            raise ValueError("precision must be 'fp64' or 'mixed'") from None
+
+    def setPrecision(self, precision):
+        """'fp64' (plain FP64, the drop-in default) or 'mixed' (FP32 amplitudes, FP64 reductions)."""
+        self._precision = self._parse_precision(precision)
+
+    def getPrecision(self) -> str:
+        return "mixed" if self._precision == 1 else "fp64"
+
+    # ------------------------------------------------------------ counts/names
+    def setFitMode(self, mode: int):
+        if int(mode) != 1:
+            raise RuntimeError("only fit mode 1 (vspace couplings, the reference default) is supported")
+        self._fit_mode = 1
+
+    def getFitMode(self) -> int:
+        return self._fit_mode
+
+    def getNVector(self) -> int:
+        self._check()
+        return self._lib.ctpwa_n_vector(self._h)
+
+    def getNFreeTheta(self) -> int:
+        self._check()
+        return self._lib.ctpwa_n_free_theta(self._h)
+
+    def getNParams(self) -> int:
+        self._check()
+        return self._np
+
+    def getParamNames(self):
+        self._check()
+        s = _lib.read_string(self._lib.ctpwa_param_names, self._h)
+        return s.split("\n") if s else []
+
+    def getFreeResParams(self) -> torch.Tensor:
+        """CPU float64 tensor [3, nT]: initial values, lower and upper bounds."""
+        self._check()
+        nt = self.getNFreeTheta()
+        out = torch.empty((3, nt), dtype=torch.float64)
+        if nt:
+            rc = self._lib.ctpwa_free_res_params(self._h, ctypes.cast(out.data_ptr(), ctypes.POINTER(ctypes.c_double)))
+            if rc != 0:
+                raise RuntimeError(_lib.error(self._h))
+        return out
+
+    def getModel(self) -> dict:
+        """Lowered model (amplitude columns, groups, theta slots, coupling map)."""
+        self._check()
+        return json.loads(_lib.read_string(self._lib.ctpwa_model_json, self._h))
+
+    def getNEvents(self):
+        self._check()
+        return tuple(int(self._lib.ctpwa_n_events(self._h, k)) for k in range(3))
+
+    def getAmplitudeNames(self):
+        self._check()
+        return list(self.getModel()["amplitude_names"])
+
+    def getNPolarizations(self) -> int:
+        self._check()
+        return int(self.getModel()["npol"])
+
+    def getSLVectors(self) -> torch.Tensor:
+        """Number of SL combinations per resonance block (int32, CUDA)."""
+        m = self.getModel()
+        nsl = [len(m["groups"][b["group"]]["sl_combs"]) for b in m["blocks"]]
+        return torch.tensor(nsl, dtype=torch.int32, device=f"cuda:{self._device}")
+
+    def deviceBytes(self) -> int:
+        self._check()
+        return int(self._lib.ctpwa_device_bytes(self._h))
+
+    # ------------------------------------------------------------ evaluation
+    def _check_params(self, params: torch.Tensor) -> torch.Tensor:
+        self._check()
+        if not isinstance(params, torch.Tensor) or params.dtype != torch.float64:
+            raise RuntimeError("params must be float64")
+        if not params.is_cuda or params.device.index != self._device:
+            raise RuntimeError(f"params must be on the primary GPU (cuda:{self._device}), got {params.device}")
+        if params.dim() != 1:
+            raise RuntimeError("params must be 1-dimensional")
+        if params.numel() != self._np:
+            raise RuntimeError(f"params size mismatch: got {params.numel()}, expected {self._np}")
+        return params.detach().contiguous()
+
+    def _eval(self, params: torch.Tensor, precision=None):
+        p = self._check_params(params)
+        nll = torch.empty((), dtype=torch.float64, device=p.device)
+        grad = torch.empty_like(p)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        prec = self._precision if precision is None else self._parse_precision(precision)
+        rc = self._lib.ctpwa_nll_grad(self._h, p.data_ptr(), nll.data_ptr(), grad.data_ptr(), prec,
+                                      ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return nll, grad
+
+    def getNLL(self, params: torch.Tensor) -> torch.Tensor:
+        """Negative log-likelihood (0-d float64 CUDA tensor); differentiable."""
+        self._check_params(params)
+        return _NLLFunction.apply(params, self)
+
+    def getNLLAndGrad(self, params: torch.Tensor, precision=None):
+        """(nll, grad) without autograd bookkeeping."""
+        return self._eval(params, precision)
+
+    def getNLLHost(self, params, precision=None):
+        """Evaluate from host memory through the C ABI's host-buffer entry point."""
+        self._check()
+        import numpy as np
+
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64))
+        if p.size != self._np:
+            raise RuntimeError(f"params size mismatch: got {p.size}, expected {self._np}")
+        g = np.empty_like(p)
+        v = ctypes.c_double()
+        dp = ctypes.POINTER(ctypes.c_double)
+        prec = self._precision if precision is None else self._parse_precision(precision)
+        rc = self._lib.ctpwa_nll_grad_host(self._h, p.ctypes.data_as(dp), ctypes.byref(v), g.ctypes.data_as(dp),
+                                           prec, None)
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return v.value, g
+
+    def getIntensity(self, params: torch.Tensor, kind: int = 1) -> torch.Tensor:
+        """Per-event intensities (float64 CUDA [n]) of sample kind 0 = phase space, 1 = data, 2 = background."""
+        p = self._check_params(params)
+        n = self.getNEvents()[kind]
+        out = torch.empty(n, dtype=torch.float64, device=p.device)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        rc = self._lib.ctpwa_intensity(self._h, p.data_ptr(), int(kind), out.data_ptr(), ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return out
+
+    def lastParts(self):
+        """[data_nll, bkg_nll, sum_phsp_intensity, W_data, W_bkg, n_phsp] of the last evaluation."""
+        self._check()
+        import numpy as np
+
+        out = np.zeros(6)
+        stream = torch.cuda.current_stream(self._device).cuda_stream
+        rc = self._lib.ctpwa_last_parts(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return out
+
+    def getHessian(self, params: torch.Tensor) -> torch.Tensor:
+        """Hessian [(2nV+nT), (2nV+nT)] (float64, CUDA), grouped [Re p, Im p, theta]."""
+        p = self._check_params(params)
+        return _hessian_fd(self, p)
+
+
+def _hessian_fd(ana: "analysis", p: torch.Tensor) -> torch.Tensor:
+    """Central differences of the exact device gradient (symmetrised)."""
+    n = p.numel()
+    H = torch.empty((n, n), dtype=torch.float64, device=p.device)
+    scale = torch.clamp(p.abs(), min=1e-2)
+    h = 1e-5 * scale
+    for i in range(n):
+        q = p.clone()
+        q[i] += h[i]
+        _, gp = ana._eval(q, 0)
+        q[i] -= 2 * h[i]
+        _, gm = ana._eval(q, 0)
+        H[i] = (gp - gm) / (2 * h[i])
+    return 0.5 * (H + H.T)

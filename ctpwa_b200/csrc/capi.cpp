@@ -1,0 +1,228 @@
+// C ABI (include/ctpwa_b200.h) over the C++ engine: status codes instead of
+// exceptions, host-buffer convenience entry point, model introspection.
+#include "../../include/ctpwa_b200.h"
+
+#include "engine.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+struct ctpwa_handle {
+    std::unique_ptr<ctpwa::Engine> eng;
+    std::string err;
+    double* d_params = nullptr;  // host-entry staging
+    double* d_out = nullptr;     // [1 + n_params]
+    double* h_pin = nullptr;     // pinned [1 + 2 n_params]
+};
+
+namespace {
+std::mutex g_err_mu;
+std::string g_create_err;
+
+int setErr(ctpwa_handle* h, int code, const std::string& m)
+{
+    if (h) h->err = m;
+    else {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_create_err = m;
+    }
+    return code;
+}
+
+int copyOut(const std::string& s, char* buf, size_t cap)
+{
+    if (buf && cap > 0) {
+        size_t n = std::min(cap - 1, s.size());
+        std::memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return (int)s.size() + 1;
+}
+}  // namespace
+
+extern "C" {
+
+ctpwa_handle* ctpwa_create(const char* config_path, int device, int* status, char* err, size_t errlen)
+{
+    auto h = std::make_unique<ctpwa_handle>();
+    int code = CTPWA_OK;
+    std::string msg;
+    try {
+        ctpwa::EngineOptions opt;
+        opt.device = device;
+        h->eng = std::make_unique<ctpwa::Engine>(config_path ? config_path : "config.yml", opt);
+        int np = h->eng->nParams();
+        if (cudaMalloc(&h->d_params, sizeof(double) * std::max(1, np)) != cudaSuccess ||
+            cudaMalloc(&h->d_out, sizeof(double) * (1 + np)) != cudaSuccess ||
+            cudaMallocHost(&h->h_pin, sizeof(double) * (1 + 2 * np)) != cudaSuccess)
+            throw std::runtime_error("CUDA allocation of evaluation buffers failed");
+    } catch (const std::exception& e) {
+        msg = e.what();
+        code = (msg.rfind("CUDA", 0) == 0 || msg.find("NVRTC") != std::string::npos) ? CTPWA_ERR_CUDA : CTPWA_ERR_CONFIG;
+    }
+    if (status) *status = code;
+    if (code != CTPWA_OK) {
+        setErr(nullptr, code, msg);
+        if (err && errlen) copyOut(msg, err, errlen);
+        return nullptr;
+    }
+    return h.release();
+}
+
+void ctpwa_destroy(ctpwa_handle* h)
+{
+    if (!h) return;
+    cudaFree(h->d_params);
+    cudaFree(h->d_out);
+    cudaFreeHost(h->h_pin);
+    delete h;
+}
+
+int ctpwa_n_vector(const ctpwa_handle* h) { return h ? h->eng->model().nVector() : CTPWA_ERR_ARG; }
+int ctpwa_n_free_theta(const ctpwa_handle* h) { return h ? h->eng->model().nTheta() : CTPWA_ERR_ARG; }
+int ctpwa_n_params(const ctpwa_handle* h) { return h ? h->eng->nParams() : CTPWA_ERR_ARG; }
+
+int ctpwa_param_names(const ctpwa_handle* h, char* buf, size_t cap)
+{
+    if (!h) return CTPWA_ERR_ARG;
+    std::string s;
+    for (const auto& n : h->eng->model().param_names) {
+        if (!s.empty()) s += "\n";
+        s += n;
+    }
+    return copyOut(s, buf, cap);
+}
+
+int ctpwa_free_res_params(const ctpwa_handle* h, double* out)
+{
+    if (!h || !out) return CTPWA_ERR_ARG;
+    const auto& sl = h->eng->model().slots;
+    int n = (int)sl.size();
+    for (int i = 0; i < n; ++i) {
+        out[i] = sl[i].init;
+        out[n + i] = sl[i].lower;
+        out[2 * n + i] = sl[i].upper;
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_nll_grad(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision, void* stream)
+{
+    if (!h || !d_params || !d_nll || !d_grad) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (precision != CTPWA_FP64 && precision != CTPWA_MIXED) return setErr(h, CTPWA_ERR_ARG, "precision must be 0 or 1");
+    try {
+        h->eng->nllGrad(d_params, d_nll, d_grad, precision, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_nll_grad_host(ctpwa_handle* h, const double* params, double* nll, double* grad, int precision, void* stream)
+{
+    if (!h || !params || !nll || !grad) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    int np = h->eng->nParams();
+    cudaStream_t s = (cudaStream_t)stream;
+    try {
+        std::memcpy(h->h_pin, params, sizeof(double) * np);
+        if (cudaMemcpyAsync(h->d_params, h->h_pin, sizeof(double) * np, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            throw std::runtime_error("CUDA error: host-to-device copy failed");
+        int rc = ctpwa_nll_grad(h, h->d_params, h->d_out, h->d_out + 1, precision, stream);
+        if (rc != CTPWA_OK) return rc;
+        if (cudaMemcpyAsync(h->h_pin + np, h->d_out, sizeof(double) * (1 + np), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
+        *nll = h->h_pin[np];
+        std::memcpy(grad, h->h_pin + np + 1, sizeof(double) * np);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_intensity(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream)
+{
+    if (!h || !d_params || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    try {
+        h->eng->intensity(d_params, kind, d_out, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream)
+{
+    if (!h || !out6) return CTPWA_ERR_ARG;
+    try {
+        h->eng->lastParts(out6, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+long long ctpwa_n_events(const ctpwa_handle* h, int kind)
+{
+    if (!h || kind < 0 || kind > 2) return CTPWA_ERR_ARG;
+    return h->eng->nEvents(kind);
+}
+
+int ctpwa_model_json(const ctpwa_handle* h, char* buf, size_t cap)
+{
+    if (!h) return CTPWA_ERR_ARG;
+    return copyOut(ctpwa::modelToJson(h->eng->model()), buf, cap);
+}
+
+size_t ctpwa_device_bytes(const ctpwa_handle* h) { return h ? h->eng->deviceBytes() : 0; }
+
+double ctpwa_jit_seconds(const ctpwa_handle* h) { return h ? h->eng->jitSeconds() : -1.0; }
+
+const char* ctpwa_last_error(const ctpwa_handle* h)
+{
+    if (h) return h->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_create_err.c_str();
+}
+
+int ctpwa_describe(const char* config_path, char* buf, size_t cap, char* err, size_t errlen)
+{
+    try {
+        ctpwa::Config cfg = ctpwa::loadConfig(config_path ? config_path : "config.yml");
+        if (!cfg.valid())
+            throw std::runtime_error("analysis not initialized: invalid or missing config file \"" +
+                                     std::string(config_path ? config_path : "config.yml") + "\"");
+        ctpwa::Model m = ctpwa::buildModel(cfg, 1);
+        for (const auto& b : m.blocks)
+            for (const auto& r : b.res)
+                if (r.type == ctpwa::ModelType::Custom) ctpwa::checkCustomExpr(r.options.at("expr"), r.param_names);
+        return copyOut(ctpwa::modelToJson(m), buf, cap);
+    } catch (const std::exception& e) {
+        std::string m = e.what();
+        setErr(nullptr, CTPWA_ERR_CONFIG, m);
+        if (err && errlen) copyOut(m, err, errlen);
+        return CTPWA_ERR_CONFIG;
+    }
+}
+
+int ctpwa_precompile(const char* config_path, double* seconds, char* err, size_t errlen)
+{
+    try {
+        double s = ctpwa::precompileConfig(config_path ? config_path : "config.yml");
+        if (seconds) *seconds = s;
+    } catch (const std::exception& e) {
+        std::string m = e.what();
+        setErr(nullptr, CTPWA_ERR_CONFIG, m);
+        if (err && errlen) copyOut(m, err, errlen);
+        return m.find("NVRTC") != std::string::npos ? CTPWA_ERR_CUDA : CTPWA_ERR_CONFIG;
+    }
+    return CTPWA_OK;
+}
+
+const char* ctpwa_version(void) { return "ctpwa_b200 0.1.0"; }
+
+}  // extern "C"

@@ -1,0 +1,1160 @@
+// Likelihood engine (see engine.hpp).
+//
+// Per analysis (init):
+//   1. config -> lowered model (model.cpp); samples read (dataio.cpp) and
+//      uploaded; four-momenta transposed to SoA on the device.
+//   2. ag_group_kernel: per event and angular group, the spin-orbit amplitude
+//      tensors are built and contracted into SoA planes [plane][pol][event]
+//      (FP64, plus an FP32 copy for the mixed path), and the per-event
+//      kinematics the lineshapes need (invariant masses, breakup momenta) are
+//      cached.
+//   3. The model-specific fused kernel (kernels/fused_nll.cuh + generated
+//      model.cuh) is compiled with NVRTC for sm_100a (cached on disk).
+// Per evaluation (stream ordered, no host synchronisation, graph capturable):
+//   ct_prepare (couplings) -> fused kernel (one pass over every event of every
+//   sample) -> ct_finalize (deterministic reduction, loss/gradient assembly,
+//   coupling-gradient transform).
+#include "engine.hpp"
+
+#include "angular.cuh"
+
+#include <dlfcn.h>
+#include <nvrtc.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+namespace ctpwa {
+
+#define CT_CUDA(x)                                                                                    \
+    do {                                                                                              \
+        cudaError_t e_ = (x);                                                                         \
+        if (e_ != cudaSuccess)                                                                        \
+            throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " + \
+                                     __FILE__ + ":" + std::to_string(__LINE__));                      \
+    } while (0)
+
+// ============================================================================
+// Host tables: Clebsch-Gordan products, Y_lm norms, Wigner small-d sums.
+// The factorial uses the same scheme as the reference (exact up to 11.5,
+// Stirling with two corrections for integers >= 12, Lanczos otherwise;
+// src/Amplitude.cu:5-98) so that high-spin coefficients agree with it.
+// ============================================================================
+namespace {
+
+double refFactorial(float n)
+{
+    if (n < 0.0f || std::isnan(n)) return 0.0;
+    double r = std::round(n);
+    bool is_int = std::fabs(n - r) < 1e-10;
+    bool is_half = !is_int && std::fabs(n - std::round(2.0 * n) / 2.0) < 1e-10;
+    if (n <= 11.5f && (is_int || is_half)) {
+        if (is_int) {
+            double f = 1.0;
+            for (int i = 2; i <= (int)r; ++i) f *= i;
+            return f;
+        }
+        return std::tgamma((double)n + 1.0);
+    }
+    if (is_int && r >= 12) {
+        int k = (int)r;
+        return std::sqrt(2.0 * M_PI * k) * std::pow(k / M_E, k) * (1.0 + 1.0 / (12.0 * k) + 1.0 / (288.0 * k * k));
+    }
+    // Lanczos approximation (g = 7, 9 published coefficients) of Gamma(n + 1)
+    const double g = 7.0;
+    const double c[9] = {0.99999999999980993, 676.5203681218851,   -1259.1392167224028,
+                         771.32342877765313,  -176.61502916214059, 12.507343278686905,
+                         -0.13857109526572012, 9.9843695780195716e-6, 1.5056327351493116e-7};
+    double x = n - 1.0, a = c[0], t = x + g + 0.5;
+    for (int i = 1; i < 9; ++i) a += c[i] / (x + i);
+    return std::sqrt(2 * M_PI) * std::pow(t, x + 0.5) * std::exp(-t) * a;
+}
+
+// Racah formula for <j1 m1 j2 m2 | J M> (dims 2j+1, m doubled)
+double clebschGordan(int dj1, int m1x2, int dj2, int m2x2, int dJ, int Mx2)
+{
+    float j1 = (dj1 - 1) / 2.0f, j2 = (dj2 - 1) / 2.0f, J = (dJ - 1) / 2.0f;
+    float m1 = m1x2 / 2.0f, m2 = m2x2 / 2.0f, M = Mx2 / 2.0f;
+    if (std::fabs(M - (m1 + m2)) > 1e-10) return 0.0;
+    if (J < std::fabs(j1 - j2) || J > j1 + j2) return 0.0;
+    if (std::fabs(m1) > j1 || std::fabs(m2) > j2 || std::fabs(M) > J) return 0.0;
+    double a = std::sqrt((2.0 * J + 1.0) * refFactorial(j1 + j2 - J) * refFactorial(j1 - j2 + J) *
+                         refFactorial(-j1 + j2 + J) / refFactorial(j1 + j2 + J + 1.0f));
+    double b = std::sqrt(refFactorial(J + M) * refFactorial(J - M) * refFactorial(j1 - m1) * refFactorial(j1 + m1) *
+                         refFactorial(j2 - m2) * refFactorial(j2 + m2));
+    int kmin = (int)std::ceil(std::fmax(0.0, std::fmax(j2 - J - m1, j1 - J + m2)));
+    int kmax = (int)std::floor(std::fmin(j1 + j2 - J, std::fmin(j1 - m1, j2 + m2)));
+    double sum = 0.0;
+    for (int k = kmin; k <= kmax; ++k) {
+        double den = refFactorial((float)k) * refFactorial(j1 + j2 - J - k) * refFactorial(j1 - m1 - k) *
+                     refFactorial(j2 + m2 - k) * refFactorial(J - j2 + m1 + k) * refFactorial(J - j1 - m2 + k);
+        if (std::fabs(den) > 1e-15) sum += ((k % 2 == 0) ? 1.0 : -1.0) / den;
+    }
+    return a * b * sum;
+}
+
+}  // namespace
+
+// ============================================================================
+// Device: angular tensors
+// ============================================================================
+struct V4 {
+    double E, x, y, z;
+};
+
+__device__ __forceinline__ V4 v4add(const V4& a, const V4& b) { return {a.E + b.E, a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ double v4mass(const V4& p)
+{
+    double m2 = p.E * p.E - p.x * p.x - p.y * p.y - p.z * p.z;
+    return m2 < 0 ? 0.0 : sqrt(m2);
+}
+__device__ __forceinline__ double v4p(const V4& p) { return sqrt(p.x * p.x + p.y * p.y + p.z * p.z); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// polar angles and breakup momentum of p1 in the (p1+p2) rest frame
+__device__ void agFrame(const V4& p1, const V4& p2, double& theta, double& phi, double& q)
+{
+    double m1 = v4mass(p1), m2 = v4mass(p2);
+    double dot = p1.E * p2.E - (p1.x * p2.x + p1.y * p2.y + p1.z * p2.z);
+    double m = sqrt(m1 * m1 + m2 * m2 + 2 * dot);
+    double lamb = (2 * m * p1.E + m * m + m1 * m1 - m2 * m2) / (2 * m * (m + p1.E + p2.E));
+    double dm = m1 * m1 - m2 * m2;
+    q = sqrt(m * m * m * m + dm * dm - 2 * m * m * (m1 * m1 + m2 * m2)) / (2 * m);
+    double nx = (p1.x - lamb * (p1.x + p2.x)) / q;
+    double ny = (p1.y - lamb * (p1.y + p2.y)) / q;
+    double nz = (p1.z - lamb * (p1.z + p2.z)) / q;
+    nz = fmax(-1.0, fmin(1.0, nz));
+    theta = acos(nz);
+    phi = atan2(ny, nx);
+}
+
+// associated Legendre P_l^m(x), m >= 0, Condon-Shortley phase
+__device__ double agLegendre(int l, int m, double x)
+{
+    if (m == 0) {
+        if (l == 0) return 1.0;
+        if (l == 1) return x;
+        if (l == 2) return 0.5 * (3.0 * x * x - 1.0);
+        if (l == 3) return 0.5 * (5.0 * x * x * x - 3.0 * x);
+        double a = 1.0, b = x, c = 0.0;
+        for (int k = 2; k <= l; ++k) {
+            c = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
+            a = b;
+            b = c;
+        }
+        return c;
+    }
+    double s = sqrt(1.0 - x * x), pmm = 1.0;
+    for (int i = 1; i <= m; ++i) pmm *= (2 * i - 1) * s;
+    if (m & 1) pmm = -pmm;
+    if (l == m) return pmm;
+    double pm1 = x * (2.0 * m + 1.0) * pmm;
+    if (l == m + 1) return pm1;
+    double a = pmm, b = pm1, c = 0.0;
+    for (int k = m + 2; k <= l; ++k) {
+        c = ((2.0 * k - 1.0) * x * b - (k + m - 1.0) * a) / (k - m);
+        a = b;
+        b = c;
+    }
+    return c;
+}
+
+__device__ __forceinline__ double ipow(double x, int n)
+{
+    double r = 1.0;
+    for (int i = 0; i < n; ++i) r *= x;
+    return r;
+}
+
+// d^j_{m1 m2}(beta) from tabulated sum coefficients [count, (c, a, b)...]
+__device__ double agSmallD(const AgTables& T, int dim, int i1, int i2, double beta)
+{
+    const double* t = T.dcoef + T.doff[(dim * AG_MAXD + i1) * AG_MAXD + i2];
+    int cnt = (int)t[0];
+    double ch = cos(beta / 2.0), sh = sin(beta / 2.0), s = 0.0;
+    for (int k = 0; k < cnt; ++k) s += t[1 + 3 * k] * ipow(ch, (int)t[2 + 3 * k]) * ipow(sh, (int)t[3 + 3 * k]);
+    return s;
+}
+
+// D-matrix element e^{i m1 a} d(b) e^{i m2 g}, m = (dim - 1 - 2 i) / 2
+__device__ void agDMatrix(const AgTables& T, int dim, double a, double b, double g, double2* out)
+{
+    for (int i = 0; i < dim; ++i) {
+        double m1 = (dim - 1 - 2 * i) / 2.0;
+        for (int j = 0; j < dim; ++j) {
+            double m2 = (dim - 1 - 2 * j) / 2.0;
+            double d = agSmallD(T, dim, i, j, b);
+            double s1, c1, s2, c2;
+            sincos(m1 * a, &s1, &c1);
+            sincos(m2 * g, &s2, &c2);
+            out[i * dim + j] = cmul(make_double2(c1 * d, s1 * d), make_double2(c2, s2));
+        }
+    }
+}
+
+__device__ void agMatMul(const double2* a, const double2* b, double2* c, int n)
+{
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            double2 s = make_double2(0, 0);
+            for (int k = 0; k < n; ++k) s = cadd(s, cmul(a[i * n + k], b[k * n + j]));
+            c[i * n + j] = s;
+        }
+}
+
+// Wigner rotation of a massive particle q as seen from P (reference MassiveTrans)
+__device__ __noinline__ void agMassive(const AgTables& T, const V4& P, const V4& q, int dim, double2* tr)
+{
+    for (int i = 0; i < dim * dim; ++i) tr[i] = make_double2(0, 0);
+    for (int i = 0; i < dim; ++i) tr[i * dim + i] = make_double2(1, 0);
+    double hx = P.y * q.z - P.z * q.y, hy = P.z * q.x - P.x * q.z, hz = P.x * q.y - P.y * q.x;
+    if (fabs(hx) < 1e-10 && fabs(hy) < 1e-10 && fabs(hz) < 1e-10) return;
+    double Pp = v4p(P), Pq = v4p(q);
+    double g1 = P.E / v4mass(P), g2 = q.E / v4mass(q);
+    double ca = (P.x * q.x + P.y * q.y + P.z * q.z) / (-1.0 * Pp * Pq);
+    double sa = sqrt(1 - ca * ca);
+    double nrm = sqrt(hx * hx + hy * hy + hz * hz);
+    double th = acos(hz / nrm), ph = atan2(hy / nrm, hx / nrm);
+    double psi = 2.0 * atan2(sa * sqrt((g1 - 1.0) * (g2 - 1.0)),
+                             sqrt((g1 + 1.0) * (g2 + 1.0)) + ca * sqrt((g1 - 1.0) * (g2 - 1.0)));
+    double2 w1[AG_MAXD * AG_MAXD], w2[AG_MAXD * AG_MAXD];
+    agDMatrix(T, dim, -ph, -th, -psi, w1);
+    agDMatrix(T, dim, 0.0, th, ph, w2);
+    agMatMul(w1, w2, tr, dim);
+}
+
+// massless-particle phase rotation (reference MasslessTrans)
+__device__ __noinline__ void agMassless(const V4& P, const V4& p, int dim, double2* tr)
+{
+    for (int i = 0; i < dim * dim; ++i) tr[i] = make_double2(0, 0);
+    for (int i = 0; i < dim; ++i) tr[i * dim + i] = make_double2(1, 0);
+    double PM = v4p(P);
+    if (PM < 1e-10) return;
+    double pm = v4p(p);
+    if (pm < 1e-10) return;
+    double n1x = -P.x / PM, n1y = -P.y / PM, n1z = -P.z / PM;
+    double n2x = p.x / pm, n2y = p.y / pm, n2z = p.z / pm;
+    double b1 = PM / P.E, g1 = 1.0 / sqrt(1.0 - b1 * b1);
+    double sh1 = sqrt((g1 - 1.0) / 2.0), ch1 = sqrt((g1 + 1.0) / 2.0);
+    double dot = n1x * n2x + n1y * n2y + n1z * n2z, cz = n1x * n2y - n1y * n2x;
+    double x12 = sh1 * (dot - n1z) + ch1 * (1.0 - n2z), y12 = sh1 * cz;
+    double x22 = sh1 * (dot + n1z) + ch1 * (1.0 + n2z), y22 = -y12;
+    double tot = -(atan2(y12, x12) + atan2(y22, x22));
+    for (int i = 0; i < dim; ++i) {
+        double m2 = (dim - 1 - 2 * i) / 2.0, s, c;
+        sincos(m2 * tot, &s, &c);
+        tr[i * dim + i] = make_double2(c, s);
+    }
+}
+
+__device__ __noinline__ void agDLeft(const AgTables& T, double2* mat, int dim, double a, double b, double g)
+{
+    double2 d[AG_MAXD * AG_MAXD], t[AG_MAXD * AG_MAXD];
+    agDMatrix(T, dim, a, b, g, d);
+    agMatMul(d, mat, t, dim);
+    for (int i = 0; i < dim * dim; ++i) mat[i] = t[i];
+}
+
+// one decay vertex: amp[s][s1][s2] (x10), reference pwa_amp semantics
+__device__ __noinline__ void agVertex(const AgTables& T, const AgNodeVar& var, const V4& p1, int dj1, const V4& p2, int dj2, int dj,
+                         const double* ylm_norm, double2* amp)
+{
+    double theta, phi, q;
+    agFrame(p1, p2, theta, phi, q);
+    const int L = var.L;
+    const double ql = ipow(q, L);
+    const double x = cos(theta);
+    const double* cg = T.cg + var.cg_off;
+    const int kd = dj1 * dj2;
+    for (int s = 0; s < dj; ++s) {
+        int sx2 = dj - 1 - 2 * s;
+        for (int s1 = 0; s1 < dj1; ++s1) {
+            int s1x2 = dj1 - 1 - 2 * s1;
+            for (int s2 = 0; s2 < dj2; ++s2) {
+                int s2x2 = dj2 - 1 - 2 * s2;
+                double c = cg[s * kd + s1 * dj2 + s2];
+                double2 y = make_double2(0, 0);
+                int m = (sx2 - s1x2 - s2x2) / 2;
+                int am = m < 0 ? -m : m;
+                if (c != 0.0 && am <= L) {
+                    double P = agLegendre(L, am, x);
+                    double a = ylm_norm[L * AG_MAXD + am] * P;
+                    if (m < 0 && (am & 1)) a = -a;
+                    double sn, cs;
+                    sincos(m * (-phi), &sn, &cs);
+                    y = make_double2(a * cs, a * sn);
+                }
+                amp[s * kd + s1 * dj2 + s2] = make_double2(ql * c * y.x, ql * c * y.y);
+            }
+        }
+    }
+    // daughters' Wigner rotations
+    V4 Pt = v4add(p1, p2);
+    double2 t1[AG_MAXD * AG_MAXD], t2[AG_MAXD * AG_MAXD];
+    if (v4mass(p1) > 1e-10) agMassive(T, Pt, p1, dj1, t1);
+    else {
+        agMassless(Pt, p1, dj1, t1);
+        agDLeft(T, t1, dj1, -phi, -theta, 0.0);
+    }
+    if (v4mass(p2) > 1e-10) agMassive(T, Pt, p2, dj2, t2);
+    else {
+        agMassless(Pt, p2, dj2, t2);
+        agDLeft(T, t2, dj2, -(M_PI + phi), -(M_PI - theta), 0.0);
+    }
+    bool trivial = (dj1 == 1 && dj2 == 1);
+    if (!trivial) {
+        double2 mid[AG_MAXT];
+        for (int s = 0; s < dj; ++s) {
+            double2* a = amp + s * kd;
+            for (int n1 = 0; n1 < dj1; ++n1)
+                for (int o2 = 0; o2 < dj2; ++o2) {
+                    double2 sum = make_double2(0, 0);
+                    for (int o1 = 0; o1 < dj1; ++o1) sum = cadd(sum, cmul(t1[n1 + dj1 * o1], a[o1 * dj2 + o2]));
+                    mid[n1 * dj2 + o2] = sum;
+                }
+            for (int n1 = 0; n1 < dj1; ++n1)
+                for (int n2 = 0; n2 < dj2; ++n2) {
+                    double2 sum = make_double2(0, 0);
+                    for (int o2 = 0; o2 < dj2; ++o2) sum = cadd(sum, cmul(mid[n1 * dj2 + o2], t2[n2 + dj2 * o2]));
+                    a[n1 * dj2 + n2] = sum;
+                }
+        }
+    } else {
+        double2 r = cmul(t1[0], t2[0]);
+        if (r.x != 1.0 || r.y != 0.0)
+            for (int s = 0; s < dj; ++s) amp[s] = cmul(r, amp[s]);
+    }
+    for (int i = 0; i < dj * kd; ++i) amp[i] = make_double2(amp[i].x * 10.0, amp[i].y * 10.0);
+}
+
+__global__ void ag_transpose_kernel(const double* __restrict__ aos, double* __restrict__ soa, long long n, int nfin)
+{
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    for (int k = 0; k < nfin * 4; ++k) soa[(long long)k * n + e] = aos[e * nfin * 4 + k];
+}
+
+__global__ void __launch_bounds__(128) ag_group_kernel(AgGroup G, AgTables T, const double* __restrict__ p4, long long n,
+                                                       double2* __restrict__ out64, float2* __restrict__ out32,
+                                                       double* __restrict__ kin)
+{
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    V4 mom[AG_MAXP];
+    V4 parent = {0, 0, 0, 0};
+    for (int f = 0; f < G.nfin; ++f) {
+        V4 pf = {p4[(long long)(4 * f) * n + e], p4[(long long)(4 * f + 1) * n + e], p4[(long long)(4 * f + 2) * n + e],
+                 p4[(long long)(4 * f + 3) * n + e]};
+        parent = v4add(parent, pf);
+    }
+    for (int k = 0; k < G.np; ++k) {
+        int idx = G.build_order[k];
+        int s = G.input_slot[idx];
+        if (s >= 0)
+            mom[idx] = {p4[(long long)(4 * s) * n + e], p4[(long long)(4 * s + 1) * n + e], p4[(long long)(4 * s + 2) * n + e],
+                        p4[(long long)(4 * s + 3) * n + e]};
+        else if (s == -1) mom[idx] = parent;
+        else mom[idx] = v4add(mom[G.sum_a[idx]], mom[G.sum_b[idx]]);
+    }
+    // kinematic cache
+    for (int k = 0; k < G.nkin; ++k) {
+        const int* d = G.kin + 5 * k;
+        const V4& a = mom[d[1]];
+        double val = 0.0;
+        switch (d[0]) {
+        case AG_K_MASS: val = v4mass(a); break;
+        case AG_K_Q: {
+            double m = v4mass(a), m1 = v4mass(mom[d[2]]), m2 = v4mass(mom[d[3]]);
+            double q2 = (m * m - (m1 + m2) * (m1 + m2)) * (m * m - (m1 - m2) * (m1 - m2));
+            val = q2 <= 0.0 ? 0.0 : sqrt(q2) / (2.0 * m);
+            break;
+        }
+        case AG_K_QRAW: {
+            double m = v4mass(a), m1 = v4mass(mom[d[2]]), m2 = v4mass(mom[d[3]]);
+            val = sqrt((m * m - (m1 + m2) * (m1 + m2)) * (m * m - (m1 - m2) * (m1 - m2))) / 2 / m;
+            break;
+        }
+        case AG_K_P: val = v4p(a); break;
+        case AG_K_E: val = a.E; break;
+        case AG_K_CT: {
+            double pp = v4p(a);
+            val = pp > 0 ? a.z / pp : 0.0;
+            break;
+        }
+        case AG_K_PHI: val = atan2(a.y, a.x); break;
+        }
+        kin[(long long)d[4] * n + e] = val;
+    }
+    // spin-orbit tensors and chain contraction
+    double2 cur[AG_MAXT], nxt[AG_MAXT], node[AG_MAXT];
+    int shape[AG_MAXN + 2], labels[AG_MAXN + 2];
+    for (int s = 0; s < G.nsl; ++s) {
+        int rank = 0;
+        for (int ni = 0; ni < G.nnodes; ++ni) {
+            const AgNode& nd = G.nodes[ni];
+            const AgNodeVar& var = T.vars[nd.var_off + G.sl_var[s * G.nnodes + ni]];
+            agVertex(T, var, mom[nd.d1], nd.dj1, mom[nd.d2], nd.dj2, nd.dj, T.ylm_norm, ni == 0 ? cur : node);
+            if (ni == 0) {
+                shape[0] = nd.dj;
+                shape[1] = nd.dj1;
+                shape[2] = nd.dj2;
+                labels[0] = nd.mother;
+                labels[1] = nd.d1;
+                labels[2] = nd.d2;
+                rank = 3;
+                continue;
+            }
+            int c = 0;
+            for (int j = 0; j < rank; ++j)
+                if (labels[j] == nd.mother) {
+                    c = j;
+                    break;
+                }
+            // strides of cur
+            int st[AG_MAXN + 2];
+            st[rank - 1] = 1;
+            for (int j = rank - 2; j >= 0; --j) st[j] = st[j + 1] * shape[j + 1];
+            int oshape[AG_MAXN + 2], ro = 0;
+            for (int j = 0; j < rank; ++j)
+                if (j != c) oshape[ro++] = shape[j];
+            oshape[ro++] = nd.dj1;
+            oshape[ro++] = nd.dj2;
+            int total = 1;
+            for (int j = 0; j < ro; ++j) total *= oshape[j];
+            for (int idx = 0; idx < total; ++idx) {
+                int t = idx, ic[AG_MAXN + 2];
+                for (int j = ro - 1; j >= 0; --j) {
+                    ic[j] = t % oshape[j];
+                    t /= oshape[j];
+                }
+                int base = 0, pos = 0;
+                for (int j = 0; j < rank; ++j)
+                    if (j != c) base += ic[pos++] * st[j];
+                int e1 = ic[ro - 2], e2 = ic[ro - 1];
+                double2 sum = make_double2(0, 0);
+                for (int sg = 0; sg < shape[c]; ++sg)
+                    sum = cadd(sum, cmul(cur[base + sg * st[c]], node[(sg * nd.dj1 + e1) * nd.dj2 + e2]));
+                nxt[idx] = sum;
+            }
+            for (int i = 0; i < total; ++i) cur[i] = nxt[i];
+            for (int j = 0; j < ro; ++j) shape[j] = oshape[j];
+            for (int j = c; j < rank - 1; ++j) labels[j] = labels[j + 1];
+            labels[rank - 1] = nd.d1;
+            labels[rank] = nd.d2;
+            rank = ro;
+        }
+        const long long plane = (long long)(G.plane0 + s) * G.npol;
+        for (int p = 0; p < G.npol; ++p) {
+            double2 v = G.pol_map ? cur[G.pol_map[p]] : cur[p];
+            out64[(plane + p) * n + e] = v;
+            if (out32) out32[(plane + p) * n + e] = make_float2((float)v.x, (float)v.y);
+        }
+    }
+}
+
+// ============================================================================
+// Device: per-evaluation prologue / epilogue
+// ============================================================================
+
+// v[a] = ratio[a] * p[chain[a]], params = [Re p (nc), Im p (nc), theta]
+__global__ void ct_prepare_kernel(const double* __restrict__ params, const int* __restrict__ chain,
+                                  const double* __restrict__ ratio, int nA, int nc, double* __restrict__ v)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nA) return;
+    int c = chain[a];
+    v[2 * a] = params[c] * ratio[a];
+    v[2 * a + 1] = params[nc + c] * ratio[a];
+}
+
+struct FinalizeArgs {
+    const double* partials;
+    int nacc, nA, nc, nT;
+    int cta[3][2];  // per sample kind: begin, count
+    int has[3];
+    double n_phsp, W_data, W_bkg;
+    const double* params;
+    const double* v;
+    const int* chain;
+    const int* gauss_idx;
+    const double* gauss_ms;
+    int ngauss;
+    double* out_nll;
+    double* out_grad;
+    double* out_parts;
+};
+
+// One CTA: deterministic column sums of the CTA partials, then loss/gradient
+// assembly (src/Analysis.cu:1134-1183) and the coupling-gradient transform
+// dL/dp_c = (1/p_c) sum_{a in c} conj(g_a) v_a (src/AmpGen.cu:3581-3637).
+__global__ void __launch_bounds__(256) ct_finalize_kernel(FinalizeArgs A)
+{
+    extern __shared__ double sh[];  // [3][nacc] sample sums, then gv [2 nA], gt [nT]
+    double* sums = sh;
+    for (int i = threadIdx.x; i < 3 * A.nacc; i += blockDim.x) {
+        int k = i / A.nacc, j = i % A.nacc;
+        double s = 0.0;
+        if (A.has[k])
+            for (int b = 0; b < A.cta[k][1]; ++b) s += A.partials[(long long)(A.cta[k][0] + b) * A.nacc + j];
+        sums[i] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const double* P = sums;               // phase space
+    const double* Dd = sums + A.nacc;     // data
+    const double* B = sums + 2 * A.nacc;  // background
+    double pf = A.n_phsp > 0 ? P[1] / A.n_phsp : 0.0;
+    if (pf <= 1e-30 || isnan(pf) || isinf(pf)) pf = 1e-30;
+    double Weff = A.W_data - A.W_bkg;
+    double loss = Dd[0] - B[0] + Weff * log(pf);
+    const double* theta = A.params + 2 * A.nc;
+    for (int g = 0; g < A.ngauss; ++g) {
+        double dl = theta[A.gauss_idx[g]] - A.gauss_ms[2 * g];
+        loss += dl * dl / (2.0 * A.gauss_ms[2 * g + 1] * A.gauss_ms[2 * g + 1]);
+    }
+    bool reset = isnan(loss) || isinf(loss);
+    if (reset) loss = 1e30;
+    double* gv = sums + 3 * A.nacc;
+    for (int a = 0; a < A.nA; ++a) {
+        double r = Dd[2 + 2 * a] - B[2 + 2 * a] + (Weff / pf) * P[2 + 2 * a];
+        double i = Dd[3 + 2 * a] - B[3 + 2 * a] + (Weff / pf) * P[3 + 2 * a];
+        gv[2 * a] = reset ? 0.0 : r;
+        gv[2 * a + 1] = reset ? 0.0 : i;
+    }
+    for (int c = 0; c < A.nc; ++c) {
+        double sr = 0.0, si = 0.0;
+        for (int a = 0; a < A.nA; ++a) {
+            if (A.chain[a] != c) continue;
+            double gr = gv[2 * a], gi = gv[2 * a + 1], vr = A.v[2 * a], vi = A.v[2 * a + 1];
+            sr += gr * vr + gi * vi;
+            si += gr * vi - gi * vr;
+        }
+        double pr = A.params[c], pi = A.params[A.nc + c];
+        double ps = pr * pr + pi * pi;
+        if (ps < 1e-30) ps = 1e-30;
+        A.out_grad[c] = 2.0 * (sr * pr + si * pi) / ps;
+        A.out_grad[A.nc + c] = -2.0 * (si * pr - sr * pi) / ps;
+    }
+    for (int j = 0; j < A.nT; ++j) {
+        double g = Dd[2 + 2 * A.nA + j] - B[2 + 2 * A.nA + j] + (Weff / (pf * A.n_phsp)) * P[2 + 2 * A.nA + j];
+        A.out_grad[2 * A.nc + j] = reset ? 0.0 : g;
+    }
+    if (!reset)
+        for (int g = 0; g < A.ngauss; ++g) {
+            int j = A.gauss_idx[g];
+            A.out_grad[2 * A.nc + j] += (theta[j] - A.gauss_ms[2 * g]) / (A.gauss_ms[2 * g + 1] * A.gauss_ms[2 * g + 1]);
+        }
+    *A.out_nll = loss;
+    if (A.out_parts) {
+        A.out_parts[0] = Dd[0];
+        A.out_parts[1] = B[0];
+        A.out_parts[2] = P[1];
+        A.out_parts[3] = A.W_data;
+        A.out_parts[4] = A.W_bkg;
+        A.out_parts[5] = A.n_phsp;
+    }
+}
+
+// ============================================================================
+// Host: engine
+// ============================================================================
+namespace {
+
+std::string readFile(const std::string& p)
+{
+    std::ifstream f(p, std::ios::binary);
+    if (!f) throw std::runtime_error("cannot read " + p);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return ss.str();
+}
+
+std::string kernelDir()
+{
+    const char* e = std::getenv("CTPWA_B200_KERNEL_DIR");
+    if (e && *e) return e;
+    // next to this library: <pkg>/csrc/kernels
+    Dl_info info;
+    if (dladdr((void*)&kernelDir, &info) && info.dli_fname) {
+        std::filesystem::path p = std::filesystem::path(info.dli_fname).parent_path() / "csrc" / "kernels";
+        if (std::filesystem::exists(p)) return p.string();
+    }
+    return "ctpwa_b200/csrc/kernels";
+}
+
+uint64_t fnv1a(const std::string& s)
+{
+    uint64_t h = 1469598103934665603ULL;
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+std::string cacheDir()
+{
+    const char* e = std::getenv("CTPWA_JIT_CACHE_DIR");
+    if (e && *e) return e;
+    // next to this library (travels with the package), else the user cache
+    Dl_info info;
+    if (dladdr((void*)&cacheDir, &info) && info.dli_fname) {
+        std::filesystem::path p = std::filesystem::path(info.dli_fname).parent_path() / "_jitcache";
+        std::error_code ec;
+        std::filesystem::create_directories(p, ec);
+        if (!ec && access(p.c_str(), W_OK) == 0) return p.string();
+    }
+    const char* home = std::getenv("HOME");
+    return std::string(home ? home : "/tmp") + "/.cache/ctpwa_b200_jit";
+}
+
+}  // namespace
+
+Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(opt)
+{
+    Config cfg = loadConfig(config_path);
+    if (!cfg.valid()) {
+        std::string w = cfg.warnings.empty() ? "" : (": " + cfg.warnings.front());
+        throw std::runtime_error("analysis not initialized: invalid or missing config file \"" + config_path + "\"" + w);
+    }
+    model_ = buildModel(cfg, 1);
+    if (model_.nAmp() == 0) throw std::runtime_error("the configuration defines no amplitudes");
+    for (const auto& b : model_.blocks)
+        for (const auto& r : b.res)
+            if (r.type == ModelType::Custom) checkCustomExpr(r.options.at("expr"), r.param_names);
+    gen_ = generateModel(model_);
+    int ndev = 0;
+    CT_CUDA(cudaGetDeviceCount(&ndev));
+    if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
+    CT_CUDA(cudaSetDevice(opt_.device));
+    compileKernel();
+    loadSamples();
+    buildTables();
+    for (int k = 0; k < 3; ++k)
+        if (samples_[k].n > 0 || k < 2) computeAngular(k);
+    // evaluation buffers
+    int nA = model_.nAmp();
+    CT_CUDA(cudaMalloc(&d_v_, sizeof(double) * 2 * nA));
+    std::vector<double> ratio = model_.coupling.ratio;
+    CT_CUDA(cudaMalloc(&d_amp_chain_, sizeof(int) * nA));
+    CT_CUDA(cudaMalloc(&d_ratio_, sizeof(double) * nA));
+    CT_CUDA(cudaMemcpy(d_amp_chain_, model_.coupling.amp_chain.data(), sizeof(int) * nA, cudaMemcpyHostToDevice));
+    CT_CUDA(cudaMemcpy(d_ratio_, ratio.data(), sizeof(double) * nA, cudaMemcpyHostToDevice));
+    int ng = (int)model_.gauss.size();
+    CT_CUDA(cudaMalloc(&d_gauss_idx_, sizeof(int) * std::max(1, ng)));
+    CT_CUDA(cudaMalloc(&d_gauss_ms_, sizeof(double) * 2 * std::max(1, ng)));
+    if (ng) {
+        std::vector<int> gi;
+        std::vector<double> gm;
+        for (const auto& g : model_.gauss) {
+            gi.push_back(g.first);
+            gm.push_back(g.second.first);
+            gm.push_back(g.second.second);
+        }
+        CT_CUDA(cudaMemcpy(d_gauss_idx_, gi.data(), sizeof(int) * ng, cudaMemcpyHostToDevice));
+        CT_CUDA(cudaMemcpy(d_gauss_ms_, gm.data(), sizeof(double) * 2 * ng, cudaMemcpyHostToDevice));
+    }
+    // grid: CTAs per sample proportional to its size, multiple of the SM count
+    int sms = 148;
+    CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    long long tot = 0;
+    for (int k = 0; k < 3; ++k) tot += samples_[k].n;
+    int target = sms * 8;
+    int begin = 0;
+    for (int k = 0; k < 3; ++k) {
+        int cnt = 0;
+        if (samples_[k].n > 0) {
+            long long want = (long long)std::ceil((double)target * samples_[k].n / std::max(1LL, tot));
+            long long maxc = (samples_[k].n + 255) / 256;
+            cnt = (int)std::max(1LL, std::min(want, maxc));
+        }
+        cta_[k][0] = begin;
+        cta_[k][1] = cnt;
+        begin += cnt;
+    }
+    grid_ = std::max(1, begin);
+    int nacc = 2 + 2 * nA + model_.nTheta();
+    CT_CUDA(cudaMalloc(&d_partials_, sizeof(double) * (size_t)grid_ * nacc));
+    CT_CUDA(cudaMalloc(&d_parts_, sizeof(double) * 8));
+    CT_CUDA(cudaDeviceSynchronize());
+}
+
+Engine::~Engine()
+{
+    for (auto& s : samples_) {
+        cudaFree(s.p4);
+        cudaFree(s.slamp64);
+        cudaFree(s.slamp32);
+        cudaFree(s.kin);
+        cudaFree(s.w);
+    }
+    cudaFree(d_ag_tables_);
+    cudaFree(d_v_);
+    cudaFree(d_partials_);
+    cudaFree(d_parts_);
+    cudaFree(d_amp_chain_);
+    cudaFree(d_ratio_);
+    cudaFree(d_gauss_idx_);
+    cudaFree(d_gauss_ms_);
+    if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
+}
+
+void Engine::loadSamples()
+{
+    const char* kinds[3] = {"phsp", "data", "bkg"};
+    const char* wkeys[3] = {"phsp_weights", "data_weights", "bkg_weights"};
+    int nfin = (int)model_.final_order.size();
+    for (int k = 0; k < 3; ++k) {
+        auto it = model_.cfg.data_files.find(kinds[k]);
+        if (it == model_.cfg.data_files.end()) {
+            if (k < 2) throw std::runtime_error(std::string("config has no Data.") + kinds[k] + " entry");
+            continue;
+        }
+        Sample s = readSample(it->second, nfin);
+        DeviceSample& d = samples_[k];
+        d.n = s.n;
+        if (k == 2) has_bkg_ = true;
+        std::vector<double> w;
+        auto wi = model_.cfg.data_files.find(wkeys[k]);
+        if (wi != model_.cfg.data_files.end() && (k != 2 || has_bkg_)) w = readWeights(wi->second, s.n);
+        d.wsum = 0.0;
+        if (w.empty()) d.wsum = (double)s.n;
+        else
+            for (double x : w) d.wsum += x;
+        if (s.n == 0) continue;
+        size_t bytes = sizeof(double) * (size_t)s.n * nfin * 4;
+        double* tmp = nullptr;
+        CT_CUDA(cudaMalloc(&tmp, bytes));
+        CT_CUDA(cudaMemcpy(tmp, s.p4.data(), bytes, cudaMemcpyHostToDevice));
+        CT_CUDA(cudaMalloc(&d.p4, bytes));
+        ag_transpose_kernel<<<(unsigned)((s.n + 255) / 256), 256>>>(tmp, d.p4, s.n, nfin);
+        CT_CUDA(cudaGetLastError());
+        CT_CUDA(cudaDeviceSynchronize());
+        CT_CUDA(cudaFree(tmp));
+        if (!w.empty()) {
+            CT_CUDA(cudaMalloc(&d.w, sizeof(double) * s.n));
+            CT_CUDA(cudaMemcpy(d.w, w.data(), sizeof(double) * s.n, cudaMemcpyHostToDevice));
+        }
+        device_bytes_ += bytes + (w.empty() ? 0 : sizeof(double) * s.n);
+    }
+}
+
+void Engine::buildTables()
+{
+    // Layout of one device allocation: vars | cg | ylm_norm | dcoef | doff | per-group (sl_var, pol_map, kin)
+    std::vector<AgNodeVar> vars;
+    std::vector<double> cg;
+    std::vector<double> ylm(AG_MAXD * AG_MAXD, 0.0);
+    for (int l = 0; l < AG_MAXD; ++l)
+        for (int am = 0; am <= l; ++am)
+            ylm[l * AG_MAXD + am] = (l == 0) ? 0.5 * std::sqrt(1.0 / M_PI)
+                                             : std::sqrt((2.0 * l + 1.0) * refFactorial((float)(l - am)) /
+                                                         (4.0 * M_PI * refFactorial((float)(l + am))));
+    std::vector<double> dcoef;
+    std::vector<int> doff((AG_MAXD + 1) * AG_MAXD * AG_MAXD, 0);
+    for (int dim = 1; dim <= AG_MAXD; ++dim) {
+        float j = (dim - 1) / 2.0f;
+        for (int i1 = 0; i1 < dim; ++i1)
+            for (int i2 = 0; i2 < dim; ++i2) {
+                float m1 = (dim - 1 - 2 * i1) / 2.0f, m2 = (dim - 1 - 2 * i2) / 2.0f;
+                doff[(dim * AG_MAXD + i1) * AG_MAXD + i2] = (int)dcoef.size();
+                size_t cnt_pos = dcoef.size();
+                dcoef.push_back(0.0);
+                int kmin = (m1 < m2) ? 0 : (int)(m1 - m2);
+                int kmax = (m1 > -m2) ? (int)(j - m2) : (int)(j + m1);
+                int cnt = 0;
+                for (int k = kmin; k <= kmax; ++k) {
+                    double num = refFactorial(j + m2) * refFactorial(j - m2) * refFactorial(j + m1) * refFactorial(j - m1);
+                    double den = refFactorial((float)k) * refFactorial(j - m2 - k) * refFactorial(j + m1 - k) *
+                                 refFactorial(k - m1 + m2);
+                    double c = std::pow(-1.0, k - m1 + m2) * std::sqrt(num) / den;
+                    dcoef.push_back(c);
+                    dcoef.push_back(2 * j + m1 - m2 - 2 * k);
+                    dcoef.push_back(2 * k - m1 + m2);
+                    ++cnt;
+                }
+                dcoef[cnt_pos] = cnt;
+            }
+    }
+    // per-group node variants and CG products
+    struct GroupHost {
+        AgGroup g;
+        std::vector<int> sl_var, pol_map, kin;
+    };
+    std::vector<GroupHost> gh(model_.groups.size());
+    for (size_t gi = 0; gi < model_.groups.size(); ++gi) {
+        const Group& G = model_.groups[gi];
+        GroupHost& H = gh[gi];
+        AgGroup& A = H.g;
+        std::memset(&A, 0, sizeof(A));
+        if ((int)G.particle_names.size() > AG_MAXP || (int)G.nodes.size() > AG_MAXN)
+            throw std::runtime_error("decay chain too large for the angular kernel");
+        A.np = (int)G.particle_names.size();
+        A.nfin = (int)model_.final_order.size();
+        A.nnodes = (int)G.nodes.size();
+        A.nsl = G.nSL();
+        A.npol = model_.npol;
+        A.tensor_size = G.tensor_size;
+        A.plane0 = gen_.group_plane0[gi];
+        for (int i = 0; i < A.np; ++i) {
+            A.input_slot[i] = G.input_slot[i];
+            A.sum_a[i] = G.sum_of[i].first;
+            A.sum_b[i] = G.sum_of[i].second;
+            A.build_order[i] = G.build_order[i];
+        }
+        for (size_t ni = 0; ni < G.nodes.size(); ++ni) {
+            const ModelNode& n = G.nodes[ni];
+            if (n.dj > AG_MAXD || n.dj1 > AG_MAXD || n.dj2 > AG_MAXD || n.dj * n.dj1 * n.dj2 > AG_MAXT)
+                throw std::runtime_error("spin too large for the angular kernel (2J+1 <= 7, vertex tensor <= 64)");
+            AgNode& an = A.nodes[ni];
+            an.mother = n.mother;
+            an.d1 = n.d1;
+            an.d2 = n.d2;
+            an.dj = n.dj;
+            an.dj1 = n.dj1;
+            an.dj2 = n.dj2;
+            an.var_off = (int)vars.size();
+            an.nvar = (int)n.sls.size();
+            for (const auto& sl : n.sls) {
+                AgNodeVar v;
+                v.S = sl.S;
+                v.L = sl.L;
+                v.cg_off = (int)cg.size();
+                if (sl.L >= AG_MAXD) throw std::runtime_error("orbital angular momentum too large for the angular kernel");
+                for (int s = 0; s < n.dj; ++s)
+                    for (int s1 = 0; s1 < n.dj1; ++s1)
+                        for (int s2 = 0; s2 < n.dj2; ++s2) {
+                            int sx2 = n.dj - 1 - 2 * s, s1x2 = n.dj1 - 1 - 2 * s1, s2x2 = n.dj2 - 1 - 2 * s2;
+                            double c1 = clebschGordan(n.dj1, s1x2, n.dj2, s2x2, sl.S, s1x2 + s2x2);
+                            double c2 = clebschGordan(sl.S, s1x2 + s2x2, 2 * sl.L + 1, sx2 - s1x2 - s2x2, n.dj, sx2);
+                            cg.push_back(c1 * c2 / std::sqrt((double)n.dj));
+                        }
+                vars.push_back(v);
+            }
+        }
+        // contraction size check
+        {
+            int cur = G.nodes[0].dj * G.nodes[0].dj1 * G.nodes[0].dj2;
+            if (cur > AG_MAXT) throw std::runtime_error("amplitude tensor too large for the angular kernel");
+            std::vector<int> shape = {G.nodes[0].dj, G.nodes[0].dj1, G.nodes[0].dj2};
+            std::vector<int> labels = {G.nodes[0].mother, G.nodes[0].d1, G.nodes[0].d2};
+            for (size_t ni = 1; ni < G.nodes.size(); ++ni) {
+                const auto& n = G.nodes[ni];
+                auto it = std::find(labels.begin(), labels.end(), n.mother);
+                size_t c = it - labels.begin();
+                shape.erase(shape.begin() + c);
+                labels.erase(it);
+                shape.push_back(n.dj1);
+                shape.push_back(n.dj2);
+                labels.push_back(n.d1);
+                labels.push_back(n.d2);
+                int t = 1;
+                for (int x : shape) t *= x;
+                if (t > AG_MAXT) throw std::runtime_error("amplitude tensor too large for the angular kernel");
+            }
+        }
+        for (int s = 0; s < G.nSL(); ++s)
+            for (size_t ni = 0; ni < G.nodes.size(); ++ni) H.sl_var.push_back(G.sl_combs[s][ni]);
+        H.pol_map = model_.pol_map;
+        for (size_t k = 0; k < gen_.slots.size(); ++k) {
+            const KinSlot& ks = gen_.slots[k];
+            if (ks.group != (int)gi) continue;
+            H.kin.insert(H.kin.end(), {ks.type, ks.a, ks.b, ks.c, (int)k});
+        }
+        A.nkin = (int)H.kin.size() / 5;
+    }
+    // pack everything into one allocation
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t off = 0;
+    size_t o_vars = off;
+    off = align(off + vars.size() * sizeof(AgNodeVar));
+    size_t o_cg = off;
+    off = align(off + cg.size() * sizeof(double));
+    size_t o_ylm = off;
+    off = align(off + ylm.size() * sizeof(double));
+    size_t o_dc = off;
+    off = align(off + dcoef.size() * sizeof(double));
+    size_t o_doff = off;
+    off = align(off + doff.size() * sizeof(int));
+    std::vector<size_t> o_slv(gh.size()), o_pm(gh.size()), o_kin(gh.size());
+    for (size_t g = 0; g < gh.size(); ++g) {
+        o_slv[g] = off;
+        off = align(off + gh[g].sl_var.size() * sizeof(int) + 4);
+        o_pm[g] = off;
+        off = align(off + gh[g].pol_map.size() * sizeof(int) + 4);
+        o_kin[g] = off;
+        off = align(off + gh[g].kin.size() * sizeof(int) + 4);
+    }
+    std::vector<char> img(off, 0);
+    std::memcpy(img.data() + o_vars, vars.data(), vars.size() * sizeof(AgNodeVar));
+    std::memcpy(img.data() + o_cg, cg.data(), cg.size() * sizeof(double));
+    std::memcpy(img.data() + o_ylm, ylm.data(), ylm.size() * sizeof(double));
+    std::memcpy(img.data() + o_dc, dcoef.data(), dcoef.size() * sizeof(double));
+    std::memcpy(img.data() + o_doff, doff.data(), doff.size() * sizeof(int));
+    for (size_t g = 0; g < gh.size(); ++g) {
+        std::memcpy(img.data() + o_slv[g], gh[g].sl_var.data(), gh[g].sl_var.size() * sizeof(int));
+        std::memcpy(img.data() + o_pm[g], gh[g].pol_map.data(), gh[g].pol_map.size() * sizeof(int));
+        std::memcpy(img.data() + o_kin[g], gh[g].kin.data(), gh[g].kin.size() * sizeof(int));
+    }
+    CT_CUDA(cudaMalloc(&d_ag_tables_, off));
+    CT_CUDA(cudaMemcpy(d_ag_tables_, img.data(), off, cudaMemcpyHostToDevice));
+    char* base = (char*)d_ag_tables_;
+    AgTables T;
+    T.vars = (const AgNodeVar*)(base + o_vars);
+    T.cg = (const double*)(base + o_cg);
+    T.ylm_norm = (const double*)(base + o_ylm);
+    T.dcoef = (const double*)(base + o_dc);
+    T.doff = (const int*)(base + o_doff);
+    ag_host_.assign((char*)&T, (char*)&T + sizeof(T));
+    group_desc_.clear();
+    for (size_t g = 0; g < gh.size(); ++g) {
+        AgGroup A = gh[g].g;
+        A.sl_var = (const int*)(base + o_slv[g]);
+        A.pol_map = gh[g].pol_map.empty() ? nullptr : (const int*)(base + o_pm[g]);
+        A.kin = (const int*)(base + o_kin[g]);
+        group_desc_.emplace_back((char*)&A, (char*)&A + sizeof(A));
+    }
+}
+
+void Engine::computeAngular(int kind)
+{
+    DeviceSample& d = samples_[kind];
+    long long n = d.n;
+    int npol = model_.npol;
+    size_t nplanes = (size_t)gen_.nplane * npol;
+    size_t b64 = sizeof(double2) * nplanes * std::max(1LL, n);
+    CT_CUDA(cudaMalloc(&d.slamp64, b64));
+    device_bytes_ += b64;
+    if (opt_.mixed_tables) {
+        CT_CUDA(cudaMalloc(&d.slamp32, b64 / 2));
+        device_bytes_ += b64 / 2;
+    }
+    size_t bk = sizeof(double) * std::max<size_t>(1, gen_.slots.size()) * std::max(1LL, n);
+    CT_CUDA(cudaMalloc(&d.kin, bk));
+    device_bytes_ += bk;
+    if (n == 0) return;
+    AgTables T;
+    std::memcpy(&T, ag_host_.data(), sizeof(T));
+    for (size_t g = 0; g < group_desc_.size(); ++g) {
+        AgGroup G;
+        std::memcpy(&G, group_desc_[g].data(), sizeof(G));
+        ag_group_kernel<<<(unsigned)((n + 127) / 128), 128>>>(G, T, d.p4, n, d.slamp64, d.slamp32, d.kin);
+        CT_CUDA(cudaGetLastError());
+    }
+    CT_CUDA(cudaDeviceSynchronize());
+    if (!opt_.keep_momenta) {
+        CT_CUDA(cudaFree(d.p4));
+        d.p4 = nullptr;
+    }
+}
+
+// NVRTC compile of the fused kernel for one generated model, with a disk cache
+// keyed by the FNV-1a hash of all sources, options and the NVRTC version.
+std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
+{
+    std::string dir = kernelDir();
+    std::string jet = readFile(dir + "/jet.cuh");
+    std::string ls = readFile(dir + "/lineshapes.cuh");
+    std::string fused = readFile(dir + "/fused_nll.cuh");
+    std::string src = "#include \"fused_nll.cuh\"\n";
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
+                          "--fmad=true", "-lineinfo"};
+    const int nopts = 6;
+    std::string key_src = jet + ls + fused + gen.header;
+    for (int i = 0; i < nopts; ++i) key_src += opts[i];
+    int nvmaj = 0, nvmin = 0;
+    nvrtcVersion(&nvmaj, &nvmin);
+    key_src += std::to_string(nvmaj) + "." + std::to_string(nvmin);
+    char key[32];
+    std::snprintf(key, sizeof key, "%016llx", (unsigned long long)fnv1a(key_src));
+    std::string cpath = cacheDir() + "/" + key + ".cubin";
+    std::string cubin;
+    {
+        std::ifstream f(cpath, std::ios::binary);
+        if (f) {
+            std::stringstream ss;
+            ss << f.rdbuf();
+            cubin = ss.str();
+        }
+    }
+    if (cache_hit) *cache_hit = !cubin.empty();
+    if (!cubin.empty()) return cubin;
+    const char* hdr_src[] = {jet.c_str(), ls.c_str(), fused.c_str(), gen.header.c_str()};
+    const char* hdr_names[] = {"jet.cuh", "lineshapes.cuh", "fused_nll.cuh", "model.cuh"};
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, src.c_str(), "ctpwa_fused.cu", 4, hdr_src, hdr_names) != NVRTC_SUCCESS)
+        throw std::runtime_error("NVRTC: program creation failed");
+    nvrtcResult r = nvrtcCompileProgram(prog, nopts, opts);
+    if (r != NVRTC_SUCCESS) {
+        size_t ls2 = 0;
+        nvrtcGetProgramLogSize(prog, &ls2);
+        std::string log(ls2, '\0');
+        nvrtcGetProgramLog(prog, &log[0]);
+        nvrtcDestroyProgram(&prog);
+        throw std::runtime_error("NVRTC compile of the fused kernel failed:\n" + log.substr(0, 4000));
+    }
+    size_t n = 0;
+    nvrtcGetCUBINSize(prog, &n);
+    cubin.resize(n);
+    nvrtcGetCUBIN(prog, &cubin[0]);
+    nvrtcDestroyProgram(&prog);
+    std::error_code ec;
+    std::filesystem::create_directories(cacheDir(), ec);
+    std::string tmpp = cpath + ".tmp" + std::to_string((long long)getpid());
+    {
+        std::ofstream f(tmpp, std::ios::binary);
+        f.write(cubin.data(), (std::streamsize)cubin.size());
+    }
+    std::filesystem::rename(tmpp, cpath, ec);
+    return cubin;
+}
+
+void Engine::compileKernel()
+{
+    auto t0 = std::chrono::steady_clock::now();
+    std::string cubin = jitCubin(gen_, &jit_cache_hit_);
+    cudaLibrary_t lib;
+    CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+    lib_ = (void*)lib;
+    cudaKernel_t k64, kmx, kin;
+    CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
+    CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
+    CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
+    k_f64_ = (void*)k64;
+    k_mixed_ = (void*)kmx;
+    k_int_ = (void*)kin;
+    jit_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+double precompileConfig(const std::string& config_path)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    Config cfg = loadConfig(config_path);
+    if (!cfg.valid()) throw std::runtime_error("analysis not initialized: invalid or missing config file \"" + config_path + "\"");
+    Model m = buildModel(cfg, 1);
+    GeneratedModel g = generateModel(m);
+    bool hit = false;
+    jitCubin(g, &hit);
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// argument block of the fused kernel (must match CtArgs in kernels/fused_nll.cuh)
+struct CtSampleH {
+    const void* slamp;
+    const double* kin;
+    const double* w;
+    long long n;
+    int kind;
+    int cta_begin;
+    int cta_count;
+    int pad;
+    double vw_scale;
+};
+struct CtArgsH {
+    CtSampleH s[3];
+    int nsamp;
+    int pad;
+    const double* theta;
+    const double* v;
+    double* partials;
+};
+
+void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
+{
+    const Model& m = model_;
+    int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    int ns = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (cta_[k][1] == 0) continue;
+        CtSampleH& s = a.s[ns++];
+        const DeviceSample& d = samples_[k];
+        s.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
+        s.kin = d.kin;
+        s.w = d.w;
+        s.n = d.n;
+        s.kind = k;
+        s.cta_begin = cta_[k][0];
+        s.cta_count = cta_[k][1];
+        s.vw_scale = 1.0 / (samples_[0].wsum > 0 ? samples_[0].wsum : 1.0);
+    }
+    a.nsamp = ns;
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.partials = d_partials_;
+    if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
+    void* args[] = {&a};
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    FinalizeArgs f;
+    std::memset(&f, 0, sizeof(f));
+    f.partials = d_partials_;
+    f.nacc = 2 + 2 * nA + nT;
+    f.nA = nA;
+    f.nc = nc;
+    f.nT = nT;
+    for (int k = 0; k < 3; ++k) {
+        f.cta[k][0] = cta_[k][0];
+        f.cta[k][1] = cta_[k][1];
+        f.has[k] = cta_[k][1] > 0;
+    }
+    f.n_phsp = (double)samples_[0].n;
+    f.W_data = samples_[1].wsum;
+    f.W_bkg = has_bkg_ ? samples_[2].wsum : 0.0;
+    f.params = d_params;
+    f.v = d_v_;
+    f.chain = d_amp_chain_;
+    f.gauss_idx = d_gauss_idx_;
+    f.gauss_ms = d_gauss_ms_;
+    f.ngauss = (int)m.gauss.size();
+    f.out_nll = d_nll;
+    f.out_grad = d_grad;
+    f.out_parts = d_parts_;
+    size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
+    ct_finalize_kernel<<<1, 256, shm, stream>>>(f);
+    CT_CUDA(cudaGetLastError());
+}
+
+void Engine::intensity(const double* d_params, int kind, double* d_out, cudaStream_t stream)
+{
+    if (kind < 0 || kind > 2 || samples_[kind].n == 0) throw std::runtime_error("intensity: empty or unknown sample");
+    const Model& m = model_;
+    int nA = m.nAmp(), nc = m.nVector();
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    const DeviceSample& d = samples_[kind];
+    a.s[0].slamp = d.slamp64;
+    a.s[0].kin = d.kin;
+    a.s[0].n = d.n;
+    a.s[0].kind = kind;
+    a.s[0].cta_count = 1;
+    a.nsamp = 1;
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.partials = d_partials_;
+    void* args[] = {&a, &d_out};
+    int grid = (int)std::min<long long>((d.n + 255) / 256, 148LL * 16);
+    CT_CUDA(cudaLaunchKernel(k_int_, dim3(grid), dim3(256), args, 0, stream));
+}
+
+void Engine::lastParts(double* out6, cudaStream_t stream)
+{
+    CT_CUDA(cudaMemcpyAsync(out6, d_parts_, sizeof(double) * 6, cudaMemcpyDeviceToHost, stream));
+    CT_CUDA(cudaStreamSynchronize(stream));
+}
+
+}  // namespace ctpwa

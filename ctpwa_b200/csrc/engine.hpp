@@ -1,0 +1,102 @@
+// Likelihood engine: device-resident samples, angular/kinematic caches,
+// the JIT-compiled fused NLL + adjoint kernel and its finalize step.
+#pragma once
+
+#include "codegen.hpp"
+#include "dataio.hpp"
+#include "model.hpp"
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+namespace ctpwa {
+
+enum Precision : int { kFP64 = 0, kMixed = 1 };
+
+struct DeviceSample {
+    long long n = 0;
+    double* p4 = nullptr;      // SoA [n_final * 4][n]
+    double2* slamp64 = nullptr;  // [nplane * npol][n]
+    float2* slamp32 = nullptr;   // mixed-precision copy
+    double* kin = nullptr;     // [nkin][n]
+    double* w = nullptr;       // weights or nullptr
+    double wsum = 0.0;         // sum of weights (or n)
+};
+
+struct EngineOptions {
+    int device = 0;
+    bool keep_momenta = false;
+    bool mixed_tables = true;  // build the FP32 angular table for the mixed path
+};
+
+// Compile (or find in the disk cache) the fused kernel of a config's model
+// without touching a GPU; returns seconds spent.
+double precompileConfig(const std::string& config_path);
+
+class Engine {
+public:
+    Engine(const std::string& config_path, const EngineOptions& opt);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    const Model& model() const { return model_; }
+    int nParams() const { return model_.nParams(); }
+
+    // NLL and gradient in the reference layout [Re p, Im p, theta]; all
+    // pointers are device pointers; stream-ordered, no host synchronisation.
+    void nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
+    // Per-event intensities of sample `kind` at d_params (device output [n]).
+    void intensity(const double* d_params, int kind, double* d_out, cudaStream_t stream);
+    // Per-sample partial sums of the last evaluation (diagnostics):
+    // [data_nll, bkg_nll, phsp_sum, W_data, W_bkg, n_phsp]
+    void lastParts(double* out6, cudaStream_t stream);
+
+    long long nEvents(int kind) const { return samples_[kind].n; }
+    size_t deviceBytes() const { return device_bytes_; }
+    const GeneratedModel& generated() const { return gen_; }
+    double jitSeconds() const { return jit_seconds_; }
+    bool jitCacheHit() const { return jit_cache_hit_; }
+
+private:
+    void loadSamples();
+    void buildTables();
+    void computeAngular(int kind);
+    void compileKernel();
+
+    Model model_;
+    EngineOptions opt_;
+    GeneratedModel gen_;
+    DeviceSample samples_[3];  // phsp, data, bkg
+    bool has_bkg_ = false;
+    size_t device_bytes_ = 0;
+
+    // angular tables (device)
+    void* d_ag_tables_ = nullptr;  // single allocation holding all host-built tables
+    std::vector<char> ag_host_;     // host image of group descriptors
+    struct GroupDev;
+    std::vector<std::vector<char>> group_desc_;  // AgGroup images per group
+
+    // JIT
+    void* lib_ = nullptr;  // cudaLibrary_t
+    void* k_f64_ = nullptr;
+    void* k_mixed_ = nullptr;
+    void* k_int_ = nullptr;
+    double jit_seconds_ = 0.0;
+    bool jit_cache_hit_ = false;
+
+    // evaluation buffers
+    double* d_v_ = nullptr;         // [2 nA]
+    double* d_partials_ = nullptr;  // [grid][nacc]
+    double* d_parts_ = nullptr;     // [8]
+    int* d_amp_chain_ = nullptr;
+    double* d_ratio_ = nullptr;
+    int* d_gauss_idx_ = nullptr;
+    double* d_gauss_ms_ = nullptr;  // [mu, sigma] pairs
+    int grid_ = 0;
+    int cta_[3][2] = {};  // per sample: begin, count
+};
+
+}  // namespace ctpwa

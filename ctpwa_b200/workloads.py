@@ -1,0 +1,218 @@
+"""Benchmark / test workloads: the J/psi -> 3 meson models used to measure
+this engine, as config.yml text plus seeded synthetic samples.
+
+* ``pipi_rho``    J/psi -> pi+ pi- pi0, one chain rho(770) -> pi+ pi- (BWR, m and width free)
+* ``pipi_3rho``   J/psi -> pi+ pi- pi0, chains rho0 pi0, rho+ pi-, rho- pi+, each with
+                  rho(770), rho(1450), rho(1700) (BWR; masses/widths free, shared by name)
+* ``kkpi``        J/psi -> K+ K- pi0: K*(892)+-, K*(1410)+- (J=1), K*2(1430)+- (J=2, D wave)
+                  as BWR plus a K+K- J=1 state with a custom Flatte lineshape
+                  (mass 1.68, couplings 0.3 / 0.1 to KK / pipi); all parameters free
+
+Samples are uniform three-body phase space (seeded) for phsp and background;
+data are drawn by accept-reject against the model at the true couplings
+(|v| in [0.1, 1], uniform phase, first coupling 1 + 0i, seeded) using the
+engine's per-event intensities, or taken as flat phase space when
+``accept_reject=False`` (enough for parity checks).
+"""
+from __future__ import annotations
+
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import toymc
+
+M_JPSI = 3.0969
+M_PIC = 0.13975
+M_PI0 = 0.13495
+M_K = 0.493677
+
+_PARTICLES_PIPI = """Particles:
+  Jpsi: {J: 1, P: -1, mass: 3.0969}
+  pip:  {J: 0, P: -1, mass: 0.13975}
+  pim:  {J: 0, P: -1, mass: 0.13975}
+  pi0:  {J: 0, P: -1, mass: 0.13495}
+"""
+
+_TEMPLATES = {
+    "pipi_rho": _PARTICLES_PIPI + """Data:
+  order: [pip, pim, pi0]
+  data: [npy, "@DATA@"]
+  phsp: [npy, "@PHSP@"]
+@BKG@DecayChains:
+  rho:
+    Jpsi: [[pi0, R_pm]]
+    R_pm: [pip, pim]
+    intermediates:
+      R_pm:
+        - [J: 1, P: -1]: [rho770]
+Resonances:
+  rho770: {J: 1, P: -1, model: BWR, parameters: [0.775, 0.149], free: [0, 1]}
+""",
+    "pipi_3rho": _PARTICLES_PIPI + """Data:
+  order: [pip, pim, pi0]
+  data: [npy, "@DATA@"]
+  phsp: [npy, "@PHSP@"]
+@BKG@DecayChains:
+  rho0:
+    Jpsi: [[pi0, R_pm]]
+    R_pm: [pip, pim]
+    intermediates:
+      R_pm:
+        - [J: 1, P: -1]: [rho770, rho1450, rho1700]
+  rhop:
+    Jpsi: [[pim, R_p0]]
+    R_p0: [pip, pi0]
+    intermediates:
+      R_p0:
+        - [J: 1, P: -1]: [rho770, rho1450, rho1700]
+  rhom:
+    Jpsi: [[pip, R_m0]]
+    R_m0: [pim, pi0]
+    intermediates:
+      R_m0:
+        - [J: 1, P: -1]: [rho770, rho1450, rho1700]
+Resonances:
+  rho770:  {J: 1, P: -1, model: BWR, parameters: [0.775, 0.149], free: [0, 1]}
+  rho1450: {J: 1, P: -1, model: BWR, parameters: [1.465, 0.400], free: [0, 1]}
+  rho1700: {J: 1, P: -1, model: BWR, parameters: [1.720, 0.250], free: [0, 1]}
+""",
+    "kkpi": """Particles:
+  Jpsi: {J: 1, P: -1, mass: 3.0969}
+  Kp:   {J: 0, P: -1, mass: 0.493677}
+  Km:   {J: 0, P: -1, mass: 0.493677}
+  pi0:  {J: 0, P: -1, mass: 0.13495}
+Data:
+  order: [Kp, Km, pi0]
+  data: [npy, "@DATA@"]
+  phsp: [npy, "@PHSP@"]
+@BKG@DecayChains:
+  kstp:
+    Jpsi: [[Km, R_Kp]]
+    R_Kp: [Kp, pi0]
+    intermediates:
+      R_Kp:
+        - [J: 1, P: -1]: [Kst892, Kst1410]
+        - [J: 2, P: +1]: [Kst2_1430]
+  kstm:
+    Jpsi: [[Kp, R_Km]]
+    R_Km: [Km, pi0]
+    intermediates:
+      R_Km:
+        - [J: 1, P: -1]: [Kst892, Kst1410]
+        - [J: 2, P: +1]: [Kst2_1430]
+  xkk:
+    Jpsi: [[pi0, R_KK]]
+    R_KK: [Kp, Km]
+    intermediates:
+      R_KK:
+        - [J: 1, P: -1]: [X1680]
+Resonances:
+  Kst892:    {J: 1, P: -1, model: BWR, parameters: [0.8955, 0.047], free: [0, 1]}
+  Kst1410:   {J: 1, P: -1, model: BWR, parameters: [1.414, 0.232], free: [0, 1]}
+  Kst2_1430: {J: 2, P: 1, model: BWR, parameters: [1.4256, 0.0985], free: [0, 1]}
+  X1680:
+    J: 1
+    P: -1
+    model: Custom
+    paramValues: [1.68, 0.3, 0.1]
+    paramNames: [mass, gKK, gpipi]
+    free: [0, 1, 2]
+    expr: "Flatte(mass, gKK, gpipi, 0.493677, 0.493677, 0.13957, 0.13957) * Bf(1, q, q0, 3.0)"
+""",
+}
+MASSES = {
+    "pipi_rho": (M_PIC, M_PIC, M_PI0),
+    "pipi_3rho": (M_PIC, M_PIC, M_PI0),
+    "kkpi": (M_K, M_K, M_PI0),
+}
+
+# sizes (phsp, data, bkg, bkg weight) of the measured configurations
+SIZES = {
+    "pipi_rho": (200_000, 20_000, 0, None),
+    "pipi_3rho": (5_000_000, 500_000, 50_000, 0.8),
+    "kkpi": (10_000_000, 1_000_000, 100_000, 0.3),
+}
+
+
+def config_text(name, phsp, data, bkg=None, bkg_weight=None):
+    bkg_block = ""
+    if bkg is not None:
+        bkg_block = f'  bkg: [npy, "{bkg}"]\n'
+        if bkg_weight is not None:
+            bkg_block += f"  bkg_weights: [{bkg_weight}]\n"
+    return _TEMPLATES[name].replace("@PHSP@", str(phsp)).replace("@DATA@", str(data)).replace("@BKG@", bkg_block)
+
+
+def true_params(n_vector, theta_init, seed=4001):
+    """Seeded couplings |v| ~ U[0.1, 1], phase ~ U[0, 2pi), first = 1 + 0i; theta at its initial values."""
+    rng = np.random.default_rng(seed)
+    mag = rng.uniform(0.1, 1.0, n_vector)
+    ph = rng.uniform(0.0, 2.0 * math.pi, n_vector)
+    re, im = mag * np.cos(ph), mag * np.sin(ph)
+    re[0], im[0] = 1.0, 0.0
+    return np.concatenate([re, im, np.asarray(theta_init, dtype=np.float64)])
+
+
+def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, seed=0, accept_reject=True,
+         device=0):
+    """Write samples + config.yml for workload `name` into outdir; returns the config path.
+
+    accept_reject=True draws the data sample against the model at the true
+    parameters (needs a GPU); otherwise data are flat phase space."""
+    sp, sd, sb, sw = SIZES[name]
+    n_phsp = sp if n_phsp is None else n_phsp
+    n_data = sd if n_data is None else n_data
+    n_bkg = sb if n_bkg is None else n_bkg
+    bkg_weight = sw if bkg_weight is None else bkg_weight
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    masses = MASSES[name]
+    phsp = toymc.phase_space(M_JPSI, masses, n_phsp, 1001 + seed)
+    toymc.write_npy(out / "phsp.npy", phsp)
+    bkg_path = None
+    if n_bkg:
+        toymc.write_npy(out / "bkg.npy", toymc.phase_space(M_JPSI, masses, n_bkg, 3001 + seed))
+        bkg_path = str(out / "bkg.npy")
+    if accept_reject:
+        data = _accept_reject(name, out, masses, n_data, seed, device)
+    else:
+        data = toymc.phase_space(M_JPSI, masses, n_data, 2001 + seed)
+    toymc.write_npy(out / "data.npy", data)
+    cfg = out / "config.yml"
+    cfg.write_text(config_text(name, str(out / "phsp.npy"), str(out / "data.npy"), bkg_path, bkg_weight))
+    return str(cfg)
+
+
+def _accept_reject(name, out, masses, n_data, seed, device):
+    import torch
+
+    from . import analysis
+
+    ncand = int(n_data * 12) + 10_000
+    cand = toymc.phase_space(M_JPSI, masses, ncand, 5001 + seed)
+    toymc.write_npy(out / "cand.npy", cand)
+    tiny = toymc.phase_space(M_JPSI, masses, 1000, 7001 + seed)
+    toymc.write_npy(out / "tiny.npy", tiny)
+    cfg = out / "cand.yml"
+    cfg.write_text(config_text(name, str(out / "tiny.npy"), str(out / "cand.npy")))
+    ana = analysis(str(cfg), device=device)
+    p = true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
+    I = ana.getIntensity(torch.tensor(p, dtype=torch.float64, device=f"cuda:{device}"), kind=1).cpu().numpy()
+    del ana
+    sel = toymc.accept_reject(cand, I, seed=6001 + seed, safety=1.2)
+    while sel.shape[0] < n_data:  # rare: top up from a fresh candidate batch
+        more = toymc.phase_space(M_JPSI, masses, ncand, 8001 + seed + sel.shape[0])
+        toymc.write_npy(out / "cand.npy", more)
+        ana = analysis(str(cfg), device=device)
+        I2 = ana.getIntensity(torch.tensor(p, dtype=torch.float64, device=f"cuda:{device}"), kind=1).cpu().numpy()
+        del ana
+        sel = np.concatenate([sel, toymc.accept_reject(more, I2, seed=9001 + seed, safety=1.2)])
+    for f in ("cand.npy", "tiny.npy", "cand.yml"):
+        try:
+            os.remove(out / f)
+        except OSError:
+            pass
+    return sel[:n_data]

@@ -1,0 +1,121 @@
+/*
+ * ctpwa_b200 C ABI — the drop-in boundary of the B200 likelihood engine.
+ *
+ * Each entry point replaces one member of the reference's pybind11 class
+ * `ctpwa.analysis` (src/main.cu:91-131), whose methods a Python, ctypes,
+ * cffi or C/C++ host binds; the Python module ctpwa_b200 binds these with
+ * ctypes and keeps the reference method names and tensor contracts.
+ *
+ * Conventions
+ *  - Parameter vectors use the reference layout [Re p (nV), Im p (nV), theta (nT)]
+ *    (src/Analysis.cu:629-681, src/Parameters.cu:263-300), nV = ctpwa_n_vector,
+ *    nT = ctpwa_n_free_theta.
+ *  - Functions return 0 on success and a negative status on failure; the
+ *    message is available from ctpwa_last_error (no exit(), no exceptions
+ *    across the ABI).
+ *  - Evaluation entry points taking device pointers are stream ordered on the
+ *    given cudaStream_t (passed as void*, 0 = legacy default stream), perform
+ *    no host synchronisation and no allocation, and may be captured in a CUDA
+ *    graph. Each handle owns its scratch; different handles are independent.
+ */
+#ifndef CTPWA_B200_H
+#define CTPWA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ctpwa_handle ctpwa_handle;
+
+#define CTPWA_OK 0
+#define CTPWA_ERR_CONFIG (-1)   /* invalid config / model (reference: isValid()=False, runtime_error) */
+#define CTPWA_ERR_CUDA (-2)     /* CUDA runtime / NVRTC failure */
+#define CTPWA_ERR_ARG (-3)      /* bad argument (reference: TORCH_CHECK -> RuntimeError) */
+
+#define CTPWA_FP64 0            /* plain FP64 path (reference built with CTPWA_DOUBLE_COMPLEX) */
+#define CTPWA_MIXED 1           /* FP32 amplitudes, FP64 reductions */
+
+/* Replaces: analysis(config_file) — src/Analysis.cu:1271-1281 (initialize :3849-4208).
+ * Builds the model, reads the samples, computes the angular/kinematic caches on
+ * `device` and JIT-compiles the model's fused kernel. Returns NULL on failure
+ * with *status set and the message copied to err (if non-NULL). */
+ctpwa_handle* ctpwa_create(const char* config_path, int device, int* status, char* err, size_t errlen);
+
+/* Releases device memory of the handle (the reference never frees; src/Analysis.cu:1284-1290). */
+void ctpwa_destroy(ctpwa_handle* h);
+
+/* Replaces: analysis::getNVector — src/Analysis.cu:1311-1315 (vspace fit mode). */
+int ctpwa_n_vector(const ctpwa_handle* h);
+
+/* Replaces: analysis::getNFreeTheta — src/Analysis.cu:1316. */
+int ctpwa_n_free_theta(const ctpwa_handle* h);
+
+/* Replaces: analysis::getNParams — src/Analysis.cu:1344 (= 2 nV + nT). */
+int ctpwa_n_params(const ctpwa_handle* h);
+
+/* Replaces: analysis::getParamNames — src/Analysis.cu:1318-1342.
+ * Writes the names separated by '\n' (NUL-terminated); returns the number of
+ * bytes needed including the terminator (call with cap = 0 to size). */
+int ctpwa_param_names(const ctpwa_handle* h, char* buf, size_t cap);
+
+/* Replaces: analysis::getFreeResParams — src/Analysis.cu:3779-3792.
+ * out: host array [3][nT] = (initial value, lower bound, upper bound). */
+int ctpwa_free_res_params(const ctpwa_handle* h, double* out);
+
+/* Replaces: analysis::getNLL forward + NLLFunction::backward — src/Analysis.cu:625-1261.
+ * d_params [n_params], d_nll [1], d_grad [n_params]: device pointers.
+ * precision: CTPWA_FP64 or CTPWA_MIXED. */
+int ctpwa_nll_grad(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision, void* stream);
+
+/* Same evaluation from host buffers: copies params host->device, evaluates,
+ * copies NLL and gradient back, and synchronises the stream. */
+int ctpwa_nll_grad_host(ctpwa_handle* h, const double* params, double* nll, double* grad, int precision, void* stream);
+
+/* Per-sample parts of the last evaluation (host, synchronising):
+ * [data_nll, bkg_nll, sum_phsp_intensity, W_data, W_bkg, n_phsp]. */
+int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream);
+
+/* Per-event intensity f_e = sum_pol |sum_a v_a A_a|^2 of sample kind (0 phase
+ * space, 1 data, 2 background) at d_params; d_out: device array [n_events].
+ * The reference computes the same quantity inside computeFactorNLL
+ * (src/ComputeNLL.cu:21-84) and for its result export (ComputeResults.cu:22). */
+int ctpwa_intensity(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream);
+
+/* Event counts of phase space (kind 0), data (1), background (2). */
+long long ctpwa_n_events(const ctpwa_handle* h, int kind);
+
+/* Lowered model as JSON (columns, groups, theta slots, coupling map); same
+ * sizing convention as ctpwa_param_names. */
+int ctpwa_model_json(const ctpwa_handle* h, char* buf, size_t cap);
+
+/* Device bytes held by the handle's event caches. */
+size_t ctpwa_device_bytes(const ctpwa_handle* h);
+
+/* Seconds spent compiling (or loading from the disk cache) the fused kernel. */
+double ctpwa_jit_seconds(const ctpwa_handle* h);
+
+/* Message of the last failure on this handle (or of the last failed create when h is NULL). */
+const char* ctpwa_last_error(const ctpwa_handle* h);
+
+/* Host-only model description (no GPU): the lowered model of a config as
+ * JSON, as ctpwa_model_json. Replaces the reference's DecayInfo class
+ * (src/main.cu:41-51, src/Info.cu:43-357) for inspection of amplitude and
+ * parameter names. Returns the bytes needed (>0) or a negative status. */
+int ctpwa_describe(const char* config_path, char* buf, size_t cap, char* err, size_t errlen);
+
+/* Ahead-of-time compile of a config's fused kernel into the kernel cache
+ * (NVRTC only; no GPU needed). The reference compiles its lineshape JIT on the
+ * first getNLL call (src/JITCustom.cu:894-1003); this moves that cost out of
+ * the first evaluation. seconds (optional) receives the time spent. */
+int ctpwa_precompile(const char* config_path, double* seconds, char* err, size_t errlen);
+
+/* Library version string. */
+const char* ctpwa_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTPWA_B200_H */

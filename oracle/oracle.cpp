@@ -777,3 +777,33 @@ int orc_model_eval(int type, int Lmin, double d, int P, int n_ch, const double* 
     return 0;
 }
 }
+
+extern "C" {
+// Per-event intensity f_e = sum_p |sum_a v_a A_{a,p}|^2 of sample k at params.
+int orc_intensity(void* h, int k, const double* params, double* out)
+{
+    auto* o = static_cast<Oracle*>(h);
+    const Model& m = o->m;
+    int nA = m.nAmp(), nc = m.nVector(), npol = m.npol;
+    long n = o->smp[k].s.n;
+    std::vector<double> A((size_t)n * npol * nA * 2);
+    orc_columns(h, k, params + 2 * nc, A.data());
+    const cplx* Ac = reinterpret_cast<const cplx*>(A.data());
+    std::vector<cplx> v(nA);
+    for (int a = 0; a < nA; ++a) {
+        int c = m.coupling.amp_chain[a];
+        v[a] = m.coupling.ratio[a] * cplx(params[c], params[nc + c]);
+    }
+#pragma omp parallel for schedule(static)
+    for (long e = 0; e < n; ++e) {
+        double f = 0.0;
+        for (int p = 0; p < npol; ++p) {
+            cplx s = 0.0;
+            for (int a = 0; a < nA; ++a) s += Ac[((size_t)e * npol + p) * nA + a] * v[a];
+            f += s.real() * s.real() + s.imag() * s.imag();
+        }
+        out[e] = f;
+    }
+    return 0;
+}
+}

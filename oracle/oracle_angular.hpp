@@ -33,36 +33,28 @@ struct LV {
     LV operator+(const LV& o) const { return LV(E + o.E, Px + o.Px, Py + o.Py, Pz + o.Pz); }
 };
 
-// n! for integer and half-integer n (Gamma(n+1)); table up to 11.5, the
+// n! for integer and half-integer n (Gamma(n+1)): exact up to 11.5, the
 // Stirling series with two correction terms for integers >= 12, and the
-// Lanczos (g = 7, 9 terms) Gamma approximation otherwise (src/Amplitude.cu:5-98).
+// Lanczos (g = 7, 9 published terms) Gamma approximation otherwise, the
+// same scheme as src/Amplitude.cu:5-98.
 inline double factorial(float n)
 {
     if (n < 0.0 || std::isnan(n)) return 0.0;
-    static const double tab[24] = {
-        1.0, 0.886226925452758, 1.0, 1.329340388179137, 2.0, 3.323350970447842, 6.0, 11.63172839656745,
-        24.0, 52.34277778455352, 120.0, 287.8852778150444, 720.0, 1871.254305797788, 5040.0, 14034.40729348341,
-        40320.0, 119292.461994609, 362880.0, 1133278.388948785, 3628800.0, 11899423.0839622, 39916800.0,
-        136843365.9027724};
     double r = std::round(n);
     bool is_int = std::fabs(n - r) < 1e-10;
-    double hr = std::round(2.0 * n) / 2.0;
-    bool is_half = !is_int && std::fabs(n - hr) < 1e-10;
-    if (n >= 0.0 && n <= 11.5) {
+    bool is_half = !is_int && std::fabs(n - std::round(2.0 * n) / 2.0) < 1e-10;
+    if (n >= 0.0 && n <= 11.5 && (is_int || is_half)) {
         if (is_int) {
-            int k = (int)r;
-            if (k >= 0 && k <= 11) return tab[2 * k];
-        } else if (is_half) {
-            int k = (int)std::round(2.0 * n - 1.0);
-            if (k >= 0 && k <= 22) return tab[k + 1];
+            double f = 1.0;
+            for (int i = 2; i <= (int)r; ++i) f *= i;
+            return f;
         }
+        return std::tgamma((double)n + 1.0);  // half-integer: Gamma(n + 1)
     }
-    if (is_int) {
+    if (is_int && r >= 12) {
         int k = (int)r;
-        if (k >= 12) {
-            double st = std::sqrt(2.0 * M_PI * k) * std::pow(k / M_E, k);
-            return st * (1.0 + 1.0 / (12.0 * k) + 1.0 / (288.0 * k * k));
-        }
+        double st = std::sqrt(2.0 * M_PI * k) * std::pow(k / M_E, k);
+        return st * (1.0 + 1.0 / (12.0 * k) + 1.0 / (288.0 * k * k));
     }
     const double g = 7.0;
     const double c[9] = {0.99999999999980993, 676.5203681218851, -1259.1392167224028, 771.32342877765313,

@@ -1,0 +1,110 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so) and of the
+reference-math shim (oracle/_ref/libref_math.so) for tests."""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libref_math.so")
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+_orc = None
+
+
+def oracle_lib():
+    global _orc
+    if _orc is None:
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.orc_open.restype = ctypes.c_void_p
+        lib.orc_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+        lib.orc_close.argtypes = [ctypes.c_void_p]
+        lib.orc_sizes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
+        lib.orc_group_nsl.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.orc_slamp.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D]
+        lib.orc_columns.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D]
+        lib.orc_nll_grad.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, ctypes.c_int]
+        lib.orc_pwa_amp.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
+        lib.orc_clebsch.restype = ctypes.c_double
+        lib.orc_clebsch.argtypes = [ctypes.c_int] * 6
+        lib.orc_custom_eval.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, _D, ctypes.c_char_p, ctypes.c_int]
+        lib.orc_model_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
+                                       _I, _D, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]
+        lib.orc_intensity.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D]
+        lib.orc_error.restype = ctypes.c_char_p
+        lib.orc_error.argtypes = [ctypes.c_void_p]
+        _orc = lib
+    return _orc
+
+
+def ref_lib():
+    if not os.path.exists(REF_SO):
+        return None
+    lib = ctypes.CDLL(REF_SO)
+    V = ctypes.c_void_p
+    lib.ref_pwa_amp.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
+    lib.ref_clebsch.restype = ctypes.c_double
+    lib.ref_clebsch.argtypes = [ctypes.c_int] * 6
+    lib.ref_model_build.restype = V
+    lib.ref_model_build.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_int, _D, _I, _D, ctypes.c_int]
+    lib.ref_custom_build.restype = V
+    lib.ref_custom_build.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    lib.ref_aux_eval.argtypes = [V, _D, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, _D, _D]
+    lib.ref_aux_free.argtypes = [V]
+    return lib
+
+
+def ptr(a):
+    return a.ctypes.data_as(_D)
+
+
+class Oracle:
+    """FP64 CPU oracle of one config (test infrastructure)."""
+
+    def __init__(self, config_path):
+        self.lib = oracle_lib()
+        err = ctypes.create_string_buffer(1024)
+        self.h = self.lib.orc_open(str(config_path).encode(), err, 1024)
+        if not self.h:
+            raise RuntimeError("oracle: " + err.value.decode())
+        sz = (ctypes.c_long * 8)()
+        self.lib.orc_sizes(self.h, sz)
+        self.nA, self.nT, self.nV, self.npol, self.nG = sz[0], sz[1], sz[2], sz[3], sz[4]
+        self.nev = (sz[5], sz[6], sz[7])
+
+    def close(self):
+        if self.h:
+            self.lib.orc_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def nll_grad(self, params, nthreads=0):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        g = np.zeros_like(p)
+        v = ctypes.c_double()
+        parts = np.zeros(6)
+        rc = self.lib.orc_nll_grad(self.h, ptr(p), ctypes.byref(v), ptr(g), ptr(parts), nthreads)
+        if rc != 0:
+            raise RuntimeError(self.lib.orc_error(self.h).decode())
+        return v.value, g, parts
+
+    def columns(self, kind, theta):
+        t = np.ascontiguousarray(theta, dtype=np.float64)
+        out = np.zeros((self.nev[kind], self.npol, self.nA), dtype=np.complex128)
+        self.lib.orc_columns(self.h, kind, ptr(t), out.ctypes.data_as(_D))
+        return out
+
+    def intensity(self, kind, params):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        out = np.zeros(self.nev[kind])
+        self.lib.orc_intensity(self.h, kind, ptr(p), ptr(out))
+        return out

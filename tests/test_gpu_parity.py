@@ -1,0 +1,106 @@
+"""Device path vs the FP64 CPU oracle on the same seeded inputs.
+
+Tolerances: plain FP64 path 1e-10 relative on the NLL and 1e-9 (relative to
+the largest component) on the gradient; mixed path |dNLL| < 1e-3 absolute
+and 1e-4 relative on the gradient.
+"""
+import numpy as np
+import pytest
+
+from ctpwa_b200 import workloads
+from tests.oracle_binding import Oracle
+
+pytestmark = pytest.mark.gpu
+
+SMALL = {"pipi_rho": (20_000, 5_000, 0), "pipi_3rho": (20_000, 5_000, 1_000), "kkpi": (20_000, 5_000, 1_000)}
+
+
+@pytest.fixture(scope="module")
+def setups(tmp_path_factory):
+    import torch
+    import ctpwa_b200
+
+    out = {}
+    for name, (nph, nda, nbk) in SMALL.items():
+        d = tmp_path_factory.mktemp(name)
+        cfg = workloads.make(name, d, n_phsp=nph, n_data=nda, n_bkg=nbk, accept_reject=False, seed=3)
+        ana = ctpwa_b200.analysis(cfg)
+        orc = Oracle(cfg)
+        rng = np.random.default_rng(11)
+        p = workloads.true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
+        p[2 * ana.getNVector():] *= 1 + 0.01 * rng.standard_normal(ana.getNFreeTheta())
+        out[name] = (ana, orc, torch.tensor(p, dtype=torch.float64, device="cuda"), p)
+    return out
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_counts_and_names_match_oracle(setups, name):
+    ana, orc, _, _ = setups[name]
+    assert ana.getNVector() == orc.nV
+    assert ana.getNFreeTheta() == orc.nT
+    assert ana.getNEvents() == orc.nev
+    assert len(ana.getParamNames()) == ana.getNParams()
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_fp64_nll_grad_parity(setups, name):
+    ana, orc, pt, p = setups[name]
+    nll, g = ana.getNLLAndGrad(pt, "fp64")
+    onll, og, _ = orc.nll_grad(p)
+    nll = float(nll)
+    g = g.cpu().numpy()
+    assert abs(nll - onll) <= 1e-10 * max(1.0, abs(onll)), (nll, onll)
+    assert np.max(np.abs(g - og)) <= 1e-9 * np.max(np.abs(og)), (g, og)
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_mixed_nll_grad_close(setups, name):
+    ana, orc, pt, p = setups[name]
+    nll, g = ana.getNLLAndGrad(pt, "mixed")
+    onll, og, _ = orc.nll_grad(p)
+    assert abs(float(nll) - onll) < 1e-3
+    assert np.max(np.abs(g.cpu().numpy() - og)) <= 1e-4 * np.max(np.abs(og))
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_intensity_parity(setups, name):
+    ana, orc, pt, p = setups[name]
+    for kind in (0, 1):
+        f = ana.getIntensity(pt, kind).cpu().numpy()
+        of = orc.intensity(kind, p)
+        assert np.max(np.abs(f - of) / np.maximum(np.abs(of), 1e-300)) < 1e-11
+
+
+def test_bitwise_reproducible(setups):
+    ana, _, pt, _ = setups["kkpi"]
+    a = ana.getNLLAndGrad(pt, "fp64")
+    b = ana.getNLLAndGrad(pt, "fp64")
+    assert float(a[0]) == float(b[0])
+    assert bool((a[1] == b[1]).all())
+
+
+def test_autograd_and_host_entry(setups):
+    import torch
+
+    ana, _, pt, p = setups["kkpi"]
+    q = pt.clone().requires_grad_(True)
+    nll = ana.getNLL(q)
+    (g,) = torch.autograd.grad(nll, q)
+    nll2, g2 = ana.getNLLAndGrad(pt, "fp64")
+    assert float(nll) == float(nll2)
+    assert bool((g == g2).all())
+    hn, hg = ana.getNLLHost(p)
+    assert hn == float(nll2)
+    assert np.array_equal(hg, g2.cpu().numpy())
+
+
+def test_param_checks(setups):
+    import torch
+
+    ana, _, pt, _ = setups["pipi_rho"]
+    with pytest.raises(RuntimeError):
+        ana.getNLL(pt.float())
+    with pytest.raises(RuntimeError):
+        ana.getNLL(pt.cpu())
+    with pytest.raises(RuntimeError):
+        ana.getNLL(pt[:-1])
