@@ -259,14 +259,141 @@ private:
 };
 
 // ------------------------------------------------------------- generator
+using dag::Cx;
+using dag::Graph;
+
+// DAG builders of the lineshapes, written so that parameter-only factors and
+// event-only factors multiply separately (both hoist / share cleanly).
+struct Shapes {
+    Graph& g;
+    explicit Shapes(Graph& gg) : g(gg) {}
+    int sq(int a) { return g.mul(a, a); }
+    // per-call q0: sqrt((m0^2-(m1+m2)^2)(m0^2-(m1-m2)^2)/(4 m0^2)), 0 below threshold
+    int q0(int m0, int m1, int m2)
+    {
+        int s = g.add(m1, m2), d = g.sub(m1, m2), m0s = sq(m0);
+        int q2 = g.mul(g.mul(g.sub(m0s, sq(s)), g.sub(m0s, sq(d))), g.recip(g.mul(g.cnst(4.0), m0s)));
+        return g.sel(dag::LT0, q2, g.zero(), g.sqrt(q2));
+    }
+    // breakup momentum sqrt((m^2-(m1+m2)^2)(m^2-(m1-m2)^2))/(2m), 0 at or below threshold
+    int breakup(int m, int m1, int m2)
+    {
+        int s = g.add(m1, m2), d = g.sub(m1, m2), ms = sq(m);
+        int q2 = g.mul(g.sub(ms, sq(s)), g.sub(ms, sq(d)));
+        return g.sel(dag::LE0, q2, g.zero(), g.mul(g.sqrt(q2), g.recip(g.mul(g.cnst(2.0), m))));
+    }
+    int poly(int L, int z)
+    {
+        static const double C[7][7] = {{1}, {1, 1}, {9, 3, 1}, {225, 45, 6, 1}, {11025, 1575, 135, 10, 1},
+                                       {893025, 99225, 6300, 315, 15, 1},
+                                       {540326025, 6185025, 363825, 17325, 630, 21, 1}};
+        int z2 = sq(z);
+        int r = g.cnst(1.0);
+        for (int k = L - 1; k >= 0; --k) r = g.add(g.mul(r, z2), g.cnst(C[L][k]));
+        return r;
+    }
+    // Bf(L, q, q0, d) = sqrt(N(q0 d)) * sqrt(1 / N(q d))
+    int bf(int L, int q, int q0v, double d)
+    {
+        if (L <= 0 || L > 6) return g.one();
+        int dn = g.cnst(d);
+        return g.mul(g.sqrt(poly(L, g.mul(q0v, dn))), g.sqrt(g.recip(poly(L, g.mul(q, dn)))));
+    }
+    int bf2(int L, int q, int q0v, double d)
+    {
+        if (L <= 0 || L > 6) return g.one();
+        int dn = g.cnst(d);
+        return g.mul(poly(L, g.mul(q0v, dn)), g.recip(poly(L, g.mul(q, dn))));
+    }
+    // 1 / (m0^2 - m^2 - i m0 G(m)), G = G0 (q/q0)^(2L+1) (m0/m) Bf^2
+    Cx bwr(int m, int m0, int g0, int L, int q, int q0v, double d)
+    {
+        int x = g.sub(sq(m0), sq(m));
+        int thp = g.mul(g.mul(g0, sq(m0)), g.powi(g.recip(q0v), 2 * L + 1));
+        int evp = g.mul(g.powi(q, 2 * L + 1), g.recip(m));
+        int y;
+        if (L > 0 && L <= 6 && d != 0.0) {
+            int dn = g.cnst(d);
+            thp = g.mul(thp, poly(L, g.mul(q0v, dn)));
+            evp = g.mul(evp, g.recip(poly(L, g.mul(q, dn))));
+        }
+        y = g.mul(thp, evp);
+        int is = g.recip(g.add(sq(x), sq(y)));
+        return {g.mul(x, is), g.mul(y, is)};
+    }
+    Cx bw(int m, int m0, int g0)
+    {
+        int x = g.sub(sq(m0), sq(m)), y = g.mul(m0, g0);
+        int is = g.recip(g.add(sq(x), sq(y)));
+        return {g.mul(x, is), g.mul(y, is)};
+    }
+    // Flatte (FlatteC), per-call form: (A - iB) / (A^2 + B^2)
+    Cx flatte(int m, int m0, const std::vector<int>& gs, const std::vector<int>& ch)
+    {
+        int s = sq(m);
+        int A = sq(m0), B = g.zero(), half = g.mul(m0, g.cnst(0.5));
+        for (size_t i = 0; i < gs.size(); ++i) {
+            int gw = g.mul(gs[i], half);
+            A = g.add(A, g.mul(gw, g.rho(true, s, ch[2 * i], ch[2 * i + 1])));
+            B = g.sub(B, g.mul(gw, g.rho(false, s, ch[2 * i], ch[2 * i + 1])));
+        }
+        A = g.sub(A, s);
+        int iD = g.recip(g.add(sq(A), sq(B)));
+        return {g.mul(A, iD), g.neg(g.mul(B, iD))};
+    }
+    // Flatte, fixed-parameter form (same value, reference arrangement)
+    Cx flatteFixed(int m, int m0, const std::vector<int>& gs, const std::vector<int>& ch)
+    {
+        int s = sq(m), tr = g.zero(), ti = g.zero();
+        for (size_t i = 0; i < gs.size(); ++i) {
+            int gw = g.mul(g.mul(m0, g.cnst(0.5)), gs[i]);
+            tr = g.add(tr, g.mul(gw, g.rho(false, s, ch[2 * i], ch[2 * i + 1])));
+            ti = g.add(ti, g.mul(gw, g.rho(true, s, ch[2 * i], ch[2 * i + 1])));
+        }
+        int dre = g.add(g.sub(sq(m0), s), ti), dim = g.neg(tr);
+        int is = g.recip(g.add(sq(dre), sq(dim)));
+        return {g.mul(dre, is), g.neg(g.mul(dim, is))};
+    }
+    // Gounaris-Sakurai (rho -> pi pi), per-call form
+    Cx gs(int m, int q, int m0, int g0, int q0v, double mpi)
+    {
+        const double pi = 3.14159265358979323846;
+        auto C = [&](double v) { return g.cnst(v); };
+        int hm = g.mul(C(2.0 / pi), g.mul(g.div(q, m), g.log(g.mul(g.add(m, g.mul(C(2.0), q)), C(1.0 / (2.0 * mpi))))));
+        int q02 = sq(q0v), q03 = g.mul(q02, q0v);
+        int mpi2 = C(mpi * mpi);
+        int la = g.log(g.mul(g.add(m0, g.mul(C(2.0), q0v)), C(1.0 / (2.0 * mpi))));
+        int dv = g.sub(g.add(g.mul(g.mul(C(3.0 / pi), g.div(mpi2, q02)), la), g.div(m0, g.mul(C(2.0 * pi), q0v))),
+                       g.div(g.mul(mpi2, m0), g.mul(C(pi), q03)));
+        int h0 = g.mul(C(2.0 / pi), g.mul(g.div(q0v, m0), la));
+        int m0s = sq(m0);
+        int dh0 = g.add(g.mul(h0, g.sub(g.recip(g.mul(C(8.0), q02)), g.recip(g.mul(C(2.0), m0s)))),
+                        g.recip(g.mul(C(2.0 * pi), m0s)));
+        int qr = g.div(q, q0v);
+        int gam = g.mul(g.mul(g0, g.mul(g.mul(qr, qr), qr)), g.div(m0, m));
+        int f = g.mul(g.mul(g0, g.div(m0s, q03)),
+                      g.add(g.mul(sq(q), g.sub(hm, h0)), g.mul(g.mul(g.sub(m0s, sq(m)), q02), dh0)));
+        int num = g.add(C(1.0), g.div(g.mul(dv, g0), m0));
+        int dre = g.add(g.sub(m0s, sq(m)), f);
+        int dim = g.neg(g.mul(m0, gam));
+        int is = g.recip(g.add(sq(dre), sq(dim)));
+        return {g.mul(g.mul(num, dre), is), g.neg(g.mul(g.mul(num, dim), is))};
+    }
+};
+
 struct Gen {
     const Model& m;
     GeneratedModel out;
+    Graph G;
+    Shapes S{G};
     std::map<std::tuple<int, unsigned, unsigned, unsigned>, int> slot_of;
-    std::ostringstream body;
-    std::ostringstream globals;
-    int tmp = 0;
-    int ntab = 0;
+    std::vector<std::vector<double>> tables;  // Hist / Interp tables
+    struct ColOut {
+        int re, im;
+        std::vector<std::pair<int, std::pair<int, int>>> der;  // theta -> (d re, d im)
+    };
+    std::vector<ColOut> cols;
+    std::vector<std::pair<int, int>> extra;  // opaque per-event values: (table id, mass node) placeholders
 
     explicit Gen(const Model& mm) : m(mm) {}
 
@@ -279,8 +406,8 @@ struct Gen {
     }
     int slot(int type, int g, int a, int b = -1, int c = -1)
     {
-        const Group& G = m.groups[g];
-        auto key = std::make_tuple(type, mask(G, a), b >= 0 ? mask(G, b) : 0u, c >= 0 ? mask(G, c) : 0u);
+        const Group& Gr = m.groups[g];
+        auto key = std::make_tuple(type, mask(Gr, a), b >= 0 ? mask(Gr, b) : 0u, c >= 0 ? mask(Gr, c) : 0u);
         auto it = slot_of.find(key);
         if (it != slot_of.end()) return it->second;
         int id = (int)out.slots.size();
@@ -288,134 +415,102 @@ struct Gen {
         slot_of[key] = id;
         return id;
     }
-    std::string kv(int s) { return "kv[" + std::to_string(s) + "]"; }
-    std::string t() { return "t" + std::to_string(tmp++); }
+    int kin(int type, int g, int a, int b = -1, int c = -1) { return G.kin(slot(type, g, a, b, c)); }
 
-    // custom expression -> CJet<N> temporaries; returns variable name
+    // custom expression -> DAG (complex)
     struct XCtx {
-        int N;
-        std::string mm, qq, md1, md2, L, d;
-        std::vector<std::string> par;  // Jet<N> parameter names
-        int gi = -1, d1 = -1, d2 = -1; // daughters for p1*/p2* variables (-1: zero)
+        int mm, qq, md1, md2, d;
+        int L;
+        std::vector<int> par;
+        int gi = -1, d1 = -1, d2 = -1;
     };
-    std::string emitX(const XP& x, const XCtx& c)
+    Cx emitX(const XP& x, const XCtx& c)
     {
-        std::string N = std::to_string(c.N);
-        auto J = [&](const std::string& e) { return "cjr(" + e + ")"; };
-        auto K = [&](const std::string& e) { return "cjr(jc<" + N + ">(" + e + "))"; };
-        std::string r = t(), e;
         switch (x->k) {
-        case XNode::Num: e = "cjc<" + N + ">(" + num(x->v) + ", 0.0)"; break;
-        case XNode::Param: e = J(c.par[x->idx]); break;
+        case XNode::Num: return G.c(x->v);
+        case XNode::Param: return G.cr(c.par[x->idx]);
         case XNode::Var: {
             const std::string& v = x->id;
-            if (v == "m") e = K(c.mm);
-            else if (v == "q") e = K(c.qq);
-            else if (v == "L") e = K("(double)" + c.L);
-            else if (v == "d") e = K(c.d);
-            else if (v == "md1") e = J(c.md1);
-            else if (v == "md2") e = J(c.md2);
-            else {
-                static const char* pv[] = {"p1p", "p1e", "p1costheta", "p1phi", "p2p", "p2e", "p2costheta", "p2phi"};
-                static const int pt[] = {AG_K_P_, AG_K_E_, AG_K_CT_, AG_K_PHI_};
-                for (int i = 0; i < 8; ++i)
-                    if (v == pv[i]) e = K(c.gi < 0 ? std::string("0.0") : kv(slot(pt[i % 4], c.gi, i < 4 ? c.d1 : c.d2)));
-            }
-            break;
+            if (v == "m") return G.cr(c.mm);
+            if (v == "q") return G.cr(c.qq);
+            if (v == "L") return G.c((double)c.L);
+            if (v == "d") return G.cr(c.d);
+            if (v == "md1") return G.cr(c.md1);
+            if (v == "md2") return G.cr(c.md2);
+            static const char* pv[] = {"p1p", "p1e", "p1costheta", "p1phi", "p2p", "p2e", "p2costheta", "p2phi"};
+            static const int pt[] = {AG_K_P_, AG_K_E_, AG_K_CT_, AG_K_PHI_};
+            for (int i = 0; i < 8; ++i)
+                if (v == pv[i]) return c.gi < 0 ? G.c(0.0) : G.cr(kin(pt[i % 4], c.gi, i < 4 ? c.d1 : c.d2));
+            return G.c(0.0);
         }
-        case XNode::Add: e = emitX(x->kids[0], c) + " + " + emitX(x->kids[1], c); break;
-        case XNode::Sub: e = emitX(x->kids[0], c) + " - " + emitX(x->kids[1], c); break;
-        case XNode::Mul: e = emitX(x->kids[0], c) + " * " + emitX(x->kids[1], c); break;
-        case XNode::Div: { auto a = emitX(x->kids[0], c), b = emitX(x->kids[1], c); e = "c_div(" + a + ", " + b + ")"; break; }
-        case XNode::Pow: { auto a = emitX(x->kids[0], c), b = emitX(x->kids[1], c); e = "c_pow(" + a + ", " + b + ")"; break; }
-        case XNode::Neg: e = "-" + emitX(x->kids[0], c); break;
-        case XNode::Func: e = "c_" + x->id + "(" + emitX(x->kids[0], c) + ")"; break;
+        case XNode::Add: return G.cadd(emitX(x->kids[0], c), emitX(x->kids[1], c));
+        case XNode::Sub: return G.csub(emitX(x->kids[0], c), emitX(x->kids[1], c));
+        case XNode::Mul: return G.cmul(emitX(x->kids[0], c), emitX(x->kids[1], c));
+        case XNode::Div: return G.cdivRef(emitX(x->kids[0], c), emitX(x->kids[1], c));
+        case XNode::Pow: return G.cpow(emitX(x->kids[0], c), emitX(x->kids[1], c));
+        case XNode::Neg: return G.cneg(emitX(x->kids[0], c));
+        case XNode::Func: {
+            Cx a = emitX(x->kids[0], c);
+            const std::string& f = x->id;
+            if (f == "exp") return G.cexp(a);
+            if (f == "log") return G.clogRef(a);
+            if (f == "sin") return G.csin(a);
+            if (f == "cos") return G.ccos(a);
+            if (f == "sqrt") return G.csqrt(a);
+            if (f == "abs") return G.cr(G.sqrt(G.add(G.mul(a.re, a.re), G.mul(a.im, a.im))));
+            if (f == "re") return G.cr(a.re);
+            if (f == "im") return G.cr(a.im);
+            if (f == "conj") return {a.re, G.neg(a.im)};
+            return a;
+        }
         case XNode::Model: {
             const std::string& id = x->id;
-            if (id == "i") e = "cjc<" + N + ">(0.0, 1.0)";
-            else if (id == "q0") {
-                auto a = emitX(x->kids[0], c), b = emitX(x->kids[1], c), d = emitX(x->kids[2], c);
-                e = "c_q0(" + a + ", " + b + ", " + d + ")";
-            } else if (id == "bf") {
-                auto q = emitX(x->kids[1], c), q0 = emitX(x->kids[2], c), d = emitX(x->kids[3], c);
-                e = "c_bf(" + std::to_string((int)x->kids[0]->v) + ", " + q + ", " + q0 + ", " + d + ".re.v)";
-            } else if (id == "bw") {
-                auto a = emitX(x->kids[0], c), b = emitX(x->kids[1], c), d = emitX(x->kids[2], c);
-                e = "c_bw(" + a + ", " + b + ", " + d + ")";
-            } else if (id == "bwr") {
-                auto mm = emitX(x->kids[0], c), m0 = emitX(x->kids[1], c), g0 = emitX(x->kids[2], c);
-                auto q = emitX(x->kids[4], c), q0 = emitX(x->kids[5], c);
-                e = "c_bwr(" + mm + ", " + m0 + ", " + g0 + ", " + std::to_string((int)x->kids[3]->v) + ", " + q + ", " + q0 +
-                    ", " + num(x->kids[6]->v) + ")";
-            } else if (id == "rho_re" || id == "rho_im") {
-                auto s = emitX(x->kids[0], c), a = emitX(x->kids[1], c), b = emitX(x->kids[2], c);
-                e = "c_" + id + "(" + s + ", " + a + ", " + b + ")";
+            if (id == "i") return G.c(0.0, 1.0);
+            if (id == "q0") {
+                Cx a = emitX(x->kids[0], c), b = emitX(x->kids[1], c), d = emitX(x->kids[2], c);
+                return G.cr(S.q0(a.re, b.re, d.re));
             }
-            break;
+            if (id == "bf") {
+                Cx q = emitX(x->kids[1], c), q0 = emitX(x->kids[2], c), d = emitX(x->kids[3], c);
+                if (!G.isConst(d.re)) throw std::runtime_error("CustomExpr: Bf d must not depend on the event or parameters");
+                return G.cr(S.bf((int)x->kids[0]->v, q.re, q0.re, G.val(d.re)));
+            }
+            if (id == "bw") {
+                Cx mm = emitX(x->kids[0], c), m0 = emitX(x->kids[1], c), g0 = emitX(x->kids[2], c);
+                return S.bw(mm.re, m0.re, g0.re);
+            }
+            if (id == "bwr") {
+                Cx mm = emitX(x->kids[0], c), m0 = emitX(x->kids[1], c), g0 = emitX(x->kids[2], c);
+                Cx q = emitX(x->kids[4], c), q0 = emitX(x->kids[5], c);
+                return S.bwr(mm.re, m0.re, g0.re, (int)x->kids[3]->v, q.re, q0.re, x->kids[6]->v);
+            }
+            if (id == "rho_re" || id == "rho_im") {
+                Cx s = emitX(x->kids[0], c), a = emitX(x->kids[1], c), b = emitX(x->kids[2], c);
+                return G.cr(G.rho(id == "rho_im", s.re, a.re, b.re));
+            }
+            return G.c(1.0);
         }
         }
-        body << "      const CJet<" << N << "> " << r << " = " << e << ";\n";
-        return r;
+        return G.c(0.0);
     }
 
-    std::string table(const std::vector<double>& v)
+    // parameter value nodes of block b: theta leaves (per-call blocks) or constants
+    std::vector<std::vector<int>> params(const Block& b)
     {
-        std::string name = "ct_tab" + std::to_string(ntab++);
-        globals << "__device__ const double " << name << "[" << std::max<size_t>(1, v.size()) << "] = {";
-        for (size_t i = 0; i < v.size(); ++i) globals << (i ? ", " : "") << num(v[i]);
-        if (v.empty()) globals << "0.0";
-        globals << "};\n";
-        return name;
-    }
-
-    void block(int bi, int& der)
-    {
-        const Block& b = m.blocks[bi];
-        const Group& g = m.groups[b.group];
-        // local fitted parameters
-        std::vector<std::vector<std::string>> par(b.res.size());
-        std::vector<int> loc_theta;
-        for (size_t r = 0; r < b.res.size(); ++r)
-            for (size_t p = 0; p < b.res[r].params.size(); ++p)
-                if (b.res[r].theta[p] >= 0 && b.free_path) loc_theta.push_back(b.res[r].theta[p]);
-        int N = (int)loc_theta.size();
-        if (N > 16) throw std::runtime_error("more than 16 fitted parameters in one amplitude block");
-        std::string NS = std::to_string(N);
-        body << "  { // block " << bi << ":";
-        for (const auto& r : b.res) body << " " << r.name;
-        body << (b.free_path ? " (per-call)" : " (fixed)") << "\n";
-        int k = 0;
+        std::vector<std::vector<int>> par(b.res.size());
         for (size_t r = 0; r < b.res.size(); ++r)
             for (size_t p = 0; p < b.res[r].params.size(); ++p) {
-                std::string nm = "r" + std::to_string(r) + "p" + std::to_string(p);
-                par[r].push_back(nm);
                 int th = b.free_path ? b.res[r].theta[p] : -1;
-                if (th >= 0) body << "    const Jet<" << NS << "> " << nm << " = jvar<" << NS << ">(th[" << th << "], " << k++ << ");\n";
-                else body << "    const Jet<" << NS << "> " << nm << " = jc<" << NS << ">(" << num(b.res[r].params[p]) << ");\n";
+                par[r].push_back(th >= 0 ? G.theta(th) : G.cnst(b.res[r].params[p]));
             }
-        for (int s = 0; s < g.nSL(); ++s) {
-            int a = b.site + s;
-            body << "    { // column " << a << "\n";
-            body << "      CJet<" << NS << "> F = cjc<" << NS << ">(1.0, 0.0);\n";
-            for (size_t ni = 0; ni < g.nodes.size(); ++ni) nodeFactor(b, g, (int)ni, s, N, par);
-            body << "      Fr[" << a << "] = F.re.v; Fi[" << a << "] = F.im.v;\n";
-            for (int q = 0; q < N; ++q)
-                body << "      dFr[" << der + q << "] = F.re.d[" << q << "]; dFi[" << der + q << "] = F.im.d[" << q << "];\n";
-            body << "    }\n";
-            for (int q = 0; q < N; ++q) der_entries.push_back({a, loc_theta[q]});
-            der += N;
-        }
-        body << "  }\n";
+        return par;
     }
-    std::vector<std::pair<int, int>> der_entries;
 
-    void nodeFactor(const Block& b, const Group& g, int ni, int s, int N, const std::vector<std::vector<std::string>>& par)
+    Cx nodeFactor(const Block& b, const Group& g, int ni, int s, const std::vector<std::vector<int>>& par)
     {
         const ModelNode& n = g.nodes[ni];
         int gi = b.group;
         int L = n.sls[g.sl_combs[s][ni]].L;
-        std::string NS = std::to_string(N);
-        auto jcs = [&](const std::string& e) { return "jc<" + NS + ">(" + e + ")"; };
         if (b.free_path) {
             int match = -1;
             for (size_t r = 0; r < b.res.size(); ++r)
@@ -423,102 +518,71 @@ struct Gen {
                     match = (int)r;
                     break;
                 }
-            std::string qq = kv(slot(AG_K_Q_, gi, n.mother, n.d1, n.d2));
-            auto mdq = [&](int k) -> std::string {
-                if (n.mass[k + 1] > 0) return jcs(num(n.mass[k + 1]));
+            int qq = kin(AG_K_Q_, gi, n.mother, n.d1, n.d2);
+            auto mdq = [&](int k) -> int {
+                if (n.mass[k + 1] > 0) return G.cnst(n.mass[k + 1]);
                 int di = k == 0 ? n.d1 : n.d2;
                 for (size_t r = 0; r < b.res.size(); ++r)
                     if (b.res[r].particle_idx == di && !par[r].empty()) return par[r][0];
-                return jcs(kv(slot(AG_K_MASS_, gi, di)));
+                return kin(AG_K_MASS_, gi, di);
             };
-            std::string md1 = mdq(0), md2 = mdq(1);
+            int md1 = mdq(0), md2 = mdq(1);
             if (match < 0) {
-                if (!n.has_bf) return;
-                std::string m0q;
-                m0q = jcs(num(n.mass[0] > 0 ? n.mass[0] : 1.0));
-                body << "      F = F * cjr(ls_bf<" << NS << ">(" << L << ", " << jcs(qq) << ", ls_breakup<" << NS << ">(" << m0q
-                     << ", " << md1 << ", " << md2 << "), " << num(n.bf_d) << "));\n";
-                return;
+                if (!n.has_bf) return G.c(1.0);
+                int q0 = S.breakup(G.cnst(n.mass[0] > 0 ? n.mass[0] : 1.0), md1, md2);
+                return G.cr(S.bf(L, qq, q0, n.bf_d));
             }
             const ResInstance& R = b.res[match];
             const auto& P = par[match];
-            std::string mm = kv(slot(AG_K_MASS_, gi, n.mother));
-            std::string m0 = P.empty() ? jcs("1.0") : P[0];
-            auto dep = [&](int k) -> std::string {
-                if (R.md_src[k] == MassSource::Fixed) return jcs(num(R.md_fixed[k]));
+            int mm = kin(AG_K_MASS_, gi, n.mother);
+            int m0 = P.empty() ? G.one() : P[0];
+            auto dep = [&](int k) -> int {
+                if (R.md_src[k] == MassSource::Fixed) return G.cnst(R.md_fixed[k]);
                 if (R.md_src[k] == MassSource::M0Param) return m0;
                 return k == 0 ? md1 : md2;
             };
-            std::string q0r = "ls_q0<" + NS + ">(" + m0 + ", " + dep(0) + ", " + dep(1) + ")";
-            std::string bfx = R.has_bf ? " * cjr(ls_bf<" + NS + ">(" + std::to_string(L) + ", " + jcs(qq) + ", q0r, " + num(R.d) + "))" : "";
-            body << "      {\n        const Jet<" << NS << "> q0r = " << q0r << ";\n";
+            int q0r = S.q0(m0, dep(0), dep(1));
+            Cx bfx = R.has_bf ? G.cr(S.bf(L, qq, q0r, R.d)) : G.c(1.0);
             switch (R.type) {
-            case ModelType::BWR:
-                body << "        F = F * (ls_bwr<" << NS << ">(" << jcs(mm) << ", " << P[0] << ", " << P[1] << ", " << R.Lmin << ", "
-                     << jcs(qq) << ", q0r, " << num(R.has_bf ? R.d : 0.0) << ")" << bfx << ");\n";
-                break;
-            case ModelType::BW:
-                body << "        F = F * ls_bw<" << NS << ">(" << jcs(mm) << ", " << P[0] << ", " << P[1] << ");\n";
-                break;
-            case ModelType::ONE:
-                if (R.has_bf) body << "        F = F * cjr(ls_bf<" << NS << ">(" << L << ", " << jcs(qq) << ", q0r, " << num(R.d) << "));\n";
-                break;
+            case ModelType::BWR: return G.cmul(S.bwr(mm, P[0], P[1], R.Lmin, qq, q0r, R.has_bf ? R.d : 0.0), bfx);
+            case ModelType::BW: return S.bw(mm, P[0], P[1]);
+            case ModelType::ONE: return bfx;
             case ModelType::Flatte: {
-                int nch = (int)R.channels.size();
-                std::vector<double> ch;
-                for (auto& c : R.channels) {
-                    ch.push_back(c.first);
-                    ch.push_back(c.second);
+                std::vector<int> gs, ch;
+                for (size_t i = 0; i < R.channels.size(); ++i) {
+                    gs.push_back(1 + i < P.size() ? P[1 + i] : G.zero());
+                    ch.push_back(G.cnst(R.channels[i].first));
+                    ch.push_back(G.cnst(R.channels[i].second));
                 }
-                body << "        const Jet<" << NS << "> gg[" << std::max(1, nch) << "] = {";
-                for (int i = 0; i < std::max(1, nch); ++i)
-                    body << (i ? ", " : "") << ((size_t)(1 + i) < P.size() ? P[1 + i] : jcs("0.0"));
-                body << "};\n        F = F * (ls_flatte<" << NS << ", " << nch << ">(" << jcs(mm) << ", " << P[0] << ", gg, "
-                     << table(ch) << ")" << bfx << ");\n";
-                break;
+                return G.cmul(S.flatte(mm, P[0], gs, ch), bfx);
             }
             case ModelType::GS: {
                 double mpi = R.channels.empty() ? 0.1396 : R.channels[0].first;
-                body << "        F = F * (ls_gs<" << NS << ">(" << jcs(mm) << ", " << jcs(qq) << ", " << P[0] << ", " << P[1]
-                     << ", q0r, " << num(mpi) << ")" << bfx << ");\n";
-                break;
+                return G.cmul(S.gs(mm, qq, P[0], P[1], q0r, mpi), bfx);
             }
             case ModelType::Custom: {
                 XParser ps(R.options.at("expr"), R.param_names);
-                XP x = ps.parse();
                 XCtx c;
-                c.N = N;
                 c.mm = mm;
                 c.qq = qq;
                 c.md1 = md1;
                 c.md2 = md2;
-                c.L = std::to_string(L);
-                c.d = num(n.bf_d);
+                c.d = G.cnst(n.bf_d);
+                c.L = L;
                 c.par = P;
                 c.gi = gi;
                 c.d1 = n.d1;
                 c.d2 = n.d2;
-                std::string r = emitX(x, c);
-                body << "        F = F * " << r << ";\n";
-                break;
+                return emitX(ps.parse(), c);
             }
-            case ModelType::Interp: {
-                std::string tb = table(R.aux);
-                body << "        { double fr, fi; ls_interp(" << tb << ", " << mm << ", fr, fi); F = F * cjc<" << NS << ">(fr, fi); }\n";
-                break;
+            case ModelType::Interp: return table(R.aux, mm, true);
+            case ModelType::Hist: return table(R.aux, mm, false);
             }
-            case ModelType::Hist: {
-                std::string tb = table(R.aux);
-                body << "        F = F * cjc<" << NS << ">(ls_hist(" << mm << ", " << tb << "), 0.0);\n";
-                break;
-            }
-            }
-            body << "      }\n";
-            return;
+            return G.c(1.0);
         }
-        // ---- fixed-parameter block ----
-        std::string mm = kv(slot(AG_K_MASS_, gi, n.mother));
-        std::string qq = kv(slot(AG_K_QRAW_, gi, n.mother, n.d1, n.d2));
+        // ---- fixed-parameter block (values only) ----
+        int mm = kin(AG_K_MASS_, gi, n.mother);
+        int qq = kin(AG_K_QRAW_, gi, n.mother, n.d1, n.d2);
         int match = -1;
         for (size_t r = 0; r < b.res.size(); ++r)
             if (b.res[r].particle_idx == n.mother) {
@@ -535,105 +599,242 @@ struct Gen {
         };
         ma = sub(ma, n.d1);
         mb = sub(mb, n.d2);
-        double q0 = std::sqrt((mo * mo - std::pow(ma + mb, 2)) * (mo * mo - std::pow(ma - mb, 2))) / 2 / mo;
-        std::string Q = jcs(qq), Q0 = jcs(num(q0));
-        if (ni == 0) {
-            if (n.has_bf) body << "      F = F * cjr(ls_bf<" << NS << ">(" << L << ", " << Q << ", " << Q0 << ", " << num(n.bf_d) << "));\n";
-            return;
-        }
-        if (match < 0) return;
+        int q0 = G.cnst(std::sqrt((mo * mo - std::pow(ma + mb, 2)) * (mo * mo - std::pow(ma - mb, 2))) / 2 / mo);
+        if (ni == 0) return n.has_bf ? G.cr(S.bf(L, qq, q0, n.bf_d)) : G.c(1.0);
+        if (match < 0) return G.c(1.0);
         const ResInstance& R = b.res[match];
         const auto& P = par[match];
-        std::string bfx = n.has_bf ? " * cjr(ls_bf<" + NS + ">(" + std::to_string(L) + ", " + Q + ", " + Q0 + ", " + num(n.bf_d) + "))" : "";
+        Cx bfx = n.has_bf ? G.cr(S.bf(L, qq, q0, n.bf_d)) : G.c(1.0);
         switch (R.type) {
-        case ModelType::BWR:
-            body << "      F = F * (ls_bwr<" << NS << ">(" << jcs(mm) << ", " << P[0] << ", " << P[1] << ", " << n.l_min << ", " << Q
-                 << ", " << Q0 << ", " << num(n.has_bf ? n.bf_d : 0.0) << ")" << bfx << ");\n";
-            break;
-        case ModelType::BW: body << "      F = F * ls_bw<" << NS << ">(" << jcs(mm) << ", " << P[0] << ", " << P[1] << ");\n"; break;
-        case ModelType::ONE: if (n.has_bf) body << "      F = F * cjr(ls_bf<" << NS << ">(" << L << ", " << Q << ", " << Q0 << ", " << num(n.bf_d) << "));\n"; break;
+        case ModelType::BWR: return G.cmul(S.bwr(mm, P[0], P[1], n.l_min, qq, q0, n.has_bf ? n.bf_d : 0.0), bfx);
+        case ModelType::BW: return S.bw(mm, P[0], P[1]);
+        case ModelType::ONE: return bfx;
         case ModelType::Flatte: {
-            int nch = (int)R.channels.size();
-            std::vector<double> ch;
-            for (auto& c : R.channels) {
-                ch.push_back(c.first);
-                ch.push_back(c.second);
+            std::vector<int> gs, ch;
+            for (size_t i = 0; i < R.channels.size(); ++i) {
+                gs.push_back(1 + i < P.size() ? P[1 + i] : G.zero());
+                ch.push_back(G.cnst(R.channels[i].first));
+                ch.push_back(G.cnst(R.channels[i].second));
             }
-            body << "      { const Jet<" << NS << "> gg[" << std::max(1, nch) << "] = {";
-            for (int i = 0; i < std::max(1, nch); ++i) body << (i ? ", " : "") << ((size_t)(1 + i) < P.size() ? P[1 + i] : jcs("0.0"));
-            body << "};\n        F = F * (ls_flatte_fixed<" << NS << ", " << nch << ">(" << jcs(mm) << ", " << P[0] << ", gg, "
-                 << table(ch) << ")" << bfx << "); }\n";
-            break;
+            return G.cmul(S.flatteFixed(mm, P[0], gs, ch), bfx);
         }
-        case ModelType::Hist: body << "      F = F * cjc<" << NS << ">(ls_hist(" << mm << ", " << table(R.aux) << "), 0.0);\n"; break;
+        case ModelType::Hist: return table(R.aux, mm, false);
         case ModelType::Custom: {
             // value segment with md1 = md2 = 0, no daughter kinematics, at most 3 params
             XParser ps(R.options.at("expr"), R.param_names);
-            XP x = ps.parse();
             XCtx c;
-            c.N = N;
             c.mm = mm;
             c.qq = qq;
-            c.md1 = jcs("0.0");
-            c.md2 = jcs("0.0");
-            c.L = std::to_string(L);
-            c.d = num(n.bf_d);
-            for (size_t i = 0; i < P.size(); ++i) c.par.push_back(i < 3 ? P[i] : jcs("0.0"));
-            body << "      {\n";
-            std::string r = emitX(x, c);
-            body << "      F = F * " << r << ";\n      }\n";
-            break;
+            c.md1 = G.zero();
+            c.md2 = G.zero();
+            c.d = G.cnst(n.bf_d);
+            c.L = L;
+            for (size_t i = 0; i < P.size(); ++i) c.par.push_back(i < 3 ? P[i] : G.zero());
+            return emitX(ps.parse(), c);
         }
-        default: break;  // GS / Interp: no fixed-parameter factor in the reference
+        default: return G.c(1.0);  // GS / Interp have no fixed-parameter factor in the reference
         }
     }
 
-    // slot type ids mirrored from angular.cuh
-    static constexpr int AG_K_MASS_ = 0, AG_K_Q_ = 1, AG_K_QRAW_ = 2, AG_K_P_ = 3, AG_K_E_ = 4, AG_K_CT_ = 5, AG_K_PHI_ = 6;
-
-    void run()
+    // table lookups become opaque per-event values computed by generated helper calls
+    struct TabUse {
+        int table, mnode;
+        bool interp;
+        int re_kin, im_kin;  // pseudo kin slots holding the looked-up values
+    };
+    std::vector<TabUse> tab_uses;
+    Cx table(const std::vector<double>& aux, int mnode, bool interp)
     {
-        out.group_plane0.clear();
-        int pl = 0;
-        for (const auto& g : m.groups) {
-            out.group_plane0.push_back(pl);
-            pl += g.nSL();
-        }
-        out.nplane = pl;
-        int der = 0;
-        for (size_t b = 0; b < m.blocks.size(); ++b) block((int)b, der);
-        out.nder = der;
-        std::ostringstream h;
-        h << "// generated by ctpwa_b200 codegen: model-specific lineshape products\n#pragma once\n";
-        h << "#define M_NA " << m.nAmp() << "\n#define M_NPOL " << m.npol << "\n#define M_NPLANE " << out.nplane
-          << "\n#define M_NKIN " << out.slots.size() << "\n#define M_NTH " << m.nTheta() << "\n#define M_NDER " << der << "\n";
-        h << "__device__ __forceinline__ double ct_nan() { return __longlong_as_double(0x7ff8000000000000LL); }\n";
-        h << "__device__ __forceinline__ double ct_inf() { return __longlong_as_double(0x7ff0000000000000LL); }\n";
-        h << "__device__ __forceinline__ int col_plane(int a) {\n  switch (a) {\n";
-        for (const auto& b : m.blocks)
-            for (int s = 0; s < m.groups[b.group].nSL(); ++s)
-                h << "  case " << b.site + s << ": return " << out.group_plane0[b.group] + s << ";\n";
-        h << "  default: return 0;\n  }\n}\n";
-        h << "__device__ __forceinline__ int der_col(int k) {\n  switch (k) {\n";
-        for (size_t k = 0; k < der_entries.size(); ++k) h << "  case " << k << ": return " << der_entries[k].first << ";\n";
-        h << "  default: return 0;\n  }\n}\n";
-        h << "__device__ __forceinline__ int der_th(int k) {\n  switch (k) {\n";
-        for (size_t k = 0; k < der_entries.size(); ++k) h << "  case " << k << ": return " << der_entries[k].second << ";\n";
-        h << "  default: return 0;\n  }\n}\n";
-        h << globals.str();
-        h << "__device__ __forceinline__ void model_columns(const double* __restrict__ kv, const double* __restrict__ th,\n"
-             "    double* Fr, double* Fi, double* dFr, double* dFi)\n{\n  (void)kv; (void)th; (void)dFr; (void)dFi;\n";
-        h << body.str() << "}\n";
-        out.header = h.str();
+        int t = (int)tables.size();
+        tables.push_back(aux);
+        // represent the looked-up value as pseudo "kin" leaves with negative ids resolved at emission
+        int re = G.kin(-1000 - 2 * (int)tab_uses.size()), im = G.kin(-1001 - 2 * (int)tab_uses.size());
+        tab_uses.push_back({t, mnode, interp, re, im});
+        return {re, interp ? im : G.zero()};
     }
+
+    std::string emit();
 };
+
+std::string Gen::emit()
+{
+    const auto& N = G.nodes;
+    // roots
+    std::vector<int> roots;
+    for (const auto& c : cols) {
+        roots.push_back(c.re);
+        roots.push_back(c.im);
+        for (const auto& d : c.der) {
+            roots.push_back(d.second.first);
+            roots.push_back(d.second.second);
+        }
+    }
+    for (const auto& t : tab_uses) roots.push_back(t.mnode);
+    std::vector<char> live(N.size(), 0);
+    std::vector<int> stack(roots.begin(), roots.end());
+    while (!stack.empty()) {
+        int x = stack.back();
+        stack.pop_back();
+        if (x < 0 || live[x]) continue;
+        live[x] = 1;
+        for (int k : {N[x].a, N[x].b, N[x].c})
+            if (k >= 0) stack.push_back(k);
+    }
+    // constant slots: theta-only nodes used by event nodes or roots
+    std::vector<int> cslot(N.size(), -1);
+    int ncon = 0;
+    auto isTheta = [&](int x) { return N[x].dep == dag::DEP_THETA; };
+    std::vector<char> needC(N.size(), 0);
+    for (size_t x = 0; x < N.size(); ++x) {
+        if (!live[x] || !(N[x].dep & dag::DEP_EVENT)) continue;
+        for (int k : {N[x].a, N[x].b, N[x].c})
+            if (k >= 0 && isTheta(k)) needC[k] = 1;
+    }
+    for (int r : roots)
+        if (r >= 0 && isTheta(r)) needC[r] = 1;
+    for (size_t x = 0; x < N.size(); ++x)
+        if (needC[x] && N[x].op != dag::Theta) cslot[x] = ncon++;
+    auto lit = [&](double v) { return num(v); };
+    // expression of node x in a context (prologue: theta-only names; event: C[] / event names)
+    auto ref = [&](int x, bool event_ctx) -> std::string {
+        const auto& nd = N[x];
+        if (nd.op == dag::Const) return lit(nd.v);
+        if (nd.op == dag::Theta) return "th[" + std::to_string(nd.idx) + "]";
+        if (event_ctx && nd.dep == dag::DEP_THETA) return "C[" + std::to_string(cslot[x]) + "]";
+        return (event_ctx ? "e" : "t") + std::to_string(x);
+    };
+    auto expr = [&](int x, bool ev) -> std::string {
+        const auto& nd = N[x];
+        auto A = [&]() { return ref(nd.a, ev); };
+        auto B = [&]() { return ref(nd.b, ev); };
+        switch (nd.op) {
+        case dag::Kin: {
+            if (nd.idx >= 0) return "kv[" + std::to_string(nd.idx) + "]";
+            int u = (-nd.idx - 1000) / 2;
+            return ((-nd.idx - 1000) % 2 == 0 ? "tre" : "tim") + std::to_string(u);
+        }
+        case dag::Add: return A() + " + " + B();
+        case dag::Sub: return A() + " - " + B();
+        case dag::Mul: return A() + " * " + B();
+        case dag::Recip: return "1.0 / " + A();
+        case dag::Neg: return "-" + A();
+        case dag::Sqrt: return "sqrt(" + A() + ")";
+        case dag::Log: return "log(" + A() + ")";
+        case dag::Exp: return "exp(" + A() + ")";
+        case dag::Sin: return "sin(" + A() + ")";
+        case dag::Cos: return "cos(" + A() + ")";
+        case dag::Atan2: return "atan2(" + A() + ", " + B() + ")";
+        case dag::Sel: {
+            static const char* ops[] = {">=", ">", "<=", "<", "=="};
+            return "(" + ref(nd.c, ev) + " " + ops[nd.cmp] + " 0.0 ? " + A() + " : " + B() + ")";
+        }
+        case dag::RhoRe: return "ct_rho(" + A() + ", " + B() + ", " + ref(nd.c, ev) + ", 0)";
+        case dag::RhoIm: return "ct_rho(" + A() + ", " + B() + ", " + ref(nd.c, ev) + ", 1)";
+        default: return lit(nd.v);
+        }
+    };
+    std::ostringstream pro, evs;
+    for (size_t x = 0; x < N.size(); ++x) {
+        if (!live[x] || N[x].op == dag::Const || N[x].op == dag::Theta) continue;
+        if (N[x].dep == dag::DEP_THETA) {
+            pro << "  const double t" << x << " = " << expr((int)x, false) << ";\n";
+            if (cslot[x] >= 0) pro << "  C[" << cslot[x] << "] = t" << x << ";\n";
+        }
+    }
+    // table lookups (opaque per-event values) first
+    for (size_t u = 0; u < tab_uses.size(); ++u) {
+        const auto& t = tab_uses[u];
+        if (t.interp)
+            evs << "  double tre" << u << ", tim" << u << "; ls_interp(ct_tab" << t.table << ", " << ref(t.mnode, true)
+                << ", tre" << u << ", tim" << u << ");\n";
+        else
+            evs << "  const double tre" << u << " = ls_hist(" << ref(t.mnode, true) << ", ct_tab" << t.table
+                << "), tim" << u << " = 0.0;\n";
+    }
+    for (size_t x = 0; x < N.size(); ++x) {
+        if (!live[x] || N[x].op == dag::Const || N[x].op == dag::Theta) continue;
+        if (N[x].dep & dag::DEP_EVENT) evs << "  const double e" << x << " = " << expr((int)x, true) << ";\n";
+    }
+    // outputs
+    int k = 0;
+    std::vector<std::pair<int, int>> der_entries;
+    for (size_t a = 0; a < cols.size(); ++a) {
+        evs << "  Fr[" << a << "] = " << ref(cols[a].re, true) << "; Fi[" << a << "] = " << ref(cols[a].im, true) << ";\n";
+        for (const auto& d : cols[a].der) {
+            evs << "  dFr[" << k << "] = " << ref(d.second.first, true) << "; dFi[" << k << "] = "
+                << ref(d.second.second, true) << ";\n";
+            der_entries.push_back({(int)a, d.first});
+            ++k;
+        }
+    }
+    out.nder = k;
+    std::ostringstream h;
+    h << "// generated by ctpwa_b200 codegen: model-specific lineshape products\n#pragma once\n";
+    h << "#define M_NA " << m.nAmp() << "\n#define M_NPOL " << m.npol << "\n#define M_NPLANE " << out.nplane
+      << "\n#define M_NKIN " << out.slots.size() << "\n#define M_NTH " << m.nTheta() << "\n#define M_NDER " << k
+      << "\n#define M_NCONST " << ncon << "\n";
+    h << "__device__ __forceinline__ int col_plane(int a) {\n  switch (a) {\n";
+    for (const auto& b : m.blocks)
+        for (int s = 0; s < m.groups[b.group].nSL(); ++s)
+            h << "  case " << b.site + s << ": return " << out.group_plane0[b.group] + s << ";\n";
+    h << "  default: return 0;\n  }\n}\n";
+    h << "__device__ __forceinline__ int der_col(int k) {\n  switch (k) {\n";
+    for (size_t q = 0; q < der_entries.size(); ++q) h << "  case " << q << ": return " << der_entries[q].first << ";\n";
+    h << "  default: return 0;\n  }\n}\n";
+    h << "__device__ __forceinline__ int der_th(int k) {\n  switch (k) {\n";
+    for (size_t q = 0; q < der_entries.size(); ++q) h << "  case " << q << ": return " << der_entries[q].second << ";\n";
+    h << "  default: return 0;\n  }\n}\n";
+    for (size_t t = 0; t < tables.size(); ++t) {
+        h << "__device__ const double ct_tab" << t << "[" << std::max<size_t>(1, tables[t].size()) << "] = {";
+        for (size_t i = 0; i < tables[t].size(); ++i) h << (i ? ", " : "") << num(tables[t][i]);
+        if (tables[t].empty()) h << "0.0";
+        h << "};\n";
+    }
+    h << "// parameter-only subexpressions, evaluated once per likelihood call\n";
+    h << "__device__ __forceinline__ void model_prologue(const double* __restrict__ th, double* __restrict__ C)\n{\n"
+         "  (void)th; (void)C;\n"
+      << pro.str() << "}\n";
+    h << "// per-event lineshape products and their parameter derivatives\n";
+    h << "__device__ __forceinline__ void model_columns(const double* __restrict__ kv, const double* __restrict__ C,\n"
+         "    double* Fr, double* Fi, double* dFr, double* dFi)\n{\n  (void)kv; (void)C; (void)dFr; (void)dFi;\n"
+      << evs.str() << "}\n";
+    return h.str();
+}
 
 }  // namespace
 
 GeneratedModel generateModel(const Model& m)
 {
     Gen g(m);
-    g.run();
+    int pl = 0;
+    for (const auto& gr : m.groups) {
+        g.out.group_plane0.push_back(pl);
+        pl += gr.nSL();
+    }
+    g.out.nplane = pl;
+    g.cols.resize(m.nAmp());
+    for (const auto& b : m.blocks) {
+        const Group& gr = m.groups[b.group];
+        auto par = g.params(b);
+        std::vector<int> ths;
+        if (b.free_path)
+            for (const auto& r : b.res)
+                for (int t : r.theta)
+                    if (t >= 0 && std::find(ths.begin(), ths.end(), t) == ths.end()) ths.push_back(t);
+        for (int s = 0; s < gr.nSL(); ++s) {
+            Cx F = g.G.c(1.0);
+            for (size_t ni = 0; ni < gr.nodes.size(); ++ni) F = g.G.cmul(F, g.nodeFactor(b, gr, (int)ni, s, par));
+            auto& col = g.cols[b.site + s];
+            col.re = F.re;
+            col.im = F.im;
+            for (int t : ths) {
+                int dr = g.G.deriv(F.re, t), di = g.G.deriv(F.im, t);
+                if (g.G.isConst(dr) && g.G.val(dr) == 0.0 && g.G.isConst(di) && g.G.val(di) == 0.0) continue;
+                col.der.push_back({t, {dr, di}});
+            }
+        }
+    }
+    g.out.header = g.emit();
     return g.out;
 }
 

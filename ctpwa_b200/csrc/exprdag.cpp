@@ -1,0 +1,298 @@
+// Expression DAG (see exprdag.hpp).
+#include "exprdag.hpp"
+
+#include <cmath>
+#include <stdexcept>
+
+namespace ctpwa {
+namespace dag {
+
+namespace {
+double foldUnary(Op op, double x)
+{
+    switch (op) {
+    case Neg: return -x;
+    case Sqrt: return std::sqrt(x);
+    case Log: return std::log(x);
+    case Exp: return std::exp(x);
+    case Sin: return std::sin(x);
+    case Cos: return std::cos(x);
+    default: return x;
+    }
+}
+bool cmpTrue(Cmp c, double x)
+{
+    switch (c) {
+    case GE0: return x >= 0.0;
+    case GT0: return x > 0.0;
+    case LE0: return x <= 0.0;
+    case LT0: return x < 0.0;
+    case EQ0: return x == 0.0;
+    }
+    return false;
+}
+}  // namespace
+
+Graph::Graph()
+{
+    zero_ = cnst(0.0);
+    one_ = cnst(1.0);
+}
+
+int Graph::make(Node n)
+{
+    auto key = std::make_tuple((int)n.op, (int)n.cmp, n.a, n.b, n.c, n.v, n.idx);
+    auto it = memo_.find(key);
+    if (it != memo_.end()) return it->second;
+    uint8_t dep = 0;
+    if (n.op == Theta) dep = DEP_THETA;
+    else if (n.op == Kin) dep = DEP_EVENT;
+    for (int k : {n.a, n.b, n.c})
+        if (k >= 0) dep |= nodes[k].dep;
+    n.dep = dep;
+    int id = (int)nodes.size();
+    nodes.push_back(n);
+    memo_[key] = id;
+    return id;
+}
+
+int Graph::cnst(double v)
+{
+    Node n;
+    n.op = Const;
+    n.v = v == 0.0 ? 0.0 : v;  // fold -0.0
+    return make(n);
+}
+int Graph::theta(int j)
+{
+    Node n;
+    n.op = Theta;
+    n.idx = j;
+    return make(n);
+}
+int Graph::kin(int k)
+{
+    Node n;
+    n.op = Kin;
+    n.idx = k;
+    return make(n);
+}
+
+int Graph::add(int a, int b)
+{
+    if (isConst(a) && isConst(b)) return cnst(val(a) + val(b));
+    if (isConst(a) && val(a) == 0.0) return b;
+    if (isConst(b) && val(b) == 0.0) return a;
+    if (a > b) std::swap(a, b);
+    Node n;
+    n.op = Add;
+    n.a = a;
+    n.b = b;
+    return make(n);
+}
+int Graph::sub(int a, int b)
+{
+    if (isConst(a) && isConst(b)) return cnst(val(a) - val(b));
+    if (isConst(b) && val(b) == 0.0) return a;
+    if (isConst(a) && val(a) == 0.0) return neg(b);
+    if (a == b) return zero_;
+    Node n;
+    n.op = Sub;
+    n.a = a;
+    n.b = b;
+    return make(n);
+}
+int Graph::mul(int a, int b)
+{
+    if (isConst(a) && isConst(b)) return cnst(val(a) * val(b));
+    if ((isConst(a) && val(a) == 0.0) || (isConst(b) && val(b) == 0.0)) return zero_;
+    if (isConst(a) && val(a) == 1.0) return b;
+    if (isConst(b) && val(b) == 1.0) return a;
+    if (isConst(a) && val(a) == -1.0) return neg(b);
+    if (isConst(b) && val(b) == -1.0) return neg(a);
+    if (a > b) std::swap(a, b);
+    Node n;
+    n.op = Mul;
+    n.a = a;
+    n.b = b;
+    return make(n);
+}
+int Graph::recip(int a)
+{
+    if (isConst(a)) return cnst(1.0 / val(a));
+    if (nodes[a].op == Recip) return nodes[a].a;
+    Node n;
+    n.op = Recip;
+    n.a = a;
+    return make(n);
+}
+
+// a / b as a * (1/b): one reciprocal per denominator, shared by every use and
+// by every derivative (d(1/b) = -(1/b)^2 db needs no further division)
+int Graph::div(int a, int b)
+{
+    if (isConst(a) && isConst(b)) return cnst(val(a) / val(b));
+    if (isConst(b) && val(b) == 1.0) return a;
+    if (isConst(a) && val(a) == 0.0) return zero_;
+    return mul(a, recip(b));
+}
+
+int Graph::neg(int a)
+{
+    if (isConst(a)) return cnst(-val(a));
+    if (nodes[a].op == Neg) return nodes[a].a;
+    Node n;
+    n.op = Neg;
+    n.a = a;
+    return make(n);
+}
+
+#define CT_UNARY(name, OP)             \
+    int Graph::name(int a)             \
+    {                                  \
+        if (isConst(a)) return cnst(foldUnary(OP, val(a))); \
+        Node n;                        \
+        n.op = OP;                     \
+        n.a = a;                       \
+        return make(n);                \
+    }
+CT_UNARY(sqrt, Sqrt)
+CT_UNARY(log, Log)
+CT_UNARY(exp, Exp)
+CT_UNARY(sin, Sin)
+CT_UNARY(cos, Cos)
+#undef CT_UNARY
+
+int Graph::atan2(int y, int x)
+{
+    if (isConst(y) && isConst(x)) return cnst(std::atan2(val(y), val(x)));
+    Node n;
+    n.op = Atan2;
+    n.a = y;
+    n.b = x;
+    return make(n);
+}
+
+int Graph::sel(Cmp cmp, int c, int a, int b)
+{
+    if (isConst(c)) return cmpTrue(cmp, val(c)) ? a : b;
+    if (a == b) return a;
+    Node n;
+    n.op = Sel;
+    n.cmp = cmp;
+    n.a = a;
+    n.b = b;
+    n.c = c;
+    return make(n);
+}
+
+int Graph::rho(bool im, int s, int ma, int mb)
+{
+    Node n;
+    n.op = im ? RhoIm : RhoRe;
+    n.a = s;
+    n.b = ma;
+    n.c = mb;
+    if (isConst(s) && isConst(ma) && isConst(mb)) {
+        double S = (val(ma) + val(mb)) * (val(ma) + val(mb)), D = (val(ma) - val(mb)) * (val(ma) - val(mb));
+        double f1 = 1.0 - S / val(s), f2s = 1.0 - D / val(s), f2 = f2s > 0 ? std::sqrt(f2s) : 0.0;
+        double re = f1 >= 0 ? std::sqrt(f1) * f2 : 0.0, imv = f1 >= 0 ? 0.0 : std::sqrt(-f1) * f2;
+        return cnst(im ? imv : re);
+    }
+    return make(n);
+}
+
+int Graph::powi(int a, int n)
+{
+    if (n < 0) return recip(powi(a, -n));
+    if (n == 0) return one_;
+    if (n == 1) return a;
+    int h = powi(a, n / 2);
+    int h2 = mul(h, h);
+    return (n % 2) ? mul(h2, a) : h2;
+}
+
+int Graph::deriv(int n, int j)
+{
+    const Node nd = nodes[n];
+    if (!(nd.dep & DEP_THETA)) return zero_;
+    auto key = std::make_pair(n, j);
+    auto it = dmemo_.find(key);
+    if (it != dmemo_.end()) return it->second;
+    int r = zero_;
+    switch (nd.op) {
+    case Const:
+    case Kin:
+    case RhoRe:
+    case RhoIm: r = zero_; break;
+    case Theta: r = nd.idx == j ? one_ : zero_; break;
+    case Add: r = add(deriv(nd.a, j), deriv(nd.b, j)); break;
+    case Sub: r = sub(deriv(nd.a, j), deriv(nd.b, j)); break;
+    case Mul: r = add(mul(deriv(nd.a, j), nd.b), mul(nd.a, deriv(nd.b, j))); break;
+    case Recip: r = neg(mul(mul(n, n), deriv(nd.a, j))); break;
+    case Neg: r = neg(deriv(nd.a, j)); break;
+    case Sqrt: r = mul(mul(cnst(0.5), deriv(nd.a, j)), recip(n)); break;
+    case Log: r = div(deriv(nd.a, j), nd.a); break;
+    case Exp: r = mul(n, deriv(nd.a, j)); break;
+    case Sin: r = mul(cos(nd.a), deriv(nd.a, j)); break;
+    case Cos: r = neg(mul(sin(nd.a), deriv(nd.a, j))); break;
+    case Atan2: {
+        int y = nd.a, x = nd.b;
+        int den = add(mul(x, x), mul(y, y));
+        r = div(sub(mul(x, deriv(y, j)), mul(y, deriv(x, j))), den);
+        break;
+    }
+    case Sel: r = sel((Cmp)nd.cmp, nd.c, deriv(nd.a, j), deriv(nd.b, j)); break;
+    }
+    dmemo_[key] = r;
+    return r;
+}
+
+Cx Graph::cmul(Cx a, Cx b)
+{
+    return {sub(mul(a.re, b.re), mul(a.im, b.im)), add(mul(a.re, b.im), mul(a.im, b.re))};
+}
+
+Cx Graph::cdivRef(Cx a, Cx b)
+{
+    int s = add(mul(b.re, b.re), mul(b.im, b.im));
+    s = sel(EQ0, s, cnst(1e-30), s);
+    int is = recip(s);
+    return {mul(add(mul(a.re, b.re), mul(a.im, b.im)), is), mul(sub(mul(a.im, b.re), mul(a.re, b.im)), is)};
+}
+
+Cx Graph::cexp(Cx a)
+{
+    int e = exp(a.re);
+    return {mul(e, cos(a.im)), mul(e, sin(a.im))};
+}
+
+Cx Graph::clogRef(Cx a)
+{
+    int r = sqrt(add(mul(a.re, a.re), mul(a.im, a.im)));
+    r = sel(EQ0, r, cnst(1e-30), r);
+    return {log(r), atan2(a.im, a.re)};
+}
+
+Cx Graph::csqrt(Cx a)
+{
+    int r = sqrt(add(mul(a.re, a.re), mul(a.im, a.im)));
+    int re = sqrt(mul(add(r, a.re), cnst(0.5)));
+    int im = sqrt(mul(sub(r, a.re), cnst(0.5)));
+    return {re, sel(LT0, a.im, neg(im), im)};
+}
+
+Cx Graph::csin(Cx a)
+{
+    int ep = exp(a.im), em = exp(neg(a.im));
+    return {mul(mul(sin(a.re), add(ep, em)), cnst(0.5)), mul(mul(cos(a.re), sub(ep, em)), cnst(0.5))};
+}
+
+Cx Graph::ccos(Cx a)
+{
+    int ep = exp(a.im), em = exp(neg(a.im));
+    return {mul(mul(cos(a.re), add(ep, em)), cnst(0.5)), neg(mul(mul(sin(a.re), sub(ep, em)), cnst(0.5)))};
+}
+
+}  // namespace dag
+}  // namespace ctpwa

@@ -39,7 +39,7 @@ def test_counts_and_names_match_oracle(setups, name):
     assert ana.getNVector() == orc.nV
     assert ana.getNFreeTheta() == orc.nT
     assert ana.getNEvents() == orc.nev
-    assert len(ana.getParamNames()) == ana.getNParams()
+    assert len(ana.getParamNames()) == ana.getNVector() + ana.getNFreeTheta()
 
 
 @pytest.mark.parametrize("name", list(SMALL))
