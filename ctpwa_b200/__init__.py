@@ -309,6 +309,21 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return out
 
+    def setKernelTiming(self, slots: int):
+        """Record CUDA events around each fused-kernel launch (ring of `slots`; 0 = off)."""
+        self._check()
+        if self._lib.ctpwa_kernel_timing(self._h, int(slots)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+
+    def kernelTimes(self, cap: int = 1 << 16):
+        """Durations (ms) of the most recent fused-kernel launches, oldest first."""
+        self._check()
+        buf = (ctypes.c_float * cap)()
+        n = self._lib.ctpwa_kernel_times(self._h, buf, cap)
+        if n < 0:
+            raise RuntimeError(_lib.error(self._h))
+        return [buf[i] for i in range(n)]
+
     def lastParts(self):
         """[data_nll, bkg_nll, sum_phsp_intensity, W_data, W_bkg, n_phsp] of the last evaluation."""
         self._check()

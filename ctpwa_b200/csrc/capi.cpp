@@ -166,6 +166,27 @@ int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream)
     return CTPWA_OK;
 }
 
+int ctpwa_kernel_timing(ctpwa_handle* h, int slots)
+{
+    if (!h) return CTPWA_ERR_ARG;
+    try {
+        h->eng->setKernelTiming(slots);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_kernel_times(ctpwa_handle* h, float* ms, int cap)
+{
+    if (!h || (!ms && cap > 0) || cap < 0) return setErr(h, CTPWA_ERR_ARG, "bad argument");
+    try {
+        return h->eng->kernelTimes(ms, cap);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+}
+
 long long ctpwa_n_events(const ctpwa_handle* h, int kind)
 {
     if (!h || kind < 0 || kind > 2) return CTPWA_ERR_ARG;

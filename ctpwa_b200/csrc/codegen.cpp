@@ -8,6 +8,10 @@
 //                    computeNodeFactor (include/ResModel.cuh:103-181)
 #include "codegen.hpp"
 
+#include "exprdag.hpp"
+
+#include <algorithm>
+
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -259,6 +263,9 @@ private:
 };
 
 // ------------------------------------------------------------- generator
+// kinematic slot types (angular.cuh AG_K_*)
+constexpr int AG_K_MASS_ = 0, AG_K_Q_ = 1, AG_K_QRAW_ = 2, AG_K_P_ = 3, AG_K_E_ = 4, AG_K_CT_ = 5, AG_K_PHI_ = 6;
+
 using dag::Cx;
 using dag::Graph;
 
@@ -768,6 +775,7 @@ std::string Gen::emit()
         }
     }
     out.nder = k;
+    out.nconst = ncon;
     std::ostringstream h;
     h << "// generated by ctpwa_b200 codegen: model-specific lineshape products\n#pragma once\n";
     h << "#define M_NA " << m.nAmp() << "\n#define M_NPOL " << m.npol << "\n#define M_NPLANE " << out.nplane

@@ -28,6 +28,7 @@ struct GeneratedModel {
     int nplane = 0;              // angular planes = sum over groups of nSL
     std::vector<int> group_plane0;
     int nder = 0;
+    int nconst = 0;              // parameter-only subexpressions kept per call
 };
 
 GeneratedModel generateModel(const Model& m);

@@ -645,6 +645,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     // evaluation buffers
     int nA = model_.nAmp();
     CT_CUDA(cudaMalloc(&d_v_, sizeof(double) * 2 * nA));
+    CT_CUDA(cudaMalloc(&d_consts_, sizeof(double) * std::max(1, gen_.nconst)));
     std::vector<double> ratio = model_.coupling.ratio;
     CT_CUDA(cudaMalloc(&d_amp_chain_, sizeof(int) * nA));
     CT_CUDA(cudaMalloc(&d_ratio_, sizeof(double) * nA));
@@ -700,12 +701,17 @@ Engine::~Engine()
     }
     cudaFree(d_ag_tables_);
     cudaFree(d_v_);
+    cudaFree(d_consts_);
     cudaFree(d_partials_);
     cudaFree(d_parts_);
     cudaFree(d_amp_chain_);
     cudaFree(d_ratio_);
     cudaFree(d_gauss_idx_);
     cudaFree(d_gauss_ms_);
+    for (size_t i = 0; i < ev_begin_.size(); ++i) {
+        cudaEventDestroy(ev_begin_[i]);
+        cudaEventDestroy(ev_end_[i]);
+    }
     if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
 }
 
@@ -963,14 +969,13 @@ void Engine::computeAngular(int kind)
 std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
 {
     std::string dir = kernelDir();
-    std::string jet = readFile(dir + "/jet.cuh");
-    std::string ls = readFile(dir + "/lineshapes.cuh");
+    std::string helpers = readFile(dir + "/device_helpers.cuh");
     std::string fused = readFile(dir + "/fused_nll.cuh");
     std::string src = "#include \"fused_nll.cuh\"\n";
     const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
                           "--fmad=true", "-lineinfo"};
     const int nopts = 6;
-    std::string key_src = jet + ls + fused + gen.header;
+    std::string key_src = helpers + fused + gen.header;
     for (int i = 0; i < nopts; ++i) key_src += opts[i];
     int nvmaj = 0, nvmin = 0;
     nvrtcVersion(&nvmaj, &nvmin);
@@ -989,10 +994,10 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     }
     if (cache_hit) *cache_hit = !cubin.empty();
     if (!cubin.empty()) return cubin;
-    const char* hdr_src[] = {jet.c_str(), ls.c_str(), fused.c_str(), gen.header.c_str()};
-    const char* hdr_names[] = {"jet.cuh", "lineshapes.cuh", "fused_nll.cuh", "model.cuh"};
+    const char* hdr_src[] = {helpers.c_str(), fused.c_str(), gen.header.c_str()};
+    const char* hdr_names[] = {"device_helpers.cuh", "fused_nll.cuh", "model.cuh"};
     nvrtcProgram prog;
-    if (nvrtcCreateProgram(&prog, src.c_str(), "ctpwa_fused.cu", 4, hdr_src, hdr_names) != NVRTC_SUCCESS)
+    if (nvrtcCreateProgram(&prog, src.c_str(), "ctpwa_fused.cu", 3, hdr_src, hdr_names) != NVRTC_SUCCESS)
         throw std::runtime_error("NVRTC: program creation failed");
     nvrtcResult r = nvrtcCompileProgram(prog, nopts, opts);
     if (r != NVRTC_SUCCESS) {
@@ -1026,7 +1031,9 @@ void Engine::compileKernel()
     cudaLibrary_t lib;
     CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
     lib_ = (void*)lib;
-    cudaKernel_t k64, kmx, kin;
+    cudaKernel_t k64, kmx, kin, kpro;
+    CT_CUDA(cudaLibraryGetKernel(&kpro, lib, "ct_prologue"));
+    k_pro_ = (void*)kpro;
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
@@ -1067,6 +1074,7 @@ struct CtArgsH {
     const double* theta;
     const double* v;
     double* partials;
+    double* consts;
 };
 
 void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
@@ -1095,9 +1103,17 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     a.theta = d_params + 2 * nc;
     a.v = d_v_;
     a.partials = d_partials_;
+    a.consts = d_consts_;
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    const size_t slot = ev_begin_.empty() ? 0 : (size_t)(ev_count_ % (long long)ev_begin_.size());
+    if (!ev_begin_.empty()) CT_CUDA(cudaEventRecord(ev_begin_[slot], stream));
     CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    if (!ev_begin_.empty()) {
+        CT_CUDA(cudaEventRecord(ev_end_[slot], stream));
+        ++ev_count_;
+    }
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     f.partials = d_partials_;
@@ -1146,9 +1162,46 @@ void Engine::intensity(const double* d_params, int kind, double* d_out, cudaStre
     a.theta = d_params + 2 * nc;
     a.v = d_v_;
     a.partials = d_partials_;
+    a.consts = d_consts_;
+    void* pargs[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), pargs, 0, stream));
     void* args[] = {&a, &d_out};
     int grid = (int)std::min<long long>((d.n + 255) / 256, 148LL * 16);
     CT_CUDA(cudaLaunchKernel(k_int_, dim3(grid), dim3(256), args, 0, stream));
+}
+
+void Engine::setKernelTiming(int slots)
+{
+    CT_CUDA(cudaSetDevice(opt_.device));
+    for (size_t i = 0; i < ev_begin_.size(); ++i) {
+        cudaEventSynchronize(ev_end_[i]);
+        cudaEventDestroy(ev_begin_[i]);
+        cudaEventDestroy(ev_end_[i]);
+    }
+    ev_begin_.clear();
+    ev_end_.clear();
+    ev_count_ = 0;
+    if (slots < 0 || slots > (1 << 20)) throw std::runtime_error("kernel timing: slots must be in [0, 2^20]");
+    ev_begin_.resize(slots);
+    ev_end_.resize(slots);
+    for (int i = 0; i < slots; ++i) {
+        CT_CUDA(cudaEventCreate(&ev_begin_[i]));
+        CT_CUDA(cudaEventCreate(&ev_end_[i]));
+    }
+}
+
+int Engine::kernelTimes(float* ms, int cap)
+{
+    if (ev_begin_.empty()) return 0;
+    const long long ring = (long long)ev_begin_.size();
+    const long long avail = std::min<long long>(ev_count_, ring);
+    const long long n = std::min<long long>(avail, cap);
+    for (long long i = 0; i < n; ++i) {
+        const size_t slot = (size_t)((ev_count_ - n + i) % ring);
+        CT_CUDA(cudaEventSynchronize(ev_end_[slot]));
+        CT_CUDA(cudaEventElapsedTime(&ms[i], ev_begin_[slot], ev_end_[slot]));
+    }
+    return (int)n;
 }
 
 void Engine::lastParts(double* out6, cudaStream_t stream)

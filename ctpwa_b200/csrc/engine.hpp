@@ -54,6 +54,13 @@ public:
     // [data_nll, bkg_nll, phsp_sum, W_data, W_bkg, n_phsp]
     void lastParts(double* out6, cudaStream_t stream);
 
+    // Optional per-launch timing of the fused kernel: CUDA events recorded on
+    // the launching stream around each fused launch into a ring of `slots`
+    // pairs (0 switches timing off). kernelTimes synchronises on the recorded
+    // events and returns the durations (ms) of the most recent launches.
+    void setKernelTiming(int slots);
+    int kernelTimes(float* ms, int cap);
+
     long long nEvents(int kind) const { return samples_[kind].n; }
     size_t deviceBytes() const { return device_bytes_; }
     const GeneratedModel& generated() const { return gen_; }
@@ -84,11 +91,13 @@ private:
     void* k_f64_ = nullptr;
     void* k_mixed_ = nullptr;
     void* k_int_ = nullptr;
+    void* k_pro_ = nullptr;
     double jit_seconds_ = 0.0;
     bool jit_cache_hit_ = false;
 
     // evaluation buffers
     double* d_v_ = nullptr;         // [2 nA]
+    double* d_consts_ = nullptr;    // [nconst] parameter-only subexpressions
     double* d_partials_ = nullptr;  // [grid][nacc]
     double* d_parts_ = nullptr;     // [8]
     int* d_amp_chain_ = nullptr;
@@ -97,6 +106,10 @@ private:
     double* d_gauss_ms_ = nullptr;  // [mu, sigma] pairs
     int grid_ = 0;
     int cta_[3][2] = {};  // per sample: begin, count
+
+    // fused-kernel timing ring
+    std::vector<cudaEvent_t> ev_begin_, ev_end_;
+    long long ev_count_ = 0;
 };
 
 }  // namespace ctpwa

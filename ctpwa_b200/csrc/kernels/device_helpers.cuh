@@ -1,0 +1,86 @@
+// Value-only helpers called by the generated lineshape code: channel
+// phase-space factors of the Flatte lineshape and table lookups (Hist,
+// Interp). Same conventions as the reference (include/ResModel.cuh:66-82,
+// 248-293, 419-451; src/CustomExpr.cu:1150-1169).
+#pragma once
+
+// rho = csqrt(1 - (ma+mb)^2/s) * sqrt(max(0, 1 - (ma-mb)^2/s)); which = 0: Re, 1: Im
+__device__ __forceinline__ double ct_rho(double s, double ma, double mb, int which)
+{
+    double S = (ma + mb) * (ma + mb), Dd = (ma - mb) * (ma - mb);
+    double f1 = 1.0 - S / s;
+    double f2s = 1.0 - Dd / s;
+    double f2 = f2s > 0.0 ? sqrt(f2s) : 0.0;
+    if (which == 0) return f1 >= 0.0 ? sqrt(f1) * f2 : 0.0;
+    return f1 >= 0.0 ? 0.0 : sqrt(-f1) * f2;
+}
+
+// Histogram shape: aux = [m_min, m_max, nbins, values...], linear interpolation
+__device__ __forceinline__ double ls_hist(double m, const double* aux)
+{
+    if (!(m >= 0.0)) return 0.0;
+    double lo = aux[0], hi = aux[1];
+    int n = (int)aux[2];
+    const double* v = aux + 3;
+    if (n < 2 || hi <= lo) return 0.0;
+    if (m <= lo) return v[0];
+    if (m >= hi) return v[n - 1];
+    double x = (m - lo) / (hi - lo) * n;
+    if (x < 0.0) x = 0.0;
+    if (x >= (double)(n - 1)) x = (double)(n - 2);
+    int i = (int)x;
+    double fr = x - i;
+    return v[i] * (1.0 - fr) + v[i + 1] * fr;
+}
+
+__device__ __forceinline__ double ls_interp1(const double* y, int i, double fr, int method, int N)
+{
+    if (method == 1) return y[i] + (y[i + 1] - y[i]) * fr;
+    if (method == 2) {
+        double y0 = (i > 0) ? y[i - 1] : y[i] - (y[i + 1] - y[i]);
+        double y1 = y[i], y2 = y[i + 1];
+        double y3 = (i + 2 < N) ? y[i + 2] : y[i + 1] + (y[i + 1] - y[i]);
+        double f2 = fr * fr, f3 = f2 * fr;
+        return 0.5 * ((2 * y1) + (-y0 + y2) * fr + (2 * y0 - 5 * y1 + 4 * y2 - y3) * f2 +
+                      (-y0 + 3 * y1 - 3 * y2 + y3) * f3);
+    }
+    return y[i];
+}
+
+// Interpolated complex table (Interp model aux format)
+__device__ __forceinline__ void ls_interp(const double* t, double x, double& Fr, double& Fi)
+{
+    int hdr = (int)t[0];
+    int method = hdr >= 0 ? hdr : -(hdr + 1);
+    int N = (int)t[1];
+    int i;
+    double fr;
+    const double *re, *im;
+    if (hdr >= 0) {
+        double xmin = t[2], dx = t[3];
+        re = t + 4;
+        im = t + 4 + N;
+        double pos = (x - xmin) / dx;
+        i = (int)pos;
+        if (i < 0) { i = 0; fr = 0.0; }
+        else if (i >= N - 1) { i = N - 2; fr = 1.0; }
+        else fr = pos - (double)i;
+    } else {
+        const double* xv = t + 2;
+        re = t + 2 + N;
+        im = t + 2 + 2 * N;
+        int lo = 0, hi = N - 1;
+        while (lo < hi - 1) {
+            int mid = (lo + hi) / 2;
+            if (x < xv[mid]) hi = mid;
+            else lo = mid;
+        }
+        i = lo;
+        if (i < 0) { i = 0; fr = 0.0; }
+        else if (i >= N - 1) { i = N - 2; fr = 1.0; }
+        else fr = (x - xv[i]) / (xv[i + 1] - xv[i]);
+        if (method == 2) method = 0;
+    }
+    Fr = ls_interp1(re, i, fr, method, N);
+    Fi = ls_interp1(im, i, fr, method, N);
+}

@@ -25,9 +25,11 @@
 // R is the arithmetic type of the per-polarisation complex algebra (double for
 // the plain path, float for the mixed path); SL2 is the stored angular-table
 // element (double2 / float2). Lineshapes, the log and all accumulations are FP64.
+// Parameter-only parts of the lineshapes are computed once per call by
+// ct_prologue and staged in shared memory by every CTA.
 #pragma once
 
-#include "lineshapes.cuh"
+#include "device_helpers.cuh"
 #include "model.cuh"
 
 #ifndef CT_BLOCK
@@ -55,7 +57,22 @@ struct CtArgs {
     const double* theta;  // fitted resonance parameters
     const double* v;      // couplings, interleaved (re, im) x M_NA
     double* partials;     // [gridDim.x][CT_NACC]
+    double* consts;       // [M_NCONST] parameter-only subexpressions of this call
 };
+
+// One thread: the parameter-only part of every lineshape (prologue).
+extern "C" __global__ void ct_prologue(CtArgs A)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) model_prologue(A.theta, A.consts);
+}
+
+#define CT_NCONST_ALLOC (M_NCONST > 0 ? M_NCONST : 1)
+
+__device__ __forceinline__ void ct_stage_consts(const CtArgs& A, double* sC)
+{
+    for (int i = threadIdx.x; i < M_NCONST; i += blockDim.x) sC[i] = A.consts[i];
+    __syncthreads();
+}
 
 template <typename T>
 struct CtVec2;
@@ -109,9 +126,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #pragma unroll
     for (int i = 0; i < CT_NACC; ++i) acc[i] = 0.0;
 
-    double th[M_NTH > 0 ? M_NTH : 1];
-#pragma unroll
-    for (int j = 0; j < M_NTH; ++j) th[j] = __ldg(A.theta + j);
+    __shared__ double sC[CT_NCONST_ALLOC];
+    ct_stage_consts(A, sC);
     double vr[M_NA], vi[M_NA];
 #pragma unroll
     for (int a = 0; a < M_NA; ++a) {
@@ -126,7 +142,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #pragma unroll
         for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(kin + (long long)k * n + e);
         double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        model_columns(kv, th, Fr, Fi, dFr, dFi);
+        model_columns(kv, sC, Fr, Fi, dFr, dFi);
 
         // ---- coherent sum over amplitudes ----
         SL2 sl[M_NPLANE * M_NPOL];
@@ -229,15 +245,14 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_intensity_f64(CtArgs A
     const CtSample& S = A.s[0];
     const long long n = S.n;
     const double2* __restrict__ slamp = (const double2*)S.slamp;
-    double th[M_NTH > 0 ? M_NTH : 1];
-#pragma unroll
-    for (int j = 0; j < M_NTH; ++j) th[j] = __ldg(A.theta + j);
+    __shared__ double sC[CT_NCONST_ALLOC];
+    ct_stage_consts(A, sC);
     for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
         for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * n + e);
         double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        model_columns(kv, th, Fr, Fi, dFr, dFi);
+        model_columns(kv, sC, Fr, Fi, dFr, dFi);
         double f = 0.0;
 #pragma unroll
         for (int p = 0; p < M_NPOL; ++p) {

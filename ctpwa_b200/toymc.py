@@ -79,6 +79,67 @@ def phase_space(M, masses, n, seed):
     return out
 
 
+def phase_space_gpu(M, masses, n, seed, device="cuda"):
+    """Same generator on the GPU with torch's seeded Philox RNG (large samples).
+
+    Returns a float64 numpy array (n, 3, 4)."""
+    import torch
+
+    m1, m2, m3 = (float(x) for x in masses)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed))
+    lo, hi = m1 + m2, M - m3
+    grid = np.linspace(lo, hi, 20001)[1:-1]
+    wmax = 1.05 * float(np.max(_breakup(M, grid, m3) * _breakup(grid, m1, m2)))
+    f64 = dict(dtype=torch.float64, device=device)
+
+    def brk(m, a, b):
+        q2 = (m * m - (a + b) ** 2) * (m * m - (a - b) ** 2)
+        return torch.sqrt(torch.clamp(q2, min=0.0)) / (2.0 * m)
+
+    def rdir(k):
+        cth = torch.rand(k, generator=gen, **f64) * 2.0 - 1.0
+        phi = torch.rand(k, generator=gen, **f64) * (2.0 * np.pi)
+        sth = torch.sqrt(1.0 - cth * cth)
+        return torch.stack([sth * torch.cos(phi), sth * torch.sin(phi), cth], dim=1)
+
+    out = torch.empty((n, 3, 4), **f64)
+    filled = 0
+    while filled < n:
+        k = max(4096, int((n - filled) * 2.2))
+        m12 = lo + (hi - lo) * torch.rand(k, generator=gen, **f64)
+        w = brk(M, m12, m3) * brk(m12, m1, m2)
+        keep = torch.rand(k, generator=gen, **f64) * wmax < w
+        m12 = m12[keep]
+        k = m12.numel()
+        if k == 0:
+            continue
+        q3 = brk(M, m12, m3)
+        d3 = rdir(k)
+        p3 = torch.cat([torch.sqrt(m3 * m3 + q3 * q3)[:, None], -q3[:, None] * d3], dim=1)
+        e12 = torch.sqrt(m12 * m12 + q3 * q3)
+        q12 = brk(m12, m1, m2)
+        d1 = rdir(k)
+        p1r = torch.cat([torch.sqrt(m1 * m1 + q12 * q12)[:, None], q12[:, None] * d1], dim=1)
+        p2r = torch.cat([torch.sqrt(m2 * m2 + q12 * q12)[:, None], -q12[:, None] * d1], dim=1)
+        beta = (q3[:, None] * d3) / e12[:, None]
+        b2 = (beta * beta).sum(1)
+        gamma = 1.0 / torch.sqrt(1.0 - b2)
+        coef = torch.where(b2 > 0, (gamma - 1.0) / torch.where(b2 > 0, b2, torch.ones_like(b2)), torch.zeros_like(b2))
+
+        def boost(p):
+            bp = (beta * p[:, 1:]).sum(1)
+            return torch.cat([(gamma * (p[:, 0] + bp))[:, None],
+                              p[:, 1:] + (coef * bp + gamma * p[:, 0])[:, None] * beta], dim=1)
+
+        take = min(k, n - filled)
+        out[filled:filled + take, 0] = boost(p1r)[:take]
+        out[filled:filled + take, 1] = boost(p2r)[:take]
+        out[filled:filled + take, 2] = p3[:take]
+        filled += take
+    return out.cpu().numpy()
+
+
 def write_dat(path, p4):
     """Reference .dat layout: one 'E px py pz' line per particle."""
     flat = np.ascontiguousarray(p4, dtype=np.float64).reshape(-1, 4)

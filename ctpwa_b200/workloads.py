@@ -156,12 +156,20 @@ def true_params(n_vector, theta_init, seed=4001):
     return np.concatenate([re, im, np.asarray(theta_init, dtype=np.float64)])
 
 
+def _gen(M, masses, n, seed, gpu, device):
+    if gpu and n >= 200_000:
+        return toymc.phase_space_gpu(M, masses, n, seed, device=f"cuda:{device}")
+    return toymc.phase_space(M, masses, n, seed)
+
+
 def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, seed=0, accept_reject=True,
-         device=0):
+         device=0, gpu_generator=None):
     """Write samples + config.yml for workload `name` into outdir; returns the config path.
 
     accept_reject=True draws the data sample against the model at the true
-    parameters (needs a GPU); otherwise data are flat phase space."""
+    parameters (needs a GPU); otherwise data are flat phase space. Large
+    samples are generated on the GPU when one is present (gpu_generator=None)
+    or when gpu_generator=True."""
     sp, sd, sb, sw = SIZES[name]
     n_phsp = sp if n_phsp is None else n_phsp
     n_data = sd if n_data is None else n_data
@@ -170,29 +178,36 @@ def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, se
     out = Path(outdir)
     out.mkdir(parents=True, exist_ok=True)
     masses = MASSES[name]
-    phsp = toymc.phase_space(M_JPSI, masses, n_phsp, 1001 + seed)
+    if gpu_generator is None:
+        try:
+            import torch
+
+            gpu_generator = torch.cuda.is_available()
+        except Exception:
+            gpu_generator = False
+    phsp = _gen(M_JPSI, masses, n_phsp, 1001 + seed, gpu_generator, device)
     toymc.write_npy(out / "phsp.npy", phsp)
     bkg_path = None
     if n_bkg:
-        toymc.write_npy(out / "bkg.npy", toymc.phase_space(M_JPSI, masses, n_bkg, 3001 + seed))
+        toymc.write_npy(out / "bkg.npy", _gen(M_JPSI, masses, n_bkg, 3001 + seed, gpu_generator, device))
         bkg_path = str(out / "bkg.npy")
     if accept_reject:
-        data = _accept_reject(name, out, masses, n_data, seed, device)
+        data = _accept_reject(name, out, masses, n_data, seed, device, gpu_generator)
     else:
-        data = toymc.phase_space(M_JPSI, masses, n_data, 2001 + seed)
+        data = _gen(M_JPSI, masses, n_data, 2001 + seed, gpu_generator, device)
     toymc.write_npy(out / "data.npy", data)
     cfg = out / "config.yml"
     cfg.write_text(config_text(name, str(out / "phsp.npy"), str(out / "data.npy"), bkg_path, bkg_weight))
     return str(cfg)
 
 
-def _accept_reject(name, out, masses, n_data, seed, device):
+def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator):
     import torch
 
     from . import analysis
 
     ncand = int(n_data * 12) + 10_000
-    cand = toymc.phase_space(M_JPSI, masses, ncand, 5001 + seed)
+    cand = _gen(M_JPSI, masses, ncand, 5001 + seed, gpu_generator, device)
     toymc.write_npy(out / "cand.npy", cand)
     tiny = toymc.phase_space(M_JPSI, masses, 1000, 7001 + seed)
     toymc.write_npy(out / "tiny.npy", tiny)
@@ -204,7 +219,7 @@ def _accept_reject(name, out, masses, n_data, seed, device):
     del ana
     sel = toymc.accept_reject(cand, I, seed=6001 + seed, safety=1.2)
     while sel.shape[0] < n_data:  # rare: top up from a fresh candidate batch
-        more = toymc.phase_space(M_JPSI, masses, ncand, 8001 + seed + sel.shape[0])
+        more = _gen(M_JPSI, masses, ncand, 8001 + seed + sel.shape[0], gpu_generator, device)
         toymc.write_npy(out / "cand.npy", more)
         ana = analysis(str(cfg), device=device)
         I2 = ana.getIntensity(torch.tensor(p, dtype=torch.float64, device=f"cuda:{device}"), kind=1).cpu().numpy()

@@ -83,6 +83,16 @@ int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream);
  * (src/ComputeNLL.cu:21-84) and for its result export (ComputeResults.cu:22). */
 int ctpwa_intensity(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream);
 
+/* Per-launch timing of the fused likelihood kernel (no counterpart in the
+ * reference, which times nothing on the device). slots > 0 records a CUDA
+ * event pair on the launching stream around every fused launch, in a ring of
+ * `slots` pairs; slots = 0 switches timing off. */
+int ctpwa_kernel_timing(ctpwa_handle* h, int slots);
+
+/* Durations in milliseconds of the most recent fused launches (at most cap,
+ * oldest first); waits for their end events. Returns the number written. */
+int ctpwa_kernel_times(ctpwa_handle* h, float* ms, int cap);
+
 /* Event counts of phase space (kind 0), data (1), background (2). */
 long long ctpwa_n_events(const ctpwa_handle* h, int kind);
 
