@@ -1,0 +1,468 @@
+#!/usr/bin/env python
+"""Throughput of the event-parallel likelihood: NLL + gradient evaluations per second.
+
+Workload: J/psi -> K+ K- pi0 with K*(892)+-, K*(1410)+-, K*2(1430)+- (BWR) and
+a K+K- J=1 state with a custom Flatte lineshape; 10M phase-space, 1M data
+(accept-reject against the model) and 100k background events (weight 0.3),
+seeded synthetic four-momenta. One step = one NLL + full gradient
+(couplings and all 9 resonance parameters) with the resonance parameters
+perturbed every step, so every lineshape is recomputed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One JSON line on rank 0. `value` is the mixed-precision path (FP32 angular
+tables and coherent sum, FP64 lineshapes, logs and accumulations) with the
+events resident in HBM; the FP64 path is timed beside it; `e2e` goes through
+the host-buffer C-ABI entry point. Multi-GPU: each rank holds its own shard of
+the same size (weak scaling) and the per-step exchange is one NCCL all-reduce
+of the packed (NLL, gradient) buffer.
+
+`--impl reference`: the reference has no CPU path and its CUDA build needs
+yaml-cpp and ROOT, which are absent, so this arm times the FP64 OpenMP port of
+the reference's algorithm (oracle/) on all host cores, each step on a bounded
+sample of the same workload, scaled to full-size evaluations per second.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "NLL+grad evals/s at 1M evt (mixed vs FP64 plain, |ΔNLL|<1e-3); toy-fit p50/p99"
+UNIT = "evals/s"
+WORKLOAD = "kkpi"
+WORKLOAD_TEXT = ("J/psi->K+K-pi0: K*(892)+-, K*(1410)+-, K*2(1430)+- BWR + K+K- J=1 custom Flatte; "
+                 "10M phsp / 1M data / 100k bkg (w=0.3)")
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--e2e-steps", type=int, default=None, help="host-buffer steps (default: steps)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--data-dir", default=os.environ.get("CTPWA_BENCH_DIR", "/tmp/ctpwa_bench"))
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--fraction", type=float, default=1.0,
+                    help="scale the event counts (profiling of a small case; 1.0 = the full workload)")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- helpers
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return None
+
+
+def ncu_traffic(precision):
+    """DRAM bytes per fused launch from the committed ncu summary (None if absent)."""
+    f = ROOT / "profiles" / "ct_fused_kkpi.md"
+    try:
+        for line in f.read_text().splitlines():
+            if line.startswith(f"traffic_bytes_per_launch_{precision}:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, device):
+        import torch
+
+        self.sel = []
+        try:
+            uuid = str(torch.cuda.get_device_properties(device).uuid)
+            sel = ["-i", uuid if uuid.startswith("GPU-") else "GPU-" + uuid]
+            probe = subprocess.run(["nvidia-smi", *sel, "--query-gpu=clocks.sm", "--format=csv,noheader"],
+                                   capture_output=True, text=True, timeout=30)
+            if probe.returncode == 0:
+                self.sel = sel
+            else:
+                vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+                self.sel = ["-i", vis[device].strip() if device < len(vis) and vis[device].strip() else str(device)]
+        except Exception:
+            self.sel = ["-i", str(device)]
+        self.proc = None
+        self.err = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", *self.sel, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+        except OSError as e:
+            self.err = str(e)
+
+    def stop(self):
+        if self.proc is None:
+            return {"error": self.err or "nvidia-smi unavailable"}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, power, reasons = [], [], [], set()
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+                power.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(self.NAMES, f[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"error": "no samples"}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------- CPU port (oracle)
+def oracle_sample(data_dir, fraction, seed):
+    """Bounded CPU sample of the workload: same generator and accept-reject, intensities from the oracle."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from binding import Oracle  # noqa: E402  (CPU baseline only)
+
+    from ctpwa_b200 import workloads
+
+    n_p, n_d, n_b, w_b = workloads.SIZES[WORKLOAD]
+    n_p, n_d, n_b = (max(100, int(round(x * fraction))) for x in (n_p, n_d, n_b))
+    out = Path(data_dir) / f"cpu_{WORKLOAD}_{n_p}_{n_d}_{n_b}_s{seed}"
+    cfg = out / "config.yml"
+    if not (out / "done").exists():
+
+        def intensity(cand_cfg, params):
+            o = Oracle(cand_cfg)
+            try:
+                return o.intensity(1, params)
+            finally:
+                o.close()
+
+        workloads.make(WORKLOAD, out, n_phsp=n_p, n_data=n_d, n_bkg=n_b, bkg_weight=w_b, seed=seed,
+                       gpu_generator=False, intensity=intensity)
+        (out / "done").write_text("ok")
+    return str(cfg), (n_p, n_d, n_b)
+
+
+def time_oracle(cfg, n_threads, min_seconds, min_evals=3, max_evals=None, seed=0):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from binding import Oracle  # noqa: E402
+
+    from ctpwa_b200 import workloads
+
+    o = Oracle(cfg)
+    p0 = workloads.true_params(o.nV, o.theta_init()[0])
+    rng = np.random.default_rng(seed + 17)
+    nV = o.nV
+    times = []
+    o.nll_grad(p0, n_threads)  # warm-up
+    t_start = time.perf_counter()
+    while True:
+        p = p0.copy()
+        p[2 * nV:] *= 1.0 + 1e-4 * rng.standard_normal(p.size - 2 * nV)
+        t0 = time.perf_counter()
+        o.nll_grad(p, n_threads)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= min_evals and time.perf_counter() - t_start >= min_seconds:
+            break
+        if max_evals and len(times) >= max_evals:
+            break
+    o.close()
+    return times
+
+
+def full_size_events():
+    from ctpwa_b200 import workloads
+
+    n_p, n_d, n_b, _ = workloads.SIZES[WORKLOAD]
+    return n_p + n_d + n_b
+
+
+def cpu_baseline(data_dir, seed):
+    """Oracle on a 1 % sample of the workload, all host threads, >= 10 s of evaluations."""
+    fraction = 0.01
+    cfg, sizes = oracle_sample(data_dir, fraction, seed)
+    cores = cpu_cores()
+    times = time_oracle(cfg, cores, min_seconds=10.0, seed=seed)
+    t = statistics.median(times)
+    scale = full_size_events() / float(sum(sizes))
+    return {"value": 1.0 / (t * scale), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"{sizes[0]} phsp / {sizes[1]} data / {sizes[2]} bkg events (1% of the workload), "
+                       f"median of {len(times)} FP64 NLL+grad evals ({t:.3f} s each), scaled x{scale:.1f} "
+                       f"by event count to full size")}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    cores = cpu_cores()
+    # size the per-step sample so that warm-up + steps finish in about two minutes
+    pilot_cfg, pilot_sizes = oracle_sample(args.data_dir, 0.001, args.seed)
+    t_pilot = statistics.median(time_oracle(pilot_cfg, cores, min_seconds=1.0, max_evals=20, seed=args.seed))
+    per_event = t_pilot / sum(pilot_sizes)
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    fraction = min(0.01, max(0.001, budget / (per_event * full_size_events())))
+    fraction = float(f"{fraction:.2g}")
+    cfg, sizes = oracle_sample(args.data_dir, fraction, args.seed)
+    times = time_oracle(cfg, cores, min_seconds=0.0, min_evals=args.steps + args.warmup,
+                        max_evals=args.steps + args.warmup, seed=args.seed)[args.warmup:]
+    t = sum(times) / len(times)
+    scale = full_size_events() / float(sum(sizes))
+    value = 1.0 / (t * scale)
+    sample = (f"{sizes[0]} phsp / {sizes[1]} data / {sizes[2]} bkg events ({100 * fraction:.2g}% of the workload) "
+              f"per step, FP64 NLL+grad, mean step {t:.4f} s, scaled x{scale:.1f} by event count to full size")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t * scale, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, CPU generator)",
+        "config": {"workload": WORKLOAD_TEXT, "sample_fraction": fraction,
+                   "note": "reference has no CPU path and its CUDA build needs yaml-cpp/ROOT: timed the OpenMP FP64 "
+                           "port of its algorithm (oracle/) on the host cores"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- GPU arm
+def gpu_workload(args, rank, device):
+    from ctpwa_b200 import workloads
+
+    seed = args.seed + 1000 * rank
+    n_p, n_d, n_b, w_b = workloads.SIZES[WORKLOAD]
+    f = args.fraction
+    n_p, n_d, n_b = (max(100, int(round(x * f))) for x in (n_p, n_d, n_b))
+    out = Path(args.data_dir) / f"gpu_{WORKLOAD}_{n_p}_{n_d}_{n_b}_s{seed}"
+    if not (out / "done").exists():
+        workloads.make(WORKLOAD, out, n_phsp=n_p, n_data=n_d, n_bkg=n_b, bkg_weight=w_b, seed=seed, device=device)
+        (out / "done").write_text("ok")
+    return str(out / "config.yml")
+
+
+def algorithmic_bytes(layout, n_events, precision):
+    """Minimum bytes streamed per evaluation with the angular tables cached:
+    per event nC*nPol complex angular values + nM invariant masses (+ one
+    weight for weighted samples)."""
+    sc = 16 if precision == "fp64" else 8
+    sr = 8 if precision == "fp64" else 4
+    per = layout["planes"] * layout["npol"] * sc + layout["nmass"] * sr
+    n_p, n_d, n_b = n_events
+    return per * (n_p + n_d + n_b) + 8 * n_b, per
+
+
+def streamed_bytes(layout, n_events, precision):
+    """Bytes the fused kernel actually reads per evaluation in this layout."""
+    sc = 16 if precision == "fp64" else 8
+    per = layout["planes"] * layout["npol"] * sc + layout["nkin"] * 8
+    n_p, n_d, n_b = n_events
+    return per * (n_p + n_d + n_b) + 8 * n_b
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import ctpwa_b200
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    W = max(3, args.warmup)
+    K = args.steps
+    cfg = gpu_workload(args, rank, local_rank)
+    ana = ctpwa_b200.analysis(cfg, device=local_rank)
+    nV, nT, nP = ana.getNVector(), ana.getNFreeTheta(), ana.getNParams()
+    n_events = tuple(int(x) for x in ana.getNEvents())
+    layout = ana.eventLayout()
+
+    from ctpwa_b200 import workloads
+
+    p0 = workloads.true_params(nV, ana.getFreeResParams()[0].numpy())
+    rng = np.random.default_rng(12345 + rank)
+    P = np.tile(p0, (W + K, 1))
+    P[:, 2 * nV:] *= 1.0 + 1e-4 * rng.standard_normal((W + K, nT))  # new theta every step
+    Pd = torch.tensor(P, dtype=torch.float64, device=dev)
+    packed = torch.empty(1 + nP, dtype=torch.float64, device=dev)
+
+    def step(i, prec):
+        nll, g = ana.getNLLAndGrad(Pd[i], prec)
+        if world > 1:
+            packed[0] = nll
+            packed[1:] = g
+            dist.all_reduce(packed)
+        return nll
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t)
+
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    clocks = None
+    for prec in ("fp64", "mixed"):
+        for i in range(W):
+            step(i, prec)
+        ana.setKernelTiming(K)
+        barrier()
+        sampler = ClockSampler(local_rank) if prec == "mixed" else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(K):
+            step(W + i, prec)
+        e1.record(stream)
+        barrier()
+        if sampler:
+            clocks = sampler.stop()
+        ms = max_over_ranks(e0.elapsed_time(e1) / K)
+        kt = ana.kernelTimes(K)
+        ana.setKernelTiming(0)
+        res[prec] = {"ms": ms, "kernel_ms": max_over_ranks(sum(kt) / len(kt)), "launches": len(kt)}
+
+    # accuracy of the mixed path against FP64 at the same parameters (this rank's shard)
+    n64, g64 = ana.getNLLAndGrad(Pd[0], "fp64")
+    nmx, gmx = ana.getNLLAndGrad(Pd[0], "mixed")
+    dnll = abs(float(n64) - float(nmx))
+    grel = float((g64 - gmx).abs().max() / g64.abs().max().clamp_min(1e-300))
+
+    # end to end through the host-buffer entry point (params in, NLL + gradient out)
+    E = args.e2e_steps or K
+    Ph = [np.ascontiguousarray(P[i % (W + K)]) for i in range(W + E)]
+    host_group = dist.new_group(backend="gloo") if world > 1 else None
+    for i in range(W):
+        ana.getNLLHost(Ph[i], "mixed")
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(E):
+        v, g = ana.getNLLHost(Ph[W + i], "mixed")
+        if world > 1:
+            t = torch.from_numpy(np.concatenate([[v], g]))
+            dist.all_reduce(t, group=host_group)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": world * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * nP, "d2h_bytes_per_step": 8 * (1 + nP),
+           "ms_per_step": 1e3 * e2e_s / E}
+
+    if rank != 0:
+        return 0
+    peaks = measured_peaks()
+    if peaks and peaks.get("hbm_gbs"):
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    alg, per_evt = algorithmic_bytes(layout, n_events, "mixed")
+    kms = res["mixed"]["kernel_ms"]
+    achieved = alg / (kms * 1e-3) / 1e9
+    alg64, per64 = algorithmic_bytes(layout, n_events, "fp64")
+    ach64 = alg64 / (res["fp64"]["kernel_ms"] * 1e-3) / 1e9
+    traffic = ncu_traffic("mixed")
+    line = {
+        "metric": METRIC,
+        "value": world * 1e3 / res["mixed"]["ms"],
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": res["mixed"]["ms"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64 (mixed: FP32 angular tables and coherent sum; FP64 lineshapes, log and sums)",
+        "data": "synthetic (seeded phase space, accept-reject data, uniform background), events resident in HBM",
+        "config": {"workload": WORKLOAD_TEXT, "events_per_rank": {"phsp": n_events[0], "data": n_events[1],
+                                                                  "bkg": n_events[2]},
+                   "n_params": nP, "theta_perturbed_every_step": True, "fraction": args.fraction,
+                   "l2": f"inputs larger than L2: {streamed_bytes(layout, n_events, 'mixed') / 1e9:.2f} GB streamed "
+                         f"per step vs {L2_BYTES / 1e6:.0f} MB L2, no flush",
+                   "exchange": "NCCL all-reduce of packed (NLL, grad) per step" if world > 1 else "none (1 GPU)"},
+        "fp64": {"value": world * 1e3 / res["fp64"]["ms"], "unit": UNIT, "ms_per_step": res["fp64"]["ms"],
+                 "kernel_ms": res["fp64"]["kernel_ms"], "roofline_frac": ach64 / peak,
+                 "algorithmic_bytes_per_event": per64},
+        "mixed_over_fp64": res["fp64"]["ms"] / res["mixed"]["ms"],
+        "accuracy": {"abs_dnll_mixed_vs_fp64": dnll, "grad_rel_err_mixed_vs_fp64": grel},
+        "clocks": clocks,
+        "e2e": e2e,
+        "gpu_launches": 4 * K,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_src, "kernel": "ct_fused_mixed",
+                     "kernel_ms": kms, "algorithmic_bytes_per_launch": alg, "algorithmic_bytes_per_event": per_evt,
+                     "streamed_bytes_per_launch": streamed_bytes(layout, n_events, "mixed")},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.data_dir, args.seed)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus != world and world > 1:
+        print(f"warning: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    import torch.distributed as dist
+
+    if world > 1:
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+    try:
+        return run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

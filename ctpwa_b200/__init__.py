@@ -309,6 +309,14 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return out
 
+    def eventLayout(self) -> dict:
+        """Per-event cache layout: angular planes, polarisations, kinematic values, invariant masses."""
+        self._check()
+        out = (ctypes.c_int * 4)()
+        if self._lib.ctpwa_event_layout(self._h, out) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return {"planes": out[0], "npol": out[1], "nkin": out[2], "nmass": out[3]}
+
     def setKernelTiming(self, slots: int):
         """Record CUDA events around each fused-kernel launch (ring of `slots`; 0 = off)."""
         self._check()

@@ -166,6 +166,19 @@ int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream)
     return CTPWA_OK;
 }
 
+int ctpwa_event_layout(const ctpwa_handle* h, int* out4)
+{
+    if (!h || !out4) return CTPWA_ERR_ARG;
+    const ctpwa::GeneratedModel& g = h->eng->generated();
+    int nmass = 0;
+    for (const auto& s : g.slots) nmass += s.type == 0 ? 1 : 0;  // AG_K_MASS
+    out4[0] = g.nplane;
+    out4[1] = h->eng->model().npol;
+    out4[2] = (int)g.slots.size();
+    out4[3] = nmass;
+    return CTPWA_OK;
+}
+
 int ctpwa_kernel_timing(ctpwa_handle* h, int slots)
 {
     if (!h) return CTPWA_ERR_ARG;

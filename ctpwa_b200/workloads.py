@@ -156,6 +156,11 @@ def true_params(n_vector, theta_init, seed=4001):
     return np.concatenate([re, im, np.asarray(theta_init, dtype=np.float64)])
 
 
+def params_for(model):
+    """True parameters of a lowered model (``describe``): seeded couplings and initial theta."""
+    return true_params(int(model["coupling"]["n_free"]), [s["init"] for s in model["slots"]])
+
+
 def _gen(M, masses, n, seed, gpu, device):
     if gpu and n >= 200_000:
         return toymc.phase_space_gpu(M, masses, n, seed, device=f"cuda:{device}")
@@ -163,11 +168,13 @@ def _gen(M, masses, n, seed, gpu, device):
 
 
 def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, seed=0, accept_reject=True,
-         device=0, gpu_generator=None):
+         device=0, gpu_generator=None, intensity=None):
     """Write samples + config.yml for workload `name` into outdir; returns the config path.
 
     accept_reject=True draws the data sample against the model at the true
-    parameters (needs a GPU); otherwise data are flat phase space. Large
+    parameters; otherwise data are flat phase space. The per-candidate
+    intensities come from ``intensity(config_path, params)`` (intensities of
+    the config's data sample) when given, else from the GPU engine. Large
     samples are generated on the GPU when one is present (gpu_generator=None)
     or when gpu_generator=True."""
     sp, sd, sb, sw = SIZES[name]
@@ -192,7 +199,7 @@ def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, se
         toymc.write_npy(out / "bkg.npy", _gen(M_JPSI, masses, n_bkg, 3001 + seed, gpu_generator, device))
         bkg_path = str(out / "bkg.npy")
     if accept_reject:
-        data = _accept_reject(name, out, masses, n_data, seed, device, gpu_generator)
+        data = _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, intensity)
     else:
         data = _gen(M_JPSI, masses, n_data, 2001 + seed, gpu_generator, device)
     toymc.write_npy(out / "data.npy", data)
@@ -201,11 +208,26 @@ def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, se
     return str(cfg)
 
 
-def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator):
-    import torch
+def _gpu_intensity(device):
+    def run(cfg, params):
+        import torch
 
-    from . import analysis
+        from . import analysis
 
+        ana = analysis(str(cfg), device=device)
+        p = torch.tensor(params, dtype=torch.float64, device=f"cuda:{device}")
+        I = ana.getIntensity(p, kind=1).cpu().numpy()
+        del ana
+        return I
+
+    return run
+
+
+def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, intensity=None):
+    from . import describe
+
+    if intensity is None:
+        intensity = _gpu_intensity(device)
     ncand = int(n_data * 12) + 10_000
     cand = _gen(M_JPSI, masses, ncand, 5001 + seed, gpu_generator, device)
     toymc.write_npy(out / "cand.npy", cand)
@@ -213,17 +235,13 @@ def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator):
     toymc.write_npy(out / "tiny.npy", tiny)
     cfg = out / "cand.yml"
     cfg.write_text(config_text(name, str(out / "tiny.npy"), str(out / "cand.npy")))
-    ana = analysis(str(cfg), device=device)
-    p = true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
-    I = ana.getIntensity(torch.tensor(p, dtype=torch.float64, device=f"cuda:{device}"), kind=1).cpu().numpy()
-    del ana
+    p = params_for(describe(str(cfg)))
+    I = intensity(cfg, p)
     sel = toymc.accept_reject(cand, I, seed=6001 + seed, safety=1.2)
     while sel.shape[0] < n_data:  # rare: top up from a fresh candidate batch
         more = _gen(M_JPSI, masses, ncand, 8001 + seed + sel.shape[0], gpu_generator, device)
         toymc.write_npy(out / "cand.npy", more)
-        ana = analysis(str(cfg), device=device)
-        I2 = ana.getIntensity(torch.tensor(p, dtype=torch.float64, device=f"cuda:{device}"), kind=1).cpu().numpy()
-        del ana
+        I2 = intensity(cfg, p)
         sel = np.concatenate([sel, toymc.accept_reject(more, I2, seed=9001 + seed, safety=1.2)])
     for f in ("cand.npy", "tiny.npy", "cand.yml"):
         try:

@@ -83,6 +83,11 @@ int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream);
  * (src/ComputeNLL.cu:21-84) and for its result export (ComputeResults.cu:22). */
 int ctpwa_intensity(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream);
 
+/* Per-event layout of the device event caches (no counterpart in the
+ * reference): out[0] angular planes, out[1] polarisation states, out[2]
+ * cached kinematic values, out[3] of which invariant masses. */
+int ctpwa_event_layout(const ctpwa_handle* h, int* out4);
+
 /* Per-launch timing of the fused likelihood kernel (no counterpart in the
  * reference, which times nothing on the device). slots > 0 records a CUDA
  * event pair on the launching stream around every fused launch, in a ring of

@@ -1,5 +1,8 @@
 """ctypes binding of the CPU oracle (oracle/liboracle.so) and of the
-reference-math shim (oracle/_ref/libref_math.so) for tests."""
+reference-math shim (oracle/_ref/libref_math.so).
+
+Test infrastructure: used by tests/, by the smoke check and by the CPU
+baseline leg of bench.py, never by the product path."""
 import ctypes
 import os
 
@@ -22,6 +25,7 @@ def oracle_lib():
         lib.orc_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
         lib.orc_close.argtypes = [ctypes.c_void_p]
         lib.orc_sizes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
+        lib.orc_theta_init.argtypes = [ctypes.c_void_p, _D]
         lib.orc_group_nsl.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.orc_slamp.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D]
         lib.orc_columns.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D]
@@ -96,6 +100,12 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(self.lib.orc_error(self.h).decode())
         return v.value, g, parts
+
+    def theta_init(self):
+        """[3, nT]: initial value, lower and upper bound of every free resonance parameter."""
+        out = np.zeros((3, self.nT))
+        self.lib.orc_theta_init(self.h, ptr(out))
+        return out
 
     def columns(self, kind, theta):
         t = np.ascontiguousarray(theta, dtype=np.float64)

@@ -575,6 +575,19 @@ int orc_sizes(void* h, long* out)
     return 0;
 }
 
+// Free resonance parameters: out[3][nTheta] = (initial value, lower, upper)
+int orc_theta_init(void* h, double* out)
+{
+    auto* o = static_cast<Oracle*>(h);
+    const int nT = o->m.nTheta();
+    for (int j = 0; j < nT; ++j) {
+        out[j] = o->m.slots[j].init;
+        out[nT + j] = o->m.slots[j].lower;
+        out[2 * nT + j] = o->m.slots[j].upper;
+    }
+    return 0;
+}
+
 int orc_group_nsl(void* h, int g)
 {
     auto* o = static_cast<Oracle*>(h);

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from ctpwa_b200 import workloads
-from tests.oracle_binding import Oracle
+from oracle.binding import Oracle
 
 pytestmark = pytest.mark.gpu
 

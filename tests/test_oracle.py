@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from ctpwa_b200 import toymc, workloads
-from tests.oracle_binding import Oracle, oracle_lib, ptr, ref_lib
+from oracle.binding import Oracle, oracle_lib, ptr, ref_lib
 
 _I = ctypes.POINTER(ctypes.c_int)
 
