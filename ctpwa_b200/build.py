@@ -67,6 +67,20 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+def precompile_workloads() -> None:
+    """Fill the package kernel cache with the fused kernels of the bundled
+    benchmark models (NVRTC for sm_100a, no GPU needed)."""
+    import tempfile
+
+    from . import precompile, workloads
+
+    with tempfile.TemporaryDirectory(prefix="ctpwa_pre_") as d:
+        for name in workloads.SIZES:
+            cfg = Path(d) / f"{name}.yml"
+            cfg.write_text(workloads.config_text(name, f"{d}/phsp.npy", f"{d}/data.npy", f"{d}/bkg.npy", 0.5))
+            precompile(str(cfg))
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(LIB)

@@ -243,7 +243,8 @@ private:
             // Flatte expanded to (A - iB)/(A^2 + B^2) (src/CustomExpr.cu:844-872)
             int n = (int)(a.size() - 1) / 3;
             XP sq = xn(XNode::Mul, {m, m});
-            XP A = xn(XNode::Mul, {a[0], a[0]}), B = xn(XNode::Num, {}, 0.0);
+            // (m0^2 - m^2) is formed first so that the cancelling pair is one subtraction
+            XP A = xn(XNode::Sub, {xn(XNode::Mul, {a[0], a[0]}), sq}), B = xn(XNode::Num, {}, 0.0);
             XP half = xn(XNode::Mul, {a[0], xn(XNode::Num, {}, 0.5)});
             for (int i = 0; i < n; ++i) {
                 XP R = xn(XNode::Model, {sq, a[1 + n + 2 * i], a[2 + n + 2 * i]}, 0, "rho_re");
@@ -252,7 +253,6 @@ private:
                 A = xn(XNode::Add, {A, xn(XNode::Mul, {gw, I})});
                 B = xn(XNode::Sub, {B, xn(XNode::Mul, {gw, R})});
             }
-            A = xn(XNode::Sub, {A, sq});
             XP Dn = xn(XNode::Add, {xn(XNode::Mul, {A, A}), xn(XNode::Mul, {B, B})});
             return xn(XNode::Add, {xn(XNode::Div, {A, Dn}), xn(XNode::Mul, {xn(XNode::Neg, {xn(XNode::Div, {B, Dn})}), xn(XNode::Model, {}, 0, "i")})});
         }
@@ -338,13 +338,13 @@ struct Shapes {
     Cx flatte(int m, int m0, const std::vector<int>& gs, const std::vector<int>& ch)
     {
         int s = sq(m);
-        int A = sq(m0), B = g.zero(), half = g.mul(m0, g.cnst(0.5));
+        // m0^2 - s first: the cancelling pair stays one subtraction
+        int A = g.sub(sq(m0), s), B = g.zero(), half = g.mul(m0, g.cnst(0.5));
         for (size_t i = 0; i < gs.size(); ++i) {
             int gw = g.mul(gs[i], half);
             A = g.add(A, g.mul(gw, g.rho(true, s, ch[2 * i], ch[2 * i + 1])));
             B = g.sub(B, g.mul(gw, g.rho(false, s, ch[2 * i], ch[2 * i + 1])));
         }
-        A = g.sub(A, s);
         int iD = g.recip(g.add(sq(A), sq(B)));
         return {g.mul(A, iD), g.neg(g.mul(B, iD))};
     }
@@ -663,6 +663,17 @@ struct Gen {
     std::string emit();
 };
 
+std::string numf(double v)
+{
+    if (std::isnan(v)) return "ct_nanf()";
+    if (std::isinf(v)) return v > 0 ? "ct_inff()" : "(-ct_inff())";
+    char b[40];
+    std::snprintf(b, sizeof b, "%.9g", v);
+    std::string s(b);
+    if (s.find_first_of(".eEn") == std::string::npos) s += ".0";
+    return s + "f";
+}
+
 std::string Gen::emit()
 {
     const auto& N = G.nodes;
@@ -687,7 +698,8 @@ std::string Gen::emit()
         for (int k : {N[x].a, N[x].b, N[x].c})
             if (k >= 0) stack.push_back(k);
     }
-    // constant slots: theta-only nodes used by event nodes or roots
+    // constant slots: parameter-only nodes (theta leaves included) used by
+    // event nodes or taken directly as an output
     std::vector<int> cslot(N.size(), -1);
     int ncon = 0;
     auto isTheta = [&](int x) { return N[x].dep == dag::DEP_THETA; };
@@ -700,80 +712,215 @@ std::string Gen::emit()
     for (int r : roots)
         if (r >= 0 && isTheta(r)) needC[r] = 1;
     for (size_t x = 0; x < N.size(); ++x)
-        if (needC[x] && N[x].op != dag::Theta) cslot[x] = ncon++;
-    auto lit = [&](double v) { return num(v); };
-    // expression of node x in a context (prologue: theta-only names; event: C[] / event names)
-    auto ref = [&](int x, bool event_ctx) -> std::string {
+        if (needC[x]) cslot[x] = ncon++;
+
+    // ---------------- parameter-only prologue (FP64) ----------------
+    std::ostringstream pro;
+    auto proRef = [&](int x) -> std::string {
         const auto& nd = N[x];
-        if (nd.op == dag::Const) return lit(nd.v);
+        if (nd.op == dag::Const) return num(nd.v);
         if (nd.op == dag::Theta) return "th[" + std::to_string(nd.idx) + "]";
-        if (event_ctx && nd.dep == dag::DEP_THETA) return "C[" + std::to_string(cslot[x]) + "]";
-        return (event_ctx ? "e" : "t") + std::to_string(x);
+        return "t" + std::to_string(x);
     };
-    auto expr = [&](int x, bool ev) -> std::string {
-        const auto& nd = N[x];
-        auto A = [&]() { return ref(nd.a, ev); };
-        auto B = [&]() { return ref(nd.b, ev); };
+    auto opExpr = [&](const dag::Node& nd, const std::string& A, const std::string& B, const std::string& Cc,
+                      bool f32) -> std::string {
         switch (nd.op) {
-        case dag::Kin: {
-            if (nd.idx >= 0) return "kv[" + std::to_string(nd.idx) + "]";
-            int u = (-nd.idx - 1000) / 2;
-            return ((-nd.idx - 1000) % 2 == 0 ? "tre" : "tim") + std::to_string(u);
-        }
-        case dag::Add: return A() + " + " + B();
-        case dag::Sub: return A() + " - " + B();
-        case dag::Mul: return A() + " * " + B();
-        case dag::Recip: return "1.0 / " + A();
-        case dag::Neg: return "-" + A();
-        case dag::Sqrt: return "sqrt(" + A() + ")";
-        case dag::Log: return "log(" + A() + ")";
-        case dag::Exp: return "exp(" + A() + ")";
-        case dag::Sin: return "sin(" + A() + ")";
-        case dag::Cos: return "cos(" + A() + ")";
-        case dag::Atan2: return "atan2(" + A() + ", " + B() + ")";
+        case dag::Add: return A + " + " + B;
+        case dag::Sub: return A + " - " + B;
+        case dag::Mul: return A + " * " + B;
+        case dag::Recip: return f32 ? "ct_rcpf(" + A + ")" : "1.0 / " + A;
+        case dag::Neg: return "-" + A;
+        case dag::Sqrt: return f32 ? "ct_sqrtf(" + A + ")" : "sqrt(" + A + ")";
+        case dag::Log: return "log(" + A + ")";
+        case dag::Exp: return "exp(" + A + ")";
+        case dag::Sin: return "sin(" + A + ")";
+        case dag::Cos: return "cos(" + A + ")";
+        case dag::Atan2: return "atan2(" + A + ", " + B + ")";
         case dag::Sel: {
             static const char* ops[] = {">=", ">", "<=", "<", "=="};
-            return "(" + ref(nd.c, ev) + " " + ops[nd.cmp] + " 0.0 ? " + A() + " : " + B() + ")";
+            return "(" + Cc + " " + ops[nd.cmp] + (f32 ? " 0.0f ? " : " 0.0 ? ") + A + " : " + B + ")";
         }
-        case dag::RhoRe: return "ct_rho(" + A() + ", " + B() + ", " + ref(nd.c, ev) + ", 0)";
-        case dag::RhoIm: return "ct_rho(" + A() + ", " + B() + ", " + ref(nd.c, ev) + ", 1)";
-        default: return lit(nd.v);
+        case dag::RhoRe: return std::string(f32 ? "(float)" : "") + "ct_rho(" + A + ", " + B + ", " + Cc + ", 0)";
+        case dag::RhoIm: return std::string(f32 ? "(float)" : "") + "ct_rho(" + A + ", " + B + ", " + Cc + ", 1)";
+        default: return num(nd.v);
         }
     };
-    std::ostringstream pro, evs;
     for (size_t x = 0; x < N.size(); ++x) {
-        if (!live[x] || N[x].op == dag::Const || N[x].op == dag::Theta) continue;
-        if (N[x].dep == dag::DEP_THETA) {
-            pro << "  const double t" << x << " = " << expr((int)x, false) << ";\n";
-            if (cslot[x] >= 0) pro << "  C[" << cslot[x] << "] = t" << x << ";\n";
+        if (!live[x] || N[x].op == dag::Const) continue;
+        if (N[x].dep != dag::DEP_THETA) continue;
+        if (N[x].op != dag::Theta) {
+            const auto& nd = N[x];
+            pro << "  const double t" << x << " = "
+                << opExpr(nd, nd.a >= 0 ? proRef(nd.a) : "", nd.b >= 0 ? proRef(nd.b) : "", nd.c >= 0 ? proRef(nd.c) : "",
+                          false)
+                << ";\n";
         }
+        if (cslot[x] >= 0) pro << "  C[" << cslot[x] << "] = " << proRef((int)x) << ";\n";
     }
-    // table lookups (opaque per-event values) first
-    for (size_t u = 0; u < tab_uses.size(); ++u) {
-        const auto& t = tab_uses[u];
-        if (t.interp)
-            evs << "  double tre" << u << ", tim" << u << "; ls_interp(ct_tab" << t.table << ", " << ref(t.mnode, true)
-                << ", tre" << u << ", tim" << u << ");\n";
-        else
-            evs << "  const double tre" << u << " = ls_hist(" << ref(t.mnode, true) << ", ct_tab" << t.table
-                << "), tim" << u << " = 0.0;\n";
-    }
-    for (size_t x = 0; x < N.size(); ++x) {
-        if (!live[x] || N[x].op == dag::Const || N[x].op == dag::Theta) continue;
-        if (N[x].dep & dag::DEP_EVENT) evs << "  const double e" << x << " = " << expr((int)x, true) << ";\n";
-    }
-    // outputs
-    int k = 0;
+
+    // ---------------- per-event code ----------------
+    // f32 = false: everything in FP64.
+    // f32 = true: the mixed form. Event nodes built from kinematic values and
+    // constants by + - * only, that feed a subtraction (or an addition of
+    // terms of unknown sign), stay FP64, so the cancellation in m0^2 - m^2
+    // and the like happens in full precision; transcendental functions are
+    // FP64 too (their FP32 versions are not correctly rounded, and a bias
+    // would not average out over a sample); everything else is FP32 with
+    // correctly rounded reciprocals and square roots.
+    auto events = [&](bool f32) -> std::string {
+        std::vector<char> cap(N.size(), 0), dbl(N.size(), 0);
+        if (f32) {
+            for (size_t x = 0; x < N.size(); ++x) {
+                const auto& nd = N[x];
+                if (!live[x] || !(nd.dep & dag::DEP_EVENT)) continue;
+                if (nd.op == dag::Kin) {
+                    cap[x] = nd.idx >= 0;
+                    continue;
+                }
+                if (nd.op != dag::Add && nd.op != dag::Sub && nd.op != dag::Mul && nd.op != dag::Neg) continue;
+                bool ok = true;
+                for (int k : {nd.a, nd.b})
+                    if (k >= 0 && (N[k].dep & dag::DEP_EVENT) && !cap[k]) ok = false;
+                cap[x] = ok;
+            }
+            // nodes known to be >= 0 (an addition of two of them cannot cancel)
+            std::vector<char> nonneg(N.size(), 0);
+            for (size_t x = 0; x < N.size(); ++x) {
+                const auto& nd = N[x];
+                switch (nd.op) {
+                case dag::Const: nonneg[x] = nd.v >= 0.0; break;
+                case dag::Kin:
+                    nonneg[x] = nd.idx >= 0 && out.slots[nd.idx].type != AG_K_CT_ && out.slots[nd.idx].type != AG_K_PHI_;
+                    break;
+                case dag::Mul: nonneg[x] = nd.a == nd.b || (nonneg[nd.a] && nonneg[nd.b]); break;
+                case dag::Add: nonneg[x] = nonneg[nd.a] && nonneg[nd.b]; break;
+                case dag::Recip:
+                case dag::Sqrt: nonneg[x] = nonneg[nd.a]; break;
+                case dag::Exp: nonneg[x] = 1; break;
+                default: break;
+                }
+            }
+            for (size_t x = 0; x < N.size(); ++x) {
+                const auto& nd = N[x];
+                if (live[x] && (nd.dep & dag::DEP_EVENT) &&
+                    (nd.op == dag::Log || nd.op == dag::Exp || nd.op == dag::Sin || nd.op == dag::Cos || nd.op == dag::Atan2))
+                    dbl[x] = 1;
+            }
+            for (size_t x = N.size(); x-- > 0;) {
+                const auto& nd = N[x];
+                if (!cap[x]) continue;
+                if (nd.op == dag::Sub) dbl[x] = 1;
+                if (nd.op == dag::Add && nd.a != nd.b && !(nonneg[nd.a] && nonneg[nd.b])) dbl[x] = 1;
+                if (!dbl[x]) continue;
+                for (int k : {nd.a, nd.b})
+                    if (k >= 0 && cap[k]) dbl[k] = 1;
+            }
+        }
+        // reference to node x from a consumer evaluated in FP32 (wantF) or FP64
+        auto ref = [&](int x, bool wantF) -> std::string {
+            const auto& nd = N[x];
+            if (nd.op == dag::Const) return wantF ? numf(nd.v) : num(nd.v);
+            if (nd.dep == dag::DEP_THETA) return (wantF ? "Cfh[" : "C[") + std::to_string(cslot[x]) + "]";
+            if (nd.op == dag::Kin && nd.idx >= 0) return (wantF ? "kf" : "kv[") + std::to_string(nd.idx) + (wantF ? "" : "]");
+            if (nd.op == dag::Kin) {
+                int u = (-nd.idx - 1000) / 2;
+                std::string v = ((-nd.idx - 1000) % 2 == 0 ? "tre" : "tim") + std::to_string(u);
+                return wantF ? "(float)" + v : v;
+            }
+            bool isF = f32 && !dbl[x];
+            std::string v = "e" + std::to_string(x);
+            if (wantF && !isF) return "(float)" + v;
+            if (!wantF && isF) return "(double)" + v;
+            return v;
+        };
+        std::ostringstream evs;
+        if (f32)
+            for (size_t k = 0; k < out.slots.size(); ++k)
+                evs << "  const float kf" << k << " = (float)kv[" << k << "]; (void)kf" << k << ";\n";
+        for (size_t u = 0; u < tab_uses.size(); ++u) {
+            const auto& t = tab_uses[u];
+            if (t.interp)
+                evs << "  double tre" << u << ", tim" << u << "; ls_interp(ct_tab" << t.table << ", " << ref(t.mnode, false)
+                    << ", tre" << u << ", tim" << u << ");\n";
+            else
+                evs << "  const double tre" << u << " = ls_hist(" << ref(t.mnode, false) << ", ct_tab" << t.table
+                    << "), tim" << u << " = 0.0;\n";
+        }
+        for (size_t x = 0; x < N.size(); ++x) {
+            const auto& nd = N[x];
+            if (!live[x] || nd.op == dag::Const || nd.op == dag::Theta || nd.op == dag::Kin) continue;
+            if (!(nd.dep & dag::DEP_EVENT)) continue;
+            bool isF = f32 && !dbl[x];
+            std::string A, B, Cc;
+            if (nd.op == dag::RhoRe || nd.op == dag::RhoIm) {
+                // channel factors are evaluated by an FP64 helper
+                A = ref(nd.a, false);
+                B = ref(nd.b, false);
+                Cc = ref(nd.c, false);
+            } else {
+                A = nd.a >= 0 ? ref(nd.a, isF) : "";
+                B = nd.b >= 0 ? ref(nd.b, isF) : "";
+                if (nd.c >= 0) {
+                    // the condition is tested in the precision it was computed in
+                    const auto& cn = N[nd.c];
+                    bool cF = f32 && (cn.dep & dag::DEP_EVENT) && cn.op != dag::Kin && !dbl[nd.c];
+                    Cc = ref(nd.c, cF);
+                }
+            }
+            std::string rhs = opExpr(nd, A, B, Cc, isF);
+            if (isF && (nd.op == dag::Add || nd.op == dag::Sub || nd.op == dag::Mul)) {
+                // An event-independent operand enters as hi + lo and the
+                // product is rounded once (fmaf): rounding it to FP32 first
+                // would bias every event alike, and so would rounding the
+                // product of two FP32-grid factors (structured low bits).
+                std::string hi, lo;
+                auto split = [&](int y) -> bool {
+                    const auto& yn = N[y];
+                    if (yn.op == dag::Const) {
+                        float h = (float)yn.v;
+                        double l = yn.v - (double)h;
+                        if (l == 0.0 || !std::isfinite(yn.v)) return false;
+                        hi = numf((double)h);
+                        lo = numf(l);
+                        return true;
+                    }
+                    if (yn.dep == dag::DEP_THETA) {
+                        hi = "Cfh[" + std::to_string(cslot[y]) + "]";
+                        lo = "Cfl[" + std::to_string(cslot[y]) + "]";
+                        return true;
+                    }
+                    return false;
+                };
+                const bool ca = split(nd.a);
+                const std::string ha = hi, la = lo;
+                const bool cb = split(nd.b);
+                const std::string hb = hi, lb = lo;
+                if (ca != cb) {
+                    const std::string ev = ca ? B : A, h = ca ? ha : hb, l = ca ? la : lb;
+                    if (nd.op == dag::Mul) rhs = "fmaf(" + ev + ", " + h + ", " + ev + " * " + l + ")";
+                    else if (nd.op == dag::Add) rhs = "(" + ev + " + " + h + ") + " + l;
+                    else if (ca) rhs = "(" + h + " - " + ev + ") + " + l;  // const - event
+                    else rhs = "(" + ev + " - " + h + ") - " + l;          // event - const
+                }
+            }
+            evs << "  const " << (isF ? "float" : "double") << " e" << x << " = " << rhs << ";\n";
+        }
+        int k = 0;
+        for (size_t a = 0; a < cols.size(); ++a) {
+            evs << "  Fr[" << a << "] = " << ref(cols[a].re, f32) << "; Fi[" << a << "] = " << ref(cols[a].im, f32) << ";\n";
+            for (const auto& d : cols[a].der) {
+                evs << "  dFr[" << k << "] = " << ref(d.second.first, f32) << "; dFi[" << k << "] = "
+                    << ref(d.second.second, f32) << ";\n";
+                ++k;
+            }
+        }
+        return evs.str();
+    };
+
     std::vector<std::pair<int, int>> der_entries;
-    for (size_t a = 0; a < cols.size(); ++a) {
-        evs << "  Fr[" << a << "] = " << ref(cols[a].re, true) << "; Fi[" << a << "] = " << ref(cols[a].im, true) << ";\n";
-        for (const auto& d : cols[a].der) {
-            evs << "  dFr[" << k << "] = " << ref(d.second.first, true) << "; dFi[" << k << "] = "
-                << ref(d.second.second, true) << ";\n";
-            der_entries.push_back({(int)a, d.first});
-            ++k;
-        }
-    }
+    for (size_t a = 0; a < cols.size(); ++a)
+        for (const auto& d : cols[a].der) der_entries.push_back({(int)a, d.first});
+    const int k = (int)der_entries.size();
     out.nder = k;
     out.nconst = ncon;
     std::ostringstream h;
@@ -802,10 +949,16 @@ std::string Gen::emit()
     h << "__device__ __forceinline__ void model_prologue(const double* __restrict__ th, double* __restrict__ C)\n{\n"
          "  (void)th; (void)C;\n"
       << pro.str() << "}\n";
-    h << "// per-event lineshape products and their parameter derivatives\n";
+    h << "// per-event lineshape products and their parameter derivatives (FP64)\n";
     h << "__device__ __forceinline__ void model_columns(const double* __restrict__ kv, const double* __restrict__ C,\n"
          "    double* Fr, double* Fi, double* dFr, double* dFi)\n{\n  (void)kv; (void)C; (void)dFr; (void)dFi;\n"
-      << evs.str() << "}\n";
+      << events(false) << "}\n";
+    h << "// the same in the mixed form (FP32 except cancellation-prone polynomial parts and\n"
+         "// transcendental functions; parameter-only constants enter as hi + lo FP32 pairs)\n";
+    h << "__device__ __forceinline__ void model_columns_f32(const double* __restrict__ kv, const double* __restrict__ C,\n"
+         "    const float* __restrict__ Cfh, const float* __restrict__ Cfl, float* Fr, float* Fi, float* dFr, float* dFi)\n{\n"
+         "  (void)kv; (void)C; (void)Cfh; (void)Cfl; (void)dFr; (void)dFi;\n"
+      << events(true) << "}\n";
     return h.str();
 }
 

@@ -497,16 +497,21 @@ struct FinalizeArgs {
 // One CTA: deterministic column sums of the CTA partials, then loss/gradient
 // assembly (src/Analysis.cu:1134-1183) and the coupling-gradient transform
 // dL/dp_c = (1/p_c) sum_{a in c} conj(g_a) v_a (src/AmpGen.cu:3581-3637).
-__global__ void __launch_bounds__(256) ct_finalize_kernel(FinalizeArgs A)
+__global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
 {
     extern __shared__ double sh[];  // [3][nacc] sample sums, then gv [2 nA], gt [nT]
     double* sums = sh;
-    for (int i = threadIdx.x; i < 3 * A.nacc; i += blockDim.x) {
+    // one warp per (sample, column): lanes stride over the CTA rows, then a
+    // fixed-order shuffle tree, so the sums are bit-reproducible
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int i = warp; i < 3 * A.nacc; i += nwarp) {
         int k = i / A.nacc, j = i % A.nacc;
         double s = 0.0;
         if (A.has[k])
-            for (int b = 0; b < A.cta[k][1]; ++b) s += A.partials[(long long)(A.cta[k][0] + b) * A.nacc + j];
-        sums[i] = s;
+            for (int b = lane; b < A.cta[k][1]; b += 32) s += A.partials[(long long)(A.cta[k][0] + b) * A.nacc + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) sums[i] = s;
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
@@ -972,9 +977,18 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     std::string helpers = readFile(dir + "/device_helpers.cuh");
     std::string fused = readFile(dir + "/fused_nll.cuh");
     std::string src = "#include \"fused_nll.cuh\"\n";
-    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
-                          "--fmad=true", "-lineinfo"};
-    const int nopts = 6;
+    std::vector<std::string> optv = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
+                                     "--fmad=true", "-lineinfo"};
+    // tuning knob: minimum resident CTAs per SM of the mixed phase-space kernel
+    if (const char* e = std::getenv("CTPWA_PH_MINB")) {
+        int v = std::atoi(e);
+        if (v < 1 || v > 8) throw std::runtime_error("CTPWA_PH_MINB must be in [1, 8]");
+        optv.push_back("-DCT_PH_MINB=" + std::to_string(v));
+    }
+    std::vector<const char*> optp;
+    for (const auto& o : optv) optp.push_back(o.c_str());
+    const char* const* opts = optp.data();
+    const int nopts = (int)optp.size();
     std::string key_src = helpers + fused + gen.header;
     for (int i = 0; i < nopts; ++i) key_src += opts[i];
     int nvmaj = 0, nvmin = 0;
@@ -1031,14 +1045,16 @@ void Engine::compileKernel()
     cudaLibrary_t lib;
     CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
     lib_ = (void*)lib;
-    cudaKernel_t k64, kmx, kin, kpro;
+    cudaKernel_t k64, kmx, kmxp, kin, kpro;
     CT_CUDA(cudaLibraryGetKernel(&kpro, lib, "ct_prologue"));
     k_pro_ = (void*)kpro;
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
+    CT_CUDA(cudaLibraryGetKernel(&kmxp, lib, "ct_fused_mixed_ph"));
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
     k_f64_ = (void*)k64;
     k_mixed_ = (void*)kmx;
+    k_mixed_ph_ = (void*)kmxp;
     k_int_ = (void*)kin;
     jit_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -1075,6 +1091,8 @@ struct CtArgsH {
     const double* v;
     double* partials;
     double* consts;
+    int cta_base;
+    int pad2;
 };
 
 void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
@@ -1109,7 +1127,22 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     const size_t slot = ev_begin_.empty() ? 0 : (size_t)(ev_count_ % (long long)ev_begin_.size());
     if (!ev_begin_.empty()) CT_CUDA(cudaEventRecord(ev_begin_[slot], stream));
-    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    if (precision == kMixed) {
+        // phase space with FP32 lineshapes, then data and background with FP64
+        // lineshapes; both write their rows of the same partials table
+        const int nph = cta_[0][1];
+        if (nph > 0) {
+            a.cta_base = 0;
+            CT_CUDA(cudaLaunchKernel(k_mixed_ph_, dim3(nph), dim3(256), args, 0, stream));
+        }
+        if (grid_ > nph) {
+            a.cta_base = nph;
+            CT_CUDA(cudaLaunchKernel(k_mixed_, dim3(grid_ - nph), dim3(256), args, 0, stream));
+        }
+    } else {
+        a.cta_base = 0;
+        CT_CUDA(cudaLaunchKernel(k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    }
     if (!ev_begin_.empty()) {
         CT_CUDA(cudaEventRecord(ev_end_[slot], stream));
         ++ev_count_;
@@ -1139,7 +1172,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     f.out_grad = d_grad;
     f.out_parts = d_parts_;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
-    ct_finalize_kernel<<<1, 256, shm, stream>>>(f);
+    ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
 }
 

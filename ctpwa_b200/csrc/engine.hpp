@@ -54,10 +54,12 @@ public:
     // [data_nll, bkg_nll, phsp_sum, W_data, W_bkg, n_phsp]
     void lastParts(double* out6, cudaStream_t stream);
 
-    // Optional per-launch timing of the fused kernel: CUDA events recorded on
-    // the launching stream around each fused launch into a ring of `slots`
-    // pairs (0 switches timing off). kernelTimes synchronises on the recorded
-    // events and returns the durations (ms) of the most recent launches.
+    // Optional timing of the fused pass (the one fused launch of the plain
+    // path, or the phase-space and data/background launches of the mixed
+    // form): CUDA events recorded on the launching stream around it into a
+    // ring of `slots` pairs (0 switches timing off). kernelTimes synchronises
+    // on the recorded events and returns the durations (ms) of the most
+    // recent passes.
     void setKernelTiming(int slots);
     int kernelTimes(float* ms, int cap);
 
@@ -89,7 +91,8 @@ private:
     // JIT
     void* lib_ = nullptr;  // cudaLibrary_t
     void* k_f64_ = nullptr;
-    void* k_mixed_ = nullptr;
+    void* k_mixed_ = nullptr;     // mixed form, data and background
+    void* k_mixed_ph_ = nullptr;  // mixed form, phase space
     void* k_int_ = nullptr;
     void* k_pro_ = nullptr;
     double jit_seconds_ = 0.0;

@@ -84,3 +84,14 @@ __device__ __forceinline__ void ls_interp(const double* t, double x, double& Fr,
     Fr = ls_interp1(re, i, fr, method, N);
     Fi = ls_interp1(im, i, fr, method, N);
 }
+
+__device__ __forceinline__ double ct_nan() { return __longlong_as_double(0x7ff8000000000000LL); }
+__device__ __forceinline__ double ct_inf() { return __longlong_as_double(0x7ff0000000000000LL); }
+__device__ __forceinline__ float ct_nanf() { return __int_as_float(0x7fc00000); }
+__device__ __forceinline__ float ct_inff() { return __int_as_float(0x7f800000); }
+
+// FP32 reciprocal and square root of the mixed-form lineshapes, correctly
+// rounded: their errors are symmetric, so they average out over a sample
+// instead of biasing the phase-space normalisation.
+__device__ __forceinline__ float ct_rcpf(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float ct_sqrtf(float x) { return __fsqrt_rn(x); }

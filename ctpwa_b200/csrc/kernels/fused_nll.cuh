@@ -5,12 +5,15 @@
 //   M_NA, M_NPOL, M_NPLANE, M_NKIN, M_NTH, M_NDER     sizes
 //   col_plane(a)   angular plane (group, SL combination) of amplitude column a
 //   der_col(k), der_th(k)   column / theta index of derivative entry k
-//   model_columns(kin, th, Fr, Fi, dFr, dFi)   lineshape products F_a and their
-//       theta derivatives for one event (straight-line generated code)
+//   model_prologue(theta, C)   parameter-only subexpressions, once per call
+//   model_columns(kin, C, Fr, Fi, dFr, dFi)   lineshape products F_a and their
+//       theta derivatives for one event (straight-line generated code, FP64)
+//   model_columns_f32(...)   the same in the mixed form (FP32 except the
+//       cancellation-prone polynomial parts such as m0^2 - m^2)
 //
 // Per event e of a sample (phase space, data or background) the kernel forms
 //   A_{a,p} = F_a * SL_{plane(a),p},   S_p = sum_a v_a A_{a,p},   f = sum_p |S_p|^2
-// and accumulates, per thread, in FP64:
+// and accumulates, per thread:
 //   data/bkg: nll += -w log f;  u_p = clamp(w S_p / f);  T_c = sum_p conj(SL_{c,p}) u_p
 //             gv_a += -conj(F_a) T_{plane(a)};  gt_j += -2 Re(v_a dF_{a,j} conj(T_{plane(a)}))
 //   phsp:     fsum += f;  T_c = sum_p conj(SL_{c,p}) S_p
@@ -22,11 +25,14 @@
 // memory and writes one row of partial sums; a separate finalize kernel sums
 // the rows in a fixed order, so results are bit-reproducible.
 //
-// R is the arithmetic type of the per-polarisation complex algebra (double for
-// the plain path, float for the mixed path); SL2 is the stored angular-table
-// element (double2 / float2). Lineshapes, the log and all accumulations are FP64.
-// Parameter-only parts of the lineshapes are computed once per call by
-// ct_prologue and staged in shared memory by every CTA.
+// Precision. Plain path (ct_fused_f64): everything FP64. Mixed form: the
+// angular tables and the per-polarisation algebra are FP32 for every sample;
+// data and background (the log-likelihood sample, ct_fused_mixed) keep FP64
+// lineshapes; phase space (the normalisation average, ct_fused_mixed_ph) uses
+// the FP32 lineshapes and FP32 per-thread gradient sums. The log, the
+// log-likelihood and phase-space intensity sums and every cross-thread
+// reduction are FP64 in all forms. Parameter-only parts of the lineshapes
+// are computed once per call by ct_prologue and staged in shared memory.
 #pragma once
 
 #include "device_helpers.cuh"
@@ -56,8 +62,10 @@ struct CtArgs {
     int pad;
     const double* theta;  // fitted resonance parameters
     const double* v;      // couplings, interleaved (re, im) x M_NA
-    double* partials;     // [gridDim.x][CT_NACC]
+    double* partials;     // [total CTAs][CT_NACC]
     double* consts;       // [M_NCONST] parameter-only subexpressions of this call
+    int cta_base;         // CTA index of this launch's first block (split launches)
+    int pad2;
 };
 
 // One thread: the parameter-only part of every lineshape (prologue).
@@ -85,14 +93,16 @@ struct CtVec2<float> {
     typedef float2 type;
 };
 
-template <typename R>
-__device__ __forceinline__ void ct_block_reduce_store(double* acc, double* out)
+// CTA reduction of the per-thread accumulators: two FP64 sums (log-likelihood
+// and phase-space intensity) and the gradient terms (type G), reduced in FP64.
+template <typename G>
+__device__ __forceinline__ void ct_block_reduce_store(const double* accd, const G* accg, double* out)
 {
     __shared__ double red[CT_BLOCK / 32][CT_NACC];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int i = 0; i < CT_NACC; ++i) {
-        double x = acc[i];
+        double x = i < 2 ? accd[i] : (double)accg[i - 2];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0) red[warp][i] = x;
@@ -106,43 +116,83 @@ __device__ __forceinline__ void ct_block_reduce_store(double* acc, double* out)
     }
 }
 
-template <typename R>
+template <typename L>
+struct CtLineshape;
+template <>
+struct CtLineshape<double> {
+    static __device__ __forceinline__ void eval(const double* kv, const double* C, const float*, const float*,
+                                                double* Fr, double* Fi, double* dFr, double* dFi)
+    {
+        model_columns(kv, C, Fr, Fi, dFr, dFi);
+    }
+};
+template <>
+struct CtLineshape<float> {
+    static __device__ __forceinline__ void eval(const double* kv, const double* C, const float* Cfh, const float* Cfl,
+                                                float* Fr, float* Fi, float* dFr, float* dFi)
+    {
+        model_columns_f32(kv, C, Cfh, Cfl, Fr, Fi, dFr, dFi);
+    }
+};
+
+// R: type of the per-polarisation complex algebra and of the stored angular
+//    table (double: plain path; float: mixed form)
+// L: type of the lineshapes, their derivatives and the per-thread gradient
+//    sums (double, or float for the mixed form's phase-space pass)
+// PH_ONLY: the launch serves phase-space events only
+template <typename R, typename L, bool PH_ONLY>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 {
     typedef typename CtVec2<R>::type SL2;
+    const int cta = (int)blockIdx.x + A.cta_base;
     // which sample does this CTA serve?
     int si = 0;
 #pragma unroll
     for (int k = 1; k < 3; ++k)
-        if (k < A.nsamp && (int)blockIdx.x >= A.s[k].cta_begin) si = k;
+        if (k < A.nsamp && cta >= A.s[k].cta_begin) si = k;
     const CtSample& S = A.s[si];
-    const int kind = S.kind;
+    const int kind = PH_ONLY ? 0 : S.kind;
     const long long n = S.n;
     const SL2* __restrict__ slamp = (const SL2*)S.slamp;
     const double* __restrict__ kin = S.kin;
     const double* __restrict__ wts = S.w;
 
-    double acc[CT_NACC];
+    double accd[2] = {0.0, 0.0};
+    L accg[CT_NACC - 2];
 #pragma unroll
-    for (int i = 0; i < CT_NACC; ++i) acc[i] = 0.0;
+    for (int i = 0; i < CT_NACC - 2; ++i) accg[i] = (L)0;
 
+    // parameter-only constants: FP64, and as FP32 hi + lo pairs for the
+    // FP32 lineshapes (a single FP32 rounding would bias every event alike)
     __shared__ double sC[CT_NCONST_ALLOC];
-    ct_stage_consts(A, sC);
-    double vr[M_NA], vi[M_NA];
+    __shared__ float sCfh[CT_NCONST_ALLOC], sCfl[CT_NCONST_ALLOC];
+    for (int i = threadIdx.x; i < M_NCONST; i += blockDim.x) {
+        const double c = A.consts[i];
+        const float h = (float)c;
+        sC[i] = c;
+        sCfh[i] = h;
+        sCfl[i] = (float)(c - (double)h);
+    }
+    __syncthreads();
+    // couplings: (hi, lo) pairs in the FP32 form for the same reason
+    L vr[M_NA], vi[M_NA], vrl[M_NA], vil[M_NA];
 #pragma unroll
     for (int a = 0; a < M_NA; ++a) {
-        vr[a] = __ldg(A.v + 2 * a);
-        vi[a] = __ldg(A.v + 2 * a + 1);
+        const double r = __ldg(A.v + 2 * a), i = __ldg(A.v + 2 * a + 1);
+        vr[a] = (L)r;
+        vi[a] = (L)i;
+        vrl[a] = (L)(r - (double)vr[a]);
+        vil[a] = (L)(i - (double)vi[a]);
     }
 
     const long long stride = (long long)S.cta_count * CT_BLOCK;
-    for (long long e = (long long)(blockIdx.x - S.cta_begin) * CT_BLOCK + threadIdx.x; e < n; e += stride) {
-        // ---- lineshapes (FP64, with theta derivatives) ----
+    for (long long e = (long long)(cta - S.cta_begin) * CT_BLOCK + threadIdx.x; e < n; e += stride) {
+        // ---- lineshapes with parameter derivatives ----
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
         for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(kin + (long long)k * n + e);
-        double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        model_columns(kv, sC, Fr, Fi, dFr, dFi);
+        L Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
+        CtLineshape<L>::eval(kv, sC, sCfh, sCfl, Fr, Fi, dFr, dFi);
 
         // ---- coherent sum over amplitudes ----
         SL2 sl[M_NPLANE * M_NPOL];
@@ -151,8 +201,18 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         R cr[M_NA], ci[M_NA];
 #pragma unroll
         for (int a = 0; a < M_NA; ++a) {
-            cr[a] = (R)(vr[a] * Fr[a] - vi[a] * Fi[a]);
-            ci[a] = (R)(vr[a] * Fi[a] + vi[a] * Fr[a]);
+            if constexpr (sizeof(L) == 4) {
+                // Each product of a per-event value with a coupling is rounded
+                // once, from the full-precision coupling (hi + lo): rounding the
+                // product with the FP32 coupling alone would bias the sample
+                // mean by ~1e-9 (both factors on the FP32 grid), which the
+                // normalisation term multiplies by the data weight sum.
+                cr[a] = fmaf(Fr[a], vr[a], Fr[a] * vrl[a]) - fmaf(Fi[a], vi[a], Fi[a] * vil[a]);
+                ci[a] = fmaf(Fi[a], vr[a], Fi[a] * vrl[a]) + fmaf(Fr[a], vi[a], Fr[a] * vil[a]);
+            } else {
+                cr[a] = (R)(vr[a] * Fr[a] - vi[a] * Fi[a]);
+                ci[a] = (R)(vr[a] * Fi[a] + vi[a] * Fr[a]);
+            }
         }
         R Sr[M_NPOL], Si[M_NPOL];
         R f = (R)0;
@@ -171,25 +231,26 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         }
 
         // ---- per-event weight of the adjoint ----
-        const double we = wts ? __ldg(wts + e) : 1.0;
         R ur[M_NPOL], ui[M_NPOL];
-        R gscale;  // factor applied to v-gradient contributions
-        R tscale;  // factor applied to theta-gradient contributions
+        L gscale;  // factor applied to v-gradient contributions
+        L tscale;  // factor applied to theta-gradient contributions
         if (kind == 0) {
-            acc[1] += (double)f;
+            const double we = wts ? __ldg(wts + e) : 1.0;
+            accd[1] += (double)f;
 #pragma unroll
             for (int p = 0; p < M_NPOL; ++p) {
                 ur[p] = Sr[p];
                 ui[p] = Si[p];
             }
-            gscale = (R)(we * S.vw_scale);
-            tscale = (R)2;
+            gscale = (L)(we * S.vw_scale);
+            tscale = (L)2;
         } else {
+            const double we = wts ? __ldg(wts + e) : 1.0;
             if (f == (R)0) {
-                acc[0] += -log(1e-10) * we;
+                accd[0] += -log(1e-10) * we;
                 continue;
             }
-            acc[0] += -log((double)f) * we;
+            accd[0] += -log((double)f) * we;
             const R inv = (R)(we / (double)f);
             const R kmax = (R)1e10;
 #pragma unroll
@@ -197,8 +258,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 ur[p] = fmin(fmax(Sr[p] * inv, -kmax), kmax);
                 ui[p] = fmin(fmax(Si[p] * inv, -kmax), kmax);
             }
-            gscale = (R)-1;
-            tscale = (R)-2;
+            gscale = (L)-1;
+            tscale = (L)-2;
         }
         // T_c = sum_p conj(SL_{c,p}) u_p
         R Tr[M_NPLANE], Ti[M_NPLANE];
@@ -218,25 +279,34 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #pragma unroll
         for (int a = 0; a < M_NA; ++a) {
             const int c = col_plane(a);
-            R fr = (R)Fr[a], fi = (R)Fi[a];
-            acc[2 + 2 * a] += (double)(gscale * (fr * Tr[c] + fi * Ti[c]));
-            acc[3 + 2 * a] += (double)(gscale * (fr * Ti[c] - fi * Tr[c]));
+            const L fr = Fr[a], fi = Fi[a];
+            const L tr = (L)Tr[c], ti = (L)Ti[c];
+            accg[2 * a] += gscale * (fr * tr + fi * ti);
+            accg[2 * a + 1] += gscale * (fr * ti - fi * tr);
         }
         // theta-gradient: Re(v_a dF conj(T))
 #pragma unroll
         for (int k = 0; k < M_NDER; ++k) {
             const int a = der_col(k), c = col_plane(a);
-            double xr = vr[a] * dFr[k] - vi[a] * dFi[k];
-            double xi = vr[a] * dFi[k] + vi[a] * dFr[k];
-            R re = (R)xr * Tr[c] + (R)xi * Ti[c];
-            acc[2 + 2 * M_NA + der_th(k)] += (double)(tscale * re);
+            const L xr = vr[a] * dFr[k] - vi[a] * dFi[k];
+            const L xi = vr[a] * dFi[k] + vi[a] * dFr[k];
+            accg[2 * M_NA + der_th(k)] += tscale * (xr * (L)Tr[c] + xi * (L)Ti[c]);
         }
     }
-    ct_block_reduce_store<R>(acc, A.partials + (long long)blockIdx.x * CT_NACC);
+    ct_block_reduce_store<L>(accd, accg, A.partials + (long long)cta * CT_NACC);
 }
 
-extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_fused_f64(CtArgs a) { ct_fused_body<double>(a); }
-extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_fused_mixed(CtArgs a) { ct_fused_body<float>(a); }
+extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_fused_f64(CtArgs a) { ct_fused_body<double, double, false>(a); }
+// mixed form, data and background (FP64 lineshapes)
+extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_fused_mixed(CtArgs a) { ct_fused_body<float, double, false>(a); }
+// mixed form, phase space (FP32 lineshapes)
+#ifndef CT_PH_MINB
+#define CT_PH_MINB 2
+#endif
+extern "C" __global__ void __launch_bounds__(CT_BLOCK, CT_PH_MINB) ct_fused_mixed_ph(CtArgs a)
+{
+    ct_fused_body<float, float, true>(a);
+}
 
 // Per-event intensity f_e = sum_p |S_p|^2 of sample s[0] (FP64), for
 // accept-reject toy generation and per-event weights.
