@@ -22,6 +22,8 @@ SIGNATURES = {
     "ctpwa_free_res_params": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "ctpwa_nll_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_int, ctypes.c_void_p]),
+    "ctpwa_nll_grad_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int, ctypes.c_void_p]),
     "ctpwa_nll_grad_host": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p,
                                            ctypes.c_int, ctypes.c_void_p]),
     "ctpwa_intensity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,

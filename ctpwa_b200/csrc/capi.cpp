@@ -9,6 +9,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <stdexcept>
 #include <string>
 
 struct ctpwa_handle {
@@ -116,6 +117,21 @@ int ctpwa_nll_grad(ctpwa_handle* h, const double* d_params, double* d_nll, doubl
     if (precision != CTPWA_FP64 && precision != CTPWA_MIXED) return setErr(h, CTPWA_ERR_ARG, "precision must be 0 or 1");
     try {
         h->eng->nllGrad(d_params, d_nll, d_grad, precision, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision,
+                          void* stream)
+{
+    if (!h || !d_params || !d_nll || !d_grad) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (precision != CTPWA_FP64 && precision != CTPWA_MIXED) return setErr(h, CTPWA_ERR_ARG, "precision must be 0 or 1");
+    try {
+        h->eng->nllGradStatic(d_params, d_nll, d_grad, precision, (cudaStream_t)stream);
+    } catch (const std::length_error& e) {
+        return setErr(h, CTPWA_ERR_ARG, e.what());
     } catch (const std::exception& e) {
         return setErr(h, CTPWA_ERR_CUDA, e.what());
     }

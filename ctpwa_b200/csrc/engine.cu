@@ -29,6 +29,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
+#include <mutex>
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
@@ -1171,6 +1172,144 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     f.out_nll = d_nll;
     f.out_grad = d_grad;
     f.out_parts = d_parts_;
+    size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
+    ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
+    CT_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free evaluation: scratch in a fixed array of this library.
+//
+// Every GPU that loads the library holds this 2 MiB array until the process
+// exits. Host code may not use the symbol's name as a device address (it names
+// a host-side stand-in); the address comes from cudaGetSymbolAddress, once per
+// device, with that device current, the first time a handle on the device
+// calls nllGradStatic. That first call should therefore come before any stream
+// capture is begun on the device.
+//
+// Every call writes all of the scratch it later reads (couplings by
+// ct_prepare_kernel, constants by ct_prologue, one full partial row per CTA,
+// the parts by ct_finalize_kernel), so nothing has to start at zero. All
+// handles on a device share the array and it keeps the last call's contents:
+// calls whose GPU work overlaps (different streams, threads or handles
+// without ordering between them) race on it.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_ct_static_scratch[Engine::kStaticScratchBytes / sizeof(double)];
+
+namespace {
+
+double* staticScratchAddress(int device)
+{
+    static std::mutex mu;
+    static std::vector<double*> addr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0) throw std::runtime_error("static scratch: bad device");
+    if ((size_t)device >= addr.size()) addr.resize((size_t)device + 1, nullptr);
+    if (addr[device]) return addr[device];
+    int prev = -1;
+    CT_CUDA(cudaGetDevice(&prev));
+    CT_CUDA(cudaSetDevice(device));
+    double* p = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress((void**)&p, g_ct_static_scratch);
+    cudaError_t rc2 = cudaSetDevice(prev);
+    if (rc != cudaSuccess)
+        throw std::runtime_error(std::string("static scratch: cudaGetSymbolAddress failed: ") + cudaGetErrorString(rc));
+    if (rc2 != cudaSuccess)
+        throw std::runtime_error(std::string("static scratch: cudaSetDevice failed: ") + cudaGetErrorString(rc2));
+    addr[device] = p;
+    return p;
+}
+
+}  // namespace
+
+void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
+{
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    const int nacc = 2 + 2 * nA + nT;
+    // layout in doubles, each part on a 256-byte boundary
+    auto up = [](size_t x) { return (x + 31) / 32 * 32; };
+    const size_t off_v = 0;
+    const size_t off_c = off_v + up((size_t)2 * nA);
+    const size_t off_p = off_c + up((size_t)std::max(1, gen_.nconst));
+    const size_t off_parts = off_p + up((size_t)grid_ * nacc);
+    const size_t need = off_parts + 8;
+    const size_t cap = kStaticScratchBytes / sizeof(double);
+    if (need > cap)
+        throw std::length_error("ctpwa_nll_grad_static: this model needs " + std::to_string(need * sizeof(double)) +
+                                " bytes of scratch (" + std::to_string(grid_) + " CTA rows of " + std::to_string(nacc) +
+                                " sums), more than the fixed " + std::to_string(kStaticScratchBytes) +
+                                " bytes; use ctpwa_nll_grad");
+    double* base = staticScratchAddress(opt_.device);
+    double* s_v = base + off_v;
+    double* s_consts = base + off_c;
+    double* s_partials = base + off_p;
+    double* s_parts = base + off_parts;
+
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, s_v);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    int ns = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (cta_[k][1] == 0) continue;
+        CtSampleH& sm = a.s[ns++];
+        const DeviceSample& d = samples_[k];
+        sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
+        sm.kin = d.kin;
+        sm.w = d.w;
+        sm.n = d.n;
+        sm.kind = k;
+        sm.cta_begin = cta_[k][0];
+        sm.cta_count = cta_[k][1];
+        sm.vw_scale = 1.0 / (samples_[0].wsum > 0 ? samples_[0].wsum : 1.0);
+    }
+    a.nsamp = ns;
+    a.theta = d_params + 2 * nc;
+    a.v = s_v;
+    a.partials = s_partials;
+    a.consts = s_consts;
+    if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
+    void* args[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    if (precision == kMixed) {
+        const int nph = cta_[0][1];
+        if (nph > 0) {
+            a.cta_base = 0;
+            CT_CUDA(cudaLaunchKernel(k_mixed_ph_, dim3(nph), dim3(256), args, 0, stream));
+        }
+        if (grid_ > nph) {
+            a.cta_base = nph;
+            CT_CUDA(cudaLaunchKernel(k_mixed_, dim3(grid_ - nph), dim3(256), args, 0, stream));
+        }
+    } else {
+        a.cta_base = 0;
+        CT_CUDA(cudaLaunchKernel(k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    }
+    FinalizeArgs f;
+    std::memset(&f, 0, sizeof(f));
+    f.partials = s_partials;
+    f.nacc = nacc;
+    f.nA = nA;
+    f.nc = nc;
+    f.nT = nT;
+    for (int k = 0; k < 3; ++k) {
+        f.cta[k][0] = cta_[k][0];
+        f.cta[k][1] = cta_[k][1];
+        f.has[k] = cta_[k][1] > 0;
+    }
+    f.n_phsp = (double)samples_[0].n;
+    f.W_data = samples_[1].wsum;
+    f.W_bkg = has_bkg_ ? samples_[2].wsum : 0.0;
+    f.params = d_params;
+    f.v = s_v;
+    f.chain = d_amp_chain_;
+    f.gauss_idx = d_gauss_idx_;
+    f.gauss_ms = d_gauss_ms_;
+    f.ngauss = (int)m.gauss.size();
+    f.out_nll = d_nll;
+    f.out_grad = d_grad;
+    f.out_parts = s_parts;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());

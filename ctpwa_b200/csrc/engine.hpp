@@ -48,6 +48,13 @@ public:
     // NLL and gradient in the reference layout [Re p, Im p, theta]; all
     // pointers are device pointers; stream-ordered, no host synchronisation.
     void nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
+    // The same evaluation with its scratch (couplings, parameter-only
+    // constants, per-CTA partial rows, per-sample parts) in one fixed array
+    // compiled into the library instead of the handle's buffers; allocates
+    // nothing. Throws std::length_error when this model's scratch exceeds the
+    // array (kStaticScratchBytes). All handles on a device share the array.
+    void nllGradStatic(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
+    static constexpr size_t kStaticScratchBytes = size_t(2) << 20;
     // Per-event intensities of sample `kind` at d_params (device output [n]).
     void intensity(const double* d_params, int kind, double* d_out, cudaStream_t stream);
     // Per-sample partial sums of the last evaluation (diagnostics):

@@ -69,6 +69,31 @@ int ctpwa_free_res_params(const ctpwa_handle* h, double* out);
  * precision: CTPWA_FP64 or CTPWA_MIXED. */
 int ctpwa_nll_grad(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision, void* stream);
 
+/* Allocation-free variant of ctpwa_nll_grad. No counterpart in the reference.
+ *
+ * For callers that cannot let a library allocate device memory for them: a
+ * host program that hands all device memory to its own pool allocator after
+ * start-up, or one that counts every device byte against a fixed budget (a
+ * serving loop that admits jobs by memory). The evaluation scratch (coupling
+ * vector, parameter-only constants, one partial-sum row per CTA) lives in one
+ * fixed 2 MiB array compiled into libctpwa_b200.so, present on every GPU that
+ * loads the library until the process exits; the call allocates nothing and
+ * uses none of the handle's own scratch. Same arguments, results and stream
+ * ordering as ctpwa_nll_grad.
+ *  - A model whose scratch does not fit (about 4 + 2 nA + nT doubles per CTA
+ *    row, up to 8 rows per SM) is rejected with CTPWA_ERR_ARG and a message;
+ *    use ctpwa_nll_grad for it.
+ *  - The first call on a device looks the array's address up (once per
+ *    device, with the handle's device current); make that first call before
+ *    beginning any stream capture on the device.
+ *  - Every call writes all the scratch it reads, so nothing needs clearing,
+ *    but all handles on a device share the one array: calls whose GPU work
+ *    can overlap (other streams, threads or handles without ordering between
+ *    them) race and give wrong results. ctpwa_last_parts does not see these
+ *    calls. */
+int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision,
+                          void* stream);
+
 /* Same evaluation from host buffers: copies params host->device, evaluates,
  * copies NLL and gradient back, and synchronises the stream. */
 int ctpwa_nll_grad_host(ctpwa_handle* h, const double* params, double* nll, double* grad, int precision, void* stream);
