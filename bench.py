@@ -14,8 +14,9 @@ One JSON line on rank 0. `value` is the mixed-precision path (FP32 angular
 tables and coherent sum, FP64 lineshapes, logs and accumulations) with the
 events resident in HBM; the FP64 path is timed beside it; `e2e` goes through
 the host-buffer C-ABI entry point. Multi-GPU: each rank holds its own shard of
-the same size (weak scaling) and the per-step exchange is one NCCL all-reduce
-of the packed (NLL, gradient) buffer.
+the same size (weak scaling); the per-step exchange is one NCCL all-reduce of
+the ranks' per-sample sums, after which every rank forms the loss and
+gradient of the union of the shards.
 
 `--impl reference`: the reference has no CPU path and its CUDA build needs
 yaml-cpp and ROOT, which are absent, so this arm times the FP64 OpenMP port of
@@ -302,6 +303,7 @@ def run_gpu(args, rank, world, local_rank):
     import torch.distributed as dist
 
     import ctpwa_b200
+    from ctpwa_b200 import shards
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -320,14 +322,13 @@ def run_gpu(args, rank, world, local_rank):
     P = np.tile(p0, (W + K, 1))
     P[:, 2 * nV:] *= 1.0 + 1e-4 * rng.standard_normal((W + K, nT))  # new theta every step
     Pd = torch.tensor(P, dtype=torch.float64, device=dev)
-    packed = torch.empty(1 + nP, dtype=torch.float64, device=dev)
 
     def step(i, prec):
-        nll, g = ana.getNLLAndGrad(Pd[i], prec)
         if world > 1:
-            packed[0] = nll
-            packed[1:] = g
-            dist.all_reduce(packed)
+            # this rank's per-sample sums, one NCCL all-reduce, loss and gradient of the union
+            nll, g = shards.nll_grad(ana, Pd[i], precision=prec)
+        else:
+            nll, g = ana.getNLLAndGrad(Pd[i], prec)
         return nll
 
     def barrier():
@@ -373,19 +374,28 @@ def run_gpu(args, rank, world, local_rank):
     dnll = abs(float(n64) - float(nmx))
     grel = float((g64 - gmx).abs().max() / g64.abs().max().clamp_min(1e-300))
 
-    # end to end through the host-buffer entry point (params in, NLL + gradient out)
+    # end to end from host memory: params in, NLL + gradient out. One GPU: the
+    # host-buffer C-ABI entry point. Several: pinned host params -> device,
+    # the sharded evaluation, result -> host.
     E = args.e2e_steps or K
     Ph = [np.ascontiguousarray(P[i % (W + K)]) for i in range(W + E)]
-    host_group = dist.new_group(backend="gloo") if world > 1 else None
+    pin = torch.empty(nP, dtype=torch.float64).pin_memory()
+    dpar = torch.empty(nP, dtype=torch.float64, device=dev)
+
+    def host_step(i):
+        if world == 1:
+            return ana.getNLLHost(Ph[i], "mixed")
+        pin.copy_(torch.from_numpy(Ph[i]))
+        dpar.copy_(pin, non_blocking=True)
+        nll, g = shards.nll_grad(ana, dpar, precision="mixed")
+        return float(nll), g.cpu().numpy()
+
     for i in range(W):
-        ana.getNLLHost(Ph[i], "mixed")
+        host_step(i)
     barrier()
     t0 = time.perf_counter()
     for i in range(E):
-        v, g = ana.getNLLHost(Ph[W + i], "mixed")
-        if world > 1:
-            t = torch.from_numpy(np.concatenate([[v], g]))
-            dist.all_reduce(t, group=host_group)
+        host_step(W + i)
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * nP, "d2h_bytes_per_step": 8 * (1 + nP),
            "ms_per_step": 1e3 * e2e_s / E}
@@ -422,7 +432,8 @@ def run_gpu(args, rank, world, local_rank):
                    "n_params": nP, "theta_perturbed_every_step": True, "fraction": args.fraction,
                    "l2": f"inputs larger than L2: {streamed_bytes(layout, n_events, 'mixed') / 1e9:.2f} GB streamed "
                          f"per step vs {L2_BYTES / 1e6:.0f} MB L2, no flush",
-                   "exchange": "NCCL all-reduce of packed (NLL, grad) per step" if world > 1 else "none (1 GPU)"},
+                   "exchange": ("NCCL all-reduce of the per-sample sums per step (3*(2+2nA+nT)+4 doubles), "
+                                "then loss/gradient of the union on every rank") if world > 1 else "none (1 GPU)"},
         "fp64": {"value": world * 1e3 / res["fp64"]["ms"], "unit": UNIT, "ms_per_step": res["fp64"]["ms"],
                  "kernel_ms": res["fp64"]["kernel_ms"], "roofline_frac": ach64 / peak,
                  "traffic": ncu_traffic("fp64") if args.fraction == 1.0 else None,
@@ -432,7 +443,9 @@ def run_gpu(args, rank, world, local_rank):
         "clocks": clocks,
         "e2e": e2e,
         # per mixed step: prepare, prologue, phase-space pass, data/background pass, finalize
-        "gpu_launches": (3 + (2 if n_events[0] > 0 and n_events[1] + n_events[2] > 0 else 1)) * K,
+        # (multi-GPU: + per-sample row sums and a second prepare before the finalize)
+        "gpu_launches": (3 + (2 if n_events[0] > 0 and n_events[1] + n_events[2] > 0 else 1) + (2 if world > 1 else 0))
+                        * K,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src,
                      "kernel": "fused pass: ct_fused_mixed_ph + ct_fused_mixed",

@@ -127,7 +127,9 @@ class analysis:
     """Likelihood of one config.yml model over its phase-space, data and
     background samples (reference ``ctpwa.analysis``)."""
 
-    def __init__(self, config_file: str = "config.yml", device=None, precision: str = "fp64"):
+    def __init__(self, config_file: str = "config.yml", device=None, precision: str = "fp64", shard=None):
+        """shard=(rank, world) keeps event block `rank` of `world` of every
+        sample (multi-GPU event sharding; see getShardSums)."""
         self._h = None
         self._lib = _lib.load()
         if device is None:
@@ -137,7 +139,10 @@ class analysis:
         self._fit_mode = 1
         status = ctypes.c_int(0)
         err = ctypes.create_string_buffer(4096)
-        h = self._lib.ctpwa_create(str(config_file).encode(), self._device, ctypes.byref(status), err, 4096)
+        rank, world = (0, 1) if shard is None else (int(shard[0]), int(shard[1]))
+        self._shard = (rank, world)
+        h = self._lib.ctpwa_create_shard(str(config_file).encode(), self._device, rank, world, ctypes.byref(status),
+                                         err, 4096)
         if not h:
             msg = err.value.decode("utf-8", "replace")
             if status.value == -1 and msg.startswith("analysis not initialized"):
@@ -297,6 +302,31 @@ class analysis:
         if rc != 0:
             raise RuntimeError(_lib.error(self._h))
         return v.value, g
+
+    def getShardSums(self, params: torch.Tensor, precision=None) -> torch.Tensor:
+        """This shard's per-sample sums (float64 CUDA, to be summed over shards
+        with one all-reduce and passed to finalizeShardSums)."""
+        p = self._check_params(params)
+        out = torch.empty(self._lib.ctpwa_sums_size(self._h), dtype=torch.float64, device=p.device)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        prec = self._precision if precision is None else self._parse_precision(precision)
+        if self._lib.ctpwa_shard_sums(self._h, p.data_ptr(), prec, out.data_ptr(), ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return out
+
+    def finalizeShardSums(self, params: torch.Tensor, sums: torch.Tensor):
+        """(nll, grad) of the union of the shards from the summed shard sums."""
+        p = self._check_params(params)
+        if sums.dtype != torch.float64 or not sums.is_cuda or sums.numel() != self._lib.ctpwa_sums_size(self._h):
+            raise RuntimeError("sums must be the float64 CUDA buffer of getShardSums")
+        sums = sums.contiguous()
+        nll = torch.empty((), dtype=torch.float64, device=p.device)
+        grad = torch.empty_like(p)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        if self._lib.ctpwa_finalize_sums(self._h, p.data_ptr(), sums.data_ptr(), nll.data_ptr(), grad.data_ptr(),
+                                         ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return nll, grad
 
     def getIntensity(self, params: torch.Tensor, kind: int = 1) -> torch.Tensor:
         """Per-event intensities (float64 CUDA [n]) of sample kind 0 = phase space, 1 = data, 2 = background."""

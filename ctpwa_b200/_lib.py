@@ -14,7 +14,14 @@ _c_double_p = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "ctpwa_create": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                        ctypes.c_char_p, ctypes.c_size_t]),
+    "ctpwa_create_shard": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_size_t]),
     "ctpwa_destroy": (None, [ctypes.c_void_p]),
+    "ctpwa_sums_size": (ctypes.c_int, [ctypes.c_void_p]),
+    "ctpwa_shard_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+    "ctpwa_finalize_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_n_vector": (ctypes.c_int, [ctypes.c_void_p]),
     "ctpwa_n_free_theta": (ctypes.c_int, [ctypes.c_void_p]),
     "ctpwa_n_params": (ctypes.c_int, [ctypes.c_void_p]),

@@ -49,12 +49,27 @@ extern "C" {
 
 ctpwa_handle* ctpwa_create(const char* config_path, int device, int* status, char* err, size_t errlen)
 {
+    return ctpwa_create_shard(config_path, device, 0, 1, status, err, errlen);
+}
+
+ctpwa_handle* ctpwa_create_shard(const char* config_path, int device, int rank, int world, int* status, char* err,
+                                 size_t errlen)
+{
     auto h = std::make_unique<ctpwa_handle>();
     int code = CTPWA_OK;
     std::string msg;
+    if (world < 1 || rank < 0 || rank >= world) {
+        msg = "shard: need 0 <= rank < world";
+        if (status) *status = CTPWA_ERR_ARG;
+        setErr(nullptr, CTPWA_ERR_ARG, msg);
+        if (err && errlen) copyOut(msg, err, errlen);
+        return nullptr;
+    }
     try {
         ctpwa::EngineOptions opt;
         opt.device = device;
+        opt.shard_rank = rank;
+        opt.shard_world = world;
         h->eng = std::make_unique<ctpwa::Engine>(config_path ? config_path : "config.yml", opt);
         int np = h->eng->nParams();
         if (cudaMalloc(&h->d_params, sizeof(double) * std::max(1, np)) != cudaSuccess ||
@@ -132,6 +147,32 @@ int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll
         h->eng->nllGradStatic(d_params, d_nll, d_grad, precision, (cudaStream_t)stream);
     } catch (const std::length_error& e) {
         return setErr(h, CTPWA_ERR_ARG, e.what());
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_sums_size(const ctpwa_handle* h) { return h ? h->eng->sumsSize() : CTPWA_ERR_ARG; }
+
+int ctpwa_shard_sums(ctpwa_handle* h, const double* d_params, int precision, double* d_sums, void* stream)
+{
+    if (!h || !d_params || !d_sums) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (precision != CTPWA_FP64 && precision != CTPWA_MIXED) return setErr(h, CTPWA_ERR_ARG, "precision must be 0 or 1");
+    try {
+        h->eng->shardSums(d_params, precision, d_sums, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_finalize_sums(ctpwa_handle* h, const double* d_params, const double* d_sums, double* d_nll, double* d_grad,
+                        void* stream)
+{
+    if (!h || !d_params || !d_sums || !d_nll || !d_grad) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    try {
+        h->eng->finalizeSums(d_params, d_sums, d_nll, d_grad, (cudaStream_t)stream);
     } catch (const std::exception& e) {
         return setErr(h, CTPWA_ERR_CUDA, e.what());
     }

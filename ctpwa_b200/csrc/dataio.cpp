@@ -134,4 +134,23 @@ std::vector<double> readWeights(const std::vector<std::string>& fi, long n_event
     return w;
 }
 
+void shardSample(Sample& s, std::vector<double>& weights, int rank, int world)
+{
+    if (world < 1 || rank < 0 || rank >= world) throw std::runtime_error("shard: need 0 <= rank < world");
+    if (world == 1) return;
+    const long lo = (long)((__int128)s.n * rank / world), hi = (long)((__int128)s.n * (rank + 1) / world);
+    const size_t stride = (size_t)s.n_final * 4;
+    std::vector<double> p(s.p4.begin() + (size_t)lo * stride, s.p4.begin() + (size_t)hi * stride);
+    s.p4.swap(p);
+    if (!weights.empty()) {
+        std::vector<double> w(weights.begin() + lo, weights.begin() + hi);
+        weights.swap(w);
+    }
+    if (!s.weights.empty()) {
+        std::vector<double> w(s.weights.begin() + lo, s.weights.begin() + hi);
+        s.weights.swap(w);
+    }
+    s.n = hi - lo;
+}
+
 }  // namespace ctpwa

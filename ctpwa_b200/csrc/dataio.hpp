@@ -27,4 +27,10 @@ Sample readSample(const std::vector<std::string>& fileinfo, int n_final);
 // Weights for an existing sample: {"0.8"} (constant) or {"dat", path}.
 std::vector<double> readWeights(const std::vector<std::string>& fileinfo, long n_events);
 
+// Keep shard `rank` of `world` contiguous event blocks of a sample (and of
+// its per-event weights, when given): events [n*rank/world, n*(rank+1)/world).
+// Event-sharded evaluation over several devices (src/Analysis.cu:4210-4238
+// splits its samples the same way).
+void shardSample(Sample& s, std::vector<double>& weights, int rank, int world);
+
 }  // namespace ctpwa

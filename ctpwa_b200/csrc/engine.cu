@@ -493,7 +493,34 @@ struct FinalizeArgs {
     double* out_nll;
     double* out_grad;
     double* out_parts;
+    // event-sharded mode: summed per-sample sums [3][nacc] + [n_phsp, W_phsp,
+    // W_data, W_bkg] replace the partial rows and the sample totals; the
+    // phase-space coupling-gradient sums are then divided by W_phsp here
+    const double* sums;
 };
+
+// Per-sample sums of the partial rows plus the sample totals (event-sharded
+// evaluation); same fixed-order reduction as ct_finalize_kernel.
+__global__ void __launch_bounds__(1024) ct_rowsum_kernel(const double* __restrict__ partials, int nacc, FinalizeArgs A,
+                                                         double W_phsp, double* __restrict__ out)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int i = warp; i < 3 * nacc; i += nwarp) {
+        int k = i / nacc, j = i % nacc;
+        double s = 0.0;
+        if (A.has[k])
+            for (int b = lane; b < A.cta[k][1]; b += 32) s += partials[(long long)(A.cta[k][0] + b) * nacc + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) out[i] = s;
+    }
+    if (threadIdx.x == 0) {
+        out[3 * nacc + 0] = A.n_phsp;
+        out[3 * nacc + 1] = W_phsp;
+        out[3 * nacc + 2] = A.W_data;
+        out[3 * nacc + 3] = A.W_bkg;
+    }
+}
 
 // One CTA: deterministic column sums of the CTA partials, then loss/gradient
 // assembly (src/Analysis.cu:1134-1183) and the coupling-gradient transform
@@ -505,23 +532,33 @@ __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
     // one warp per (sample, column): lanes stride over the CTA rows, then a
     // fixed-order shuffle tree, so the sums are bit-reproducible
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int i = warp; i < 3 * A.nacc; i += nwarp) {
-        int k = i / A.nacc, j = i % A.nacc;
-        double s = 0.0;
-        if (A.has[k])
-            for (int b = lane; b < A.cta[k][1]; b += 32) s += A.partials[(long long)(A.cta[k][0] + b) * A.nacc + j];
+    double n_phsp = A.n_phsp, W_data = A.W_data, W_bkg = A.W_bkg, gv_phsp_scale = 1.0;
+    if (A.sums) {
+        for (int i = threadIdx.x; i < 3 * A.nacc; i += blockDim.x) sums[i] = A.sums[i];
+        n_phsp = A.sums[3 * A.nacc + 0];
+        const double Wp = A.sums[3 * A.nacc + 1];
+        gv_phsp_scale = 1.0 / (Wp > 0 ? Wp : 1.0);
+        W_data = A.sums[3 * A.nacc + 2];
+        W_bkg = A.sums[3 * A.nacc + 3];
+    } else {
+        for (int i = warp; i < 3 * A.nacc; i += nwarp) {
+            int k = i / A.nacc, j = i % A.nacc;
+            double s = 0.0;
+            if (A.has[k])
+                for (int b = lane; b < A.cta[k][1]; b += 32) s += A.partials[(long long)(A.cta[k][0] + b) * A.nacc + j];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) sums[i] = s;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) sums[i] = s;
+        }
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
     const double* P = sums;               // phase space
     const double* Dd = sums + A.nacc;     // data
     const double* B = sums + 2 * A.nacc;  // background
-    double pf = A.n_phsp > 0 ? P[1] / A.n_phsp : 0.0;
+    double pf = n_phsp > 0 ? P[1] / n_phsp : 0.0;
     if (pf <= 1e-30 || isnan(pf) || isinf(pf)) pf = 1e-30;
-    double Weff = A.W_data - A.W_bkg;
+    double Weff = W_data - W_bkg;
     double loss = Dd[0] - B[0] + Weff * log(pf);
     const double* theta = A.params + 2 * A.nc;
     for (int g = 0; g < A.ngauss; ++g) {
@@ -532,8 +569,8 @@ __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
     if (reset) loss = 1e30;
     double* gv = sums + 3 * A.nacc;
     for (int a = 0; a < A.nA; ++a) {
-        double r = Dd[2 + 2 * a] - B[2 + 2 * a] + (Weff / pf) * P[2 + 2 * a];
-        double i = Dd[3 + 2 * a] - B[3 + 2 * a] + (Weff / pf) * P[3 + 2 * a];
+        double r = Dd[2 + 2 * a] - B[2 + 2 * a] + (Weff / pf) * (P[2 + 2 * a] * gv_phsp_scale);
+        double i = Dd[3 + 2 * a] - B[3 + 2 * a] + (Weff / pf) * (P[3 + 2 * a] * gv_phsp_scale);
         gv[2 * a] = reset ? 0.0 : r;
         gv[2 * a + 1] = reset ? 0.0 : i;
     }
@@ -552,7 +589,7 @@ __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
         A.out_grad[A.nc + c] = -2.0 * (si * pr - sr * pi) / ps;
     }
     for (int j = 0; j < A.nT; ++j) {
-        double g = Dd[2 + 2 * A.nA + j] - B[2 + 2 * A.nA + j] + (Weff / (pf * A.n_phsp)) * P[2 + 2 * A.nA + j];
+        double g = Dd[2 + 2 * A.nA + j] - B[2 + 2 * A.nA + j] + (Weff / (pf * n_phsp)) * P[2 + 2 * A.nA + j];
         A.out_grad[2 * A.nc + j] = reset ? 0.0 : g;
     }
     if (!reset)
@@ -565,9 +602,9 @@ __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
         A.out_parts[0] = Dd[0];
         A.out_parts[1] = B[0];
         A.out_parts[2] = P[1];
-        A.out_parts[3] = A.W_data;
-        A.out_parts[4] = A.W_bkg;
-        A.out_parts[5] = A.n_phsp;
+        A.out_parts[3] = W_data;
+        A.out_parts[4] = W_bkg;
+        A.out_parts[5] = n_phsp;
     }
 }
 
@@ -734,11 +771,12 @@ void Engine::loadSamples()
         }
         Sample s = readSample(it->second, nfin);
         DeviceSample& d = samples_[k];
-        d.n = s.n;
         if (k == 2) has_bkg_ = true;
         std::vector<double> w;
         auto wi = model_.cfg.data_files.find(wkeys[k]);
         if (wi != model_.cfg.data_files.end() && (k != 2 || has_bkg_)) w = readWeights(wi->second, s.n);
+        shardSample(s, w, opt_.shard_rank, opt_.shard_world);
+        d.n = s.n;
         d.wsum = 0.0;
         if (w.empty()) d.wsum = (double)s.n;
         else
@@ -1310,6 +1348,93 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     f.out_nll = d_nll;
     f.out_grad = d_grad;
     f.out_parts = s_parts;
+    size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
+    ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
+    CT_CUDA(cudaGetLastError());
+}
+
+void Engine::shardSums(const double* d_params, int precision, double* d_sums, cudaStream_t stream)
+{
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    const int nacc = 2 + 2 * nA + nT;
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    int ns = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (cta_[k][1] == 0) continue;
+        CtSampleH& sm = a.s[ns++];
+        const DeviceSample& d = samples_[k];
+        sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
+        sm.kin = d.kin;
+        sm.w = d.w;
+        sm.n = d.n;
+        sm.kind = k;
+        sm.cta_begin = cta_[k][0];
+        sm.cta_count = cta_[k][1];
+        sm.vw_scale = 1.0;  // the phase-space weight total is global: applied after the sums are combined
+    }
+    a.nsamp = ns;
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.partials = d_partials_;
+    a.consts = d_consts_;
+    if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
+    void* args[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    if (precision == kMixed) {
+        const int nph = cta_[0][1];
+        if (nph > 0) {
+            a.cta_base = 0;
+            CT_CUDA(cudaLaunchKernel(k_mixed_ph_, dim3(nph), dim3(256), args, 0, stream));
+        }
+        if (grid_ > nph) {
+            a.cta_base = nph;
+            CT_CUDA(cudaLaunchKernel(k_mixed_, dim3(grid_ - nph), dim3(256), args, 0, stream));
+        }
+    } else {
+        a.cta_base = 0;
+        CT_CUDA(cudaLaunchKernel(k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    }
+    FinalizeArgs f;
+    std::memset(&f, 0, sizeof(f));
+    for (int k = 0; k < 3; ++k) {
+        f.cta[k][0] = cta_[k][0];
+        f.cta[k][1] = cta_[k][1];
+        f.has[k] = cta_[k][1] > 0;
+    }
+    f.n_phsp = (double)samples_[0].n;
+    f.W_data = samples_[1].wsum;
+    f.W_bkg = has_bkg_ ? samples_[2].wsum : 0.0;
+    ct_rowsum_kernel<<<1, 1024, 0, stream>>>(d_partials_, nacc, f, samples_[0].wsum, d_sums);
+    CT_CUDA(cudaGetLastError());
+}
+
+void Engine::finalizeSums(const double* d_params, const double* d_sums, double* d_nll, double* d_grad,
+                          cudaStream_t stream)
+{
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    FinalizeArgs f;
+    std::memset(&f, 0, sizeof(f));
+    f.nacc = 2 + 2 * nA + nT;
+    f.nA = nA;
+    f.nc = nc;
+    f.nT = nT;
+    f.params = d_params;
+    f.v = d_v_;
+    f.chain = d_amp_chain_;
+    f.gauss_idx = d_gauss_idx_;
+    f.gauss_ms = d_gauss_ms_;
+    f.ngauss = (int)m.gauss.size();
+    f.out_nll = d_nll;
+    f.out_grad = d_grad;
+    f.out_parts = d_parts_;
+    f.sums = d_sums;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());

@@ -29,6 +29,8 @@ struct EngineOptions {
     int device = 0;
     bool keep_momenta = false;
     bool mixed_tables = true;  // build the FP32 angular table for the mixed path
+    int shard_rank = 0;        // keep event block shard_rank of shard_world of every sample
+    int shard_world = 1;
 };
 
 // Compile (or find in the disk cache) the fused kernel of a config's model
@@ -55,6 +57,12 @@ public:
     // array (kStaticScratchBytes). All handles on a device share the array.
     void nllGradStatic(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
     static constexpr size_t kStaticScratchBytes = size_t(2) << 20;
+    // Event-sharded evaluation: the per-sample sums of this handle's events,
+    // [3][nacc] + [n_phsp, W_phsp, W_data, W_bkg] (sumsSize() doubles), ready
+    // to be summed over shards; then loss and gradient from summed sums.
+    int sumsSize() const { return 3 * (2 + 2 * model_.nAmp() + model_.nTheta()) + 4; }
+    void shardSums(const double* d_params, int precision, double* d_sums, cudaStream_t stream);
+    void finalizeSums(const double* d_params, const double* d_sums, double* d_nll, double* d_grad, cudaStream_t stream);
     // Per-event intensities of sample `kind` at d_params (device output [n]).
     void intensity(const double* d_params, int kind, double* d_out, cudaStream_t stream);
     // Per-sample partial sums of the last evaluation (diagnostics):

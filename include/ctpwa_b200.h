@@ -43,6 +43,12 @@ typedef struct ctpwa_handle ctpwa_handle;
  * with *status set and the message copied to err (if non-NULL). */
 ctpwa_handle* ctpwa_create(const char* config_path, int device, int* status, char* err, size_t errlen);
 
+/* Event-sharded variant of ctpwa_create for multi-GPU evaluation: keeps the
+ * contiguous event block `rank` of `world` of every sample, as the
+ * reference's multi-device split does (src/Analysis.cu:4210-4238). */
+ctpwa_handle* ctpwa_create_shard(const char* config_path, int device, int rank, int world, int* status, char* err,
+                                 size_t errlen);
+
 /* Releases device memory of the handle (the reference never frees; src/Analysis.cu:1284-1290). */
 void ctpwa_destroy(ctpwa_handle* h);
 
@@ -93,6 +99,20 @@ int ctpwa_nll_grad(ctpwa_handle* h, const double* d_params, double* d_nll, doubl
  *    calls. */
 int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision,
                           void* stream);
+
+/* Event-sharded evaluation, the exchange step of the reference's multi-device
+ * NLL (src/Analysis.cu:4210-4238, which gathers per-device partial results
+ * with peer copies). ctpwa_shard_sums writes this shard's per-sample sums
+ * (ctpwa_sums_size doubles: [phase space, data, background] x [sum -w log f,
+ * sum f, coupling-gradient terms (re, im) x nA, theta-gradient terms x nT],
+ * then [n_phsp, W_phsp, W_data, W_bkg]); the caller sums these buffers over
+ * the shards (one all-reduce) and ctpwa_finalize_sums turns the total into
+ * the NLL and gradient of the union of the shards. Device pointers,
+ * stream-ordered, no host synchronisation. */
+int ctpwa_sums_size(const ctpwa_handle* h);
+int ctpwa_shard_sums(ctpwa_handle* h, const double* d_params, int precision, double* d_sums, void* stream);
+int ctpwa_finalize_sums(ctpwa_handle* h, const double* d_params, const double* d_sums, double* d_nll, double* d_grad,
+                        void* stream);
 
 /* Same evaluation from host buffers: copies params host->device, evaluates,
  * copies NLL and gradient back, and synchronises the stream. */

@@ -23,6 +23,10 @@ def oracle_lib():
         lib = ctypes.CDLL(ORACLE_SO)
         lib.orc_open.restype = ctypes.c_void_p
         lib.orc_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+        lib.orc_open_shard.restype = ctypes.c_void_p
+        lib.orc_open_shard.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        lib.orc_shard_sums.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int]
+        lib.orc_finalize_sums.argtypes = [ctypes.c_void_p, _D, _D, _D, _D]
         lib.orc_close.argtypes = [ctypes.c_void_p]
         lib.orc_sizes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
         lib.orc_theta_init.argtypes = [ctypes.c_void_p, _D]
@@ -72,10 +76,11 @@ def ptr(a):
 class Oracle:
     """FP64 CPU oracle of one config (test infrastructure)."""
 
-    def __init__(self, config_path):
+    def __init__(self, config_path, shard=None):
         self.lib = oracle_lib()
         err = ctypes.create_string_buffer(1024)
-        self.h = self.lib.orc_open(str(config_path).encode(), err, 1024)
+        rank, world = (0, 1) if shard is None else shard
+        self.h = self.lib.orc_open_shard(str(config_path).encode(), int(rank), int(world), err, 1024)
         if not self.h:
             raise RuntimeError("oracle: " + err.value.decode())
         sz = (ctypes.c_long * 8)()
@@ -100,6 +105,24 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(self.lib.orc_error(self.h).decode())
         return v.value, g, parts
+
+    def shard_sums(self, params, nthreads=0):
+        """Per-sample sums of this oracle's events (layout of the engine's shard sums)."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        out = np.zeros(3 * (2 + 2 * self.nA + self.nT) + 4)
+        if self.lib.orc_shard_sums(self.h, ptr(p), ptr(out), nthreads) != 0:
+            raise RuntimeError(self.lib.orc_error(self.h).decode())
+        return out
+
+    def finalize_sums(self, params, sums):
+        """(nll, grad) from summed shard sums."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        s = np.ascontiguousarray(sums, dtype=np.float64)
+        g = np.zeros_like(p)
+        v = ctypes.c_double()
+        if self.lib.orc_finalize_sums(self.h, ptr(p), ptr(s), ctypes.byref(v), ptr(g)) != 0:
+            raise RuntimeError(self.lib.orc_error(self.h).decode())
+        return v.value, g
 
     def theta_init(self):
         """[3, nT]: initial value, lower and upper bound of every free resonance parameter."""

@@ -495,7 +495,13 @@ int fail(char* err, int len, const std::string& msg)
 
 extern "C" {
 
-void* orc_open(const char* config_path, char* err, int errlen)
+void* orc_open_shard(const char* config_path, int rank, int world, char* err, int errlen);
+
+void* orc_open(const char* config_path, char* err, int errlen) { return orc_open_shard(config_path, 0, 1, err, errlen); }
+
+// Oracle over event block `rank` of `world` of every sample (the same blocks
+// as the engine's shards).
+void* orc_open_shard(const char* config_path, int rank, int world, char* err, int errlen)
 {
     try {
         auto o = std::make_unique<Oracle>();
@@ -520,6 +526,10 @@ void* orc_open(const char* config_path, char* err, int errlen)
         wt("phsp_weights", 0);
         wt("data_weights", 1);
         if (o->has_bkg) wt("bkg_weights", 2);
+        for (int k = 0; k < 3; ++k) {
+            std::vector<double> none;
+            ctpwa::shardSample(o->smp[k].s, none, rank, world);
+        }
         for (int k = 0; k < 3; ++k) {
             auto& S = o->smp[k];
             S.slamp.resize(m.groups.size());
@@ -633,73 +643,170 @@ int orc_columns(void* h, int k, const double* theta, double* out)
 
 // NLL and gradient in the reference parameter layout [Re p, Im p, theta].
 // parts (optional, 6 doubles): data_nll, bkg_nll, phsp_factor, W_data, W_bkg, n_phsp
+namespace {
+
+std::vector<cplx> couplings(const Model& m, const double* params)
+{
+    int nA = m.nAmp(), nc = m.nVector();
+    std::vector<cplx> v(nA);
+    for (int a = 0; a < nA; ++a) {
+        int c = m.coupling.amp_chain[a];
+        v[a] = m.coupling.ratio[a] * cplx(params[c], params[nc + c]);
+    }
+    return v;
+}
+
+// Loss and gradient from the three samples' sums (src/Analysis.cu:1134-1183)
+// and the coupling transform (src/AmpGen.cu:3581-3637). ap.gv is already
+// divided by the phase-space weight total.
+void assemble(const Model& m, const double* params, const std::vector<cplx>& v, const Accum& ap, const Accum& ad,
+              const Accum& ab, double Np, double W_data, double W_bkg, double* nll, double* grad, double* parts)
+{
+    int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    const double* theta = params + 2 * nc;
+    double pf = Np > 0 ? ap.fsum / Np : 0.0;
+    if (pf <= 1e-30 || std::isnan(pf) || std::isinf(pf)) pf = 1e-30;
+    double Weff = W_data - W_bkg;
+    double loss = ad.nll - ab.nll + Weff * std::log(pf);
+    for (const auto& g : m.gauss) {
+        double dlt = theta[g.first] - g.second.first;
+        loss += dlt * dlt / (2.0 * g.second.second * g.second.second);
+    }
+    std::vector<cplx> gv(nA);
+    std::vector<double> gt(nT);
+    bool reset = std::isnan(loss) || std::isinf(loss);
+    if (reset) loss = 1e30;
+    for (int a = 0; a < nA; ++a) gv[a] = reset ? 0.0 : ad.gv[a] - ab.gv[a] + (Weff / pf) * ap.gv[a];
+    for (int j = 0; j < nT; ++j) gt[j] = reset ? 0.0 : ad.gt[j] - ab.gt[j] + (Weff / (pf * Np)) * ap.gt[j];
+    if (!reset)
+        for (const auto& g : m.gauss)
+            gt[g.first] += (theta[g.first] - g.second.first) / (g.second.second * g.second.second);
+    // coupling transform (src/AmpGen.cu:3581-3637): dL = (1/p) sum conj(g_a) v_a
+    for (int c = 0; c < nc; ++c) {
+        cplx sum = 0.0;
+        for (int a = 0; a < nA; ++a)
+            if (m.coupling.amp_chain[a] == c) sum += std::conj(gv[a]) * v[a];
+        double pr = params[c], pi = params[nc + c];
+        double ps = pr * pr + pi * pi;
+        if (ps < 1e-30) ps = 1e-30;
+        double dr = (sum.real() * pr + sum.imag() * pi) / ps;
+        double di = (sum.imag() * pr - sum.real() * pi) / ps;
+        grad[c] = 2.0 * dr;
+        grad[nc + c] = -2.0 * di;
+    }
+    for (int j = 0; j < nT; ++j) grad[2 * nc + j] = gt[j];
+    *nll = loss;
+    if (parts) {
+        parts[0] = ad.nll;
+        parts[1] = ab.nll;
+        parts[2] = pf;
+        parts[3] = W_data;
+        parts[4] = W_bkg;
+        parts[5] = Np;
+    }
+}
+
+double phspWeight(const Oracle& o)
+{
+    const auto& ph = o.smp[0].s;
+    double Wp = 0;
+    if (ph.weights.empty()) Wp = (double)ph.n;
+    else
+        for (double w : ph.weights) Wp += w;
+    return Wp;
+}
+
+void evalAll(Oracle& o, const std::vector<cplx>& v, const double* theta, double Wp, Accum& ap, Accum& ad, Accum& ab,
+             int nthreads)
+{
+    int nA = o.m.nAmp(), nT = o.m.nTheta();
+    evalSample(o, 0, v, theta, Wp, ap, nthreads);
+    evalSample(o, 1, v, theta, Wp, ad, nthreads);
+    if (o.has_bkg) evalSample(o, 2, v, theta, Wp, ab, nthreads);
+    else {
+        ab.gv.assign(nA, 0.0);
+        ab.gt.assign(nT, 0.0);
+    }
+}
+
+}  // namespace
+
 int orc_nll_grad(void* h, const double* params, double* nll, double* grad, double* parts, int nthreads)
 {
     auto* o = static_cast<Oracle*>(h);
     try {
         const Model& m = o->m;
-        int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
-        std::vector<cplx> v(nA);
-        for (int a = 0; a < nA; ++a) {
-            int c = m.coupling.amp_chain[a];
-            v[a] = m.coupling.ratio[a] * cplx(params[c], params[nc + c]);
-        }
-        const double* theta = params + 2 * nc;
-        double Wp = 0;
-        const auto& ph = o->smp[0].s;
-        if (ph.weights.empty()) Wp = (double)ph.n;
-        else
-            for (double w : ph.weights) Wp += w;
+        std::vector<cplx> v = couplings(m, params);
+        double Wp = phspWeight(*o);
         if (Wp <= 0) Wp = 1.0;
         Accum ap, ad, ab;
-        evalSample(*o, 0, v, theta, Wp, ap, nthreads);
-        evalSample(*o, 1, v, theta, Wp, ad, nthreads);
-        if (o->has_bkg) evalSample(*o, 2, v, theta, Wp, ab, nthreads);
-        else {
-            ab.gv.assign(nA, 0.0);
-            ab.gt.assign(nT, 0.0);
+        evalAll(*o, v, params + 2 * m.nVector(), Wp, ap, ad, ab, nthreads);
+        assemble(m, params, v, ap, ad, ab, (double)o->smp[0].s.n, o->W_data, o->W_bkg, nll, grad, parts);
+        return 0;
+    } catch (const std::exception& e) {
+        o->err = e.what();
+        return -1;
+    }
+}
+
+// Partial sums of this oracle's samples (one shard of an event-sharded
+// evaluation), in the device layout: per sample (phase space, data,
+// background) [nll, fsum, gv (re, im) x nA, gt x nT], the phase-space gv not
+// yet divided by the phase-space weight total; then [n_phsp, W_phsp, W_data,
+// W_bkg]. Summing these over shards and calling orc_finalize_sums gives the
+// evaluation of the union of the shards.
+int orc_shard_sums(void* h, const double* params, double* out, int nthreads)
+{
+    auto* o = static_cast<Oracle*>(h);
+    try {
+        const Model& m = o->m;
+        int nA = m.nAmp(), nT = m.nTheta(), nacc = 2 + 2 * nA + nT;
+        std::vector<cplx> v = couplings(m, params);
+        Accum acc[3];
+        evalAll(*o, v, params + 2 * m.nVector(), 1.0, acc[0], acc[1], acc[2], nthreads);
+        for (int k = 0; k < 3; ++k) {
+            double* r = out + k * nacc;
+            r[0] = acc[k].nll;
+            r[1] = acc[k].fsum;
+            for (int a = 0; a < nA; ++a) {
+                r[2 + 2 * a] = acc[k].gv[a].real();
+                r[3 + 2 * a] = acc[k].gv[a].imag();
+            }
+            for (int j = 0; j < nT; ++j) r[2 + 2 * nA + j] = acc[k].gt[j];
         }
-        double Np = (double)ph.n;
-        double pf = Np > 0 ? ap.fsum / Np : 0.0;
-        if (pf <= 1e-30 || std::isnan(pf) || std::isinf(pf)) pf = 1e-30;
-        double Weff = o->W_data - o->W_bkg;
-        double loss = ad.nll - ab.nll + Weff * std::log(pf);
-        for (const auto& g : m.gauss) {
-            double dlt = theta[g.first] - g.second.first;
-            loss += dlt * dlt / (2.0 * g.second.second * g.second.second);
+        out[3 * nacc + 0] = (double)o->smp[0].s.n;
+        out[3 * nacc + 1] = phspWeight(*o);
+        out[3 * nacc + 2] = o->W_data;
+        out[3 * nacc + 3] = o->W_bkg;
+        return 0;
+    } catch (const std::exception& e) {
+        o->err = e.what();
+        return -1;
+    }
+}
+
+// Loss and gradient from summed shard sums (layout of orc_shard_sums).
+int orc_finalize_sums(void* h, const double* params, const double* sums, double* nll, double* grad)
+{
+    auto* o = static_cast<Oracle*>(h);
+    try {
+        const Model& m = o->m;
+        int nA = m.nAmp(), nT = m.nTheta(), nacc = 2 + 2 * nA + nT;
+        std::vector<cplx> v = couplings(m, params);
+        Accum acc[3];
+        double Wp = sums[3 * nacc + 1];
+        if (Wp <= 0) Wp = 1.0;
+        for (int k = 0; k < 3; ++k) {
+            const double* r = sums + k * nacc;
+            acc[k].nll = r[0];
+            acc[k].fsum = r[1];
+            acc[k].gv.resize(nA);
+            acc[k].gt.resize(nT);
+            for (int a = 0; a < nA; ++a) acc[k].gv[a] = cplx(r[2 + 2 * a], r[3 + 2 * a]) / (k == 0 ? Wp : 1.0);
+            for (int j = 0; j < nT; ++j) acc[k].gt[j] = r[2 + 2 * nA + j];
         }
-        std::vector<cplx> gv(nA);
-        std::vector<double> gt(nT);
-        bool reset = std::isnan(loss) || std::isinf(loss);
-        if (reset) loss = 1e30;
-        for (int a = 0; a < nA; ++a) gv[a] = reset ? 0.0 : ad.gv[a] - ab.gv[a] + (Weff / pf) * ap.gv[a];
-        for (int j = 0; j < nT; ++j) gt[j] = reset ? 0.0 : ad.gt[j] - ab.gt[j] + (Weff / (pf * Np)) * ap.gt[j];
-        if (!reset)
-            for (const auto& g : m.gauss)
-                gt[g.first] += (theta[g.first] - g.second.first) / (g.second.second * g.second.second);
-        // coupling transform (src/AmpGen.cu:3581-3637): dL = (1/p) sum conj(g_a) v_a
-        for (int c = 0; c < nc; ++c) {
-            cplx sum = 0.0;
-            for (int a = 0; a < nA; ++a)
-                if (m.coupling.amp_chain[a] == c) sum += std::conj(gv[a]) * v[a];
-            double pr = params[c], pi = params[nc + c];
-            double ps = pr * pr + pi * pi;
-            if (ps < 1e-30) ps = 1e-30;
-            double dr = (sum.real() * pr + sum.imag() * pi) / ps;
-            double di = (sum.imag() * pr - sum.real() * pi) / ps;
-            grad[c] = 2.0 * dr;
-            grad[nc + c] = -2.0 * di;
-        }
-        for (int j = 0; j < nT; ++j) grad[2 * nc + j] = gt[j];
-        *nll = loss;
-        if (parts) {
-            parts[0] = ad.nll;
-            parts[1] = ab.nll;
-            parts[2] = pf;
-            parts[3] = o->W_data;
-            parts[4] = o->W_bkg;
-            parts[5] = Np;
-        }
+        assemble(m, params, v, acc[0], acc[1], acc[2], sums[3 * nacc + 0], sums[3 * nacc + 2], sums[3 * nacc + 3], nll,
+                 grad, nullptr);
         return 0;
     } catch (const std::exception& e) {
         o->err = e.what();

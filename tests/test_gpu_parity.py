@@ -124,3 +124,29 @@ def test_mixed_unbiased_at_scale(tmp_path, name):
     nmx, gmx = ana.getNLLAndGrad(pt, "mixed")
     assert abs(float(n64) - float(nmx)) < 5e-4, (float(n64), float(nmx))
     assert float((g64 - gmx).abs().max()) <= 1e-4 * float(g64.abs().max())
+
+
+def test_shard_sums_match_oracle_and_unsharded(tmp_path):
+    """Device shard sums (multi-GPU exchange buffer) against the oracle's, and
+    two shards combined against the unsharded evaluation."""
+    import torch
+    import ctpwa_b200
+
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=30_001, n_data=6_003, n_bkg=1_001, accept_reject=False, seed=12)
+    full = ctpwa_b200.analysis(cfg)
+    p = workloads.true_params(full.getNVector(), full.getFreeResParams()[0].numpy())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    shards = [ctpwa_b200.analysis(cfg, shard=(r, 2)) for r in range(2)]
+    dev = [a.getShardSums(pt, "fp64") for a in shards]
+    for r, s in enumerate(dev):
+        os_ = Oracle(cfg, shard=(r, 2)).shard_sums(p)
+        s = s.cpu().numpy()
+        assert np.max(np.abs(s - os_)) <= 1e-10 * np.max(np.abs(os_)), r
+    tot = dev[0] + dev[1]
+    for prec in ("fp64", "mixed"):
+        tot = shards[0].getShardSums(pt, prec) + shards[1].getShardSums(pt, prec)
+        nll, g = shards[0].finalizeShardSums(pt, tot)
+        n_ref, g_ref = full.getNLLAndGrad(pt, prec)
+        tol = 1e-10 if prec == "fp64" else 1e-6
+        assert abs(float(nll) - float(n_ref)) <= tol * max(1.0, abs(float(n_ref))), (prec, float(nll), float(n_ref))
+        assert float((g - g_ref).abs().max()) <= tol * 10 * float(g_ref.abs().max()), prec

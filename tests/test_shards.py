@@ -1,0 +1,83 @@
+"""Event-sharded evaluation (multi-GPU decomposition), checked on the CPU.
+
+Two gloo ranks each take one event block of the same workload, compute their
+per-sample sums with the CPU oracle, all-reduce them and finalize; the result
+must equal the unsharded evaluation. The GPU engine's shard sums use the same
+layout (tests/test_gpu_parity.py checks them against these)."""
+import os
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from ctpwa_b200 import workloads
+from oracle.binding import Oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _rank(rank, world, cfg, p, port, q):
+    import sys
+
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, ROOT)
+    from oracle.binding import Oracle as Orc
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        o = Orc(cfg, shard=(rank, world))
+        sums = torch.from_numpy(o.shard_sums(p, nthreads=2))
+        dist.all_reduce(sums)
+        nll, g = o.finalize_sums(p, sums.numpy())
+        q.put((rank, nll, g, o.nev))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.fixture(scope="module")
+def workload(tmp_path_factory):
+    d = tmp_path_factory.mktemp("shards")
+    cfg = workloads.make("kkpi", d, n_phsp=6_001, n_data=1_503, n_bkg=301, bkg_weight=0.3, accept_reject=False,
+                         seed=9, gpu_generator=False)
+    o = Oracle(cfg)
+    p = workloads.true_params(o.nV, o.theta_init()[0])
+    p[2 * o.nV:] *= 1.003
+    return cfg, p, o
+
+
+def test_shard_blocks_partition_the_samples(workload):
+    cfg, p, full = workload
+    counts = np.array([Oracle(cfg, shard=(r, 3)).nev for r in range(3)])
+    assert tuple(counts.sum(axis=0)) == full.nev
+
+
+def test_single_process_sum_of_shards_equals_full(workload):
+    cfg, p, full = workload
+    sums = sum(Oracle(cfg, shard=(r, 3)).shard_sums(p) for r in range(3))
+    nll, g = full.finalize_sums(p, sums)
+    onll, og, _ = full.nll_grad(p)
+    assert abs(nll - onll) <= 1e-10 * abs(onll)
+    assert np.max(np.abs(g - og)) <= 1e-9 * np.max(np.abs(og))
+
+
+def test_two_gloo_ranks_equal_unsharded(workload):
+    cfg, p, full = workload
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + (os.getpid() % 1000)
+    procs = [ctx.Process(target=_rank, args=(r, 2, cfg, p, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    onll, og, _ = full.nll_grad(p)
+    for rank, nll, g, nev in res:
+        assert abs(nll - onll) <= 1e-10 * abs(onll), (rank, nll, onll)
+        assert np.max(np.abs(g - og)) <= 1e-9 * np.max(np.abs(og))
+    assert sum(np.array(r[3]) for r in res).tolist() == list(full.nev)
