@@ -11,7 +11,7 @@ perturbed every step, so every lineshape is recomputed.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 One JSON line on rank 0. `value` is the mixed-precision path (FP32 angular
-tables and coherent sum, FP64 lineshapes, logs and accumulations) with the
+tables, lineshapes and coherent sum; FP64 logs and accumulations) with the
 events resident in HBM; the FP64 path is timed beside it; `e2e` goes through
 the host-buffer C-ABI entry point. Multi-GPU: each rank holds its own shard of
 the same size (weak scaling); the per-step exchange is one NCCL all-reduce of
@@ -425,7 +425,7 @@ def run_gpu(args, rank, world, local_rank):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32+f64 (mixed: FP32 angular tables and coherent sum; FP64 lineshapes, log and sums)",
+        "dtype": "f32+f64 (mixed: FP32 angular tables, lineshapes and coherent sum; FP64 m0^2-m^2, log and sums)",
         "data": "synthetic (seeded phase space, accept-reject data, uniform background), events resident in HBM",
         "config": {"workload": WORKLOAD_TEXT, "events_per_rank": {"phsp": n_events[0], "data": n_events[1],
                                                                   "bkg": n_events[2]},
@@ -442,13 +442,12 @@ def run_gpu(args, rank, world, local_rank):
         "accuracy": {"abs_dnll_mixed_vs_fp64": dnll, "grad_rel_err_mixed_vs_fp64": grel},
         "clocks": clocks,
         "e2e": e2e,
-        # per mixed step: prepare, prologue, phase-space pass, data/background pass, finalize
+        # per step: prepare, prologue, fused pass, finalize
         # (multi-GPU: + per-sample row sums and a second prepare before the finalize)
-        "gpu_launches": (3 + (2 if n_events[0] > 0 and n_events[1] + n_events[2] > 0 else 1) + (2 if world > 1 else 0))
-                        * K,
+        "gpu_launches": (4 + (2 if world > 1 else 0)) * K,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "fused pass: ct_fused_mixed_ph + ct_fused_mixed",
+                     "kernel": "ct_fused_mixed",
                      "kernel_ms": kms, "algorithmic_bytes_per_launch": alg, "algorithmic_bytes_per_event": per_evt,
                      "streamed_bytes_per_launch": streamed_bytes(layout, n_events, "mixed")},
     }

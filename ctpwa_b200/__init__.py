@@ -375,23 +375,12 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return out
 
-    def getHessian(self, params: torch.Tensor) -> torch.Tensor:
-        """Hessian [(2nV+nT), (2nV+nT)] (float64, CUDA), grouped [Re p, Im p, theta]."""
+    def getHessian(self, params: torch.Tensor, rel_step: float = 1e-5) -> torch.Tensor:
+        """Hessian [(2nV+nT), (2nV+nT)] (float64, CUDA), grouped [Re p, Im p, theta]:
+        central differences of the exact FP64 device gradient, formed on the device."""
         p = self._check_params(params)
-        return _hessian_fd(self, p)
-
-
-def _hessian_fd(ana: "analysis", p: torch.Tensor) -> torch.Tensor:
-    """Central differences of the exact device gradient (symmetrised)."""
-    n = p.numel()
-    H = torch.empty((n, n), dtype=torch.float64, device=p.device)
-    scale = torch.clamp(p.abs(), min=1e-2)
-    h = 1e-5 * scale
-    for i in range(n):
-        q = p.clone()
-        q[i] += h[i]
-        _, gp = ana._eval(q, 0)
-        q[i] -= 2 * h[i]
-        _, gm = ana._eval(q, 0)
-        H[i] = (gp - gm) / (2 * h[i])
-    return 0.5 * (H + H.T)
+        H = torch.empty((self._np, self._np), dtype=torch.float64, device=p.device)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        if self._lib.ctpwa_hessian(self._h, p.data_ptr(), H.data_ptr(), float(rel_step), ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return H

@@ -17,6 +17,8 @@ SIGNATURES = {
     "ctpwa_create_shard": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_size_t]),
     "ctpwa_destroy": (None, [ctypes.c_void_p]),
+    "ctpwa_hessian": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                     ctypes.c_void_p]),
     "ctpwa_sums_size": (ctypes.c_int, [ctypes.c_void_p]),
     "ctpwa_shard_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                         ctypes.c_void_p]),

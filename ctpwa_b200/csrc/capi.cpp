@@ -153,6 +153,18 @@ int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll
     return CTPWA_OK;
 }
 
+int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, double rel_step, void* stream)
+{
+    if (!h || !d_params || !d_hess) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (!(rel_step > 0.0) || rel_step > 1e-2) return setErr(h, CTPWA_ERR_ARG, "rel_step must be in (0, 1e-2]");
+    try {
+        h->eng->hessian(d_params, d_hess, rel_step, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_sums_size(const ctpwa_handle* h) { return h ? h->eng->sumsSize() : CTPWA_ERR_ARG; }
 
 int ctpwa_shard_sums(ctpwa_handle* h, const double* d_params, int precision, double* d_sums, void* stream)

@@ -680,6 +680,9 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     CT_CUDA(cudaGetDeviceCount(&ndev));
     if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
     CT_CUDA(cudaSetDevice(opt_.device));
+    // initialisation work goes to a private non-blocking stream, so a handle
+    // being created does not serialise with other handles' evaluations
+    CT_CUDA(cudaStreamCreateWithFlags(&init_stream_, cudaStreamNonBlocking));
     compileKernel();
     loadSamples();
     buildTables();
@@ -692,8 +695,8 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     std::vector<double> ratio = model_.coupling.ratio;
     CT_CUDA(cudaMalloc(&d_amp_chain_, sizeof(int) * nA));
     CT_CUDA(cudaMalloc(&d_ratio_, sizeof(double) * nA));
-    CT_CUDA(cudaMemcpy(d_amp_chain_, model_.coupling.amp_chain.data(), sizeof(int) * nA, cudaMemcpyHostToDevice));
-    CT_CUDA(cudaMemcpy(d_ratio_, ratio.data(), sizeof(double) * nA, cudaMemcpyHostToDevice));
+    CT_CUDA(cudaMemcpyAsync(d_amp_chain_, model_.coupling.amp_chain.data(), sizeof(int) * nA, cudaMemcpyHostToDevice, init_stream_));
+    CT_CUDA(cudaMemcpyAsync(d_ratio_, ratio.data(), sizeof(double) * nA, cudaMemcpyHostToDevice, init_stream_));
     int ng = (int)model_.gauss.size();
     CT_CUDA(cudaMalloc(&d_gauss_idx_, sizeof(int) * std::max(1, ng)));
     CT_CUDA(cudaMalloc(&d_gauss_ms_, sizeof(double) * 2 * std::max(1, ng)));
@@ -705,8 +708,8 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
             gm.push_back(g.second.first);
             gm.push_back(g.second.second);
         }
-        CT_CUDA(cudaMemcpy(d_gauss_idx_, gi.data(), sizeof(int) * ng, cudaMemcpyHostToDevice));
-        CT_CUDA(cudaMemcpy(d_gauss_ms_, gm.data(), sizeof(double) * 2 * ng, cudaMemcpyHostToDevice));
+        CT_CUDA(cudaMemcpyAsync(d_gauss_idx_, gi.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, init_stream_));
+        CT_CUDA(cudaMemcpyAsync(d_gauss_ms_, gm.data(), sizeof(double) * 2 * ng, cudaMemcpyHostToDevice, init_stream_));
     }
     // grid: CTAs per sample proportional to its size, multiple of the SM count
     int sms = 148;
@@ -730,7 +733,10 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     int nacc = 2 + 2 * nA + model_.nTheta();
     CT_CUDA(cudaMalloc(&d_partials_, sizeof(double) * (size_t)grid_ * nacc));
     CT_CUDA(cudaMalloc(&d_parts_, sizeof(double) * 8));
-    CT_CUDA(cudaDeviceSynchronize());
+    CT_CUDA(cudaMalloc(&d_hscratch_, sizeof(double) * (3 * (size_t)std::max(1, model_.nParams()) + 1)));
+    CT_CUDA(cudaStreamSynchronize(init_stream_));
+    cudaStreamDestroy(init_stream_);
+    init_stream_ = nullptr;
 }
 
 Engine::~Engine()
@@ -747,6 +753,7 @@ Engine::~Engine()
     cudaFree(d_consts_);
     cudaFree(d_partials_);
     cudaFree(d_parts_);
+    cudaFree(d_hscratch_);
     cudaFree(d_amp_chain_);
     cudaFree(d_ratio_);
     cudaFree(d_gauss_idx_);
@@ -755,6 +762,7 @@ Engine::~Engine()
         cudaEventDestroy(ev_begin_[i]);
         cudaEventDestroy(ev_end_[i]);
     }
+    if (init_stream_) cudaStreamDestroy(init_stream_);
     if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
 }
 
@@ -784,17 +792,18 @@ void Engine::loadSamples()
         if (s.n == 0) continue;
         size_t bytes = sizeof(double) * (size_t)s.n * nfin * 4;
         double* tmp = nullptr;
-        CT_CUDA(cudaMalloc(&tmp, bytes));
-        CT_CUDA(cudaMemcpy(tmp, s.p4.data(), bytes, cudaMemcpyHostToDevice));
-        CT_CUDA(cudaMalloc(&d.p4, bytes));
-        ag_transpose_kernel<<<(unsigned)((s.n + 255) / 256), 256>>>(tmp, d.p4, s.n, nfin);
+        CT_CUDA(cudaMallocAsync((void**)&tmp, bytes, init_stream_));
+        CT_CUDA(cudaMemcpyAsync(tmp, s.p4.data(), bytes, cudaMemcpyHostToDevice, init_stream_));
+        CT_CUDA(cudaMallocAsync((void**)&d.p4, bytes, init_stream_));
+        ag_transpose_kernel<<<(unsigned)((s.n + 255) / 256), 256, 0, init_stream_>>>(tmp, d.p4, s.n, nfin);
         CT_CUDA(cudaGetLastError());
-        CT_CUDA(cudaDeviceSynchronize());
-        CT_CUDA(cudaFree(tmp));
+        CT_CUDA(cudaFreeAsync(tmp, init_stream_));
         if (!w.empty()) {
             CT_CUDA(cudaMalloc(&d.w, sizeof(double) * s.n));
-            CT_CUDA(cudaMemcpy(d.w, w.data(), sizeof(double) * s.n, cudaMemcpyHostToDevice));
+            CT_CUDA(cudaMemcpyAsync(d.w, w.data(), sizeof(double) * s.n, cudaMemcpyHostToDevice, init_stream_));
         }
+        // the host sample is released at the end of this iteration
+        CT_CUDA(cudaStreamSynchronize(init_stream_));
         device_bytes_ += bytes + (w.empty() ? 0 : sizeof(double) * s.n);
     }
 }
@@ -957,7 +966,8 @@ void Engine::buildTables()
         std::memcpy(img.data() + o_kin[g], gh[g].kin.data(), gh[g].kin.size() * sizeof(int));
     }
     CT_CUDA(cudaMalloc(&d_ag_tables_, off));
-    CT_CUDA(cudaMemcpy(d_ag_tables_, img.data(), off, cudaMemcpyHostToDevice));
+    CT_CUDA(cudaMemcpyAsync(d_ag_tables_, img.data(), off, cudaMemcpyHostToDevice, init_stream_));
+    CT_CUDA(cudaStreamSynchronize(init_stream_));
     char* base = (char*)d_ag_tables_;
     AgTables T;
     T.vars = (const AgNodeVar*)(base + o_vars);
@@ -998,14 +1008,15 @@ void Engine::computeAngular(int kind)
     for (size_t g = 0; g < group_desc_.size(); ++g) {
         AgGroup G;
         std::memcpy(&G, group_desc_[g].data(), sizeof(G));
-        ag_group_kernel<<<(unsigned)((n + 127) / 128), 128>>>(G, T, d.p4, n, d.slamp64, d.slamp32, d.kin);
+        ag_group_kernel<<<(unsigned)((n + 127) / 128), 128, 0, init_stream_>>>(G, T, d.p4, n, d.slamp64, d.slamp32,
+                                                                                 d.kin);
         CT_CUDA(cudaGetLastError());
     }
-    CT_CUDA(cudaDeviceSynchronize());
     if (!opt_.keep_momenta) {
-        CT_CUDA(cudaFree(d.p4));
+        CT_CUDA(cudaFreeAsync(d.p4, init_stream_));
         d.p4 = nullptr;
     }
+    CT_CUDA(cudaStreamSynchronize(init_stream_));
 }
 
 // NVRTC compile of the fused kernel for one generated model, with a disk cache
@@ -1018,11 +1029,11 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     std::string src = "#include \"fused_nll.cuh\"\n";
     std::vector<std::string> optv = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
                                      "--fmad=true", "-lineinfo"};
-    // tuning knob: minimum resident CTAs per SM of the mixed phase-space kernel
-    if (const char* e = std::getenv("CTPWA_PH_MINB")) {
+    // tuning knob: minimum resident CTAs per SM of the mixed-form kernel
+    if (const char* e = std::getenv("CTPWA_MX_MINB")) {
         int v = std::atoi(e);
-        if (v < 1 || v > 8) throw std::runtime_error("CTPWA_PH_MINB must be in [1, 8]");
-        optv.push_back("-DCT_PH_MINB=" + std::to_string(v));
+        if (v < 1 || v > 8) throw std::runtime_error("CTPWA_MX_MINB must be in [1, 8]");
+        optv.push_back("-DCT_MX_MINB=" + std::to_string(v));
     }
     std::vector<const char*> optp;
     for (const auto& o : optv) optp.push_back(o.c_str());
@@ -1084,16 +1095,14 @@ void Engine::compileKernel()
     cudaLibrary_t lib;
     CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
     lib_ = (void*)lib;
-    cudaKernel_t k64, kmx, kmxp, kin, kpro;
+    cudaKernel_t k64, kmx, kin, kpro;
     CT_CUDA(cudaLibraryGetKernel(&kpro, lib, "ct_prologue"));
     k_pro_ = (void*)kpro;
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
-    CT_CUDA(cudaLibraryGetKernel(&kmxp, lib, "ct_fused_mixed_ph"));
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
     k_f64_ = (void*)k64;
     k_mixed_ = (void*)kmx;
-    k_mixed_ph_ = (void*)kmxp;
     k_int_ = (void*)kin;
     jit_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -1166,22 +1175,8 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     const size_t slot = ev_begin_.empty() ? 0 : (size_t)(ev_count_ % (long long)ev_begin_.size());
     if (!ev_begin_.empty()) CT_CUDA(cudaEventRecord(ev_begin_[slot], stream));
-    if (precision == kMixed) {
-        // phase space with FP32 lineshapes, then data and background with FP64
-        // lineshapes; both write their rows of the same partials table
-        const int nph = cta_[0][1];
-        if (nph > 0) {
-            a.cta_base = 0;
-            CT_CUDA(cudaLaunchKernel(k_mixed_ph_, dim3(nph), dim3(256), args, 0, stream));
-        }
-        if (grid_ > nph) {
-            a.cta_base = nph;
-            CT_CUDA(cudaLaunchKernel(k_mixed_, dim3(grid_ - nph), dim3(256), args, 0, stream));
-        }
-    } else {
-        a.cta_base = 0;
-        CT_CUDA(cudaLaunchKernel(k_f64_, dim3(grid_), dim3(256), args, 0, stream));
-    }
+    a.cta_base = 0;
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
     if (!ev_begin_.empty()) {
         CT_CUDA(cudaEventRecord(ev_end_[slot], stream));
         ++ev_count_;
@@ -1310,20 +1305,8 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
-    if (precision == kMixed) {
-        const int nph = cta_[0][1];
-        if (nph > 0) {
-            a.cta_base = 0;
-            CT_CUDA(cudaLaunchKernel(k_mixed_ph_, dim3(nph), dim3(256), args, 0, stream));
-        }
-        if (grid_ > nph) {
-            a.cta_base = nph;
-            CT_CUDA(cudaLaunchKernel(k_mixed_, dim3(grid_ - nph), dim3(256), args, 0, stream));
-        }
-    } else {
-        a.cta_base = 0;
-        CT_CUDA(cudaLaunchKernel(k_f64_, dim3(grid_), dim3(256), args, 0, stream));
-    }
+    a.cta_base = 0;
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     f.partials = s_partials;
@@ -1384,20 +1367,8 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
-    if (precision == kMixed) {
-        const int nph = cta_[0][1];
-        if (nph > 0) {
-            a.cta_base = 0;
-            CT_CUDA(cudaLaunchKernel(k_mixed_ph_, dim3(nph), dim3(256), args, 0, stream));
-        }
-        if (grid_ > nph) {
-            a.cta_base = nph;
-            CT_CUDA(cudaLaunchKernel(k_mixed_, dim3(grid_ - nph), dim3(256), args, 0, stream));
-        }
-    } else {
-        a.cta_base = 0;
-        CT_CUDA(cudaLaunchKernel(k_f64_, dim3(grid_), dim3(256), args, 0, stream));
-    }
+    a.cta_base = 0;
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     for (int k = 0; k < 3; ++k) {
@@ -1437,6 +1408,65 @@ void Engine::finalizeSums(const double* d_params, const double* d_sums, double* 
     f.sums = d_sums;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
+    CT_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+__device__ __forceinline__ double ct_hstep(const double* p, int i, double rel)
+{
+    return rel * fmax(fabs(p[i]), 1e-2);
+}
+
+// out = p with p_i shifted by sign * h_i
+__global__ void ct_perturb_kernel(const double* __restrict__ p, double* __restrict__ out, int n, int i, double sign,
+                                  double rel)
+{
+    for (int k = threadIdx.x; k < n; k += blockDim.x) out[k] = p[k];
+    __syncthreads();
+    if (threadIdx.x == 0) out[i] = p[i] + sign * ct_hstep(p, i, rel);
+}
+
+// row i of the Hessian from the gradients at p + h_i e_i and p - h_i e_i
+__global__ void ct_hess_row_kernel(const double* __restrict__ p, const double* __restrict__ gp,
+                                   const double* __restrict__ gm, int n, int i, double rel, double* __restrict__ H)
+{
+    const double h = ct_hstep(p, i, rel);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) H[(size_t)i * n + k] = (gp[k] - gm[k]) / (2.0 * h);
+}
+
+__global__ void ct_symmetrize_kernel(double* __restrict__ H, int n)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+        int i = idx / n, k = idx % n;
+        if (k <= i) continue;
+        double s = 0.5 * (H[(size_t)i * n + k] + H[(size_t)k * n + i]);
+        H[(size_t)i * n + k] = s;
+        H[(size_t)k * n + i] = s;
+    }
+}
+
+}  // namespace
+
+void Engine::hessian(const double* d_params, double* d_hess, double rel_step, cudaStream_t stream)
+{
+    const int n = model_.nParams();
+    if (!(rel_step > 0.0)) throw std::runtime_error("hessian: step must be positive");
+    double* pp = d_hscratch_;
+    double* gp = d_hscratch_ + n;
+    double* gm = d_hscratch_ + 2 * n;
+    double* nl = d_hscratch_ + 3 * n;
+    for (int i = 0; i < n; ++i) {
+        ct_perturb_kernel<<<1, 256, 0, stream>>>(d_params, pp, n, i, +1.0, rel_step);
+        CT_CUDA(cudaGetLastError());
+        nllGrad(pp, nl, gp, kFP64, stream);
+        ct_perturb_kernel<<<1, 256, 0, stream>>>(d_params, pp, n, i, -1.0, rel_step);
+        CT_CUDA(cudaGetLastError());
+        nllGrad(pp, nl, gm, kFP64, stream);
+        ct_hess_row_kernel<<<1, 256, 0, stream>>>(d_params, gp, gm, n, i, rel_step, d_hess);
+        CT_CUDA(cudaGetLastError());
+    }
+    ct_symmetrize_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, stream>>>(d_hess, n);
     CT_CUDA(cudaGetLastError());
 }
 

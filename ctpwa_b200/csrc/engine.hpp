@@ -63,18 +63,21 @@ public:
     int sumsSize() const { return 3 * (2 + 2 * model_.nAmp() + model_.nTheta()) + 4; }
     void shardSums(const double* d_params, int precision, double* d_sums, cudaStream_t stream);
     void finalizeSums(const double* d_params, const double* d_sums, double* d_nll, double* d_grad, cudaStream_t stream);
+    // Hessian [nP][nP] (row-major, symmetric) of the FP64 NLL at d_params:
+    // central differences of the exact device gradient, step
+    // h_i = rel_step * max(|p_i|, 1e-2), 2 nP gradient evaluations queued on
+    // the stream with no host synchronisation.
+    void hessian(const double* d_params, double* d_hess, double rel_step, cudaStream_t stream);
     // Per-event intensities of sample `kind` at d_params (device output [n]).
     void intensity(const double* d_params, int kind, double* d_out, cudaStream_t stream);
     // Per-sample partial sums of the last evaluation (diagnostics):
     // [data_nll, bkg_nll, phsp_sum, W_data, W_bkg, n_phsp]
     void lastParts(double* out6, cudaStream_t stream);
 
-    // Optional timing of the fused pass (the one fused launch of the plain
-    // path, or the phase-space and data/background launches of the mixed
-    // form): CUDA events recorded on the launching stream around it into a
-    // ring of `slots` pairs (0 switches timing off). kernelTimes synchronises
-    // on the recorded events and returns the durations (ms) of the most
-    // recent passes.
+    // Optional per-launch timing of the fused kernel: CUDA events recorded on
+    // the launching stream around each fused launch into a ring of `slots`
+    // pairs (0 switches timing off). kernelTimes synchronises on the recorded
+    // events and returns the durations (ms) of the most recent launches.
     void setKernelTiming(int slots);
     int kernelTimes(float* ms, int cap);
 
@@ -106,8 +109,7 @@ private:
     // JIT
     void* lib_ = nullptr;  // cudaLibrary_t
     void* k_f64_ = nullptr;
-    void* k_mixed_ = nullptr;     // mixed form, data and background
-    void* k_mixed_ph_ = nullptr;  // mixed form, phase space
+    void* k_mixed_ = nullptr;
     void* k_int_ = nullptr;
     void* k_pro_ = nullptr;
     double jit_seconds_ = 0.0;
@@ -118,12 +120,15 @@ private:
     double* d_consts_ = nullptr;    // [nconst] parameter-only subexpressions
     double* d_partials_ = nullptr;  // [grid][nacc]
     double* d_parts_ = nullptr;     // [8]
+    double* d_hscratch_ = nullptr;  // Hessian: perturbed params, two gradients, nll [3 nP + 1]
     int* d_amp_chain_ = nullptr;
     double* d_ratio_ = nullptr;
     int* d_gauss_idx_ = nullptr;
     double* d_gauss_ms_ = nullptr;  // [mu, sigma] pairs
     int grid_ = 0;
     int cta_[3][2] = {};  // per sample: begin, count
+
+    cudaStream_t init_stream_ = nullptr;  // initialisation only
 
     // fused-kernel timing ring
     std::vector<cudaEvent_t> ev_begin_, ev_end_;

@@ -25,14 +25,13 @@
 // memory and writes one row of partial sums; a separate finalize kernel sums
 // the rows in a fixed order, so results are bit-reproducible.
 //
-// Precision. Plain path (ct_fused_f64): everything FP64. Mixed form: the
-// angular tables and the per-polarisation algebra are FP32 for every sample;
-// data and background (the log-likelihood sample, ct_fused_mixed) keep FP64
-// lineshapes; phase space (the normalisation average, ct_fused_mixed_ph) uses
-// the FP32 lineshapes and FP32 per-thread gradient sums. The log, the
-// log-likelihood and phase-space intensity sums and every cross-thread
-// reduction are FP64 in all forms. Parameter-only parts of the lineshapes
-// are computed once per call by ct_prologue and staged in shared memory.
+// Precision. Plain path (ct_fused_f64): everything FP64. Mixed form
+// (ct_fused_mixed): FP32 angular tables, FP32 lineshapes (cancellation-prone
+// parts FP64, see model_columns_f32), FP32 per-polarisation algebra and
+// per-thread gradient sums. The log, the log-likelihood and phase-space
+// intensity sums and every cross-thread reduction are FP64 in both forms.
+// Parameter-only parts of the lineshapes are computed once per call by
+// ct_prologue and staged in shared memory.
 #pragma once
 
 #include "device_helpers.cuh"
@@ -138,7 +137,7 @@ struct CtLineshape<float> {
 // R: type of the per-polarisation complex algebra and of the stored angular
 //    table (double: plain path; float: mixed form)
 // L: type of the lineshapes, their derivatives and the per-thread gradient
-//    sums (double, or float for the mixed form's phase-space pass)
+//    sums
 // PH_ONLY: the launch serves phase-space events only
 template <typename R, typename L, bool PH_ONLY>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
@@ -297,15 +296,13 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 }
 
 extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_fused_f64(CtArgs a) { ct_fused_body<double, double, false>(a); }
-// mixed form, data and background (FP64 lineshapes)
-extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_fused_mixed(CtArgs a) { ct_fused_body<float, double, false>(a); }
-// mixed form, phase space (FP32 lineshapes)
-#ifndef CT_PH_MINB
-#define CT_PH_MINB 2
+// mixed form (FP32 lineshapes and algebra, FP64 logs and sums), all samples
+#ifndef CT_MX_MINB
+#define CT_MX_MINB 2
 #endif
-extern "C" __global__ void __launch_bounds__(CT_BLOCK, CT_PH_MINB) ct_fused_mixed_ph(CtArgs a)
+extern "C" __global__ void __launch_bounds__(CT_BLOCK, CT_MX_MINB) ct_fused_mixed(CtArgs a)
 {
-    ct_fused_body<float, float, true>(a);
+    ct_fused_body<float, float, false>(a);
 }
 
 // Per-event intensity f_e = sum_p |S_p|^2 of sample s[0] (FP64), for

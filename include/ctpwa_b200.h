@@ -100,6 +100,14 @@ int ctpwa_nll_grad(ctpwa_handle* h, const double* d_params, double* d_nll, doubl
 int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision,
                           void* stream);
 
+/* Replaces: analysis::getHessian — src/Analysis.cu:2689-3378.
+ * d_hess: device [n_params][n_params] row-major, grouped [Re p, Im p, theta]
+ * like the reference. Central differences of the exact FP64 device gradient
+ * with steps h_i = rel_step * max(|p_i|, 1e-2) (rel_step in (0, 1e-2];
+ * 1e-5 is the library default), symmetrised; 2 n_params gradient evaluations
+ * queued on the stream, no host synchronisation, no allocation. */
+int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, double rel_step, void* stream);
+
 /* Event-sharded evaluation, the exchange step of the reference's multi-device
  * NLL (src/Analysis.cu:4210-4238, which gathers per-device partial results
  * with peer copies). ctpwa_shard_sums writes this shard's per-sample sums

@@ -150,3 +150,23 @@ def test_shard_sums_match_oracle_and_unsharded(tmp_path):
         tol = 1e-10 if prec == "fp64" else 1e-6
         assert abs(float(nll) - float(n_ref)) <= tol * max(1.0, abs(float(n_ref))), (prec, float(nll), float(n_ref))
         assert float((g - g_ref).abs().max()) <= tol * 10 * float(g_ref.abs().max()), prec
+
+
+def test_hessian_matches_oracle_fd(setups):
+    """Device Hessian (central differences of the exact device gradient) vs
+    central differences of the oracle's dual-number gradient, same steps."""
+    ana, orc, pt, p = setups["kkpi"]
+    H = ana.getHessian(pt).cpu().numpy()
+    n = p.size
+    Ho = np.zeros((n, n))
+    for i in range(n):
+        h = 1e-5 * max(abs(p[i]), 1e-2)
+        q = p.copy()
+        q[i] += h
+        _, gp, _ = orc.nll_grad(q)
+        q[i] -= 2 * h
+        _, gm, _ = orc.nll_grad(q)
+        Ho[i] = (gp - gm) / (2 * h)
+    Ho = 0.5 * (Ho + Ho.T)
+    assert np.allclose(H, H.T, rtol=0, atol=0)
+    assert np.max(np.abs(H - Ho)) <= 1e-6 * np.max(np.abs(Ho)), np.max(np.abs(H - Ho)) / np.max(np.abs(Ho))
