@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--e2e-steps", type=int, default=None, help="host-buffer steps (default: steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-toy-fit", action="store_true", help="skip the toy-fit serving stream")
+    ap.add_argument("--toy-jobs", type=int, default=12)
+    ap.add_argument("--toy-rate", type=float, default=4.0)
     ap.add_argument("--data-dir", default=os.environ.get("CTPWA_BENCH_DIR", "/tmp/ctpwa_bench"))
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--fraction", type=float, default=1.0,
@@ -298,6 +301,31 @@ def streamed_bytes(layout, n_events, precision):
     return per * (n_p + n_d + n_b) + 8 * n_b
 
 
+def toy_fit(args, device):
+    """Toy-fit serving stream: Poisson arrivals of fit jobs (single-rho and
+    three-chain rho models, N_data log-uniform 10k-200k, 10x phase space),
+    L-BFGS to convergence (<= 100 evaluations) + Hessian each, 4 concurrent
+    slots; latency percentiles per evaluation and per fit, mixed and FP64."""
+    from ctpwa_b200 import serving
+
+    out = {}
+    for prec in ("mixed", "fp64"):
+        srv = serving.Server(device=device, slots=4)
+        try:
+            jobs = serving.poisson_stream(args.toy_rate, args.toy_jobs, nd_range=(10_000, 200_000), precision=prec,
+                                          seed=17 + args.seed)
+            t = time.perf_counter()
+            res = srv.run(jobs)
+            s = serving.summary(res, time.perf_counter() - t)
+        finally:
+            srv.close()
+        out[prec] = {k: s[k] for k in ("jobs", "failed", "fits_per_hour", "evals", "eval_ms_p50", "eval_ms_p99",
+                                        "fit_ms_p50", "fit_ms_p99", "service_ms_p50", "service_ms_p99")}
+    out["config"] = {"rate_per_s": args.toy_rate, "jobs": args.toy_jobs, "slots": 4, "n_data": "log-uniform 10k-200k",
+                     "n_phsp": "10 x n_data", "models": ["pipi_rho", "pipi_3rho"], "cuda_graphs": True}
+    return out
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -451,6 +479,8 @@ def run_gpu(args, rank, world, local_rank):
                      "kernel_ms": kms, "algorithmic_bytes_per_launch": alg, "algorithmic_bytes_per_event": per_evt,
                      "streamed_bytes_per_launch": streamed_bytes(layout, n_events, "mixed")},
     }
+    if world == 1 and not args.no_toy_fit:
+        line["toy_fit"] = toy_fit(args, local_rank)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.data_dir, args.seed)
     print(json.dumps(line), flush=True)
