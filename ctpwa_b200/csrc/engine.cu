@@ -663,6 +663,58 @@ std::string cacheDir()
 
 }  // namespace
 
+// Resident 256-thread CTAs per SM of a fused kernel (occupancy query on the
+// library kernel handle; from its register count if that query is refused).
+int Engine::residentCtas(void* kernel) const
+{
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kernel, 256, 0) == cudaSuccess && nb > 0)
+        return nb;
+    cudaGetLastError();
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, (const void*)kernel) == cudaSuccess && fa.numRegs > 0) {
+        cudaGetLastError();
+        int regs = (fa.numRegs + 7) / 8 * 8;
+        return std::max(1, std::min(8, 65536 / (regs * 256)));
+    }
+    cudaGetLastError();
+    return 1;
+}
+
+// Split `target` CTAs over the samples in proportion to their event counts
+// (at least one CTA per non-empty sample, at most one per 256 events).
+void Engine::layoutCtas(int target, long long tot, CtaLayout& lay) const
+{
+    long long want[3] = {0, 0, 0}, maxc[3] = {0, 0, 0};
+    long long sum = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (samples_[k].n <= 0) continue;
+        maxc[k] = (samples_[k].n + 255) / 256;
+        want[k] = std::max(1LL, std::min(maxc[k], (long long)std::floor((double)target * samples_[k].n / std::max(1LL, tot))));
+        sum += want[k];
+    }
+    // hand the CTAs lost to rounding to the samples with the most events per CTA
+    while (sum < target) {
+        int best = -1;
+        double most = 0.0;
+        for (int k = 0; k < 3; ++k)
+            if (want[k] > 0 && want[k] < maxc[k] && (double)samples_[k].n / want[k] > most) {
+                most = (double)samples_[k].n / want[k];
+                best = k;
+            }
+        if (best < 0) break;
+        ++want[best];
+        ++sum;
+    }
+    int begin = 0;
+    for (int k = 0; k < 3; ++k) {
+        lay.cta[k][0] = begin;
+        lay.cta[k][1] = (int)want[k];
+        begin += (int)want[k];
+    }
+    lay.grid = std::max(1, begin);
+}
+
 Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(opt)
 {
     Config cfg = loadConfig(config_path);
@@ -711,27 +763,23 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
         CT_CUDA(cudaMemcpyAsync(d_gauss_idx_, gi.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, init_stream_));
         CT_CUDA(cudaMemcpyAsync(d_gauss_ms_, gm.data(), sizeof(double) * 2 * ng, cudaMemcpyHostToDevice, init_stream_));
     }
-    // grid: CTAs per sample proportional to its size, multiple of the SM count
+    // grid: one full wave of resident CTAs of the fused kernel of each
+    // precision (SMs x CTAs per SM from the kernel's occupancy), split over
+    // the samples in proportion to their sizes, so every CTA gets about the
+    // same number of events and no partial second wave is left
     int sms = 148;
     CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
     long long tot = 0;
     for (int k = 0; k < 3; ++k) tot += samples_[k].n;
-    int target = sms * 8;
-    int begin = 0;
-    for (int k = 0; k < 3; ++k) {
-        int cnt = 0;
-        if (samples_[k].n > 0) {
-            long long want = (long long)std::ceil((double)target * samples_[k].n / std::max(1LL, tot));
-            long long maxc = (samples_[k].n + 255) / 256;
-            cnt = (int)std::max(1LL, std::min(want, maxc));
-        }
-        cta_[k][0] = begin;
-        cta_[k][1] = cnt;
-        begin += cnt;
+    int maxgrid = 1;
+    for (int pr = 0; pr < 2; ++pr) {
+        int occ = residentCtas(pr == 0 ? k_f64_ : k_mixed_);
+        layoutCtas(sms * occ, tot, lay_[pr]);
+        maxgrid = std::max(maxgrid, lay_[pr].grid);
     }
-    grid_ = std::max(1, begin);
+    grid_max_ = maxgrid;
     int nacc = 2 + 2 * nA + model_.nTheta();
-    CT_CUDA(cudaMalloc(&d_partials_, sizeof(double) * (size_t)grid_ * nacc));
+    CT_CUDA(cudaMalloc(&d_partials_, sizeof(double) * (size_t)grid_max_ * nacc));
     CT_CUDA(cudaMalloc(&d_parts_, sizeof(double) * 8));
     CT_CUDA(cudaMalloc(&d_hscratch_, sizeof(double) * (3 * (size_t)std::max(1, model_.nParams()) + 1)));
     CT_CUDA(cudaStreamSynchronize(init_stream_));
@@ -1145,6 +1193,7 @@ struct CtArgsH {
 
 void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
 {
+    const CtaLayout& lay = lay_[precision == kMixed ? 1 : 0];
     const Model& m = model_;
     int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
     ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
@@ -1153,7 +1202,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     std::memset(&a, 0, sizeof(a));
     int ns = 0;
     for (int k = 0; k < 3; ++k) {
-        if (cta_[k][1] == 0) continue;
+        if (lay.cta[k][1] == 0) continue;
         CtSampleH& s = a.s[ns++];
         const DeviceSample& d = samples_[k];
         s.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
@@ -1161,8 +1210,8 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
         s.w = d.w;
         s.n = d.n;
         s.kind = k;
-        s.cta_begin = cta_[k][0];
-        s.cta_count = cta_[k][1];
+        s.cta_begin = lay.cta[k][0];
+        s.cta_count = lay.cta[k][1];
         s.vw_scale = 1.0 / (samples_[0].wsum > 0 ? samples_[0].wsum : 1.0);
     }
     a.nsamp = ns;
@@ -1176,7 +1225,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     const size_t slot = ev_begin_.empty() ? 0 : (size_t)(ev_count_ % (long long)ev_begin_.size());
     if (!ev_begin_.empty()) CT_CUDA(cudaEventRecord(ev_begin_[slot], stream));
     a.cta_base = 0;
-    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(256), args, 0, stream));
     if (!ev_begin_.empty()) {
         CT_CUDA(cudaEventRecord(ev_end_[slot], stream));
         ++ev_count_;
@@ -1189,9 +1238,9 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     f.nc = nc;
     f.nT = nT;
     for (int k = 0; k < 3; ++k) {
-        f.cta[k][0] = cta_[k][0];
-        f.cta[k][1] = cta_[k][1];
-        f.has[k] = cta_[k][1] > 0;
+        f.cta[k][0] = lay.cta[k][0];
+        f.cta[k][1] = lay.cta[k][1];
+        f.has[k] = lay.cta[k][1] > 0;
     }
     f.n_phsp = (double)samples_[0].n;
     f.W_data = samples_[1].wsum;
@@ -1257,6 +1306,7 @@ double* staticScratchAddress(int device)
 
 void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
 {
+    const CtaLayout& lay = lay_[precision == kMixed ? 1 : 0];
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
     const int nacc = 2 + 2 * nA + nT;
@@ -1265,12 +1315,12 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     const size_t off_v = 0;
     const size_t off_c = off_v + up((size_t)2 * nA);
     const size_t off_p = off_c + up((size_t)std::max(1, gen_.nconst));
-    const size_t off_parts = off_p + up((size_t)grid_ * nacc);
+    const size_t off_parts = off_p + up((size_t)lay.grid * nacc);
     const size_t need = off_parts + 8;
     const size_t cap = kStaticScratchBytes / sizeof(double);
     if (need > cap)
         throw std::length_error("ctpwa_nll_grad_static: this model needs " + std::to_string(need * sizeof(double)) +
-                                " bytes of scratch (" + std::to_string(grid_) + " CTA rows of " + std::to_string(nacc) +
+                                " bytes of scratch (" + std::to_string(lay.grid) + " CTA rows of " + std::to_string(nacc) +
                                 " sums), more than the fixed " + std::to_string(kStaticScratchBytes) +
                                 " bytes; use ctpwa_nll_grad");
     double* base = staticScratchAddress(opt_.device);
@@ -1285,7 +1335,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     std::memset(&a, 0, sizeof(a));
     int ns = 0;
     for (int k = 0; k < 3; ++k) {
-        if (cta_[k][1] == 0) continue;
+        if (lay.cta[k][1] == 0) continue;
         CtSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
         sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
@@ -1293,8 +1343,8 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
         sm.w = d.w;
         sm.n = d.n;
         sm.kind = k;
-        sm.cta_begin = cta_[k][0];
-        sm.cta_count = cta_[k][1];
+        sm.cta_begin = lay.cta[k][0];
+        sm.cta_count = lay.cta[k][1];
         sm.vw_scale = 1.0 / (samples_[0].wsum > 0 ? samples_[0].wsum : 1.0);
     }
     a.nsamp = ns;
@@ -1306,7 +1356,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     a.cta_base = 0;
-    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(256), args, 0, stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     f.partials = s_partials;
@@ -1315,9 +1365,9 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     f.nc = nc;
     f.nT = nT;
     for (int k = 0; k < 3; ++k) {
-        f.cta[k][0] = cta_[k][0];
-        f.cta[k][1] = cta_[k][1];
-        f.has[k] = cta_[k][1] > 0;
+        f.cta[k][0] = lay.cta[k][0];
+        f.cta[k][1] = lay.cta[k][1];
+        f.has[k] = lay.cta[k][1] > 0;
     }
     f.n_phsp = (double)samples_[0].n;
     f.W_data = samples_[1].wsum;
@@ -1338,6 +1388,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
 
 void Engine::shardSums(const double* d_params, int precision, double* d_sums, cudaStream_t stream)
 {
+    const CtaLayout& lay = lay_[precision == kMixed ? 1 : 0];
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
     const int nacc = 2 + 2 * nA + nT;
@@ -1347,7 +1398,7 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     std::memset(&a, 0, sizeof(a));
     int ns = 0;
     for (int k = 0; k < 3; ++k) {
-        if (cta_[k][1] == 0) continue;
+        if (lay.cta[k][1] == 0) continue;
         CtSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
         sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
@@ -1355,8 +1406,8 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
         sm.w = d.w;
         sm.n = d.n;
         sm.kind = k;
-        sm.cta_begin = cta_[k][0];
-        sm.cta_count = cta_[k][1];
+        sm.cta_begin = lay.cta[k][0];
+        sm.cta_count = lay.cta[k][1];
         sm.vw_scale = 1.0;  // the phase-space weight total is global: applied after the sums are combined
     }
     a.nsamp = ns;
@@ -1368,13 +1419,13 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     a.cta_base = 0;
-    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(grid_), dim3(256), args, 0, stream));
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(256), args, 0, stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     for (int k = 0; k < 3; ++k) {
-        f.cta[k][0] = cta_[k][0];
-        f.cta[k][1] = cta_[k][1];
-        f.has[k] = cta_[k][1] > 0;
+        f.cta[k][0] = lay.cta[k][0];
+        f.cta[k][1] = lay.cta[k][1];
+        f.has[k] = lay.cta[k][1] > 0;
     }
     f.n_phsp = (double)samples_[0].n;
     f.W_data = samples_[1].wsum;

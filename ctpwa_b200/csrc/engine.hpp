@@ -125,8 +125,14 @@ private:
     double* d_ratio_ = nullptr;
     int* d_gauss_idx_ = nullptr;
     double* d_gauss_ms_ = nullptr;  // [mu, sigma] pairs
-    int grid_ = 0;
-    int cta_[3][2] = {};  // per sample: begin, count
+    struct CtaLayout {
+        int cta[3][2] = {};  // per sample: begin, count
+        int grid = 0;
+    };
+    CtaLayout lay_[2];   // fused-kernel grid of the plain [0] and mixed [1] forms
+    int grid_max_ = 0;   // rows of the partials table
+    int residentCtas(void* kernel) const;
+    void layoutCtas(int target, long long tot, CtaLayout& lay) const;
 
     cudaStream_t init_stream_ = nullptr;  // initialisation only
 

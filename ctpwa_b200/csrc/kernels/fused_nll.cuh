@@ -283,13 +283,19 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             accg[2 * a] += gscale * (fr * tr + fi * ti);
             accg[2 * a + 1] += gscale * (fr * ti - fi * tr);
         }
-        // theta-gradient: Re(v_a dF conj(T))
+        // theta-gradient: Re(v_a dF conj(T)) = Re(dF W_a), W_a = v_a conj(T_plane(a))
+        L Wr[M_NA], Wi[M_NA];
+#pragma unroll
+        for (int a = 0; a < M_NA; ++a) {
+            const int c = col_plane(a);
+            const L tr = (L)Tr[c], ti = (L)Ti[c];
+            Wr[a] = tscale * (vr[a] * tr + vi[a] * ti);
+            Wi[a] = tscale * (vi[a] * tr - vr[a] * ti);
+        }
 #pragma unroll
         for (int k = 0; k < M_NDER; ++k) {
-            const int a = der_col(k), c = col_plane(a);
-            const L xr = vr[a] * dFr[k] - vi[a] * dFi[k];
-            const L xi = vr[a] * dFi[k] + vi[a] * dFr[k];
-            accg[2 * M_NA + der_th(k)] += tscale * (xr * (L)Tr[c] + xi * (L)Ti[c]);
+            const int a = der_col(k);
+            accg[2 * M_NA + der_th(k)] += dFr[k] * Wr[a] - dFi[k] * Wi[a];
         }
     }
     ct_block_reduce_store<L>(accd, accg, A.partials + (long long)cta * CT_NACC);
