@@ -90,8 +90,38 @@ __device__ __forceinline__ double ct_inf() { return __longlong_as_double(0x7ff00
 __device__ __forceinline__ float ct_nanf() { return __int_as_float(0x7fc00000); }
 __device__ __forceinline__ float ct_inff() { return __int_as_float(0x7f800000); }
 
-// FP32 reciprocal and square root of the mixed-form lineshapes, correctly
-// rounded: their errors are symmetric, so they average out over a sample
-// instead of biasing the phase-space normalisation.
-__device__ __forceinline__ float ct_rcpf(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ float ct_sqrtf(float x) { return __fsqrt_rn(x); }
+// FP32 reciprocal and square root of the mixed-form lineshapes. The hardware
+// approximation (rcp.approx / rsqrt.approx, relative error d of order 2^-23)
+// is refined by one Newton-Raphson step whose residual is formed exactly by
+// an FMA: the refined value carries a relative error of order d^2 (~1e-14)
+// before its final round-to-nearest, so its errors are symmetric and average
+// out over a sample instead of biasing the phase-space normalisation (a
+// one-sided approximation error would not). Zero and infinite inputs take
+// the approximation's own result (the refinement would give NaN there).
+__device__ __forceinline__ float ct_rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ct_rsqrt_approx(float x)
+{
+    float r;
+    asm("rsqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ct_rcpf(float x)
+{
+    const float r0 = ct_rcp_approx(x);
+    const float e = fmaf(-x, r0, 1.0f);  // 1 - x r0, exact
+    const float r1 = fmaf(r0, e, r0);    // r0 (1 + e) = (1/x)(1 - d^2)
+    return (x == 0.0f || fabsf(x) == __int_as_float(0x7f800000)) ? r0 : r1;
+}
+__device__ __forceinline__ float ct_sqrtf(float x)
+{
+    const float r = ct_rsqrt_approx(x);
+    const float y0 = x * r;
+    const float e = fmaf(-y0, y0, x);          // x - y0^2, exact
+    const float y1 = fmaf(0.5f * r, e, y0);    // y0 + (x - y0^2) / (2 sqrt x)
+    return (x == 0.0f || x == __int_as_float(0x7f800000)) ? x : y1;
+}
