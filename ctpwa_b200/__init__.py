@@ -328,6 +328,69 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return nll, grad
 
+    def getNBlocks(self) -> int:
+        """Number of resonance blocks (partial waves of the fit fractions)."""
+        self._check()
+        return int(self._lib.ctpwa_n_blocks(self._h))
+
+    def getPartialIntegrals(self, params: torch.Tensor, kind: int = 0) -> torch.Tensor:
+        """Per resonance block i: sum_e w_e sum_pol |sum_{a in i} v_a A_a|^2 over
+        sample kind 0 (phase space), 1 (data), 2 (background) or 3
+        (Data.phsp_truth). float64 CUDA [nBlocks]."""
+        p = self._check_params(params)
+        out = torch.empty(self.getNBlocks(), dtype=torch.float64, device=p.device)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        rc = self._lib.ctpwa_partial_integrals(self._h, p.data_ptr(), int(kind), out.data_ptr(), ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return out
+
+    def getFitFractions(self, params: torch.Tensor, hessian: torch.Tensor = None) -> torch.Tensor:
+        """Fit fractions FF_i = I_i / sum_j I_j of the resonance blocks (reference
+        analysis::getFitFractions, src/Analysis.cu:3527-3630), integrated over
+        Data.phsp_truth (or over the phase-space sample when the config has no
+        phsp_truth). Errors: J_FF H^-1 J_FF^T with the coupling block of the
+        Hessian (`hessian` if given, else getHessian(params)) over the free
+        couplings (the first coupling is the fixed reference), J_FF by central
+        differences (step 5e-6 max(|p_j|, 1)). Returns CPU float64 [nBlocks, 2] =
+        [center, error]; errors are 0 when the Hessian block is not positive
+        definite."""
+        import numpy as np
+
+        p = self._check_params(params).clone()
+        kind = 3
+        try:
+            self.getPartialIntegrals(p, 3)
+        except RuntimeError as e:
+            if "phsp_truth" not in str(e):
+                raise
+            kind = 0
+
+        def ff(q):
+            I = self.getPartialIntegrals(q, kind)
+            tot = float(I.sum())
+            return (I / (tot if tot > 0 else 1e-30)).cpu().numpy()
+
+        center = ff(p)
+        n = self.getNVector()
+        free = [j for j in range(2 * n) if j not in (0, n)]
+        errors = np.zeros_like(center)
+        if free:
+            H = hessian if hessian is not None else self.getHessian(p)
+            Hf = H[:2 * n, :2 * n].detach().to(torch.float64).cpu().numpy()[np.ix_(free, free)]
+            if np.linalg.eigvalsh(Hf)[0] > 1e-8:
+                cov = np.linalg.inv(Hf)
+                J = np.zeros((center.size, len(free)))
+                for c, j in enumerate(free):
+                    eps = 5e-6 * max(abs(float(p[j])), 1.0)
+                    qp = p.clone()
+                    qp[j] += eps
+                    qm = p.clone()
+                    qm[j] -= eps
+                    J[:, c] = (ff(qp) - ff(qm)) / (2 * eps)
+                errors = np.sqrt(np.maximum(np.einsum("ij,jk,ik->i", J, cov, J), 0.0))
+        return torch.tensor(np.stack([center, errors], axis=1), dtype=torch.float64)
+
     def getIntensity(self, params: torch.Tensor, kind: int = 1) -> torch.Tensor:
         """Per-event intensities (float64 CUDA [n]) of sample kind 0 = phase space, 1 = data, 2 = background."""
         p = self._check_params(params)

@@ -165,6 +165,21 @@ int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, doubl
     return CTPWA_OK;
 }
 
+int ctpwa_n_blocks(const ctpwa_handle* h) { return h ? h->eng->nBlocks() : CTPWA_ERR_ARG; }
+
+int ctpwa_partial_integrals(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream)
+{
+    if (!h || !d_params || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (kind < 0 || kind > 3) return setErr(h, CTPWA_ERR_ARG, "sample kind must be 0 (phsp), 1, 2 or 3 (phsp_truth)");
+    try {
+        h->eng->partialIntegrals(d_params, kind, d_out, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        std::string m = e.what();
+        return setErr(h, m.rfind("No phsp_truth", 0) == 0 ? CTPWA_ERR_CONFIG : CTPWA_ERR_CUDA, m);
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_sums_size(const ctpwa_handle* h) { return h ? h->eng->sumsSize() : CTPWA_ERR_ARG; }
 
 int ctpwa_shard_sums(ctpwa_handle* h, const double* d_params, int precision, double* d_sums, void* stream)

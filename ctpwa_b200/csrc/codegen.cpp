@@ -933,6 +933,16 @@ std::string Gen::emit()
         for (int s = 0; s < m.groups[b.group].nSL(); ++s)
             h << "  case " << b.site + s << ": return " << out.group_plane0[b.group] + s << ";\n";
     h << "  default: return 0;\n  }\n}\n";
+    // resonance blocks (partial waves of the fit fractions): first column and
+    // number of SL combinations of each
+    h << "#define M_NBLK " << m.blocks.size() << "\n";
+    h << "__device__ __forceinline__ int blk_site(int i) {\n  switch (i) {\n";
+    for (size_t i = 0; i < m.blocks.size(); ++i) h << "  case " << i << ": return " << m.blocks[i].site << ";\n";
+    h << "  default: return 0;\n  }\n}\n";
+    h << "__device__ __forceinline__ int blk_nsl(int i) {\n  switch (i) {\n";
+    for (size_t i = 0; i < m.blocks.size(); ++i)
+        h << "  case " << i << ": return " << m.groups[m.blocks[i].group].nSL() << ";\n";
+    h << "  default: return 0;\n  }\n}\n";
     h << "__device__ __forceinline__ int der_col(int k) {\n  switch (k) {\n";
     for (size_t q = 0; q < der_entries.size(); ++q) h << "  case " << q << ": return " << der_entries[q].first << ";\n";
     h << "  default: return 0;\n  }\n}\n";

@@ -1149,6 +1149,9 @@ void Engine::compileKernel()
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
+    cudaKernel_t kpart;
+    CT_CUDA(cudaLibraryGetKernel(&kpart, lib, "ct_partials_f64"));
+    k_part_ = (void*)kpart;
     k_f64_ = (void*)k64;
     k_mixed_ = (void*)kmx;
     k_int_ = (void*)kin;
@@ -1518,6 +1521,90 @@ void Engine::hessian(const double* d_params, double* d_hess, double rel_step, cu
         CT_CUDA(cudaGetLastError());
     }
     ct_symmetrize_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, stream>>>(d_hess, n);
+    CT_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+// out[j] = sum over rows r of rows[r][j] (fixed order: one warp per column)
+__global__ void ct_colsum_kernel(const double* __restrict__ rows, int nrows, int ncols, double* __restrict__ out)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int j = warp; j < ncols; j += nwarp) {
+        double s = 0.0;
+        for (int r = lane; r < nrows; r += 32) s += rows[(long long)r * ncols + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) out[j] = s;
+    }
+}
+
+}  // namespace
+
+void Engine::loadTruth()
+{
+    if (truth_loaded_) return;
+    auto it = model_.cfg.data_files.find("phsp_truth");
+    if (it == model_.cfg.data_files.end()) throw std::runtime_error("No phsp_truth in config");
+    const int nfin = (int)model_.final_order.size();
+    Sample s = readSample(it->second, nfin);
+    std::vector<double> w;
+    shardSample(s, w, opt_.shard_rank, opt_.shard_world);
+    DeviceSample& d = samples_[3];
+    d.n = s.n;
+    d.wsum = (double)s.n;
+    CT_CUDA(cudaSetDevice(opt_.device));
+    CT_CUDA(cudaStreamCreateWithFlags(&init_stream_, cudaStreamNonBlocking));
+    if (s.n > 0) {
+        size_t bytes = sizeof(double) * (size_t)s.n * nfin * 4;
+        double* tmp = nullptr;
+        CT_CUDA(cudaMallocAsync((void**)&tmp, bytes, init_stream_));
+        CT_CUDA(cudaMemcpyAsync(tmp, s.p4.data(), bytes, cudaMemcpyHostToDevice, init_stream_));
+        CT_CUDA(cudaMallocAsync((void**)&d.p4, bytes, init_stream_));
+        ag_transpose_kernel<<<(unsigned)((s.n + 255) / 256), 256, 0, init_stream_>>>(tmp, d.p4, s.n, nfin);
+        CT_CUDA(cudaGetLastError());
+        CT_CUDA(cudaFreeAsync(tmp, init_stream_));
+        CT_CUDA(cudaStreamSynchronize(init_stream_));
+        device_bytes_ += bytes;
+    }
+    computeAngular(3);
+    cudaStreamDestroy(init_stream_);
+    init_stream_ = nullptr;
+    truth_loaded_ = true;
+}
+
+void Engine::partialIntegrals(const double* d_params, int kind, double* d_out, cudaStream_t stream)
+{
+    if (kind < 0 || kind > 3) throw std::runtime_error("partial integrals: sample kind must be 0..3");
+    if (kind == 3) loadTruth();
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nb = nBlocks();
+    const DeviceSample& d = samples_[kind];
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    a.s[0].slamp = d.slamp64;
+    a.s[0].kin = d.kin;
+    a.s[0].w = d.w;
+    a.s[0].n = d.n;
+    a.s[0].kind = kind;
+    a.s[0].cta_count = 1;
+    a.nsamp = 1;
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.partials = d_partials_;
+    a.consts = d_consts_;
+    void* pargs[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), pargs, 0, stream));
+    // rows of nb sums in the partials table (nacc >= nA >= nb columns per row available)
+    const int nacc = 2 + 2 * nA + m.nTheta();
+    const long long cap_rows = (long long)grid_max_ * nacc / std::max(1, nb);
+    int grid = (int)std::max(1LL, std::min<long long>((d.n + 255) / 256, std::min<long long>(cap_rows, 148LL * 4)));
+    double* rows = d_partials_;
+    void* args[] = {&a, &rows};
+    CT_CUDA(cudaLaunchKernel(k_part_, dim3(grid), dim3(256), args, 0, stream));
+    ct_colsum_kernel<<<1, 256, 0, stream>>>(rows, grid, nb, d_out);
     CT_CUDA(cudaGetLastError());
 }
 

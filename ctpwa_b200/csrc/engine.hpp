@@ -68,6 +68,13 @@ public:
     // h_i = rel_step * max(|p_i|, 1e-2), 2 nP gradient evaluations queued on
     // the stream with no host synchronisation.
     void hessian(const double* d_params, double* d_hess, double rel_step, cudaStream_t stream);
+    // Partial-wave integrals sum_e w_e sum_p |sum_{a in block i} v_a A_{a,p}|^2
+    // per resonance block i over sample `kind` (0 phase space, 1 data,
+    // 2 background, 3 phase-space truth from the config's Data.phsp_truth,
+    // loaded on first use); d_out: device [nBlocks()]. Fit fractions are
+    // ratios of these (FP64).
+    int nBlocks() const { return (int)model_.blocks.size(); }
+    void partialIntegrals(const double* d_params, int kind, double* d_out, cudaStream_t stream);
     // Per-event intensities of sample `kind` at d_params (device output [n]).
     void intensity(const double* d_params, int kind, double* d_out, cudaStream_t stream);
     // Per-sample partial sums of the last evaluation (diagnostics):
@@ -96,7 +103,9 @@ private:
     Model model_;
     EngineOptions opt_;
     GeneratedModel gen_;
-    DeviceSample samples_[3];  // phsp, data, bkg
+    DeviceSample samples_[4];  // phsp, data, bkg, phase-space truth (loaded on first use)
+    bool truth_loaded_ = false;
+    void loadTruth();
     bool has_bkg_ = false;
     size_t device_bytes_ = 0;
 
@@ -111,6 +120,7 @@ private:
     void* k_f64_ = nullptr;
     void* k_mixed_ = nullptr;
     void* k_int_ = nullptr;
+    void* k_part_ = nullptr;
     void* k_pro_ = nullptr;
     double jit_seconds_ = 0.0;
     bool jit_cache_hit_ = false;

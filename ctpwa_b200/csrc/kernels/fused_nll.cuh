@@ -311,6 +311,63 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK, CT_MX_MINB) ct_fused_mixe
     ct_fused_body<float, float, false>(a);
 }
 
+// Partial-wave integrals of sample s[0] (FP64): per resonance block i,
+// sum_e w_e sum_p |sum_{a in block i} v_a A_{a,p}|^2 (the reference's partial
+// integrals of its fit fractions, src/ComputeBF.cu:9-60); one row of M_NBLK
+// sums per CTA.
+extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A, double* __restrict__ rows)
+{
+    const CtSample& S = A.s[0];
+    const long long n = S.n;
+    const double2* __restrict__ slamp = (const double2*)S.slamp;
+    __shared__ double sC[CT_NCONST_ALLOC];
+    ct_stage_consts(A, sC);
+    double acc[M_NBLK];
+#pragma unroll
+    for (int i = 0; i < M_NBLK; ++i) acc[i] = 0.0;
+    for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
+        double kv[M_NKIN > 0 ? M_NKIN : 1];
+#pragma unroll
+        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * n + e);
+        double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
+        model_columns(kv, sC, Fr, Fi, dFr, dFi);
+        const double we = S.w ? __ldg(S.w + e) : 1.0;
+#pragma unroll
+        for (int i = 0; i < M_NBLK; ++i) {
+            double t = 0.0;
+#pragma unroll
+            for (int p = 0; p < M_NPOL; ++p) {
+                double sr = 0.0, si = 0.0;
+                for (int a = blk_site(i); a < blk_site(i) + blk_nsl(i); ++a) {
+                    const double vr = __ldg(A.v + 2 * a), vi = __ldg(A.v + 2 * a + 1);
+                    const double cr = vr * Fr[a] - vi * Fi[a], ci = vr * Fi[a] + vi * Fr[a];
+                    const double2 x = slamp[(long long)(col_plane(a) * M_NPOL + p) * n + e];
+                    sr += cr * x.x - ci * x.y;
+                    si += cr * x.y + ci * x.x;
+                }
+                t += sr * sr + si * si;
+            }
+            acc[i] += we * t;
+        }
+    }
+    __shared__ double red[CT_BLOCK / 32][M_NBLK];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < M_NBLK; ++i) {
+        double x = acc[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp][i] = x;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < M_NBLK; i += CT_BLOCK) {
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < CT_BLOCK / 32; ++w) x += red[w][i];
+        rows[(long long)blockIdx.x * M_NBLK + i] = x;
+    }
+}
+
 // Per-event intensity f_e = sum_p |S_p|^2 of sample s[0] (FP64), for
 // accept-reject toy generation and per-event weights.
 extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_intensity_f64(CtArgs A, double* __restrict__ out)

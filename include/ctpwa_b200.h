@@ -108,6 +108,17 @@ int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll
  * queued on the stream, no host synchronisation, no allocation. */
 int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, double rel_step, void* stream);
 
+/* Number of resonance blocks (the partial waves of the fit fractions; the
+ * reference's nSLvectors_, src/Analysis.cu:1350). */
+int ctpwa_n_blocks(const ctpwa_handle* h);
+
+/* Replaces the partial integrals of analysis::getFitFractions —
+ * src/Analysis.cu:3431-3526 (computeTruthBatchIntegrals), src/ComputeBF.cu:9-60.
+ * d_out[i] = sum_e w_e sum_pol |sum_{a in block i} v_a A_a|^2 over sample kind
+ * 0 (phase space), 1 (data), 2 (background) or 3 (Data.phsp_truth, read and
+ * prepared on the first call), at d_params; device pointers, FP64. */
+int ctpwa_partial_integrals(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream);
+
 /* Event-sharded evaluation, the exchange step of the reference's multi-device
  * NLL (src/Analysis.cu:4210-4238, which gathers per-device partial results
  * with peer copies). ctpwa_shard_sums writes this shard's per-sample sums

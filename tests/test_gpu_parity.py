@@ -170,3 +170,41 @@ def test_hessian_matches_oracle_fd(setups):
     Ho = 0.5 * (Ho + Ho.T)
     assert np.allclose(H, H.T, rtol=0, atol=0)
     assert np.max(np.abs(H - Ho)) <= 1e-6 * np.max(np.abs(Ho)), np.max(np.abs(H - Ho)) / np.max(np.abs(Ho))
+
+
+def test_partial_integrals_and_fit_fractions(setups, tmp_path):
+    """Partial-wave integrals vs the oracle's amplitude columns; fit fractions
+    sum to one; phase-space truth sample read on demand."""
+    import torch
+    import ctpwa_b200
+
+    ana, orc, pt, p = setups["pipi_3rho"]
+    nV = ana.getNVector()
+    I = ana.getPartialIntegrals(pt, 0).cpu().numpy()
+    m = ana.getModel()
+    cols = orc.columns(0, p[2 * nV:])  # [ev][pol][nA]
+    chain, ratio = m["coupling"]["amp_chain"], m["coupling"]["ratio"]
+    v = np.array([ratio[a] * complex(p[chain[a]], p[nV + chain[a]]) for a in range(cols.shape[2])])
+    ref = []
+    for b in m["blocks"]:
+        nsl = len(m["groups"][b["group"]]["sl_combs"])
+        S = np.einsum("epa,a->ep", cols[:, :, b["site"]:b["site"] + nsl], v[b["site"]:b["site"] + nsl])
+        ref.append(np.sum(np.abs(S) ** 2))
+    ref = np.array(ref)
+    assert np.max(np.abs(I - ref)) <= 1e-10 * np.max(np.abs(ref))
+    ff = ana.getFitFractions(pt)
+    assert ff.shape == (ana.getNBlocks(), 2)
+    assert abs(float(ff[:, 0].sum()) - 1.0) < 1e-12
+    # a config with Data.phsp_truth integrates over that sample
+    cfg = workloads.make("pipi_rho", tmp_path, n_phsp=5_000, n_data=1_000, n_bkg=0, accept_reject=False, seed=21)
+    from ctpwa_b200 import toymc
+
+    truth = toymc.phase_space(workloads.M_JPSI, workloads.MASSES["pipi_rho"], 7_000, 77)
+    toymc.write_npy(tmp_path / "truth.npy", truth)
+    text = open(cfg).read().replace("Data:\n", f'Data:\n  phsp_truth: [npy, "{tmp_path / "truth.npy"}"]\n', 1)
+    open(cfg, "w").write(text)
+    a2 = ctpwa_b200.analysis(cfg)
+    q = torch.tensor(workloads.true_params(a2.getNVector(), a2.getFreeResParams()[0].numpy()), dtype=torch.float64,
+                     device="cuda")
+    assert float(a2.getPartialIntegrals(q, 3).sum()) > 0
+    assert abs(float(a2.getFitFractions(q)[:, 0].sum()) - 1.0) < 1e-12
