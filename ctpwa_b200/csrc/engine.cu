@@ -665,31 +665,31 @@ std::string cacheDir()
 
 // Resident 256-thread CTAs per SM of a fused kernel (occupancy query on the
 // library kernel handle; from its register count if that query is refused).
-int Engine::residentCtas(void* kernel) const
+int Engine::residentCtas(void* kernel, int block) const
 {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kernel, 256, 0) == cudaSuccess && nb > 0)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kernel, block, 0) == cudaSuccess && nb > 0)
         return nb;
     cudaGetLastError();
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, (const void*)kernel) == cudaSuccess && fa.numRegs > 0) {
         cudaGetLastError();
         int regs = (fa.numRegs + 7) / 8 * 8;
-        return std::max(1, std::min(8, 65536 / (regs * 256)));
+        return std::max(1, std::min(2048 / block, 65536 / (regs * block)));
     }
     cudaGetLastError();
     return 1;
 }
 
 // Split `target` CTAs over the samples in proportion to their event counts
-// (at least one CTA per non-empty sample, at most one per 256 events).
-void Engine::layoutCtas(int target, long long tot, CtaLayout& lay) const
+// (at least one CTA per non-empty sample, at most one per `block` events).
+void Engine::layoutCtas(int target, long long tot, int block, CtaLayout& lay) const
 {
     long long want[3] = {0, 0, 0}, maxc[3] = {0, 0, 0};
     long long sum = 0;
     for (int k = 0; k < 3; ++k) {
         if (samples_[k].n <= 0) continue;
-        maxc[k] = (samples_[k].n + 255) / 256;
+        maxc[k] = (samples_[k].n + block - 1) / block;
         want[k] = std::max(1LL, std::min(maxc[k], (long long)std::floor((double)target * samples_[k].n / std::max(1LL, tot))));
         sum += want[k];
     }
@@ -732,6 +732,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     CT_CUDA(cudaGetDeviceCount(&ndev));
     if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
     CT_CUDA(cudaSetDevice(opt_.device));
+    shape_ = fusedShape();
     // initialisation work goes to a private non-blocking stream, so a handle
     // being created does not serialise with other handles' evaluations
     CT_CUDA(cudaStreamCreateWithFlags(&init_stream_, cudaStreamNonBlocking));
@@ -773,8 +774,8 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     for (int k = 0; k < 3; ++k) tot += samples_[k].n;
     int maxgrid = 1;
     for (int pr = 0; pr < 2; ++pr) {
-        int occ = residentCtas(pr == 0 ? k_f64_ : k_mixed_);
-        layoutCtas(sms * occ, tot, lay_[pr]);
+        int occ = residentCtas(pr == 0 ? k_f64_ : k_mixed_, shape_.block[pr]);
+        layoutCtas(sms * occ, tot, shape_.block[pr], lay_[pr]);
         maxgrid = std::max(maxgrid, lay_[pr].grid);
     }
     grid_max_ = maxgrid;
@@ -1067,6 +1068,29 @@ void Engine::computeAngular(int kind)
     CT_CUDA(cudaStreamSynchronize(init_stream_));
 }
 
+// Block size and minimum resident CTAs per SM of the plain [0] and mixed [1]
+// fused kernels: 128 x 3 (170 registers, 12 warps per SM; measured 7 % faster
+// than 256 x 1) and 256 x 2 unless CTPWA_F64_BLOCK / CTPWA_F64_MINB /
+// CTPWA_MX_BLOCK / CTPWA_MX_MINB override them (tuning).
+FusedShape fusedShape()
+{
+    FusedShape sh;
+    auto get = [](const char* name, int def, int lo, int hi) {
+        const char* e = std::getenv(name);
+        if (!e || !*e) return def;
+        int v = std::atoi(e);
+        if (v < lo || v > hi) throw std::runtime_error(std::string(name) + " out of range");
+        return v;
+    };
+    sh.block[0] = get("CTPWA_F64_BLOCK", 128, 32, 1024);
+    sh.minb[0] = get("CTPWA_F64_MINB", 3, 1, 16);
+    sh.block[1] = get("CTPWA_MX_BLOCK", 256, 32, 1024);
+    sh.minb[1] = get("CTPWA_MX_MINB", 2, 1, 16);
+    for (int i = 0; i < 2; ++i)
+        if (sh.block[i] % 32) throw std::runtime_error("fused block sizes must be multiples of 32");
+    return sh;
+}
+
 // NVRTC compile of the fused kernel for one generated model, with a disk cache
 // keyed by the FNV-1a hash of all sources, options and the NVRTC version.
 std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
@@ -1077,12 +1101,12 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     std::string src = "#include \"fused_nll.cuh\"\n";
     std::vector<std::string> optv = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
                                      "--fmad=true", "-lineinfo"};
-    // tuning knob: minimum resident CTAs per SM of the mixed-form kernel
-    if (const char* e = std::getenv("CTPWA_MX_MINB")) {
-        int v = std::atoi(e);
-        if (v < 1 || v > 8) throw std::runtime_error("CTPWA_MX_MINB must be in [1, 8]");
-        optv.push_back("-DCT_MX_MINB=" + std::to_string(v));
-    }
+    // tuning knobs: block size and minimum resident CTAs per SM of the fused kernels
+    const FusedShape sh = fusedShape();
+    optv.push_back("-DCT_F64_BLOCK=" + std::to_string(sh.block[0]));
+    optv.push_back("-DCT_F64_MINB=" + std::to_string(sh.minb[0]));
+    optv.push_back("-DCT_MX_BLOCK=" + std::to_string(sh.block[1]));
+    optv.push_back("-DCT_MX_MINB=" + std::to_string(sh.minb[1]));
     std::vector<const char*> optp;
     for (const auto& o : optv) optp.push_back(o.c_str());
     const char* const* opts = optp.data();
@@ -1228,7 +1252,8 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     const size_t slot = ev_begin_.empty() ? 0 : (size_t)(ev_count_ % (long long)ev_begin_.size());
     if (!ev_begin_.empty()) CT_CUDA(cudaEventRecord(ev_begin_[slot], stream));
     a.cta_base = 0;
-    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(256), args, 0, stream));
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
+                             args, 0, stream));
     if (!ev_begin_.empty()) {
         CT_CUDA(cudaEventRecord(ev_end_[slot], stream));
         ++ev_count_;
@@ -1359,7 +1384,8 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     a.cta_base = 0;
-    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(256), args, 0, stream));
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
+                             args, 0, stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     f.partials = s_partials;
@@ -1422,7 +1448,8 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     a.cta_base = 0;
-    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(256), args, 0, stream));
+    CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
+                             args, 0, stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     for (int k = 0; k < 3; ++k) {

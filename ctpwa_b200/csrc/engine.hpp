@@ -15,6 +15,13 @@ namespace ctpwa {
 
 enum Precision : int { kFP64 = 0, kMixed = 1 };
 
+// Launch shape of the plain [0] and mixed [1] fused kernels.
+struct FusedShape {
+    int block[2] = {128, 256};
+    int minb[2] = {3, 2};
+};
+FusedShape fusedShape();
+
 struct DeviceSample {
     long long n = 0;
     double* p4 = nullptr;      // SoA [n_final * 4][n]
@@ -141,8 +148,9 @@ private:
     };
     CtaLayout lay_[2];   // fused-kernel grid of the plain [0] and mixed [1] forms
     int grid_max_ = 0;   // rows of the partials table
-    int residentCtas(void* kernel) const;
-    void layoutCtas(int target, long long tot, CtaLayout& lay) const;
+    FusedShape shape_;
+    int residentCtas(void* kernel, int block) const;
+    void layoutCtas(int target, long long tot, int block, CtaLayout& lay) const;
 
     cudaStream_t init_stream_ = nullptr;  // initialisation only
 

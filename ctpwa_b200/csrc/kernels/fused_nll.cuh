@@ -94,10 +94,10 @@ struct CtVec2<float> {
 
 // CTA reduction of the per-thread accumulators: two FP64 sums (log-likelihood
 // and phase-space intensity) and the gradient terms (type G), reduced in FP64.
-template <typename G>
+template <int BLOCK, typename G>
 __device__ __forceinline__ void ct_block_reduce_store(const double* accd, const G* accg, double* out)
 {
-    __shared__ double red[CT_BLOCK / 32][CT_NACC];
+    __shared__ double red[BLOCK / 32][CT_NACC];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int i = 0; i < CT_NACC; ++i) {
@@ -107,10 +107,10 @@ __device__ __forceinline__ void ct_block_reduce_store(const double* accd, const 
         if (lane == 0) red[warp][i] = x;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < CT_NACC; i += CT_BLOCK) {
+    for (int i = threadIdx.x; i < CT_NACC; i += BLOCK) {
         double x = 0.0;
 #pragma unroll
-        for (int w = 0; w < CT_BLOCK / 32; ++w) x += red[w][i];
+        for (int w = 0; w < BLOCK / 32; ++w) x += red[w][i];
         out[i] = x;
     }
 }
@@ -139,7 +139,7 @@ struct CtLineshape<float> {
 // L: type of the lineshapes, their derivatives and the per-thread gradient
 //    sums
 // PH_ONLY: the launch serves phase-space events only
-template <typename R, typename L, bool PH_ONLY>
+template <typename R, typename L, bool PH_ONLY, int BLOCK>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 {
     typedef typename CtVec2<R>::type SL2;
@@ -184,8 +184,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         vil[a] = (L)(i - (double)vi[a]);
     }
 
-    const long long stride = (long long)S.cta_count * CT_BLOCK;
-    for (long long e = (long long)(cta - S.cta_begin) * CT_BLOCK + threadIdx.x; e < n; e += stride) {
+    const long long stride = (long long)S.cta_count * BLOCK;
+    for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride) {
         // ---- lineshapes with parameter derivatives ----
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
@@ -298,17 +298,31 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             accg[2 * M_NA + der_th(k)] += dFr[k] * Wr[a] - dFi[k] * Wi[a];
         }
     }
-    ct_block_reduce_store<L>(accd, accg, A.partials + (long long)cta * CT_NACC);
+    ct_block_reduce_store<BLOCK, L>(accd, accg, A.partials + (long long)cta * CT_NACC);
 }
 
-extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_fused_f64(CtArgs a) { ct_fused_body<double, double, false>(a); }
-// mixed form (FP32 lineshapes and algebra, FP64 logs and sums), all samples
+// block size and minimum resident CTAs per SM of the two fused kernels (the
+// host launches with the same block sizes)
+#ifndef CT_F64_BLOCK
+#define CT_F64_BLOCK 128
+#endif
+#ifndef CT_F64_MINB
+#define CT_F64_MINB 3
+#endif
+#ifndef CT_MX_BLOCK
+#define CT_MX_BLOCK 256
+#endif
 #ifndef CT_MX_MINB
 #define CT_MX_MINB 2
 #endif
-extern "C" __global__ void __launch_bounds__(CT_BLOCK, CT_MX_MINB) ct_fused_mixed(CtArgs a)
+extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB) ct_fused_f64(CtArgs a)
 {
-    ct_fused_body<float, float, false>(a);
+    ct_fused_body<double, double, false, CT_F64_BLOCK>(a);
+}
+// mixed form (FP32 lineshapes and algebra, FP64 logs and sums), all samples
+extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_mixed(CtArgs a)
+{
+    ct_fused_body<float, float, false, CT_MX_BLOCK>(a);
 }
 
 // Partial-wave integrals of sample s[0] (FP64): per resonance block i,
