@@ -983,6 +983,7 @@ GeneratedModel generateModel(const Model& m)
         pl += gr.nSL();
     }
     g.out.nplane = pl;
+    g.out.npol = m.npol;
     g.cols.resize(m.nAmp());
     for (const auto& b : m.blocks) {
         const Group& gr = m.groups[b.group];

@@ -26,6 +26,7 @@ struct GeneratedModel {
     std::string header;          // model.cuh text
     std::vector<KinSlot> slots;  // kinematic cache layout
     int nplane = 0;              // angular planes = sum over groups of nSL
+    int npol = 1;                // polarisation states per plane
     std::vector<int> group_plane0;
     int nder = 0;
     int nconst = 0;              // parameter-only subexpressions kept per call

@@ -346,6 +346,7 @@ __global__ void ag_transpose_kernel(const double* __restrict__ aos, double* __re
 }
 
 __global__ void __launch_bounds__(128) ag_group_kernel(AgGroup G, AgTables T, const double* __restrict__ p4, long long n,
+                                                       long long ld,
                                                        double2* __restrict__ out64, float2* __restrict__ out32,
                                                        double* __restrict__ kin)
 {
@@ -394,7 +395,7 @@ __global__ void __launch_bounds__(128) ag_group_kernel(AgGroup G, AgTables T, co
         }
         case AG_K_PHI: val = atan2(a.y, a.x); break;
         }
-        kin[(long long)d[4] * n + e] = val;
+        kin[(long long)d[4] * ld + e] = val;
     }
     // spin-orbit tensors and chain contraction
     double2 cur[AG_MAXT], nxt[AG_MAXT], node[AG_MAXT];
@@ -457,8 +458,8 @@ __global__ void __launch_bounds__(128) ag_group_kernel(AgGroup G, AgTables T, co
         const long long plane = (long long)(G.plane0 + s) * G.npol;
         for (int p = 0; p < G.npol; ++p) {
             double2 v = G.pol_map ? cur[G.pol_map[p]] : cur[p];
-            out64[(plane + p) * n + e] = v;
-            if (out32) out32[(plane + p) * n + e] = make_float2((float)v.x, (float)v.y);
+            out64[(plane + p) * ld + e] = v;
+            if (out32) out32[(plane + p) * ld + e] = make_float2((float)v.x, (float)v.y);
         }
     }
 }
@@ -497,6 +498,9 @@ struct FinalizeArgs {
     // W_data, W_bkg] replace the partial rows and the sample totals; the
     // phase-space coupling-gradient sums are then divided by W_phsp here
     const double* sums;
+    // set when a fused kernel's staged copy did not arrive: the evaluation is
+    // invalid and reported like a non-finite NLL (loss 1e30, zero gradient)
+    const int* err;
 };
 
 // Per-sample sums of the partial rows plus the sample totals (event-sharded
@@ -560,6 +564,7 @@ __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
     if (pf <= 1e-30 || isnan(pf) || isinf(pf)) pf = 1e-30;
     double Weff = W_data - W_bkg;
     double loss = Dd[0] - B[0] + Weff * log(pf);
+    if (A.err && *A.err) loss = nan("");
     const double* theta = A.params + 2 * A.nc;
     for (int g = 0; g < A.ngauss; ++g) {
         double dl = theta[A.gauss_idx[g]] - A.gauss_ms[2 * g];
@@ -665,10 +670,11 @@ std::string cacheDir()
 
 // Resident 256-thread CTAs per SM of a fused kernel (occupancy query on the
 // library kernel handle; from its register count if that query is refused).
-int Engine::residentCtas(void* kernel, int block) const
+int Engine::residentCtas(void* kernel, int block, int dsmem) const
 {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kernel, block, 0) == cudaSuccess && nb > 0)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kernel, block, (size_t)dsmem) == cudaSuccess &&
+        nb > 0)
         return nb;
     cudaGetLastError();
     cudaFuncAttributes fa;
@@ -732,7 +738,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     CT_CUDA(cudaGetDeviceCount(&ndev));
     if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
     CT_CUDA(cudaSetDevice(opt_.device));
-    shape_ = fusedShape();
+    shape_ = fusedShape(gen_);
     // initialisation work goes to a private non-blocking stream, so a handle
     // being created does not serialise with other handles' evaluations
     CT_CUDA(cudaStreamCreateWithFlags(&init_stream_, cudaStreamNonBlocking));
@@ -774,7 +780,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     for (int k = 0; k < 3; ++k) tot += samples_[k].n;
     int maxgrid = 1;
     for (int pr = 0; pr < 2; ++pr) {
-        int occ = residentCtas(pr == 0 ? k_f64_ : k_mixed_, shape_.block[pr]);
+        int occ = residentCtas(pr == 0 ? k_f64_ : k_mixed_, shape_.block[pr], shape_.dsmem[pr]);
         layoutCtas(sms * occ, tot, shape_.block[pr], lay_[pr]);
         maxgrid = std::max(maxgrid, lay_[pr].grid);
     }
@@ -782,6 +788,8 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     int nacc = 2 + 2 * nA + model_.nTheta();
     CT_CUDA(cudaMalloc(&d_partials_, sizeof(double) * (size_t)grid_max_ * nacc));
     CT_CUDA(cudaMalloc(&d_parts_, sizeof(double) * 8));
+    CT_CUDA(cudaMalloc(&d_err_, sizeof(int)));
+    CT_CUDA(cudaMemsetAsync(d_err_, 0, sizeof(int), init_stream_));
     CT_CUDA(cudaMalloc(&d_hscratch_, sizeof(double) * (3 * (size_t)std::max(1, model_.nParams()) + 1)));
     CT_CUDA(cudaStreamSynchronize(init_stream_));
     cudaStreamDestroy(init_stream_);
@@ -803,6 +811,7 @@ Engine::~Engine()
     cudaFree(d_partials_);
     cudaFree(d_parts_);
     cudaFree(d_hscratch_);
+    cudaFree(d_err_);
     cudaFree(d_amp_chain_);
     cudaFree(d_ratio_);
     cudaFree(d_gauss_idx_);
@@ -1039,16 +1048,20 @@ void Engine::computeAngular(int kind)
 {
     DeviceSample& d = samples_[kind];
     long long n = d.n;
+    // table rows padded to a multiple of 256 events: every tile of the fused
+    // kernels starts on a 2 KiB boundary and may be copied whole
+    d.ld = std::max(256LL, (n + 255) / 256 * 256);
+    const long long ld = d.ld;
     int npol = model_.npol;
     size_t nplanes = (size_t)gen_.nplane * npol;
-    size_t b64 = sizeof(double2) * nplanes * std::max(1LL, n);
+    size_t b64 = sizeof(double2) * nplanes * ld;
     CT_CUDA(cudaMalloc(&d.slamp64, b64));
     device_bytes_ += b64;
     if (opt_.mixed_tables) {
         CT_CUDA(cudaMalloc(&d.slamp32, b64 / 2));
         device_bytes_ += b64 / 2;
     }
-    size_t bk = sizeof(double) * std::max<size_t>(1, gen_.slots.size()) * std::max(1LL, n);
+    size_t bk = sizeof(double) * std::max<size_t>(1, gen_.slots.size()) * ld;
     CT_CUDA(cudaMalloc(&d.kin, bk));
     device_bytes_ += bk;
     if (n == 0) return;
@@ -1057,8 +1070,8 @@ void Engine::computeAngular(int kind)
     for (size_t g = 0; g < group_desc_.size(); ++g) {
         AgGroup G;
         std::memcpy(&G, group_desc_[g].data(), sizeof(G));
-        ag_group_kernel<<<(unsigned)((n + 127) / 128), 128, 0, init_stream_>>>(G, T, d.p4, n, d.slamp64, d.slamp32,
-                                                                                 d.kin);
+        ag_group_kernel<<<(unsigned)((n + 127) / 128), 128, 0, init_stream_>>>(G, T, d.p4, n, ld, d.slamp64,
+                                                                                 d.slamp32, d.kin);
         CT_CUDA(cudaGetLastError());
     }
     if (!opt_.keep_momenta) {
@@ -1072,7 +1085,7 @@ void Engine::computeAngular(int kind)
 // fused kernels: 128 x 3 (170 registers, 12 warps per SM; measured 7 % faster
 // than 256 x 1) and 256 x 2 unless CTPWA_F64_BLOCK / CTPWA_F64_MINB /
 // CTPWA_MX_BLOCK / CTPWA_MX_MINB override them (tuning).
-FusedShape fusedShape()
+FusedShape fusedShape(const GeneratedModel& gen)
 {
     FusedShape sh;
     auto get = [](const char* name, int def, int lo, int hi) {
@@ -1088,6 +1101,25 @@ FusedShape fusedShape()
     sh.minb[1] = get("CTPWA_MX_MINB", 2, 1, 16);
     for (int i = 0; i < 2; ++i)
         if (sh.block[i] % 32) throw std::runtime_error("fused block sizes must be multiples of 32");
+    // Staging (CTPWA_STAGE=1): two tile buffers of BLOCK events (angular rows
+    // + kinematic rows) per CTA, filled by bulk copies, used when they fit at
+    // the requested residency next to the static shared memory. Off by
+    // default: the fused kernels are issue-bound, and the per-tile barrier of
+    // the pipeline cost more than the load latency it hid (K+K-pi0 on B200:
+    // mixed 0.879 ms staged vs 0.808 ms direct; plain 1.683 ms staged at
+    // 2 CTAs per SM vs 1.576 ms direct at 3).
+    const int stage_on = get("CTPWA_STAGE", 0, 0, 1);
+    const long long rowb[2] = {16, 8};  // bytes per complex angular value (FP64, FP32)
+    for (int i = 0; i < 2; ++i) {
+        const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
+        const long long bytes =
+            2LL * (npl * rowb[i] + (long long)std::max<size_t>(1, gen.slots.size()) * 8) * sh.block[i];
+        const long long per_sm = 228LL * 1024, per_cta = 227LL * 1024, reserve = 8LL * 1024;
+        if (stage_on && bytes + reserve <= per_cta && (long long)sh.minb[i] * (bytes + reserve) <= per_sm) {
+            sh.stage[i] = 1;
+            sh.dsmem[i] = (int)bytes;
+        }
+    }
     return sh;
 }
 
@@ -1102,7 +1134,9 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     std::vector<std::string> optv = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
                                      "--fmad=true", "-lineinfo"};
     // tuning knobs: block size and minimum resident CTAs per SM of the fused kernels
-    const FusedShape sh = fusedShape();
+    const FusedShape sh = fusedShape(gen);
+    optv.push_back("-DCT_F64_STAGE=" + std::to_string(sh.stage[0]));
+    optv.push_back("-DCT_MX_STAGE=" + std::to_string(sh.stage[1]));
     optv.push_back("-DCT_F64_BLOCK=" + std::to_string(sh.block[0]));
     optv.push_back("-DCT_F64_MINB=" + std::to_string(sh.minb[0]));
     optv.push_back("-DCT_MX_BLOCK=" + std::to_string(sh.block[1]));
@@ -1178,6 +1212,10 @@ void Engine::compileKernel()
     k_part_ = (void*)kpart;
     k_f64_ = (void*)k64;
     k_mixed_ = (void*)kmx;
+    for (int pr = 0; pr < 2; ++pr)
+        if (shape_.dsmem[pr] > 0)
+            CT_CUDA(cudaFuncSetAttribute((const void*)(pr == 0 ? k_f64_ : k_mixed_),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, shape_.dsmem[pr]));
     k_int_ = (void*)kin;
     jit_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -1200,6 +1238,7 @@ struct CtSampleH {
     const double* kin;
     const double* w;
     long long n;
+    long long ld;
     int kind;
     int cta_begin;
     int cta_count;
@@ -1216,6 +1255,7 @@ struct CtArgsH {
     double* consts;
     int cta_base;
     int pad2;
+    int* err;
 };
 
 void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
@@ -1236,6 +1276,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
         s.kin = d.kin;
         s.w = d.w;
         s.n = d.n;
+        s.ld = d.ld;
         s.kind = k;
         s.cta_begin = lay.cta[k][0];
         s.cta_count = lay.cta[k][1];
@@ -1246,6 +1287,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     a.v = d_v_;
     a.partials = d_partials_;
     a.consts = d_consts_;
+    a.err = d_err_;
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
@@ -1253,7 +1295,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     if (!ev_begin_.empty()) CT_CUDA(cudaEventRecord(ev_begin_[slot], stream));
     a.cta_base = 0;
     CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
-                             args, 0, stream));
+                             args, (size_t)shape_.dsmem[precision == kMixed], stream));
     if (!ev_begin_.empty()) {
         CT_CUDA(cudaEventRecord(ev_end_[slot], stream));
         ++ev_count_;
@@ -1282,6 +1324,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     f.out_nll = d_nll;
     f.out_grad = d_grad;
     f.out_parts = d_parts_;
+    f.err = d_err_;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
@@ -1344,7 +1387,8 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     const size_t off_c = off_v + up((size_t)2 * nA);
     const size_t off_p = off_c + up((size_t)std::max(1, gen_.nconst));
     const size_t off_parts = off_p + up((size_t)lay.grid * nacc);
-    const size_t need = off_parts + 8;
+    const size_t off_err = off_parts + 8;  // one int (copy-timeout flag), zeroed by this call
+    const size_t need = off_err + 1;
     const size_t cap = kStaticScratchBytes / sizeof(double);
     if (need > cap)
         throw std::length_error("ctpwa_nll_grad_static: this model needs " + std::to_string(need * sizeof(double)) +
@@ -1357,6 +1401,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     double* s_partials = base + off_p;
     double* s_parts = base + off_parts;
 
+    CT_CUDA(cudaMemsetAsync(base + off_err, 0, sizeof(int), stream));
     ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, s_v);
     CT_CUDA(cudaGetLastError());
     CtArgsH a;
@@ -1370,6 +1415,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
         sm.kin = d.kin;
         sm.w = d.w;
         sm.n = d.n;
+        sm.ld = d.ld;
         sm.kind = k;
         sm.cta_begin = lay.cta[k][0];
         sm.cta_count = lay.cta[k][1];
@@ -1380,12 +1426,13 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     a.v = s_v;
     a.partials = s_partials;
     a.consts = s_consts;
+    a.err = (int*)(base + off_err);
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     a.cta_base = 0;
     CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
-                             args, 0, stream));
+                             args, (size_t)shape_.dsmem[precision == kMixed], stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     f.partials = s_partials;
@@ -1410,6 +1457,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     f.out_nll = d_nll;
     f.out_grad = d_grad;
     f.out_parts = s_parts;
+    f.err = (const int*)(base + off_err);
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
@@ -1434,6 +1482,7 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
         sm.kin = d.kin;
         sm.w = d.w;
         sm.n = d.n;
+        sm.ld = d.ld;
         sm.kind = k;
         sm.cta_begin = lay.cta[k][0];
         sm.cta_count = lay.cta[k][1];
@@ -1444,12 +1493,13 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     a.v = d_v_;
     a.partials = d_partials_;
     a.consts = d_consts_;
+    a.err = d_err_;
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
     a.cta_base = 0;
     CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
-                             args, 0, stream));
+                             args, (size_t)shape_.dsmem[precision == kMixed], stream));
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
     for (int k = 0; k < 3; ++k) {
@@ -1487,6 +1537,7 @@ void Engine::finalizeSums(const double* d_params, const double* d_sums, double* 
     f.out_grad = d_grad;
     f.out_parts = d_parts_;
     f.sums = d_sums;
+    f.err = d_err_;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
@@ -1615,6 +1666,7 @@ void Engine::partialIntegrals(const double* d_params, int kind, double* d_out, c
     a.s[0].kin = d.kin;
     a.s[0].w = d.w;
     a.s[0].n = d.n;
+    a.s[0].ld = d.ld;
     a.s[0].kind = kind;
     a.s[0].cta_count = 1;
     a.nsamp = 1;
@@ -1622,6 +1674,7 @@ void Engine::partialIntegrals(const double* d_params, int kind, double* d_out, c
     a.v = d_v_;
     a.partials = d_partials_;
     a.consts = d_consts_;
+    a.err = d_err_;
     void* pargs[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), pargs, 0, stream));
     // rows of nb sums in the partials table (nacc >= nA >= nb columns per row available)
@@ -1648,6 +1701,7 @@ void Engine::intensity(const double* d_params, int kind, double* d_out, cudaStre
     a.s[0].slamp = d.slamp64;
     a.s[0].kin = d.kin;
     a.s[0].n = d.n;
+    a.s[0].ld = d.ld;
     a.s[0].kind = kind;
     a.s[0].cta_count = 1;
     a.nsamp = 1;
@@ -1655,6 +1709,7 @@ void Engine::intensity(const double* d_params, int kind, double* d_out, cudaStre
     a.v = d_v_;
     a.partials = d_partials_;
     a.consts = d_consts_;
+    a.err = d_err_;
     void* pargs[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), pargs, 0, stream));
     void* args[] = {&a, &d_out};

@@ -15,19 +15,24 @@ namespace ctpwa {
 
 enum Precision : int { kFP64 = 0, kMixed = 1 };
 
-// Launch shape of the plain [0] and mixed [1] fused kernels.
+// Launch shape of the plain [0] and mixed [1] fused kernels: block size,
+// minimum resident CTAs per SM, and whether the event tables are staged
+// through shared memory by bulk copies (dynamic shared memory bytes).
 struct FusedShape {
     int block[2] = {128, 256};
     int minb[2] = {3, 2};
+    int stage[2] = {0, 0};
+    int dsmem[2] = {0, 0};
 };
-FusedShape fusedShape();
+FusedShape fusedShape(const GeneratedModel& gen);
 
 struct DeviceSample {
     long long n = 0;
+    long long ld = 0;          // row stride of the tables below (n padded to 256)
     double* p4 = nullptr;      // SoA [n_final * 4][n]
-    double2* slamp64 = nullptr;  // [nplane * npol][n]
+    double2* slamp64 = nullptr;  // [nplane * npol][ld]
     float2* slamp32 = nullptr;   // mixed-precision copy
-    double* kin = nullptr;     // [nkin][n]
+    double* kin = nullptr;     // [nkin][ld]
     double* w = nullptr;       // weights or nullptr
     double wsum = 0.0;         // sum of weights (or n)
 };
@@ -137,7 +142,8 @@ private:
     double* d_consts_ = nullptr;    // [nconst] parameter-only subexpressions
     double* d_partials_ = nullptr;  // [grid][nacc]
     double* d_parts_ = nullptr;     // [8]
-    double* d_hscratch_ = nullptr;  // Hessian: perturbed params, two gradients, nll [3 nP + 1]
+    double* d_hscratch_ = nullptr;
+    int* d_err_ = nullptr;           // set by a fused kernel whose staged copy did not arrive  // Hessian: perturbed params, two gradients, nll [3 nP + 1]
     int* d_amp_chain_ = nullptr;
     double* d_ratio_ = nullptr;
     int* d_gauss_idx_ = nullptr;
@@ -149,7 +155,7 @@ private:
     CtaLayout lay_[2];   // fused-kernel grid of the plain [0] and mixed [1] forms
     int grid_max_ = 0;   // rows of the partials table
     FusedShape shape_;
-    int residentCtas(void* kernel, int block) const;
+    int residentCtas(void* kernel, int block, int dsmem) const;
     void layoutCtas(int target, long long tot, int block, CtaLayout& lay) const;
 
     cudaStream_t init_stream_ = nullptr;  // initialisation only

@@ -125,3 +125,40 @@ __device__ __forceinline__ float ct_sqrtf(float x)
     const float y1 = fmaf(0.5f * r, e, y0);    // y0 + (x - y0^2) / (2 sqrt x)
     return (x == 0.0f || x == __int_as_float(0x7f800000)) ? x : y1;
 }
+
+// ---- asynchronous bulk copies global -> shared with mbarrier completion ----
+// (cp.async.bulk: the copy engine moves whole contiguous table rows into
+// shared memory while the CTA computes on the previous tile)
+__device__ __forceinline__ unsigned ct_smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void ct_mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(ct_smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void ct_fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void ct_mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ct_smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// dst, src and bytes must be multiples of 16 bytes
+__device__ __forceinline__ void ct_bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     ct_smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(ct_smem_addr(bar))
+                 : "memory");
+}
+// Bounded wait for phase `parity` of an mbarrier: gives up after `limit`
+// polls (each poll may suspend the thread for a short hardware interval) and
+// returns false, so a copy that never completes cannot hang the kernel.
+__device__ __forceinline__ bool ct_mbar_wait(unsigned long long* bar, unsigned parity, unsigned limit)
+{
+    unsigned ok = 0;
+    for (unsigned it = 0; it < limit && !ok; ++it)
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(ct_smem_addr(bar)), "r"(parity)
+            : "memory");
+    return ok != 0;
+}

@@ -43,11 +43,24 @@
 
 #define CT_NACC (2 + 2 * M_NA + M_NTH)
 
+// shared-memory staging of the event tables (host sets them when the two
+// tile buffers fit at the requested residency)
+#ifndef CT_F64_STAGE
+#define CT_F64_STAGE 0
+#endif
+#ifndef CT_MX_STAGE
+#define CT_MX_STAGE 0
+#endif
+#ifndef CT_WAIT_LIMIT
+#define CT_WAIT_LIMIT (1u << 22)
+#endif
+
 struct CtSample {
-    const void* slamp;  // [M_NPLANE * M_NPOL planes][n] of SL2
-    const double* kin;  // [M_NKIN][n]
+    const void* slamp;  // [M_NPLANE * M_NPOL planes][ld] of SL2
+    const double* kin;  // [M_NKIN][ld]
     const double* w;    // per-event weights or nullptr (unit weights)
     long long n;
+    long long ld;       // row stride of slamp and kin: n padded to a multiple of 256
     int kind;           // 0 = phase space, 1 = data, 2 = background
     int cta_begin;
     int cta_count;
@@ -65,6 +78,7 @@ struct CtArgs {
     double* consts;       // [M_NCONST] parameter-only subexpressions of this call
     int cta_base;         // CTA index of this launch's first block (split launches)
     int pad2;
+    int* err;             // set to 1 when a staged copy did not arrive in time
 };
 
 // One thread: the parameter-only part of every lineshape (prologue).
@@ -139,7 +153,7 @@ struct CtLineshape<float> {
 // L: type of the lineshapes, their derivatives and the per-thread gradient
 //    sums
 // PH_ONLY: the launch serves phase-space events only
-template <typename R, typename L, bool PH_ONLY, int BLOCK>
+template <typename R, typename L, bool PH_ONLY, int BLOCK, bool STAGE>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 {
     typedef typename CtVec2<R>::type SL2;
@@ -184,19 +198,21 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         vil[a] = (L)(i - (double)vi[a]);
     }
 
-    const long long stride = (long long)S.cta_count * BLOCK;
-    for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride) {
+    // all per-event work: kvp / slp point at this event's kinematic values and
+    // angular values, consecutive values `ks` / `ss` elements apart
+    auto event = [&](long long e, const double* __restrict__ kvp, long long ks, const SL2* __restrict__ slp,
+                     long long ss) {
         // ---- lineshapes with parameter derivatives ----
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(kin + (long long)k * n + e);
+        for (int k = 0; k < M_NKIN; ++k) kv[k] = kvp[(long long)k * ks];
         L Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
         CtLineshape<L>::eval(kv, sC, sCfh, sCfl, Fr, Fi, dFr, dFi);
 
         // ---- coherent sum over amplitudes ----
         SL2 sl[M_NPLANE * M_NPOL];
 #pragma unroll
-        for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = slamp[(long long)c * n + e];
+        for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = slp[(long long)c * ss];
         R cr[M_NA], ci[M_NA];
 #pragma unroll
         for (int a = 0; a < M_NA; ++a) {
@@ -247,7 +263,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             const double we = wts ? __ldg(wts + e) : 1.0;
             if (f == (R)0) {
                 accd[0] += -log(1e-10) * we;
-                continue;
+                return;
             }
             accd[0] += -log((double)f) * we;
             const R inv = (R)(we / (double)f);
@@ -297,6 +313,69 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             const int a = der_col(k);
             accg[2 * M_NA + der_th(k)] += dFr[k] * Wr[a] - dFi[k] * Wi[a];
         }
+    };
+
+    if constexpr (STAGE) {
+        // Two-buffer pipeline: tile t (BLOCK consecutive events of this CTA's
+        // sample) is copied whole into shared memory by the bulk-copy engine,
+        // one copy per table row, while the CTA computes on tile t - 1. Table
+        // rows are padded to multiples of 256 events, so every copy starts
+        // on a 2 KiB boundary and moves BLOCK elements.
+        constexpr int NPL = M_NPLANE * M_NPOL;
+        constexpr unsigned SLB = BLOCK * sizeof(SL2), KB = BLOCK * sizeof(double);
+        constexpr unsigned BUF = NPL * SLB + M_NKIN * KB;
+        extern __shared__ __align__(128) unsigned char ct_stage[];
+        __shared__ __align__(8) unsigned long long ct_bar[2];
+        const long long first = cta - S.cta_begin, step = S.cta_count;
+        const long long ntiles = (n + BLOCK - 1) / BLOCK;
+        const long long my = first < ntiles ? (ntiles - 1 - first) / step + 1 : 0;
+        auto issue = [&](long long t, int b) {
+            const long long e0 = (first + t * step) * BLOCK;
+            unsigned char* buf = ct_stage + (size_t)b * BUF;
+            ct_mbar_expect_tx(&ct_bar[b], BUF);
+#pragma unroll 1
+            for (int c = 0; c < NPL; ++c) ct_bulk_g2s(buf + (size_t)c * SLB, slamp + (long long)c * S.ld + e0, SLB, &ct_bar[b]);
+#pragma unroll 1
+            for (int k = 0; k < M_NKIN; ++k)
+                ct_bulk_g2s(buf + (size_t)NPL * SLB + (size_t)k * KB, kin + (long long)k * S.ld + e0, KB, &ct_bar[b]);
+        };
+        if (threadIdx.x == 0) {
+            ct_mbar_init(&ct_bar[0], 1);
+            ct_mbar_init(&ct_bar[1], 1);
+            ct_fence_mbar_init();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (my > 0) issue(0, 0);
+            if (my > 1) issue(1, 1);
+        }
+        long long t = 0;
+        for (; t < my; ++t) {
+            const int b = (int)(t & 1);
+            const bool ok = ct_mbar_wait(&ct_bar[b], (unsigned)((t >> 1) & 1), CT_WAIT_LIMIT);
+            const long long e = (first + t * step) * BLOCK + threadIdx.x;
+            if (ok && e < n) {
+                const unsigned char* buf = ct_stage + (size_t)b * BUF;
+                event(e, (const double*)(buf + (size_t)NPL * SLB) + threadIdx.x, BLOCK, (const SL2*)buf + threadIdx.x,
+                      BLOCK);
+            }
+            // every thread is done with buffer b (and agrees whether the copy arrived)
+            if (!__syncthreads_and(ok)) break;
+            if (threadIdx.x == 0 && t + 2 < my) issue(t + 2, b);
+        }
+        if (t < my) {
+            // a copy did not complete in time: flag it, give the other
+            // buffer's copy a bounded chance to land, and stop
+            if (threadIdx.x == 0) {
+                atomicExch(A.err, 1);
+                if (t + 1 < my) ct_mbar_wait(&ct_bar[(t + 1) & 1], (unsigned)(((t + 1) >> 1) & 1), CT_WAIT_LIMIT);
+            }
+            __syncthreads();
+        }
+    } else {
+        const long long stride = (long long)S.cta_count * BLOCK;
+        for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride)
+            event(e, kin + e, S.ld, slamp + e, S.ld);
     }
     ct_block_reduce_store<BLOCK, L>(accd, accg, A.partials + (long long)cta * CT_NACC);
 }
@@ -317,12 +396,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #endif
 extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB) ct_fused_f64(CtArgs a)
 {
-    ct_fused_body<double, double, false, CT_F64_BLOCK>(a);
+    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE != 0>(a);
 }
 // mixed form (FP32 lineshapes and algebra, FP64 logs and sums), all samples
 extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_mixed(CtArgs a)
 {
-    ct_fused_body<float, float, false, CT_MX_BLOCK>(a);
+    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE != 0>(a);
 }
 
 // Partial-wave integrals of sample s[0] (FP64): per resonance block i,
@@ -342,7 +421,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
     for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * n + e);
+        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
         double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
         model_columns(kv, sC, Fr, Fi, dFr, dFi);
         const double we = S.w ? __ldg(S.w + e) : 1.0;
@@ -355,7 +434,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
                 for (int a = blk_site(i); a < blk_site(i) + blk_nsl(i); ++a) {
                     const double vr = __ldg(A.v + 2 * a), vi = __ldg(A.v + 2 * a + 1);
                     const double cr = vr * Fr[a] - vi * Fi[a], ci = vr * Fi[a] + vi * Fr[a];
-                    const double2 x = slamp[(long long)(col_plane(a) * M_NPOL + p) * n + e];
+                    const double2 x = slamp[(long long)(col_plane(a) * M_NPOL + p) * S.ld + e];
                     sr += cr * x.x - ci * x.y;
                     si += cr * x.y + ci * x.x;
                 }
@@ -394,7 +473,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_intensity_f64(CtArgs A
     for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * n + e);
+        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
         double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
         model_columns(kv, sC, Fr, Fi, dFr, dFi);
         double f = 0.0;
@@ -405,7 +484,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_intensity_f64(CtArgs A
             for (int a = 0; a < M_NA; ++a) {
                 double cr = __ldg(A.v + 2 * a) * Fr[a] - __ldg(A.v + 2 * a + 1) * Fi[a];
                 double ci = __ldg(A.v + 2 * a) * Fi[a] + __ldg(A.v + 2 * a + 1) * Fr[a];
-                double2 x = slamp[(long long)(col_plane(a) * M_NPOL + p) * n + e];
+                double2 x = slamp[(long long)(col_plane(a) * M_NPOL + p) * S.ld + e];
                 sr += cr * x.x - ci * x.y;
                 si += cr * x.y + ci * x.x;
             }

@@ -208,3 +208,23 @@ def test_partial_integrals_and_fit_fractions(setups, tmp_path):
                      device="cuda")
     assert float(a2.getPartialIntegrals(q, 3).sum()) > 0
     assert abs(float(a2.getFitFractions(q)[:, 0].sum()) - 1.0) < 1e-12
+
+
+def test_staged_tables_match_direct_loads(tmp_path, monkeypatch):
+    """The fused kernels with the event tables staged through shared memory by
+    bulk copies (CTPWA_STAGE=1) give the same results as with direct loads."""
+    import torch
+    import ctpwa_b200
+
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=70_001, n_data=9_999, n_bkg=777, accept_reject=False, seed=31)
+    direct = ctpwa_b200.analysis(cfg)
+    p = workloads.true_params(direct.getNVector(), direct.getFreeResParams()[0].numpy())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    monkeypatch.setenv("CTPWA_STAGE", "1")
+    monkeypatch.setenv("CTPWA_F64_MINB", "2")  # the plain path's two tile buffers fit at 2 CTAs per SM
+    staged = ctpwa_b200.analysis(cfg)
+    for prec in ("fp64", "mixed"):
+        n0, g0 = direct.getNLLAndGrad(pt, prec)
+        n1, g1 = staged.getNLLAndGrad(pt, prec)
+        assert abs(float(n0) - float(n1)) <= 1e-12 * abs(float(n0)), prec
+        assert float((g0 - g1).abs().max()) <= 1e-10 * float(g0.abs().max()), prec
