@@ -395,11 +395,17 @@ struct Gen {
     Shapes S{G};
     std::map<std::tuple<int, unsigned, unsigned, unsigned>, int> slot_of;
     std::vector<std::vector<double>> tables;  // Hist / Interp tables
-    struct ColOut {
-        int re, im;
+    // One term of an amplitude column: the lineshape product of one group
+    // variant (the base group, or a permutation of identical particles) and
+    // the angular plane it multiplies. Without identical particles every
+    // column has exactly one term.
+    struct TermOut {
+        int col = 0, plane = 0;
+        int re = 0, im = 0;
         std::vector<std::pair<int, std::pair<int, int>>> der;  // theta -> (d re, d im)
     };
-    std::vector<ColOut> cols;
+    std::vector<TermOut> cols;  // terms, in block / SL / variant order
+    std::vector<int> blk_term0, blk_nterm;
     std::vector<std::pair<int, int>> extra;  // opaque per-event values: (table id, mass node) placeholders
 
     explicit Gen(const Model& mm) : m(mm) {}
@@ -513,10 +519,11 @@ struct Gen {
         return par;
     }
 
-    Cx nodeFactor(const Block& b, const Group& g, int ni, int s, const std::vector<std::vector<int>>& par)
+    // gi: the group (base or permutation variant) whose kinematics are read
+    Cx nodeFactor(const Block& b, int gi, int ni, int s, const std::vector<std::vector<int>>& par)
     {
+        const Group& g = m.groups[gi];
         const ModelNode& n = g.nodes[ni];
-        int gi = b.group;
         int L = n.sls[g.sl_combs[s][ni]].L;
         if (b.free_path) {
             int match = -1;
@@ -917,35 +924,37 @@ std::string Gen::emit()
         return evs.str();
     };
 
-    std::vector<std::pair<int, int>> der_entries;
+    std::vector<std::pair<int, int>> der_entries;  // (term, theta)
     for (size_t a = 0; a < cols.size(); ++a)
         for (const auto& d : cols[a].der) der_entries.push_back({(int)a, d.first});
     const int k = (int)der_entries.size();
     out.nder = k;
     out.nconst = ncon;
     std::ostringstream h;
+    auto table = [&](const char* name, const std::vector<int>& v) {
+        h << "__device__ __forceinline__ int " << name << "(int i) {\n  switch (i) {\n";
+        for (size_t i = 0; i < v.size(); ++i) h << "  case " << i << ": return " << v[i] << ";\n";
+        h << "  default: return 0;\n  }\n}\n";
+    };
     h << "// generated by ctpwa_b200 codegen: model-specific lineshape products\n#pragma once\n";
-    h << "#define M_NA " << m.nAmp() << "\n#define M_NPOL " << m.npol << "\n#define M_NPLANE " << out.nplane
-      << "\n#define M_NKIN " << out.slots.size() << "\n#define M_NTH " << m.nTheta() << "\n#define M_NDER " << k
-      << "\n#define M_NCONST " << ncon << "\n";
-    h << "__device__ __forceinline__ int col_plane(int a) {\n  switch (a) {\n";
-    for (const auto& b : m.blocks)
-        for (int s = 0; s < m.groups[b.group].nSL(); ++s)
-            h << "  case " << b.site + s << ": return " << out.group_plane0[b.group] + s << ";\n";
-    h << "  default: return 0;\n  }\n}\n";
-    // resonance blocks (partial waves of the fit fractions): first column and
-    // number of SL combinations of each
+    h << "#define M_NA " << m.nAmp() << "\n#define M_NTERM " << cols.size() << "\n#define M_NPOL " << m.npol
+      << "\n#define M_NPLANE " << out.nplane << "\n#define M_NKIN " << out.slots.size() << "\n#define M_NTH "
+      << m.nTheta() << "\n#define M_NDER " << k << "\n#define M_NCONST " << ncon << "\n";
+    // terms: amplitude column and angular plane of each
+    std::vector<int> tcol, tplane;
+    for (const auto& t : cols) {
+        tcol.push_back(t.col);
+        tplane.push_back(t.plane);
+    }
+    table("term_col", tcol);
+    table("term_plane", tplane);
+    // resonance blocks (partial waves of the fit fractions): their terms
     h << "#define M_NBLK " << m.blocks.size() << "\n";
-    h << "__device__ __forceinline__ int blk_site(int i) {\n  switch (i) {\n";
-    for (size_t i = 0; i < m.blocks.size(); ++i) h << "  case " << i << ": return " << m.blocks[i].site << ";\n";
-    h << "  default: return 0;\n  }\n}\n";
-    h << "__device__ __forceinline__ int blk_nsl(int i) {\n  switch (i) {\n";
-    for (size_t i = 0; i < m.blocks.size(); ++i)
-        h << "  case " << i << ": return " << m.groups[m.blocks[i].group].nSL() << ";\n";
-    h << "  default: return 0;\n  }\n}\n";
-    h << "__device__ __forceinline__ int der_col(int k) {\n  switch (k) {\n";
-    for (size_t q = 0; q < der_entries.size(); ++q) h << "  case " << q << ": return " << der_entries[q].first << ";\n";
-    h << "  default: return 0;\n  }\n}\n";
+    table("blk_term0", blk_term0);
+    table("blk_nterm", blk_nterm);
+    std::vector<int> dterm;
+    for (const auto& d : der_entries) dterm.push_back(d.first);
+    table("der_term", dterm);
     h << "__device__ __forceinline__ int der_th(int k) {\n  switch (k) {\n";
     for (size_t q = 0; q < der_entries.size(); ++q) h << "  case " << q << ": return " << der_entries[q].second << ";\n";
     h << "  default: return 0;\n  }\n}\n";
@@ -984,7 +993,6 @@ GeneratedModel generateModel(const Model& m)
     }
     g.out.nplane = pl;
     g.out.npol = m.npol;
-    g.cols.resize(m.nAmp());
     for (const auto& b : m.blocks) {
         const Group& gr = m.groups[b.group];
         auto par = g.params(b);
@@ -993,18 +1001,26 @@ GeneratedModel generateModel(const Model& m)
             for (const auto& r : b.res)
                 for (int t : r.theta)
                     if (t >= 0 && std::find(ths.begin(), ths.end(), t) == ths.end()) ths.push_back(t);
-        for (int s = 0; s < gr.nSL(); ++s) {
-            Cx F = g.G.c(1.0);
-            for (size_t ni = 0; ni < gr.nodes.size(); ++ni) F = g.G.cmul(F, g.nodeFactor(b, gr, (int)ni, s, par));
-            auto& col = g.cols[b.site + s];
-            col.re = F.re;
-            col.im = F.im;
-            for (int t : ths) {
-                int dr = g.G.deriv(F.re, t), di = g.G.deriv(F.im, t);
-                if (g.G.isConst(dr) && g.G.val(dr) == 0.0 && g.G.isConst(di) && g.G.val(di) == 0.0) continue;
-                col.der.push_back({t, {dr, di}});
+        std::vector<int> vars = {b.group};
+        for (int v : gr.variants) vars.push_back(v);
+        g.blk_term0.push_back((int)g.cols.size());
+        for (int s = 0; s < gr.nSL(); ++s)
+            for (int v : vars) {
+                Cx F = g.G.c(m.groups[v].sign);
+                for (size_t ni = 0; ni < gr.nodes.size(); ++ni) F = g.G.cmul(F, g.nodeFactor(b, v, (int)ni, s, par));
+                Gen::TermOut t;
+                t.col = b.site + s;
+                t.plane = g.out.group_plane0[v] + s;
+                t.re = F.re;
+                t.im = F.im;
+                for (int th : ths) {
+                    int dr = g.G.deriv(F.re, th), di = g.G.deriv(F.im, th);
+                    if (g.G.isConst(dr) && g.G.val(dr) == 0.0 && g.G.isConst(di) && g.G.val(di) == 0.0) continue;
+                    t.der.push_back({th, {dr, di}});
+                }
+                g.cols.push_back(t);
             }
-        }
+        g.blk_nterm.push_back((int)g.cols.size() - g.blk_term0.back());
     }
     g.out.header = g.emit();
     return g.out;

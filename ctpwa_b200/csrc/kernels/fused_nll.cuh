@@ -2,9 +2,11 @@
 //
 // Compiled by NVRTC for sm_100a together with a generated header "model.cuh"
 // that supplies, for one physics model:
-//   M_NA, M_NPOL, M_NPLANE, M_NKIN, M_NTH, M_NDER     sizes
-//   col_plane(a)   angular plane (group, SL combination) of amplitude column a
-//   der_col(k), der_th(k)   column / theta index of derivative entry k
+//   M_NA, M_NTERM, M_NPOL, M_NPLANE, M_NKIN, M_NTH, M_NDER     sizes
+//   term_col(t), term_plane(t)   amplitude column and angular plane (group
+//       variant, SL combination) of term t: a column is the sum of its terms
+//       (one term, or one per permutation of identical particles)
+//   der_term(k), der_th(k)   term / theta index of derivative entry k
 //   model_prologue(theta, C)   parameter-only subexpressions, once per call
 //   model_columns(kin, C, Fr, Fi, dFr, dFi)   lineshape products F_a and their
 //       theta derivatives for one event (straight-line generated code, FP64)
@@ -206,27 +208,29 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
         for (int k = 0; k < M_NKIN; ++k) kv[k] = kvp[(long long)k * ks];
-        L Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
+        L Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
         CtLineshape<L>::eval(kv, sC, sCfh, sCfl, Fr, Fi, dFr, dFi);
 
         // ---- coherent sum over amplitudes ----
         SL2 sl[M_NPLANE * M_NPOL];
 #pragma unroll
         for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = slp[(long long)c * ss];
-        R cr[M_NA], ci[M_NA];
+        // c_t = v_col(t) F_t per term (one per column, more with identical particles)
+        R cr[M_NTERM], ci[M_NTERM];
 #pragma unroll
-        for (int a = 0; a < M_NA; ++a) {
+        for (int t = 0; t < M_NTERM; ++t) {
+            const int a = term_col(t);
             if constexpr (sizeof(L) == 4) {
                 // Each product of a per-event value with a coupling is rounded
                 // once, from the full-precision coupling (hi + lo): rounding the
                 // product with the FP32 coupling alone would bias the sample
                 // mean by ~1e-9 (both factors on the FP32 grid), which the
                 // normalisation term multiplies by the data weight sum.
-                cr[a] = fmaf(Fr[a], vr[a], Fr[a] * vrl[a]) - fmaf(Fi[a], vi[a], Fi[a] * vil[a]);
-                ci[a] = fmaf(Fi[a], vr[a], Fi[a] * vrl[a]) + fmaf(Fr[a], vi[a], Fr[a] * vil[a]);
+                cr[t] = fmaf(Fr[t], vr[a], Fr[t] * vrl[a]) - fmaf(Fi[t], vi[a], Fi[t] * vil[a]);
+                ci[t] = fmaf(Fi[t], vr[a], Fi[t] * vrl[a]) + fmaf(Fr[t], vi[a], Fr[t] * vil[a]);
             } else {
-                cr[a] = (R)(vr[a] * Fr[a] - vi[a] * Fi[a]);
-                ci[a] = (R)(vr[a] * Fi[a] + vi[a] * Fr[a]);
+                cr[t] = (R)(vr[a] * Fr[t] - vi[a] * Fi[t]);
+                ci[t] = (R)(vr[a] * Fi[t] + vi[a] * Fr[t]);
             }
         }
         R Sr[M_NPOL], Si[M_NPOL];
@@ -235,10 +239,10 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         for (int p = 0; p < M_NPOL; ++p) {
             R sr = (R)0, sim = (R)0;
 #pragma unroll
-            for (int a = 0; a < M_NA; ++a) {
-                SL2 x = sl[col_plane(a) * M_NPOL + p];
-                sr += cr[a] * x.x - ci[a] * x.y;
-                sim += cr[a] * x.y + ci[a] * x.x;
+            for (int t = 0; t < M_NTERM; ++t) {
+                SL2 x = sl[term_plane(t) * M_NPOL + p];
+                sr += cr[t] * x.x - ci[t] * x.y;
+                sim += cr[t] * x.y + ci[t] * x.x;
             }
             Sr[p] = sr;
             Si[p] = sim;
@@ -290,28 +294,28 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             Tr[c] = tr;
             Ti[c] = ti;
         }
-        // v-gradient: conj(F_a) T
+        // v-gradient: sum over the column's terms of conj(F_t) T_plane(t)
 #pragma unroll
-        for (int a = 0; a < M_NA; ++a) {
-            const int c = col_plane(a);
-            const L fr = Fr[a], fi = Fi[a];
+        for (int t = 0; t < M_NTERM; ++t) {
+            const int a = term_col(t), c = term_plane(t);
+            const L fr = Fr[t], fi = Fi[t];
             const L tr = (L)Tr[c], ti = (L)Ti[c];
             accg[2 * a] += gscale * (fr * tr + fi * ti);
             accg[2 * a + 1] += gscale * (fr * ti - fi * tr);
         }
-        // theta-gradient: Re(v_a dF conj(T)) = Re(dF W_a), W_a = v_a conj(T_plane(a))
-        L Wr[M_NA], Wi[M_NA];
+        // theta-gradient: Re(v dF_t conj(T)) = Re(dF_t W_t), W_t = v_col(t) conj(T_plane(t))
+        L Wr[M_NTERM], Wi[M_NTERM];
 #pragma unroll
-        for (int a = 0; a < M_NA; ++a) {
-            const int c = col_plane(a);
+        for (int t = 0; t < M_NTERM; ++t) {
+            const int a = term_col(t), c = term_plane(t);
             const L tr = (L)Tr[c], ti = (L)Ti[c];
-            Wr[a] = tscale * (vr[a] * tr + vi[a] * ti);
-            Wi[a] = tscale * (vi[a] * tr - vr[a] * ti);
+            Wr[t] = tscale * (vr[a] * tr + vi[a] * ti);
+            Wi[t] = tscale * (vi[a] * tr - vr[a] * ti);
         }
 #pragma unroll
         for (int k = 0; k < M_NDER; ++k) {
-            const int a = der_col(k);
-            accg[2 * M_NA + der_th(k)] += dFr[k] * Wr[a] - dFi[k] * Wi[a];
+            const int t = der_term(k);
+            accg[2 * M_NA + der_th(k)] += dFr[k] * Wr[t] - dFi[k] * Wi[t];
         }
     };
 
@@ -422,7 +426,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
         for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
-        double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
+        double Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
         model_columns(kv, sC, Fr, Fi, dFr, dFi);
         const double we = S.w ? __ldg(S.w + e) : 1.0;
 #pragma unroll
@@ -431,10 +435,11 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
 #pragma unroll
             for (int p = 0; p < M_NPOL; ++p) {
                 double sr = 0.0, si = 0.0;
-                for (int a = blk_site(i); a < blk_site(i) + blk_nsl(i); ++a) {
+                for (int t = blk_term0(i); t < blk_term0(i) + blk_nterm(i); ++t) {
+                    const int a = term_col(t);
                     const double vr = __ldg(A.v + 2 * a), vi = __ldg(A.v + 2 * a + 1);
-                    const double cr = vr * Fr[a] - vi * Fi[a], ci = vr * Fi[a] + vi * Fr[a];
-                    const double2 x = slamp[(long long)(col_plane(a) * M_NPOL + p) * S.ld + e];
+                    const double cr = vr * Fr[t] - vi * Fi[t], ci = vr * Fi[t] + vi * Fr[t];
+                    const double2 x = slamp[(long long)(term_plane(t) * M_NPOL + p) * S.ld + e];
                     sr += cr * x.x - ci * x.y;
                     si += cr * x.y + ci * x.x;
                 }
@@ -474,17 +479,18 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_intensity_f64(CtArgs A
         double kv[M_NKIN > 0 ? M_NKIN : 1];
 #pragma unroll
         for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
-        double Fr[M_NA], Fi[M_NA], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
+        double Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
         model_columns(kv, sC, Fr, Fi, dFr, dFi);
         double f = 0.0;
 #pragma unroll
         for (int p = 0; p < M_NPOL; ++p) {
             double sr = 0.0, si = 0.0;
 #pragma unroll
-            for (int a = 0; a < M_NA; ++a) {
-                double cr = __ldg(A.v + 2 * a) * Fr[a] - __ldg(A.v + 2 * a + 1) * Fi[a];
-                double ci = __ldg(A.v + 2 * a) * Fi[a] + __ldg(A.v + 2 * a + 1) * Fr[a];
-                double2 x = slamp[(long long)(col_plane(a) * M_NPOL + p) * S.ld + e];
+            for (int t = 0; t < M_NTERM; ++t) {
+                const int a = term_col(t);
+                double cr = __ldg(A.v + 2 * a) * Fr[t] - __ldg(A.v + 2 * a + 1) * Fi[t];
+                double ci = __ldg(A.v + 2 * a) * Fi[t] + __ldg(A.v + 2 * a + 1) * Fr[t];
+                double2 x = slamp[(long long)(term_plane(t) * M_NPOL + p) * S.ld + e];
                 sr += cr * x.x - ci * x.y;
                 si += cr * x.y + ci * x.x;
             }

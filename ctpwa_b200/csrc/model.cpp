@@ -215,6 +215,97 @@ struct AmpMapEntry {
 
 }  // namespace
 
+namespace {
+
+// Permutation variants of groups with identical final-state particles,
+// following AmpCasDecay::buildPermTopologies (src/AmpGen.cu:194-405): the
+// amplitude is summed over the full permutation group of each identical
+// group's members present in the chain (the stabiliser swaps of two
+// identical daughters of one decay step included), with sgn(permutation) for
+// fermions and +1 for bosons. Several identical groups in one chain combine
+// as the reference does: the non-identity elements of the groups are
+// multiplied out pairwise (src/AmpGen.cu:366-385). Members that are
+// intermediate resonances (whole subtrees permuted) are not supported.
+void addIdenticalVariants(const Config& cfg, Model& m)
+{
+    const int nbase = (int)m.groups.size();
+    for (int gi = 0; gi < nbase; ++gi) {
+        const Group& G = m.groups[gi];
+        std::map<std::string, std::vector<int>> members;  // identical group -> particle indices
+        std::map<std::string, bool> boson;
+        for (size_t i = 0; i < G.particle_names.size(); ++i) {
+            const Particle* p = cfg.findParticle(G.particle_names[i]);
+            if (!p || p->identical_group.empty() || G.input_slot[i] == -1) continue;
+            members[p->identical_group].push_back((int)i);
+            boson[p->identical_group] = !p->is_fermion();
+        }
+        std::vector<std::vector<int>> maps;  // non-identity variants: input_slot arrays
+        std::vector<double> signs;
+        bool first = true;
+        for (const auto& kv : members) {
+            const std::vector<int>& mem = kv.second;
+            if (mem.size() < 2) continue;
+            for (int i : mem)
+                if (G.input_slot[i] < 0)
+                    throw std::runtime_error("chain " + G.chain_name + ": identical particle " + G.particle_names[i] +
+                                             " is not a final-state particle (subtree permutations are not supported)");
+            const int n = (int)mem.size();
+            std::vector<int> perm(n);
+            for (int i = 0; i < n; ++i) perm[i] = i;
+            std::vector<std::vector<int>> gmaps;
+            std::vector<double> gsigns;
+            while (std::next_permutation(perm.begin(), perm.end())) {
+                // member i reads the momentum of member perm[i]
+                std::vector<int> slots(G.input_slot.size(), 0);
+                int inv = 0;
+                for (int i = 0; i < n; ++i)
+                    for (int j = i + 1; j < n; ++j)
+                        if (perm[i] > perm[j]) ++inv;
+                gmaps.push_back({});
+                for (int i = 0; i < n; ++i) gmaps.back().push_back(perm[i]);
+                gsigns.push_back(boson[kv.first] ? 1.0 : ((inv % 2) ? -1.0 : 1.0));
+            }
+            // as slot arrays over this identical group only (identity elsewhere)
+            std::vector<std::vector<int>> gslots;
+            for (const auto& pm : gmaps) {
+                std::vector<int> sl = G.input_slot;
+                for (int i = 0; i < n; ++i) sl[mem[i]] = G.input_slot[mem[pm[i]]];
+                gslots.push_back(sl);
+            }
+            if (first) {
+                maps = gslots;
+                signs = gsigns;
+                first = false;
+            } else {
+                std::vector<std::vector<int>> nm;
+                std::vector<double> ns;
+                for (size_t a = 0; a < maps.size(); ++a)
+                    for (size_t b = 0; b < gslots.size(); ++b) {
+                        std::vector<int> merged = gslots[b];
+                        for (const auto& kv2 : members)
+                            if (kv2.first != kv.first && kv2.second.size() >= 2)
+                                for (int i : kv2.second) merged[i] = maps[a][i];
+                        nm.push_back(merged);
+                        ns.push_back(signs[a] * gsigns[b]);
+                    }
+                maps = std::move(nm);
+                signs = std::move(ns);
+            }
+        }
+        for (size_t v = 0; v < maps.size(); ++v) {
+            Group var = m.groups[gi];
+            var.variants.clear();
+            var.input_slot = maps[v];
+            var.base = gi;
+            var.sign = signs[v];
+            m.groups.push_back(var);
+            m.groups[gi].variants.push_back((int)m.groups.size() - 1);
+        }
+    }
+}
+
+}  // namespace
+
 Model buildModel(const Config& cfg, int fit_mode)
 {
     if (!cfg.valid()) throw std::runtime_error("analysis not initialized: invalid or missing config file");
@@ -357,20 +448,6 @@ Model buildModel(const Config& cfg, int fit_mode)
             combs = std::move(t);
         }
 
-        // identical-particle symmetrisation (src/AmpGen.cu:194-405) is not built
-        {
-            std::set<std::string> cp;
-            for (const auto& st : chain.decay_steps) {
-                cp.insert(st.mother);
-                for (const auto& d : st.daughters) cp.insert(d);
-            }
-            std::map<std::string, int> cnt;
-            for (const auto& p : m.particles)
-                if (!p.identical_group.empty() && cp.count(p.name)) cnt[p.identical_group]++;
-            for (const auto& kv : cnt)
-                if (kv.second >= 2)
-                    throw std::runtime_error("identical-particle symmetrisation (Constraints.identical) is not supported");
-        }
 
         for (const auto& comb : combs) {
             Group g;
@@ -869,6 +946,8 @@ Model buildModel(const Config& cfg, int fit_mode)
         for (const auto& s : m.slots) m.param_names.push_back(s.name);
     }
 
+    addIdenticalVariants(cfg, m);
+
     // ---- gauss_constr (src/Analysis.cu:4003-4020) ----
     for (size_t s = 0; s < m.slots.size(); ++s) {
         auto it = cfg.gauss_constr.find(m.slots[s].name);
@@ -934,6 +1013,7 @@ std::string modelToJson(const Model& m)
         s += ",\"particles\":" + jarr(g.particle_names, jstr);
         s += ",\"spins\":" + jarr(g.particle_spin, jint);
         s += ",\"input_slot\":" + jarr(g.input_slot, jint);
+        s += ",\"base\":" + jint(g.base) + ",\"sign\":" + jnum(g.sign) + ",\"variants\":" + jarr(g.variants, jint);
         s += ",\"sum_of\":" + jarr(g.sum_of, [](const std::pair<int, int>& p) {
             return "[" + jint(p.first) + "," + jint(p.second) + "]";
         });

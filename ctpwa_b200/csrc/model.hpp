@@ -66,6 +66,14 @@ struct Group {
     std::vector<int> input_slot;
     std::vector<std::pair<int, int>> sum_of;
     std::vector<int> build_order;  // particle indices in an order where sums are ready
+    // Identical-particle symmetrisation (src/AmpGen.cu:194-405): a group whose
+    // chain contains identical final-state particles has permutation
+    // variants, each a copy of the group reading permuted final-state slots
+    // (appended after all base groups). A block's amplitude is the signed sum
+    // of its base group's and its variants' products.
+    int base = -1;              // for a variant: index of its base group
+    double sign = 1.0;          // for a variant: +1 (bosons) or sgn(permutation) (fermions)
+    std::vector<int> variants;  // for a base group: indices of its variants
     int nSL() const { return (int)sl_combs.size(); }
 };
 

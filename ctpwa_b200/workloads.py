@@ -122,11 +122,42 @@ Resonances:
     free: [0, 1, 2]
     expr: "Flatte(mass, gKK, gpipi, 0.493677, 0.493677, 0.13957, 0.13957) * Bf(1, q, q0, 3.0)"
 """,
+    # identical final-state particles (K_S K_S): every chain is summed over the
+    # exchange of the two K_S (Constraints.identical)
+    "ksks": """Particles:
+  Jpsi: {J: 1, P: -1, mass: 3.0969}
+  Ks1:  {J: 0, P: -1, mass: 0.497611}
+  Ks2:  {J: 0, P: -1, mass: 0.497611}
+  pi0:  {J: 0, P: -1, mass: 0.13495}
+Data:
+  order: [Ks1, Ks2, pi0]
+  data: [npy, "@DATA@"]
+  phsp: [npy, "@PHSP@"]
+@BKG@DecayChains:
+  kst:
+    Jpsi: [[Ks2, R_K]]
+    R_K: [Ks1, pi0]
+    intermediates:
+      R_K:
+        - [J: 1, P: -1]: [Kst892]
+  f2:
+    Jpsi: [[pi0, R_KK]]
+    R_KK: [Ks1, Ks2]
+    intermediates:
+      R_KK:
+        - [J: 2, P: 1]: [f2_1525]
+Resonances:
+  Kst892:  {J: 1, P: -1, model: BWR, parameters: [0.8955, 0.047], free: [0, 1]}
+  f2_1525: {J: 2, P: 1, model: BWR, parameters: [1.5174, 0.086], free: [0, 1]}
+Constraints:
+  identical: [[Ks1, Ks2]]
+""",
 }
 MASSES = {
     "pipi_rho": (M_PIC, M_PIC, M_PI0),
     "pipi_3rho": (M_PIC, M_PIC, M_PI0),
     "kkpi": (M_K, M_K, M_PI0),
+    "ksks": (0.497611, 0.497611, M_PI0),
 }
 
 # sizes (phsp, data, bkg, bkg weight) of the measured configurations
@@ -134,6 +165,7 @@ SIZES = {
     "pipi_rho": (200_000, 20_000, 0, None),
     "pipi_3rho": (5_000_000, 500_000, 50_000, 0.8),
     "kkpi": (10_000_000, 1_000_000, 100_000, 0.3),
+    "ksks": (1_000_000, 100_000, 0, None),
 }
 
 

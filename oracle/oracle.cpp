@@ -407,19 +407,25 @@ void evalSample(const Oracle& o, int kind, const std::vector<cplx>& v, const dou
             for (size_t bi = 0; bi < m.blocks.size(); ++bi) {
                 const Block& b = m.blocks[bi];
                 const Group& g = m.groups[b.group];
-                const LV* pm = &S.mom[b.group][(size_t)e * g.particle_names.size()];
-                std::vector<LV> pv(pm, pm + g.particle_names.size());
-                const cplx* sl = &S.slamp[b.group][(size_t)e * g.nSL() * npol];
-                for (int s = 0; s < g.nSL(); ++s) {
-                    CD F = blockFactor(m, b, bps[bi], o.expr[bi], s, pv);
-                    int a_idx = b.site + s;
-                    cplx Fv(F.re.v, F.im.v);
-                    for (int pp = 0; pp < npol; ++pp) {
-                        cplx amp = Fv * sl[s * npol + pp];
-                        A[pp * nA + a_idx] = amp;
-                        for (size_t k = 0; k < bps[bi].local_to_theta.size(); ++k) {
-                            cplx dF(F.re.g[k], F.im.g[k]);
-                            dS[pp * nT + bps[bi].local_to_theta[k]] += v[a_idx] * dF * sl[s * npol + pp];
+                // base group and its identical-particle permutations (src/AmpGen.cu:194-405)
+                std::vector<int> vars = {b.group};
+                for (int vg : g.variants) vars.push_back(vg);
+                for (int gv : vars) {
+                    const LV* pm = &S.mom[gv][(size_t)e * g.particle_names.size()];
+                    std::vector<LV> pv(pm, pm + g.particle_names.size());
+                    const cplx* sl = &S.slamp[gv][(size_t)e * g.nSL() * npol];
+                    const double sign = m.groups[gv].sign;
+                    for (int s = 0; s < g.nSL(); ++s) {
+                        CD F = blockFactor(m, b, bps[bi], o.expr[bi], s, pv);
+                        int a_idx = b.site + s;
+                        cplx Fv(sign * F.re.v, sign * F.im.v);
+                        for (int pp = 0; pp < npol; ++pp) {
+                            cplx amp = Fv * sl[s * npol + pp];
+                            A[pp * nA + a_idx] += amp;
+                            for (size_t k = 0; k < bps[bi].local_to_theta.size(); ++k) {
+                                cplx dF(sign * F.re.g[k], sign * F.im.g[k]);
+                                dS[pp * nT + bps[bi].local_to_theta[k]] += v[a_idx] * dF * sl[s * npol + pp];
+                            }
                         }
                     }
                 }
@@ -628,13 +634,21 @@ int orc_columns(void* h, int k, const double* theta, double* out)
         for (size_t bi = 0; bi < m.blocks.size(); ++bi) {
             const Block& b = m.blocks[bi];
             const Group& g = m.groups[b.group];
-            const LV* pm = &S.mom[b.group][(size_t)e * g.particle_names.size()];
-            std::vector<LV> pv(pm, pm + g.particle_names.size());
-            const cplx* sl = &S.slamp[b.group][(size_t)e * g.nSL() * npol];
-            for (int s = 0; s < g.nSL(); ++s) {
-                CD F = blockFactor(m, b, bps[bi], o->expr[bi], s, pv);
-                for (int pp = 0; pp < npol; ++pp)
-                    A[((size_t)e * npol + pp) * nA + b.site + s] = cplx(F.re.v, F.im.v) * sl[s * npol + pp];
+            for (int s = 0; s < g.nSL(); ++s)
+                for (int pp = 0; pp < npol; ++pp) A[((size_t)e * npol + pp) * nA + b.site + s] = 0.0;
+            // base group and its identical-particle permutations (src/AmpGen.cu:194-405)
+            std::vector<int> vars = {b.group};
+            for (int v : g.variants) vars.push_back(v);
+            for (int gv : vars) {
+                const LV* pm = &S.mom[gv][(size_t)e * g.particle_names.size()];
+                std::vector<LV> pv(pm, pm + g.particle_names.size());
+                const cplx* sl = &S.slamp[gv][(size_t)e * g.nSL() * npol];
+                const double sign = m.groups[gv].sign;
+                for (int s = 0; s < g.nSL(); ++s) {
+                    CD F = blockFactor(m, b, bps[bi], o->expr[bi], s, pv);
+                    for (int pp = 0; pp < npol; ++pp)
+                        A[((size_t)e * npol + pp) * nA + b.site + s] += sign * cplx(F.re.v, F.im.v) * sl[s * npol + pp];
+                }
             }
         }
     }
