@@ -391,6 +391,72 @@ class analysis:
                 errors = np.sqrt(np.maximum(np.einsum("ij,jk,ik->i", J, cov, J), 0.0))
         return torch.tensor(np.stack([center, errors], axis=1), dtype=torch.float64)
 
+    def writeResult(self, params: torch.Tensor, filename: str, is_saved_weight: int = 0, waves=()):
+        """Fit-result export (reference analysis::writeResult, src/Analysis.cu:1355-1700)
+        as a NumPy .npz file (ROOT is not available): `legends` (block names),
+        `interference` (summed 2 Re(P_i conj P_j) over phase space, diagonal
+        2|P_i|^2), `data_integral` (W_data - W_bkg), `phsp_integral` (sum of
+        the per-event totals, of the blocks in `waves` when given) and
+        `norm_factor`; with is_saved_weight=1 also per phase-space event
+        `totalweight`, `weight_<block>` and `interf_<i>_<j>` (i < j), scaled
+        to the data yield like the reference's TTree branches."""
+        import numpy as np
+
+        p = self._check_params(params)
+        nb = self.getNBlocks()
+        names = DecayInfo.__new__(DecayInfo)
+        names._m = self.getModel()
+        legends = names.resonanceNames()
+        ld = int(self._lib.ctpwa_table_stride(self._h, 0))
+        n = self.getNEvents()[0]
+        npair = nb * (nb + 1) // 2
+        dev = p.device
+        total = torch.empty(ld, dtype=torch.float64, device=dev)
+        partial = torch.empty(nb * ld, dtype=torch.float64, device=dev)
+        interf = torch.empty(npair, dtype=torch.float64, device=dev)
+        interf_ev = torch.empty(max(1, nb * (nb - 1) // 2) * ld, dtype=torch.float64, device=dev) \
+            if is_saved_weight else None
+        mask = None
+        if waves:
+            for w in waves:
+                if not 0 <= int(w) < nb:
+                    raise RuntimeError(f"waves index out of range: {w} (partials = {nb})")
+            mask = (ctypes.c_int * nb)(*[1 if i in set(int(w) for w in waves) else 0 for i in range(nb)])
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = self._lib.ctpwa_export_weights(self._h, p.data_ptr(), mask, total.data_ptr(), partial.data_ptr(),
+                                            interf_ev.data_ptr() if interf_ev is not None else None,
+                                            interf.data_ptr(), ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        # data yield: sum of data weights minus the background weight sum
+        self._eval(p, 0)
+        parts = self.lastParts()
+        W_data, W_bkg, n_bkg = parts[3], parts[4], self.getNEvents()[2]
+        data_integral = W_data - (W_bkg if W_bkg > 0 else n_bkg) if n_bkg > 0 else W_data
+        tot = total[:n].cpu().numpy()
+        phsp_integral = float(tot.sum())
+        norm = data_integral / phsp_integral if phsp_integral != 0 else 0.0
+        packed = interf.cpu().numpy()
+        M = np.zeros((nb, nb))
+        for i in range(nb):
+            for j in range(i, nb):
+                M[i, j] = M[j, i] = packed[i * nb - i * (i - 1) // 2 + (j - i)]
+        out = {"legends": np.array(legends), "interference": M, "data_integral": data_integral,
+               "phsp_integral": phsp_integral, "norm_factor": norm}
+        if is_saved_weight:
+            out["totalweight"] = tot * norm
+            part = partial.view(nb, ld)[:, :n].cpu().numpy() * norm
+            for i in range(nb):
+                out[f"weight_{i}"] = part[i]
+            ev = interf_ev.view(-1, ld)[:, :n].cpu().numpy() * norm
+            k = 0
+            for i in range(nb):
+                for j in range(i + 1, nb):
+                    out[f"interf_{i}_{j}"] = ev[k]
+                    k += 1
+        np.savez(filename, **out)
+        return out
+
     def getIntensity(self, params: torch.Tensor, kind: int = 1) -> torch.Tensor:
         """Per-event intensities (float64 CUDA [n]) of sample kind 0 = phase space, 1 = data, 2 = background."""
         p = self._check_params(params)

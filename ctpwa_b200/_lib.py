@@ -22,6 +22,10 @@ SIGNATURES = {
     "ctpwa_n_blocks": (ctypes.c_int, [ctypes.c_void_p]),
     "ctpwa_partial_integrals": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                ctypes.c_void_p]),
+    "ctpwa_table_stride": (ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int]),
+    "ctpwa_export_weights": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
     "ctpwa_sums_size": (ctypes.c_int, [ctypes.c_void_p]),
     "ctpwa_shard_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                         ctypes.c_void_p]),

@@ -180,6 +180,26 @@ int ctpwa_partial_integrals(ctpwa_handle* h, const double* d_params, int kind, d
     return CTPWA_OK;
 }
 
+long long ctpwa_table_stride(const ctpwa_handle* h, int kind)
+{
+    if (!h || kind < 0 || kind > 2) return CTPWA_ERR_ARG;
+    return h->eng->tableStride(kind);
+}
+
+int ctpwa_export_weights(ctpwa_handle* h, const double* d_params, const int* wave_mask, double* d_total,
+                         double* d_partial, double* d_interf_ev, double* d_interf, void* stream)
+{
+    if (!h || !d_params || !d_total || !d_partial || !d_interf) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    try {
+        std::vector<int> mask;
+        if (wave_mask) mask.assign(wave_mask, wave_mask + h->eng->nBlocks());
+        h->eng->exportWeights(d_params, mask, d_total, d_partial, d_interf_ev, d_interf, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_sums_size(const ctpwa_handle* h) { return h ? h->eng->sumsSize() : CTPWA_ERR_ARG; }
 
 int ctpwa_shard_sums(ctpwa_handle* h, const double* d_params, int precision, double* d_sums, void* stream)

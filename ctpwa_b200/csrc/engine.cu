@@ -789,6 +789,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     CT_CUDA(cudaMalloc(&d_partials_, sizeof(double) * (size_t)grid_max_ * nacc));
     CT_CUDA(cudaMalloc(&d_parts_, sizeof(double) * 8));
     CT_CUDA(cudaMalloc(&d_err_, sizeof(int)));
+    CT_CUDA(cudaMalloc(&d_mask_, sizeof(int) * std::max(1, (int)model_.blocks.size())));
     CT_CUDA(cudaMemsetAsync(d_err_, 0, sizeof(int), init_stream_));
     CT_CUDA(cudaMalloc(&d_hscratch_, sizeof(double) * (3 * (size_t)std::max(1, model_.nParams()) + 1)));
     CT_CUDA(cudaStreamSynchronize(init_stream_));
@@ -812,6 +813,7 @@ Engine::~Engine()
     cudaFree(d_parts_);
     cudaFree(d_hscratch_);
     cudaFree(d_err_);
+    cudaFree(d_mask_);
     cudaFree(d_amp_chain_);
     cudaFree(d_ratio_);
     cudaFree(d_gauss_idx_);
@@ -1207,9 +1209,11 @@ void Engine::compileKernel()
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
-    cudaKernel_t kpart;
+    cudaKernel_t kpart, kexp;
     CT_CUDA(cudaLibraryGetKernel(&kpart, lib, "ct_partials_f64"));
     k_part_ = (void*)kpart;
+    CT_CUDA(cudaLibraryGetKernel(&kexp, lib, "ct_export_f64"));
+    k_exp_ = (void*)kexp;
     k_f64_ = (void*)k64;
     k_mixed_ = (void*)kmx;
     for (int pr = 0; pr < 2; ++pr)
@@ -1685,6 +1689,47 @@ void Engine::partialIntegrals(const double* d_params, int kind, double* d_out, c
     void* args[] = {&a, &rows};
     CT_CUDA(cudaLaunchKernel(k_part_, dim3(grid), dim3(256), args, 0, stream));
     ct_colsum_kernel<<<1, 256, 0, stream>>>(rows, grid, nb, d_out);
+    CT_CUDA(cudaGetLastError());
+}
+
+void Engine::exportWeights(const double* d_params, const std::vector<int>& mask, double* d_total, double* d_partial,
+                           double* d_interf_ev, double* d_interf, cudaStream_t stream)
+{
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nb = nBlocks();
+    const int npair = nb * (nb + 1) / 2;
+    if (!mask.empty() && (int)mask.size() != nb) throw std::runtime_error("export: wave mask must have one entry per block");
+    const DeviceSample& d = samples_[0];
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    a.s[0].slamp = d.slamp64;
+    a.s[0].kin = d.kin;
+    a.s[0].w = d.w;
+    a.s[0].n = d.n;
+    a.s[0].ld = d.ld;
+    a.s[0].cta_count = 1;
+    a.nsamp = 1;
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.partials = d_partials_;
+    a.consts = d_consts_;
+    a.err = d_err_;
+    void* pargs[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), pargs, 0, stream));
+    const int* dmask = nullptr;
+    if (!mask.empty()) {
+        CT_CUDA(cudaMemcpyAsync(d_mask_, mask.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, stream));
+        dmask = d_mask_;
+    }
+    const int nacc = 2 + 2 * nA + m.nTheta();
+    const long long cap_rows = (long long)grid_max_ * nacc / std::max(1, npair);
+    int grid = (int)std::max(1LL, std::min<long long>((d.n + 255) / 256, std::min<long long>(cap_rows, 148LL * 4)));
+    double* rows = d_partials_;
+    void* args[] = {&a, &d_total, &d_partial, &d_interf_ev, &rows, &dmask};
+    CT_CUDA(cudaLaunchKernel(k_exp_, dim3(grid), dim3(256), args, 0, stream));
+    ct_colsum_kernel<<<1, 256, 0, stream>>>(rows, grid, npair, d_interf);
     CT_CUDA(cudaGetLastError());
 }
 

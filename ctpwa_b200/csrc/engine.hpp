@@ -87,6 +87,14 @@ public:
     // ratios of these (FP64).
     int nBlocks() const { return (int)model_.blocks.size(); }
     void partialIntegrals(const double* d_params, int kind, double* d_out, cudaStream_t stream);
+    // Result export over the phase-space sample (FP64): per event the total
+    // intensity (of the masked blocks, all when mask is empty), per block the
+    // partial intensities [nBlocks()][ld], optionally the per-event block
+    // interferences [npair][ld] (i < j pairs), and the summed interference
+    // matrix (packed i <= j, nBlocks()(nBlocks()+1)/2) into d_interf.
+    void exportWeights(const double* d_params, const std::vector<int>& mask, double* d_total, double* d_partial,
+                       double* d_interf_ev, double* d_interf, cudaStream_t stream);
+    long long tableStride(int kind) const { return samples_[kind].ld; }
     // Per-event intensities of sample `kind` at d_params (device output [n]).
     void intensity(const double* d_params, int kind, double* d_out, cudaStream_t stream);
     // Per-sample partial sums of the last evaluation (diagnostics):
@@ -133,6 +141,8 @@ private:
     void* k_mixed_ = nullptr;
     void* k_int_ = nullptr;
     void* k_part_ = nullptr;
+    void* k_exp_ = nullptr;
+    int* d_mask_ = nullptr;  // [nBlocks] export wave mask
     void* k_pro_ = nullptr;
     double jit_seconds_ = 0.0;
     bool jit_cache_hit_ = false;

@@ -431,7 +431,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
         const double we = S.w ? __ldg(S.w + e) : 1.0;
 #pragma unroll
         for (int i = 0; i < M_NBLK; ++i) {
-            double t = 0.0;
+            double blk = 0.0;
 #pragma unroll
             for (int p = 0; p < M_NPOL; ++p) {
                 double sr = 0.0, si = 0.0;
@@ -443,9 +443,9 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
                     sr += cr * x.x - ci * x.y;
                     si += cr * x.y + ci * x.x;
                 }
-                t += sr * sr + si * si;
+                blk += sr * sr + si * si;
             }
-            acc[i] += we * t;
+            acc[i] += we * blk;
         }
     }
     __shared__ double red[CT_BLOCK / 32][M_NBLK];
@@ -464,6 +464,88 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
         for (int w = 0; w < CT_BLOCK / 32; ++w) x += red[w][i];
         rows[(long long)blockIdx.x * M_NBLK + i] = x;
     }
+}
+
+// Result export over sample s[0] (FP64): per event, the block amplitudes
+// P_i,p = sum_{t in block i} v_col(t) F_t SL_plane(t),p give
+//   total[e]      = sum_p |sum_{i in mask} P_i,p|^2 (all blocks when mask is null)
+//   partial[i][e] = sum_p |P_i,p|^2
+//   interf_ev[k][e] (optional) = sum_p 2 Re(P_i,p conj(P_j,p)) for the k-th pair i < j
+// and each CTA adds sum_e sum_p 2 Re(P_i,p conj(P_j,p)) (i <= j) into its row
+// of interf_rows (reference computeResults, src/ComputeResults.cu).
+extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_export_f64(CtArgs A, double* __restrict__ total,
+                                                                    double* __restrict__ partial,
+                                                                    double* __restrict__ interf_ev,
+                                                                    double* __restrict__ interf_rows,
+                                                                    const int* __restrict__ mask)
+{
+    constexpr int NPAIR = M_NBLK * (M_NBLK + 1) / 2;
+    const CtSample& S = A.s[0];
+    const long long n = S.n;
+    const double2* __restrict__ slamp = (const double2*)S.slamp;
+    __shared__ double sC[CT_NCONST_ALLOC];
+    __shared__ double sI[NPAIR];
+    for (int i = threadIdx.x; i < NPAIR; i += CT_BLOCK) sI[i] = 0.0;
+    ct_stage_consts(A, sC);
+    for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
+        double kv[M_NKIN > 0 ? M_NKIN : 1];
+#pragma unroll
+        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
+        double Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
+        model_columns(kv, sC, Fr, Fi, dFr, dFi);
+        double Pr[M_NBLK][M_NPOL], Pi[M_NBLK][M_NPOL];
+#pragma unroll
+        for (int i = 0; i < M_NBLK; ++i)
+#pragma unroll
+            for (int p = 0; p < M_NPOL; ++p) {
+                double sr = 0.0, si = 0.0;
+                for (int t = blk_term0(i); t < blk_term0(i) + blk_nterm(i); ++t) {
+                    const int a = term_col(t);
+                    const double vr = __ldg(A.v + 2 * a), vi = __ldg(A.v + 2 * a + 1);
+                    const double cr = vr * Fr[t] - vi * Fi[t], ci = vr * Fi[t] + vi * Fr[t];
+                    const double2 x = slamp[(long long)(term_plane(t) * M_NPOL + p) * S.ld + e];
+                    sr += cr * x.x - ci * x.y;
+                    si += cr * x.y + ci * x.x;
+                }
+                Pr[i][p] = sr;
+                Pi[i][p] = si;
+            }
+        double tot = 0.0;
+#pragma unroll
+        for (int p = 0; p < M_NPOL; ++p) {
+            double sr = 0.0, si = 0.0;
+#pragma unroll
+            for (int i = 0; i < M_NBLK; ++i)
+                if (!mask || mask[i]) {
+                    sr += Pr[i][p];
+                    si += Pi[i][p];
+                }
+            tot += sr * sr + si * si;
+        }
+        total[e] = tot;
+        int k = 0, kk = 0;
+#pragma unroll
+        for (int i = 0; i < M_NBLK; ++i) {
+            double pi = 0.0;
+#pragma unroll
+            for (int p = 0; p < M_NPOL; ++p) pi += Pr[i][p] * Pr[i][p] + Pi[i][p] * Pi[i][p];
+            partial[(long long)i * S.ld + e] = pi;
+#pragma unroll
+            for (int j = i; j < M_NBLK; ++j) {
+                double x = 0.0;
+#pragma unroll
+                for (int p = 0; p < M_NPOL; ++p) x += 2.0 * (Pr[i][p] * Pr[j][p] + Pi[i][p] * Pi[j][p]);
+                atomicAdd(&sI[k], x);
+                if (j > i) {
+                    if (interf_ev) interf_ev[(long long)kk * S.ld + e] = x;
+                    ++kk;
+                }
+                ++k;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NPAIR; i += CT_BLOCK) interf_rows[(long long)blockIdx.x * NPAIR + i] = sI[i];
 }
 
 // Per-event intensity f_e = sum_p |S_p|^2 of sample s[0] (FP64), for

@@ -119,6 +119,23 @@ int ctpwa_n_blocks(const ctpwa_handle* h);
  * prepared on the first call), at d_params; device pointers, FP64. */
 int ctpwa_partial_integrals(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream);
 
+/* Row stride (events, padded to a multiple of 256) of the per-event export
+ * arrays of sample kind (0 phase space, 1 data, 2 background). */
+long long ctpwa_table_stride(const ctpwa_handle* h, int kind);
+
+/* Replaces the device part of analysis::writeResult — src/Analysis.cu:1355-1700
+ * (computeResults, src/ComputeResults.cu) — over the phase-space sample, FP64:
+ *   d_total[e]          intensity of event e (of the blocks with wave_mask[i] != 0
+ *                       when wave_mask, a host array of ctpwa_n_blocks ints, is given)
+ *   d_partial[i*ld + e] intensity of block i alone
+ *   d_interf_ev[k*ld + e] (optional, may be NULL) 2 Re(P_i conj(P_j)) of pair k (i < j)
+ *   d_interf[k]         the same summed over events for pairs i <= j (diagonal 2|P_i|^2),
+ *                       packed k = i*n - i*(i-1)/2 + (j - i)
+ * with ld = ctpwa_table_stride(h, 0); device pointers. Normalisation to the
+ * data yield is left to the caller (ctpwa_b200.analysis.writeResult). */
+int ctpwa_export_weights(ctpwa_handle* h, const double* d_params, const int* wave_mask, double* d_total,
+                         double* d_partial, double* d_interf_ev, double* d_interf, void* stream);
+
 /* Event-sharded evaluation, the exchange step of the reference's multi-device
  * NLL (src/Analysis.cu:4210-4238, which gathers per-device partial results
  * with peer copies). ctpwa_shard_sums writes this shard's per-sample sums

@@ -231,3 +231,26 @@ def test_staged_tables_match_direct_loads(tmp_path, monkeypatch):
         n1, g1 = staged.getNLLAndGrad(pt, prec)
         assert abs(float(n0) - float(n1)) <= 1e-12 * abs(float(n0)), prec
         assert float((g0 - g1).abs().max()) <= 1e-10 * float(g0.abs().max()), prec
+
+
+def test_write_result_export(setups, tmp_path):
+    """writeResult: per-event totals and block weights from the device export
+    against the oracle's amplitude columns; interference diagonal = 2 x block
+    integrals; total weights sum to the data yield."""
+    ana, orc, pt, p = setups["kkpi"]
+    out = ana.writeResult(pt, str(tmp_path / "res.npz"), is_saved_weight=1)
+    nV = ana.getNVector()
+    m = ana.getModel()
+    cols = orc.columns(0, p[2 * nV:])
+    chain, ratio = m["coupling"]["amp_chain"], m["coupling"]["ratio"]
+    v = np.array([ratio[a] * complex(p[chain[a]], p[nV + chain[a]]) for a in range(cols.shape[2])])
+    S = np.einsum("epa,a->ep", cols, v)
+    tot = np.sum(np.abs(S) ** 2, axis=1)
+    assert np.max(np.abs(out["totalweight"] / out["norm_factor"] - tot) / tot) < 1e-10
+    assert abs(out["totalweight"].sum() - out["data_integral"]) < 1e-8 * out["data_integral"]
+    I = ana.getPartialIntegrals(pt, 0).cpu().numpy()
+    assert np.allclose(np.diag(out["interference"]), 2 * I, rtol=1e-10)
+    for i in range(ana.getNBlocks()):
+        assert abs(out[f"weight_{i}"].sum() / out["norm_factor"] - I[i]) <= 1e-10 * I[i]
+    loaded = np.load(tmp_path / "res.npz")
+    assert set(loaded.files) >= {"legends", "interference", "totalweight"}
