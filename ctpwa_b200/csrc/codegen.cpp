@@ -993,6 +993,7 @@ GeneratedModel generateModel(const Model& m)
     }
     g.out.nplane = pl;
     g.out.npol = m.npol;
+    g.out.ngrad = 2 * m.nAmp() + m.nTheta();
     for (const auto& b : m.blocks) {
         const Group& gr = m.groups[b.group];
         auto par = g.params(b);

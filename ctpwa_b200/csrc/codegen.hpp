@@ -27,6 +27,7 @@ struct GeneratedModel {
     std::vector<KinSlot> slots;  // kinematic cache layout
     int nplane = 0;              // angular planes = sum over groups of nSL
     int npol = 1;                // polarisation states per plane
+    int ngrad = 0;               // gradient sums per thread: 2 nA + nTheta
     std::vector<int> group_plane0;
     int nder = 0;
     int nconst = 0;              // parameter-only subexpressions kept per call

@@ -1084,9 +1084,11 @@ void Engine::computeAngular(int kind)
 }
 
 // Block size and minimum resident CTAs per SM of the plain [0] and mixed [1]
-// fused kernels: 128 x 3 (170 registers, 12 warps per SM; measured 7 % faster
-// than 256 x 1) and 256 x 2 unless CTPWA_F64_BLOCK / CTPWA_F64_MINB /
-// CTPWA_MX_BLOCK / CTPWA_MX_MINB override them (tuning).
+// fused kernels, unless CTPWA_F64_BLOCK / CTPWA_F64_MINB / CTPWA_MX_BLOCK /
+// CTPWA_MX_MINB / CTPWA_*_ACC_SMEM override them (tuning). Measured on the
+// K+K-pi0 workload: plain 256 x 2 with the gradient sums in shared memory
+// (128 registers, 16 warps per SM) 1.371 ms, against 128 x 3 in registers
+// 1.585 ms and 256 x 1 1.717 ms; mixed 256 x 2 in registers 0.805 ms.
 FusedShape fusedShape(const GeneratedModel& gen)
 {
     FusedShape sh;
@@ -1097,10 +1099,12 @@ FusedShape fusedShape(const GeneratedModel& gen)
         if (v < lo || v > hi) throw std::runtime_error(std::string(name) + " out of range");
         return v;
     };
-    sh.block[0] = get("CTPWA_F64_BLOCK", 128, 32, 1024);
-    sh.minb[0] = get("CTPWA_F64_MINB", 3, 1, 16);
+    sh.block[0] = get("CTPWA_F64_BLOCK", 256, 32, 1024);
+    sh.minb[0] = get("CTPWA_F64_MINB", 2, 1, 16);
     sh.block[1] = get("CTPWA_MX_BLOCK", 256, 32, 1024);
     sh.minb[1] = get("CTPWA_MX_MINB", 2, 1, 16);
+    sh.acc[0] = get("CTPWA_F64_ACC_SMEM", 1, 0, 1);
+    sh.acc[1] = get("CTPWA_MX_ACC_SMEM", 0, 0, 1);
     for (int i = 0; i < 2; ++i)
         if (sh.block[i] % 32) throw std::runtime_error("fused block sizes must be multiples of 32");
     // Staging (CTPWA_STAGE=1): two tile buffers of BLOCK events (angular rows
@@ -1112,15 +1116,23 @@ FusedShape fusedShape(const GeneratedModel& gen)
     // 2 CTAs per SM vs 1.576 ms direct at 3).
     const int stage_on = get("CTPWA_STAGE", 0, 0, 1);
     const long long rowb[2] = {16, 8};  // bytes per complex angular value (FP64, FP32)
+    const long long accb[2] = {8, 4};   // bytes per gradient sum (FP64, FP32)
+    const long long per_sm = 228LL * 1024, per_cta = 227LL * 1024, reserve = 8LL * 1024;
+    auto fits = [&](int i, long long bytes) {
+        return bytes + reserve <= per_cta && (long long)sh.minb[i] * (bytes + reserve) <= per_sm;
+    };
     for (int i = 0; i < 2; ++i) {
-        const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
-        const long long bytes =
-            2LL * (npl * rowb[i] + (long long)std::max<size_t>(1, gen.slots.size()) * 8) * sh.block[i];
-        const long long per_sm = 228LL * 1024, per_cta = 227LL * 1024, reserve = 8LL * 1024;
-        if (stage_on && bytes + reserve <= per_cta && (long long)sh.minb[i] * (bytes + reserve) <= per_sm) {
-            sh.stage[i] = 1;
-            sh.dsmem[i] = (int)bytes;
+        // dynamic shared memory = [gradient-sum slots][two tile buffers]
+        long long acc_bytes = sh.acc[i] ? (gen.ngrad * sh.block[i] * accb[i] + 127) / 128 * 128 : 0;
+        if (!fits(i, acc_bytes)) {
+            sh.acc[i] = 0;
+            acc_bytes = 0;
         }
+        const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
+        const long long stage_bytes =
+            2LL * (npl * rowb[i] + (long long)std::max<size_t>(1, gen.slots.size()) * 8) * sh.block[i];
+        if (stage_on && fits(i, acc_bytes + stage_bytes)) sh.stage[i] = 1;
+        sh.dsmem[i] = (int)(acc_bytes + (sh.stage[i] ? stage_bytes : 0));
     }
     return sh;
 }
@@ -1137,6 +1149,8 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
                                      "--fmad=true", "-lineinfo"};
     // tuning knobs: block size and minimum resident CTAs per SM of the fused kernels
     const FusedShape sh = fusedShape(gen);
+    optv.push_back("-DCT_F64_ACC=" + std::to_string(sh.acc[0]));
+    optv.push_back("-DCT_MX_ACC=" + std::to_string(sh.acc[1]));
     optv.push_back("-DCT_F64_STAGE=" + std::to_string(sh.stage[0]));
     optv.push_back("-DCT_MX_STAGE=" + std::to_string(sh.stage[1]));
     optv.push_back("-DCT_F64_BLOCK=" + std::to_string(sh.block[0]));

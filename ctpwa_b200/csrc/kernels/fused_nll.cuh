@@ -53,6 +53,13 @@
 #ifndef CT_MX_STAGE
 #define CT_MX_STAGE 0
 #endif
+// per-thread gradient sums in shared memory instead of registers
+#ifndef CT_F64_ACC
+#define CT_F64_ACC 1
+#endif
+#ifndef CT_MX_ACC
+#define CT_MX_ACC 0
+#endif
 #ifndef CT_WAIT_LIMIT
 #define CT_WAIT_LIMIT (1u << 22)
 #endif
@@ -110,8 +117,38 @@ struct CtVec2<float> {
 
 // CTA reduction of the per-thread accumulators: two FP64 sums (log-likelihood
 // and phase-space intensity) and the gradient terms (type G), reduced in FP64.
+// Per-thread gradient sums: in registers, or (SMEM) in a shared-memory slot
+// per thread, which frees registers at the cost of a shared load and store
+// per update.
+template <typename L, int BLOCK, bool SMEM>
+struct CtAccG;
+template <typename L, int BLOCK>
+struct CtAccG<L, BLOCK, false> {
+    L v[CT_NACC - 2];
+    __device__ __forceinline__ void init(unsigned char*)
+    {
+#pragma unroll
+        for (int i = 0; i < CT_NACC - 2; ++i) v[i] = (L)0;
+    }
+    __device__ __forceinline__ void add(int i, L x) { v[i] += x; }
+    __device__ __forceinline__ L operator[](int i) const { return v[i]; }
+};
+template <typename L, int BLOCK>
+struct CtAccG<L, BLOCK, true> {
+    L* p;
+    // slot: the start of the CTA's dynamic shared memory (host-sized)
+    __device__ __forceinline__ void init(unsigned char* slot)
+    {
+        p = (L*)slot + threadIdx.x;
+#pragma unroll
+        for (int i = 0; i < CT_NACC - 2; ++i) p[i * BLOCK] = (L)0;
+    }
+    __device__ __forceinline__ void add(int i, L x) { p[i * BLOCK] += x; }
+    __device__ __forceinline__ L operator[](int i) const { return p[i * BLOCK]; }
+};
+
 template <int BLOCK, typename G>
-__device__ __forceinline__ void ct_block_reduce_store(const double* accd, const G* accg, double* out)
+__device__ __forceinline__ void ct_block_reduce_store(const double* accd, const G& accg, double* out)
 {
     __shared__ double red[BLOCK / 32][CT_NACC];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -155,7 +192,7 @@ struct CtLineshape<float> {
 // L: type of the lineshapes, their derivatives and the per-thread gradient
 //    sums
 // PH_ONLY: the launch serves phase-space events only
-template <typename R, typename L, bool PH_ONLY, int BLOCK, bool STAGE>
+template <typename R, typename L, bool PH_ONLY, int BLOCK, bool STAGE, bool ACC_SMEM>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 {
     typedef typename CtVec2<R>::type SL2;
@@ -172,10 +209,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     const double* __restrict__ kin = S.kin;
     const double* __restrict__ wts = S.w;
 
+    // dynamic shared memory: [gradient-sum slots (ACC_SMEM)][tile buffers (STAGE)]
+    extern __shared__ __align__(128) unsigned char ct_dyn[];
+    constexpr unsigned ACC_BYTES = ACC_SMEM ? ((CT_NACC - 2) * BLOCK * sizeof(L) + 127) / 128 * 128 : 0;
     double accd[2] = {0.0, 0.0};
-    L accg[CT_NACC - 2];
-#pragma unroll
-    for (int i = 0; i < CT_NACC - 2; ++i) accg[i] = (L)0;
+    CtAccG<L, BLOCK, ACC_SMEM> accg;
+    accg.init(ct_dyn);
 
     // parameter-only constants: FP64, and as FP32 hi + lo pairs for the
     // FP32 lineshapes (a single FP32 rounding would bias every event alike)
@@ -300,8 +339,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             const int a = term_col(t), c = term_plane(t);
             const L fr = Fr[t], fi = Fi[t];
             const L tr = (L)Tr[c], ti = (L)Ti[c];
-            accg[2 * a] += gscale * (fr * tr + fi * ti);
-            accg[2 * a + 1] += gscale * (fr * ti - fi * tr);
+            accg.add(2 * a, gscale * (fr * tr + fi * ti));
+            accg.add(2 * a + 1, gscale * (fr * ti - fi * tr));
         }
         // theta-gradient: Re(v dF_t conj(T)) = Re(dF_t W_t), W_t = v_col(t) conj(T_plane(t))
         L Wr[M_NTERM], Wi[M_NTERM];
@@ -315,7 +354,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #pragma unroll
         for (int k = 0; k < M_NDER; ++k) {
             const int t = der_term(k);
-            accg[2 * M_NA + der_th(k)] += dFr[k] * Wr[t] - dFi[k] * Wi[t];
+            accg.add(2 * M_NA + der_th(k), dFr[k] * Wr[t] - dFi[k] * Wi[t]);
         }
     };
 
@@ -328,7 +367,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         constexpr int NPL = M_NPLANE * M_NPOL;
         constexpr unsigned SLB = BLOCK * sizeof(SL2), KB = BLOCK * sizeof(double);
         constexpr unsigned BUF = NPL * SLB + M_NKIN * KB;
-        extern __shared__ __align__(128) unsigned char ct_stage[];
+        unsigned char* ct_stage = ct_dyn + ACC_BYTES;
         __shared__ __align__(8) unsigned long long ct_bar[2];
         const long long first = cta - S.cta_begin, step = S.cta_count;
         const long long ntiles = (n + BLOCK - 1) / BLOCK;
@@ -381,16 +420,16 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride)
             event(e, kin + e, S.ld, slamp + e, S.ld);
     }
-    ct_block_reduce_store<BLOCK, L>(accd, accg, A.partials + (long long)cta * CT_NACC);
+    ct_block_reduce_store<BLOCK>(accd, accg, A.partials + (long long)cta * CT_NACC);
 }
 
 // block size and minimum resident CTAs per SM of the two fused kernels (the
 // host launches with the same block sizes)
 #ifndef CT_F64_BLOCK
-#define CT_F64_BLOCK 128
+#define CT_F64_BLOCK 256
 #endif
 #ifndef CT_F64_MINB
-#define CT_F64_MINB 3
+#define CT_F64_MINB 2
 #endif
 #ifndef CT_MX_BLOCK
 #define CT_MX_BLOCK 256
@@ -400,12 +439,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #endif
 extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB) ct_fused_f64(CtArgs a)
 {
-    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE != 0>(a);
+    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE != 0, CT_F64_ACC != 0>(a);
 }
 // mixed form (FP32 lineshapes and algebra, FP64 logs and sums), all samples
 extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_mixed(CtArgs a)
 {
-    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE != 0>(a);
+    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE != 0, CT_MX_ACC != 0>(a);
 }
 
 // Partial-wave integrals of sample s[0] (FP64): per resonance block i,
