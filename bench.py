@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None, help="host-buffer steps (default: steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-toy-fit", action="store_true", help="skip the toy-fit serving stream")
+    ap.add_argument("--no-hessian", action="store_true", help="skip the full-size Hessian timing")
     ap.add_argument("--toy-jobs", type=int, default=12)
     ap.add_argument("--toy-rate", type=float, default=4.0)
     ap.add_argument("--data-dir", default=os.environ.get("CTPWA_BENCH_DIR", "/tmp/ctpwa_bench"))
@@ -439,6 +440,30 @@ def run_gpu(args, rank, world, local_rank):
     e2e = {"value": world * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * nP, "d2h_bytes_per_step": 8 * (1 + nP),
            "ms_per_step": 1e3 * e2e_s / E}
 
+    # full-size Hessian: exact (forward mode over the adjoint pass) and
+    # central differences of the exact gradient, each timed once after one
+    # untimed call; several GPUs: the sharded form (two all-reduces)
+    hess = None
+    if not args.no_hessian:
+        def hessian(method):
+            if world > 1:
+                return shards.hessian(ana, Pd[0]) if method == "exact" else None
+            return ana.getHessian(Pd[0], method=method)
+
+        hess = {"n_params": nP}
+        Hs = {}
+        for method in ("exact", "fd") if world == 1 else ("exact",):
+            hessian(method)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            Hs[method] = hessian(method)
+            e1.record(stream)
+            barrier()
+            hess[method + "_ms"] = max_over_ranks(e0.elapsed_time(e1))
+        if "fd" in Hs:
+            hess["fd_vs_exact_rel"] = float((Hs["fd"] - Hs["exact"]).abs().max() / Hs["exact"].abs().max())
+
     if rank != 0:
         return 0
     peaks = measured_peaks()
@@ -490,6 +515,8 @@ def run_gpu(args, rank, world, local_rank):
                      "kernel_ms": kms, "algorithmic_bytes_per_launch": alg, "algorithmic_bytes_per_event": per_evt,
                      "streamed_bytes_per_launch": streamed_bytes(layout, n_events, "mixed")},
     }
+    if hess is not None:
+        line["hessian"] = hess
     if world == 1 and not args.no_toy_fit:
         line["toy_fit"] = toy_fit(args, local_rank)
     if world == 1 and not args.no_cpu_baseline:

@@ -504,12 +504,72 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return out
 
-    def getHessian(self, params: torch.Tensor, rel_step: float = 1e-5) -> torch.Tensor:
-        """Hessian [(2nV+nT), (2nV+nT)] (float64, CUDA), grouped [Re p, Im p, theta]:
-        central differences of the exact FP64 device gradient, formed on the device."""
+    def getHessian(self, params: torch.Tensor, method: str = "exact", rel_step: float = 1e-5) -> torch.Tensor:
+        """Hessian [(2nV+nT), (2nV+nT)] (float64, CUDA), grouped [Re p, Im p, theta].
+
+        method "exact" (default): forward-mode (dual-number) derivatives of the
+        FP64 device gradient pass along every unit direction, symmetrised.
+        method "fd": central differences of the exact FP64 device gradient with
+        steps rel_step * max(|p_i|, 1e-2)."""
         p = self._check_params(params)
         H = torch.empty((self._np, self._np), dtype=torch.float64, device=p.device)
         stream = torch.cuda.current_stream(p.device).cuda_stream
-        if self._lib.ctpwa_hessian(self._h, p.data_ptr(), H.data_ptr(), float(rel_step), ctypes.c_void_p(stream)) != 0:
+        if method == "exact":
+            rc = self._lib.ctpwa_hessian_exact(self._h, p.data_ptr(), H.data_ptr(), ctypes.c_void_p(stream))
+        elif method == "fd":
+            rc = self._lib.ctpwa_hessian(self._h, p.data_ptr(), H.data_ptr(), float(rel_step), ctypes.c_void_p(stream))
+        else:
+            raise ValueError('method must be "exact" or "fd"')
+        if rc != 0:
             raise RuntimeError(_lib.error(self._h))
         return H
+
+    def _check_dirs(self, p: torch.Tensor, dirs: torch.Tensor) -> torch.Tensor:
+        if dirs.dim() == 1:
+            dirs = dirs.unsqueeze(0)
+        if dirs.dim() != 2 or dirs.shape[1] != self._np:
+            raise ValueError(f"directions must have shape [ndir, {self._np}]")
+        return dirs.to(device=p.device, dtype=torch.float64).contiguous()
+
+    def getHessianVectorProduct(self, params: torch.Tensor, dirs: torch.Tensor) -> torch.Tensor:
+        """Exact H(params) u for each row u of dirs ([ndir, nP] or [nP]);
+        float64 CUDA [ndir, nP]."""
+        p = self._check_params(params)
+        d = self._check_dirs(p, dirs)
+        out = torch.empty_like(d)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        if self._lib.ctpwa_hvp(self._h, p.data_ptr(), d.data_ptr(), d.shape[0], out.data_ptr(),
+                               ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return out
+
+    def getShardHvpSums(self, params: torch.Tensor, dirs: torch.Tensor) -> torch.Tensor:
+        """This shard's tangent sums for the directions (float64 CUDA, to be
+        summed over shards and passed to finalizeShardHvp)."""
+        p = self._check_params(params)
+        d = self._check_dirs(p, dirs)
+        out = torch.empty(self._lib.ctpwa_hvp_sums_size(self._h, d.shape[0]), dtype=torch.float64, device=p.device)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        if self._lib.ctpwa_shard_hvp_sums(self._h, p.data_ptr(), d.data_ptr(), d.shape[0], out.data_ptr(),
+                                          ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return out
+
+    def finalizeShardHvp(self, params: torch.Tensor, dirs: torch.Tensor, sums: torch.Tensor,
+                         hvp_sums: torch.Tensor) -> torch.Tensor:
+        """Rows H u of the union of the shards from the summed FP64 shard sums
+        (getShardSums(params, "fp64")) and the summed tangent sums."""
+        p = self._check_params(params)
+        d = self._check_dirs(p, dirs)
+        if sums.dtype != torch.float64 or not sums.is_cuda or sums.numel() != self._lib.ctpwa_sums_size(self._h):
+            raise RuntimeError("sums must be the float64 CUDA buffer of getShardSums")
+        if (hvp_sums.dtype != torch.float64 or not hvp_sums.is_cuda
+                or hvp_sums.numel() != self._lib.ctpwa_hvp_sums_size(self._h, d.shape[0])):
+            raise RuntimeError("hvp_sums must be the float64 CUDA buffer of getShardHvpSums")
+        sums, hvp_sums = sums.contiguous(), hvp_sums.contiguous()
+        out = torch.empty_like(d)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        if self._lib.ctpwa_finalize_hvp(self._h, p.data_ptr(), d.data_ptr(), d.shape[0], sums.data_ptr(),
+                                        hvp_sums.data_ptr(), out.data_ptr(), ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return out

@@ -19,6 +19,14 @@ SIGNATURES = {
     "ctpwa_destroy": (None, [ctypes.c_void_p]),
     "ctpwa_hessian": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                      ctypes.c_void_p]),
+    "ctpwa_hessian_exact": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ctpwa_hvp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                 ctypes.c_void_p]),
+    "ctpwa_hvp_sums_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ctpwa_shard_hvp_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "ctpwa_finalize_hvp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_n_blocks": (ctypes.c_int, [ctypes.c_void_p]),
     "ctpwa_partial_integrals": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                ctypes.c_void_p]),

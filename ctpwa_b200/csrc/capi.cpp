@@ -165,6 +165,61 @@ int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, doubl
     return CTPWA_OK;
 }
 
+int ctpwa_hessian_exact(ctpwa_handle* h, const double* d_params, double* d_hess, void* stream)
+{
+    if (!h || !d_params || !d_hess) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    try {
+        h->eng->hessianExact(d_params, d_hess, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_hvp(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, double* d_out, void* stream)
+{
+    if (!h || !d_params || !d_dirs || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (ndir < 0) return setErr(h, CTPWA_ERR_ARG, "ndir must be >= 0");
+    try {
+        h->eng->hessianVectorProducts(d_params, d_dirs, ndir, d_out, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_hvp_sums_size(const ctpwa_handle* h, int ndir)
+{
+    if (!h || ndir < 0) return CTPWA_ERR_ARG;
+    return h->eng->hvpSumsSize(ndir);
+}
+
+int ctpwa_shard_hvp_sums(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, double* d_tsums,
+                         void* stream)
+{
+    if (!h || !d_params || !d_dirs || !d_tsums) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (ndir < 0) return setErr(h, CTPWA_ERR_ARG, "ndir must be >= 0");
+    try {
+        h->eng->hvpSums(d_params, d_dirs, ndir, d_tsums, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_finalize_hvp(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, const double* d_vsums,
+                       const double* d_tsums, double* d_out, void* stream)
+{
+    if (!h || !d_params || !d_dirs || !d_vsums || !d_tsums || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (ndir < 0) return setErr(h, CTPWA_ERR_ARG, "ndir must be >= 0");
+    try {
+        h->eng->finalizeHvp(d_params, d_dirs, ndir, d_vsums, d_tsums, d_out, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_n_blocks(const ctpwa_handle* h) { return h ? h->eng->nBlocks() : CTPWA_ERR_ARG; }
 
 int ctpwa_partial_integrals(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream)

@@ -15,6 +15,7 @@
 #include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <functional>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -923,6 +924,81 @@ std::string Gen::emit()
         }
         return evs.str();
     };
+
+    // ---------------- dual-number form (Hessian-vector products) ----------------
+    // The same FP64 code in which every value that depends on the resonance
+    // parameters is a CtDual (value, directional derivative): the prologue
+    // runs on dual theta leaves, event nodes that depend on theta become dual,
+    // purely kinematic nodes stay double. Channel factors and table lookups
+    // take plain values (their parameter derivative is zero, as in the
+    // symbolic derivatives above).
+    {
+        auto dualRef = [&](int x) -> std::string {
+            const auto& nd = N[x];
+            if (nd.op == dag::Const) return num(nd.v);
+            if (nd.dep == dag::DEP_THETA) return "C[" + std::to_string(cslot[x]) + "]";
+            if (nd.op == dag::Kin && nd.idx >= 0) return "kv[" + std::to_string(nd.idx) + "]";
+            if (nd.op == dag::Kin) {
+                int u = (-nd.idx - 1000) / 2;
+                return ((-nd.idx - 1000) % 2 == 0 ? "tre" : "tim") + std::to_string(u);
+            }
+            return "e" + std::to_string(x);
+        };
+        auto plain = [](const std::string& s) { return "ct_value(" + s + ")"; };
+        auto rhs = [&](const dag::Node& nd, const std::function<std::string(int)>& r) {
+            const bool rho = nd.op == dag::RhoRe || nd.op == dag::RhoIm;
+            std::string A = nd.a >= 0 ? r(nd.a) : "", B = nd.b >= 0 ? r(nd.b) : "", Cc = nd.c >= 0 ? r(nd.c) : "";
+            if (rho) {
+                A = plain(A);
+                B = plain(B);
+                Cc = plain(Cc);
+            }
+            return opExpr(nd, A, B, Cc, false);
+        };
+        std::ostringstream dpro, dev;
+        for (size_t x = 0; x < N.size(); ++x) {
+            if (!live[x] || N[x].op == dag::Const || N[x].dep != dag::DEP_THETA) continue;
+            if (N[x].op != dag::Theta) dpro << "  const CtDual t" << x << " = " << rhs(N[x], proRef) << ";\n";
+            if (cslot[x] >= 0) dpro << "  C[" << cslot[x] << "] = " << proRef((int)x) << ";\n";
+        }
+        for (size_t u = 0; u < tab_uses.size(); ++u) {
+            const auto& t = tab_uses[u];
+            if (t.interp)
+                dev << "  double tre" << u << ", tim" << u << "; ls_interp(ct_tab" << t.table << ", "
+                    << plain(dualRef(t.mnode)) << ", tre" << u << ", tim" << u << ");\n";
+            else
+                dev << "  const double tre" << u << " = ls_hist(" << plain(dualRef(t.mnode)) << ", ct_tab" << t.table
+                    << "), tim" << u << " = 0.0;\n";
+        }
+        for (size_t x = 0; x < N.size(); ++x) {
+            const auto& nd = N[x];
+            if (!live[x] || nd.op == dag::Const || nd.op == dag::Theta || nd.op == dag::Kin) continue;
+            if (!(nd.dep & dag::DEP_EVENT)) continue;
+            dev << "  const " << ((nd.dep & dag::DEP_THETA) ? "CtDual" : "double") << " e" << x << " = "
+                << rhs(nd, dualRef) << ";\n";
+        }
+        int q = 0;
+        for (size_t a = 0; a < cols.size(); ++a) {
+            dev << "  Fr[" << a << "] = " << dualRef(cols[a].re) << "; Fi[" << a << "] = " << dualRef(cols[a].im) << ";\n";
+            for (const auto& d : cols[a].der) {
+                dev << "  dFr[" << q << "] = " << dualRef(d.second.first) << "; dFi[" << q << "] = "
+                    << dualRef(d.second.second) << ";\n";
+                ++q;
+            }
+        }
+        std::ostringstream dh;
+        dh << "// generated by ctpwa_b200 codegen: the lineshape products in dual numbers\n#pragma once\n";
+        dh << "// parameter-only subexpressions with their directional derivatives\n";
+        dh << "__device__ __forceinline__ void model_prologue_dual(const CtDual* __restrict__ th, CtDual* __restrict__ C)\n{\n"
+              "  (void)th; (void)C;\n"
+           << dpro.str() << "}\n";
+        dh << "// per-event lineshape products, their theta derivatives, and the directional\n"
+              "// derivatives of both (FP64)\n";
+        dh << "__device__ __forceinline__ void model_columns_dual(const double* __restrict__ kv, const CtDual* __restrict__ C,\n"
+              "    CtDual* Fr, CtDual* Fi, CtDual* dFr, CtDual* dFi)\n{\n  (void)kv; (void)C; (void)dFr; (void)dFi;\n"
+           << dev.str() << "}\n";
+        out.dual_header = dh.str();
+    }
 
     std::vector<std::pair<int, int>> der_entries;  // (term, theta)
     for (size_t a = 0; a < cols.size(); ++a)

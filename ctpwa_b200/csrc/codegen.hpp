@@ -24,6 +24,7 @@ struct KinSlot {
 
 struct GeneratedModel {
     std::string header;          // model.cuh text
+    std::string dual_header;     // model_dual.cuh text: the lineshapes in dual numbers (Hessian)
     std::vector<KinSlot> slots;  // kinematic cache layout
     int nplane = 0;              // angular planes = sum over groups of nSL
     int npol = 1;                // polarisation states per plane

@@ -823,6 +823,12 @@ Engine::~Engine()
         cudaEventDestroy(ev_end_[i]);
     }
     if (init_stream_) cudaStreamDestroy(init_stream_);
+    cudaFree(d_hdirs_);
+    cudaFree(d_hconsts_);
+    cudaFree(d_hrows_);
+    cudaFree(d_hvsums_);
+    cudaFree(d_htsums_);
+    if (hvp_lib_) cudaLibraryUnload((cudaLibrary_t)hvp_lib_);
     if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
 }
 
@@ -1137,31 +1143,18 @@ FusedShape fusedShape(const GeneratedModel& gen)
     return sh;
 }
 
-// NVRTC compile of the fused kernel for one generated model, with a disk cache
-// keyed by the FNV-1a hash of all sources, options and the NVRTC version.
-std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
+// NVRTC compile of one program (main source + named headers) for sm_100a, with
+// a disk cache keyed by the FNV-1a hash of the header texts, the options and
+// the NVRTC version.
+std::string nvrtcCubin(const std::string& src, const std::vector<std::pair<std::string, std::string>>& headers,
+                       const std::vector<std::string>& optv, const char* what, bool* cache_hit)
 {
-    std::string dir = kernelDir();
-    std::string helpers = readFile(dir + "/device_helpers.cuh");
-    std::string fused = readFile(dir + "/fused_nll.cuh");
-    std::string src = "#include \"fused_nll.cuh\"\n";
-    std::vector<std::string> optv = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DCT_BLOCK=256",
-                                     "--fmad=true", "-lineinfo"};
-    // tuning knobs: block size and minimum resident CTAs per SM of the fused kernels
-    const FusedShape sh = fusedShape(gen);
-    optv.push_back("-DCT_F64_ACC=" + std::to_string(sh.acc[0]));
-    optv.push_back("-DCT_MX_ACC=" + std::to_string(sh.acc[1]));
-    optv.push_back("-DCT_F64_STAGE=" + std::to_string(sh.stage[0]));
-    optv.push_back("-DCT_MX_STAGE=" + std::to_string(sh.stage[1]));
-    optv.push_back("-DCT_F64_BLOCK=" + std::to_string(sh.block[0]));
-    optv.push_back("-DCT_F64_MINB=" + std::to_string(sh.minb[0]));
-    optv.push_back("-DCT_MX_BLOCK=" + std::to_string(sh.block[1]));
-    optv.push_back("-DCT_MX_MINB=" + std::to_string(sh.minb[1]));
     std::vector<const char*> optp;
     for (const auto& o : optv) optp.push_back(o.c_str());
     const char* const* opts = optp.data();
     const int nopts = (int)optp.size();
-    std::string key_src = helpers + fused + gen.header;
+    std::string key_src;
+    for (const auto& h : headers) key_src += h.second;
     for (int i = 0; i < nopts; ++i) key_src += opts[i];
     int nvmaj = 0, nvmin = 0;
     nvrtcVersion(&nvmaj, &nvmin);
@@ -1180,10 +1173,14 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     }
     if (cache_hit) *cache_hit = !cubin.empty();
     if (!cubin.empty()) return cubin;
-    const char* hdr_src[] = {helpers.c_str(), fused.c_str(), gen.header.c_str()};
-    const char* hdr_names[] = {"device_helpers.cuh", "fused_nll.cuh", "model.cuh"};
+    std::vector<const char*> hdr_src, hdr_names;
+    for (const auto& h : headers) {
+        hdr_names.push_back(h.first.c_str());
+        hdr_src.push_back(h.second.c_str());
+    }
     nvrtcProgram prog;
-    if (nvrtcCreateProgram(&prog, src.c_str(), "ctpwa_fused.cu", 3, hdr_src, hdr_names) != NVRTC_SUCCESS)
+    if (nvrtcCreateProgram(&prog, src.c_str(), "ctpwa_fused.cu", (int)headers.size(), hdr_src.data(), hdr_names.data()) !=
+        NVRTC_SUCCESS)
         throw std::runtime_error("NVRTC: program creation failed");
     nvrtcResult r = nvrtcCompileProgram(prog, nopts, opts);
     if (r != NVRTC_SUCCESS) {
@@ -1192,7 +1189,7 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
         std::string log(ls2, '\0');
         nvrtcGetProgramLog(prog, &log[0]);
         nvrtcDestroyProgram(&prog);
-        throw std::runtime_error("NVRTC compile of the fused kernel failed:\n" + log.substr(0, 4000));
+        throw std::runtime_error(std::string("NVRTC compile of the ") + what + " failed:\n" + log.substr(0, 4000));
     }
     size_t n = 0;
     nvrtcGetCUBINSize(prog, &n);
@@ -1208,6 +1205,54 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     }
     std::filesystem::rename(tmpp, cpath, ec);
     return cubin;
+}
+
+const std::vector<std::string> kNvrtcBase = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device",
+                                             "-DCT_BLOCK=256", "--fmad=true", "-lineinfo"};
+
+// The fused likelihood kernels of one generated model.
+std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
+{
+    std::string dir = kernelDir();
+    std::vector<std::string> optv = kNvrtcBase;
+    // tuning knobs: block size and minimum resident CTAs per SM of the fused kernels
+    const FusedShape sh = fusedShape(gen);
+    optv.push_back("-DCT_F64_ACC=" + std::to_string(sh.acc[0]));
+    optv.push_back("-DCT_MX_ACC=" + std::to_string(sh.acc[1]));
+    optv.push_back("-DCT_F64_STAGE=" + std::to_string(sh.stage[0]));
+    optv.push_back("-DCT_MX_STAGE=" + std::to_string(sh.stage[1]));
+    optv.push_back("-DCT_F64_BLOCK=" + std::to_string(sh.block[0]));
+    optv.push_back("-DCT_F64_MINB=" + std::to_string(sh.minb[0]));
+    optv.push_back("-DCT_MX_BLOCK=" + std::to_string(sh.block[1]));
+    optv.push_back("-DCT_MX_MINB=" + std::to_string(sh.minb[1]));
+    return nvrtcCubin("#include \"fused_nll.cuh\"\n",
+                      {{"device_helpers.cuh", readFile(dir + "/device_helpers.cuh")},
+                       {"fused_nll.cuh", readFile(dir + "/fused_nll.cuh")},
+                       {"model.cuh", gen.header}},
+                      optv, "fused kernel", cache_hit);
+}
+
+// Block size of the Hessian-vector-product kernel: per-thread tangent sums
+// live in shared memory (ngrad + 2 doubles a thread), kept under 96 KiB.
+int hvpBlock(const GeneratedModel& gen)
+{
+    int b = 128;
+    while (b > 32 && (long long)(gen.ngrad + 2) * b * 8 > 96LL * 1024) b /= 2;
+    return b;
+}
+
+// The Hessian-vector-product kernels of one generated model.
+std::string jitHvpCubin(const GeneratedModel& gen, bool* cache_hit)
+{
+    std::string dir = kernelDir();
+    std::vector<std::string> optv = kNvrtcBase;
+    optv.push_back("-DCT_HVP_BLOCK=" + std::to_string(hvpBlock(gen)));
+    return nvrtcCubin("#include \"hessian.cuh\"\n",
+                      {{"device_helpers.cuh", readFile(dir + "/device_helpers.cuh")},
+                       {"hessian.cuh", readFile(dir + "/hessian.cuh")},
+                       {"model.cuh", gen.header},
+                       {"model_dual.cuh", gen.dual_header}},
+                      optv, "Hessian kernel", cache_hit);
 }
 
 void Engine::compileKernel()
@@ -1247,6 +1292,7 @@ double precompileConfig(const std::string& config_path)
     GeneratedModel g = generateModel(m);
     bool hit = false;
     jitCubin(g, &hit);
+    jitHvpCubin(g, &hit);
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
@@ -1616,6 +1662,288 @@ void Engine::hessian(const double* d_params, double* d_hess, double rel_step, cu
         ct_hess_row_kernel<<<1, 256, 0, stream>>>(d_params, gp, gm, n, i, rel_step, d_hess);
         CT_CUDA(cudaGetLastError());
     }
+    ct_symmetrize_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, stream>>>(d_hess, n);
+    CT_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Exact Hessian: forward mode over the adjoint pass (kernels/hessian.cuh)
+// ---------------------------------------------------------------------------
+
+// argument block of the Hessian-vector-product kernels (must match CtHvpArgs)
+struct CtHvpSampleH {
+    const double2* slamp;
+    const double* kin;
+    const double* w;
+    long long n;
+    long long ld;
+    int kind;
+    int cta_begin;
+    int cta_count;
+    int pad;
+};
+struct CtHvpArgsH {
+    CtHvpSampleH s[3];
+    int nsamp;
+    int ndir;
+    const double* theta;
+    const double* v;
+    const double* dirs;
+    const int* chain;
+    const double* ratio;
+    int nc;
+    int nparam;
+    double* consts;
+    double* rows;
+    int ctas;
+    int pad;
+};
+
+struct HvpFinalizeArgs {
+    const double* vsums;  // [3][nacc] + [n_phsp, W_phsp, W_data, W_bkg]
+    const double* tsums;  // [ndir][3][nacc]
+    const double* dirs;   // [ndir][nP]
+    const double* params;
+    const double* v;
+    const int* chain;
+    const int* gauss_idx;
+    const double* gauss_ms;
+    int ngauss;
+    int nacc, nA, nc, nT, ndir;
+    const int* err;
+    double* out;  // [ndir][nP]
+};
+
+namespace {
+
+// Per-direction, per-sample sums of the tangent rows: one CTA per direction,
+// one warp per (sample, column), fixed order.
+__global__ void __launch_bounds__(1024) ct_hvp_rowsum_kernel(const double* __restrict__ rows, int ctas, int nacc,
+                                                             int c0, int n0, int c1, int n1, int c2, int n2,
+                                                             double* __restrict__ out)
+{
+    const int d = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int beg[3] = {c0, c1, c2}, cnt[3] = {n0, n1, n2};
+    for (int i = warp; i < 3 * nacc; i += nwarp) {
+        const int k = i / nacc, j = i % nacc;
+        double s = 0.0;
+        for (int b = lane; b < cnt[k]; b += 32) s += rows[((long long)d * ctas + beg[k] + b) * nacc + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) out[(long long)d * 3 * nacc + i] = s;
+    }
+}
+
+// One thread per direction u: the directional derivative of the gradient
+// assembly of ct_finalize_kernel (loss terms, phase-space normalisation,
+// Gaussian constraints, coupling transform), i.e. the row H u.
+__global__ void ct_hvp_finalize_kernel(HvpFinalizeArgs A)
+{
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= A.ndir) return;
+    const int nacc = A.nacc, nP = 2 * A.nc + A.nT;
+    const double* P = A.vsums;
+    const double* Dd = A.vsums + nacc;
+    const double* B = A.vsums + 2 * nacc;
+    const double n_phsp = A.vsums[3 * nacc], Wp = A.vsums[3 * nacc + 1];
+    const double W_data = A.vsums[3 * nacc + 2], W_bkg = A.vsums[3 * nacc + 3];
+    const double* TP = A.tsums + (long long)d * 3 * nacc;
+    const double* TD = TP + nacc;
+    const double* TB = TP + 2 * nacc;
+    const double* u = A.dirs + (long long)d * nP;
+    double* out = A.out + (long long)d * nP;
+    const double* theta = A.params + 2 * A.nc;
+
+    const double pf_raw = n_phsp > 0 ? P[1] / n_phsp : 0.0;
+    const bool clamped = pf_raw <= 1e-30 || isnan(pf_raw) || isinf(pf_raw);
+    const double pf = clamped ? 1e-30 : pf_raw;
+    const double pft = clamped ? 0.0 : TP[1] / n_phsp;
+    const double Weff = W_data - W_bkg;
+    double loss = Dd[0] - B[0] + Weff * log(pf);
+    if (A.err && *A.err) loss = nan("");
+    for (int g = 0; g < A.ngauss; ++g) {
+        const double dl = theta[A.gauss_idx[g]] - A.gauss_ms[2 * g];
+        loss += dl * dl / (2.0 * A.gauss_ms[2 * g + 1] * A.gauss_ms[2 * g + 1]);
+    }
+    if (isnan(loss) || isinf(loss)) {
+        for (int k = 0; k < nP; ++k) out[k] = 0.0;
+        return;
+    }
+    const double s = 1.0 / (Wp > 0 ? Wp : 1.0);
+    const double pf2 = pf * pf;
+    for (int c = 0; c < A.nc; ++c) {
+        double sr = 0.0, si = 0.0;
+        for (int a = 0; a < A.nA; ++a) {
+            if (A.chain[a] != c) continue;
+            const double gr = TD[2 + 2 * a] - TB[2 + 2 * a] + Weff * (TP[2 + 2 * a] * s / pf - P[2 + 2 * a] * s * pft / pf2);
+            const double gi = TD[3 + 2 * a] - TB[3 + 2 * a] + Weff * (TP[3 + 2 * a] * s / pf - P[3 + 2 * a] * s * pft / pf2);
+            const double vr = A.v[2 * a], vi = A.v[2 * a + 1];
+            sr += gr * vr + gi * vi;
+            si += gr * vi - gi * vr;
+        }
+        const double pr = A.params[c], pi = A.params[A.nc + c];
+        double ps = pr * pr + pi * pi;
+        if (ps < 1e-30) ps = 1e-30;
+        out[c] = 2.0 * (sr * pr + si * pi) / ps;
+        out[A.nc + c] = -2.0 * (si * pr - sr * pi) / ps;
+    }
+    const int j0 = 2 + 2 * A.nA;
+    for (int j = 0; j < A.nT; ++j)
+        out[2 * A.nc + j] =
+            TD[j0 + j] - TB[j0 + j] + (Weff / n_phsp) * (TP[j0 + j] / pf - P[j0 + j] * pft / pf2);
+    for (int g = 0; g < A.ngauss; ++g) {
+        const int j = A.gauss_idx[g];
+        out[2 * A.nc + j] += u[2 * A.nc + j] / (A.gauss_ms[2 * g + 1] * A.gauss_ms[2 * g + 1]);
+    }
+}
+
+__global__ void ct_identity_kernel(double* __restrict__ I, int n)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x)
+        I[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
+}
+
+}  // namespace
+
+void Engine::compileHvp()
+{
+    if (k_hvp_) return;
+    bool hit = false;
+    std::string cubin = jitHvpCubin(gen_, &hit);
+    cudaLibrary_t lib;
+    CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+    hvp_lib_ = (void*)lib;
+    cudaKernel_t kp, kh;
+    CT_CUDA(cudaLibraryGetKernel(&kp, lib, "ct_hvp_prologue"));
+    CT_CUDA(cudaLibraryGetKernel(&kh, lib, "ct_hvp_f64"));
+    hvp_block_ = hvpBlock(gen_);
+    const int nacc = 2 + 2 * model_.nAmp() + model_.nTheta();
+    hvp_dsmem_ = nacc * hvp_block_ * (int)sizeof(double);
+    if (hvp_dsmem_ > 48 * 1024)
+        CT_CUDA(cudaFuncSetAttribute((const void*)kh, cudaFuncAttributeMaxDynamicSharedMemorySize, hvp_dsmem_));
+    // CTAs of one direction: one wave of resident CTAs split over the samples
+    int sms = 148;
+    CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    const int occ = residentCtas((void*)kh, hvp_block_, hvp_dsmem_);
+    long long tot = 0;
+    for (int k = 0; k < 3; ++k) tot += samples_[k].n;
+    layoutCtas(sms * occ, tot, hvp_block_, hlay_);
+    const int nP = std::max(1, model_.nParams());
+    hvp_cap_ = std::max(nP, 32);
+    CT_CUDA(cudaMalloc(&d_hdirs_, sizeof(double) * (size_t)nP * nP));
+    CT_CUDA(cudaMalloc(&d_hconsts_, sizeof(double) * 2 * (size_t)hvp_cap_ * std::max(1, gen_.nconst)));
+    CT_CUDA(cudaMalloc(&d_hrows_, sizeof(double) * (size_t)hvp_cap_ * hlay_.grid * nacc));
+    CT_CUDA(cudaMalloc(&d_hvsums_, sizeof(double) * (size_t)sumsSize()));
+    CT_CUDA(cudaMalloc(&d_htsums_, sizeof(double) * (size_t)hvp_cap_ * 3 * nacc));
+    cudaStream_t st;
+    CT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    ct_identity_kernel<<<std::max(1, std::min(1024, (nP * nP + 255) / 256)), 256, 0, st>>>(d_hdirs_, nP);
+    CT_CUDA(cudaGetLastError());
+    CT_CUDA(cudaStreamSynchronize(st));
+    cudaStreamDestroy(st);
+    k_hvp_pro_ = (void*)kp;
+    k_hvp_ = (void*)kh;
+}
+
+void Engine::hvpSums(const double* d_params, const double* d_dirs, int ndir, double* d_tsums, cudaStream_t stream)
+{
+    if (ndir <= 0) return;
+    compileHvp();
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta(), nP = m.nParams();
+    const int nacc = 2 + 2 * nA + nT;
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    CtHvpArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    int ns = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (hlay_.cta[k][1] == 0) continue;
+        CtHvpSampleH& sm = a.s[ns++];
+        const DeviceSample& d = samples_[k];
+        sm.slamp = d.slamp64;
+        sm.kin = d.kin;
+        sm.w = d.w;
+        sm.n = d.n;
+        sm.ld = d.ld;
+        sm.kind = k;
+        sm.cta_begin = hlay_.cta[k][0];
+        sm.cta_count = hlay_.cta[k][1];
+    }
+    a.nsamp = ns;
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.chain = d_amp_chain_;
+    a.ratio = d_ratio_;
+    a.nc = nc;
+    a.nparam = nP;
+    a.consts = d_hconsts_;
+    a.rows = d_hrows_;
+    a.ctas = hlay_.grid;
+    for (int d0 = 0; d0 < ndir; d0 += hvp_cap_) {
+        const int nd = std::min(hvp_cap_, ndir - d0);
+        a.ndir = nd;
+        a.dirs = d_dirs + (size_t)d0 * nP;
+        void* args[] = {&a};
+        CT_CUDA(cudaLaunchKernel(k_hvp_pro_, dim3(nd), dim3(32), args, 0, stream));
+        CT_CUDA(cudaLaunchKernel(k_hvp_, dim3(hlay_.grid, nd), dim3(hvp_block_), args, (size_t)hvp_dsmem_, stream));
+        ct_hvp_rowsum_kernel<<<nd, 1024, 0, stream>>>(d_hrows_, hlay_.grid, nacc, hlay_.cta[0][0], hlay_.cta[0][1],
+                                                      hlay_.cta[1][0], hlay_.cta[1][1], hlay_.cta[2][0], hlay_.cta[2][1],
+                                                      d_tsums + (size_t)d0 * 3 * nacc);
+        CT_CUDA(cudaGetLastError());
+    }
+}
+
+void Engine::finalizeHvp(const double* d_params, const double* d_dirs, int ndir, const double* d_vsums,
+                         const double* d_tsums, double* d_out, cudaStream_t stream)
+{
+    if (ndir <= 0) return;
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    CT_CUDA(cudaGetLastError());
+    HvpFinalizeArgs f;
+    std::memset(&f, 0, sizeof(f));
+    f.vsums = d_vsums;
+    f.tsums = d_tsums;
+    f.dirs = d_dirs;
+    f.params = d_params;
+    f.v = d_v_;
+    f.chain = d_amp_chain_;
+    f.gauss_idx = d_gauss_idx_;
+    f.gauss_ms = d_gauss_ms_;
+    f.ngauss = (int)m.gauss.size();
+    f.nacc = 2 + 2 * nA + nT;
+    f.nA = nA;
+    f.nc = nc;
+    f.nT = nT;
+    f.ndir = ndir;
+    f.err = d_err_;
+    f.out = d_out;
+    ct_hvp_finalize_kernel<<<(ndir + 63) / 64, 64, 0, stream>>>(f);
+    CT_CUDA(cudaGetLastError());
+}
+
+void Engine::hessianVectorProducts(const double* d_params, const double* d_dirs, int ndir, double* d_out,
+                                   cudaStream_t stream)
+{
+    if (ndir <= 0) return;
+    compileHvp();
+    shardSums(d_params, kFP64, d_hvsums_, stream);
+    for (int d0 = 0; d0 < ndir; d0 += hvp_cap_) {
+        const int nd = std::min(hvp_cap_, ndir - d0);
+        const size_t off = (size_t)d0 * model_.nParams();
+        hvpSums(d_params, d_dirs + off, nd, d_htsums_, stream);
+        finalizeHvp(d_params, d_dirs + off, nd, d_hvsums_, d_htsums_, d_out + off, stream);
+    }
+}
+
+void Engine::hessianExact(const double* d_params, double* d_hess, cudaStream_t stream)
+{
+    compileHvp();
+    const int n = model_.nParams();
+    hessianVectorProducts(d_params, d_hdirs_, n, d_hess, stream);
     ct_symmetrize_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, stream>>>(d_hess, n);
     CT_CUDA(cudaGetLastError());
 }

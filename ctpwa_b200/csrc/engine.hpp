@@ -81,6 +81,22 @@ public:
     // h_i = rel_step * max(|p_i|, 1e-2), 2 nP gradient evaluations queued on
     // the stream with no host synchronisation.
     void hessian(const double* d_params, double* d_hess, double rel_step, cudaStream_t stream);
+    // Exact FP64 Hessian-vector products, forward mode over the adjoint pass:
+    // for directions u_d (device [ndir][nP], parameter layout) the rows H u_d
+    // (device [ndir][nP]). Every evaluation recomputes the lineshapes and
+    // amplitudes in dual numbers; no per-parameter table is stored. The
+    // kernels are compiled on the first call.
+    void hessianVectorProducts(const double* d_params, const double* d_dirs, int ndir, double* d_out,
+                               cudaStream_t stream);
+    // The full Hessian from the nP unit directions, symmetrised.
+    void hessianExact(const double* d_params, double* d_hess, cudaStream_t stream);
+    // Event-sharded form: this handle's per-sample tangent sums
+    // [ndir][3][nacc] (ready to be summed over shards like shardSums), and the
+    // rows H u_d from summed value sums (shardSums, FP64) and tangent sums.
+    void hvpSums(const double* d_params, const double* d_dirs, int ndir, double* d_tsums, cudaStream_t stream);
+    void finalizeHvp(const double* d_params, const double* d_dirs, int ndir, const double* d_vsums,
+                     const double* d_tsums, double* d_out, cudaStream_t stream);
+    int hvpSumsSize(int ndir) const { return ndir * 3 * (2 + 2 * model_.nAmp() + model_.nTheta()); }
     // Partial-wave integrals sum_e w_e sum_p |sum_{a in block i} v_a A_{a,p}|^2
     // per resonance block i over sample `kind` (0 phase space, 1 data,
     // 2 background, 3 phase-space truth from the config's Data.phsp_truth,
@@ -120,6 +136,7 @@ private:
     void buildTables();
     void computeAngular(int kind);
     void compileKernel();
+    void compileHvp();
 
     Model model_;
     EngineOptions opt_;
@@ -153,8 +170,8 @@ private:
     double* d_consts_ = nullptr;    // [nconst] parameter-only subexpressions
     double* d_partials_ = nullptr;  // [grid][nacc]
     double* d_parts_ = nullptr;     // [8]
-    double* d_hscratch_ = nullptr;
-    int* d_err_ = nullptr;           // set by a fused kernel whose staged copy did not arrive  // Hessian: perturbed params, two gradients, nll [3 nP + 1]
+    double* d_hscratch_ = nullptr;  // finite-difference Hessian: perturbed params, two gradients, nll [3 nP + 1]
+    int* d_err_ = nullptr;          // set by a fused kernel whose staged copy did not arrive
     int* d_amp_chain_ = nullptr;
     double* d_ratio_ = nullptr;
     int* d_gauss_idx_ = nullptr;
@@ -168,6 +185,20 @@ private:
     FusedShape shape_;
     int residentCtas(void* kernel, int block, int dsmem) const;
     void layoutCtas(int target, long long tot, int block, CtaLayout& lay) const;
+
+    // Hessian-vector products (compiled and allocated on first use)
+    void* hvp_lib_ = nullptr;  // cudaLibrary_t
+    void* k_hvp_pro_ = nullptr;
+    void* k_hvp_ = nullptr;
+    int hvp_block_ = 128;
+    int hvp_dsmem_ = 0;
+    int hvp_cap_ = 0;            // directions per launch
+    CtaLayout hlay_;             // CTAs of one direction over the samples
+    double* d_hdirs_ = nullptr;  // [nP][nP] unit directions
+    double* d_hconsts_ = nullptr;  // [cap][nconst][2]
+    double* d_hrows_ = nullptr;    // [cap][ctas][nacc]
+    double* d_hvsums_ = nullptr;   // value sums
+    double* d_htsums_ = nullptr;   // [cap][3][nacc] tangent sums
 
     cudaStream_t init_stream_ = nullptr;  // initialisation only
 

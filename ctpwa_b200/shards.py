@@ -40,3 +40,20 @@ class _ShardedNLL(torch.autograd.Function):
 def getNLL(ana, params: torch.Tensor, group=None, precision=None) -> torch.Tensor:
     """Differentiable NLL of the union of all ranks' shards (0-d float64 CUDA tensor)."""
     return _ShardedNLL.apply(params, ana, group, precision)
+
+
+def hessian(ana, params: torch.Tensor, group=None) -> torch.Tensor:
+    """Exact FP64 Hessian of the union of all ranks' shards: the FP64 value
+    sums and the tangent sums along every unit direction are each summed with
+    one all-reduce, then every rank forms the same symmetrised matrix."""
+    import torch.distributed as dist
+
+    n = params.numel()
+    dirs = torch.eye(n, dtype=torch.float64, device=params.device)
+    sums = ana.getShardSums(params, "fp64")
+    tsums = ana.getShardHvpSums(params, dirs)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(sums, op=dist.ReduceOp.SUM, group=group)
+        dist.all_reduce(tsums, op=dist.ReduceOp.SUM, group=group)
+    H = ana.finalizeShardHvp(params, dirs, sums, tsums)
+    return 0.5 * (H + H.T)

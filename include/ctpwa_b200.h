@@ -108,6 +108,34 @@ int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll
  * queued on the stream, no host synchronisation, no allocation. */
 int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, double rel_step, void* stream);
 
+/* Replaces: analysis::getHessian — src/Analysis.cu:2689-3378 (with
+ * computeDataHessianContribFast, computePhspHessian, computeUnifiedHessian and
+ * transformExtendedHessian, src/ComputeHessian.cu:149-1556,
+ * src/AmpGen.cu:3020-3540, src/Parameters.cu:348-584).
+ * The exact FP64 Hessian, same layout as ctpwa_hessian: forward-mode
+ * (dual-number) derivatives of the device gradient pass along the n_params
+ * unit directions, symmetrised. The first call on a handle compiles the
+ * kernels (or loads them from the kernel cache) and allocates their buffers;
+ * later calls are queued on the stream without host synchronisation. */
+int ctpwa_hessian_exact(ctpwa_handle* h, const double* d_params, double* d_hess, void* stream);
+
+/* Exact Hessian-vector products (no counterpart in the reference, which only
+ * forms the full matrix): d_out[d] = H(d_params) d_dirs[d] for ndir directions
+ * (device [ndir][n_params] in, [ndir][n_params] out). */
+int ctpwa_hvp(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, double* d_out, void* stream);
+
+/* Event-sharded Hessian-vector products (the multi-GPU form of
+ * ctpwa_hessian_exact; the reference sums per-GPU Hessian contributions with
+ * peer copies, src/Analysis.cu:2689-3378): this handle's per-sample tangent
+ * sums, ctpwa_hvp_sums_size(h, ndir) doubles, to be summed over shards; then
+ * the rows H u_d from the summed value sums (ctpwa_shard_sums, FP64) and the
+ * summed tangent sums. */
+int ctpwa_hvp_sums_size(const ctpwa_handle* h, int ndir);
+int ctpwa_shard_hvp_sums(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, double* d_tsums,
+                         void* stream);
+int ctpwa_finalize_hvp(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, const double* d_vsums,
+                       const double* d_tsums, double* d_out, void* stream);
+
 /* Number of resonance blocks (the partial waves of the fit fractions; the
  * reference's nSLvectors_, src/Analysis.cu:1350). */
 int ctpwa_n_blocks(const ctpwa_handle* h);

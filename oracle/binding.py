@@ -141,3 +141,61 @@ class Oracle:
         out = np.zeros(self.nev[kind])
         self.lib.orc_intensity(self.h, kind, ptr(p), ptr(out))
         return out
+
+    # ---- second derivatives (checkers for the device Hessian) ----
+    # Richardson-extrapolated central differences of the oracle's exact
+    # (dual-number) gradient and of its per-sample sums: D(h) = (f(x+h) -
+    # f(x-h)) / 2h, R = (4 D(h/2) - D(h)) / 3. Steps are rel * max(|p_i|, 1e-2):
+    # with rel = 1e-5 a mass step stays ~1e-3 of a resonance width, and two
+    # step sizes agree to ~2e-10 of the largest Hessian entry (K+K-pi0).
+
+    @staticmethod
+    def _richardson(f, x, u, eps):
+        def d(h):
+            return (f(x + h * u) - f(x - h * u)) / (2 * h)
+
+        return (4 * d(eps / 2) - d(eps)) / 3
+
+    @staticmethod
+    def _step(p, u, rel):
+        m = np.abs(u) > 0
+        return rel * float(np.min(np.maximum(np.abs(p[m]), 1e-2) / np.abs(u[m])))
+
+    def hessian_fd(self, params, rel=1e-5):
+        """[nP, nP] Hessian of the oracle NLL (symmetrised)."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        n = p.size
+        H = np.zeros((n, n))
+        for i in range(n):
+            u = np.zeros(n)
+            u[i] = 1.0
+            H[i] = self._richardson(lambda q: self.nll_grad(q)[1], p, u, self._step(p, u, rel))
+        return 0.5 * (H + H.T)
+
+    def hvp_sums_fd(self, params, dirs, rel=1e-5):
+        """[ndir, 3 nacc] directional derivatives of shard_sums' per-sample sums."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        nacc = 2 + 2 * self.nA + self.nT
+        out = []
+        for u in np.atleast_2d(dirs):
+            out.append(self._richardson(lambda q: self.shard_sums(q)[:3 * nacc], p, u, self._step(p, u, rel)))
+        return np.array(out)
+
+    def finalize_hvp_fd(self, params, dirs, sums, tsums, rel=1e-5):
+        """[ndir, nP] rows H u from value sums and tangent sums: the directional
+        derivative of finalize_sums along (u, tangent sums)."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        s = np.ascontiguousarray(sums, dtype=np.float64)
+        nacc = 2 + 2 * self.nA + self.nT
+        dirs = np.atleast_2d(dirs)
+        tsums = np.asarray(tsums, dtype=np.float64).reshape(len(dirs), 3 * nacc)
+        out = []
+        for u, t in zip(dirs, tsums):
+            x = np.concatenate([p, s])
+            w = np.concatenate([u, t, np.zeros(s.size - 3 * nacc)])
+
+            def f(y):
+                return self.finalize_sums(y[:p.size], y[p.size:])[1]
+
+            out.append(self._richardson(f, x, w, self._step(p, u, rel)))
+        return np.array(out)

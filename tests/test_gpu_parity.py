@@ -159,7 +159,7 @@ def test_hessian_matches_oracle_fd(setups):
     """Device Hessian (central differences of the exact device gradient) vs
     central differences of the oracle's dual-number gradient, same steps."""
     ana, orc, pt, p = setups["kkpi"]
-    H = ana.getHessian(pt).cpu().numpy()
+    H = ana.getHessian(pt, method="fd").cpu().numpy()
     n = p.size
     Ho = np.zeros((n, n))
     for i in range(n):
@@ -173,6 +173,79 @@ def test_hessian_matches_oracle_fd(setups):
     Ho = 0.5 * (Ho + Ho.T)
     assert np.allclose(H, H.T, rtol=0, atol=0)
     assert np.max(np.abs(H - Ho)) <= 1e-6 * np.max(np.abs(Ho)), np.max(np.abs(H - Ho)) / np.max(np.abs(Ho))
+
+
+@pytest.mark.parametrize("name", ["kkpi", "pipi_3rho", "ksks"])
+def test_exact_hessian_matches_oracle(setups, name):
+    """Exact device Hessian (forward mode over the adjoint pass) vs
+    Richardson-extrapolated differences of the oracle's exact gradient
+    (accurate to ~2e-10 of the largest entry). The unsymmetrised rows H e_i
+    come from independent dual-number passes and must already be symmetric
+    to rounding."""
+    import torch
+
+    ana, orc, pt, p = setups[name]
+    n = p.size
+    rows = ana.getHessianVectorProduct(pt, torch.eye(n, dtype=torch.float64)).cpu().numpy()
+    scale = np.max(np.abs(rows))
+    assert np.max(np.abs(rows - rows.T)) <= 1e-11 * scale, np.max(np.abs(rows - rows.T)) / scale
+    H = ana.getHessian(pt).cpu().numpy()
+    assert np.array_equal(H, H.T)
+    Ho = orc.hessian_fd(p)
+    assert np.max(np.abs(H - Ho)) <= 1e-8 * scale, np.max(np.abs(H - Ho)) / scale
+    # central differences of the device gradient (step 1e-5 relative) agree to
+    # their own truncation error, a few 1e-6 of the largest entry
+    Hfd = ana.getHessian(pt, method="fd").cpu().numpy()
+    assert np.max(np.abs(H - Hfd)) <= 1e-5 * scale
+
+
+def test_hessian_vector_products_linear(setups):
+    """H u for arbitrary directions equals the full exact Hessian times u."""
+    import torch
+
+    ana, orc, pt, p = setups["kkpi"]
+    rng = np.random.default_rng(5)
+    U = rng.standard_normal((3, p.size))
+    HU = ana.getHessianVectorProduct(pt, torch.tensor(U)).cpu().numpy()
+    H = ana.getHessian(pt).cpu().numpy()
+    ref = U @ H
+    assert np.max(np.abs(HU - ref)) <= 1e-11 * np.max(np.abs(ref))
+    one = ana.getHessianVectorProduct(pt, torch.tensor(U[1])).cpu().numpy()
+    assert np.array_equal(one[0], HU[1])
+
+
+def test_sharded_exact_hessian(tmp_path):
+    """Two event shards: tangent sums vs the oracle's differentiated shard
+    sums, the finalize vs the oracle's differentiated finalize, and the summed
+    shards' Hessian vs the unsharded one."""
+    import torch
+    import ctpwa_b200
+
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=8_000, n_data=2_000, n_bkg=400, accept_reject=False, seed=5)
+    full = ctpwa_b200.analysis(cfg)
+    p = workloads.true_params(full.getNVector(), full.getFreeResParams()[0].numpy())
+    p[2 * full.getNVector():] *= 1.002
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    n = p.size
+    eye = torch.eye(n, dtype=torch.float64)
+    shards = [ctpwa_b200.analysis(cfg, shard=(r, 2)) for r in range(2)]
+    vs = [a.getShardSums(pt, "fp64") for a in shards]
+    ts = [a.getShardHvpSums(pt, eye) for a in shards]
+    rng = np.random.default_rng(2)
+    U = rng.standard_normal((2, n))
+    for r in range(2):
+        o = Oracle(cfg, shard=(r, 2))
+        t_dev = shards[r].getShardHvpSums(pt, torch.tensor(U)).cpu().numpy().reshape(2, -1)
+        t_orc = o.hvp_sums_fd(p, U)
+        assert np.max(np.abs(t_dev - t_orc)) <= 1e-8 * np.max(np.abs(t_orc)), r
+    vsum, tsum = vs[0] + vs[1], ts[0] + ts[1]
+    H = shards[0].finalizeShardHvp(pt, eye, vsum, tsum).cpu().numpy()
+    Hf = full.getHessianVectorProduct(pt, eye).cpu().numpy()
+    scale = np.max(np.abs(Hf))
+    assert np.max(np.abs(H - Hf)) <= 1e-10 * scale
+    orc = Oracle(cfg)
+    Ho = orc.finalize_hvp_fd(p, np.eye(n), vsum.cpu().numpy(), tsum.cpu().numpy())
+    assert np.max(np.abs(H - Ho)) <= 1e-8 * scale
 
 
 def test_partial_integrals_and_fit_fractions(setups, tmp_path):

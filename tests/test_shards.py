@@ -38,6 +38,42 @@ def _rank(rank, world, cfg, p, port, q):
         dist.destroy_process_group()
 
 
+def _rank_hessian(rank, world, cfg, p, port, q):
+    import sys
+
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, ROOT)
+    from ctpwa_b200 import shards
+    from oracle.binding import Oracle as Orc
+
+    class OracleShard:
+        """CPU stand-in for a sharded analysis handle: value sums from the
+        oracle; tangent sums and the finalize by differentiating the oracle's."""
+
+        def __init__(self):
+            self.o = Orc(cfg, shard=(rank, world))
+
+        def getShardSums(self, params, precision=None):
+            return torch.from_numpy(self.o.shard_sums(params.numpy(), nthreads=2))
+
+        def getShardHvpSums(self, params, dirs):
+            return torch.from_numpy(self.o.hvp_sums_fd(params.numpy(), dirs.numpy()).ravel())
+
+        def finalizeShardHvp(self, params, dirs, sums, tsums):
+            return torch.from_numpy(self.o.finalize_hvp_fd(params.numpy(), dirs.numpy(), sums.numpy(), tsums.numpy()))
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        H = shards.hessian(OracleShard(), torch.from_numpy(p))
+        q.put((rank, H.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
 @pytest.fixture(scope="module")
 def workload(tmp_path_factory):
     d = tmp_path_factory.mktemp("shards")
@@ -81,3 +117,25 @@ def test_two_gloo_ranks_equal_unsharded(workload):
         assert abs(nll - onll) <= 1e-10 * abs(onll), (rank, nll, onll)
         assert np.max(np.abs(g - og)) <= 1e-9 * np.max(np.abs(og))
     assert sum(np.array(r[3]) for r in res).tolist() == list(full.nev)
+
+
+def test_two_gloo_ranks_hessian_equals_unsharded(workload):
+    """shards.hessian: value sums and tangent sums each all-reduced once; the
+    Hessian of the union equals the unsharded oracle Hessian."""
+    cfg, p, full = workload
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 30500 + (os.getpid() % 1000)
+    procs = [ctx.Process(target=_rank_hessian, args=(r, 2, cfg, p, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    res = [q.get(timeout=600) for _ in procs]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    Ho = full.hessian_fd(p)
+    scale = np.max(np.abs(Ho))
+    for rank, H in res:
+        assert np.array_equal(H, H.T)
+        assert np.max(np.abs(H - Ho)) <= 1e-8 * scale, (rank, np.max(np.abs(H - Ho)) / scale)
+    assert np.array_equal(res[0][1], res[1][1])
