@@ -295,9 +295,11 @@ def algorithmic_bytes(layout, n_events, precision):
 
 
 def streamed_bytes(layout, n_events, precision):
-    """Bytes the fused kernel actually reads per evaluation in this layout."""
+    """Bytes the fused kernel actually reads per evaluation in this layout:
+    angular values plus the per-event frontier values."""
     sc = 16 if precision == "fp64" else 8
-    per = layout["planes"] * layout["npol"] * sc + layout["nkin"] * 8
+    ev = layout["nev64"] * 8 if precision == "fp64" else layout["nevf"] * 4 + layout["nevd"] * 8
+    per = layout["planes"] * layout["npol"] * sc + ev
     n_p, n_d, n_b = n_events
     return per * (n_p + n_d + n_b) + 8 * n_b
 

@@ -469,12 +469,18 @@ class analysis:
         return out
 
     def eventLayout(self) -> dict:
-        """Per-event cache layout: angular planes, polarisations, kinematic values, invariant masses."""
+        """Per-event cache layout: angular planes, polarisations, kinematic values,
+        invariant masses, and the frontier values each evaluation reads (FP64
+        plain path; FP32 and FP64 values of the mixed form)."""
         self._check()
         out = (ctypes.c_int * 4)()
         if self._lib.ctpwa_event_layout(self._h, out) != 0:
             raise RuntimeError(_lib.error(self._h))
-        return {"planes": out[0], "npol": out[1], "nkin": out[2], "nmass": out[3]}
+        ev = (ctypes.c_int * 3)()
+        if self._lib.ctpwa_event_cache_layout(self._h, ev) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return {"planes": out[0], "npol": out[1], "nkin": out[2], "nmass": out[3], "nev64": ev[0], "nevf": ev[1],
+                "nevd": ev[2]}
 
     def setKernelTiming(self, slots: int):
         """Record CUDA events around each fused-kernel launch (ring of `slots`; 0 = off)."""

@@ -338,6 +338,16 @@ int ctpwa_event_layout(const ctpwa_handle* h, int* out4)
     return CTPWA_OK;
 }
 
+int ctpwa_event_cache_layout(const ctpwa_handle* h, int* out3)
+{
+    if (!h || !out3) return CTPWA_ERR_ARG;
+    const ctpwa::GeneratedModel& g = h->eng->generated();
+    out3[0] = g.nev64;
+    out3[1] = g.nevf;
+    out3[2] = g.nevd;
+    return CTPWA_OK;
+}
+
 int ctpwa_kernel_timing(ctpwa_handle* h, int slots)
 {
     if (!h) return CTPWA_ERR_ARG;

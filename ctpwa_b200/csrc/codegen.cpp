@@ -767,69 +767,105 @@ std::string Gen::emit()
     }
 
     // ---------------- per-event code ----------------
-    // f32 = false: everything in FP64.
-    // f32 = true: the mixed form. Event nodes built from kinematic values and
-    // constants by + - * only, that feed a subtraction (or an addition of
-    // terms of unknown sign), stay FP64, so the cancellation in m0^2 - m^2
-    // and the like happens in full precision; transcendental functions are
-    // FP64 too (their FP32 versions are not correctly rounded, and a bias
-    // would not average out over a sample); everything else is FP32 with
-    // correctly rounded reciprocals and square roots.
-    auto events = [&](bool f32) -> std::string {
-        std::vector<char> cap(N.size(), 0), dbl(N.size(), 0);
-        if (f32) {
-            for (size_t x = 0; x < N.size(); ++x) {
-                const auto& nd = N[x];
-                if (!live[x] || !(nd.dep & dag::DEP_EVENT)) continue;
-                if (nd.op == dag::Kin) {
-                    cap[x] = nd.idx >= 0;
-                    continue;
-                }
-                if (nd.op != dag::Add && nd.op != dag::Sub && nd.op != dag::Mul && nd.op != dag::Neg) continue;
-                bool ok = true;
-                for (int k : {nd.a, nd.b})
-                    if (k >= 0 && (N[k].dep & dag::DEP_EVENT) && !cap[k]) ok = false;
-                cap[x] = ok;
+    // Event nodes come in two kinds. Event-only nodes (kinematic values,
+    // table lookups and everything built from them and constants) do not
+    // change between likelihood calls: model_event / model_event_mx evaluate
+    // them once per event when a sample is loaded and keep, as per-event
+    // tables, the ones that parameter-dependent nodes or the outputs consume
+    // (the frontier). The per-call code (model_columns*) evaluates only the
+    // parameter-dependent nodes, reading frontier values from those tables.
+    //
+    // Precision of the mixed form (f32): event nodes built from kinematic
+    // values and constants by + - * only, that feed a subtraction (or an
+    // addition of terms of unknown sign), stay FP64, so the cancellation in
+    // m0^2 - m^2 and the like happens in full precision; transcendental
+    // functions are FP64 too (their FP32 versions are not correctly rounded,
+    // and a bias would not average out over a sample); everything else is
+    // FP32 with correctly rounded reciprocals and square roots. Frontier
+    // values are stored in the precision they are computed in (kinematic
+    // values and table lookups as FP64).
+    std::vector<char> cap(N.size(), 0), dbl(N.size(), 0);
+    {
+        for (size_t x = 0; x < N.size(); ++x) {
+            const auto& nd = N[x];
+            if (!live[x] || !(nd.dep & dag::DEP_EVENT)) continue;
+            if (nd.op == dag::Kin) {
+                cap[x] = nd.idx >= 0;
+                continue;
             }
-            // nodes known to be >= 0 (an addition of two of them cannot cancel)
-            std::vector<char> nonneg(N.size(), 0);
-            for (size_t x = 0; x < N.size(); ++x) {
-                const auto& nd = N[x];
-                switch (nd.op) {
-                case dag::Const: nonneg[x] = nd.v >= 0.0; break;
-                case dag::Kin:
-                    nonneg[x] = nd.idx >= 0 && out.slots[nd.idx].type != AG_K_CT_ && out.slots[nd.idx].type != AG_K_PHI_;
-                    break;
-                case dag::Mul: nonneg[x] = nd.a == nd.b || (nonneg[nd.a] && nonneg[nd.b]); break;
-                case dag::Add: nonneg[x] = nonneg[nd.a] && nonneg[nd.b]; break;
-                case dag::Recip:
-                case dag::Sqrt: nonneg[x] = nonneg[nd.a]; break;
-                case dag::Exp: nonneg[x] = 1; break;
-                default: break;
-                }
-            }
-            for (size_t x = 0; x < N.size(); ++x) {
-                const auto& nd = N[x];
-                if (live[x] && (nd.dep & dag::DEP_EVENT) &&
-                    (nd.op == dag::Log || nd.op == dag::Exp || nd.op == dag::Sin || nd.op == dag::Cos || nd.op == dag::Atan2))
-                    dbl[x] = 1;
-            }
-            for (size_t x = N.size(); x-- > 0;) {
-                const auto& nd = N[x];
-                if (!cap[x]) continue;
-                if (nd.op == dag::Sub) dbl[x] = 1;
-                if (nd.op == dag::Add && nd.a != nd.b && !(nonneg[nd.a] && nonneg[nd.b])) dbl[x] = 1;
-                if (!dbl[x]) continue;
-                for (int k : {nd.a, nd.b})
-                    if (k >= 0 && cap[k]) dbl[k] = 1;
+            if (nd.op != dag::Add && nd.op != dag::Sub && nd.op != dag::Mul && nd.op != dag::Neg) continue;
+            bool ok = true;
+            for (int k : {nd.a, nd.b})
+                if (k >= 0 && (N[k].dep & dag::DEP_EVENT) && !cap[k]) ok = false;
+            cap[x] = ok;
+        }
+        // nodes known to be >= 0 (an addition of two of them cannot cancel)
+        std::vector<char> nonneg(N.size(), 0);
+        for (size_t x = 0; x < N.size(); ++x) {
+            const auto& nd = N[x];
+            switch (nd.op) {
+            case dag::Const: nonneg[x] = nd.v >= 0.0; break;
+            case dag::Kin:
+                nonneg[x] = nd.idx >= 0 && out.slots[nd.idx].type != AG_K_CT_ && out.slots[nd.idx].type != AG_K_PHI_;
+                break;
+            case dag::Mul: nonneg[x] = nd.a == nd.b || (nonneg[nd.a] && nonneg[nd.b]); break;
+            case dag::Add: nonneg[x] = nonneg[nd.a] && nonneg[nd.b]; break;
+            case dag::Recip:
+            case dag::Sqrt: nonneg[x] = nonneg[nd.a]; break;
+            case dag::Exp: nonneg[x] = 1; break;
+            default: break;
             }
         }
-        // reference to node x from a consumer evaluated in FP32 (wantF) or FP64
-        auto ref = [&](int x, bool wantF) -> std::string {
+        for (size_t x = 0; x < N.size(); ++x) {
+            const auto& nd = N[x];
+            if (live[x] && (nd.dep & dag::DEP_EVENT) &&
+                (nd.op == dag::Log || nd.op == dag::Exp || nd.op == dag::Sin || nd.op == dag::Cos || nd.op == dag::Atan2))
+                dbl[x] = 1;
+        }
+        for (size_t x = N.size(); x-- > 0;) {
+            const auto& nd = N[x];
+            if (!cap[x]) continue;
+            if (nd.op == dag::Sub) dbl[x] = 1;
+            if (nd.op == dag::Add && nd.a != nd.b && !(nonneg[nd.a] && nonneg[nd.b])) dbl[x] = 1;
+            if (!dbl[x]) continue;
+            for (int k : {nd.a, nd.b})
+                if (k >= 0 && cap[k]) dbl[k] = 1;
+        }
+    }
+    auto evOnly = [&](int x) { return N[x].dep == dag::DEP_EVENT && N[x].op != dag::Const; };
+    auto mixedDep = [&](int x) { return (N[x].dep & dag::DEP_EVENT) && (N[x].dep & dag::DEP_THETA); };
+    // frontier slots: FP64 table (all), mixed tables (FP32 / FP64 values)
+    std::vector<int> fs64(N.size(), -1), fsF(N.size(), -1), fsD(N.size(), -1);
+    {
+        std::vector<char> front(N.size(), 0);
+        for (size_t x = 0; x < N.size(); ++x) {
+            if (!live[x] || !mixedDep((int)x)) continue;
+            for (int k : {N[x].a, N[x].b, N[x].c})
+                if (k >= 0 && evOnly(k)) front[k] = 1;
+        }
+        for (const auto& c : cols) {
+            for (int r : {c.re, c.im})
+                if (r >= 0 && evOnly(r)) front[r] = 1;
+            for (const auto& d : c.der)
+                for (int r : {d.second.first, d.second.second})
+                    if (r >= 0 && evOnly(r)) front[r] = 1;
+        }
+        for (size_t x = 0; x < N.size(); ++x) {
+            if (!front[x]) continue;
+            fs64[x] = out.nev64++;
+            if (!dbl[x] && N[x].op != dag::Kin) fsF[x] = out.nevf++;
+            else fsD[x] = out.nevd++;
+        }
+    }
+    using RefFn = std::function<std::string(int, bool)>;
+    // reference to a kinematic leaf, a table lookup or an event node from the
+    // once-per-event code, for a consumer evaluated in FP32 (wantF) or FP64
+    auto preRef = [&](bool f32) -> RefFn {
+        return [&, f32](int x, bool wantF) -> std::string {
             const auto& nd = N[x];
             if (nd.op == dag::Const) return wantF ? numf(nd.v) : num(nd.v);
-            if (nd.dep == dag::DEP_THETA) return (wantF ? "Cfh[" : "C[") + std::to_string(cslot[x]) + "]";
-            if (nd.op == dag::Kin && nd.idx >= 0) return (wantF ? "kf" : "kv[") + std::to_string(nd.idx) + (wantF ? "" : "]");
+            if (nd.op == dag::Kin && nd.idx >= 0)
+                return (wantF ? "kf" : "kv[") + std::to_string(nd.idx) + (wantF ? "" : "]");
             if (nd.op == dag::Kin) {
                 int u = (-nd.idx - 1000) / 2;
                 std::string v = ((-nd.idx - 1000) % 2 == 0 ? "tre" : "tim") + std::to_string(u);
@@ -841,7 +877,88 @@ std::string Gen::emit()
             if (!wantF && isF) return "(double)" + v;
             return v;
         };
+    };
+    // the same from the per-call code: event-only operands are frontier values
+    auto colRef = [&](bool f32) -> RefFn {
+        return [&, f32](int x, bool wantF) -> std::string {
+            const auto& nd = N[x];
+            if (nd.op == dag::Const) return wantF ? numf(nd.v) : num(nd.v);
+            if (nd.dep == dag::DEP_THETA) return (wantF ? "Cfh[" : "C[") + std::to_string(cslot[x]) + "]";
+            if (evOnly(x)) {
+                if (fs64[x] < 0) throw std::logic_error("codegen: event value outside the frontier");
+                if (!f32) return "ev[" + std::to_string(fs64[x]) + "]";
+                if (fsF[x] >= 0) return (wantF ? "evf[" : "(double)evf[") + std::to_string(fsF[x]) + "]";
+                return (wantF ? "(float)evd[" : "evd[") + std::to_string(fsD[x]) + "]";
+            }
+            bool isF = f32 && !dbl[x];
+            std::string v = "e" + std::to_string(x);
+            if (wantF && !isF) return "(float)" + v;
+            if (!wantF && isF) return "(double)" + v;
+            return v;
+        };
+    };
+    // definition of event node x
+    auto nodeLine = [&](size_t x, bool f32, const RefFn& ref) -> std::string {
+        const auto& nd = N[x];
+        bool isF = f32 && !dbl[x];
+        std::string A, B, Cc;
+        if (nd.op == dag::RhoRe || nd.op == dag::RhoIm) {
+            // channel factors are evaluated by an FP64 helper
+            A = ref(nd.a, false);
+            B = ref(nd.b, false);
+            Cc = ref(nd.c, false);
+        } else {
+            A = nd.a >= 0 ? ref(nd.a, isF) : "";
+            B = nd.b >= 0 ? ref(nd.b, isF) : "";
+            if (nd.c >= 0) {
+                // the condition is tested in the precision it was computed in
+                const auto& cn = N[nd.c];
+                bool cF = f32 && (cn.dep & dag::DEP_EVENT) && cn.op != dag::Kin && !dbl[nd.c];
+                Cc = ref(nd.c, cF);
+            }
+        }
+        std::string rhs = opExpr(nd, A, B, Cc, isF);
+        if (isF && (nd.op == dag::Add || nd.op == dag::Sub || nd.op == dag::Mul)) {
+            // An event-independent operand enters as hi + lo and the
+            // product is rounded once (fmaf): rounding it to FP32 first
+            // would bias every event alike, and so would rounding the
+            // product of two FP32-grid factors (structured low bits).
+            std::string hi, lo;
+            auto split = [&](int y) -> bool {
+                const auto& yn = N[y];
+                if (yn.op == dag::Const) {
+                    float h = (float)yn.v;
+                    double l = yn.v - (double)h;
+                    if (l == 0.0 || !std::isfinite(yn.v)) return false;
+                    hi = numf((double)h);
+                    lo = numf(l);
+                    return true;
+                }
+                if (yn.dep == dag::DEP_THETA) {
+                    hi = "Cfh[" + std::to_string(cslot[y]) + "]";
+                    lo = "Cfl[" + std::to_string(cslot[y]) + "]";
+                    return true;
+                }
+                return false;
+            };
+            const bool ca = split(nd.a);
+            const std::string ha = hi, la = lo;
+            const bool cb = split(nd.b);
+            const std::string hb = hi, lb = lo;
+            if (ca != cb) {
+                const std::string ev = ca ? B : A, h = ca ? ha : hb, l = ca ? la : lb;
+                if (nd.op == dag::Mul) rhs = "fmaf(" + ev + ", " + h + ", " + ev + " * " + l + ")";
+                else if (nd.op == dag::Add) rhs = "(" + ev + " + " + h + ") + " + l;
+                else if (ca) rhs = "(" + h + " - " + ev + ") + " + l;  // const - event
+                else rhs = "(" + ev + " - " + h + ") - " + l;          // event - const
+            }
+        }
+        return std::string("  const ") + (isF ? "float" : "double") + " e" + std::to_string(x) + " = " + rhs + ";\n";
+    };
+    // once per event: event-only nodes, then the frontier values
+    auto eventPart = [&](bool f32) -> std::string {
         std::ostringstream evs;
+        const RefFn ref = preRef(f32);
         if (f32)
             for (size_t k = 0; k < out.slots.size(); ++k)
                 evs << "  const float kf" << k << " = (float)kv[" << k << "]; (void)kf" << k << ";\n";
@@ -854,65 +971,23 @@ std::string Gen::emit()
                 evs << "  const double tre" << u << " = ls_hist(" << ref(t.mnode, false) << ", ct_tab" << t.table
                     << "), tim" << u << " = 0.0;\n";
         }
+        for (size_t x = 0; x < N.size(); ++x)
+            if (live[x] && evOnly((int)x) && N[x].op != dag::Kin) evs << nodeLine(x, f32, ref);
         for (size_t x = 0; x < N.size(); ++x) {
-            const auto& nd = N[x];
-            if (!live[x] || nd.op == dag::Const || nd.op == dag::Theta || nd.op == dag::Kin) continue;
-            if (!(nd.dep & dag::DEP_EVENT)) continue;
-            bool isF = f32 && !dbl[x];
-            std::string A, B, Cc;
-            if (nd.op == dag::RhoRe || nd.op == dag::RhoIm) {
-                // channel factors are evaluated by an FP64 helper
-                A = ref(nd.a, false);
-                B = ref(nd.b, false);
-                Cc = ref(nd.c, false);
-            } else {
-                A = nd.a >= 0 ? ref(nd.a, isF) : "";
-                B = nd.b >= 0 ? ref(nd.b, isF) : "";
-                if (nd.c >= 0) {
-                    // the condition is tested in the precision it was computed in
-                    const auto& cn = N[nd.c];
-                    bool cF = f32 && (cn.dep & dag::DEP_EVENT) && cn.op != dag::Kin && !dbl[nd.c];
-                    Cc = ref(nd.c, cF);
-                }
-            }
-            std::string rhs = opExpr(nd, A, B, Cc, isF);
-            if (isF && (nd.op == dag::Add || nd.op == dag::Sub || nd.op == dag::Mul)) {
-                // An event-independent operand enters as hi + lo and the
-                // product is rounded once (fmaf): rounding it to FP32 first
-                // would bias every event alike, and so would rounding the
-                // product of two FP32-grid factors (structured low bits).
-                std::string hi, lo;
-                auto split = [&](int y) -> bool {
-                    const auto& yn = N[y];
-                    if (yn.op == dag::Const) {
-                        float h = (float)yn.v;
-                        double l = yn.v - (double)h;
-                        if (l == 0.0 || !std::isfinite(yn.v)) return false;
-                        hi = numf((double)h);
-                        lo = numf(l);
-                        return true;
-                    }
-                    if (yn.dep == dag::DEP_THETA) {
-                        hi = "Cfh[" + std::to_string(cslot[y]) + "]";
-                        lo = "Cfl[" + std::to_string(cslot[y]) + "]";
-                        return true;
-                    }
-                    return false;
-                };
-                const bool ca = split(nd.a);
-                const std::string ha = hi, la = lo;
-                const bool cb = split(nd.b);
-                const std::string hb = hi, lb = lo;
-                if (ca != cb) {
-                    const std::string ev = ca ? B : A, h = ca ? ha : hb, l = ca ? la : lb;
-                    if (nd.op == dag::Mul) rhs = "fmaf(" + ev + ", " + h + ", " + ev + " * " + l + ")";
-                    else if (nd.op == dag::Add) rhs = "(" + ev + " + " + h + ") + " + l;
-                    else if (ca) rhs = "(" + h + " - " + ev + ") + " + l;  // const - event
-                    else rhs = "(" + ev + " - " + h + ") - " + l;          // event - const
-                }
-            }
-            evs << "  const " << (isF ? "float" : "double") << " e" << x << " = " << rhs << ";\n";
+            if (fs64[x] < 0) continue;
+            if (!f32) evs << "  o[" << fs64[x] << "] = " << ref((int)x, false) << ";\n";
+            else if (fsF[x] >= 0) evs << "  of[" << fsF[x] << "] = " << ref((int)x, true) << ";\n";
+            else evs << "  od[" << fsD[x] << "] = " << ref((int)x, false) << ";\n";
         }
+        return evs.str();
+    };
+    // per call: parameter-dependent event nodes and the outputs
+    auto callPart = [&](bool f32) -> std::string {
+        std::ostringstream evs;
+        const RefFn ref = colRef(f32);
+        for (size_t x = 0; x < N.size(); ++x)
+            if (live[x] && mixedDep((int)x) && N[x].op != dag::Const && N[x].op != dag::Theta && N[x].op != dag::Kin)
+                evs << nodeLine(x, f32, ref);
         int k = 0;
         for (size_t a = 0; a < cols.size(); ++a) {
             evs << "  Fr[" << a << "] = " << ref(cols[a].re, f32) << "; Fi[" << a << "] = " << ref(cols[a].im, f32) << ";\n";
@@ -926,22 +1001,17 @@ std::string Gen::emit()
     };
 
     // ---------------- dual-number form (Hessian-vector products) ----------------
-    // The same FP64 code in which every value that depends on the resonance
-    // parameters is a CtDual (value, directional derivative): the prologue
-    // runs on dual theta leaves, event nodes that depend on theta become dual,
-    // purely kinematic nodes stay double. Channel factors and table lookups
-    // take plain values (their parameter derivative is zero, as in the
-    // symbolic derivatives above).
+    // The per-call FP64 code in which every parameter-dependent value is a
+    // CtDual (value, directional derivative): the prologue runs on dual theta
+    // leaves, parameter-dependent event nodes become dual, frontier values
+    // stay plain doubles. Channel factors take plain values (their parameter
+    // derivative is zero, as in the symbolic derivatives above).
     {
         auto dualRef = [&](int x) -> std::string {
             const auto& nd = N[x];
             if (nd.op == dag::Const) return num(nd.v);
             if (nd.dep == dag::DEP_THETA) return "C[" + std::to_string(cslot[x]) + "]";
-            if (nd.op == dag::Kin && nd.idx >= 0) return "kv[" + std::to_string(nd.idx) + "]";
-            if (nd.op == dag::Kin) {
-                int u = (-nd.idx - 1000) / 2;
-                return ((-nd.idx - 1000) % 2 == 0 ? "tre" : "tim") + std::to_string(u);
-            }
+            if (evOnly(x)) return "ev[" + std::to_string(fs64[x]) + "]";
             return "e" + std::to_string(x);
         };
         auto plain = [](const std::string& s) { return "ct_value(" + s + ")"; };
@@ -961,21 +1031,10 @@ std::string Gen::emit()
             if (N[x].op != dag::Theta) dpro << "  const CtDual t" << x << " = " << rhs(N[x], proRef) << ";\n";
             if (cslot[x] >= 0) dpro << "  C[" << cslot[x] << "] = " << proRef((int)x) << ";\n";
         }
-        for (size_t u = 0; u < tab_uses.size(); ++u) {
-            const auto& t = tab_uses[u];
-            if (t.interp)
-                dev << "  double tre" << u << ", tim" << u << "; ls_interp(ct_tab" << t.table << ", "
-                    << plain(dualRef(t.mnode)) << ", tre" << u << ", tim" << u << ");\n";
-            else
-                dev << "  const double tre" << u << " = ls_hist(" << plain(dualRef(t.mnode)) << ", ct_tab" << t.table
-                    << "), tim" << u << " = 0.0;\n";
-        }
         for (size_t x = 0; x < N.size(); ++x) {
             const auto& nd = N[x];
-            if (!live[x] || nd.op == dag::Const || nd.op == dag::Theta || nd.op == dag::Kin) continue;
-            if (!(nd.dep & dag::DEP_EVENT)) continue;
-            dev << "  const " << ((nd.dep & dag::DEP_THETA) ? "CtDual" : "double") << " e" << x << " = "
-                << rhs(nd, dualRef) << ";\n";
+            if (!live[x] || !mixedDep((int)x) || nd.op == dag::Const || nd.op == dag::Theta || nd.op == dag::Kin) continue;
+            dev << "  const CtDual e" << x << " = " << rhs(nd, dualRef) << ";\n";
         }
         int q = 0;
         for (size_t a = 0; a < cols.size(); ++a) {
@@ -993,9 +1052,9 @@ std::string Gen::emit()
               "  (void)th; (void)C;\n"
            << dpro.str() << "}\n";
         dh << "// per-event lineshape products, their theta derivatives, and the directional\n"
-              "// derivatives of both (FP64)\n";
-        dh << "__device__ __forceinline__ void model_columns_dual(const double* __restrict__ kv, const CtDual* __restrict__ C,\n"
-              "    CtDual* Fr, CtDual* Fi, CtDual* dFr, CtDual* dFi)\n{\n  (void)kv; (void)C; (void)dFr; (void)dFi;\n"
+              "// derivatives of both (FP64), from the event's frontier values\n";
+        dh << "__device__ __forceinline__ void model_columns_dual(const double* __restrict__ ev, const CtDual* __restrict__ C,\n"
+              "    CtDual* Fr, CtDual* Fi, CtDual* dFr, CtDual* dFi)\n{\n  (void)ev; (void)C; (void)dFr; (void)dFi;\n"
            << dev.str() << "}\n";
         out.dual_header = dh.str();
     }
@@ -1016,6 +1075,7 @@ std::string Gen::emit()
     h << "#define M_NA " << m.nAmp() << "\n#define M_NTERM " << cols.size() << "\n#define M_NPOL " << m.npol
       << "\n#define M_NPLANE " << out.nplane << "\n#define M_NKIN " << out.slots.size() << "\n#define M_NTH "
       << m.nTheta() << "\n#define M_NDER " << k << "\n#define M_NCONST " << ncon << "\n";
+    h << "#define M_NEV " << out.nev64 << "\n#define M_NEVF " << out.nevf << "\n#define M_NEVD " << out.nevd << "\n";
     // terms: amplitude column and angular plane of each
     std::vector<int> tcol, tplane;
     for (const auto& t : cols) {
@@ -1044,16 +1104,27 @@ std::string Gen::emit()
     h << "__device__ __forceinline__ void model_prologue(const double* __restrict__ th, double* __restrict__ C)\n{\n"
          "  (void)th; (void)C;\n"
       << pro.str() << "}\n";
-    h << "// per-event lineshape products and their parameter derivatives (FP64)\n";
-    h << "__device__ __forceinline__ void model_columns(const double* __restrict__ kv, const double* __restrict__ C,\n"
-         "    double* Fr, double* Fi, double* dFr, double* dFi)\n{\n  (void)kv; (void)C; (void)dFr; (void)dFi;\n"
-      << events(false) << "}\n";
+    h << "// once per event (sample loading): the parameter-independent values the\n"
+         "// per-call code reads (frontier), FP64\n";
+    h << "__device__ __forceinline__ void model_event(const double* __restrict__ kv, double* __restrict__ o)\n{\n"
+         "  (void)kv; (void)o;\n"
+      << eventPart(false) << "}\n";
+    h << "// the same for the mixed form: FP32 values (of) and FP64 values (od)\n";
+    h << "__device__ __forceinline__ void model_event_mx(const double* __restrict__ kv, float* __restrict__ of,\n"
+         "    double* __restrict__ od)\n{\n  (void)kv; (void)of; (void)od;\n"
+      << eventPart(true) << "}\n";
+    h << "// per-event lineshape products and their parameter derivatives (FP64) from the\n"
+         "// event's frontier values\n";
+    h << "__device__ __forceinline__ void model_columns(const double* __restrict__ ev, const double* __restrict__ C,\n"
+         "    double* Fr, double* Fi, double* dFr, double* dFi)\n{\n  (void)ev; (void)C; (void)dFr; (void)dFi;\n"
+      << callPart(false) << "}\n";
     h << "// the same in the mixed form (FP32 except cancellation-prone polynomial parts and\n"
          "// transcendental functions; parameter-only constants enter as hi + lo FP32 pairs)\n";
-    h << "__device__ __forceinline__ void model_columns_f32(const double* __restrict__ kv, const double* __restrict__ C,\n"
-         "    const float* __restrict__ Cfh, const float* __restrict__ Cfl, float* Fr, float* Fi, float* dFr, float* dFi)\n{\n"
-         "  (void)kv; (void)C; (void)Cfh; (void)Cfl; (void)dFr; (void)dFi;\n"
-      << events(true) << "}\n";
+    h << "__device__ __forceinline__ void model_columns_f32(const float* __restrict__ evf, const double* __restrict__ evd,\n"
+         "    const double* __restrict__ C, const float* __restrict__ Cfh, const float* __restrict__ Cfl, float* Fr, float* Fi,\n"
+         "    float* dFr, float* dFi)\n{\n"
+         "  (void)evf; (void)evd; (void)C; (void)Cfh; (void)Cfl; (void)dFr; (void)dFi;\n"
+      << callPart(true) << "}\n";
     return h.str();
 }
 

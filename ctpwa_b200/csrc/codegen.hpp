@@ -32,6 +32,11 @@ struct GeneratedModel {
     std::vector<int> group_plane0;
     int nder = 0;
     int nconst = 0;              // parameter-only subexpressions kept per call
+    // per-event frontier tables (parameter-independent values the per-call
+    // code reads): FP64 table rows; mixed form FP32 and FP64 rows
+    int nev64 = 0;
+    int nevf = 0;
+    int nevd = 0;
 };
 
 GeneratedModel generateModel(const Model& m);

@@ -804,6 +804,9 @@ Engine::~Engine()
         cudaFree(s.slamp64);
         cudaFree(s.slamp32);
         cudaFree(s.kin);
+        cudaFree(s.ev64);
+        cudaFree(s.evf);
+        cudaFree(s.evd);
         cudaFree(s.w);
     }
     cudaFree(d_ag_tables_);
@@ -1072,7 +1075,10 @@ void Engine::computeAngular(int kind)
     size_t bk = sizeof(double) * std::max<size_t>(1, gen_.slots.size()) * ld;
     CT_CUDA(cudaMalloc(&d.kin, bk));
     device_bytes_ += bk;
-    if (n == 0) return;
+    if (n == 0) {
+        buildEventCache(kind);
+        return;
+    }
     AgTables T;
     std::memcpy(&T, ag_host_.data(), sizeof(T));
     for (size_t g = 0; g < group_desc_.size(); ++g) {
@@ -1086,7 +1092,39 @@ void Engine::computeAngular(int kind)
         CT_CUDA(cudaFreeAsync(d.p4, init_stream_));
         d.p4 = nullptr;
     }
+    buildEventCache(kind);
+}
+
+// The per-event frontier tables (parameter-independent values the per-call
+// code reads) from the kinematic cache, once per sample; the kinematic cache
+// is released afterwards.
+void Engine::buildEventCache(int kind)
+{
+    DeviceSample& d = samples_[kind];
+    const long long ld = d.ld;
+    const size_t b64 = sizeof(double) * std::max(1, gen_.nev64) * ld;
+    CT_CUDA(cudaMalloc(&d.ev64, b64));
+    device_bytes_ += b64;
+    if (opt_.mixed_tables) {
+        const size_t bf = sizeof(float) * std::max(1, gen_.nevf) * ld, bd = sizeof(double) * std::max(1, gen_.nevd) * ld;
+        CT_CUDA(cudaMalloc(&d.evf, bf));
+        CT_CUDA(cudaMalloc(&d.evd, bd));
+        device_bytes_ += bf + bd;
+    }
+    if (d.n > 0) {
+        const double* kin = d.kin;
+        long long n = d.n;
+        double* o64 = d.ev64;
+        float* of = d.evf;
+        double* od = d.evd;
+        void* args[] = {(void*)&kin, (void*)&n, (void*)&ld, (void*)&o64, (void*)&of, (void*)&od};
+        const unsigned grid = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 64);
+        CT_CUDA(cudaLaunchKernel(k_evc_, dim3(grid), dim3(256), args, 0, init_stream_));
+    }
     CT_CUDA(cudaStreamSynchronize(init_stream_));
+    cudaFree(d.kin);
+    d.kin = nullptr;
+    device_bytes_ -= sizeof(double) * std::max<size_t>(1, gen_.slots.size()) * ld;
 }
 
 // Block size and minimum resident CTAs per SM of the plain [0] and mixed [1]
@@ -1135,8 +1173,8 @@ FusedShape fusedShape(const GeneratedModel& gen)
             acc_bytes = 0;
         }
         const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
-        const long long stage_bytes =
-            2LL * (npl * rowb[i] + (long long)std::max<size_t>(1, gen.slots.size()) * 8) * sh.block[i];
+        const long long evb = i == 0 ? 8LL * gen.nev64 : 4LL * gen.nevf + 8LL * gen.nevd;  // frontier bytes per event
+        const long long stage_bytes = 2LL * (npl * rowb[i] + evb) * sh.block[i];
         if (stage_on && fits(i, acc_bytes + stage_bytes)) sh.stage[i] = 1;
         sh.dsmem[i] = (int)(acc_bytes + (sh.stage[i] ? stage_bytes : 0));
     }
@@ -1265,6 +1303,9 @@ void Engine::compileKernel()
     cudaKernel_t k64, kmx, kin, kpro;
     CT_CUDA(cudaLibraryGetKernel(&kpro, lib, "ct_prologue"));
     k_pro_ = (void*)kpro;
+    cudaKernel_t kevc;
+    CT_CUDA(cudaLibraryGetKernel(&kevc, lib, "ct_event_cache"));
+    k_evc_ = (void*)kevc;
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
@@ -1299,7 +1340,8 @@ double precompileConfig(const std::string& config_path)
 // argument block of the fused kernel (must match CtArgs in kernels/fused_nll.cuh)
 struct CtSampleH {
     const void* slamp;
-    const double* kin;
+    const void* ev;
+    const double* evd;
     const double* w;
     long long n;
     long long ld;
@@ -1337,7 +1379,8 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
         CtSampleH& s = a.s[ns++];
         const DeviceSample& d = samples_[k];
         s.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
-        s.kin = d.kin;
+        s.ev = precision == kMixed ? (const void*)d.evf : (const void*)d.ev64;
+        s.evd = precision == kMixed ? d.evd : nullptr;
         s.w = d.w;
         s.n = d.n;
         s.ld = d.ld;
@@ -1476,7 +1519,8 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
         CtSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
         sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
-        sm.kin = d.kin;
+        sm.ev = precision == kMixed ? (const void*)d.evf : (const void*)d.ev64;
+        sm.evd = precision == kMixed ? d.evd : nullptr;
         sm.w = d.w;
         sm.n = d.n;
         sm.ld = d.ld;
@@ -1543,7 +1587,8 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
         CtSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
         sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
-        sm.kin = d.kin;
+        sm.ev = precision == kMixed ? (const void*)d.evf : (const void*)d.ev64;
+        sm.evd = precision == kMixed ? d.evd : nullptr;
         sm.w = d.w;
         sm.n = d.n;
         sm.ld = d.ld;
@@ -1673,7 +1718,7 @@ void Engine::hessian(const double* d_params, double* d_hess, double rel_step, cu
 // argument block of the Hessian-vector-product kernels (must match CtHvpArgs)
 struct CtHvpSampleH {
     const double2* slamp;
-    const double* kin;
+    const double* ev;
     const double* w;
     long long n;
     long long ld;
@@ -1863,7 +1908,7 @@ void Engine::hvpSums(const double* d_params, const double* d_dirs, int ndir, dou
         CtHvpSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
         sm.slamp = d.slamp64;
-        sm.kin = d.kin;
+        sm.ev = d.ev64;
         sm.w = d.w;
         sm.n = d.n;
         sm.ld = d.ld;
@@ -2009,7 +2054,7 @@ void Engine::partialIntegrals(const double* d_params, int kind, double* d_out, c
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));
     a.s[0].slamp = d.slamp64;
-    a.s[0].kin = d.kin;
+    a.s[0].ev = d.ev64;
     a.s[0].w = d.w;
     a.s[0].n = d.n;
     a.s[0].ld = d.ld;
@@ -2047,7 +2092,7 @@ void Engine::exportWeights(const double* d_params, const std::vector<int>& mask,
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));
     a.s[0].slamp = d.slamp64;
-    a.s[0].kin = d.kin;
+    a.s[0].ev = d.ev64;
     a.s[0].w = d.w;
     a.s[0].n = d.n;
     a.s[0].ld = d.ld;
@@ -2086,7 +2131,7 @@ void Engine::intensity(const double* d_params, int kind, double* d_out, cudaStre
     std::memset(&a, 0, sizeof(a));
     const DeviceSample& d = samples_[kind];
     a.s[0].slamp = d.slamp64;
-    a.s[0].kin = d.kin;
+    a.s[0].ev = d.ev64;
     a.s[0].n = d.n;
     a.s[0].ld = d.ld;
     a.s[0].kind = kind;

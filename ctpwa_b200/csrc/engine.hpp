@@ -33,7 +33,10 @@ struct DeviceSample {
     double* p4 = nullptr;      // SoA [n_final * 4][n]
     double2* slamp64 = nullptr;  // [nplane * npol][ld]
     float2* slamp32 = nullptr;   // mixed-precision copy
-    double* kin = nullptr;     // [nkin][ld]
+    double* kin = nullptr;     // [nkin][ld] kinematic cache (initialisation only)
+    double* ev64 = nullptr;    // [nev64][ld] frontier values, FP64
+    float* evf = nullptr;      // [nevf][ld] mixed form, FP32 frontier values
+    double* evd = nullptr;     // [nevd][ld] mixed form, FP64 frontier values
     double* w = nullptr;       // weights or nullptr
     double wsum = 0.0;         // sum of weights (or n)
 };
@@ -135,6 +138,7 @@ private:
     void loadSamples();
     void buildTables();
     void computeAngular(int kind);
+    void buildEventCache(int kind);
     void compileKernel();
     void compileHvp();
 
@@ -162,6 +166,7 @@ private:
     void* k_exp_ = nullptr;
     int* d_mask_ = nullptr;  // [nBlocks] export wave mask
     void* k_pro_ = nullptr;
+    void* k_evc_ = nullptr;  // ct_event_cache
     double jit_seconds_ = 0.0;
     bool jit_cache_hit_ = false;
 

@@ -3,13 +3,19 @@
 // Compiled by NVRTC for sm_100a together with a generated header "model.cuh"
 // that supplies, for one physics model:
 //   M_NA, M_NTERM, M_NPOL, M_NPLANE, M_NKIN, M_NTH, M_NDER     sizes
+//   M_NEV, M_NEVF, M_NEVD   rows of the per-event frontier tables (FP64; mixed
+//       form FP32 and FP64)
 //   term_col(t), term_plane(t)   amplitude column and angular plane (group
 //       variant, SL combination) of term t: a column is the sum of its terms
 //       (one term, or one per permutation of identical particles)
 //   der_term(k), der_th(k)   term / theta index of derivative entry k
 //   model_prologue(theta, C)   parameter-only subexpressions, once per call
-//   model_columns(kin, C, Fr, Fi, dFr, dFi)   lineshape products F_a and their
-//       theta derivatives for one event (straight-line generated code, FP64)
+//   model_event(kin, o), model_event_mx(kin, of, od)   the parameter-independent
+//       per-event values the per-call code reads (frontier), evaluated once
+//       per event by ct_event_cache when a sample is loaded
+//   model_columns(ev, C, Fr, Fi, dFr, dFi)   lineshape products F_a and their
+//       theta derivatives for one event from its frontier values
+//       (straight-line generated code, FP64)
 //   model_columns_f32(...)   the same in the mixed form (FP32 except the
 //       cancellation-prone polynomial parts such as m0^2 - m^2)
 //
@@ -66,10 +72,11 @@
 
 struct CtSample {
     const void* slamp;  // [M_NPLANE * M_NPOL planes][ld] of SL2
-    const double* kin;  // [M_NKIN][ld]
+    const void* ev;     // frontier rows [M_NEV][ld] FP64 (plain), [M_NEVF][ld] FP32 (mixed)
+    const double* evd;  // mixed form: FP64 frontier rows [M_NEVD][ld]
     const double* w;    // per-event weights or nullptr (unit weights)
     long long n;
-    long long ld;       // row stride of slamp and kin: n padded to a multiple of 256
+    long long ld;       // row stride of slamp and the frontier rows: n padded to a multiple of 256
     int kind;           // 0 = phase space, 1 = data, 2 = background
     int cta_begin;
     int cta_count;
@@ -168,24 +175,72 @@ __device__ __forceinline__ void ct_block_reduce_store(const double* accd, const 
     }
 }
 
+// One event's frontier values and its lineshape products: FP64 rows (plain
+// path) or FP32 + FP64 rows (mixed form).
+#define CT_NEV_ALLOC (M_NEV > 0 ? M_NEV : 1)
+#define CT_NEVF_ALLOC (M_NEVF > 0 ? M_NEVF : 1)
+#define CT_NEVD_ALLOC (M_NEVD > 0 ? M_NEVD : 1)
 template <typename L>
-struct CtLineshape;
+struct CtEvent;
 template <>
-struct CtLineshape<double> {
-    static __device__ __forceinline__ void eval(const double* kv, const double* C, const float*, const float*,
-                                                double* Fr, double* Fi, double* dFr, double* dFi)
+struct CtEvent<double> {
+    static constexpr int NA = M_NEV, NB = 0;  // rows of the table's type, FP64 rows
+    double v[CT_NEV_ALLOC];
+    __device__ __forceinline__ void load(const double* a, const double*, long long stride)
     {
-        model_columns(kv, C, Fr, Fi, dFr, dFi);
+#pragma unroll
+        for (int k = 0; k < M_NEV; ++k) v[k] = a[(long long)k * stride];
+    }
+    __device__ __forceinline__ void columns(const double* C, const float*, const float*, double* Fr, double* Fi,
+                                            double* dFr, double* dFi) const
+    {
+        model_columns(v, C, Fr, Fi, dFr, dFi);
     }
 };
 template <>
-struct CtLineshape<float> {
-    static __device__ __forceinline__ void eval(const double* kv, const double* C, const float* Cfh, const float* Cfl,
-                                                float* Fr, float* Fi, float* dFr, float* dFi)
+struct CtEvent<float> {
+    static constexpr int NA = M_NEVF, NB = M_NEVD;
+    float f[CT_NEVF_ALLOC];
+    double d[CT_NEVD_ALLOC];
+    __device__ __forceinline__ void load(const float* a, const double* b, long long stride)
     {
-        model_columns_f32(kv, C, Cfh, Cfl, Fr, Fi, dFr, dFi);
+#pragma unroll
+        for (int k = 0; k < M_NEVF; ++k) f[k] = a[(long long)k * stride];
+#pragma unroll
+        for (int k = 0; k < M_NEVD; ++k) d[k] = b[(long long)k * stride];
+    }
+    __device__ __forceinline__ void columns(const double* C, const float* Cfh, const float* Cfl, float* Fr, float* Fi,
+                                            float* dFr, float* dFi) const
+    {
+        model_columns_f32(f, d, C, Cfh, Cfl, Fr, Fi, dFr, dFi);
     }
 };
+
+// Once per event when a sample is loaded: the frontier tables from the
+// kinematic cache [M_NKIN][ld] (mixed tables only when evf is given).
+extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_event_cache(const double* __restrict__ kin, long long n,
+                                                                     long long ld, double* __restrict__ ev64,
+                                                                     float* __restrict__ evf, double* __restrict__ evd)
+{
+    for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
+        double kv[M_NKIN > 0 ? M_NKIN : 1];
+#pragma unroll
+        for (int k = 0; k < M_NKIN; ++k) kv[k] = kin[(long long)k * ld + e];
+        double o[CT_NEV_ALLOC];
+        model_event(kv, o);
+#pragma unroll
+        for (int k = 0; k < M_NEV; ++k) ev64[(long long)k * ld + e] = o[k];
+        if (evf) {
+            float of[CT_NEVF_ALLOC];
+            double od[CT_NEVD_ALLOC];
+            model_event_mx(kv, of, od);
+#pragma unroll
+            for (int k = 0; k < M_NEVF; ++k) evf[(long long)k * ld + e] = of[k];
+#pragma unroll
+            for (int k = 0; k < M_NEVD; ++k) evd[(long long)k * ld + e] = od[k];
+        }
+    }
+}
 
 // R: type of the per-polarisation complex algebra and of the stored angular
 //    table (double: plain path; float: mixed form)
@@ -206,7 +261,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     const int kind = PH_ONLY ? 0 : S.kind;
     const long long n = S.n;
     const SL2* __restrict__ slamp = (const SL2*)S.slamp;
-    const double* __restrict__ kin = S.kin;
+    const L* __restrict__ eva = (const L*)S.ev;
+    const double* __restrict__ evb = S.evd;
     const double* __restrict__ wts = S.w;
 
     // dynamic shared memory: [gradient-sum slots (ACC_SMEM)][tile buffers (STAGE)]
@@ -239,16 +295,16 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         vil[a] = (L)(i - (double)vi[a]);
     }
 
-    // all per-event work: kvp / slp point at this event's kinematic values and
-    // angular values, consecutive values `ks` / `ss` elements apart
-    auto event = [&](long long e, const double* __restrict__ kvp, long long ks, const SL2* __restrict__ slp,
-                     long long ss) {
+    // all per-event work: ap / bp / slp point at this event's frontier values
+    // (table type, FP64) and angular values, consecutive values `ks` / `ss`
+    // elements apart
+    auto event = [&](long long e, const L* __restrict__ ap, const double* __restrict__ bp, long long ks,
+                     const SL2* __restrict__ slp, long long ss) {
         // ---- lineshapes with parameter derivatives ----
-        double kv[M_NKIN > 0 ? M_NKIN : 1];
-#pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = kvp[(long long)k * ks];
+        CtEvent<L> ev;
+        ev.load(ap, bp, ks);
         L Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        CtLineshape<L>::eval(kv, sC, sCfh, sCfl, Fr, Fi, dFr, dFi);
+        ev.columns(sC, sCfh, sCfl, Fr, Fi, dFr, dFi);
 
         // ---- coherent sum over amplitudes ----
         SL2 sl[M_NPLANE * M_NPOL];
@@ -365,8 +421,9 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         // rows are padded to multiples of 256 events, so every copy starts
         // on a 2 KiB boundary and moves BLOCK elements.
         constexpr int NPL = M_NPLANE * M_NPOL;
-        constexpr unsigned SLB = BLOCK * sizeof(SL2), KB = BLOCK * sizeof(double);
-        constexpr unsigned BUF = NPL * SLB + M_NKIN * KB;
+        constexpr int NA = CtEvent<L>::NA, NB = CtEvent<L>::NB;
+        constexpr unsigned SLB = BLOCK * sizeof(SL2), AB = BLOCK * sizeof(L), BB = BLOCK * sizeof(double);
+        constexpr unsigned BUF = NPL * SLB + NA * AB + NB * BB;
         unsigned char* ct_stage = ct_dyn + ACC_BYTES;
         __shared__ __align__(8) unsigned long long ct_bar[2];
         const long long first = cta - S.cta_begin, step = S.cta_count;
@@ -379,8 +436,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #pragma unroll 1
             for (int c = 0; c < NPL; ++c) ct_bulk_g2s(buf + (size_t)c * SLB, slamp + (long long)c * S.ld + e0, SLB, &ct_bar[b]);
 #pragma unroll 1
-            for (int k = 0; k < M_NKIN; ++k)
-                ct_bulk_g2s(buf + (size_t)NPL * SLB + (size_t)k * KB, kin + (long long)k * S.ld + e0, KB, &ct_bar[b]);
+            for (int k = 0; k < NA; ++k)
+                ct_bulk_g2s(buf + (size_t)NPL * SLB + (size_t)k * AB, eva + (long long)k * S.ld + e0, AB, &ct_bar[b]);
+#pragma unroll 1
+            for (int k = 0; k < NB; ++k)
+                ct_bulk_g2s(buf + (size_t)NPL * SLB + (size_t)NA * AB + (size_t)k * BB, evb + (long long)k * S.ld + e0, BB,
+                            &ct_bar[b]);
         };
         if (threadIdx.x == 0) {
             ct_mbar_init(&ct_bar[0], 1);
@@ -399,8 +460,9 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             const long long e = (first + t * step) * BLOCK + threadIdx.x;
             if (ok && e < n) {
                 const unsigned char* buf = ct_stage + (size_t)b * BUF;
-                event(e, (const double*)(buf + (size_t)NPL * SLB) + threadIdx.x, BLOCK, (const SL2*)buf + threadIdx.x,
-                      BLOCK);
+                event(e, (const L*)(buf + (size_t)NPL * SLB) + threadIdx.x,
+                      (const double*)(buf + (size_t)NPL * SLB + (size_t)NA * AB) + threadIdx.x, BLOCK,
+                      (const SL2*)buf + threadIdx.x, BLOCK);
             }
             // every thread is done with buffer b (and agrees whether the copy arrived)
             if (!__syncthreads_and(ok)) break;
@@ -418,7 +480,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     } else {
         const long long stride = (long long)S.cta_count * BLOCK;
         for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride)
-            event(e, kin + e, S.ld, slamp + e, S.ld);
+            event(e, eva + e, evb ? evb + e : nullptr, S.ld, slamp + e, S.ld);
     }
     ct_block_reduce_store<BLOCK>(accd, accg, A.partials + (long long)cta * CT_NACC);
 }
@@ -462,11 +524,11 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_partials_f64(CtArgs A,
 #pragma unroll
     for (int i = 0; i < M_NBLK; ++i) acc[i] = 0.0;
     for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
-        double kv[M_NKIN > 0 ? M_NKIN : 1];
+        double ev[CT_NEV_ALLOC];
 #pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
+        for (int k = 0; k < M_NEV; ++k) ev[k] = __ldg((const double*)S.ev + (long long)k * S.ld + e);
         double Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        model_columns(kv, sC, Fr, Fi, dFr, dFi);
+        model_columns(ev, sC, Fr, Fi, dFr, dFi);
         const double we = S.w ? __ldg(S.w + e) : 1.0;
 #pragma unroll
         for (int i = 0; i < M_NBLK; ++i) {
@@ -527,11 +589,11 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_export_f64(CtArgs A, d
     for (int i = threadIdx.x; i < NPAIR; i += CT_BLOCK) sI[i] = 0.0;
     ct_stage_consts(A, sC);
     for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
-        double kv[M_NKIN > 0 ? M_NKIN : 1];
+        double ev[CT_NEV_ALLOC];
 #pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
+        for (int k = 0; k < M_NEV; ++k) ev[k] = __ldg((const double*)S.ev + (long long)k * S.ld + e);
         double Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        model_columns(kv, sC, Fr, Fi, dFr, dFi);
+        model_columns(ev, sC, Fr, Fi, dFr, dFi);
         double Pr[M_NBLK][M_NPOL], Pi[M_NBLK][M_NPOL];
 #pragma unroll
         for (int i = 0; i < M_NBLK; ++i)
@@ -597,11 +659,11 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_intensity_f64(CtArgs A
     __shared__ double sC[CT_NCONST_ALLOC];
     ct_stage_consts(A, sC);
     for (long long e = (long long)blockIdx.x * CT_BLOCK + threadIdx.x; e < n; e += (long long)gridDim.x * CT_BLOCK) {
-        double kv[M_NKIN > 0 ? M_NKIN : 1];
+        double ev[CT_NEV_ALLOC];
 #pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * S.ld + e);
+        for (int k = 0; k < M_NEV; ++k) ev[k] = __ldg((const double*)S.ev + (long long)k * S.ld + e);
         double Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        model_columns(kv, sC, Fr, Fi, dFr, dFi);
+        model_columns(ev, sC, Fr, Fi, dFr, dFi);
         double f = 0.0;
 #pragma unroll
         for (int p = 0; p < M_NPOL; ++p) {

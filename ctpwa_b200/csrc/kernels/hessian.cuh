@@ -100,7 +100,7 @@ __device__ __forceinline__ double ct_value(CtDual x) { return x.v; }
 
 struct CtHvpSample {
     const double2* slamp;  // [M_NPLANE * M_NPOL][ld] angular values
-    const double* kin;     // [M_NKIN][ld]
+    const double* ev;      // [M_NEV][ld] FP64 frontier values
     const double* w;       // per-event weights or nullptr
     long long n;
     long long ld;
@@ -194,16 +194,16 @@ extern "C" __global__ void __launch_bounds__(CT_HVP_BLOCK) ct_hvp_f64(CtHvpArgs 
     const long long n = S.n, ld = S.ld;
     const long long stride = (long long)S.cta_count * CT_HVP_BLOCK;
     for (long long e = (long long)(cta - S.cta_begin) * CT_HVP_BLOCK + threadIdx.x; e < n; e += stride) {
-        double kv[M_NKIN > 0 ? M_NKIN : 1];
+        double ev[M_NEV > 0 ? M_NEV : 1];
 #pragma unroll
-        for (int k = 0; k < M_NKIN; ++k) kv[k] = __ldg(S.kin + (long long)k * ld + e);
+        for (int k = 0; k < M_NEV; ++k) ev[k] = __ldg(S.ev + (long long)k * ld + e);
         CtDual Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
         if (thdir) {
-            model_columns_dual(kv, sC, Fr, Fi, dFr, dFi);
+            model_columns_dual(ev, sC, Fr, Fi, dFr, dFi);
         } else {
             // couplings-only direction: the lineshapes do not move
             double fr[M_NTERM], fi[M_NTERM], dfr[M_NDER > 0 ? M_NDER : 1], dfi[M_NDER > 0 ? M_NDER : 1];
-            model_columns(kv, sCv, fr, fi, dfr, dfi);
+            model_columns(ev, sCv, fr, fi, dfr, dfi);
 #pragma unroll
             for (int t = 0; t < M_NTERM; ++t) {
                 Fr[t] = CtDual(fr[t]);

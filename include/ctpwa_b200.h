@@ -194,8 +194,15 @@ int ctpwa_intensity(ctpwa_handle* h, const double* d_params, int kind, double* d
 
 /* Per-event layout of the device event caches (no counterpart in the
  * reference): out[0] angular planes, out[1] polarisation states, out[2]
- * cached kinematic values, out[3] of which invariant masses. */
+ * kinematic values the lineshapes are built from, out[3] of which invariant
+ * masses. */
 int ctpwa_event_layout(const ctpwa_handle* h, int* out4);
+
+/* Per-event frontier tables (no counterpart in the reference): the
+ * parameter-independent lineshape subexpressions each evaluation reads,
+ * computed once per event when the samples are loaded. out[0] FP64 values of
+ * the plain path, out[1] FP32 and out[2] FP64 values of the mixed form. */
+int ctpwa_event_cache_layout(const ctpwa_handle* h, int* out3);
 
 /* Per-launch timing of the fused likelihood kernel (no counterpart in the
  * reference, which times nothing on the device). slots > 0 records a CUDA
