@@ -57,6 +57,7 @@ SIGNATURES = {
     "ctpwa_model_json": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "ctpwa_device_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "ctpwa_event_cache_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "ctpwa_launch_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "ctpwa_event_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "ctpwa_kernel_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "ctpwa_kernel_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),

@@ -1130,9 +1130,11 @@ void Engine::buildEventCache(int kind)
 // Block size and minimum resident CTAs per SM of the plain [0] and mixed [1]
 // fused kernels, unless CTPWA_F64_BLOCK / CTPWA_F64_MINB / CTPWA_MX_BLOCK /
 // CTPWA_MX_MINB / CTPWA_*_ACC_SMEM override them (tuning). Measured on the
-// K+K-pi0 workload: plain 256 x 2 with the gradient sums in shared memory
-// (128 registers, 16 warps per SM) 1.371 ms, against 128 x 3 in registers
-// 1.585 ms and 256 x 1 1.717 ms; mixed 256 x 2 in registers 0.805 ms.
+// K+K-pi0 workload with the frontier tables: plain 256 x 2 with the gradient
+// sums in shared memory (128 registers, 16 warps per SM) 1.15 ms, against
+// 1.26 ms with the sums in registers, 1.63 ms at 128 x 5 and 2.55 ms at
+// 256 x 3; mixed 256 x 2 in registers 0.598 ms, against 0.70 ms at 3 CTAs
+// per SM, 0.66 ms with the sums in shared memory, 0.65 ms at 128 x 5.
 FusedShape fusedShape(const GeneratedModel& gen)
 {
     FusedShape sh;
@@ -1149,16 +1151,15 @@ FusedShape fusedShape(const GeneratedModel& gen)
     sh.minb[1] = get("CTPWA_MX_MINB", 2, 1, 16);
     sh.acc[0] = get("CTPWA_F64_ACC_SMEM", 1, 0, 1);
     sh.acc[1] = get("CTPWA_MX_ACC_SMEM", 0, 0, 1);
+
     for (int i = 0; i < 2; ++i)
         if (sh.block[i] % 32) throw std::runtime_error("fused block sizes must be multiples of 32");
-    // Staging (CTPWA_STAGE=1): two tile buffers of BLOCK events (angular rows
-    // + kinematic rows) per CTA, filled by bulk copies, used when they fit at
-    // the requested residency next to the static shared memory. Off by
-    // default: the fused kernels are issue-bound, and the per-tile barrier of
-    // the pipeline cost more than the load latency it hid (K+K-pi0 on B200:
-    // mixed 0.879 ms staged vs 0.808 ms direct; plain 1.683 ms staged at
-    // 2 CTAs per SM vs 1.576 ms direct at 3).
-    const int stage_on = get("CTPWA_STAGE", 0, 0, 1);
+    // Staging (CTPWA_STAGE=1: the frontier rows; 2: frontier and angular
+    // rows): each warp streams its 32-event tiles through two shared-memory
+    // buffers filled by bulk copies, used when they fit at the requested
+    // residency next to the static shared memory. Off by default until it
+    // measures faster.
+    const int stage_on = get("CTPWA_STAGE", 0, 0, 2);
     const long long rowb[2] = {16, 8};  // bytes per complex angular value (FP64, FP32)
     const long long accb[2] = {8, 4};   // bytes per gradient sum (FP64, FP32)
     const long long per_sm = 228LL * 1024, per_cta = 227LL * 1024, reserve = 8LL * 1024;
@@ -1174,8 +1175,8 @@ FusedShape fusedShape(const GeneratedModel& gen)
         }
         const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
         const long long evb = i == 0 ? 8LL * gen.nev64 : 4LL * gen.nevf + 8LL * gen.nevd;  // frontier bytes per event
-        const long long stage_bytes = 2LL * (npl * rowb[i] + evb) * sh.block[i];
-        if (stage_on && fits(i, acc_bytes + stage_bytes)) sh.stage[i] = 1;
+        const long long stage_bytes = 2LL * ((stage_on > 1 ? npl * rowb[i] : 0) + evb) * sh.block[i];
+        if (stage_on && fits(i, acc_bytes + stage_bytes)) sh.stage[i] = stage_on;
         sh.dsmem[i] = (int)(acc_bytes + (sh.stage[i] ? stage_bytes : 0));
     }
     return sh;
@@ -1259,6 +1260,7 @@ std::string jitCubin(const GeneratedModel& gen, bool* cache_hit)
     optv.push_back("-DCT_MX_ACC=" + std::to_string(sh.acc[1]));
     optv.push_back("-DCT_F64_STAGE=" + std::to_string(sh.stage[0]));
     optv.push_back("-DCT_MX_STAGE=" + std::to_string(sh.stage[1]));
+
     optv.push_back("-DCT_F64_BLOCK=" + std::to_string(sh.block[0]));
     optv.push_back("-DCT_F64_MINB=" + std::to_string(sh.minb[0]));
     optv.push_back("-DCT_MX_BLOCK=" + std::to_string(sh.block[1]));

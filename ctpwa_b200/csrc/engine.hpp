@@ -131,6 +131,8 @@ public:
     long long nEvents(int kind) const { return samples_[kind].n; }
     size_t deviceBytes() const { return device_bytes_; }
     const GeneratedModel& generated() const { return gen_; }
+    const FusedShape& shape() const { return shape_; }
+    int fusedGrid(int precision) const { return lay_[precision == kMixed ? 1 : 0].grid; }
     double jitSeconds() const { return jit_seconds_; }
     bool jitCacheHit() const { return jit_cache_hit_; }
 

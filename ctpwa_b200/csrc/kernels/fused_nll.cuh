@@ -51,8 +51,9 @@
 
 #define CT_NACC (2 + 2 * M_NA + M_NTH)
 
-// shared-memory staging of the event tables (host sets them when the two
-// tile buffers fit at the requested residency)
+// shared-memory staging of the event tables by per-warp bulk copies: 0 off,
+// 1 the frontier rows, 2 the frontier and angular rows (the host sets it when
+// the warps' two tile buffers fit at the requested residency)
 #ifndef CT_F64_STAGE
 #define CT_F64_STAGE 0
 #endif
@@ -247,7 +248,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_event_cache(const doub
 // L: type of the lineshapes, their derivatives and the per-thread gradient
 //    sums
 // PH_ONLY: the launch serves phase-space events only
-template <typename R, typename L, bool PH_ONLY, int BLOCK, bool STAGE, bool ACC_SMEM>
+template <typename R, typename L, bool PH_ONLY, int BLOCK, int STAGE, bool ACC_SMEM>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 {
     typedef typename CtVec2<R>::type SL2;
@@ -414,68 +415,82 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         }
     };
 
-    if constexpr (STAGE) {
-        // Two-buffer pipeline: tile t (BLOCK consecutive events of this CTA's
-        // sample) is copied whole into shared memory by the bulk-copy engine,
-        // one copy per table row, while the CTA computes on tile t - 1. Table
-        // rows are padded to multiples of 256 events, so every copy starts
-        // on a 2 KiB boundary and moves BLOCK elements.
+    if constexpr (STAGE > 0) {
+        // Warp-level two-buffer pipeline. Each warp streams its own 32-event
+        // tiles (the same events as the direct loop below); lane 0 copies the
+        // next tile's table rows (the frontier values; with STAGE 2 also the
+        // angular values) into the warp's other shared-memory buffer by bulk
+        // copies that complete on the warp's mbarrier, while the warp computes
+        // the current tile. No CTA-wide barrier: warps proceed independently.
+        // Rows are padded to multiples of 256 events, so every copy starts on
+        // a 128-byte boundary and moves a whole 32-event tile.
         constexpr int NPL = M_NPLANE * M_NPOL;
+        constexpr int W = BLOCK / 32;
         constexpr int NA = CtEvent<L>::NA, NB = CtEvent<L>::NB;
-        constexpr unsigned SLB = BLOCK * sizeof(SL2), AB = BLOCK * sizeof(L), BB = BLOCK * sizeof(double);
-        constexpr unsigned BUF = NPL * SLB + NA * AB + NB * BB;
-        unsigned char* ct_stage = ct_dyn + ACC_BYTES;
-        __shared__ __align__(8) unsigned long long ct_bar[2];
-        const long long first = cta - S.cta_begin, step = S.cta_count;
-        const long long ntiles = (n + BLOCK - 1) / BLOCK;
-        const long long my = first < ntiles ? (ntiles - 1 - first) / step + 1 : 0;
-        auto issue = [&](long long t, int b) {
-            const long long e0 = (first + t * step) * BLOCK;
-            unsigned char* buf = ct_stage + (size_t)b * BUF;
-            ct_mbar_expect_tx(&ct_bar[b], BUF);
+        constexpr unsigned AR = 32 * sizeof(L), BR = 32 * sizeof(double), SR = 32 * sizeof(SL2);
+        constexpr unsigned BUF = NA * AR + NB * BR + (STAGE > 1 ? NPL * SR : 0);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        unsigned char* wbuf = ct_dyn + ACC_BYTES + (size_t)warp * 2 * BUF;
+        __shared__ __align__(8) unsigned long long ct_wbar[W][2];
+        const long long ntiles = (n + 31) / 32;
+        const long long first = (long long)(cta - S.cta_begin) * W + warp, tstep = (long long)S.cta_count * W;
+        const long long my = first < ntiles ? (ntiles - 1 - first) / tstep + 1 : 0;
+        auto issue = [&](long long k, int b) {
+            const long long e0 = (first + k * tstep) * 32;
+            unsigned char* buf = wbuf + (size_t)b * BUF;
+            unsigned long long* bar = &ct_wbar[warp][b];
+            ct_mbar_expect_tx(bar, BUF);
 #pragma unroll 1
-            for (int c = 0; c < NPL; ++c) ct_bulk_g2s(buf + (size_t)c * SLB, slamp + (long long)c * S.ld + e0, SLB, &ct_bar[b]);
+            for (int r = 0; r < NA; ++r) ct_bulk_g2s(buf + (size_t)r * AR, eva + (long long)r * S.ld + e0, AR, bar);
 #pragma unroll 1
-            for (int k = 0; k < NA; ++k)
-                ct_bulk_g2s(buf + (size_t)NPL * SLB + (size_t)k * AB, eva + (long long)k * S.ld + e0, AB, &ct_bar[b]);
+            for (int r = 0; r < NB; ++r)
+                ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)r * BR, evb + (long long)r * S.ld + e0, BR, bar);
+            if constexpr (STAGE > 1) {
 #pragma unroll 1
-            for (int k = 0; k < NB; ++k)
-                ct_bulk_g2s(buf + (size_t)NPL * SLB + (size_t)NA * AB + (size_t)k * BB, evb + (long long)k * S.ld + e0, BB,
-                            &ct_bar[b]);
+                for (int c = 0; c < NPL; ++c)
+                    ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)NB * BR + (size_t)c * SR, slamp + (long long)c * S.ld + e0,
+                                SR, bar);
+            }
         };
-        if (threadIdx.x == 0) {
-            ct_mbar_init(&ct_bar[0], 1);
-            ct_mbar_init(&ct_bar[1], 1);
+        if (lane == 0) {
+            ct_mbar_init(&ct_wbar[warp][0], 1);
+            ct_mbar_init(&ct_wbar[warp][1], 1);
             ct_fence_mbar_init();
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        __syncwarp();
+        if (lane == 0) {
             if (my > 0) issue(0, 0);
             if (my > 1) issue(1, 1);
         }
-        long long t = 0;
-        for (; t < my; ++t) {
-            const int b = (int)(t & 1);
-            const bool ok = ct_mbar_wait(&ct_bar[b], (unsigned)((t >> 1) & 1), CT_WAIT_LIMIT);
-            const long long e = (first + t * step) * BLOCK + threadIdx.x;
-            if (ok && e < n) {
-                const unsigned char* buf = ct_stage + (size_t)b * BUF;
-                event(e, (const L*)(buf + (size_t)NPL * SLB) + threadIdx.x,
-                      (const double*)(buf + (size_t)NPL * SLB + (size_t)NA * AB) + threadIdx.x, BLOCK,
-                      (const SL2*)buf + threadIdx.x, BLOCK);
+        long long k = 0;
+        for (; k < my; ++k) {
+            const int b = (int)(k & 1);
+            const bool ok = ct_mbar_wait(&ct_wbar[warp][b], (unsigned)((k >> 1) & 1), CT_WAIT_LIMIT);
+            if (!__all_sync(0xffffffffu, ok)) break;
+            const long long e = (first + k * tstep) * 32 + lane;
+            if (e < n) {
+                const unsigned char* buf = wbuf + (size_t)b * BUF;
+                const L* ap = (const L*)buf + lane;
+                const double* bp = (const double*)(buf + (size_t)NA * AR) + lane;
+                if constexpr (STAGE > 1)
+                    event(e, ap, bp, 32, (const SL2*)(buf + (size_t)NA * AR + (size_t)NB * BR) + lane, 32);
+                else
+                    event(e, ap, bp, 32, slamp + e, S.ld);
             }
-            // every thread is done with buffer b (and agrees whether the copy arrived)
-            if (!__syncthreads_and(ok)) break;
-            if (threadIdx.x == 0 && t + 2 < my) issue(t + 2, b);
+            // every lane is done with buffer b before it is refilled
+            __syncwarp();
+            if (lane == 0 && k + 2 < my) issue(k + 2, b);
         }
-        if (t < my) {
-            // a copy did not complete in time: flag it, give the other
-            // buffer's copy a bounded chance to land, and stop
-            if (threadIdx.x == 0) {
+        if (k < my) {
+            // a copy did not complete in time: flag the evaluation and give
+            // the copies still in flight a bounded chance to land before the
+            // warp leaves
+            if (lane == 0) {
                 atomicExch(A.err, 1);
-                if (t + 1 < my) ct_mbar_wait(&ct_bar[(t + 1) & 1], (unsigned)(((t + 1) >> 1) & 1), CT_WAIT_LIMIT);
+                ct_mbar_wait(&ct_wbar[warp][k & 1], (unsigned)((k >> 1) & 1), CT_WAIT_LIMIT);
+                if (k + 1 < my) ct_mbar_wait(&ct_wbar[warp][(k + 1) & 1], (unsigned)(((k + 1) >> 1) & 1), CT_WAIT_LIMIT);
             }
-            __syncthreads();
+            __syncwarp();
         }
     } else {
         const long long stride = (long long)S.cta_count * BLOCK;
@@ -501,12 +516,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #endif
 extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB) ct_fused_f64(CtArgs a)
 {
-    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE != 0, CT_F64_ACC != 0>(a);
+    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE, CT_F64_ACC != 0>(a);
 }
 // mixed form (FP32 lineshapes and algebra, FP64 logs and sums), all samples
 extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_mixed(CtArgs a)
 {
-    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE != 0, CT_MX_ACC != 0>(a);
+    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE, CT_MX_ACC != 0>(a);
 }
 
 // Partial-wave integrals of sample s[0] (FP64): per resonance block i,

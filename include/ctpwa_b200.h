@@ -204,6 +204,13 @@ int ctpwa_event_layout(const ctpwa_handle* h, int* out4);
  * the plain path, out[1] FP32 and out[2] FP64 values of the mixed form. */
 int ctpwa_event_cache_layout(const ctpwa_handle* h, int* out3);
 
+/* Launch shape of the fused kernels (no counterpart in the reference): for
+ * the plain [0..5] and mixed [6..11] kernels: threads per CTA, minimum
+ * resident CTAs per SM, table staging mode (0 off, 1 frontier rows, 2
+ * frontier and angular rows), gradient sums in shared memory (0/1), dynamic
+ * shared memory bytes per CTA, CTAs per launch. */
+int ctpwa_launch_shape(const ctpwa_handle* h, int* out12);
+
 /* Per-launch timing of the fused likelihood kernel (no counterpart in the
  * reference, which times nothing on the device). slots > 0 records a CUDA
  * event pair on the launching stream around every fused launch, in a ring of

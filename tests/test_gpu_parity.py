@@ -286,19 +286,30 @@ def test_partial_integrals_and_fit_fractions(setups, tmp_path):
     assert abs(float(a2.getFitFractions(q)[:, 0].sum()) - 1.0) < 1e-12
 
 
-def test_staged_tables_match_direct_loads(tmp_path, monkeypatch):
-    """The fused kernels with the event tables staged through shared memory by
-    bulk copies (CTPWA_STAGE=1) give the same results as with direct loads."""
+@pytest.mark.parametrize("mode", [1, 2])
+def test_staged_tables_match_direct_loads(tmp_path, monkeypatch, mode):
+    """The fused kernels with the event tables streamed through shared memory
+    by per-warp bulk copies (CTPWA_STAGE=1: frontier rows; 2: frontier and
+    angular rows) give the same results as with direct loads."""
     import torch
     import ctpwa_b200
 
     cfg = workloads.make("kkpi", tmp_path, n_phsp=70_001, n_data=9_999, n_bkg=777, accept_reject=False, seed=31)
+    # the same launch shape for both handles (room for the buffers), so every
+    # thread sums the same events in the same order
+    monkeypatch.setenv("CTPWA_F64_ACC_SMEM", "0")
+    if mode == 2:
+        monkeypatch.setenv("CTPWA_F64_MINB", "1")
+        monkeypatch.setenv("CTPWA_MX_MINB", "1")
     direct = ctpwa_b200.analysis(cfg)
     p = workloads.true_params(direct.getNVector(), direct.getFreeResParams()[0].numpy())
     pt = torch.tensor(p, dtype=torch.float64, device="cuda")
-    monkeypatch.setenv("CTPWA_STAGE", "1")
-    monkeypatch.setenv("CTPWA_F64_MINB", "2")  # the plain path's two tile buffers fit at 2 CTAs per SM
+    monkeypatch.setenv("CTPWA_STAGE", str(mode))
     staged = ctpwa_b200.analysis(cfg)
+    shape = staged.launchShape()
+    assert shape["fp64"]["stage"] == mode and shape["mixed"]["stage"] == mode, shape
+    assert direct.launchShape()["mixed"]["stage"] == 0
+    assert direct.launchShape()["mixed"]["grid"] == shape["mixed"]["grid"]
     for prec in ("fp64", "mixed"):
         n0, g0 = direct.getNLLAndGrad(pt, prec)
         n1, g1 = staged.getNLLAndGrad(pt, prec)
