@@ -1159,7 +1159,7 @@ FusedShape fusedShape(const GeneratedModel& gen)
     // buffers filled by bulk copies, used when they fit at the requested
     // residency next to the static shared memory. Off by default until it
     // measures faster.
-    const int stage_on = get("CTPWA_STAGE", 0, 0, 2);
+    const int stage_on = get("CTPWA_STAGE", 0, 0, 3);
     const long long rowb[2] = {16, 8};  // bytes per complex angular value (FP64, FP32)
     const long long accb[2] = {8, 4};   // bytes per gradient sum (FP64, FP32)
     const long long per_sm = 228LL * 1024, per_cta = 227LL * 1024, reserve = 8LL * 1024;
@@ -1175,7 +1175,12 @@ FusedShape fusedShape(const GeneratedModel& gen)
         }
         const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
         const long long evb = i == 0 ? 8LL * gen.nev64 : 4LL * gen.nevf + 8LL * gen.nevd;  // frontier bytes per event
-        const long long stage_bytes = 2LL * ((stage_on > 1 ? npl * rowb[i] : 0) + evb) * sh.block[i];
+        long long stage_bytes = 2LL * ((stage_on == 2 ? npl * rowb[i] : 0) + evb) * sh.block[i];
+        if (stage_on == 3) {
+            // [2][NA][block] values of the table's type (16-byte rounded), then [2][NB][block] FP64
+            const long long na = i == 0 ? gen.nev64 : gen.nevf, nb = i == 0 ? 0 : gen.nevd, sz = i == 0 ? 8 : 4;
+            stage_bytes = (2LL * std::max(1LL, na) * sh.block[i] * sz + 15) / 16 * 16 + 2LL * nb * sh.block[i] * 8;
+        }
         if (stage_on && fits(i, acc_bytes + stage_bytes)) sh.stage[i] = stage_on;
         sh.dsmem[i] = (int)(acc_bytes + (sh.stage[i] ? stage_bytes : 0));
     }

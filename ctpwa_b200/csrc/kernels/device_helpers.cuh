@@ -148,6 +148,23 @@ __device__ __forceinline__ void ct_bulk_g2s(void* dst, const void* src, unsigned
                  "l"(src), "r"(bytes), "r"(ct_smem_addr(bar))
                  : "memory");
 }
+// ---- per-thread asynchronous copies global -> shared (cp.async) ----
+// 4-, 8- or 16-byte copies issued by one thread and waited for by the same
+// thread (commit groups), no barrier with other threads
+template <int BYTES>
+__device__ __forceinline__ void ct_cp_async(void* dst, const void* src)
+{
+    static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async copies 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(ct_smem_addr(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void ct_cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most N of this thread's most recent groups are pending
+template <int N>
+__device__ __forceinline__ void ct_cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Bounded wait for phase `parity` of an mbarrier: gives up after `limit`
 // polls (each poll may suspend the thread for a short hardware interval) and
 // returns false, so a copy that never completes cannot hang the kernel.

@@ -51,9 +51,10 @@
 
 #define CT_NACC (2 + 2 * M_NA + M_NTH)
 
-// shared-memory staging of the event tables by per-warp bulk copies: 0 off,
-// 1 the frontier rows, 2 the frontier and angular rows (the host sets it when
-// the warps' two tile buffers fit at the requested residency)
+// shared-memory staging of the event tables: 0 off; by per-warp bulk copies
+// 1 the frontier rows, 2 the frontier and angular rows; 3 the frontier values
+// by per-thread asynchronous copies (the host sets it when the two buffers
+// fit at the requested residency)
 #ifndef CT_F64_STAGE
 #define CT_F64_STAGE 0
 #endif
@@ -415,7 +416,38 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         }
     };
 
-    if constexpr (STAGE > 0) {
+    if constexpr (STAGE == 3) {
+        // Per-thread two-buffer pipeline of the frontier values: each thread
+        // copies its next event's frontier values into its own shared-memory
+        // slots by cp.async while it computes the current event, and waits
+        // only for its own copies; the angular values are loaded directly
+        // (they are first needed after the lineshapes).
+        constexpr int NA = CtEvent<L>::NA, NB = CtEvent<L>::NB;
+        constexpr unsigned ABYTES = (2u * (NA > 0 ? NA : 1) * BLOCK * sizeof(L) + 15) / 16 * 16;
+        L* abuf = (L*)(ct_dyn + ACC_BYTES);                  // [2][NA][BLOCK]
+        double* bbuf = (double*)(ct_dyn + ACC_BYTES + ABYTES);  // [2][NB][BLOCK]
+        const int tid = threadIdx.x;
+        auto fetch = [&](long long e, int b) {
+#pragma unroll
+            for (int k = 0; k < NA; ++k)
+                ct_cp_async<sizeof(L)>(abuf + ((size_t)b * NA + k) * BLOCK + tid, eva + (long long)k * S.ld + e);
+#pragma unroll
+            for (int k = 0; k < NB; ++k)
+                ct_cp_async<8>(bbuf + ((size_t)b * NB + k) * BLOCK + tid, evb + (long long)k * S.ld + e);
+            ct_cp_async_commit();
+        };
+        const long long stride = (long long)S.cta_count * BLOCK;
+        long long e = (long long)(cta - S.cta_begin) * BLOCK + tid;
+        if (e < n) fetch(e, 0);
+        for (int it = 0; e < n; e += stride, ++it) {
+            const int b = it & 1;
+            if (e + stride < n) fetch(e + stride, b ^ 1);
+            else ct_cp_async_commit();  // empty group: the wait below covers buffer b alike
+            ct_cp_async_wait<1>();
+            event(e, abuf + (size_t)b * NA * BLOCK + tid, bbuf + (size_t)b * NB * BLOCK + tid, BLOCK, slamp + e, S.ld);
+        }
+        ct_cp_async_wait<0>();
+    } else if constexpr (STAGE > 0) {
         // Warp-level two-buffer pipeline. Each warp streams its own 32-event
         // tiles (the same events as the direct loop below); lane 0 copies the
         // next tile's table rows (the frontier values; with STAGE 2 also the

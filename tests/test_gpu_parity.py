@@ -286,11 +286,12 @@ def test_partial_integrals_and_fit_fractions(setups, tmp_path):
     assert abs(float(a2.getFitFractions(q)[:, 0].sum()) - 1.0) < 1e-12
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 def test_staged_tables_match_direct_loads(tmp_path, monkeypatch, mode):
     """The fused kernels with the event tables streamed through shared memory
-    by per-warp bulk copies (CTPWA_STAGE=1: frontier rows; 2: frontier and
-    angular rows) give the same results as with direct loads."""
+    (CTPWA_STAGE=1: frontier rows by per-warp bulk copies; 2: frontier and
+    angular rows; 3: frontier values by per-thread asynchronous copies) give
+    the same results as with direct loads."""
     import torch
     import ctpwa_b200
 
