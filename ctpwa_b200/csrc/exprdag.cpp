@@ -110,6 +110,42 @@ int Graph::mul(int a, int b)
     if (isConst(b) && val(b) == 1.0) return a;
     if (isConst(a) && val(a) == -1.0) return neg(b);
     if (isConst(b) && val(b) == -1.0) return neg(a);
+    // A product that depends on both the parameters and the event is
+    // regrouped by dependence: its event-only factors are multiplied together
+    // (one per-event value, evaluated once per event) and its parameter-only
+    // factors together (one per-call value), so e.g. the Blatt-Weisskopf
+    // factors of q at both vertices of a chain become one per-event value.
+    auto cls = [&](int x) { return nodes[x].dep == DEP_NONE ? (int)DEP_THETA : (int)nodes[x].dep; };
+    if ((cls(a) | cls(b)) == (DEP_THETA | DEP_EVENT)) {
+        std::vector<int> f;
+        std::vector<std::pair<int, int>> st = {{a, 0}, {b, 0}};
+        while (!st.empty()) {
+            auto [x, depth] = st.back();
+            st.pop_back();
+            if (nodes[x].op == Mul && cls(x) == (DEP_THETA | DEP_EVENT) && depth < 3) {
+                st.push_back({nodes[x].a, depth + 1});
+                st.push_back({nodes[x].b, depth + 1});
+            } else {
+                f.push_back(x);
+            }
+        }
+        if (f.size() > 2) {
+            int e = -1, t = -1, m = -1;
+            for (int x : f) {
+                int& acc = cls(x) == DEP_EVENT ? e : cls(x) == DEP_THETA ? t : m;
+                acc = acc < 0 ? x : (cls(x) == (DEP_THETA | DEP_EVENT) ? mulRaw(acc, x) : mul(acc, x));
+            }
+            int r = m;
+            for (int x : {t, e})
+                if (x >= 0) r = r < 0 ? x : mulRaw(r, x);
+            return r;
+        }
+    }
+    return mulRaw(a, b);
+}
+
+int Graph::mulRaw(int a, int b)
+{
     if (a > b) std::swap(a, b);
     Node n;
     n.op = Mul;

@@ -109,6 +109,7 @@ public:
 
 private:
     int make(Node n);
+    int mulRaw(int a, int b);  // a * b as one node, no regrouping
     int zero_, one_;
     std::map<std::tuple<int, int, int, int, int, double, int>, int> memo_;
     std::map<std::pair<int, int>, int> dmemo_;
