@@ -496,6 +496,7 @@ def run_gpu(args, rank, world, local_rank):
         "config": {"workload": WORKLOAD_TEXT, "events_per_rank": {"phsp": n_events[0], "data": n_events[1],
                                                                   "bkg": n_events[2]},
                    "n_params": nP, "theta_perturbed_every_step": True, "fraction": args.fraction,
+                   "launch": ana.launchShape(),
                    "l2": f"inputs larger than L2: {streamed_bytes(layout, n_events, 'mixed') / 1e9:.2f} GB streamed "
                          f"per step vs {L2_BYTES / 1e6:.0f} MB L2, no flush",
                    "exchange": ("NCCL all-reduce of the per-sample sums per step (3*(2+2nA+nT)+4 doubles), "

@@ -751,6 +751,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     int nA = model_.nAmp();
     CT_CUDA(cudaMalloc(&d_v_, sizeof(double) * 2 * nA));
     CT_CUDA(cudaMalloc(&d_consts_, sizeof(double) * std::max(1, gen_.nconst)));
+    CT_CUDA(cudaMalloc(&d_kblock_, k_sym_bytes_));
     std::vector<double> ratio = model_.coupling.ratio;
     CT_CUDA(cudaMalloc(&d_amp_chain_, sizeof(int) * nA));
     CT_CUDA(cudaMalloc(&d_ratio_, sizeof(double) * nA));
@@ -812,6 +813,7 @@ Engine::~Engine()
     cudaFree(d_ag_tables_);
     cudaFree(d_v_);
     cudaFree(d_consts_);
+    cudaFree(d_kblock_);
     cudaFree(d_partials_);
     cudaFree(d_parts_);
     cudaFree(d_hscratch_);
@@ -1154,12 +1156,18 @@ FusedShape fusedShape(const GeneratedModel& gen)
 
     for (int i = 0; i < 2; ++i)
         if (sh.block[i] % 32) throw std::runtime_error("fused block sizes must be multiples of 32");
-    // Staging (CTPWA_STAGE=1: the frontier rows; 2: frontier and angular
-    // rows): each warp streams its 32-event tiles through two shared-memory
-    // buffers filled by bulk copies, used when they fit at the requested
-    // residency next to the static shared memory. Off by default until it
-    // measures faster.
-    const int stage_on = get("CTPWA_STAGE", 0, 0, 3);
+    // Staging of the event tables through shared memory, used when its two
+    // buffers fit at the requested residency next to the static shared
+    // memory: 1 the frontier rows and 2 the frontier and angular rows, by
+    // per-warp bulk copies of 32-event tiles; 3 the frontier values by
+    // per-thread asynchronous copies of the next event's values. CTPWA_STAGE
+    // sets it for both kernels. Default: 3 for the mixed form (K+K-pi0:
+    // 0.52-0.53 ms, against 0.63 ms direct, 0.744 ms with mode 1 and 1.10 ms
+    // with mode 2 at 1 CTA per SM), off for the plain path (its gradient-sum
+    // slots leave no room for the buffers at 2 CTAs per SM; with the slots
+    // in registers instead, mode 3 measured 1.39 ms against 1.15 ms).
+    const int st = get("CTPWA_STAGE", -1, 0, 3);
+    const int stage_req[2] = {st >= 0 ? st : 0, st >= 0 ? st : 3};
     const long long rowb[2] = {16, 8};  // bytes per complex angular value (FP64, FP32)
     const long long accb[2] = {8, 4};   // bytes per gradient sum (FP64, FP32)
     const long long per_sm = 228LL * 1024, per_cta = 227LL * 1024, reserve = 8LL * 1024;
@@ -1175,6 +1183,7 @@ FusedShape fusedShape(const GeneratedModel& gen)
         }
         const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
         const long long evb = i == 0 ? 8LL * gen.nev64 : 4LL * gen.nevf + 8LL * gen.nevd;  // frontier bytes per event
+        const int stage_on = stage_req[i];
         long long stage_bytes = 2LL * ((stage_on == 2 ? npl * rowb[i] : 0) + evb) * sh.block[i];
         if (stage_on == 3) {
             // [2][NA][block] values of the table's type (16-byte rounded), then [2][NB][block] FP64
@@ -1313,6 +1322,7 @@ void Engine::compileKernel()
     cudaKernel_t kevc;
     CT_CUDA(cudaLibraryGetKernel(&kevc, lib, "ct_event_cache"));
     k_evc_ = (void*)kevc;
+    CT_CUDA(cudaLibraryGetGlobal(&k_sym_, &k_sym_bytes_, lib, "ct_k"));
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
@@ -1369,6 +1379,7 @@ struct CtArgsH {
     int cta_base;
     int pad2;
     int* err;
+    void* kblock;
 };
 
 void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
@@ -1402,9 +1413,11 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     a.partials = d_partials_;
     a.consts = d_consts_;
     a.err = d_err_;
+    a.kblock = d_kblock_;
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    CT_CUDA(cudaMemcpyAsync(k_sym_, d_kblock_, k_sym_bytes_, cudaMemcpyDeviceToDevice, stream));
     const size_t slot = ev_begin_.empty() ? 0 : (size_t)(ev_count_ % (long long)ev_begin_.size());
     if (!ev_begin_.empty()) CT_CUDA(cudaEventRecord(ev_begin_[slot], stream));
     a.cta_base = 0;
@@ -1502,7 +1515,8 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     const size_t off_p = off_c + up((size_t)std::max(1, gen_.nconst));
     const size_t off_parts = off_p + up((size_t)lay.grid * nacc);
     const size_t off_err = off_parts + 8;  // one int (copy-timeout flag), zeroed by this call
-    const size_t need = off_err + 1;
+    const size_t off_k = up(off_err + 1);  // constant-bank image of this call
+    const size_t need = off_k + up((k_sym_bytes_ + 7) / 8);
     const size_t cap = kStaticScratchBytes / sizeof(double);
     if (need > cap)
         throw std::length_error("ctpwa_nll_grad_static: this model needs " + std::to_string(need * sizeof(double)) +
@@ -1542,9 +1556,11 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     a.partials = s_partials;
     a.consts = s_consts;
     a.err = (int*)(base + off_err);
+    a.kblock = base + off_k;
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    CT_CUDA(cudaMemcpyAsync(k_sym_, base + off_k, k_sym_bytes_, cudaMemcpyDeviceToDevice, stream));
     a.cta_base = 0;
     CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
                              args, (size_t)shape_.dsmem[precision == kMixed], stream));
@@ -1610,9 +1626,11 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     a.partials = d_partials_;
     a.consts = d_consts_;
     a.err = d_err_;
+    a.kblock = d_kblock_;
     if (precision == kMixed && !samples_[0].slamp32) throw std::runtime_error("mixed-precision tables were not built");
     void* args[] = {&a};
     CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    CT_CUDA(cudaMemcpyAsync(k_sym_, d_kblock_, k_sym_bytes_, cudaMemcpyDeviceToDevice, stream));
     a.cta_base = 0;
     CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid), dim3(shape_.block[precision == kMixed]),
                              args, (size_t)shape_.dsmem[precision == kMixed], stream));

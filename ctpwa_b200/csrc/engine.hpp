@@ -175,6 +175,9 @@ private:
     // evaluation buffers
     double* d_v_ = nullptr;         // [2 nA]
     double* d_consts_ = nullptr;    // [nconst] parameter-only subexpressions
+    void* d_kblock_ = nullptr;      // constant-bank image of the last call (CtConsts)
+    void* k_sym_ = nullptr;         // address of the fused kernels' constant-bank block (ct_k)
+    size_t k_sym_bytes_ = 0;
     double* d_partials_ = nullptr;  // [grid][nacc]
     double* d_parts_ = nullptr;     // [8]
     double* d_hscratch_ = nullptr;  // finite-difference Hessian: perturbed params, two gradients, nll [3 nP + 1]

@@ -39,7 +39,7 @@
 // per-thread gradient sums. The log, the log-likelihood and phase-space
 // intensity sums and every cross-thread reduction are FP64 in both forms.
 // Parameter-only parts of the lineshapes are computed once per call by
-// ct_prologue and staged in shared memory.
+// ct_prologue and, with the couplings, read from the constant bank.
 #pragma once
 
 #include "device_helpers.cuh"
@@ -97,15 +97,49 @@ struct CtArgs {
     int cta_base;         // CTA index of this launch's first block (split launches)
     int pad2;
     int* err;             // set to 1 when a staged copy did not arrive in time
+    void* kblock;         // CtConsts image of this call (written by ct_prologue) or nullptr
 };
 
-// One thread: the parameter-only part of every lineshape (prologue).
+#define CT_NCONST_ALLOC (M_NCONST > 0 ? M_NCONST : 1)
+
+// Per-call constants of the fused kernels in the constant bank: the
+// parameter-only subexpressions (FP64, and FP32 hi + lo pairs) and the
+// couplings (FP64, and FP32 hi + lo pairs). ct_prologue writes their image
+// into a device buffer, which the host copies to ct_k before each fused
+// launch; the fused kernels read them as constant-bank operands, with no load
+// instruction or register per use.
+struct CtConsts {
+    double c[CT_NCONST_ALLOC];
+    double v[2 * M_NA];
+    float ch[CT_NCONST_ALLOC], cl[CT_NCONST_ALLOC];
+    float vh[2 * M_NA], vl[2 * M_NA];
+};
+__constant__ CtConsts ct_k;
+
+// The parameter-only part of every lineshape (prologue, one thread), then
+// the constant-bank image of this call (one warp).
 extern "C" __global__ void ct_prologue(CtArgs A)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) model_prologue(A.theta, A.consts);
+    if (blockIdx.x != 0) return;
+    if (threadIdx.x == 0) model_prologue(A.theta, A.consts);
+    __syncthreads();
+    if (!A.kblock) return;
+    CtConsts* K = (CtConsts*)A.kblock;
+    for (int i = threadIdx.x; i < M_NCONST; i += blockDim.x) {
+        const double c = A.consts[i];
+        const float h = (float)c;
+        K->c[i] = c;
+        K->ch[i] = h;
+        K->cl[i] = (float)(c - (double)h);
+    }
+    for (int i = threadIdx.x; i < 2 * M_NA; i += blockDim.x) {
+        const double v = A.v[i];
+        const float h = (float)v;
+        K->v[i] = v;
+        K->vh[i] = h;
+        K->vl[i] = (float)(v - (double)h);
+    }
 }
-
-#define CT_NCONST_ALLOC (M_NCONST > 0 ? M_NCONST : 1)
 
 __device__ __forceinline__ void ct_stage_consts(const CtArgs& A, double* sC)
 {
@@ -274,28 +308,16 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     CtAccG<L, BLOCK, ACC_SMEM> accg;
     accg.init(ct_dyn);
 
-    // parameter-only constants: FP64, and as FP32 hi + lo pairs for the
-    // FP32 lineshapes (a single FP32 rounding would bias every event alike)
-    __shared__ double sC[CT_NCONST_ALLOC];
-    __shared__ float sCfh[CT_NCONST_ALLOC], sCfl[CT_NCONST_ALLOC];
-    for (int i = threadIdx.x; i < M_NCONST; i += blockDim.x) {
-        const double c = A.consts[i];
-        const float h = (float)c;
-        sC[i] = c;
-        sCfh[i] = h;
-        sCfl[i] = (float)(c - (double)h);
-    }
-    __syncthreads();
-    // couplings: (hi, lo) pairs in the FP32 form for the same reason
-    L vr[M_NA], vi[M_NA], vrl[M_NA], vil[M_NA];
-#pragma unroll
-    for (int a = 0; a < M_NA; ++a) {
-        const double r = __ldg(A.v + 2 * a), i = __ldg(A.v + 2 * a + 1);
-        vr[a] = (L)r;
-        vi[a] = (L)i;
-        vrl[a] = (L)(r - (double)vr[a]);
-        vil[a] = (L)(i - (double)vi[a]);
-    }
+    // parameter-only constants and couplings from the constant bank: FP64,
+    // and FP32 hi + lo pairs for the FP32 form (a single FP32 rounding would
+    // bias every event alike)
+    const double* sC = ct_k.c;
+    const float* sCfh = ct_k.ch;
+    const float* sCfl = ct_k.cl;
+    auto vr = [](int a) -> L { return sizeof(L) == 4 ? (L)ct_k.vh[2 * a] : (L)ct_k.v[2 * a]; };
+    auto vi = [](int a) -> L { return sizeof(L) == 4 ? (L)ct_k.vh[2 * a + 1] : (L)ct_k.v[2 * a + 1]; };
+    auto vrl = [](int a) -> L { return (L)ct_k.vl[2 * a]; };
+    auto vil = [](int a) -> L { return (L)ct_k.vl[2 * a + 1]; };
 
     // all per-event work: ap / bp / slp point at this event's frontier values
     // (table type, FP64) and angular values, consecutive values `ks` / `ss`
@@ -323,11 +345,11 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 // product with the FP32 coupling alone would bias the sample
                 // mean by ~1e-9 (both factors on the FP32 grid), which the
                 // normalisation term multiplies by the data weight sum.
-                cr[t] = fmaf(Fr[t], vr[a], Fr[t] * vrl[a]) - fmaf(Fi[t], vi[a], Fi[t] * vil[a]);
-                ci[t] = fmaf(Fi[t], vr[a], Fi[t] * vrl[a]) + fmaf(Fr[t], vi[a], Fr[t] * vil[a]);
+                cr[t] = fmaf(Fr[t], vr(a), Fr[t] * vrl(a)) - fmaf(Fi[t], vi(a), Fi[t] * vil(a));
+                ci[t] = fmaf(Fi[t], vr(a), Fi[t] * vrl(a)) + fmaf(Fr[t], vi(a), Fr[t] * vil(a));
             } else {
-                cr[t] = (R)(vr[a] * Fr[t] - vi[a] * Fi[t]);
-                ci[t] = (R)(vr[a] * Fi[t] + vi[a] * Fr[t]);
+                cr[t] = (R)(vr(a) * Fr[t] - vi(a) * Fi[t]);
+                ci[t] = (R)(vr(a) * Fi[t] + vi(a) * Fr[t]);
             }
         }
         R Sr[M_NPOL], Si[M_NPOL];
@@ -406,8 +428,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         for (int t = 0; t < M_NTERM; ++t) {
             const int a = term_col(t), c = term_plane(t);
             const L tr = (L)Tr[c], ti = (L)Ti[c];
-            Wr[t] = tscale * (vr[a] * tr + vi[a] * ti);
-            Wi[t] = tscale * (vi[a] * tr - vr[a] * ti);
+            Wr[t] = tscale * (vr(a) * tr + vi(a) * ti);
+            Wi[t] = tscale * (vi(a) * tr - vr(a) * ti);
         }
 #pragma unroll
         for (int k = 0; k < M_NDER; ++k) {

@@ -299,6 +299,7 @@ def test_staged_tables_match_direct_loads(tmp_path, monkeypatch, mode):
     # the same launch shape for both handles (room for the buffers), so every
     # thread sums the same events in the same order
     monkeypatch.setenv("CTPWA_F64_ACC_SMEM", "0")
+    monkeypatch.setenv("CTPWA_STAGE", "0")
     if mode == 2:
         monkeypatch.setenv("CTPWA_F64_MINB", "1")
         monkeypatch.setenv("CTPWA_MX_MINB", "1")
