@@ -1135,8 +1135,9 @@ void Engine::buildEventCache(int kind)
 // K+K-pi0 workload with the frontier tables: plain 256 x 2 with the gradient
 // sums in shared memory (128 registers, 16 warps per SM) 1.15 ms, against
 // 1.26 ms with the sums in registers, 1.63 ms at 128 x 5 and 2.55 ms at
-// 256 x 3; mixed 256 x 2 in registers 0.598 ms, against 0.70 ms at 3 CTAs
-// per SM, 0.66 ms with the sums in shared memory, 0.65 ms at 128 x 5.
+// 256 x 3; mixed (frontier values by asynchronous copies, constants in the
+// constant bank) 256 x 2 with the sums in shared memory 0.491 ms, against
+// 0.51 ms in registers, 0.77 ms at 3 CTAs per SM, 0.55 ms at 128 x 4.
 FusedShape fusedShape(const GeneratedModel& gen)
 {
     FusedShape sh;
@@ -1152,7 +1153,7 @@ FusedShape fusedShape(const GeneratedModel& gen)
     sh.block[1] = get("CTPWA_MX_BLOCK", 256, 32, 1024);
     sh.minb[1] = get("CTPWA_MX_MINB", 2, 1, 16);
     sh.acc[0] = get("CTPWA_F64_ACC_SMEM", 1, 0, 1);
-    sh.acc[1] = get("CTPWA_MX_ACC_SMEM", 0, 0, 1);
+    sh.acc[1] = get("CTPWA_MX_ACC_SMEM", 1, 0, 1);
 
     for (int i = 0; i < 2; ++i)
         if (sh.block[i] % 32) throw std::runtime_error("fused block sizes must be multiples of 32");

@@ -66,7 +66,7 @@
 #define CT_F64_ACC 1
 #endif
 #ifndef CT_MX_ACC
-#define CT_MX_ACC 0
+#define CT_MX_ACC 1
 #endif
 #ifndef CT_WAIT_LIMIT
 #define CT_WAIT_LIMIT (1u << 22)
