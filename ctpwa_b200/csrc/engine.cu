@@ -1132,10 +1132,10 @@ void Engine::buildEventCache(int kind)
 // Block size and minimum resident CTAs per SM of the plain [0] and mixed [1]
 // fused kernels, unless CTPWA_F64_BLOCK / CTPWA_F64_MINB / CTPWA_MX_BLOCK /
 // CTPWA_MX_MINB / CTPWA_*_ACC_SMEM override them (tuning). Measured on the
-// K+K-pi0 workload with the frontier tables: plain 256 x 2 with the gradient
-// sums in shared memory (128 registers, 16 warps per SM) 1.15 ms, against
-// 1.26 ms with the sums in registers, 1.63 ms at 128 x 5 and 2.55 ms at
-// 256 x 3; mixed (frontier values by asynchronous copies, constants in the
+// K+K-pi0 workload with the frontier tables and the constant bank: plain
+// 192 x 2 with the gradient sums in shared memory (170 registers, 12 warps
+// per SM, no spills) 0.95 ms, against 0.95 ms at 96 x 4, 0.99 ms at 128 x 3,
+// 1.15 ms at 256 x 2 (128 registers, spills) and 1.17 ms at 224 x 2; mixed (frontier values by asynchronous copies, constants in the
 // constant bank) 256 x 2 with the sums in shared memory 0.491 ms, against
 // 0.51 ms in registers, 0.77 ms at 3 CTAs per SM, 0.55 ms at 128 x 4.
 FusedShape fusedShape(const GeneratedModel& gen)
@@ -1148,7 +1148,7 @@ FusedShape fusedShape(const GeneratedModel& gen)
         if (v < lo || v > hi) throw std::runtime_error(std::string(name) + " out of range");
         return v;
     };
-    sh.block[0] = get("CTPWA_F64_BLOCK", 256, 32, 1024);
+    sh.block[0] = get("CTPWA_F64_BLOCK", 192, 32, 1024);
     sh.minb[0] = get("CTPWA_F64_MINB", 2, 1, 16);
     sh.block[1] = get("CTPWA_MX_BLOCK", 256, 32, 1024);
     sh.minb[1] = get("CTPWA_MX_MINB", 2, 1, 16);

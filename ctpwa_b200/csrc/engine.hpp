@@ -19,7 +19,7 @@ enum Precision : int { kFP64 = 0, kMixed = 1 };
 // minimum resident CTAs per SM, and whether the event tables are staged
 // through shared memory by bulk copies (dynamic shared memory bytes).
 struct FusedShape {
-    int block[2] = {256, 256};
+    int block[2] = {192, 256};
     int minb[2] = {2, 2};
     int stage[2] = {0, 0};
     int acc[2] = {1, 1};  // per-thread gradient sums in shared memory

@@ -557,7 +557,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 // block size and minimum resident CTAs per SM of the two fused kernels (the
 // host launches with the same block sizes)
 #ifndef CT_F64_BLOCK
-#define CT_F64_BLOCK 256
+#define CT_F64_BLOCK 192
 #endif
 #ifndef CT_F64_MINB
 #define CT_F64_MINB 2
