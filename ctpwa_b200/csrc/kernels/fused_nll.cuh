@@ -190,8 +190,11 @@ struct CtAccG<L, BLOCK, true> {
     __device__ __forceinline__ L operator[](int i) const { return p[i * BLOCK]; }
 };
 
+// (the v-gradient sums are scaled by vscale and the theta-gradient sums by
+// tscale on the way out: the per-event factors common to a CTA's sample)
 template <int BLOCK, typename G>
-__device__ __forceinline__ void ct_block_reduce_store(const double* accd, const G& accg, double* out)
+__device__ __forceinline__ void ct_block_reduce_store(const double* accd, const G& accg, double* out, double vscale,
+                                                      double tscale)
 {
     __shared__ double red[BLOCK / 32][CT_NACC];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -207,7 +210,7 @@ __device__ __forceinline__ void ct_block_reduce_store(const double* accd, const 
         double x = 0.0;
 #pragma unroll
         for (int w = 0; w < BLOCK / 32; ++w) x += red[w][i];
-        out[i] = x;
+        out[i] = i < 2 ? x : (i < 2 + 2 * M_NA ? x * vscale : x * tscale);
     }
 }
 
@@ -369,9 +372,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         }
 
         // ---- per-event weight of the adjoint ----
+        // (the sample's common factors of the gradient terms, w / W or -1 for
+        // the v-gradient and 2 or -2 for the theta-gradient, are applied to
+        // the CTA sums; a weighted phase-space event scales its v-gradient
+        // terms by its weight here)
         R ur[M_NPOL], ui[M_NPOL];
-        L gscale;  // factor applied to v-gradient contributions
-        L tscale;  // factor applied to theta-gradient contributions
+        L gw = (L)1;
         if (kind == 0) {
             const double we = wts ? __ldg(wts + e) : 1.0;
             accd[1] += (double)f;
@@ -380,8 +386,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 ur[p] = Sr[p];
                 ui[p] = Si[p];
             }
-            gscale = (L)(we * S.vw_scale);
-            tscale = (L)2;
+            gw = (L)we;
         } else {
             const double we = wts ? __ldg(wts + e) : 1.0;
             if (f == (R)0) {
@@ -396,8 +401,6 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 ur[p] = fmin(fmax(Sr[p] * inv, -kmax), kmax);
                 ui[p] = fmin(fmax(Si[p] * inv, -kmax), kmax);
             }
-            gscale = (L)-1;
-            tscale = (L)-2;
         }
         // T_c = sum_p conj(SL_{c,p}) u_p
         R Tr[M_NPLANE], Ti[M_NPLANE];
@@ -414,13 +417,24 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             Ti[c] = ti;
         }
         // v-gradient: sum over the column's terms of conj(F_t) T_plane(t)
+        if (kind == 0 && wts) {
 #pragma unroll
-        for (int t = 0; t < M_NTERM; ++t) {
-            const int a = term_col(t), c = term_plane(t);
-            const L fr = Fr[t], fi = Fi[t];
-            const L tr = (L)Tr[c], ti = (L)Ti[c];
-            accg.add(2 * a, gscale * (fr * tr + fi * ti));
-            accg.add(2 * a + 1, gscale * (fr * ti - fi * tr));
+            for (int t = 0; t < M_NTERM; ++t) {
+                const int a = term_col(t), c = term_plane(t);
+                const L fr = Fr[t], fi = Fi[t];
+                const L tr = (L)Tr[c], ti = (L)Ti[c];
+                accg.add(2 * a, gw * (fr * tr + fi * ti));
+                accg.add(2 * a + 1, gw * (fr * ti - fi * tr));
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < M_NTERM; ++t) {
+                const int a = term_col(t), c = term_plane(t);
+                const L fr = Fr[t], fi = Fi[t];
+                const L tr = (L)Tr[c], ti = (L)Ti[c];
+                accg.add(2 * a, fr * tr + fi * ti);
+                accg.add(2 * a + 1, fr * ti - fi * tr);
+            }
         }
         // theta-gradient: Re(v dF_t conj(T)) = Re(dF_t W_t), W_t = v_col(t) conj(T_plane(t))
         L Wr[M_NTERM], Wi[M_NTERM];
@@ -428,8 +442,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         for (int t = 0; t < M_NTERM; ++t) {
             const int a = term_col(t), c = term_plane(t);
             const L tr = (L)Tr[c], ti = (L)Ti[c];
-            Wr[t] = tscale * (vr(a) * tr + vi(a) * ti);
-            Wi[t] = tscale * (vi(a) * tr - vr(a) * ti);
+            Wr[t] = vr(a) * tr + vi(a) * ti;
+            Wi[t] = vi(a) * tr - vr(a) * ti;
         }
 #pragma unroll
         for (int k = 0; k < M_NDER; ++k) {
@@ -551,7 +565,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride)
             event(e, eva + e, evb ? evb + e : nullptr, S.ld, slamp + e, S.ld);
     }
-    ct_block_reduce_store<BLOCK>(accd, accg, A.partials + (long long)cta * CT_NACC);
+    ct_block_reduce_store<BLOCK>(accd, accg, A.partials + (long long)cta * CT_NACC, kind == 0 ? S.vw_scale : -1.0,
+                                 kind == 0 ? 2.0 : -2.0);
 }
 
 // block size and minimum resident CTAs per SM of the two fused kernels (the
