@@ -153,6 +153,56 @@ class analysis:
         self._h = ctypes.c_void_p(h)
         self._np = self._lib.ctpwa_n_params(self._h)
 
+    @classmethod
+    def from_device(cls, config_file: str, phsp, data, bkg=None, weights=None, device=None,
+                    precision: str = "fp64") -> "analysis":
+        """Analysis over in-memory samples: the model from config_file, the
+        events from float64 CUDA tensors [n, n_final, 4] (E, px, py, pz in the
+        config's Data.order) instead of the config's Data files. weights: None
+        or three per-event float64 CUDA tensors / None (phase space, data,
+        background). The tensors are copied; pending work on the current
+        stream is waited for first."""
+        self = cls.__new__(cls)
+        self._h = None
+        self._lib = _lib.load()
+        if device is None:
+            device = phsp.device.index if phsp.is_cuda else torch.cuda.current_device()
+        self._device = int(device)
+        self._precision = self._parse_precision(precision)
+        self._fit_mode = 1
+        self._shard = (0, 1)
+        samples = [phsp, data, bkg]
+        ws = list(weights) if weights is not None else [None, None, None]
+        keep = []
+        p4 = (ctypes.c_void_p * 3)()
+        n = (ctypes.c_longlong * 3)()
+        w = (ctypes.c_void_p * 3)()
+        for k, t in enumerate(samples):
+            if t is None:
+                continue
+            if t.dtype != torch.float64 or not t.is_cuda or t.dim() != 3 or t.shape[2] != 4:
+                raise RuntimeError("in-memory samples must be float64 CUDA tensors [n, n_final, 4]")
+            t = t.contiguous()
+            keep.append(t)
+            p4[k] = t.data_ptr()
+            n[k] = t.shape[0]
+            if ws[k] is not None:
+                wt = ws[k].to(device=t.device, dtype=torch.float64).contiguous()
+                if wt.numel() != t.shape[0]:
+                    raise RuntimeError("one weight per event")
+                keep.append(wt)
+                w[k] = wt.data_ptr()
+        torch.cuda.current_stream(self._device).synchronize()
+        status = ctypes.c_int(0)
+        err = ctypes.create_string_buffer(4096)
+        h = self._lib.ctpwa_create_from_device(str(config_file).encode(), self._device, p4, n, w,
+                                               ctypes.byref(status), err, 4096)
+        if not h:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        self._h = ctypes.c_void_p(h)
+        self._np = self._lib.ctpwa_n_params(self._h)
+        return self
+
     # ------------------------------------------------------------ lifecycle
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None

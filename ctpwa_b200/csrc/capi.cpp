@@ -52,24 +52,14 @@ ctpwa_handle* ctpwa_create(const char* config_path, int device, int* status, cha
     return ctpwa_create_shard(config_path, device, 0, 1, status, err, errlen);
 }
 
-ctpwa_handle* ctpwa_create_shard(const char* config_path, int device, int rank, int world, int* status, char* err,
-                                 size_t errlen)
+namespace {
+ctpwa_handle* createWith(const char* config_path, const ctpwa::EngineOptions& opt, int* status, char* err,
+                         size_t errlen)
 {
     auto h = std::make_unique<ctpwa_handle>();
     int code = CTPWA_OK;
     std::string msg;
-    if (world < 1 || rank < 0 || rank >= world) {
-        msg = "shard: need 0 <= rank < world";
-        if (status) *status = CTPWA_ERR_ARG;
-        setErr(nullptr, CTPWA_ERR_ARG, msg);
-        if (err && errlen) copyOut(msg, err, errlen);
-        return nullptr;
-    }
     try {
-        ctpwa::EngineOptions opt;
-        opt.device = device;
-        opt.shard_rank = rank;
-        opt.shard_world = world;
         h->eng = std::make_unique<ctpwa::Engine>(config_path ? config_path : "config.yml", opt);
         int np = h->eng->nParams();
         if (cudaMalloc(&h->d_params, sizeof(double) * std::max(1, np)) != cudaSuccess ||
@@ -87,6 +77,46 @@ ctpwa_handle* ctpwa_create_shard(const char* config_path, int device, int rank, 
         return nullptr;
     }
     return h.release();
+}
+}  // namespace
+
+ctpwa_handle* ctpwa_create_shard(const char* config_path, int device, int rank, int world, int* status, char* err,
+                                 size_t errlen)
+{
+    if (world < 1 || rank < 0 || rank >= world) {
+        const std::string msg = "shard: need 0 <= rank < world";
+        if (status) *status = CTPWA_ERR_ARG;
+        setErr(nullptr, CTPWA_ERR_ARG, msg);
+        if (err && errlen) copyOut(msg, err, errlen);
+        return nullptr;
+    }
+    ctpwa::EngineOptions opt;
+    opt.device = device;
+    opt.shard_rank = rank;
+    opt.shard_world = world;
+    return createWith(config_path, opt, status, err, errlen);
+}
+
+ctpwa_handle* ctpwa_create_from_device(const char* config_path, int device, const double* const* p4,
+                                       const long long* n, const double* const* w, int* status, char* err,
+                                       size_t errlen)
+{
+    if (!p4 || !n) {
+        const std::string msg = "null argument";
+        if (status) *status = CTPWA_ERR_ARG;
+        setErr(nullptr, CTPWA_ERR_ARG, msg);
+        if (err && errlen) copyOut(msg, err, errlen);
+        return nullptr;
+    }
+    ctpwa::EngineOptions opt;
+    opt.device = device;
+    opt.device_samples = true;
+    for (int k = 0; k < 3; ++k) {
+        opt.dev_p4[k] = p4[k];
+        opt.dev_n[k] = n[k];
+        opt.dev_w[k] = w ? w[k] : nullptr;
+    }
+    return createWith(config_path, opt, status, err, errlen);
 }
 
 void ctpwa_destroy(ctpwa_handle* h)

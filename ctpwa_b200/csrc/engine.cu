@@ -842,6 +842,37 @@ void Engine::loadSamples()
     const char* kinds[3] = {"phsp", "data", "bkg"};
     const char* wkeys[3] = {"phsp_weights", "data_weights", "bkg_weights"};
     int nfin = (int)model_.final_order.size();
+    if (opt_.device_samples) {
+        // events from the caller's device arrays: transposed straight into
+        // the SoA planes, weights copied (and summed on the host)
+        for (int k = 0; k < 3; ++k) {
+            const long long n = opt_.dev_n[k];
+            if (n < 0 || (n > 0 && !opt_.dev_p4[k])) throw std::runtime_error("in-memory sample: bad event array");
+            if (k < 2 && n == 0) throw std::runtime_error(std::string("in-memory samples need a ") + kinds[k] + " sample");
+            DeviceSample& d = samples_[k];
+            d.n = n;
+            d.wsum = (double)n;
+            if (k == 2) has_bkg_ = n > 0;
+            if (n == 0) continue;
+            const size_t bytes = sizeof(double) * (size_t)n * nfin * 4;
+            CT_CUDA(cudaMallocAsync((void**)&d.p4, bytes, init_stream_));
+            ag_transpose_kernel<<<(unsigned)((n + 255) / 256), 256, 0, init_stream_>>>(opt_.dev_p4[k], d.p4, n, nfin);
+            CT_CUDA(cudaGetLastError());
+            device_bytes_ += bytes;
+            if (opt_.dev_w[k]) {
+                CT_CUDA(cudaMalloc(&d.w, sizeof(double) * n));
+                CT_CUDA(cudaMemcpyAsync(d.w, opt_.dev_w[k], sizeof(double) * n, cudaMemcpyDeviceToDevice, init_stream_));
+                std::vector<double> w((size_t)n);
+                CT_CUDA(cudaMemcpyAsync(w.data(), opt_.dev_w[k], sizeof(double) * n, cudaMemcpyDeviceToHost, init_stream_));
+                CT_CUDA(cudaStreamSynchronize(init_stream_));
+                d.wsum = 0.0;
+                for (double x : w) d.wsum += x;
+                device_bytes_ += sizeof(double) * n;
+            }
+            CT_CUDA(cudaStreamSynchronize(init_stream_));
+        }
+        return;
+    }
     for (int k = 0; k < 3; ++k) {
         auto it = model_.cfg.data_files.find(kinds[k]);
         if (it == model_.cfg.data_files.end()) {

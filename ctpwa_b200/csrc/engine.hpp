@@ -47,6 +47,13 @@ struct EngineOptions {
     bool mixed_tables = true;  // build the FP32 angular table for the mixed path
     int shard_rank = 0;        // keep event block shard_rank of shard_world of every sample
     int shard_world = 1;
+    // In-memory samples: when set, the events come from these device arrays
+    // (AoS [n][n_final][4], the config's Data.order; weights or nullptr)
+    // instead of the config's Data files; the arrays are copied.
+    bool device_samples = false;
+    const double* dev_p4[3] = {nullptr, nullptr, nullptr};
+    long long dev_n[3] = {0, 0, 0};
+    const double* dev_w[3] = {nullptr, nullptr, nullptr};
 };
 
 // Compile (or find in the disk cache) the fused kernel of a config's model

@@ -3,8 +3,9 @@
 The workload pattern of the reference's fit driver (example/fit.py:115-216,
 600-650) as a service: jobs arrive over time (a Poisson stream), each brings
 its own seeded event sample (data by accept-reject against the model, 10x
-phase space), runs a quasi-Newton fit (L-BFGS, about 100 NLL + gradient
-evaluations) and ends with one Hessian.
+phase space, generated and kept on the GPU), runs a quasi-Newton fit
+(L-BFGS-B on the host, at most 100 NLL + gradient evaluations on the device)
+and ends with one exact Hessian.
 
 * Admission by device memory: a job is admitted when a slot is free and its
   estimated resident bytes (event caches, from a per-model bytes-per-event
@@ -72,6 +73,9 @@ class JobResult:
     setup_done: float = 0.0
     finished: float = 0.0
     error: Optional[str] = None
+    # phases of the service time (ms): toy-MC generation, handle creation
+    # (model, kernels, angular pass), fit, Hessian
+    phase_ms: dict = field(default_factory=dict)
 
     @property
     def fit_latency(self) -> float:
@@ -134,10 +138,12 @@ class Server:
         return self._bpe[model]
 
     def job_bytes(self, spec: JobSpec) -> int:
-        # resident caches plus the transient momenta of the angular pass and
-        # the accept-reject candidates (12x data) during set-up
+        # resident caches plus, during set-up, the accept-reject candidates
+        # (12x data: their momenta and the caches of the handle that weighs
+        # them) and the transient momenta of the angular passes
         events = spec.n_data + spec.n_phsp
-        return int(self.bytes_per_event(spec.model) * events + 96 * (events + 12 * spec.n_data))
+        cand = 12 * spec.n_data + 10_000
+        return int(self.bytes_per_event(spec.model) * (events + cand) + 96 * (2 * events + 2 * cand))
 
     def try_reserve(self, nbytes: int) -> bool:
         with self._lock:
@@ -162,9 +168,16 @@ class Server:
         stream = torch.cuda.Stream(device=self.device)
         try:
             with torch.cuda.device(self.device), torch.cuda.stream(stream):
-                cfg = workloads.make(spec.model, d, n_phsp=spec.n_phsp, n_data=spec.n_data, n_bkg=0,
-                                     seed=spec.seed, accept_reject=True, device=self.device)
-                ana = analysis(cfg, device=self.device, precision=spec.precision)
+                # toy-MC events generated and kept on the device, the job's
+                # handle built from them (no file round trip)
+                t1 = time.perf_counter()
+                cfg, phsp, data = workloads.make_device(spec.model, d, spec.n_phsp, spec.n_data, seed=spec.seed,
+                                                        device=self.device)
+                t2 = time.perf_counter()
+                ana = analysis.from_device(cfg, phsp, data, device=self.device, precision=spec.precision)
+                del phsp, data
+                stream.synchronize()
+                t3 = time.perf_counter()
                 nV = ana.getNVector()
                 truth = workloads.true_params(nV, ana.getFreeResParams()[0].numpy())
                 rng = np.random.default_rng(spec.seed + 7)
@@ -174,8 +187,13 @@ class Server:
                 start[2 * nV:] *= 1.0 + 0.002 * rng.standard_normal(start.size - 2 * nV)
                 res.setup_done = time.perf_counter() - t0
                 p, nll, n_evals, lat = self._fit(ana, start, spec, stream)
+                stream.synchronize()
+                t4 = time.perf_counter()
                 H = ana.getHessian(p)
                 stream.synchronize()
+                t5 = time.perf_counter()
+                res.phase_ms = {"generate": 1e3 * (t2 - t1), "handle": 1e3 * (t3 - t2), "fit": 1e3 * (t4 - t3),
+                                "hessian": 1e3 * (t5 - t4)}
                 res.params = p.cpu().numpy()
                 res.hessian = H.cpu().numpy()
                 res.nll = nll
@@ -190,54 +208,74 @@ class Server:
         return res
 
     def _fit(self, ana, start, spec: JobSpec, stream):
-        """L-BFGS with strong-Wolfe line search; every closure call is one
-        NLL + gradient evaluation (a CUDA-graph replay when graphs are on)."""
+        """L-BFGS-B on the host (bounds on the resonance parameters as the
+        reference's fit clamps them); every function call is one NLL +
+        gradient evaluation on the device: parameters in through pinned
+        memory, a CUDA-graph replay (when graphs are on), NLL and gradient
+        back in one copy."""
         import torch
+        from scipy.optimize import minimize
 
         dev = torch.device("cuda", self.device)
+        n = start.size
         static_p = torch.tensor(start, dtype=torch.float64, device=dev)
+        out_dev = torch.empty(n + 1, dtype=torch.float64, device=dev)
+        pin_in = torch.empty(n, dtype=torch.float64).pin_memory()
+        pin_out = torch.empty(n + 1, dtype=torch.float64).pin_memory()
+
+        def device_eval():
+            nll, grad = ana.getNLLAndGrad(static_p)
+            out_dev[0] = nll
+            out_dev[1:] = grad
+
         if self.graphs:
             # warm-up on the capture stream, then capture one evaluation
             for _ in range(2):
-                ana.getNLLAndGrad(static_p)
+                device_eval()
             stream.synchronize()
             graph = torch.cuda.CUDAGraph()
             # capture restrictions apply to this thread only; captures are serialised
             with self._capture_lock, torch.cuda.graph(graph, stream=stream, capture_error_mode="thread_local"):
-                g_nll, g_grad = ana.getNLLAndGrad(static_p)
-
-            def evaluate(x):
-                static_p.copy_(x)
-                graph.replay()
-                return g_nll, g_grad
+                device_eval()
+            run = graph.replay
         else:
-            def evaluate(x):
-                return ana.getNLLAndGrad(x)
+            run = device_eval
+
+        lat = []
+
+        def evaluate(x):
+            t = time.perf_counter()
+            pin_in.numpy()[:] = x
+            static_p.copy_(pin_in, non_blocking=True)
+            run()
+            pin_out.copy_(out_dev, non_blocking=True)
+            stream.synchronize()
+            lat.append(1e3 * (time.perf_counter() - t))
+            r = pin_out.numpy()
+            return float(r[0]), r[1:].copy()
 
         # the first coupling stays at its start value (overall phase and scale
         # of the couplings are not measured: example/fit.py:48 fixes it)
         nV = ana.getNVector()
-        free = torch.ones(start.size, dtype=torch.float64, device=dev)
-        free[0] = 0.0
-        free[nV] = 0.0
-        x = torch.tensor(start, dtype=torch.float64, device=dev, requires_grad=True)
-        opt = torch.optim.LBFGS([x], lr=1.0, max_iter=spec.max_evals, max_eval=spec.max_evals,
-                                tolerance_grad=1e-9, tolerance_change=1e-12, history_size=20,
-                                line_search_fn="strong_wolfe")
-        lat = []
+        free = np.ones(n, dtype=bool)
+        free[0] = False
+        free[nV] = False
+        lo_hi = ana.getFreeResParams().numpy()
+        bounds = [(None, None)] * (2 * nV) + [(float(l), float(h)) for l, h in zip(lo_hi[1], lo_hi[2])]
+        bounds = [b for b, f in zip(bounds, free) if f]
+        x_full = start.astype(np.float64).copy()
 
-        def closure():
-            t = time.perf_counter()
-            nll, grad = evaluate(x.detach())
-            x.grad = grad * free
-            v = nll.clone()
-            float(v)  # the optimiser needs the value on the host
-            lat.append(1e3 * (time.perf_counter() - t))
-            return v
+        def fun(xf):
+            x_full[free] = xf
+            f, g = evaluate(x_full)
+            return f, g[free]
 
-        opt.step(closure)
-        nll, _ = evaluate(x.detach())
-        return x.detach().clone(), float(nll), len(lat), lat
+        opt = minimize(fun, x_full[free], jac=True, method="L-BFGS-B", bounds=bounds,
+                       options={"maxfun": spec.max_evals, "maxcor": 20, "ftol": 1e-13, "gtol": 1e-9})
+        x_full[free] = opt.x
+        nll, _ = evaluate(x_full)
+        lat.pop()
+        return torch.tensor(x_full, dtype=torch.float64, device=dev), nll, len(lat), lat
 
     # ----------------------------------------------------------- the stream
     def run(self, jobs: List[JobSpec], realtime: bool = True) -> List[JobResult]:
@@ -304,6 +342,8 @@ def summary(results: List[JobResult], wall_s: float) -> dict:
         "fit_ms_p99": percentile(fits, 99),
         "service_ms_p50": percentile(service, 50),
         "service_ms_p99": percentile(service, 99),
+        "phase_ms_p50": {k: percentile([r.phase_ms[k] for r in ok if k in r.phase_ms], 50)
+                         for k in ("generate", "handle", "fit", "hessian")},
         "errors": [r.error for r in results if r.error][:5],
     }
 

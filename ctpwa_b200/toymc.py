@@ -79,10 +79,10 @@ def phase_space(M, masses, n, seed):
     return out
 
 
-def phase_space_gpu(M, masses, n, seed, device="cuda"):
+def phase_space_gpu(M, masses, n, seed, device="cuda", as_tensor=False):
     """Same generator on the GPU with torch's seeded Philox RNG (large samples).
 
-    Returns a float64 numpy array (n, 3, 4)."""
+    Returns a float64 numpy array (n, 3, 4), or the CUDA tensor (as_tensor)."""
     import torch
 
     m1, m2, m3 = (float(x) for x in masses)
@@ -137,7 +137,7 @@ def phase_space_gpu(M, masses, n, seed, device="cuda"):
         out[filled:filled + take, 1] = boost(p2r)[:take]
         out[filled:filled + take, 2] = p3[:take]
         filled += take
-    return out.cpu().numpy()
+    return out if as_tensor else out.cpu().numpy()
 
 
 def write_dat(path, p4):

@@ -281,3 +281,42 @@ def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, inten
         except OSError:
             pass
     return sel[:n_data]
+
+
+def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2):
+    """Toy-MC samples of workload `name` generated and kept on the GPU:
+    phase space from the seeded GPU generator, data by accept-reject of GPU
+    candidates against the model's intensity at the true parameters (the
+    candidates' intensities from an in-memory analysis, the draw on the
+    device). Writes only config.yml (its Data entries name no files that are
+    read) and returns (config_path, phsp, data) with float64 CUDA tensors
+    [n, 3, 4] for ``analysis.from_device``."""
+    import torch
+
+    from . import analysis, describe
+
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    masses = MASSES[name]
+    dev = f"cuda:{device}"
+    cfg = out / "config.yml"
+    cfg.write_text(config_text(name, "in-memory-phsp", "in-memory-data"))
+    phsp = toymc.phase_space_gpu(M_JPSI, masses, n_phsp, 1001 + seed, device=dev, as_tensor=True)
+    tiny = toymc.phase_space_gpu(M_JPSI, masses, 1000, 7001 + seed, device=dev, as_tensor=True)
+    p = torch.tensor(params_for(describe(str(cfg))), dtype=torch.float64, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(6001 + seed)
+    chunks, have, batch = [], 0, 0
+    while have < n_data:
+        ncand = int((n_data - have) * 12) + 10_000
+        cand = toymc.phase_space_gpu(M_JPSI, masses, ncand, 5001 + seed + 7919 * batch, device=dev, as_tensor=True)
+        ana = analysis.from_device(str(cfg), tiny, cand, device=device)
+        I = ana.getIntensity(p, kind=1)
+        del ana
+        u = torch.rand(ncand, generator=gen, dtype=torch.float64, device=dev) * (safety * I.max())
+        sel = cand[u < I]
+        chunks.append(sel)
+        have += sel.shape[0]
+        batch += 1
+    data = torch.cat(chunks)[:n_data].contiguous()
+    return str(cfg), phsp, data

@@ -49,6 +49,18 @@ ctpwa_handle* ctpwa_create(const char* config_path, int device, int* status, cha
 ctpwa_handle* ctpwa_create_shard(const char* config_path, int device, int rank, int world, int* status, char* err,
                                  size_t errlen);
 
+/* In-memory samples (no counterpart in the reference, which reads every
+ * sample from the files of its config): the model from config_path, the
+ * events from device arrays instead of the config's Data files. For k = 0
+ * phase space, 1 data, 2 background: p4[k] device pointer to AoS
+ * [n[k]][n_final][4] (E, px, py, pz in the config's Data.order; n[2] = 0 for
+ * no background), w[k] device per-event weights or nullptr (unit weights).
+ * The arrays are copied during the call; the caller keeps them. For toy-MC
+ * jobs whose events are generated on the device (no file round trip). */
+ctpwa_handle* ctpwa_create_from_device(const char* config_path, int device, const double* const* p4,
+                                       const long long* n, const double* const* w, int* status, char* err,
+                                       size_t errlen);
+
 /* Releases device memory of the handle (the reference never frees; src/Analysis.cu:1284-1290). */
 void ctpwa_destroy(ctpwa_handle* h);
 

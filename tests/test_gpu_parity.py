@@ -340,3 +340,35 @@ def test_write_result_export(setups, tmp_path):
         assert abs(out[f"weight_{i}"].sum() / out["norm_factor"] - I[i]) <= 1e-10 * I[i]
     loaded = np.load(tmp_path / "res.npz")
     assert set(loaded.files) >= {"legends", "interference", "totalweight"}
+
+
+def test_in_memory_samples_match_files(tmp_path):
+    """analysis.from_device over the same events as a file-based analysis
+    gives bit-identical results; the on-device toy generator is seeded."""
+    import torch
+    import ctpwa_b200
+    from ctpwa_b200 import toymc
+
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=30_001, n_data=4_001, n_bkg=999, accept_reject=False, seed=21)
+    files = ctpwa_b200.analysis(cfg)
+    dev = [torch.from_numpy(np.load(tmp_path / f)).cuda() for f in ("phsp.npy", "data.npy", "bkg.npy")]
+    w = [None, None, torch.full((dev[2].shape[0],), 0.3, dtype=torch.float64, device="cuda")]
+    mem = ctpwa_b200.analysis.from_device(cfg, dev[0], dev[1], dev[2], weights=w)
+    assert tuple(mem.getNEvents()) == tuple(files.getNEvents())
+    p = workloads.true_params(files.getNVector(), files.getFreeResParams()[0].numpy())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    for prec in ("fp64", "mixed"):
+        n0, g0 = files.getNLLAndGrad(pt, prec)
+        n1, g1 = mem.getNLLAndGrad(pt, prec)
+        assert float(n0) == float(n1) and torch.equal(g0, g1), prec
+    c1, ph1, d1 = workloads.make_device("pipi_rho", tmp_path / "a", 50_000, 5_000, seed=4)
+    c2, ph2, d2 = workloads.make_device("pipi_rho", tmp_path / "b", 50_000, 5_000, seed=4)
+    assert ph1.shape == (50_000, 3, 4) and d1.shape == (5_000, 3, 4)
+    assert torch.equal(ph1, ph2) and torch.equal(d1, d2)
+    # accept-reject favours the resonance: data are not flat phase space
+    flat = torch.from_numpy(toymc.phase_space(workloads.M_JPSI, workloads.MASSES["pipi_rho"], 5_000, 3))
+    def m12(x):
+        s = x[:, 0] + x[:, 1]
+        return torch.sqrt(s[:, 0] ** 2 - (s[:, 1:] ** 2).sum(1))
+    near = lambda m: float(((m > 0.65) & (m < 0.9)).double().mean())
+    assert near(m12(d1.cpu())) > 1.5 * near(m12(flat))
