@@ -307,8 +307,9 @@ def streamed_bytes(layout, n_events, precision):
 def toy_fit(args, device):
     """Toy-fit serving stream: Poisson arrivals of fit jobs (single-rho and
     three-chain rho models, N_data log-uniform 10k-200k, 10x phase space),
-    L-BFGS to convergence (<= 100 evaluations) + Hessian each, 4 concurrent
-    slots; latency percentiles per evaluation and per fit, mixed and FP64."""
+    events generated on the GPU, L-BFGS-B to convergence (<= 100
+    evaluations) + exact Hessian each, 4 concurrent slots; latency
+    percentiles per evaluation and per fit, mixed and FP64."""
     from ctpwa_b200 import serving
 
     out = {}
@@ -334,7 +335,8 @@ def toy_fit(args, device):
         finally:
             srv.close()
         out[prec] = {k: s[k] for k in ("jobs", "failed", "fits_per_hour", "evals", "eval_ms_p50", "eval_ms_p99",
-                                        "fit_ms_p50", "fit_ms_p99", "service_ms_p50", "service_ms_p99")}
+                                        "fit_ms_p50", "fit_ms_p99", "service_ms_p50", "service_ms_p99",
+                                        "phase_ms_p50")}
     out["config"] = {"rate_per_s": args.toy_rate, "jobs": args.toy_jobs, "slots": 4, "n_data": "log-uniform 10k-200k",
                      "n_phsp": "10 x n_data", "models": ["pipi_rho", "pipi_3rho"], "cuda_graphs": True}
     return out

@@ -208,6 +208,9 @@ class analysis:
         h, self._h = getattr(self, "_h", None), None
         if h is not None:
             try:
+                # the handle's memory goes back to the pool without waiting
+                # for other streams: let work queued on the current one finish
+                torch.cuda.current_stream(self._device).synchronize()
                 self._lib.ctpwa_destroy(h)
             except Exception:
                 pass

@@ -29,6 +29,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
+#include <map>
 #include <mutex>
 #include <fstream>
 #include <sstream>
@@ -668,6 +669,42 @@ std::string cacheDir()
 
 }  // namespace
 
+// The library's device-memory pool of one device (created on first use,
+// kept for the process): freed blocks stay in the pool for later handles.
+cudaMemPool_t enginePool(int device)
+{
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool;
+    CT_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = ~0ull;
+    CT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[device] = pool;
+    return pool;
+}
+
+void* Engine::devAlloc(size_t bytes)
+{
+    void* p = nullptr;
+    CT_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), enginePool(opt_.device), mem_stream_));
+    // usable on any stream once the allocating stream has reached it
+    CT_CUDA(cudaStreamSynchronize(mem_stream_));
+    return p;
+}
+
+void Engine::devFree(void* p)
+{
+    if (p) cudaFreeAsync(p, mem_stream_);
+}
+
 // Resident 256-thread CTAs per SM of a fused kernel (occupancy query on the
 // library kernel handle; from its register count if that query is refused).
 int Engine::residentCtas(void* kernel, int block, int dsmem) const
@@ -738,6 +775,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     CT_CUDA(cudaGetDeviceCount(&ndev));
     if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
     CT_CUDA(cudaSetDevice(opt_.device));
+    CT_CUDA(cudaStreamCreateWithFlags(&mem_stream_, cudaStreamNonBlocking));
     shape_ = fusedShape(gen_);
     // initialisation work goes to a private non-blocking stream, so a handle
     // being created does not serialise with other handles' evaluations
@@ -749,17 +787,17 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
         if (samples_[k].n > 0 || k < 2) computeAngular(k);
     // evaluation buffers
     int nA = model_.nAmp();
-    CT_CUDA(cudaMalloc(&d_v_, sizeof(double) * 2 * nA));
-    CT_CUDA(cudaMalloc(&d_consts_, sizeof(double) * std::max(1, gen_.nconst)));
-    CT_CUDA(cudaMalloc(&d_kblock_, k_sym_bytes_));
+    alloc(d_v_, sizeof(double) * 2 * nA);
+    alloc(d_consts_, sizeof(double) * std::max(1, gen_.nconst));
+    alloc(d_kblock_, k_sym_bytes_);
     std::vector<double> ratio = model_.coupling.ratio;
-    CT_CUDA(cudaMalloc(&d_amp_chain_, sizeof(int) * nA));
-    CT_CUDA(cudaMalloc(&d_ratio_, sizeof(double) * nA));
+    alloc(d_amp_chain_, sizeof(int) * nA);
+    alloc(d_ratio_, sizeof(double) * nA);
     CT_CUDA(cudaMemcpyAsync(d_amp_chain_, model_.coupling.amp_chain.data(), sizeof(int) * nA, cudaMemcpyHostToDevice, init_stream_));
     CT_CUDA(cudaMemcpyAsync(d_ratio_, ratio.data(), sizeof(double) * nA, cudaMemcpyHostToDevice, init_stream_));
     int ng = (int)model_.gauss.size();
-    CT_CUDA(cudaMalloc(&d_gauss_idx_, sizeof(int) * std::max(1, ng)));
-    CT_CUDA(cudaMalloc(&d_gauss_ms_, sizeof(double) * 2 * std::max(1, ng)));
+    alloc(d_gauss_idx_, sizeof(int) * std::max(1, ng));
+    alloc(d_gauss_ms_, sizeof(double) * 2 * std::max(1, ng));
     if (ng) {
         std::vector<int> gi;
         std::vector<double> gm;
@@ -787,12 +825,12 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     }
     grid_max_ = maxgrid;
     int nacc = 2 + 2 * nA + model_.nTheta();
-    CT_CUDA(cudaMalloc(&d_partials_, sizeof(double) * (size_t)grid_max_ * nacc));
-    CT_CUDA(cudaMalloc(&d_parts_, sizeof(double) * 8));
-    CT_CUDA(cudaMalloc(&d_err_, sizeof(int)));
-    CT_CUDA(cudaMalloc(&d_mask_, sizeof(int) * std::max(1, (int)model_.blocks.size())));
+    alloc(d_partials_, sizeof(double) * (size_t)grid_max_ * nacc);
+    alloc(d_parts_, sizeof(double) * 8);
+    alloc(d_err_, sizeof(int));
+    alloc(d_mask_, sizeof(int) * std::max(1, (int)model_.blocks.size()));
     CT_CUDA(cudaMemsetAsync(d_err_, 0, sizeof(int), init_stream_));
-    CT_CUDA(cudaMalloc(&d_hscratch_, sizeof(double) * (3 * (size_t)std::max(1, model_.nParams()) + 1)));
+    alloc(d_hscratch_, sizeof(double) * (3 * (size_t)std::max(1, model_.nParams()) + 1));
     CT_CUDA(cudaStreamSynchronize(init_stream_));
     cudaStreamDestroy(init_stream_);
     init_stream_ = nullptr;
@@ -801,38 +839,42 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
 Engine::~Engine()
 {
     for (auto& s : samples_) {
-        cudaFree(s.p4);
-        cudaFree(s.slamp64);
-        cudaFree(s.slamp32);
-        cudaFree(s.kin);
-        cudaFree(s.ev64);
-        cudaFree(s.evf);
-        cudaFree(s.evd);
-        cudaFree(s.w);
+        devFree(s.p4);
+        devFree(s.slamp64);
+        devFree(s.slamp32);
+        devFree(s.kin);
+        devFree(s.ev64);
+        devFree(s.evf);
+        devFree(s.evd);
+        devFree(s.w);
     }
-    cudaFree(d_ag_tables_);
-    cudaFree(d_v_);
-    cudaFree(d_consts_);
-    cudaFree(d_kblock_);
-    cudaFree(d_partials_);
-    cudaFree(d_parts_);
-    cudaFree(d_hscratch_);
-    cudaFree(d_err_);
-    cudaFree(d_mask_);
-    cudaFree(d_amp_chain_);
-    cudaFree(d_ratio_);
-    cudaFree(d_gauss_idx_);
-    cudaFree(d_gauss_ms_);
+    devFree(d_ag_tables_);
+    devFree(d_v_);
+    devFree(d_consts_);
+    devFree(d_kblock_);
+    devFree(d_partials_);
+    devFree(d_parts_);
+    devFree(d_hscratch_);
+    devFree(d_err_);
+    devFree(d_mask_);
+    devFree(d_amp_chain_);
+    devFree(d_ratio_);
+    devFree(d_gauss_idx_);
+    devFree(d_gauss_ms_);
     for (size_t i = 0; i < ev_begin_.size(); ++i) {
         cudaEventDestroy(ev_begin_[i]);
         cudaEventDestroy(ev_end_[i]);
     }
     if (init_stream_) cudaStreamDestroy(init_stream_);
-    cudaFree(d_hdirs_);
-    cudaFree(d_hconsts_);
-    cudaFree(d_hrows_);
-    cudaFree(d_hvsums_);
-    cudaFree(d_htsums_);
+    devFree(d_hdirs_);
+    devFree(d_hconsts_);
+    devFree(d_hrows_);
+    devFree(d_hvsums_);
+    devFree(d_htsums_);
+    if (mem_stream_) {
+        cudaStreamSynchronize(mem_stream_);
+        cudaStreamDestroy(mem_stream_);
+    }
     if (hvp_lib_) cudaLibraryUnload((cudaLibrary_t)hvp_lib_);
     if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
 }
@@ -855,12 +897,12 @@ void Engine::loadSamples()
             if (k == 2) has_bkg_ = n > 0;
             if (n == 0) continue;
             const size_t bytes = sizeof(double) * (size_t)n * nfin * 4;
-            CT_CUDA(cudaMallocAsync((void**)&d.p4, bytes, init_stream_));
+            CT_CUDA(cudaMallocFromPoolAsync((void**)&d.p4, bytes, enginePool(opt_.device), init_stream_));
             ag_transpose_kernel<<<(unsigned)((n + 255) / 256), 256, 0, init_stream_>>>(opt_.dev_p4[k], d.p4, n, nfin);
             CT_CUDA(cudaGetLastError());
             device_bytes_ += bytes;
             if (opt_.dev_w[k]) {
-                CT_CUDA(cudaMalloc(&d.w, sizeof(double) * n));
+                alloc(d.w, sizeof(double) * n);
                 CT_CUDA(cudaMemcpyAsync(d.w, opt_.dev_w[k], sizeof(double) * n, cudaMemcpyDeviceToDevice, init_stream_));
                 std::vector<double> w((size_t)n);
                 CT_CUDA(cudaMemcpyAsync(w.data(), opt_.dev_w[k], sizeof(double) * n, cudaMemcpyDeviceToHost, init_stream_));
@@ -894,14 +936,14 @@ void Engine::loadSamples()
         if (s.n == 0) continue;
         size_t bytes = sizeof(double) * (size_t)s.n * nfin * 4;
         double* tmp = nullptr;
-        CT_CUDA(cudaMallocAsync((void**)&tmp, bytes, init_stream_));
+        CT_CUDA(cudaMallocFromPoolAsync((void**)&tmp, bytes, enginePool(opt_.device), init_stream_));
         CT_CUDA(cudaMemcpyAsync(tmp, s.p4.data(), bytes, cudaMemcpyHostToDevice, init_stream_));
-        CT_CUDA(cudaMallocAsync((void**)&d.p4, bytes, init_stream_));
+        CT_CUDA(cudaMallocFromPoolAsync((void**)&d.p4, bytes, enginePool(opt_.device), init_stream_));
         ag_transpose_kernel<<<(unsigned)((s.n + 255) / 256), 256, 0, init_stream_>>>(tmp, d.p4, s.n, nfin);
         CT_CUDA(cudaGetLastError());
         CT_CUDA(cudaFreeAsync(tmp, init_stream_));
         if (!w.empty()) {
-            CT_CUDA(cudaMalloc(&d.w, sizeof(double) * s.n));
+            alloc(d.w, sizeof(double) * s.n);
             CT_CUDA(cudaMemcpyAsync(d.w, w.data(), sizeof(double) * s.n, cudaMemcpyHostToDevice, init_stream_));
         }
         // the host sample is released at the end of this iteration
@@ -1067,7 +1109,7 @@ void Engine::buildTables()
         std::memcpy(img.data() + o_pm[g], gh[g].pol_map.data(), gh[g].pol_map.size() * sizeof(int));
         std::memcpy(img.data() + o_kin[g], gh[g].kin.data(), gh[g].kin.size() * sizeof(int));
     }
-    CT_CUDA(cudaMalloc(&d_ag_tables_, off));
+    alloc(d_ag_tables_, off);
     CT_CUDA(cudaMemcpyAsync(d_ag_tables_, img.data(), off, cudaMemcpyHostToDevice, init_stream_));
     CT_CUDA(cudaStreamSynchronize(init_stream_));
     char* base = (char*)d_ag_tables_;
@@ -1099,14 +1141,14 @@ void Engine::computeAngular(int kind)
     int npol = model_.npol;
     size_t nplanes = (size_t)gen_.nplane * npol;
     size_t b64 = sizeof(double2) * nplanes * ld;
-    CT_CUDA(cudaMalloc(&d.slamp64, b64));
+    alloc(d.slamp64, b64);
     device_bytes_ += b64;
     if (opt_.mixed_tables) {
-        CT_CUDA(cudaMalloc(&d.slamp32, b64 / 2));
+        alloc(d.slamp32, b64 / 2);
         device_bytes_ += b64 / 2;
     }
     size_t bk = sizeof(double) * std::max<size_t>(1, gen_.slots.size()) * ld;
-    CT_CUDA(cudaMalloc(&d.kin, bk));
+    alloc(d.kin, bk);
     device_bytes_ += bk;
     if (n == 0) {
         buildEventCache(kind);
@@ -1136,12 +1178,12 @@ void Engine::buildEventCache(int kind)
     DeviceSample& d = samples_[kind];
     const long long ld = d.ld;
     const size_t b64 = sizeof(double) * std::max(1, gen_.nev64) * ld;
-    CT_CUDA(cudaMalloc(&d.ev64, b64));
+    alloc(d.ev64, b64);
     device_bytes_ += b64;
     if (opt_.mixed_tables) {
         const size_t bf = sizeof(float) * std::max(1, gen_.nevf) * ld, bd = sizeof(double) * std::max(1, gen_.nevd) * ld;
-        CT_CUDA(cudaMalloc(&d.evf, bf));
-        CT_CUDA(cudaMalloc(&d.evd, bd));
+        alloc(d.evf, bf);
+        alloc(d.evd, bd);
         device_bytes_ += bf + bd;
     }
     if (d.n > 0) {
@@ -1155,7 +1197,7 @@ void Engine::buildEventCache(int kind)
         CT_CUDA(cudaLaunchKernel(k_evc_, dim3(grid), dim3(256), args, 0, init_stream_));
     }
     CT_CUDA(cudaStreamSynchronize(init_stream_));
-    cudaFree(d.kin);
+    devFree(d.kin);
     d.kin = nullptr;
     device_bytes_ -= sizeof(double) * std::max<size_t>(1, gen_.slots.size()) * ld;
 }
@@ -1933,11 +1975,11 @@ void Engine::compileHvp()
     layoutCtas(sms * occ, tot, hvp_block_, hlay_);
     const int nP = std::max(1, model_.nParams());
     hvp_cap_ = std::max(nP, 32);
-    CT_CUDA(cudaMalloc(&d_hdirs_, sizeof(double) * (size_t)nP * nP));
-    CT_CUDA(cudaMalloc(&d_hconsts_, sizeof(double) * 2 * (size_t)hvp_cap_ * std::max(1, gen_.nconst)));
-    CT_CUDA(cudaMalloc(&d_hrows_, sizeof(double) * (size_t)hvp_cap_ * hlay_.grid * nacc));
-    CT_CUDA(cudaMalloc(&d_hvsums_, sizeof(double) * (size_t)sumsSize()));
-    CT_CUDA(cudaMalloc(&d_htsums_, sizeof(double) * (size_t)hvp_cap_ * 3 * nacc));
+    alloc(d_hdirs_, sizeof(double) * (size_t)nP * nP);
+    alloc(d_hconsts_, sizeof(double) * 2 * (size_t)hvp_cap_ * std::max(1, gen_.nconst));
+    alloc(d_hrows_, sizeof(double) * (size_t)hvp_cap_ * hlay_.grid * nacc);
+    alloc(d_hvsums_, sizeof(double) * (size_t)sumsSize());
+    alloc(d_htsums_, sizeof(double) * (size_t)hvp_cap_ * 3 * nacc);
     cudaStream_t st;
     CT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     ct_identity_kernel<<<std::max(1, std::min(1024, (nP * nP + 255) / 256)), 256, 0, st>>>(d_hdirs_, nP);
@@ -2084,9 +2126,9 @@ void Engine::loadTruth()
     if (s.n > 0) {
         size_t bytes = sizeof(double) * (size_t)s.n * nfin * 4;
         double* tmp = nullptr;
-        CT_CUDA(cudaMallocAsync((void**)&tmp, bytes, init_stream_));
+        CT_CUDA(cudaMallocFromPoolAsync((void**)&tmp, bytes, enginePool(opt_.device), init_stream_));
         CT_CUDA(cudaMemcpyAsync(tmp, s.p4.data(), bytes, cudaMemcpyHostToDevice, init_stream_));
-        CT_CUDA(cudaMallocAsync((void**)&d.p4, bytes, init_stream_));
+        CT_CUDA(cudaMallocFromPoolAsync((void**)&d.p4, bytes, enginePool(opt_.device), init_stream_));
         ag_transpose_kernel<<<(unsigned)((s.n + 255) / 256), 256, 0, init_stream_>>>(tmp, d.p4, s.n, nfin);
         CT_CUDA(cudaGetLastError());
         CT_CUDA(cudaFreeAsync(tmp, init_stream_));

@@ -219,6 +219,20 @@ private:
 
     cudaStream_t init_stream_ = nullptr;  // initialisation only
 
+    // Device memory of the handle: stream-ordered allocations from a
+    // per-device pool of this library that keeps freed memory for the next
+    // handle (no device-wide synchronisation, no page mapping on reuse).
+    // Frees do not wait for work on other streams: the caller's work on a
+    // handle must be complete before it is destroyed.
+    cudaStream_t mem_stream_ = nullptr;
+    void* devAlloc(size_t bytes);
+    void devFree(void* p);
+    template <typename T>
+    void alloc(T*& p, size_t bytes)
+    {
+        p = static_cast<T*>(devAlloc(bytes));
+    }
+
     // fused-kernel timing ring
     std::vector<cudaEvent_t> ev_begin_, ev_end_;
     long long ev_count_ = 0;

@@ -114,7 +114,6 @@ class Server:
         self.budget = int(budget_bytes)
         base = workdir or ("/dev/shm" if os.path.isdir("/dev/shm") else None)
         self.workdir = tempfile.mkdtemp(prefix="ctpwa_serve_", dir=base)
-        self._bpe = {}
         self._lock = threading.Lock()
         self._capture_lock = threading.Lock()
         self._in_use = 0
@@ -123,8 +122,11 @@ class Server:
         shutil.rmtree(self.workdir, ignore_errors=True)
 
     # ----------------------------------------------------------- admission
+    # resident device bytes per event of each model, shared by all servers of the process
+    _bpe: dict = {}
+
     def bytes_per_event(self, model: str) -> float:
-        """Resident device bytes per event of a model, measured once on a prototype."""
+        """Resident device bytes per event of a model, measured once per process on a prototype."""
         if model not in self._bpe:
             from . import analysis
 
@@ -364,6 +366,10 @@ def main(argv=None):
     a = ap.parse_args(argv)
     srv = Server(device=a.device, slots=a.slots, graphs=not a.no_graphs)
     try:
+        # untimed small jobs first: one-time process costs (library and kernel
+        # loading, the per-model memory figure) are not stream latency
+        srv.run([JobSpec(job_id=-1 - i, model=m, n_data=5_000, n_phsp=50_000, seed=90 + i, max_evals=5,
+                         precision=a.precision) for i, m in enumerate(("pipi_rho", "pipi_3rho"))], realtime=False)
         jobs = poisson_stream(a.rate, a.jobs, nd_range=(a.nd_min, a.nd_max), precision=a.precision)
         t = time.perf_counter()
         res = srv.run(jobs)

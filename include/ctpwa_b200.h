@@ -61,7 +61,10 @@ ctpwa_handle* ctpwa_create_from_device(const char* config_path, int device, cons
                                        const long long* n, const double* const* w, int* status, char* err,
                                        size_t errlen);
 
-/* Releases device memory of the handle (the reference never frees; src/Analysis.cu:1284-1290). */
+/* Releases device memory of the handle (the reference never frees;
+ * src/Analysis.cu:1284-1290) into this library's per-device memory pool,
+ * where later handles reuse it. It does not wait for work on the caller's
+ * streams: work queued on the handle must be complete. */
 void ctpwa_destroy(ctpwa_handle* h);
 
 /* Replaces: analysis::getNVector — src/Analysis.cu:1311-1315 (vspace fit mode). */
