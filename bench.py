@@ -313,12 +313,13 @@ def toy_fit(args, device):
     from ctpwa_b200 import serving
 
     out = {}
-    # one untimed small job per model and precision first: process-level
-    # one-time costs (library and kernel loading, allocator growth, first
-    # graph capture) are not part of a serving stream's latency
+    # one untimed job per model and precision first, at the stream's largest
+    # size: process-level one-time costs (library and kernel loading, growth
+    # of the memory pools to the largest job, first graph capture) are not
+    # part of a serving stream's latency
     warm = serving.Server(device=device, slots=2)
     try:
-        warm.run([serving.JobSpec(job_id=i, model=m, n_data=5_000, n_phsp=50_000, seed=90 + i, max_evals=5,
+        warm.run([serving.JobSpec(job_id=i, model=m, n_data=200_000, n_phsp=2_000_000, seed=90 + i, max_evals=5,
                                   precision=p)
                   for i, (m, p) in enumerate([(m, p) for m in ("pipi_rho", "pipi_3rho") for p in ("mixed", "fp64")])],
                  realtime=False)

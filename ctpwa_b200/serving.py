@@ -366,9 +366,10 @@ def main(argv=None):
     a = ap.parse_args(argv)
     srv = Server(device=a.device, slots=a.slots, graphs=not a.no_graphs)
     try:
-        # untimed small jobs first: one-time process costs (library and kernel
-        # loading, the per-model memory figure) are not stream latency
-        srv.run([JobSpec(job_id=-1 - i, model=m, n_data=5_000, n_phsp=50_000, seed=90 + i, max_evals=5,
+        # untimed jobs of the largest size first: one-time process costs
+        # (library and kernel loading, the per-model memory figure, growth of
+        # the memory pools) are not stream latency
+        srv.run([JobSpec(job_id=-1 - i, model=m, n_data=a.nd_max, n_phsp=10 * a.nd_max, seed=90 + i, max_evals=5,
                          precision=a.precision) for i, m in enumerate(("pipi_rho", "pipi_3rho"))], realtime=False)
         jobs = poisson_stream(a.rate, a.jobs, nd_range=(a.nd_min, a.nd_max), precision=a.precision)
         t = time.perf_counter()
