@@ -117,6 +117,12 @@ class Server:
         self._lock = threading.Lock()
         self._capture_lock = threading.Lock()
         self._in_use = 0
+        # one CUDA stream per slot, reused by the jobs that run in it: the
+        # tensor allocator caches memory per stream, so a new stream per job
+        # would allocate (and later release) fresh device memory every time
+        self._streams: "queue.Queue" = queue.Queue()
+        for _ in range(self.slots):
+            self._streams.put(torch.cuda.Stream(device=self.device))
 
     def close(self):
         shutil.rmtree(self.workdir, ignore_errors=True)
@@ -167,14 +173,15 @@ class Server:
         res = JobResult(job_id=spec.job_id, model=spec.model, n_data=spec.n_data, n_phsp=spec.n_phsp,
                         precision=spec.precision, arrival=spec.arrival, admitted=time.perf_counter() - t0)
         d = os.path.join(self.workdir, f"job{spec.job_id}")
-        stream = torch.cuda.Stream(device=self.device)
+        stream = self._streams.get()
         try:
             with torch.cuda.device(self.device), torch.cuda.stream(stream):
                 # toy-MC events generated and kept on the device, the job's
                 # handle built from them (no file round trip)
                 t1 = time.perf_counter()
+                gen_ms = {}
                 cfg, phsp, data = workloads.make_device(spec.model, d, spec.n_phsp, spec.n_data, seed=spec.seed,
-                                                        device=self.device)
+                                                        device=self.device, timing=gen_ms)
                 t2 = time.perf_counter()
                 ana = analysis.from_device(cfg, phsp, data, device=self.device, precision=spec.precision)
                 del phsp, data
@@ -196,6 +203,7 @@ class Server:
                 t5 = time.perf_counter()
                 res.phase_ms = {"generate": 1e3 * (t2 - t1), "handle": 1e3 * (t3 - t2), "fit": 1e3 * (t4 - t3),
                                 "hessian": 1e3 * (t5 - t4)}
+                res.phase_ms.update({"generate." + k: v for k, v in gen_ms.items()})
                 res.params = p.cpu().numpy()
                 res.hessian = H.cpu().numpy()
                 res.nll = nll
@@ -205,6 +213,8 @@ class Server:
         except Exception as e:  # a failing job is reported, the server keeps going
             res.error = f"{type(e).__name__}: {e}"
         finally:
+            stream.synchronize()
+            self._streams.put(stream)
             shutil.rmtree(d, ignore_errors=True)
         res.finished = time.perf_counter() - t0
         return res
@@ -345,7 +355,7 @@ def summary(results: List[JobResult], wall_s: float) -> dict:
         "service_ms_p50": percentile(service, 50),
         "service_ms_p99": percentile(service, 99),
         "phase_ms_p50": {k: percentile([r.phase_ms[k] for r in ok if k in r.phase_ms], 50)
-                         for k in ("generate", "handle", "fit", "hessian")},
+                         for k in sorted({k for r in ok for k in r.phase_ms})},
         "errors": [r.error for r in results if r.error][:5],
     }
 
@@ -363,6 +373,7 @@ def main(argv=None):
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--seed", type=int, default=17)
     a = ap.parse_args(argv)
     srv = Server(device=a.device, slots=a.slots, graphs=not a.no_graphs)
     try:
@@ -371,7 +382,7 @@ def main(argv=None):
         # the memory pools) are not stream latency
         srv.run([JobSpec(job_id=-1 - i, model=m, n_data=a.nd_max, n_phsp=10 * a.nd_max, seed=90 + i, max_evals=5,
                          precision=a.precision) for i, m in enumerate(("pipi_rho", "pipi_3rho"))], realtime=False)
-        jobs = poisson_stream(a.rate, a.jobs, nd_range=(a.nd_min, a.nd_max), precision=a.precision)
+        jobs = poisson_stream(a.rate, a.jobs, nd_range=(a.nd_min, a.nd_max), precision=a.precision, seed=a.seed)
         t = time.perf_counter()
         res = srv.run(jobs)
         out = summary(res, time.perf_counter() - t)

@@ -283,17 +283,29 @@ def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, inten
     return sel[:n_data]
 
 
-def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2):
+def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2, timing=None):
     """Toy-MC samples of workload `name` generated and kept on the GPU:
     phase space from the seeded GPU generator, data by accept-reject of GPU
     candidates against the model's intensity at the true parameters (the
     candidates' intensities from an in-memory analysis, the draw on the
     device). Writes only config.yml (its Data entries name no files that are
     read) and returns (config_path, phsp, data) with float64 CUDA tensors
-    [n, 3, 4] for ``analysis.from_device``."""
+    [n, 3, 4] for ``analysis.from_device``. `timing` (a dict) receives the
+    host time of each step in ms."""
+    import time
+
     import torch
 
     from . import analysis, describe
+
+    clock = [time.perf_counter()]
+
+    def lap(key):
+        if timing is not None:
+            torch.cuda.current_stream(device).synchronize()
+            t = time.perf_counter()
+            timing[key] = timing.get(key, 0.0) + 1e3 * (t - clock[0])
+            clock[0] = t
 
     out = Path(outdir)
     out.mkdir(parents=True, exist_ok=True)
@@ -304,17 +316,21 @@ def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2):
     phsp = toymc.phase_space_gpu(M_JPSI, masses, n_phsp, 1001 + seed, device=dev, as_tensor=True)
     tiny = toymc.phase_space_gpu(M_JPSI, masses, 1000, 7001 + seed, device=dev, as_tensor=True)
     p = torch.tensor(params_for(describe(str(cfg))), dtype=torch.float64, device=dev)
+    lap("phsp")
     gen = torch.Generator(device=dev)
     gen.manual_seed(6001 + seed)
     chunks, have, batch = [], 0, 0
     while have < n_data:
         ncand = int((n_data - have) * 12) + 10_000
         cand = toymc.phase_space_gpu(M_JPSI, masses, ncand, 5001 + seed + 7919 * batch, device=dev, as_tensor=True)
+        lap("candidates")
         ana = analysis.from_device(str(cfg), tiny, cand, device=device)
+        lap("cand_handle")
         I = ana.getIntensity(p, kind=1)
         del ana
         u = torch.rand(ncand, generator=gen, dtype=torch.float64, device=dev) * (safety * I.max())
         sel = cand[u < I]
+        lap("select")
         chunks.append(sel)
         have += sel.shape[0]
         batch += 1
