@@ -86,6 +86,14 @@ __device__ __forceinline__ CtDual atan2(CtDual y, CtDual x)
 }
 __device__ __forceinline__ CtDual atan2(CtDual y, double x) { return atan2(y, CtDual(x)); }
 __device__ __forceinline__ CtDual atan2(double y, CtDual x) { return atan2(CtDual(y), x); }
+template <typename A, typename B>
+struct CtSame {
+    static constexpr bool value = false;
+};
+template <typename A>
+struct CtSame<A, A> {
+    static constexpr bool value = true;
+};
 __device__ __forceinline__ double ct_value(double x) { return x; }
 __device__ __forceinline__ double ct_value(CtDual x) { return x.v; }
 
@@ -193,109 +201,102 @@ extern "C" __global__ void __launch_bounds__(CT_HVP_BLOCK) ct_hvp_f64(CtHvpArgs 
 
     const long long n = S.n, ld = S.ld;
     const long long stride = (long long)S.cta_count * CT_HVP_BLOCK;
-    for (long long e = (long long)(cta - S.cta_begin) * CT_HVP_BLOCK + threadIdx.x; e < n; e += stride) {
-        double ev[M_NEV > 0 ? M_NEV : 1];
+    // FT: type of the lineshapes and their derivatives, CtDual when the
+    // direction moves a resonance parameter, plain FP64 when it moves only
+    // couplings (the lineshapes do not move: no tangent arithmetic on them)
+    auto run = [&](auto tag) {
+        using FT = decltype(tag);
+        for (long long e = (long long)(cta - S.cta_begin) * CT_HVP_BLOCK + threadIdx.x; e < n; e += stride) {
+            double ev[M_NEV > 0 ? M_NEV : 1];
 #pragma unroll
-        for (int k = 0; k < M_NEV; ++k) ev[k] = __ldg(S.ev + (long long)k * ld + e);
-        CtDual Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
-        if (thdir) {
-            model_columns_dual(ev, sC, Fr, Fi, dFr, dFi);
-        } else {
-            // couplings-only direction: the lineshapes do not move
-            double fr[M_NTERM], fi[M_NTERM], dfr[M_NDER > 0 ? M_NDER : 1], dfi[M_NDER > 0 ? M_NDER : 1];
-            model_columns(ev, sCv, fr, fi, dfr, dfi);
+            for (int k = 0; k < M_NEV; ++k) ev[k] = __ldg(S.ev + (long long)k * ld + e);
+            FT Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
+            if constexpr (CtSame<FT, CtDual>::value) model_columns_dual(ev, sC, Fr, Fi, dFr, dFi);
+            else model_columns(ev, sCv, Fr, Fi, dFr, dFi);
+            double2 sl[M_NPLANE * M_NPOL];
+#pragma unroll
+            for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = __ldg(S.slamp + (long long)c * ld + e);
+            CtDual cr[M_NTERM], ci[M_NTERM];
 #pragma unroll
             for (int t = 0; t < M_NTERM; ++t) {
-                Fr[t] = CtDual(fr[t]);
-                Fi[t] = CtDual(fi[t]);
+                const int a = term_col(t);
+                cr[t] = vr[a] * Fr[t] - vi[a] * Fi[t];
+                ci[t] = vr[a] * Fi[t] + vi[a] * Fr[t];
+            }
+            CtDual Sr[M_NPOL], Si[M_NPOL];
+            CtDual f(0.0);
+#pragma unroll
+            for (int p = 0; p < M_NPOL; ++p) {
+                CtDual sr(0.0), sim(0.0);
+#pragma unroll
+                for (int t = 0; t < M_NTERM; ++t) {
+                    const double2 x = sl[term_plane(t) * M_NPOL + p];
+                    sr += cr[t] * x.x - ci[t] * x.y;
+                    sim += cr[t] * x.y + ci[t] * x.x;
+                }
+                Sr[p] = sr;
+                Si[p] = sim;
+                f += sr * sr + sim * sim;
+            }
+            CtDual ur[M_NPOL], ui[M_NPOL];
+            double gscale, tscale;
+            const double we = S.w ? __ldg(S.w + e) : 1.0;
+            if (kind == 0) {
+                acc[1 * CT_HVP_BLOCK] += f.t;
+#pragma unroll
+                for (int p = 0; p < M_NPOL; ++p) {
+                    ur[p] = Sr[p];
+                    ui[p] = Si[p];
+                }
+                gscale = we;
+                tscale = 2.0;
+            } else {
+                if (f.v == 0.0) continue;  // constant -w log(1e-10): no derivative
+                acc[0] += -we * f.t / f.v;
+                const CtDual inv = we / f;
+#pragma unroll
+                for (int p = 0; p < M_NPOL; ++p) {
+                    ur[p] = ct_clamp(Sr[p] * inv, 1e10);
+                    ui[p] = ct_clamp(Si[p] * inv, 1e10);
+                }
+                gscale = -1.0;
+                tscale = -2.0;
+            }
+            CtDual Tr[M_NPLANE], Ti[M_NPLANE];
+#pragma unroll
+            for (int c = 0; c < M_NPLANE; ++c) {
+                CtDual tr(0.0), ti(0.0);
+#pragma unroll
+                for (int p = 0; p < M_NPOL; ++p) {
+                    const double2 x = sl[c * M_NPOL + p];
+                    tr += x.x * ur[p] + x.y * ui[p];
+                    ti += x.x * ui[p] - x.y * ur[p];
+                }
+                Tr[c] = tr;
+                Ti[c] = ti;
+            }
+#pragma unroll
+            for (int t = 0; t < M_NTERM; ++t) {
+                const int a = term_col(t), c = term_plane(t);
+                acc[(2 + 2 * a) * CT_HVP_BLOCK] += gscale * (Fr[t] * Tr[c] + Fi[t] * Ti[c]).t;
+                acc[(3 + 2 * a) * CT_HVP_BLOCK] += gscale * (Fr[t] * Ti[c] - Fi[t] * Tr[c]).t;
+            }
+            CtDual Wr[M_NTERM], Wi[M_NTERM];
+#pragma unroll
+            for (int t = 0; t < M_NTERM; ++t) {
+                const int a = term_col(t), c = term_plane(t);
+                Wr[t] = tscale * (vr[a] * Tr[c] + vi[a] * Ti[c]);
+                Wi[t] = tscale * (vi[a] * Tr[c] - vr[a] * Ti[c]);
             }
 #pragma unroll
             for (int k = 0; k < M_NDER; ++k) {
-                dFr[k] = CtDual(dfr[k]);
-                dFi[k] = CtDual(dfi[k]);
+                const int t = der_term(k);
+                acc[(2 + 2 * M_NA + der_th(k)) * CT_HVP_BLOCK] += (dFr[k] * Wr[t] - dFi[k] * Wi[t]).t;
             }
         }
-        double2 sl[M_NPLANE * M_NPOL];
-#pragma unroll
-        for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = __ldg(S.slamp + (long long)c * ld + e);
-        CtDual cr[M_NTERM], ci[M_NTERM];
-#pragma unroll
-        for (int t = 0; t < M_NTERM; ++t) {
-            const int a = term_col(t);
-            cr[t] = vr[a] * Fr[t] - vi[a] * Fi[t];
-            ci[t] = vr[a] * Fi[t] + vi[a] * Fr[t];
-        }
-        CtDual Sr[M_NPOL], Si[M_NPOL];
-        CtDual f(0.0);
-#pragma unroll
-        for (int p = 0; p < M_NPOL; ++p) {
-            CtDual sr(0.0), sim(0.0);
-#pragma unroll
-            for (int t = 0; t < M_NTERM; ++t) {
-                const double2 x = sl[term_plane(t) * M_NPOL + p];
-                sr += cr[t] * x.x - ci[t] * x.y;
-                sim += cr[t] * x.y + ci[t] * x.x;
-            }
-            Sr[p] = sr;
-            Si[p] = sim;
-            f += sr * sr + sim * sim;
-        }
-        CtDual ur[M_NPOL], ui[M_NPOL];
-        double gscale, tscale;
-        const double we = S.w ? __ldg(S.w + e) : 1.0;
-        if (kind == 0) {
-            acc[1 * CT_HVP_BLOCK] += f.t;
-#pragma unroll
-            for (int p = 0; p < M_NPOL; ++p) {
-                ur[p] = Sr[p];
-                ui[p] = Si[p];
-            }
-            gscale = we;
-            tscale = 2.0;
-        } else {
-            if (f.v == 0.0) continue;  // constant -w log(1e-10): no derivative
-            acc[0] += -we * f.t / f.v;
-            const CtDual inv = we / f;
-#pragma unroll
-            for (int p = 0; p < M_NPOL; ++p) {
-                ur[p] = ct_clamp(Sr[p] * inv, 1e10);
-                ui[p] = ct_clamp(Si[p] * inv, 1e10);
-            }
-            gscale = -1.0;
-            tscale = -2.0;
-        }
-        CtDual Tr[M_NPLANE], Ti[M_NPLANE];
-#pragma unroll
-        for (int c = 0; c < M_NPLANE; ++c) {
-            CtDual tr(0.0), ti(0.0);
-#pragma unroll
-            for (int p = 0; p < M_NPOL; ++p) {
-                const double2 x = sl[c * M_NPOL + p];
-                tr += x.x * ur[p] + x.y * ui[p];
-                ti += x.x * ui[p] - x.y * ur[p];
-            }
-            Tr[c] = tr;
-            Ti[c] = ti;
-        }
-#pragma unroll
-        for (int t = 0; t < M_NTERM; ++t) {
-            const int a = term_col(t), c = term_plane(t);
-            acc[(2 + 2 * a) * CT_HVP_BLOCK] += gscale * (Fr[t] * Tr[c] + Fi[t] * Ti[c]).t;
-            acc[(3 + 2 * a) * CT_HVP_BLOCK] += gscale * (Fr[t] * Ti[c] - Fi[t] * Tr[c]).t;
-        }
-        CtDual Wr[M_NTERM], Wi[M_NTERM];
-#pragma unroll
-        for (int t = 0; t < M_NTERM; ++t) {
-            const int a = term_col(t), c = term_plane(t);
-            Wr[t] = tscale * (vr[a] * Tr[c] + vi[a] * Ti[c]);
-            Wi[t] = tscale * (vi[a] * Tr[c] - vr[a] * Ti[c]);
-        }
-#pragma unroll
-        for (int k = 0; k < M_NDER; ++k) {
-            const int t = der_term(k);
-            acc[(2 + 2 * M_NA + der_th(k)) * CT_HVP_BLOCK] += (dFr[k] * Wr[t] - dFi[k] * Wi[t]).t;
-        }
-    }
+    };
+    if (thdir) run(CtDual(0.0));
+    else run(0.0);
     __syncthreads();
     // CTA sums, one warp per column in a fixed order
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
