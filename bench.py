@@ -317,7 +317,7 @@ def toy_fit(args, device):
     # size: process-level one-time costs (library and kernel loading, growth
     # of the memory pools to the largest job, first graph capture) are not
     # part of a serving stream's latency
-    warm = serving.Server(device=device, slots=2)
+    warm = serving.Server(device=device, slots=4)
     try:
         warm.run([serving.JobSpec(job_id=i, model=m, n_data=200_000, n_phsp=2_000_000, seed=90 + i, max_evals=5,
                                   precision=p)

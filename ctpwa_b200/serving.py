@@ -117,12 +117,16 @@ class Server:
         self._lock = threading.Lock()
         self._capture_lock = threading.Lock()
         self._in_use = 0
-        # one CUDA stream per slot, reused by the jobs that run in it: the
-        # tensor allocator caches memory per stream, so a new stream per job
-        # would allocate (and later release) fresh device memory every time
+        # one CUDA stream per slot, reused by the jobs that run in it and by
+        # later servers of the process: the tensor allocator caches memory
+        # per stream, so a new stream per job (or per server) would allocate
+        # fresh device memory
+        pool = Server._stream_pool.setdefault(self.device, [])
+        while len(pool) < self.slots:
+            pool.append(torch.cuda.Stream(device=self.device))
         self._streams: "queue.Queue" = queue.Queue()
-        for _ in range(self.slots):
-            self._streams.put(torch.cuda.Stream(device=self.device))
+        for st in pool[:self.slots]:
+            self._streams.put(st)
 
     def close(self):
         shutil.rmtree(self.workdir, ignore_errors=True)
@@ -130,6 +134,8 @@ class Server:
     # ----------------------------------------------------------- admission
     # resident device bytes per event of each model, shared by all servers of the process
     _bpe: dict = {}
+    # the process's job streams per device
+    _stream_pool: dict = {}
 
     def bytes_per_event(self, model: str) -> float:
         """Resident device bytes per event of a model, measured once per process on a prototype."""
@@ -380,8 +386,8 @@ def main(argv=None):
         # untimed jobs of the largest size first: one-time process costs
         # (library and kernel loading, the per-model memory figure, growth of
         # the memory pools) are not stream latency
-        srv.run([JobSpec(job_id=-1 - i, model=m, n_data=a.nd_max, n_phsp=10 * a.nd_max, seed=90 + i, max_evals=5,
-                         precision=a.precision) for i, m in enumerate(("pipi_rho", "pipi_3rho"))], realtime=False)
+        srv.run([JobSpec(job_id=-1 - i, model=("pipi_rho", "pipi_3rho")[i % 2], n_data=a.nd_max, n_phsp=10 * a.nd_max,
+                         seed=90 + i, max_evals=5, precision=a.precision) for i in range(a.slots)], realtime=False)
         jobs = poisson_stream(a.rate, a.jobs, nd_range=(a.nd_min, a.nd_max), precision=a.precision, seed=a.seed)
         t = time.perf_counter()
         res = srv.run(jobs)
