@@ -182,6 +182,8 @@ class analysis:
                 continue
             if t.dtype != torch.float64 or not t.is_cuda or t.dim() != 3 or t.shape[2] != 4:
                 raise RuntimeError("in-memory samples must be float64 CUDA tensors [n, n_final, 4]")
+            if t.device.index != self._device:
+                raise RuntimeError(f"in-memory samples must be on cuda:{self._device}")
             t = t.contiguous()
             keep.append(t)
             p4[k] = t.data_ptr()

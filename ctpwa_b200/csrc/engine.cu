@@ -890,6 +890,17 @@ void Engine::loadSamples()
         for (int k = 0; k < 3; ++k) {
             const long long n = opt_.dev_n[k];
             if (n < 0 || (n > 0 && !opt_.dev_p4[k])) throw std::runtime_error("in-memory sample: bad event array");
+            // the arrays must be device memory of this handle's GPU
+            for (const void* ptr : {(const void*)opt_.dev_p4[k], (const void*)opt_.dev_w[k]}) {
+                if (!ptr || n == 0) continue;
+                cudaPointerAttributes at;
+                if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+                    at.device != opt_.device) {
+                    cudaGetLastError();
+                    throw std::runtime_error(std::string("in-memory ") + kinds[k] +
+                                             " sample: not device memory of the handle's GPU");
+                }
+            }
             if (k < 2 && n == 0) throw std::runtime_error(std::string("in-memory samples need a ") + kinds[k] + " sample");
             DeviceSample& d = samples_[k];
             d.n = n;
