@@ -836,6 +836,49 @@ std::string Gen::emit()
     auto mixedDep = [&](int x) { return (N[x].dep & dag::DEP_EVENT) && (N[x].dep & dag::DEP_THETA); };
     // frontier slots: FP64 table (all), mixed tables (FP32 / FP64 values)
     std::vector<int> fs64(N.size(), -1), fsF(N.size(), -1), fsD(N.size(), -1);
+    std::vector<char> shifted(N.size(), 0), shiftUser(N.size(), 0);
+    std::vector<double> shiftR(N.size(), 0.0);
+    // value of a parameter-only node at the initial parameters
+    std::vector<double> tval(N.size(), std::nan(""));
+    std::vector<char> tdone(N.size(), 0);
+    std::function<double(int)> thetaValue = [&](int x) -> double {
+        if (tdone[x]) return tval[x];
+        const auto& nd = N[x];
+        auto v = [&](int k) { return k >= 0 ? thetaValue(k) : 0.0; };
+        double r = std::nan("");
+        switch (nd.op) {
+        case dag::Const: r = nd.v; break;
+        case dag::Theta: r = nd.idx < (int)m.slots.size() ? m.slots[nd.idx].init : std::nan(""); break;
+        case dag::Add: r = v(nd.a) + v(nd.b); break;
+        case dag::Sub: r = v(nd.a) - v(nd.b); break;
+        case dag::Mul: r = v(nd.a) * v(nd.b); break;
+        case dag::Recip: r = 1.0 / v(nd.a); break;
+        case dag::Neg: r = -v(nd.a); break;
+        case dag::Sqrt: r = std::sqrt(v(nd.a)); break;
+        case dag::Log: r = std::log(v(nd.a)); break;
+        case dag::Exp: r = std::exp(v(nd.a)); break;
+        case dag::Sin: r = std::sin(v(nd.a)); break;
+        case dag::Cos: r = std::cos(v(nd.a)); break;
+        case dag::Atan2: r = std::atan2(v(nd.a), v(nd.b)); break;
+        case dag::Sel: {
+            const double c = v(nd.c);
+            bool t = false;
+            switch ((dag::Cmp)nd.cmp) {
+            case dag::GE0: t = c >= 0.0; break;
+            case dag::GT0: t = c > 0.0; break;
+            case dag::LE0: t = c <= 0.0; break;
+            case dag::LT0: t = c < 0.0; break;
+            case dag::EQ0: t = c == 0.0; break;
+            }
+            r = t ? v(nd.a) : v(nd.b);
+            break;
+        }
+        default: break;  // channel factors: not needed for a reference value
+        }
+        tdone[x] = 1;
+        tval[x] = r;
+        return r;
+    };
     {
         std::vector<char> front(N.size(), 0);
         for (size_t x = 0; x < N.size(); ++x) {
@@ -850,10 +893,61 @@ std::string Gen::emit()
                 for (int r : {d.second.first, d.second.second})
                     if (r >= 0 && evOnly(r)) front[r] = 1;
         }
+        // Shifted FP32 storage for the mixed form: a cancellation-prone FP64
+        // event value X (such as m^2) whose every use is T - X, X - T or
+        // T + X with a parameter-only T, and whose results are used in FP32
+        // only, is stored as the FP32 value X - R (R: T at the initial
+        // parameters); the per-call code forms (T - R) - X' in FP32. The
+        // difference keeps the relative precision of an FP32 rounding of
+        // T - X (|X - R| stays of the order of |T - X| while the fit moves T
+        // near its start), as the FP64 subtraction rounded to FP32 did, from
+        // 4 bytes instead of 8.
+        std::vector<std::vector<int>> users(N.size());
+        for (size_t y = 0; y < N.size(); ++y) {
+            if (!live[y] || !(N[y].dep & dag::DEP_EVENT)) continue;
+            for (int k : {N[y].a, N[y].b, N[y].c})
+                if (k >= 0) users[k].push_back((int)y);
+        }
+        std::vector<char> isRoot(N.size(), 0);
+        for (const auto& c : cols) {
+            for (int r : {c.re, c.im})
+                if (r >= 0) isRoot[r] = 1;
+            for (const auto& d : c.der)
+                for (int r : {d.second.first, d.second.second})
+                    if (r >= 0) isRoot[r] = 1;
+        }
+        for (size_t x = 0; x < N.size(); ++x) {
+            if (!front[x] || !dbl[x] || N[x].op == dag::Kin || isRoot[x] || users[x].empty()) continue;
+            bool ok = true;
+            int tfirst = -1;
+            for (int y : users[x]) {
+                const auto& yn = N[y];
+                const int other = yn.a == (int)x ? yn.b : yn.a;
+                if (!mixedDep(y) || (yn.op != dag::Sub && yn.op != dag::Add) || yn.a == yn.b || other < 0 ||
+                    N[other].dep != dag::DEP_THETA || isRoot[y]) {
+                    ok = false;
+                    break;
+                }
+                for (int z : users[y])
+                    if (dbl[z] || N[z].op == dag::RhoRe || N[z].op == dag::RhoIm) ok = false;
+                for (const auto& t : tab_uses)
+                    if (t.mnode == y) ok = false;
+                if (tfirst < 0) tfirst = other;
+            }
+            if (!ok || tfirst < 0) continue;
+            const double R = thetaValue(tfirst);
+            if (!std::isfinite(R)) continue;
+            shiftR[x] = R;
+            shifted[x] = 1;
+            for (int y : users[x]) {
+                shiftUser[y] = 1;
+                dbl[y] = 0;
+            }
+        }
         for (size_t x = 0; x < N.size(); ++x) {
             if (!front[x]) continue;
             fs64[x] = out.nev64++;
-            if (!dbl[x] && N[x].op != dag::Kin) fsF[x] = out.nevf++;
+            if ((!dbl[x] && N[x].op != dag::Kin) || shifted[x]) fsF[x] = out.nevf++;
             else fsD[x] = out.nevd++;
         }
     }
@@ -920,6 +1014,20 @@ std::string Gen::emit()
     // definition of event node x
     auto nodeLine = [&](size_t x, bool f32, const RefFn& ref) -> std::string {
         const auto& nd = N[x];
+        if (f32 && shiftUser[x]) {
+            // T - X, X - T or T + X from the shifted FP32 value X' = X - R
+            const bool xa = shifted[nd.a] != 0;
+            const int xs = xa ? nd.a : nd.b, t = xa ? nd.b : nd.a;
+            const std::string T = ref(t, false), Xs = "evf[" + std::to_string(fsF[xs]) + "]",
+                              R = num(shiftR[xs]);
+            // the parameter-only part enters as hi + lo (a single FP32
+            // rounding of it would shift every event alike)
+            std::string rhs;
+            if (nd.op == dag::Add) rhs = "ct_split_add(" + T + " + " + R + ", " + Xs + ")";
+            else if (xa) rhs = "-ct_split_sub(" + T + " - " + R + ", " + Xs + ")";  // X - T
+            else rhs = "ct_split_sub(" + T + " - " + R + ", " + Xs + ")";         // T - X
+            return "  const float e" + std::to_string(x) + " = " + rhs + ";\n";
+        }
         bool isF = f32 && !dbl[x];
         std::string A, B, Cc;
         if (nd.op == dag::RhoRe || nd.op == dag::RhoIm) {
@@ -996,6 +1104,8 @@ std::string Gen::emit()
         for (size_t x = 0; x < N.size(); ++x) {
             if (fs64[x] < 0) continue;
             if (!f32) evs << "  o[" << fs64[x] << "] = " << ref((int)x, false) << ";\n";
+            else if (shifted[x]) evs << "  of[" << fsF[x] << "] = (float)(" << ref((int)x, false) << " - " << num(shiftR[x])
+                                     << ");\n";
             else if (fsF[x] >= 0) evs << "  of[" << fsF[x] << "] = " << ref((int)x, true) << ";\n";
             else evs << "  od[" << fsD[x] << "] = " << ref((int)x, false) << ";\n";
         }

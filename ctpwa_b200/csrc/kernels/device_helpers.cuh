@@ -126,6 +126,19 @@ __device__ __forceinline__ float ct_sqrtf(float x)
     return (x == 0.0f || x == __int_as_float(0x7f800000)) ? x : y1;
 }
 
+// t - x and t + x for an FP64 parameter-only t and an FP32 event value x, with
+// t entering as hi + lo (the FP32 forms of the mixed lineshapes)
+__device__ __forceinline__ float ct_split_sub(double t, float x)
+{
+    const float hi = (float)t, lo = (float)(t - (double)hi);
+    return (hi - x) + lo;
+}
+__device__ __forceinline__ float ct_split_add(double t, float x)
+{
+    const float hi = (float)t, lo = (float)(t - (double)hi);
+    return (hi + x) + lo;
+}
+
 // ---- asynchronous bulk copies global -> shared with mbarrier completion ----
 // (cp.async.bulk: the copy engine moves whole contiguous table rows into
 // shared memory while the CTA computes on the previous tile)
