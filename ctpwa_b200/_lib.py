@@ -59,6 +59,8 @@ SIGNATURES = {
     "ctpwa_n_events": (ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int]),
     "ctpwa_model_json": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "ctpwa_device_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "ctpwa_phase_space": (ctypes.c_int, [ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_longlong,
+                                         ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_event_cache_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "ctpwa_launch_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "ctpwa_event_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),

@@ -22,7 +22,7 @@ HOSTCXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SRCS = ["yaml_lite.cpp", "config.cpp", "model.cpp", "dataio.cpp", "exprdag.cpp", "codegen.cpp", "capi.cpp"]
-CUDA_SRCS = ["engine.cu"]
+CUDA_SRCS = ["engine.cu", "toymc.cu"]
 
 
 def _newer(target: Path, deps) -> bool:

@@ -368,6 +368,19 @@ int ctpwa_event_layout(const ctpwa_handle* h, int* out4)
     return CTPWA_OK;
 }
 
+int ctpwa_phase_space(double M, const double* masses3, long long n, unsigned long long seed, double* d_out,
+                      void* stream)
+{
+    if (!masses3 || (n > 0 && !d_out)) return setErr(nullptr, CTPWA_ERR_ARG, "null argument");
+    try {
+        ctpwa::phaseSpace(M, masses3, n, seed, d_out, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        const std::string m = e.what();
+        return setErr(nullptr, m.rfind("CUDA", 0) == 0 ? CTPWA_ERR_CUDA : CTPWA_ERR_ARG, m);
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_event_cache_layout(const ctpwa_handle* h, int* out3)
 {
     if (!h || !out3) return CTPWA_ERR_ARG;

@@ -60,6 +60,12 @@ struct EngineOptions {
 // without touching a GPU; returns seconds spent.
 double precompileConfig(const std::string& config_path);
 
+// Seeded three-body phase space for a parent of mass M at rest on the current
+// device: d_out [n][3][4] (E, px, py, pz), event i a function of (seed, i)
+// only (csrc/toymc.cu).
+void phaseSpace(double M, const double* masses, long long n, unsigned long long seed, double* d_out,
+                cudaStream_t stream);
+
 class Engine {
 public:
     Engine(const std::string& config_path, const EngineOptions& opt);

@@ -140,6 +140,30 @@ def phase_space_gpu(M, masses, n, seed, device="cuda", as_tensor=False):
     return out if as_tensor else out.cpu().numpy()
 
 
+def phase_space_device(M, masses, n, seed, device=0):
+    """Uniform three-body phase space generated by the library's CUDA kernel
+    (counter-based Philox random numbers: event i depends only on (seed, i)).
+
+    Returns a float64 CUDA tensor (n, 3, 4) on `device`, written on its
+    current stream."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+
+    dev = torch.device("cuda", int(device) if not isinstance(device, torch.device) else device.index)
+    out = torch.empty((int(n), 3, 4), dtype=torch.float64, device=dev)
+    m = (ctypes.c_double * 3)(*(float(x) for x in masses))
+    lib = _lib.load()
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = lib.ctpwa_phase_space(float(M), m, int(n), int(seed) & (2**64 - 1), out.data_ptr(), ctypes.c_void_p(stream))
+    if rc != 0:
+        raise RuntimeError(_lib.error(None))
+    return out
+
+
 def write_dat(path, p4):
     """Reference .dat layout: one 'E px py pz' line per particle."""
     flat = np.ascontiguousarray(p4, dtype=np.float64).reshape(-1, 4)

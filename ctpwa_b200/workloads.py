@@ -313,8 +313,8 @@ def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2, timi
     dev = f"cuda:{device}"
     cfg = out / "config.yml"
     cfg.write_text(config_text(name, "in-memory-phsp", "in-memory-data"))
-    phsp = toymc.phase_space_gpu(M_JPSI, masses, n_phsp, 1001 + seed, device=dev, as_tensor=True)
-    tiny = toymc.phase_space_gpu(M_JPSI, masses, 1000, 7001 + seed, device=dev, as_tensor=True)
+    phsp = toymc.phase_space_device(M_JPSI, masses, n_phsp, 1001 + seed, device=device)
+    tiny = toymc.phase_space_device(M_JPSI, masses, 1000, 7001 + seed, device=device)
     p = torch.tensor(params_for(describe(str(cfg))), dtype=torch.float64, device=dev)
     lap("phsp")
     gen = torch.Generator(device=dev)
@@ -322,7 +322,7 @@ def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2, timi
     chunks, have, batch = [], 0, 0
     while have < n_data:
         ncand = int((n_data - have) * 12) + 10_000
-        cand = toymc.phase_space_gpu(M_JPSI, masses, ncand, 5001 + seed + 7919 * batch, device=dev, as_tensor=True)
+        cand = toymc.phase_space_device(M_JPSI, masses, ncand, 5001 + seed + 7919 * batch, device=device)
         lap("candidates")
         ana = analysis.from_device(str(cfg), tiny, cand, device=device)
         lap("cand_handle")

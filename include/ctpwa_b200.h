@@ -207,6 +207,14 @@ int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream);
  * (src/ComputeNLL.cu:21-84) and for its result export (ComputeResults.cu:22). */
 int ctpwa_intensity(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream);
 
+/* Toy-MC events on the device (no counterpart in the reference, whose toys
+ * are generated outside the library): n events of uniform three-body phase
+ * space for a parent of mass M at rest decaying to masses[0..2], written to
+ * d_out [n][3][4] (E, px, py, pz per particle) on the current device; event i
+ * depends only on (seed, i) (counter-based Philox-4x32-10 random numbers). */
+int ctpwa_phase_space(double M, const double* masses3, long long n, unsigned long long seed, double* d_out,
+                      void* stream);
+
 /* Per-event layout of the device event caches (no counterpart in the
  * reference): out[0] angular planes, out[1] polarisation states, out[2]
  * kinematic values the lineshapes are built from, out[3] of which invariant

@@ -372,3 +372,28 @@ def test_in_memory_samples_match_files(tmp_path):
         return torch.sqrt(s[:, 0] ** 2 - (s[:, 1:] ** 2).sum(1))
     near = lambda m: float(((m > 0.65) & (m < 0.9)).double().mean())
     assert near(m12(d1.cpu())) > 1.5 * near(m12(flat))
+
+
+def test_device_phase_space_generator():
+    """The CUDA phase-space generator: on-shell masses, momentum balance, flat
+    Dalitz density, event i a function of (seed, i) only."""
+    import torch
+    from ctpwa_b200 import toymc
+
+    M, masses = workloads.M_JPSI, (0.13975, 0.13975, 0.13495)
+    p = toymc.phase_space_device(M, masses, 200_000, 9).cpu().numpy()
+    m2 = p[..., 0] ** 2 - np.sum(p[..., 1:] ** 2, axis=-1)
+    assert np.allclose(np.sqrt(np.maximum(m2, 0)), np.array(masses)[None, :], rtol=1e-9)
+    tot = p.sum(axis=1)
+    assert np.allclose(tot[:, 0], M, rtol=1e-12) and np.allclose(tot[:, 1:], 0.0, atol=1e-12)
+    s12 = p[:, 0] + p[:, 1]
+    s12 = s12[:, 0] ** 2 - np.sum(s12[:, 1:] ** 2, axis=1)
+    s13 = p[:, 0] + p[:, 2]
+    s13 = s13[:, 0] ** 2 - np.sum(s13[:, 1:] ** 2, axis=1)
+    sel = (s12 > 2.0) & (s12 < 2.5)
+    h, _ = np.histogram(s13[sel], bins=10)
+    assert h[2:-2].std() / h[2:-2].mean() < 0.05
+    a = toymc.phase_space_device(M, masses, 1_000, 5)
+    b = toymc.phase_space_device(M, masses, 3_000, 5)
+    assert torch.equal(a, b[:1_000])
+    assert not torch.equal(a, toymc.phase_space_device(M, masses, 1_000, 6))
