@@ -16,8 +16,11 @@ namespace ctpwa {
 enum Precision : int { kFP64 = 0, kMixed = 1 };
 
 // Launch shape of the plain [0] and mixed [1] fused kernels: block size,
-// minimum resident CTAs per SM, and whether the event tables are staged
-// through shared memory by bulk copies (dynamic shared memory bytes).
+// minimum resident CTAs per SM, the staging of the event tables through
+// shared memory (0 off; 1, 2 per-warp bulk copies; 3 per-thread
+// asynchronous copies of the frontier values), gradient sums in shared
+// memory, and the dynamic shared memory bytes per CTA (fusedShape decides
+// them per model).
 struct FusedShape {
     int block[2] = {192, 256};
     int minb[2] = {2, 2};
