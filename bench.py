@@ -270,17 +270,18 @@ def run_reference(args, rank, world):
 
 # --------------------------------------------------------------------------- GPU arm
 def gpu_workload(args, rank, device):
+    """This rank's events, generated and kept on its GPU (phase space and
+    background from the library's generator, data by accept-reject against
+    the model on the device): (config, phsp, data, bkg, weights)."""
     from ctpwa_b200 import workloads
 
     seed = args.seed + 1000 * rank
     n_p, n_d, n_b, w_b = workloads.SIZES[WORKLOAD]
     f = args.fraction
     n_p, n_d, n_b = (max(100, int(round(x * f))) for x in (n_p, n_d, n_b))
-    out = Path(args.data_dir) / f"gpu_{WORKLOAD}_{n_p}_{n_d}_{n_b}_s{seed}"
-    if not (out / "done").exists():
-        workloads.make(WORKLOAD, out, n_phsp=n_p, n_data=n_d, n_bkg=n_b, bkg_weight=w_b, seed=seed, device=device)
-        (out / "done").write_text("ok")
-    return str(out / "config.yml")
+    out = Path(args.data_dir) / f"dev_{WORKLOAD}_r{rank}"
+    return workloads.make_device_samples(WORKLOAD, out, n_p, n_d, n_bkg=n_b, bkg_weight=w_b, seed=seed,
+                                         device=device)
 
 
 def algorithmic_bytes(layout, n_events, precision):
@@ -354,8 +355,9 @@ def run_gpu(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     W = max(3, args.warmup)
     K = args.steps
-    cfg = gpu_workload(args, rank, local_rank)
-    ana = ctpwa_b200.analysis(cfg, device=local_rank)
+    cfg, phsp, data, bkg, wts = gpu_workload(args, rank, local_rank)
+    ana = ctpwa_b200.analysis.from_device(cfg, phsp, data, bkg, weights=wts, device=local_rank)
+    del phsp, data, bkg, wts
     nV, nT, nP = ana.getNVector(), ana.getNFreeTheta(), ana.getNParams()
     n_events = tuple(int(x) for x in ana.getNEvents())
     layout = ana.eventLayout()
@@ -495,7 +497,8 @@ def run_gpu(args, rank, world, local_rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32+f64 (mixed: FP32 angular tables, lineshapes and coherent sum; FP64 m0^2-m^2, log and sums)",
-        "data": "synthetic (seeded phase space, accept-reject data, uniform background), events resident in HBM",
+        "data": "synthetic, generated on the GPU (seeded phase space, accept-reject data, uniform background), "
+                "events resident in HBM",
         "config": {"workload": WORKLOAD_TEXT, "events_per_rank": {"phsp": n_events[0], "data": n_events[1],
                                                                   "bkg": n_events[2]},
                    "n_params": nP, "theta_perturbed_every_step": True, "fraction": args.fraction,

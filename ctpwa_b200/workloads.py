@@ -283,6 +283,22 @@ def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, inten
     return sel[:n_data]
 
 
+def make_device_samples(name, outdir, n_phsp, n_data, n_bkg=0, bkg_weight=None, seed=0, device=0):
+    """Workload `name` generated and kept on the GPU, background included:
+    returns (config_path, phsp, data, bkg, weights) for
+    ``analysis.from_device(config_path, phsp, data, bkg, weights=weights)``
+    (bkg None when n_bkg is 0; weights: None or [None, None, bkg weights])."""
+    import torch
+
+    cfg, phsp, data = make_device(name, outdir, n_phsp, n_data, seed=seed, device=device)
+    if not n_bkg:
+        return cfg, phsp, data, None, None
+    w = SIZES[name][3] if bkg_weight is None else bkg_weight
+    bkg = toymc.phase_space_device(M_JPSI, MASSES[name], n_bkg, 3001 + seed, device=device)
+    wt = torch.full((n_bkg,), float(w), dtype=torch.float64, device=bkg.device)
+    return cfg, phsp, data, bkg, [None, None, wt]
+
+
 def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2, timing=None):
     """Toy-MC samples of workload `name` generated and kept on the GPU:
     phase space from the seeded GPU generator, data by accept-reject of GPU
