@@ -4,7 +4,8 @@
 Workload: J/psi -> K+ K- pi0 with K*(892)+-, K*(1410)+-, K*2(1430)+- (BWR) and
 a K+K- J=1 state with a custom Flatte lineshape; 10M phase-space, 1M data
 (accept-reject against the model) and 100k background events (weight 0.3),
-seeded synthetic four-momenta. One step = one NLL + full gradient
+seeded synthetic four-momenta generated on the GPU and kept there (the
+engine's handle is built from the device arrays). One step = one NLL + full gradient
 (couplings and all 9 resonance parameters) with the resonance parameters
 perturbed every step, so every lineshape is recomputed.
 
