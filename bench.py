@@ -296,12 +296,14 @@ def algorithmic_bytes(layout, n_events, precision):
     return per * (n_p + n_d + n_b) + 8 * n_b, per
 
 
-def streamed_bytes(layout, n_events, precision):
+def streamed_bytes(layout, n_events, precision, paired=False):
     """Bytes the fused kernel actually reads per evaluation in this layout:
-    angular values plus the per-event frontier values."""
+    angular values (of the stored polarisations) plus the per-event frontier
+    values."""
     sc = 16 if precision == "fp64" else 8
     ev = layout["nev64"] * 8 if precision == "fp64" else layout["nevf"] * 4 + layout["nevd"] * 8
-    per = layout["planes"] * layout["npol"] * sc + ev
+    npol = (layout["npol"] + 1) // 2 if paired else layout["npol"]
+    per = layout["planes"] * npol * sc + ev
     n_p, n_d, n_b = n_events
     return per * (n_p + n_d + n_b) + 8 * n_b
 
@@ -474,6 +476,7 @@ def run_gpu(args, rank, world, local_rank):
 
     if rank != 0:
         return 0
+    paired_mx = bool(ana.launchShape()["mixed"]["pol_paired"])
     peaks = measured_peaks()
     if peaks and peaks.get("hbm_gbs"):
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
@@ -504,7 +507,7 @@ def run_gpu(args, rank, world, local_rank):
                                                                   "bkg": n_events[2]},
                    "n_params": nP, "theta_perturbed_every_step": True, "fraction": args.fraction,
                    "launch": ana.launchShape(),
-                   "l2": f"inputs larger than L2: {streamed_bytes(layout, n_events, 'mixed') / 1e9:.2f} GB streamed "
+                   "l2": f"inputs larger than L2: {streamed_bytes(layout, n_events, 'mixed', paired_mx) / 1e9:.2f} GB streamed "
                          f"per step vs {L2_BYTES / 1e6:.0f} MB L2, no flush",
                    "exchange": ("NCCL all-reduce of the per-sample sums per step (3*(2+2nA+nT)+4 doubles), "
                                 "then loss/gradient of the union on every rank") if world > 1 else "none (1 GPU)"},
@@ -523,7 +526,7 @@ def run_gpu(args, rank, world, local_rank):
                      "traffic": traffic, "peak_source": peak_src,
                      "kernel": "ct_fused_mixed",
                      "kernel_ms": kms, "algorithmic_bytes_per_launch": alg, "algorithmic_bytes_per_event": per_evt,
-                     "streamed_bytes_per_launch": streamed_bytes(layout, n_events, "mixed")},
+                     "streamed_bytes_per_launch": streamed_bytes(layout, n_events, "mixed", paired_mx)},
     }
     if hess is not None:
         line["hessian"] = hess

@@ -540,13 +540,14 @@ class analysis:
     def launchShape(self) -> dict:
         """Launch shape of the fused kernels per precision: threads per CTA,
         minimum resident CTAs per SM, table staging mode, gradient sums in
-        shared memory, dynamic shared memory bytes, CTAs per launch."""
+        shared memory, dynamic shared memory bytes, CTAs per launch, and
+        whether the angular tables store conjugate-paired polarisations once."""
         self._check()
-        out = (ctypes.c_int * 12)()
+        out = (ctypes.c_int * 14)()
         if self._lib.ctpwa_launch_shape(self._h, out) != 0:
             raise RuntimeError(_lib.error(self._h))
-        keys = ("block", "min_ctas_per_sm", "stage", "acc_smem", "dyn_smem", "grid")
-        return {pr: dict(zip(keys, out[6 * i:6 * i + 6])) for i, pr in enumerate(("fp64", "mixed"))}
+        keys = ("block", "min_ctas_per_sm", "stage", "acc_smem", "dyn_smem", "grid", "pol_paired")
+        return {pr: dict(zip(keys, out[7 * i:7 * i + 7])) for i, pr in enumerate(("fp64", "mixed"))}
 
     def setKernelTiming(self, slots: int):
         """Record CUDA events around each fused-kernel launch (ring of `slots`; 0 = off)."""

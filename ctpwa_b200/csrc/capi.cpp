@@ -391,18 +391,19 @@ int ctpwa_event_cache_layout(const ctpwa_handle* h, int* out3)
     return CTPWA_OK;
 }
 
-int ctpwa_launch_shape(const ctpwa_handle* h, int* out12)
+int ctpwa_launch_shape(const ctpwa_handle* h, int* out14)
 {
-    if (!h || !out12) return CTPWA_ERR_ARG;
+    if (!h || !out14) return CTPWA_ERR_ARG;
     const ctpwa::FusedShape& sh = h->eng->shape();
     for (int pr = 0; pr < 2; ++pr) {
-        int* o = out12 + 6 * pr;
+        int* o = out14 + 7 * pr;
         o[0] = sh.block[pr];
         o[1] = sh.minb[pr];
         o[2] = sh.stage[pr];
         o[3] = sh.acc[pr];
         o[4] = sh.dsmem[pr];
         o[5] = h->eng->fusedGrid(pr);
+        o[6] = h->eng->polPaired(pr) ? 1 : 0;
     }
     return CTPWA_OK;
 }

@@ -785,6 +785,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     buildTables();
     for (int k = 0; k < 3; ++k)
         if (samples_[k].n > 0 || k < 2) computeAngular(k);
+    pairPolarisations();
     // evaluation buffers
     int nA = model_.nAmp();
     alloc(d_v_, sizeof(double) * 2 * nA);
@@ -842,6 +843,7 @@ Engine::~Engine()
         devFree(s.p4);
         devFree(s.slamp64);
         devFree(s.slamp32);
+        devFree(s.slamp64p);
         devFree(s.kin);
         devFree(s.ev64);
         devFree(s.evf);
@@ -1141,6 +1143,121 @@ void Engine::buildTables()
     }
 }
 
+namespace {
+
+// max over events of |SL_{c, npol-1-q} - conj(SL_{c,q})| and of
+// |SL_{c, npol-1-q} + conj(SL_{c,q})| per (plane c, pair q), and of |SL|:
+// out[(c * npair + q) * 2 + 0 / 1], out[2 * nplane * npair] (doubles >= 0,
+// compared through their bit patterns)
+__global__ void ct_pair_check_kernel(const double2* __restrict__ sl, long long n, long long ld, int nplane, int npol,
+                                     unsigned long long* __restrict__ out)
+{
+    const int npair = npol / 2;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double big = 0.0;
+        for (int c = 0; c < nplane; ++c) {
+            for (int q = 0; q < npair; ++q) {
+                const double2 a = sl[(long long)(c * npol + q) * ld + e];
+                const double2 b = sl[(long long)(c * npol + npol - 1 - q) * ld + e];
+                const double dp = hypot(b.x - a.x, b.y + a.y), dn = hypot(b.x + a.x, b.y - a.y);
+                atomicMax(out + (c * npair + q) * 2, (unsigned long long)__double_as_longlong(dp));
+                atomicMax(out + (c * npair + q) * 2 + 1, (unsigned long long)__double_as_longlong(dn));
+            }
+            for (int p = 0; p < npol; ++p) {
+                const double2 a = sl[(long long)(c * npol + p) * ld + e];
+                big = fmax(big, hypot(a.x, a.y));
+            }
+        }
+        atomicMax(out + 2 * nplane * npair, (unsigned long long)__double_as_longlong(big));
+    }
+}
+
+}  // namespace
+
+// Decides whether the polarisations pair up as SL_{npol-1-q} = conj(SL_q) on
+// every event of the phase-space, data and background samples (to 1e-12 of
+// the largest |SL|; e.g. the M = -1 and M = +1 states of a J/psi decaying to
+// spin-0 particles), and if so switches the fused kernels to their paired
+// variants (ct_fused_*_pc) with compact tables holding polarisations
+// 0 .. (npol+1)/2 - 1: the FP32 table is replaced, the plain kernel gets an
+// FP64 copy (the other kernels keep the full FP64 table). The check also
+// measures the minus-sign relation, which the paired kernels do not use.
+// Runs on the constructor's initialisation stream.
+void Engine::pairPolarisations()
+{
+    const int npol = model_.npol, nplane = gen_.nplane, npair = npol / 2;
+    const char* off = std::getenv("CTPWA_NO_POL_PAIRING");
+    if (npair == 0 || nplane * npair > 32 || (off && *off && *off != '0')) return;
+    const int nout = 2 * nplane * npair + 1;
+    unsigned long long* d_out = nullptr;
+    alloc(d_out, sizeof(unsigned long long) * nout);
+    std::vector<double> worst(2 * nplane * npair, 0.0);
+    double big = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        const DeviceSample& d = samples_[k];
+        if (d.n <= 0) continue;
+        CT_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * nout, init_stream_));
+        const unsigned grid = (unsigned)std::min<long long>((d.n + 255) / 256, 148LL * 32);
+        ct_pair_check_kernel<<<grid, 256, 0, init_stream_>>>(d.slamp64, d.n, d.ld, nplane, npol, d_out);
+        CT_CUDA(cudaGetLastError());
+        std::vector<unsigned long long> h(nout);
+        CT_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(unsigned long long) * nout, cudaMemcpyDeviceToHost, init_stream_));
+        CT_CUDA(cudaStreamSynchronize(init_stream_));
+        for (int i = 0; i < 2 * nplane * npair; ++i) {
+            double x;
+            std::memcpy(&x, &h[i], sizeof(double));
+            worst[i] = std::max(worst[i], x);
+        }
+        double b;
+        std::memcpy(&b, &h[2 * nplane * npair], sizeof(double));
+        big = std::max(big, b);
+    }
+    devFree(d_out);
+    const double tol = 1e-12 * big;
+    unsigned neg = 0;
+    bool ok = big > 0.0;
+    for (int c = 0; c < nplane && ok; ++c)
+        for (int q = 0; q < npair && ok; ++q) {
+            const double dp = worst[(c * npair + q) * 2], dn = worst[(c * npair + q) * 2 + 1];
+            if (dp <= tol) continue;
+            if (dn <= tol) neg |= 1u << (c * npair + q);
+            else ok = false;
+        }
+    // the paired kernels rebuild conjugates with a plus sign
+    if (!ok || neg != 0) return;
+    const int ns = (npol + 1) / 2;
+    paired_[0] = true;
+    paired_[1] = opt_.mixed_tables;
+    for (int pr = 0; pr < 2; ++pr)
+        if (paired_[pr]) (pr == 0 ? k_f64_ : k_mixed_) = k_pc_[pr];
+    for (int k = 0; k < 3; ++k) {
+        DeviceSample& d = samples_[k];
+        if (!d.slamp64) continue;
+        const size_t rows = (size_t)nplane * ns;
+        if (paired_[0]) {
+            alloc(d.slamp64p, sizeof(double2) * rows * d.ld);
+            device_bytes_ += sizeof(double2) * rows * d.ld;
+            for (int c = 0; c < nplane; ++c)
+                for (int q = 0; q < ns; ++q)
+                    CT_CUDA(cudaMemcpyAsync(d.slamp64p + (size_t)(c * ns + q) * d.ld, d.slamp64 + (size_t)(c * npol + q) * d.ld,
+                                            sizeof(double2) * d.ld, cudaMemcpyDeviceToDevice, init_stream_));
+        }
+        if (paired_[1] && d.slamp32) {
+            float2* compact = nullptr;
+            alloc(compact, sizeof(float2) * rows * d.ld);
+            for (int c = 0; c < nplane; ++c)
+                for (int q = 0; q < ns; ++q)
+                    CT_CUDA(cudaMemcpyAsync(compact + (size_t)(c * ns + q) * d.ld, d.slamp32 + (size_t)(c * npol + q) * d.ld,
+                                            sizeof(float2) * d.ld, cudaMemcpyDeviceToDevice, init_stream_));
+            CT_CUDA(cudaStreamSynchronize(init_stream_));
+            devFree(d.slamp32);
+            device_bytes_ -= sizeof(float2) * (size_t)(npol - ns) * nplane * d.ld;
+            d.slamp32 = compact;
+        }
+    }
+    CT_CUDA(cudaStreamSynchronize(init_stream_));
+}
+
 void Engine::computeAngular(int kind)
 {
     DeviceSample& d = samples_[kind];
@@ -1410,6 +1527,11 @@ void Engine::compileKernel()
     CT_CUDA(cudaLibraryGetGlobal(&k_sym_, &k_sym_bytes_, lib, "ct_k"));
     CT_CUDA(cudaLibraryGetKernel(&k64, lib, "ct_fused_f64"));
     CT_CUDA(cudaLibraryGetKernel(&kmx, lib, "ct_fused_mixed"));
+    cudaKernel_t k64p, kmxp;
+    CT_CUDA(cudaLibraryGetKernel(&k64p, lib, "ct_fused_f64_pc"));
+    CT_CUDA(cudaLibraryGetKernel(&kmxp, lib, "ct_fused_mixed_pc"));
+    k_pc_[0] = (void*)k64p;
+    k_pc_[1] = (void*)kmxp;
     CT_CUDA(cudaLibraryGetKernel(&kin, lib, "ct_intensity_f64"));
     cudaKernel_t kpart, kexp;
     CT_CUDA(cudaLibraryGetKernel(&kpart, lib, "ct_partials_f64"));
@@ -1420,8 +1542,8 @@ void Engine::compileKernel()
     k_mixed_ = (void*)kmx;
     for (int pr = 0; pr < 2; ++pr)
         if (shape_.dsmem[pr] > 0)
-            CT_CUDA(cudaFuncSetAttribute((const void*)(pr == 0 ? k_f64_ : k_mixed_),
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, shape_.dsmem[pr]));
+            for (void* k : {pr == 0 ? k_f64_ : k_mixed_, k_pc_[pr]})
+                CT_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, shape_.dsmem[pr]));
     k_int_ = (void*)kin;
     jit_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -1481,7 +1603,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
         if (lay.cta[k][1] == 0) continue;
         CtSampleH& s = a.s[ns++];
         const DeviceSample& d = samples_[k];
-        s.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
+        s.slamp = precision == kMixed ? (const void*)d.slamp32 : (paired_[0] ? (const void*)d.slamp64p : (const void*)d.slamp64);
         s.ev = precision == kMixed ? (const void*)d.evf : (const void*)d.ev64;
         s.evd = precision == kMixed ? d.evd : nullptr;
         s.w = d.w;
@@ -1624,7 +1746,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
         if (lay.cta[k][1] == 0) continue;
         CtSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
-        sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
+        sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (paired_[0] ? (const void*)d.slamp64p : (const void*)d.slamp64);
         sm.ev = precision == kMixed ? (const void*)d.evf : (const void*)d.ev64;
         sm.evd = precision == kMixed ? d.evd : nullptr;
         sm.w = d.w;
@@ -1694,7 +1816,7 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
         if (lay.cta[k][1] == 0) continue;
         CtSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
-        sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (const void*)d.slamp64;
+        sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (paired_[0] ? (const void*)d.slamp64p : (const void*)d.slamp64);
         sm.ev = precision == kMixed ? (const void*)d.evf : (const void*)d.ev64;
         sm.evd = precision == kMixed ? d.evd : nullptr;
         sm.w = d.w;

@@ -35,7 +35,8 @@ struct DeviceSample {
     long long ld = 0;          // row stride of the tables below (n padded to 256)
     double* p4 = nullptr;      // SoA [n_final * 4][n]
     double2* slamp64 = nullptr;  // [nplane * npol][ld]
-    float2* slamp32 = nullptr;   // mixed-precision copy
+    float2* slamp32 = nullptr;   // mixed-precision copy (polarisation-paired when the engine pairs them)
+    double2* slamp64p = nullptr; // polarisation-paired FP64 copy for the plain fused kernel
     double* kin = nullptr;     // [nkin][ld] kinematic cache (initialisation only)
     double* ev64 = nullptr;    // [nev64][ld] frontier values, FP64
     float* evf = nullptr;      // [nevf][ld] mixed form, FP32 frontier values
@@ -149,6 +150,7 @@ public:
     const GeneratedModel& generated() const { return gen_; }
     const FusedShape& shape() const { return shape_; }
     int fusedGrid(int precision) const { return lay_[precision == kMixed ? 1 : 0].grid; }
+    bool polPaired(int precision) const { return paired_[precision == kMixed ? 1 : 0]; }
     double jitSeconds() const { return jit_seconds_; }
     bool jitCacheHit() const { return jit_cache_hit_; }
 
@@ -157,6 +159,11 @@ private:
     void buildTables();
     void computeAngular(int kind);
     void buildEventCache(int kind);
+    void pairPolarisations();
+    // SL_{npol-1-q} = conj(SL_q) on every event of every sample: the fused
+    // kernels' tables keep the first (npol + 1) / 2 polarisations
+    bool paired_[2] = {false, false};  // plain, mixed fused kernels use the paired tables
+    void* k_pc_[2] = {nullptr, nullptr};  // ct_fused_f64_pc, ct_fused_mixed_pc
     void compileKernel();
     void compileHvp();
 

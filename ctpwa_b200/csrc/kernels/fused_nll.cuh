@@ -102,6 +102,13 @@ struct CtArgs {
 
 #define CT_NCONST_ALLOC (M_NCONST > 0 ? M_NCONST : 1)
 
+// Conjugate-paired polarisations: when every event satisfies
+// SL_{plane, npol-1-q} = conj(SL_{plane, q}) (checked on all samples when they
+// are loaded), the angular tables of the fused kernels store the first
+// CT_NPOL_STORED polarisations only, [plane][q][ld], and the *_pc kernels
+// rebuild the others as conjugates (the negation folds into the FMAs).
+#define CT_NPOL_STORED ((M_NPOL + 1) / 2)
+
 // Per-call constants of the fused kernels in the constant bank: the
 // parameter-only subexpressions (FP64, and FP32 hi + lo pairs) and the
 // couplings (FP64, and FP32 hi + lo pairs). ct_prologue writes their image
@@ -286,7 +293,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_event_cache(const doub
 // L: type of the lineshapes, their derivatives and the per-thread gradient
 //    sums
 // PH_ONLY: the launch serves phase-space events only
-template <typename R, typename L, bool PH_ONLY, int BLOCK, int STAGE, bool ACC_SMEM>
+template <typename R, typename L, bool PH_ONLY, int BLOCK, int STAGE, bool ACC_SMEM, bool PAIRED>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 {
     typedef typename CtVec2<R>::type SL2;
@@ -335,8 +342,22 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 
         // ---- coherent sum over amplitudes ----
         SL2 sl[M_NPLANE * M_NPOL];
+        if constexpr (PAIRED) {
 #pragma unroll
-        for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = slp[(long long)c * ss];
+            for (int c = 0; c < M_NPLANE; ++c) {
+#pragma unroll
+                for (int q = 0; q < CT_NPOL_STORED; ++q) sl[c * M_NPOL + q] = slp[(long long)(c * CT_NPOL_STORED + q) * ss];
+#pragma unroll
+                for (int p = CT_NPOL_STORED; p < M_NPOL; ++p) {
+                    const SL2 x = sl[c * M_NPOL + M_NPOL - 1 - p];
+                    sl[c * M_NPOL + p].x = x.x;
+                    sl[c * M_NPOL + p].y = -x.y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = slp[(long long)c * ss];
+        }
         // c_t = v_col(t) F_t per term (one per column, more with identical particles)
         R cr[M_NTERM], ci[M_NTERM];
 #pragma unroll
@@ -492,7 +513,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         // the current tile. No CTA-wide barrier: warps proceed independently.
         // Rows are padded to multiples of 256 events, so every copy starts on
         // a 128-byte boundary and moves a whole 32-event tile.
-        constexpr int NPL = M_NPLANE * M_NPOL;
+        constexpr int NPL = M_NPLANE * (PAIRED ? CT_NPOL_STORED : M_NPOL);  // table rows
         constexpr int W = BLOCK / 32;
         constexpr int NA = CtEvent<L>::NA, NB = CtEvent<L>::NB;
         constexpr unsigned AR = 32 * sizeof(L), BR = 32 * sizeof(double), SR = 32 * sizeof(SL2);
@@ -585,12 +606,20 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 #endif
 extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB) ct_fused_f64(CtArgs a)
 {
-    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE, CT_F64_ACC != 0>(a);
+    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE, CT_F64_ACC != 0, false>(a);
+}
+extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB) ct_fused_f64_pc(CtArgs a)
+{
+    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE, CT_F64_ACC != 0, true>(a);
 }
 // mixed form (FP32 lineshapes and algebra, FP64 logs and sums), all samples
 extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_mixed(CtArgs a)
 {
-    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE, CT_MX_ACC != 0>(a);
+    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE, CT_MX_ACC != 0, false>(a);
+}
+extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_mixed_pc(CtArgs a)
+{
+    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE, CT_MX_ACC != 0, true>(a);
 }
 
 // Partial-wave integrals of sample s[0] (FP64): per resonance block i,

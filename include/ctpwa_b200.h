@@ -228,11 +228,13 @@ int ctpwa_event_layout(const ctpwa_handle* h, int* out4);
 int ctpwa_event_cache_layout(const ctpwa_handle* h, int* out3);
 
 /* Launch shape of the fused kernels (no counterpart in the reference): for
- * the plain [0..5] and mixed [6..11] kernels: threads per CTA, minimum
+ * the plain [0..6] and mixed [7..13] kernels: threads per CTA, minimum
  * resident CTAs per SM, table staging mode (0 off, 1 frontier rows, 2
- * frontier and angular rows), gradient sums in shared memory (0/1), dynamic
- * shared memory bytes per CTA, CTAs per launch. */
-int ctpwa_launch_shape(const ctpwa_handle* h, int* out12);
+ * frontier and angular rows, 3 frontier values by asynchronous copies),
+ * gradient sums in shared memory (0/1), dynamic shared memory bytes per CTA,
+ * CTAs per launch, polarisation pairing of the angular tables (1: only the
+ * first (npol+1)/2 polarisations stored, the others their conjugates). */
+int ctpwa_launch_shape(const ctpwa_handle* h, int* out14);
 
 /* Per-launch timing of the fused likelihood kernel (no counterpart in the
  * reference, which times nothing on the device). slots > 0 records a CUDA

@@ -301,6 +301,9 @@ def test_staged_tables_match_direct_loads(tmp_path, monkeypatch, mode):
     monkeypatch.setenv("CTPWA_F64_ACC_SMEM", "0")
     monkeypatch.setenv("CTPWA_STAGE", "0")
     if mode == 2:
+        # full tables in both handles: at one CTA per SM the unstaged kernel
+        # still fits two, the staged one with the angular rows only one
+        monkeypatch.setenv("CTPWA_NO_POL_PAIRING", "1")
         monkeypatch.setenv("CTPWA_F64_MINB", "1")
         monkeypatch.setenv("CTPWA_MX_MINB", "1")
     direct = ctpwa_b200.analysis(cfg)
@@ -397,3 +400,32 @@ def test_device_phase_space_generator():
     b = toymc.phase_space_device(M, masses, 3_000, 5)
     assert torch.equal(a, b[:1_000])
     assert not torch.equal(a, toymc.phase_space_device(M, masses, 1_000, 6))
+
+
+def test_polarisation_pairing(tmp_path, monkeypatch):
+    """J/psi -> K+K-pi0: the M = +1 and M = -1 angular values are complex
+    conjugates on every event, so the fused kernels store two of the three
+    polarisations; results equal those of the full tables."""
+    import torch
+    import ctpwa_b200
+
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=40_001, n_data=6_001, n_bkg=1_001, accept_reject=False, seed=33)
+    paired = ctpwa_b200.analysis(cfg)
+    shape = paired.launchShape()
+    assert shape["fp64"]["pol_paired"] == 1 and shape["mixed"]["pol_paired"] == 1
+    monkeypatch.setenv("CTPWA_NO_POL_PAIRING", "1")
+    full = ctpwa_b200.analysis(cfg)
+    assert full.launchShape()["mixed"]["pol_paired"] == 0
+    p = workloads.true_params(full.getNVector(), full.getFreeResParams()[0].numpy())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    n0, g0 = full.getNLLAndGrad(pt, "fp64")
+    n1, g1 = paired.getNLLAndGrad(pt, "fp64")
+    assert abs(float(n0) - float(n1)) <= 1e-12 * abs(float(n0))
+    assert float((g0 - g1).abs().max()) <= 1e-10 * float(g0.abs().max())
+    m0, h0 = full.getNLLAndGrad(pt, "mixed")
+    m1, h1 = paired.getNLLAndGrad(pt, "mixed")
+    assert abs(float(m0) - float(m1)) < 1e-5
+    assert float((h0 - h1).abs().max()) <= 1e-6 * float(h0.abs().max())
+    orc = Oracle(cfg)
+    onll, og, _ = orc.nll_grad(p)
+    assert abs(float(n1) - onll) <= 1e-10 * abs(onll)
