@@ -341,23 +341,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         ev.columns(sC, sCfh, sCfl, Fr, Fi, dFr, dFi);
 
         // ---- coherent sum over amplitudes ----
-        SL2 sl[M_NPLANE * M_NPOL];
-        if constexpr (PAIRED) {
+        // (paired tables: SL_{c,NPOL-1-p} = conj(SL_{c,p}), only the first
+        // CT_NPOL_STORED polarisations are stored and read)
+        constexpr int NPS = PAIRED ? CT_NPOL_STORED : M_NPOL;
+        SL2 sl[M_NPLANE * NPS];
 #pragma unroll
-            for (int c = 0; c < M_NPLANE; ++c) {
-#pragma unroll
-                for (int q = 0; q < CT_NPOL_STORED; ++q) sl[c * M_NPOL + q] = slp[(long long)(c * CT_NPOL_STORED + q) * ss];
-#pragma unroll
-                for (int p = CT_NPOL_STORED; p < M_NPOL; ++p) {
-                    const SL2 x = sl[c * M_NPOL + M_NPOL - 1 - p];
-                    sl[c * M_NPOL + p].x = x.x;
-                    sl[c * M_NPOL + p].y = -x.y;
-                }
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = slp[(long long)c * ss];
-        }
+        for (int c = 0; c < M_NPLANE * NPS; ++c) sl[c] = slp[(long long)c * ss];
         // c_t = v_col(t) F_t per term (one per column, more with identical particles)
         R cr[M_NTERM], ci[M_NTERM];
 #pragma unroll
@@ -377,20 +366,40 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             }
         }
         R Sr[M_NPOL], Si[M_NPOL];
+#pragma unroll
+        for (int p = 0; p < NPS; ++p) {
+            const int q = M_NPOL - 1 - p;
+            if (PAIRED && q != p) {
+                // S_p = sum c (x + iy), S_q = sum c (x - iy) from the same four
+                // products per term
+                R xr = (R)0, yi = (R)0, yr = (R)0, xi = (R)0;
+#pragma unroll
+                for (int t = 0; t < M_NTERM; ++t) {
+                    SL2 x = sl[term_plane(t) * NPS + p];
+                    xr += cr[t] * x.x;
+                    yi += ci[t] * x.y;
+                    yr += cr[t] * x.y;
+                    xi += ci[t] * x.x;
+                }
+                Sr[p] = xr - yi;
+                Si[p] = yr + xi;
+                Sr[q] = xr + yi;
+                Si[q] = xi - yr;
+            } else {
+                R sr = (R)0, sim = (R)0;
+#pragma unroll
+                for (int t = 0; t < M_NTERM; ++t) {
+                    SL2 x = sl[term_plane(t) * NPS + p];
+                    sr += cr[t] * x.x - ci[t] * x.y;
+                    sim += cr[t] * x.y + ci[t] * x.x;
+                }
+                Sr[p] = sr;
+                Si[p] = sim;
+            }
+        }
         R f = (R)0;
 #pragma unroll
-        for (int p = 0; p < M_NPOL; ++p) {
-            R sr = (R)0, sim = (R)0;
-#pragma unroll
-            for (int t = 0; t < M_NTERM; ++t) {
-                SL2 x = sl[term_plane(t) * M_NPOL + p];
-                sr += cr[t] * x.x - ci[t] * x.y;
-                sim += cr[t] * x.y + ci[t] * x.x;
-            }
-            Sr[p] = sr;
-            Si[p] = sim;
-            f += sr * sr + sim * sim;
-        }
+        for (int p = 0; p < M_NPOL; ++p) f += Sr[p] * Sr[p] + Si[p] * Si[p];
 
         // ---- per-event weight of the adjoint ----
         // (the sample's common factors of the gradient terms, w / W or -1 for
@@ -424,15 +433,32 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             }
         }
         // T_c = sum_p conj(SL_{c,p}) u_p
+        // (paired: conj(SL_p) u_p + SL_p u_q = x (u_p + u_q) + i y (u_q - u_p))
+        R ar[NPS], br[NPS], ai[NPS], bi[NPS];
+#pragma unroll
+        for (int p = 0; p < NPS; ++p) {
+            const int q = M_NPOL - 1 - p;
+            if (PAIRED && q != p) {
+                ar[p] = ur[p] + ur[q];
+                br[p] = ui[p] - ui[q];
+                ai[p] = ui[p] + ui[q];
+                bi[p] = ur[q] - ur[p];
+            } else {
+                ar[p] = ur[p];
+                br[p] = ui[p];
+                ai[p] = ui[p];
+                bi[p] = -ur[p];
+            }
+        }
         R Tr[M_NPLANE], Ti[M_NPLANE];
 #pragma unroll
         for (int c = 0; c < M_NPLANE; ++c) {
             R tr = (R)0, ti = (R)0;
 #pragma unroll
-            for (int p = 0; p < M_NPOL; ++p) {
-                SL2 x = sl[c * M_NPOL + p];
-                tr += x.x * ur[p] + x.y * ui[p];
-                ti += x.x * ui[p] - x.y * ur[p];
+            for (int p = 0; p < NPS; ++p) {
+                SL2 x = sl[c * NPS + p];
+                tr += x.x * ar[p] + x.y * br[p];
+                ti += x.x * ai[p] + x.y * bi[p];
             }
             Tr[c] = tr;
             Ti[c] = ti;
