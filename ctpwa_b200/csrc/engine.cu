@@ -1145,31 +1145,57 @@ void Engine::buildTables()
 
 namespace {
 
+__device__ __forceinline__ double ct_warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// a NaN or infinite distance counts as infinitely far
+__device__ __forceinline__ double ct_dist(double x, double y)
+{
+    const double d = hypot(x, y);
+    return d == d ? d : (double)INFINITY;
+}
+
 // max over events of |SL_{c, npol-1-q} - conj(SL_{c,q})| and of
 // |SL_{c, npol-1-q} + conj(SL_{c,q})| per (plane c, pair q), and of |SL|:
 // out[(c * npair + q) * 2 + 0 / 1], out[2 * nplane * npair] (doubles >= 0,
 // compared through their bit patterns)
+//
+// Each thread keeps its own maxima over its events, one pair at a time;
+// warps combine them by shuffles and lane 0 issues one atomic per warp and
+// value (blocks are whole warps).
 __global__ void ct_pair_check_kernel(const double2* __restrict__ sl, long long n, long long ld, int nplane, int npol,
                                      unsigned long long* __restrict__ out)
 {
-    const int npair = npol / 2;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        double big = 0.0;
-        for (int c = 0; c < nplane; ++c) {
-            for (int q = 0; q < npair; ++q) {
-                const double2 a = sl[(long long)(c * npol + q) * ld + e];
-                const double2 b = sl[(long long)(c * npol + npol - 1 - q) * ld + e];
-                const double dp = hypot(b.x - a.x, b.y + a.y), dn = hypot(b.x + a.x, b.y - a.y);
+    const int npair = npol / 2, lane = threadIdx.x & 31;
+    const long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    for (int c = 0; c < nplane; ++c)
+        for (int q = 0; q < npair; ++q) {
+            const double2* __restrict__ ra = sl + (long long)(c * npol + q) * ld;
+            const double2* __restrict__ rb = sl + (long long)(c * npol + npol - 1 - q) * ld;
+            double dp = 0.0, dn = 0.0;
+            for (long long e = e0; e < n; e += stride) {
+                const double2 a = ra[e], b = rb[e];
+                dp = fmax(dp, ct_dist(b.x - a.x, b.y + a.y));
+                dn = fmax(dn, ct_dist(b.x + a.x, b.y - a.y));
+            }
+            dp = ct_warp_max(dp);
+            dn = ct_warp_max(dn);
+            if (lane == 0) {
                 atomicMax(out + (c * npair + q) * 2, (unsigned long long)__double_as_longlong(dp));
                 atomicMax(out + (c * npair + q) * 2 + 1, (unsigned long long)__double_as_longlong(dn));
             }
-            for (int p = 0; p < npol; ++p) {
-                const double2 a = sl[(long long)(c * npol + p) * ld + e];
-                big = fmax(big, hypot(a.x, a.y));
-            }
         }
-        atomicMax(out + 2 * nplane * npair, (unsigned long long)__double_as_longlong(big));
+    double big = 0.0;
+    for (int r = 0; r < nplane * npol; ++r) {
+        const double2* __restrict__ ra = sl + (long long)r * ld;
+        for (long long e = e0; e < n; e += stride) big = fmax(big, ct_dist(ra[e].x, ra[e].y));
     }
+    big = ct_warp_max(big);
+    if (lane == 0) atomicMax(out + 2 * nplane * npair, (unsigned long long)__double_as_longlong(big));
 }
 
 }  // namespace
@@ -1197,7 +1223,7 @@ void Engine::pairPolarisations()
         const DeviceSample& d = samples_[k];
         if (d.n <= 0) continue;
         CT_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * nout, init_stream_));
-        const unsigned grid = (unsigned)std::min<long long>((d.n + 255) / 256, 148LL * 32);
+        const unsigned grid = (unsigned)std::min<long long>((d.n + 255) / 256, 148LL * 8);
         ct_pair_check_kernel<<<grid, 256, 0, init_stream_>>>(d.slamp64, d.n, d.ld, nplane, npol, d_out);
         CT_CUDA(cudaGetLastError());
         std::vector<unsigned long long> h(nout);
