@@ -1362,9 +1362,13 @@ void Engine::buildEventCache(int kind)
 // K+K-pi0 workload with the frontier tables and the constant bank: plain
 // 192 x 2 with the gradient sums in shared memory (170 registers, 12 warps
 // per SM, no spills) 0.95 ms, against 0.95 ms at 96 x 4, 0.99 ms at 128 x 3,
-// 1.15 ms at 256 x 2 (128 registers, spills) and 1.17 ms at 224 x 2; mixed (frontier values by asynchronous copies, constants in the
-// constant bank) 256 x 2 with the sums in shared memory 0.491 ms, against
-// 0.51 ms in registers, 0.77 ms at 3 CTAs per SM, 0.55 ms at 128 x 4.
+// 1.15 ms at 256 x 2 (128 registers, spills) and 1.17 ms at 224 x 2; mixed
+// (frontier values by asynchronous copies, constants in the constant bank,
+// paired polarisations) 256 x 2 with the sums in registers 0.4125 ms,
+// against 0.4214 ms in shared memory (0.583 ms with each add a
+// shared-memory atomic); before the pairing, with 12 more live registers,
+// the shared-memory sums were ahead (0.491 against 0.51 ms), and 3 CTAs per
+// SM ran 0.77 ms, 128 x 4 0.55 ms.
 FusedShape fusedShape(const GeneratedModel& gen)
 {
     FusedShape sh;
@@ -1380,7 +1384,7 @@ FusedShape fusedShape(const GeneratedModel& gen)
     sh.block[1] = get("CTPWA_MX_BLOCK", 256, 32, 1024);
     sh.minb[1] = get("CTPWA_MX_MINB", 2, 1, 16);
     sh.acc[0] = get("CTPWA_F64_ACC_SMEM", 1, 0, 1);
-    sh.acc[1] = get("CTPWA_MX_ACC_SMEM", 1, 0, 1);
+    sh.acc[1] = get("CTPWA_MX_ACC_SMEM", 0, 0, 1);
 
     for (int i = 0; i < 2; ++i)
         if (sh.block[i] % 32) throw std::runtime_error("fused block sizes must be multiples of 32");
@@ -1581,6 +1585,13 @@ double precompileConfig(const std::string& config_path)
     if (!cfg.valid()) throw std::runtime_error("analysis not initialized: invalid or missing config file \"" + config_path + "\"");
     Model m = buildModel(cfg, 1);
     GeneratedModel g = generateModel(m);
+    // CTPWA_MODEL_SOURCE_OUT=<file>: also write the generated model header
+    // (the CUDA source the kernels include) for inspection
+    if (const char* out = std::getenv("CTPWA_MODEL_SOURCE_OUT"); out && *out) {
+        std::ofstream f(out);
+        f << g.header;
+        if (!f) throw std::runtime_error(std::string("cannot write ") + out);
+    }
     bool hit = false;
     jitCubin(g, &hit);
     jitHvpCubin(g, &hit);

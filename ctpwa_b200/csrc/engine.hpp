@@ -25,7 +25,7 @@ struct FusedShape {
     int block[2] = {192, 256};
     int minb[2] = {2, 2};
     int stage[2] = {0, 0};
-    int acc[2] = {1, 1};  // per-thread gradient sums in shared memory
+    int acc[2] = {1, 0};  // per-thread gradient sums in shared memory
     int dsmem[2] = {0, 0};
 };
 FusedShape fusedShape(const GeneratedModel& gen);

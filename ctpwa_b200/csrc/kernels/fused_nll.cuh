@@ -66,7 +66,7 @@
 #define CT_F64_ACC 1
 #endif
 #ifndef CT_MX_ACC
-#define CT_MX_ACC 1
+#define CT_MX_ACC 0
 #endif
 #ifndef CT_WAIT_LIMIT
 #define CT_WAIT_LIMIT (1u << 22)
@@ -358,8 +358,11 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 // product with the FP32 coupling alone would bias the sample
                 // mean by ~1e-9 (both factors on the FP32 grid), which the
                 // normalisation term multiplies by the data weight sum.
-                cr[t] = fmaf(Fr[t], vr(a), Fr[t] * vrl(a)) - fmaf(Fi[t], vi(a), Fi[t] * vil(a));
-                ci[t] = fmaf(Fi[t], vr(a), Fi[t] * vrl(a)) + fmaf(Fr[t], vi(a), Fr[t] * vil(a));
+                // (the lo products first, then each hi product fused into
+                // the running sum: every rounding is of a sum that holds the
+                // full-precision coupling's products)
+                cr[t] = fmaf(Fr[t], vr(a), fmaf(-Fi[t], vi(a), fmaf(Fr[t], vrl(a), -Fi[t] * vil(a))));
+                ci[t] = fmaf(Fi[t], vr(a), fmaf(Fr[t], vi(a), fmaf(Fi[t], vrl(a), Fr[t] * vil(a))));
             } else {
                 cr[t] = (R)(vr(a) * Fr[t] - vi(a) * Fi[t]);
                 ci[t] = (R)(vr(a) * Fi[t] + vi(a) * Fr[t]);
