@@ -921,6 +921,9 @@ std::string Gen::emit()
             bool ok = true;
             int tfirst = -1;
             for (int y : users[x]) {
+                // event-only users are evaluated once per event, at load, from
+                // the FP64 value itself: only the per-call users read X'
+                if (evOnly(y)) continue;
                 const auto& yn = N[y];
                 const int other = yn.a == (int)x ? yn.b : yn.a;
                 if (!mixedDep(y) || (yn.op != dag::Sub && yn.op != dag::Add) || yn.a == yn.b || other < 0 ||
@@ -940,6 +943,7 @@ std::string Gen::emit()
             shiftR[x] = R;
             shifted[x] = 1;
             for (int y : users[x]) {
+                if (evOnly(y)) continue;
                 shiftUser[y] = 1;
                 dbl[y] = 0;
             }
