@@ -311,7 +311,7 @@ def streamed_bytes(layout, n_events, precision, paired=False):
 def toy_fit(args, device):
     """Toy-fit serving stream: Poisson arrivals of fit jobs (single-rho and
     three-chain rho models, N_data log-uniform 10k-200k, 10x phase space),
-    events generated on the GPU, L-BFGS-B to convergence (<= 100
+    events generated on the GPU, projected L-BFGS to convergence (<= 100
     evaluations) + exact Hessian each, 4 concurrent slots; latency
     percentiles per evaluation and per fit, mixed and FP64."""
     from ctpwa_b200 import serving
@@ -343,7 +343,8 @@ def toy_fit(args, device):
                                         "fit_ms_p50", "fit_ms_p99", "service_ms_p50", "service_ms_p99",
                                         "phase_ms_p50")}
     out["config"] = {"rate_per_s": args.toy_rate, "jobs": args.toy_jobs, "slots": 4, "n_data": "log-uniform 10k-200k",
-                     "n_phsp": "10 x n_data", "models": ["pipi_rho", "pipi_3rho"], "cuda_graphs": True}
+                     "n_phsp": "10 x n_data", "models": ["pipi_rho", "pipi_3rho"],
+                     "fit": "native projected L-BFGS (ctpwa_fit), GIL released"}
     return out
 
 

@@ -358,6 +358,56 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return v.value, g
 
+    def fit(self, start, lower=None, upper=None, free=None, max_evals=100, history=20, ftol=1e-13, gtol=1e-9,
+            precision=None, stream=None):
+        """Minimise the NLL from `start` (host array of all parameters) by the
+        library's projected limited-memory BFGS (``ctpwa_fit``), one
+        host-buffer evaluation per function call, the whole loop in native
+        code on this thread (the GIL is released meanwhile).
+
+        Defaults follow the reference's fit (example/fit.py:113-160): the
+        first coupling (real and imaginary part) stays fixed, the couplings are
+        unbounded and the free resonance parameters stay within their bounds
+        (getFreeResParams). `lower` / `upper` / `free` (length n_params)
+        replace those defaults. Returns (params, nll, evaluations, iterations,
+        status, eval_ms); status 0: projected gradient <= gtol, 1: relative
+        decrease <= ftol, 2: max_evals spent, 3: no decrease found."""
+        self._check()
+        import numpy as np
+
+        n = self._np
+        x = np.ascontiguousarray(np.asarray(start, dtype=np.float64)).copy()
+        if x.size != n:
+            raise RuntimeError(f"params size mismatch: got {x.size}, expected {n}")
+        nV = self.getNVector()
+        if lower is None or upper is None:
+            res = self.getFreeResParams().numpy()
+            lo = np.concatenate([np.full(2 * nV, -np.inf), res[1]])
+            hi = np.concatenate([np.full(2 * nV, np.inf), res[2]])
+            lower = lo if lower is None else lower
+            upper = hi if upper is None else upper
+        lo = np.ascontiguousarray(lower, dtype=np.float64)
+        hi = np.ascontiguousarray(upper, dtype=np.float64)
+        if free is None:
+            free = np.ones(n, dtype=np.uint8)
+            free[0] = free[nV] = 0
+        fr = np.ascontiguousarray(free, dtype=np.uint8)
+        if lo.size != n or hi.size != n or fr.size != n:
+            raise RuntimeError("fit: lower, upper and free need n_params entries")
+        out = np.zeros(4)
+        lat = np.zeros(max(1, int(max_evals)), dtype=np.float32)
+        dp = ctypes.POINTER(ctypes.c_double)
+        prec = self._precision if precision is None else self._parse_precision(precision)
+        sp = None if stream is None else ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
+        rc = self._lib.ctpwa_fit(self._h, x.ctypes.data_as(dp), fr.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                 lo.ctypes.data_as(dp), hi.ctypes.data_as(dp), prec, int(max_evals), int(history),
+                                 float(ftol), float(gtol), out.ctypes.data_as(dp),
+                                 lat.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), sp)
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        ne = int(out[1])
+        return x, float(out[0]), ne, int(out[2]), int(out[3]), lat[:min(ne, lat.size)].astype(np.float64).tolist()
+
     def getShardSums(self, params: torch.Tensor, precision=None) -> torch.Tensor:
         """This shard's per-sample sums (float64 CUDA, to be summed over shards
         with one all-reduce and passed to finalizeShardSums)."""

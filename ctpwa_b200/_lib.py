@@ -73,7 +73,17 @@ SIGNATURES = {
     "ctpwa_precompile": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.c_char_p,
                                         ctypes.c_size_t]),
     "ctpwa_version": (ctypes.c_char_p, []),
+    "ctpwa_fit": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.POINTER(ctypes.c_ubyte), _c_double_p,
+                                 _c_double_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_double, _c_double_p, ctypes.POINTER(ctypes.c_float), ctypes.c_void_p]),
+    "ctpwa_minimize_box": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _c_double_p,
+                                          ctypes.POINTER(ctypes.c_ubyte), _c_double_p, _c_double_p, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_double, ctypes.c_double, _c_double_p]),
 }
+
+# host function for ctpwa_minimize_box: fn(x, &f, g, user) -> status
+FG_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
 
 _lib = None
 

@@ -3,9 +3,11 @@
 #include "../../include/ctpwa_b200.h"
 
 #include "engine.hpp"
+#include "fit.hpp"
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -330,6 +332,62 @@ int ctpwa_nll_grad_host(ctpwa_handle* h, const double* params, double* nll, doub
     } catch (const std::exception& e) {
         return setErr(h, CTPWA_ERR_CUDA, e.what());
     }
+    return CTPWA_OK;
+}
+
+int ctpwa_fit(ctpwa_handle* h, double* params, const unsigned char* free_mask, const double* lo, const double* hi,
+              int precision, int max_evals, int history, double ftol, double gtol, double* out4, float* eval_ms,
+              void* stream)
+{
+    if (!h || !params || !free_mask || !lo || !hi || !out4) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (max_evals < 1 || history < 1) return setErr(h, CTPWA_ERR_ARG, "max_evals and history must be >= 1");
+    const int np = h->eng->nParams();
+    for (int i = 0; i < np; ++i)
+        if (!(lo[i] <= hi[i])) return setErr(h, CTPWA_ERR_ARG, "lower bound above upper bound");
+    ctpwa::BoxLbfgsOptions opt;
+    opt.max_evals = max_evals;
+    opt.m = history;
+    opt.ftol = ftol;
+    opt.gtol = gtol;
+    int ne = 0;
+    auto fg = [&](const double* x, double* f, double* g) -> int {
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = ctpwa_nll_grad_host(h, x, f, g, precision, stream);
+        if (eval_ms && ne < max_evals)
+            eval_ms[ne] = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        ++ne;
+        return rc;
+    };
+    ctpwa::BoxLbfgsResult r;
+    const int rc = ctpwa::boxLbfgs(fg, np, params, free_mask, lo, hi, opt, &r);
+    if (rc != 0) return rc;
+    out4[0] = r.f;
+    out4[1] = r.evals;
+    out4[2] = r.iters;
+    out4[3] = r.status;
+    return CTPWA_OK;
+}
+
+int ctpwa_minimize_box(ctpwa_fg_fn fn, void* user, int n, double* x, const unsigned char* free_mask, const double* lo,
+                       const double* hi, int max_evals, int history, double ftol, double gtol, double* out4)
+{
+    if (!fn || !x || !free_mask || !lo || !hi || !out4 || n < 1) return setErr(nullptr, CTPWA_ERR_ARG, "bad argument");
+    if (max_evals < 1 || history < 1) return setErr(nullptr, CTPWA_ERR_ARG, "max_evals and history must be >= 1");
+    for (int i = 0; i < n; ++i)
+        if (!(lo[i] <= hi[i])) return setErr(nullptr, CTPWA_ERR_ARG, "lower bound above upper bound");
+    ctpwa::BoxLbfgsOptions opt;
+    opt.max_evals = max_evals;
+    opt.m = history;
+    opt.ftol = ftol;
+    opt.gtol = gtol;
+    ctpwa::BoxLbfgsResult r;
+    const int rc = ctpwa::boxLbfgs([&](const double* xx, double* f, double* g) { return fn(xx, f, g, user); }, n, x,
+                                   free_mask, lo, hi, opt, &r);
+    if (rc != 0) return rc;
+    out4[0] = r.f;
+    out4[1] = r.evals;
+    out4[2] = r.iters;
+    out4[3] = r.status;
     return CTPWA_OK;
 }
 

@@ -3,9 +3,9 @@
 The workload pattern of the reference's fit driver (example/fit.py:115-216,
 600-650) as a service: jobs arrive over time (a Poisson stream), each brings
 its own seeded event sample (data by accept-reject against the model, 10x
-phase space, generated and kept on the GPU), runs a quasi-Newton fit
-(L-BFGS-B on the host, at most 100 NLL + gradient evaluations on the device)
-and ends with one exact Hessian.
+phase space, generated and kept on the GPU), runs a quasi-Newton fit (the
+library's projected limited-memory BFGS, at most 100 NLL + gradient
+evaluations on the device) and ends with one exact Hessian.
 
 * Admission by device memory: a job is admitted when a slot is free and its
   estimated resident bytes (event caches, from a per-model bytes-per-event
@@ -16,9 +16,9 @@ and ends with one exact Hessian.
   its own CUDA stream, so jobs that arrive while others are on the GPU start
   as soon as a slot and memory free up, and their kernels overlap on the
   device; the C ABI calls release the GIL.
-* Each job's evaluation (coupling map, parameter prologue, fused pass,
-  finalize) is captured once in a CUDA graph and replayed per evaluation,
-  which removes the launch cost that dominates small jobs.
+* Each job's fit loop runs in native code (``analysis.fit`` over
+  ``ctpwa_fit``) with the GIL released: the four slots' evaluations do not
+  queue behind one another's Python between device calls.
 * Latency is recorded per evaluation and per fit; `summary()` reports
   p50/p99 and fits/hour.
 
@@ -101,13 +101,12 @@ def poisson_stream(rate: float, n_jobs: int, models=("pipi_rho", "pipi_3rho"), n
 class Server:
     """Runs fit jobs on one GPU with `slots` concurrent jobs and a device-memory budget."""
 
-    def __init__(self, device: int = 0, slots: int = 4, budget_bytes: Optional[int] = None, graphs: bool = True,
+    def __init__(self, device: int = 0, slots: int = 4, budget_bytes: Optional[int] = None,
                  workdir: Optional[str] = None):
         import torch
 
         self.device = int(device)
         self.slots = int(slots)
-        self.graphs = graphs
         if budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             budget_bytes = int(0.6 * free)
@@ -115,7 +114,6 @@ class Server:
         base = workdir or ("/dev/shm" if os.path.isdir("/dev/shm") else None)
         self.workdir = tempfile.mkdtemp(prefix="ctpwa_serve_", dir=base)
         self._lock = threading.Lock()
-        self._capture_lock = threading.Lock()
         self._in_use = 0
         # one CUDA stream per slot, reused by the jobs that run in it and by
         # later servers of the process: the tensor allocator caches memory
@@ -226,74 +224,17 @@ class Server:
         return res
 
     def _fit(self, ana, start, spec: JobSpec, stream):
-        """L-BFGS-B on the host (bounds on the resonance parameters as the
-        reference's fit clamps them); every function call is one NLL +
-        gradient evaluation on the device: parameters in through pinned
-        memory, a CUDA-graph replay (when graphs are on), NLL and gradient
-        back in one copy."""
+        """The library's fit driver (``analysis.fit``: projected limited-memory
+        BFGS in native code, the GIL released, one host-buffer evaluation per
+        function call on the job's stream); the first coupling stays at its
+        start value (overall phase and scale of the couplings are not
+        measured: example/fit.py:48 fixes it) and the resonance parameters
+        within their bounds, as the reference's fit clamps them."""
         import torch
-        from scipy.optimize import minimize
 
-        dev = torch.device("cuda", self.device)
-        n = start.size
-        static_p = torch.tensor(start, dtype=torch.float64, device=dev)
-        out_dev = torch.empty(n + 1, dtype=torch.float64, device=dev)
-        pin_in = torch.empty(n, dtype=torch.float64).pin_memory()
-        pin_out = torch.empty(n + 1, dtype=torch.float64).pin_memory()
-
-        def device_eval():
-            nll, grad = ana.getNLLAndGrad(static_p)
-            out_dev[0] = nll
-            out_dev[1:] = grad
-
-        if self.graphs:
-            # warm-up on the capture stream, then capture one evaluation
-            for _ in range(2):
-                device_eval()
-            stream.synchronize()
-            graph = torch.cuda.CUDAGraph()
-            # capture restrictions apply to this thread only; captures are serialised
-            with self._capture_lock, torch.cuda.graph(graph, stream=stream, capture_error_mode="thread_local"):
-                device_eval()
-            run = graph.replay
-        else:
-            run = device_eval
-
-        lat = []
-
-        def evaluate(x):
-            t = time.perf_counter()
-            pin_in.numpy()[:] = x
-            static_p.copy_(pin_in, non_blocking=True)
-            run()
-            pin_out.copy_(out_dev, non_blocking=True)
-            stream.synchronize()
-            lat.append(1e3 * (time.perf_counter() - t))
-            r = pin_out.numpy()
-            return float(r[0]), r[1:].copy()
-
-        # the first coupling stays at its start value (overall phase and scale
-        # of the couplings are not measured: example/fit.py:48 fixes it)
-        nV = ana.getNVector()
-        free = np.ones(n, dtype=bool)
-        free[0] = False
-        free[nV] = False
-        lo_hi = ana.getFreeResParams().numpy()
-        bounds = [(None, None)] * (2 * nV) + [(float(l), float(h)) for l, h in zip(lo_hi[1], lo_hi[2])]
-        bounds = [b for b, f in zip(bounds, free) if f]
-        x_full = start.astype(np.float64).copy()
-
-        def fun(xf):
-            x_full[free] = xf
-            f, g = evaluate(x_full)
-            return f, g[free]
-
-        opt = minimize(fun, x_full[free], jac=True, method="L-BFGS-B", bounds=bounds,
-                       options={"maxfun": spec.max_evals, "maxcor": 20, "ftol": 1e-13, "gtol": 1e-9})
-        x_full[free] = opt.x
-        nll, _ = evaluate(x_full)
-        lat.pop()
-        return torch.tensor(x_full, dtype=torch.float64, device=dev), nll, len(lat), lat
+        x, nll, n_evals, _, _, lat = ana.fit(start, max_evals=spec.max_evals, history=20, ftol=1e-13, gtol=1e-9,
+                                             stream=stream)
+        return torch.tensor(x, dtype=torch.float64, device=torch.device("cuda", self.device)), nll, n_evals, lat
 
     # ----------------------------------------------------------- the stream
     def run(self, jobs: List[JobSpec], realtime: bool = True) -> List[JobResult]:
@@ -377,11 +318,10 @@ def main(argv=None):
     ap.add_argument("--nd-min", type=int, default=10_000)
     ap.add_argument("--nd-max", type=int, default=200_000)
     ap.add_argument("--precision", default="mixed")
-    ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--seed", type=int, default=17)
     a = ap.parse_args(argv)
-    srv = Server(device=a.device, slots=a.slots, graphs=not a.no_graphs)
+    srv = Server(device=a.device, slots=a.slots)
     try:
         # untimed jobs of the largest size first: one-time process costs
         # (library and kernel loading, the per-model memory figure, growth of
@@ -392,7 +332,7 @@ def main(argv=None):
         t = time.perf_counter()
         res = srv.run(jobs)
         out = summary(res, time.perf_counter() - t)
-        out.update({"rate_per_s": a.rate, "slots": a.slots, "precision": a.precision, "graphs": not a.no_graphs})
+        out.update({"rate_per_s": a.rate, "slots": a.slots, "precision": a.precision, "fit": "native projected L-BFGS"})
         print(json.dumps(out))
     finally:
         srv.close()

@@ -197,6 +197,28 @@ int ctpwa_finalize_sums(ctpwa_handle* h, const double* d_params, const double* d
  * copies NLL and gradient back, and synchronises the stream. */
 int ctpwa_nll_grad_host(ctpwa_handle* h, const double* params, double* nll, double* grad, int precision, void* stream);
 
+/* Fit driver: minimises the NLL over the parameters with free[i] != 0 within
+ * lo[i] <= p[i] <= hi[i] (host arrays of n_params; +-INFINITY for none) by
+ * projected limited-memory BFGS (history correction pairs), one evaluation
+ * through ctpwa_nll_grad_host per function call, on the calling thread and
+ * stream. Replaces the reference's fit loop, torch.optim.LBFGS over
+ * parameters clamped into their bounds with the gradient components that
+ * point out of an active bound zeroed (example/fit.py:113-200). params (host)
+ * holds the start and receives the best point found; out4 receives {nll at
+ * that point, evaluations, iterations, status}: status 0 projected gradient
+ * <= gtol, 1 relative decrease <= ftol, 2 max_evals spent, 3 no decrease
+ * along the search direction. eval_ms (optional, capacity max_evals)
+ * receives each evaluation's host latency in ms. */
+int ctpwa_fit(ctpwa_handle* h, double* params, const unsigned char* free_mask, const double* lo, const double* hi,
+              int precision, int max_evals, int history, double ftol, double gtol, double* out4, float* eval_ms,
+              void* stream);
+
+/* The same minimiser over a host function (no GPU): fn(x, &f, g, user)
+ * returns 0, or a nonzero code that ends the minimisation and is returned. */
+typedef int (*ctpwa_fg_fn)(const double* x, double* f, double* g, void* user);
+int ctpwa_minimize_box(ctpwa_fg_fn fn, void* user, int n, double* x, const unsigned char* free_mask, const double* lo,
+                       const double* hi, int max_evals, int history, double ftol, double gtol, double* out4);
+
 /* Per-sample parts of the last evaluation (host, synchronising):
  * [data_nll, bkg_nll, sum_phsp_intensity, W_data, W_bkg, n_phsp]. */
 int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream);

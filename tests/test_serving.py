@@ -72,3 +72,45 @@ def test_results_same_alone_and_in_the_mix():
         assert abs(a.nll - m.nll) <= 1e-12 * abs(a.nll), (a.job_id, a.nll, m.nll)
         assert np.allclose(a.params, m.params, rtol=1e-12, atol=0)
         assert np.allclose(a.hessian, m.hessian, rtol=1e-10, atol=1e-10 * np.max(np.abs(a.hessian)))
+
+
+@pytest.mark.gpu
+def test_native_fit_reaches_the_scipy_minimum(tmp_path):
+    """analysis.fit (projected L-BFGS in native code) from a perturbed start
+    ends at the minimum scipy's L-BFGS-B finds over the same host-buffer
+    evaluations, with every evaluation inside the resonance bounds."""
+    import numpy as np
+    from scipy.optimize import minimize
+
+    import ctpwa_b200
+    from ctpwa_b200 import workloads
+
+    cfg = workloads.make("pipi_3rho", tmp_path, n_phsp=60_000, n_data=6_000, n_bkg=0, seed=21)
+    ana = ctpwa_b200.analysis(cfg, precision="fp64")
+    nV = ana.getNVector()
+    res = ana.getFreeResParams().numpy()
+    start = workloads.true_params(nV, res[0])
+    rng = np.random.default_rng(5)
+    start[1:nV] *= 1 + 0.1 * rng.standard_normal(nV - 1)
+    start[nV + 1:2 * nV] *= 1 + 0.1 * rng.standard_normal(nV - 1)
+    start[2 * nV:] *= 1 + 0.003 * rng.standard_normal(start.size - 2 * nV)
+    x, nll, ne, it, status, lat = ana.fit(start, max_evals=300)
+    assert status in (0, 1) and ne <= 300 and len(lat) == ne
+    assert np.all(x[2 * nV:] >= res[1]) and np.all(x[2 * nV:] <= res[2])
+    assert x[0] == start[0] and x[nV] == start[nV]
+    assert abs(ana.getNLLHost(x)[0] - nll) == 0.0
+
+    free = np.ones(start.size, dtype=bool)
+    free[0] = free[nV] = False
+    bounds = [(None, None)] * (2 * nV) + [(float(lo), float(hi)) for lo, hi in zip(res[1], res[2])]
+    xf = start.copy()
+
+    def fun(v):
+        xf[free] = v
+        f, g = ana.getNLLHost(xf)
+        return f, g[free]
+
+    ref = minimize(fun, start[free], jac=True, method="L-BFGS-B", bounds=[b for b, f in zip(bounds, free) if f],
+                   options={"maxfun": 300, "maxcor": 20, "ftol": 1e-13, "gtol": 1e-9})
+    assert nll <= ref.fun + 1e-6 * max(1.0, abs(ref.fun)), (nll, ref.fun)
+    assert abs(nll - ref.fun) <= 1e-5 * max(1.0, abs(ref.fun)), (nll, ref.fun)
