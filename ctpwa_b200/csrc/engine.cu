@@ -30,6 +30,7 @@
 #include <cstring>
 #include <filesystem>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <fstream>
 #include <sstream>
@@ -628,6 +629,33 @@ std::string readFile(const std::string& p)
     return ss.str();
 }
 
+// Code generation is a pure function of the model, and the model of the
+// configuration text, its chain-filter patterns and its lineshape tables:
+// handles built from the same ones (a serving loop creates several per model)
+// share one generated model.
+GeneratedModel cachedGenerate(const Model& m, const std::string& config_path)
+{
+    std::string key = readFile(config_path);
+    for (const auto& c : m.cfg.chain_filter) key += "\n#chain " + c;
+    for (const auto& b : m.blocks)
+        for (const auto& r : b.res) {
+            key += "\n#aux ";
+            key.append((const char*)r.aux.data(), r.aux.size() * sizeof(double));
+        }
+    static std::mutex mu;
+    static std::map<std::string, std::shared_ptr<const GeneratedModel>> cache;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return *it->second;
+    }
+    auto g = std::make_shared<const GeneratedModel>(generateModel(m));
+    std::lock_guard<std::mutex> lk(mu);
+    if (cache.size() >= 32) cache.clear();
+    cache.emplace(key, g);
+    return *g;
+}
+
 std::string kernelDir()
 {
     const char* e = std::getenv("CTPWA_B200_KERNEL_DIR");
@@ -770,7 +798,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     for (const auto& b : model_.blocks)
         for (const auto& r : b.res)
             if (r.type == ModelType::Custom) checkCustomExpr(r.options.at("expr"), r.param_names);
-    gen_ = generateModel(model_);
+    gen_ = cachedGenerate(model_, config_path);
     int ndev = 0;
     CT_CUDA(cudaGetDeviceCount(&ndev));
     if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
@@ -1446,6 +1474,23 @@ std::string nvrtcCubin(const std::string& src, const std::vector<std::pair<std::
     key_src += std::to_string(nvmaj) + "." + std::to_string(nvmin);
     char key[32];
     std::snprintf(key, sizeof key, "%016llx", (unsigned long long)fnv1a(key_src));
+    // process-wide copy of the cubins already read or compiled, by the full
+    // key text (handles of one model share them)
+    static std::mutex mem_mu;
+    static std::map<std::string, std::string> mem;
+    {
+        std::lock_guard<std::mutex> lk(mem_mu);
+        auto it = mem.find(key_src);
+        if (it != mem.end()) {
+            if (cache_hit) *cache_hit = true;
+            return it->second;
+        }
+    }
+    auto remember = [&](const std::string& c) {
+        std::lock_guard<std::mutex> lk(mem_mu);
+        if (mem.size() >= 32) mem.clear();
+        mem.emplace(key_src, c);
+    };
     std::string cpath = cacheDir() + "/" + key + ".cubin";
     std::string cubin;
     {
@@ -1457,7 +1502,10 @@ std::string nvrtcCubin(const std::string& src, const std::vector<std::pair<std::
         }
     }
     if (cache_hit) *cache_hit = !cubin.empty();
-    if (!cubin.empty()) return cubin;
+    if (!cubin.empty()) {
+        remember(cubin);
+        return cubin;
+    }
     std::vector<const char*> hdr_src, hdr_names;
     for (const auto& h : headers) {
         hdr_names.push_back(h.first.c_str());
@@ -1489,6 +1537,7 @@ std::string nvrtcCubin(const std::string& src, const std::vector<std::pair<std::
         f.write(cubin.data(), (std::streamsize)cubin.size());
     }
     std::filesystem::rename(tmpp, cpath, ec);
+    remember(cubin);
     return cubin;
 }
 
