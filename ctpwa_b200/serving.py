@@ -54,6 +54,11 @@ class JobSpec:
     arrival: float = 0.0       # seconds after the stream starts
     max_evals: int = 100
     precision: str = "mixed"
+    # profile-likelihood scan after the fit: parameter `scan_param` fixed at
+    # the fitted value + s * sigma for each s in scan_sigmas (sigma from the
+    # job's Hessian), the other parameters refitted from the best fit
+    scan_param: int = -1
+    scan_sigmas: tuple = ()
 
 
 @dataclass
@@ -74,8 +79,10 @@ class JobResult:
     finished: float = 0.0
     error: Optional[str] = None
     # phases of the service time (ms): toy-MC generation, handle creation
-    # (model, kernels, angular pass), fit, Hessian
+    # (model, kernels, angular pass), fit, Hessian, scan
     phase_ms: dict = field(default_factory=dict)
+    # profile scan: (parameter value, NLL - best-fit NLL) per point
+    scan: List[tuple] = field(default_factory=list)
 
     @property
     def fit_latency(self) -> float:
@@ -207,6 +214,9 @@ class Server:
                 t5 = time.perf_counter()
                 res.phase_ms = {"generate": 1e3 * (t2 - t1), "handle": 1e3 * (t3 - t2), "fit": 1e3 * (t4 - t3),
                                 "hessian": 1e3 * (t5 - t4)}
+                if spec.scan_param >= 0 and spec.scan_sigmas:
+                    res.scan = self._scan(ana, p.cpu().numpy(), nll, H.cpu().numpy(), spec, stream)
+                    res.phase_ms["scan"] = 1e3 * (time.perf_counter() - t5)
                 res.phase_ms.update({"generate." + k: v for k, v in gen_ms.items()})
                 res.params = p.cpu().numpy()
                 res.hessian = H.cpu().numpy()
@@ -235,6 +245,34 @@ class Server:
         x, nll, n_evals, _, _, lat = ana.fit(start, max_evals=spec.max_evals, history=20, ftol=1e-13, gtol=1e-9,
                                              stream=stream)
         return torch.tensor(x, dtype=torch.float64, device=torch.device("cuda", self.device)), nll, n_evals, lat
+
+    @staticmethod
+    def _scan(ana, best, nll_best, H, spec: JobSpec, stream):
+        """Profile-likelihood scan of parameter spec.scan_param around the
+        fit: sigma from the inverse Hessian over the free parameters, one
+        refit (parameter fixed) per point, started from the best fit."""
+        nV = ana.getNVector()
+        n = best.size
+        i = int(spec.scan_param)
+        if not 0 <= i < n or i in (0, nV):
+            raise ValueError(f"scan_param {i} is not a free parameter")
+        free = np.ones(n, dtype=bool)
+        free[0] = free[nV] = False
+        idx = np.flatnonzero(free)
+        cov = np.linalg.inv(H[np.ix_(idx, idx)])
+        sigma = float(np.sqrt(cov[np.searchsorted(idx, i), np.searchsorted(idx, i)]))
+        res = ana.getFreeResParams().numpy()
+        lo = np.concatenate([np.full(2 * nV, -np.inf), res[1]])
+        hi = np.concatenate([np.full(2 * nV, np.inf), res[2]])
+        fr = free.astype(np.uint8)
+        fr[i] = 0
+        out = []
+        for s_ in spec.scan_sigmas:
+            x0 = best.copy()
+            x0[i] = min(max(best[i] + float(s_) * sigma, lo[i]), hi[i])
+            _, f, _, _, _, _ = ana.fit(x0, lower=lo, upper=hi, free=fr, max_evals=spec.max_evals, stream=stream)
+            out.append((float(x0[i]), f - nll_best))
+        return out
 
     # ----------------------------------------------------------- the stream
     def run(self, jobs: List[JobSpec], realtime: bool = True) -> List[JobResult]:
@@ -320,6 +358,8 @@ def main(argv=None):
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--seed", type=int, default=17)
+    ap.add_argument("--scan-param", type=int, default=-1,
+                    help="after each fit, profile-scan this parameter index at +-1, +-2 sigma")
     a = ap.parse_args(argv)
     srv = Server(device=a.device, slots=a.slots)
     try:
@@ -329,6 +369,9 @@ def main(argv=None):
         srv.run([JobSpec(job_id=-1 - i, model=("pipi_rho", "pipi_3rho")[i % 2], n_data=a.nd_max, n_phsp=10 * a.nd_max,
                          seed=90 + i, max_evals=5, precision=a.precision) for i in range(a.slots)], realtime=False)
         jobs = poisson_stream(a.rate, a.jobs, nd_range=(a.nd_min, a.nd_max), precision=a.precision, seed=a.seed)
+        if a.scan_param >= 0:
+            for j in jobs:
+                j.scan_param, j.scan_sigmas = a.scan_param, (-2.0, -1.0, 1.0, 2.0)
         t = time.perf_counter()
         res = srv.run(jobs)
         out = summary(res, time.perf_counter() - t)

@@ -114,3 +114,27 @@ def test_native_fit_reaches_the_scipy_minimum(tmp_path):
                    options={"maxfun": 300, "maxcor": 20, "ftol": 1e-13, "gtol": 1e-9})
     assert nll <= ref.fun + 1e-6 * max(1.0, abs(ref.fun)), (nll, ref.fun)
     assert abs(nll - ref.fun) <= 1e-5 * max(1.0, abs(ref.fun)), (nll, ref.fun)
+
+
+@pytest.mark.gpu
+def test_profile_scan_is_parabolic_near_the_minimum():
+    """Profile-likelihood scan (the other parameters refitted at each point):
+    at the fitted value +- 1 and 2 sigma (sigma from the exact Hessian) the
+    NLL rises by about s^2 / 2, and never falls below the best fit."""
+    nV = 1  # pipi_rho: one coupling; parameter 2 is the rho mass, 3 its width
+    jobs = [serving.JobSpec(job_id=0, model="pipi_rho", n_data=40_000, n_phsp=400_000, seed=31, max_evals=300,
+                            precision="fp64", scan_param=2 * nV, scan_sigmas=(-2.0, -1.0, 1.0, 2.0)),
+            serving.JobSpec(job_id=1, model="pipi_rho", n_data=40_000, n_phsp=400_000, seed=31, max_evals=300,
+                            precision="fp64", scan_param=2 * nV + 1, scan_sigmas=(-1.0, 1.0))]
+    srv = serving.Server(slots=2)
+    try:
+        res = srv.run(jobs, realtime=False)
+    finally:
+        srv.close()
+    for r, spec in zip(res, jobs):
+        assert r.error is None, r.error
+        assert len(r.scan) == len(spec.scan_sigmas) and "scan" in r.phase_ms
+        for (v, dnll), s in zip(r.scan, spec.scan_sigmas):
+            assert dnll > -1e-6, (v, dnll)
+            assert abs(dnll - 0.5 * s * s) <= 0.15 * s * s, (s, dnll)
+        assert r.scan[0][0] < r.params[spec.scan_param] < r.scan[-1][0]
