@@ -1577,11 +1577,12 @@ int hvpBlock(const GeneratedModel& gen)
 }
 
 // The Hessian-vector-product kernels of one generated model.
-std::string jitHvpCubin(const GeneratedModel& gen, bool* cache_hit)
+std::string jitHvpCubin(const GeneratedModel& gen, bool paired, bool* cache_hit)
 {
     std::string dir = kernelDir();
     std::vector<std::string> optv = kNvrtcBase;
     optv.push_back("-DCT_HVP_BLOCK=" + std::to_string(hvpBlock(gen)));
+    optv.push_back(std::string("-DCT_HVP_PAIRED=") + (paired ? "1" : "0"));
     return nvrtcCubin("#include \"hessian.cuh\"\n",
                       {{"device_helpers.cuh", readFile(dir + "/device_helpers.cuh")},
                        {"hessian.cuh", readFile(dir + "/hessian.cuh")},
@@ -1643,7 +1644,7 @@ double precompileConfig(const std::string& config_path)
     }
     bool hit = false;
     jitCubin(g, &hit);
-    jitHvpCubin(g, &hit);
+    jitHvpCubin(g, false, &hit);
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
@@ -2173,7 +2174,7 @@ void Engine::compileHvp()
 {
     if (k_hvp_) return;
     bool hit = false;
-    std::string cubin = jitHvpCubin(gen_, &hit);
+    std::string cubin = jitHvpCubin(gen_, paired_[0], &hit);
     cudaLibrary_t lib;
     CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
     hvp_lib_ = (void*)lib;
@@ -2225,7 +2226,7 @@ void Engine::hvpSums(const double* d_params, const double* d_dirs, int ndir, dou
         if (hlay_.cta[k][1] == 0) continue;
         CtHvpSampleH& sm = a.s[ns++];
         const DeviceSample& d = samples_[k];
-        sm.slamp = d.slamp64;
+        sm.slamp = paired_[0] ? d.slamp64p : d.slamp64;
         sm.ev = d.ev64;
         sm.w = d.w;
         sm.n = d.n;

@@ -102,6 +102,11 @@ __device__ __forceinline__ double ct_value(CtDual x) { return x.v; }
 #ifndef CT_HVP_BLOCK
 #define CT_HVP_BLOCK 128
 #endif
+// paired polarisations (SL_{c,NPOL-1-p} = conj(SL_{c,p}) on every event): the
+// tables hold polarisations 0 .. (M_NPOL+1)/2 - 1 only, [plane][p][ld]
+#ifndef CT_HVP_PAIRED
+#define CT_HVP_PAIRED 0
+#endif
 
 #define CT_HNACC (2 + 2 * M_NA + M_NTH)
 #define CT_HCONST_ALLOC (M_NCONST > 0 ? M_NCONST : 1)
@@ -213,9 +218,10 @@ extern "C" __global__ void __launch_bounds__(CT_HVP_BLOCK) ct_hvp_f64(CtHvpArgs 
             FT Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
             if constexpr (CtSame<FT, CtDual>::value) model_columns_dual(ev, sC, Fr, Fi, dFr, dFi);
             else model_columns(ev, sCv, Fr, Fi, dFr, dFi);
-            double2 sl[M_NPLANE * M_NPOL];
+            constexpr int NPS = CT_HVP_PAIRED ? (M_NPOL + 1) / 2 : M_NPOL;
+            double2 sl[M_NPLANE * NPS];
 #pragma unroll
-            for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = __ldg(S.slamp + (long long)c * ld + e);
+            for (int c = 0; c < M_NPLANE * NPS; ++c) sl[c] = __ldg(S.slamp + (long long)c * ld + e);
             CtDual cr[M_NTERM], ci[M_NTERM];
 #pragma unroll
             for (int t = 0; t < M_NTERM; ++t) {
@@ -224,20 +230,39 @@ extern "C" __global__ void __launch_bounds__(CT_HVP_BLOCK) ct_hvp_f64(CtHvpArgs 
                 ci[t] = vr[a] * Fi[t] + vi[a] * Fr[t];
             }
             CtDual Sr[M_NPOL], Si[M_NPOL];
+#pragma unroll
+            for (int p = 0; p < NPS; ++p) {
+                const int q = M_NPOL - 1 - p;
+                if (CT_HVP_PAIRED && q != p) {
+                    // S_p = sum c (x + iy), S_q = sum c (x - iy) from the same products
+                    CtDual xr(0.0), yi(0.0), yr(0.0), xi(0.0);
+#pragma unroll
+                    for (int t = 0; t < M_NTERM; ++t) {
+                        const double2 x = sl[term_plane(t) * NPS + p];
+                        xr += cr[t] * x.x;
+                        yi += ci[t] * x.y;
+                        yr += cr[t] * x.y;
+                        xi += ci[t] * x.x;
+                    }
+                    Sr[p] = xr - yi;
+                    Si[p] = yr + xi;
+                    Sr[q] = xr + yi;
+                    Si[q] = xi - yr;
+                } else {
+                    CtDual sr(0.0), sim(0.0);
+#pragma unroll
+                    for (int t = 0; t < M_NTERM; ++t) {
+                        const double2 x = sl[term_plane(t) * NPS + p];
+                        sr += cr[t] * x.x - ci[t] * x.y;
+                        sim += cr[t] * x.y + ci[t] * x.x;
+                    }
+                    Sr[p] = sr;
+                    Si[p] = sim;
+                }
+            }
             CtDual f(0.0);
 #pragma unroll
-            for (int p = 0; p < M_NPOL; ++p) {
-                CtDual sr(0.0), sim(0.0);
-#pragma unroll
-                for (int t = 0; t < M_NTERM; ++t) {
-                    const double2 x = sl[term_plane(t) * M_NPOL + p];
-                    sr += cr[t] * x.x - ci[t] * x.y;
-                    sim += cr[t] * x.y + ci[t] * x.x;
-                }
-                Sr[p] = sr;
-                Si[p] = sim;
-                f += sr * sr + sim * sim;
-            }
+            for (int p = 0; p < M_NPOL; ++p) f += Sr[p] * Sr[p] + Si[p] * Si[p];
             CtDual ur[M_NPOL], ui[M_NPOL];
             double gscale, tscale;
             const double we = S.w ? __ldg(S.w + e) : 1.0;
@@ -262,15 +287,32 @@ extern "C" __global__ void __launch_bounds__(CT_HVP_BLOCK) ct_hvp_f64(CtHvpArgs 
                 gscale = -1.0;
                 tscale = -2.0;
             }
+            // (paired: conj(SL_p) u_p + SL_p u_q = x (u_p + u_q) + iy (u_q - u_p))
+            CtDual ar[NPS], br[NPS], ai[NPS], bi[NPS];
+#pragma unroll
+            for (int p = 0; p < NPS; ++p) {
+                const int q = M_NPOL - 1 - p;
+                if (CT_HVP_PAIRED && q != p) {
+                    ar[p] = ur[p] + ur[q];
+                    br[p] = ui[p] - ui[q];
+                    ai[p] = ui[p] + ui[q];
+                    bi[p] = ur[q] - ur[p];
+                } else {
+                    ar[p] = ur[p];
+                    br[p] = ui[p];
+                    ai[p] = ui[p];
+                    bi[p] = -ur[p];
+                }
+            }
             CtDual Tr[M_NPLANE], Ti[M_NPLANE];
 #pragma unroll
             for (int c = 0; c < M_NPLANE; ++c) {
                 CtDual tr(0.0), ti(0.0);
 #pragma unroll
-                for (int p = 0; p < M_NPOL; ++p) {
-                    const double2 x = sl[c * M_NPOL + p];
-                    tr += x.x * ur[p] + x.y * ui[p];
-                    ti += x.x * ui[p] - x.y * ur[p];
+                for (int p = 0; p < NPS; ++p) {
+                    const double2 x = sl[c * NPS + p];
+                    tr += x.x * ar[p] + x.y * br[p];
+                    ti += x.x * ai[p] + x.y * bi[p];
                 }
                 Tr[c] = tr;
                 Ti[c] = ti;
