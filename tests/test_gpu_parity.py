@@ -431,3 +431,74 @@ def test_polarisation_pairing(tmp_path, monkeypatch):
     orc = Oracle(cfg)
     onll, og, _ = orc.nll_grad(p)
     assert abs(float(n1) - onll) <= 1e-10 * abs(onll)
+
+
+def _weighted_config(tmp_path, n_phsp, n_data, n_bkg, seed, short_bkg=False):
+    """kkpi config with per-event weight files for data, phase space and
+    background (.dat, one value per event; with short_bkg the background file
+    lists fewer values than events, which the reader pads with zeros)."""
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=n_phsp, n_data=n_data, n_bkg=n_bkg, accept_reject=False, seed=seed,
+                         gpu_generator=False)
+    rng = np.random.default_rng(seed + 100)
+    lines = []
+    for key, n, lo, hi in (("data_weights", n_data, 0.5, 1.5), ("phsp_weights", n_phsp, 0.8, 1.2),
+                           ("bkg_weights", n_bkg - 3 if short_bkg else n_bkg, 0.1, 0.5)):
+        if n <= 0 and key == "bkg_weights" and n_bkg == 0:
+            continue
+        f = tmp_path / f"{key}.dat"
+        np.savetxt(f, rng.uniform(lo, hi, max(n, 0)))
+        lines.append(f'  {key}: [dat, "{f}"]')
+    text = open(cfg).read()
+    text = "\n".join(l for l in text.splitlines() if not l.strip().startswith("bkg_weights:"))
+    text = text.replace("Data:\n", "Data:\n" + "\n".join(lines) + "\n", 1)
+    open(cfg, "w").write(text + "\n")
+    return cfg
+
+
+@pytest.mark.parametrize("short_bkg", [False, True])
+def test_per_event_weight_files(tmp_path, short_bkg):
+    """Per-event weights from .dat files for data, phase space (weighted
+    normalisation) and background, against the oracle reading the same
+    files; a background weight file shorter than the sample is padded with
+    zeros as the reference's reader does."""
+    import torch
+    import ctpwa_b200
+
+    cfg = _weighted_config(tmp_path, 20_011, 3_001, 507, seed=41, short_bkg=short_bkg)
+    ana = ctpwa_b200.analysis(cfg)
+    orc = Oracle(cfg)
+    p = workloads.true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    onll, og, _ = orc.nll_grad(p)
+    nll, g = ana.getNLLAndGrad(pt, "fp64")
+    assert abs(float(nll) - onll) <= 1e-10 * max(1.0, abs(onll)), (float(nll), onll)
+    assert np.max(np.abs(g.cpu().numpy() - og)) <= 1e-9 * np.max(np.abs(og))
+    nmx, gmx = ana.getNLLAndGrad(pt, "mixed")
+    assert abs(float(nmx) - onll) < 1e-3
+    assert np.max(np.abs(gmx.cpu().numpy() - og)) <= 1e-4 * np.max(np.abs(og))
+
+
+@pytest.mark.parametrize("sizes", [(1, 1, 0), (33, 5, 1), (257, 31, 2), (1000, 1, 0)])
+def test_tiny_and_ragged_samples(tmp_path, sizes):
+    """Samples of one event and sizes off every tile boundary: FP64 against
+    the oracle, the mixed form within its bar, the exact Hessian symmetric."""
+    import torch
+    import ctpwa_b200
+
+    n_phsp, n_data, n_bkg = sizes
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=n_phsp, n_data=n_data, n_bkg=n_bkg, accept_reject=False, seed=43,
+                         gpu_generator=False)
+    ana = ctpwa_b200.analysis(cfg)
+    orc = Oracle(cfg)
+    assert ana.getNEvents() == orc.nev
+    p = workloads.true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    onll, og, _ = orc.nll_grad(p)
+    nll, g = ana.getNLLAndGrad(pt, "fp64")
+    assert abs(float(nll) - onll) <= 1e-10 * max(1.0, abs(onll)), (float(nll), onll)
+    assert np.max(np.abs(g.cpu().numpy() - og)) <= 1e-9 * max(1e-300, np.max(np.abs(og)))
+    nmx, _ = ana.getNLLAndGrad(pt, "mixed")
+    assert abs(float(nmx) - onll) < 1e-3
+    H = ana.getHessian(pt).cpu().numpy()
+    assert np.all(np.isfinite(H))
+    assert np.max(np.abs(H - H.T)) <= 1e-9 * max(1e-300, np.max(np.abs(H)))
