@@ -955,6 +955,32 @@ std::string Gen::emit()
             else fsD[x] = out.nevd++;
         }
     }
+    // The parameter-only part of every shifted use, T - R (T + R for an
+    // addition), becomes a constant of its own, set at the end of the
+    // prologue: its FP32 hi + lo then come with the constant bank, and the
+    // per-event code adds no FP64 arithmetic or conversion for it.
+    std::vector<int> shiftSlot(N.size(), -1);
+    std::string shiftPro;
+    {
+        std::map<std::tuple<int, bool, double>, int> seen;
+        for (size_t y = 0; y < N.size(); ++y) {
+            if (!shiftUser[y]) continue;
+            const auto& nd = N[y];
+            const bool xa = shifted[nd.a] != 0;
+            const int xs = xa ? nd.a : nd.b, t = xa ? nd.b : nd.a;
+            const bool add = nd.op == dag::Add;
+            if (cslot[t] < 0) throw std::logic_error("codegen: shifted use without a constant slot");
+            const auto key = std::make_tuple(cslot[t], add, shiftR[xs]);
+            auto it = seen.find(key);
+            if (it == seen.end()) {
+                it = seen.emplace(key, ncon++).first;
+                shiftPro += "  C[" + std::to_string(it->second) + "] = C[" + std::to_string(cslot[t]) + "]" +
+                            (add ? " + " : " - ") + num(shiftR[xs]) + ";\n";
+            }
+            shiftSlot[y] = it->second;
+        }
+    }
+    pro << shiftPro;
     using RefFn = std::function<std::string(int, bool)>;
     // reference to a kinematic leaf, a table lookup or an event node from the
     // once-per-event code, for a consumer evaluated in FP32 (wantF) or FP64
@@ -1022,14 +1048,15 @@ std::string Gen::emit()
             // T - X, X - T or T + X from the shifted FP32 value X' = X - R
             const bool xa = shifted[nd.a] != 0;
             const int xs = xa ? nd.a : nd.b, t = xa ? nd.b : nd.a;
-            const std::string T = ref(t, false), Xs = "evf[" + std::to_string(fsF[xs]) + "]",
-                              R = num(shiftR[xs]);
-            // the parameter-only part enters as hi + lo (a single FP32
-            // rounding of it would shift every event alike)
+            (void)t;
+            const std::string Xs = "evf[" + std::to_string(fsF[xs]) + "]", ks = std::to_string(shiftSlot[x]),
+                              Dh = "Cfh[" + ks + "]", Dl = "Cfl[" + ks + "]";
+            // the parameter-only part D = T -+ R enters as hi + lo (a single
+            // FP32 rounding of it would shift every event alike)
             std::string rhs;
-            if (nd.op == dag::Add) rhs = "ct_split_add(" + T + " + " + R + ", " + Xs + ")";
-            else if (xa) rhs = "-ct_split_sub(" + T + " - " + R + ", " + Xs + ")";  // X - T
-            else rhs = "ct_split_sub(" + T + " - " + R + ", " + Xs + ")";         // T - X
+            if (nd.op == dag::Add) rhs = "(" + Dh + " + " + Xs + ") + " + Dl;     // (T + R) + X'
+            else if (xa) rhs = "-((" + Dh + " - " + Xs + ") + " + Dl + ")";      // X - T
+            else rhs = "(" + Dh + " - " + Xs + ") + " + Dl;                      // (T - R) - X'
             return "  const float e" + std::to_string(x) + " = " + rhs + ";\n";
         }
         bool isF = f32 && !dbl[x];
@@ -1165,6 +1192,7 @@ std::string Gen::emit()
             if (N[x].op != dag::Theta) dpro << "  const CtDual t" << x << " = " << rhs(N[x], proRef) << ";\n";
             if (cslot[x] >= 0) dpro << "  C[" << cslot[x] << "] = " << proRef((int)x) << ";\n";
         }
+        dpro << shiftPro;
         for (size_t x = 0; x < N.size(); ++x) {
             const auto& nd = N[x];
             if (!live[x] || !mixedDep((int)x) || nd.op == dag::Const || nd.op == dag::Theta || nd.op == dag::Kin) continue;
