@@ -83,6 +83,12 @@ int Graph::add(int a, int b)
     if (isConst(a) && isConst(b)) return cnst(val(a) + val(b));
     if (isConst(a) && val(a) == 0.0) return b;
     if (isConst(b) && val(b) == 0.0) return a;
+    // x + x for a product x with a parameter-only factor: the 2 joins that
+    // factor (2 c is a per-call constant; doubling is exact either way)
+    if (a == b && nodes[a].op == Mul && nodes[a].dep == (DEP_THETA | DEP_EVENT)) {
+        auto pOnly = [&](int x) { return nodes[x].dep == DEP_THETA || nodes[x].dep == DEP_NONE; };
+        if (pOnly(nodes[a].a) || pOnly(nodes[a].b)) return mul(cnst(2.0), a);
+    }
     if (a > b) std::swap(a, b);
     Node n;
     n.op = Add;
