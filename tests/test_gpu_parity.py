@@ -502,3 +502,51 @@ def test_tiny_and_ragged_samples(tmp_path, sizes):
     H = ana.getHessian(pt).cpu().numpy()
     assert np.all(np.isfinite(H))
     assert np.max(np.abs(H - H.T)) <= 1e-9 * max(1e-300, np.max(np.abs(H)))
+
+
+def _features_config(tmp_path, n_phsp=20_011, n_data=3_001):
+    """tests/golden/features.yml (trans folding, var_range, gauss_constr,
+    fix_var, a multi-mode intermediate, an expanded chain) over seeded
+    K+ K- eta phase-space samples written next to it."""
+    import os
+    import shutil
+
+    from ctpwa_b200 import toymc
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    cfg = tmp_path / "config.yml"
+    shutil.copy(os.path.join(here, "golden", "features.yml"), cfg)
+    masses = [0.493677, 0.493677, 0.547862]
+    toymc.write_npy(tmp_path / "phsp.npy", toymc.phase_space(3.0969, masses, n_phsp, 51))
+    toymc.write_npy(tmp_path / "data.npy", toymc.phase_space(3.0969, masses, n_data, 52))
+    return str(cfg)
+
+
+def test_feature_config_parity(tmp_path, monkeypatch):
+    """The feature config evaluated on the device against the oracle: FP64
+    NLL and gradient (folded couplings, Gaussian constraint, fixed and
+    range-limited parameters), the mixed form, and the exact Hessian against
+    Richardson differences of the oracle's gradient."""
+    import torch
+    import ctpwa_b200
+
+    monkeypatch.chdir(tmp_path)  # the config names its samples relative to its directory
+    cfg = _features_config(tmp_path)
+    ana = ctpwa_b200.analysis(cfg)
+    assert ana.isValid()
+    orc = Oracle(cfg)
+    assert ana.getNVector() == orc.nV and ana.getNFreeTheta() == orc.nT
+    p = workloads.true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
+    rng = np.random.default_rng(9)
+    p[2 * ana.getNVector():] *= 1 + 0.01 * rng.standard_normal(ana.getNFreeTheta())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    onll, og, _ = orc.nll_grad(p)
+    nll, g = ana.getNLLAndGrad(pt, "fp64")
+    assert abs(float(nll) - onll) <= 1e-10 * max(1.0, abs(onll)), (float(nll), onll)
+    assert np.max(np.abs(g.cpu().numpy() - og)) <= 1e-9 * np.max(np.abs(og))
+    nmx, gmx = ana.getNLLAndGrad(pt, "mixed")
+    assert abs(float(nmx) - onll) < 1e-3
+    assert np.max(np.abs(gmx.cpu().numpy() - og)) <= 1e-4 * np.max(np.abs(og))
+    H = ana.getHessian(pt).cpu().numpy()
+    Ho = orc.hessian_fd(p)
+    assert np.max(np.abs(H - Ho)) <= 1e-6 * np.max(np.abs(Ho)), np.max(np.abs(H - Ho)) / np.max(np.abs(Ho))
