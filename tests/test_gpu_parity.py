@@ -550,3 +550,60 @@ def test_feature_config_parity(tmp_path, monkeypatch):
     H = ana.getHessian(pt).cpu().numpy()
     Ho = orc.hessian_fd(p)
     assert np.max(np.abs(H - Ho)) <= 1e-6 * np.max(np.abs(Ho)), np.max(np.abs(H - Ho)) / np.max(np.abs(Ho))
+
+
+_SHAPES = {
+    "bw_gs_hist_flatte": """Resonances:
+  Kst892:    {J: 1, P: -1, model: BW, parameters: [0.8955, 0.047], free: [0, 1]}
+  Kst1410:   {J: 1, P: -1, model: GS, parameters: [1.414, 0.232], free: [0, 1]}
+  Kst2_1430: {J: 2, P: 1, model: Hist, file: "@DIR@/hist.dat", bins: 40, range: [0.6, 2.7]}
+  X1680: {J: 1, P: -1, model: Flatte, parameters: [1.68, 0.3, 0.1], free: [0, 1, 2], channels: [[0.493677, 0.493677], [0.13957, 0.13957]]}
+""",
+    "interp": """Resonances:
+  Kst892:    {J: 1, P: -1, model: BWR, parameters: [0.8955, 0.047], free: [0, 1]}
+  Kst1410:   {J: 1, P: -1, model: Interp, file: "@DIR@/interp.dat"}
+  Kst2_1430: {J: 2, P: 1, model: BWR, parameters: [1.4256, 0.0985], free: [0, 1]}
+  X1680: {J: 1, P: -1, model: BWR, parameters: [1.68, 0.15], free: [0, 1]}
+""",
+}
+
+
+def _shapes_config(tmp_path, variant):
+    """K+K-pi0 chains with the other built-in lineshapes: BW, GS, a histogram
+    (Hist), Flatte with channels, a complex interpolation table (Interp)."""
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=20_011, n_data=3_001, n_bkg=0, accept_reject=False, seed=61,
+                         gpu_generator=False)
+    x = np.linspace(0.6, 2.7, 40)
+    np.savetxt(tmp_path / "hist.dat", 1.0 + 0.5 * np.sin(3 * x))
+    xi = np.linspace(0.55, 2.75, 60)
+    np.savetxt(tmp_path / "interp.dat", np.c_[xi, np.cos(2 * xi) / (1 + xi), np.sin(xi) / (1 + xi)])
+    text = open(cfg).read()
+    text = text[:text.index("Resonances:")] + _SHAPES[variant].replace("@DIR@", str(tmp_path))
+    open(cfg, "w").write(text)
+    return cfg
+
+
+@pytest.mark.parametrize("variant", list(_SHAPES))
+def test_builtin_lineshapes_parity(tmp_path, variant):
+    """BW, GS, Hist, Flatte and Interp lineshapes in the fused kernels: FP64
+    NLL and gradient against the oracle, the mixed form within its bar."""
+    import torch
+    import ctpwa_b200
+
+    cfg = _shapes_config(tmp_path, variant)
+    ana = ctpwa_b200.analysis(cfg)
+    assert ana.isValid()
+    orc = Oracle(cfg)
+    assert ana.getNVector() == orc.nV and ana.getNFreeTheta() == orc.nT
+    p = workloads.true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
+    p[2 * ana.getNVector():] *= 1 + 0.01 * np.random.default_rng(3).standard_normal(ana.getNFreeTheta())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    onll, og, _ = orc.nll_grad(p)
+    nll, g = ana.getNLLAndGrad(pt, "fp64")
+    assert abs(float(nll) - onll) <= 1e-10 * max(1.0, abs(onll)), (float(nll), onll)
+    assert np.max(np.abs(g.cpu().numpy() - og)) <= 1e-9 * np.max(np.abs(og))
+    nmx, gmx = ana.getNLLAndGrad(pt, "mixed")
+    assert abs(float(nmx) - onll) < 1e-3
+    assert np.max(np.abs(gmx.cpu().numpy() - og)) <= 1e-4 * np.max(np.abs(og))
+    H = ana.getHessian(pt).cpu().numpy()
+    assert np.max(np.abs(H - H.T)) <= 1e-9 * np.max(np.abs(H))
