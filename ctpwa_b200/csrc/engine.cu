@@ -1394,7 +1394,8 @@ void Engine::buildEventCache(int kind)
 // (frontier values by asynchronous copies, constants in the constant bank,
 // paired polarisations) 256 x 2 with the sums in registers 0.4125 ms,
 // against 0.4214 ms in shared memory (0.583 ms with each add a
-// shared-memory atomic); before the pairing, with 12 more live registers,
+// shared-memory atomic); later, at 0.399 ms for 256 x 2: 128 x 4 0.416 ms,
+// 192 x 2 0.421 ms, 128 x 3 0.450 ms, 224 x 2 0.453 ms, 288 x 2 0.490 ms; before the pairing, with 12 more live registers,
 // the shared-memory sums were ahead (0.491 against 0.51 ms), and 3 CTAs per
 // SM ran 0.77 ms, 128 x 4 0.55 ms.
 FusedShape fusedShape(const GeneratedModel& gen)
