@@ -21,7 +21,7 @@ NVCC = str(CUDA / "bin" / "nvcc")
 HOSTCXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-HOST_SRCS = ["yaml_lite.cpp", "config.cpp", "model.cpp", "dataio.cpp", "exprdag.cpp", "codegen.cpp", "fit.cpp",
+HOST_SRCS = ["yaml_lite.cpp", "config.cpp", "model.cpp", "dataio.cpp", "exprdag.cpp", "lineshape_lang.cpp", "codegen.cpp", "fit.cpp",
              "capi.cpp"]
 CUDA_SRCS = ["engine.cu", "toymc.cu"]
 

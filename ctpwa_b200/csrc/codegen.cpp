@@ -3,12 +3,14 @@
 // Lineshape assembly follows the reference kernels:
 //   per-call blocks  src/AmpGen.cu:1593-1932 (computeCustomAmpsKernelT), with the
 //                    builtin lineshapes as built by buildModelAST (src/ResModel.cu:376-588)
-//                    and custom expressions as parsed by src/CustomExpr.cu:236-528
+//                    and custom expressions in the language of src/CustomExpr.cu:236-528
+//                    (front end: lineshape_lang.cpp)
 //   fixed blocks     src/AmpGen.cu:1396-1585 (computeAmpsKernelT) with
 //                    computeNodeFactor (include/ResModel.cuh:103-181)
 #include "codegen.hpp"
 
 #include "exprdag.hpp"
+#include "lineshape_lang.hpp"
 
 #include <algorithm>
 
@@ -36,232 +38,6 @@ std::string num(double v)
     if (s.find_first_of(".eEn") == std::string::npos) s += ".0";
     return s;
 }
-
-// ------------------------------------------------------------- expressions
-struct XNode {
-    enum K { Num, Var, Param, Add, Sub, Mul, Div, Pow, Neg, Func, Model } k = Num;
-    double v = 0;
-    std::string id;  // var / func / model name
-    int idx = 0;     // param index
-    std::vector<std::shared_ptr<XNode>> kids;
-};
-using XP = std::shared_ptr<XNode>;
-
-XP xn(XNode::K k, std::vector<XP> kids = {}, double v = 0, std::string id = "", int idx = 0)
-{
-    auto n = std::make_shared<XNode>();
-    n->k = k;
-    n->kids = std::move(kids);
-    n->v = v;
-    n->id = std::move(id);
-    n->idx = idx;
-    return n;
-}
-
-// Recursive-descent parser of the custom-lineshape language
-// (grammar of src/CustomExpr.cu:236-528).
-class XParser {
-public:
-    XParser(const std::string& s, const std::vector<std::string>& params) : params_(params) { lex(s); }
-    XP parse()
-    {
-        XP e = expr();
-        if (t_[p_].k != T::End) throw std::runtime_error("CustomExpr: trailing tokens");
-        return e;
-    }
-
-private:
-    struct T {
-        enum Kind { Num, Id, Op, LP, RP, Comma, End } k;
-        double v = 0;
-        std::string s;
-    };
-    std::vector<T> t_;
-    size_t p_ = 0;
-    const std::vector<std::string>& params_;
-
-    void lex(const std::string& s)
-    {
-        size_t i = 0;
-        while (i < s.size()) {
-            char c = s[i];
-            if (std::isspace((unsigned char)c)) { ++i; continue; }
-            if (std::isdigit((unsigned char)c) || c == '.') {
-                if (c == '1' && i + 1 < s.size() && (s[i + 1] == 'j' || s[i + 1] == 'i')) {
-                    t_.push_back({T::Id, 0, "1j"});
-                    i += 2;
-                    continue;
-                }
-                size_t j = i;
-                while (j < s.size() && (std::isdigit((unsigned char)s[j]) || s[j] == '.' || s[j] == 'e' || s[j] == 'E' ||
-                                        ((s[j] == '+' || s[j] == '-') && j > i && (s[j - 1] == 'e' || s[j - 1] == 'E'))))
-                    ++j;
-                t_.push_back({T::Num, std::stod(s.substr(i, j - i)), ""});
-                i = j;
-                continue;
-            }
-            if (std::isalpha((unsigned char)c) || c == '_') {
-                size_t j = i;
-                while (j < s.size() && (std::isalnum((unsigned char)s[j]) || s[j] == '_')) ++j;
-                t_.push_back({T::Id, 0, s.substr(i, j - i)});
-                i = j;
-                continue;
-            }
-            if (std::string("+-*/^").find(c) != std::string::npos) { t_.push_back({T::Op, 0, std::string(1, c)}); ++i; continue; }
-            if (c == '(') { t_.push_back({T::LP, 0, ""}); ++i; continue; }
-            if (c == ')') { t_.push_back({T::RP, 0, ""}); ++i; continue; }
-            if (c == ',') { t_.push_back({T::Comma, 0, ""}); ++i; continue; }
-            throw std::runtime_error(std::string("CustomExpr: unexpected char '") + c + "'");
-        }
-        t_.push_back({T::End, 0, ""});
-    }
-    bool op(const char* o) const { return t_[p_].k == T::Op && t_[p_].s == o; }
-    XP expr()
-    {
-        XP l = term();
-        while (op("+") || op("-")) {
-            bool a = t_[p_++].s == "+";
-            l = xn(a ? XNode::Add : XNode::Sub, {l, term()});
-        }
-        return l;
-    }
-    XP term()
-    {
-        XP l = factor();
-        while (op("*") || op("/")) {
-            bool m = t_[p_++].s == "*";
-            l = xn(m ? XNode::Mul : XNode::Div, {l, factor()});
-        }
-        return l;
-    }
-    XP factor()
-    {
-        XP b = unary();
-        if (op("^")) {
-            ++p_;
-            return xn(XNode::Pow, {b, factor()});
-        }
-        return b;
-    }
-    XP unary()
-    {
-        if (op("-")) {
-            ++p_;
-            return xn(XNode::Neg, {unary()});
-        }
-        if (op("+")) {
-            ++p_;
-            return unary();
-        }
-        return primary();
-    }
-    std::vector<XP> args()
-    {
-        if (t_[p_].k != T::LP) throw std::runtime_error("CustomExpr: function needs (");
-        ++p_;
-        std::vector<XP> a;
-        if (t_[p_].k == T::RP) {
-            ++p_;
-            return a;
-        }
-        while (true) {
-            a.push_back(expr());
-            if (t_[p_].k == T::Comma) { ++p_; continue; }
-            break;
-        }
-        if (t_[p_].k != T::RP) throw std::runtime_error("CustomExpr: missing )");
-        ++p_;
-        return a;
-    }
-    XP q0node()
-    {
-        return xn(XNode::Model, {params_.empty() ? xn(XNode::Num, {}, 1.0) : xn(XNode::Param, {}, 0, "", 0),
-                                 xn(XNode::Var, {}, 0, "md1"), xn(XNode::Var, {}, 0, "md2")},
-                  0, "q0");
-    }
-    XP primary()
-    {
-        T t = t_[p_];
-        if (t.k == T::Num) {
-            ++p_;
-            return xn(XNode::Num, {}, t.v);
-        }
-        if (t.k == T::LP) {
-            ++p_;
-            XP e = expr();
-            if (t_[p_].k != T::RP) throw std::runtime_error("CustomExpr: missing )");
-            ++p_;
-            return e;
-        }
-        if (t.k != T::Id) throw std::runtime_error("CustomExpr: unexpected token");
-        ++p_;
-        const std::string& s = t.s;
-        if (s == "1j") return xn(XNode::Model, {}, 0, "i");
-        if (s == "pi") return xn(XNode::Num, {}, 3.14159265358979323846);
-        if (s == "q0" && t_[p_].k != T::LP) return q0node();
-        static const char* vars[] = {"m", "q", "L", "d", "p1p", "p1e", "p1costheta", "p1phi",
-                                     "p2p", "p2e", "p2costheta", "p2phi"};
-        for (const char* v : vars)
-            if (s == v) return xn(XNode::Var, {}, 0, s);
-        static const std::map<std::string, std::string> funcs = {
-            {"exp", "exp"}, {"log", "log"}, {"ln", "log"}, {"sin", "sin"}, {"cos", "cos"}, {"sqrt", "sqrt"},
-            {"abs", "abs"}, {"Re", "re"}, {"real", "re"}, {"Im", "im"}, {"imag", "im"}, {"conj", "conj"}, {"csqrt", "sqrt"}};
-        auto fi = funcs.find(s);
-        if (fi != funcs.end()) {
-            if (t_[p_].k != T::LP) throw std::runtime_error("CustomExpr: function '" + s + "' needs (");
-            ++p_;
-            XP a = expr();
-            if (t_[p_].k != T::RP) throw std::runtime_error("CustomExpr: missing )");
-            ++p_;
-            return xn(XNode::Func, {a}, 0, fi->second);
-        }
-        if (s == "BW" || s == "BWR" || s == "Bf" || s == "Flatte" || (s == "q0" && t_[p_].k == T::LP)) {
-            auto a = args();
-            XP m = xn(XNode::Var, {}, 0, "m");
-            if (s == "BW") {
-                if (a.size() != 2) throw std::runtime_error("CustomExpr: BW(m0, w0) needs exactly 2 args");
-                return xn(XNode::Model, {m, a[0], a[1]}, 0, "bw");
-            }
-            if (s == "BWR") {
-                if (a.size() < 2 || a.size() > 4) throw std::runtime_error("CustomExpr: BWR(m0, g0[, L, d]) needs 2~4 args");
-                if (a.size() >= 3 && a[2]->k != XNode::Num) throw std::runtime_error("CustomExpr: BWR L must be a literal (e.g. 1)");
-                if (a.size() >= 4 && a[3]->k != XNode::Num) throw std::runtime_error("CustomExpr: BWR d must be a literal (e.g. 3.0)");
-                double Lv = a.size() >= 3 ? a[2]->v : 1.0, dv = a.size() >= 4 ? a[3]->v : 3.0;
-                return xn(XNode::Model, {m, a[0], a[1], xn(XNode::Num, {}, Lv), xn(XNode::Var, {}, 0, "q"), q0node(), xn(XNode::Num, {}, dv)}, 0, "bwr");
-            }
-            if (s == "Bf") {
-                if (a.size() != 4) throw std::runtime_error("CustomExpr: Bf(L, q, q0, d) needs exactly 4 args");
-                if (a[0]->k != XNode::Num) throw std::runtime_error("CustomExpr: Bf L must be a literal (e.g. 1)");
-                return xn(XNode::Model, a, 0, "bf");
-            }
-            if (s == "q0") {
-                if (a.size() == 1) return xn(XNode::Model, {a[0], xn(XNode::Var, {}, 0, "md1"), xn(XNode::Var, {}, 0, "md2")}, 0, "q0");
-                if (a.size() == 3) return xn(XNode::Model, a, 0, "q0");
-                throw std::runtime_error("CustomExpr: q0(x) or q0(x, md1, md2) expected");
-            }
-            if (a.size() < 4 || (a.size() - 1) % 3 != 0)
-                throw std::runtime_error("CustomExpr: Flatte(m0, g..., (ma,mb)...) needs 1+3n args (n>=1)");
-            // Flatte expanded to (A - iB)/(A^2 + B^2) (src/CustomExpr.cu:844-872)
-            int n = (int)(a.size() - 1) / 3;
-            XP sq = xn(XNode::Mul, {m, m});
-            // (m0^2 - m^2) is formed first so that the cancelling pair is one subtraction
-            XP A = xn(XNode::Sub, {xn(XNode::Mul, {a[0], a[0]}), sq}), B = xn(XNode::Num, {}, 0.0);
-            XP half = xn(XNode::Mul, {a[0], xn(XNode::Num, {}, 0.5)});
-            for (int i = 0; i < n; ++i) {
-                XP R = xn(XNode::Model, {sq, a[1 + n + 2 * i], a[2 + n + 2 * i]}, 0, "rho_re");
-                XP I = xn(XNode::Model, {sq, a[1 + n + 2 * i], a[2 + n + 2 * i]}, 0, "rho_im");
-                XP gw = xn(XNode::Mul, {a[1 + i], half});
-                A = xn(XNode::Add, {A, xn(XNode::Mul, {gw, I})});
-                B = xn(XNode::Sub, {B, xn(XNode::Mul, {gw, R})});
-            }
-            XP Dn = xn(XNode::Add, {xn(XNode::Mul, {A, A}), xn(XNode::Mul, {B, B})});
-            return xn(XNode::Add, {xn(XNode::Div, {A, Dn}), xn(XNode::Mul, {xn(XNode::Neg, {xn(XNode::Div, {B, Dn})}), xn(XNode::Model, {}, 0, "i")})});
-        }
-        for (size_t i = 0; i < params_.size(); ++i)
-            if (params_[i] == s) return xn(XNode::Param, {}, 0, "", (int)i);
-        throw std::runtime_error("CustomExpr: unknown identifier '" + s + "'");
-    }
-};
 
 // ------------------------------------------------------------- generator
 // kinematic slot types (angular.cuh AG_K_*)
@@ -486,7 +262,7 @@ struct Gen {
             }
             if (id == "bf") {
                 Cx q = emitX(x->kids[1], c), q0 = emitX(x->kids[2], c), d = emitX(x->kids[3], c);
-                if (!G.isConst(d.re)) throw std::runtime_error("CustomExpr: Bf d must not depend on the event or parameters");
+                if (!G.isConst(d.re)) throw std::runtime_error("custom lineshape: the barrier radius d of Bf must be a constant");
                 return G.cr(S.bf((int)x->kids[0]->v, q.re, q0.re, G.val(d.re)));
             }
             if (id == "bw") {
@@ -576,7 +352,7 @@ struct Gen {
                 return G.cmul(S.gs(mm, qq, P[0], P[1], q0r, mpi), bfx);
             }
             case ModelType::Custom: {
-                XParser ps(R.options.at("expr"), R.param_names);
+                XP expr = parseLineshapeExpr(R.options.at("expr"), R.param_names);
                 XCtx c;
                 c.mm = mm;
                 c.qq = qq;
@@ -588,7 +364,7 @@ struct Gen {
                 c.gi = gi;
                 c.d1 = n.d1;
                 c.d2 = n.d2;
-                return emitX(ps.parse(), c);
+                return emitX(expr, c);
             }
             case ModelType::Interp: return table(R.aux, mm, true);
             case ModelType::Hist: return table(R.aux, mm, false);
@@ -636,7 +412,7 @@ struct Gen {
         case ModelType::Hist: return table(R.aux, mm, false);
         case ModelType::Custom: {
             // value segment with md1 = md2 = 0, no daughter kinematics, at most 3 params
-            XParser ps(R.options.at("expr"), R.param_names);
+            XP expr = parseLineshapeExpr(R.options.at("expr"), R.param_names);
             XCtx c;
             c.mm = mm;
             c.qq = qq;
@@ -645,7 +421,7 @@ struct Gen {
             c.d = G.cnst(n.bf_d);
             c.L = L;
             for (size_t i = 0; i < P.size(); ++i) c.par.push_back(i < 3 ? P[i] : G.zero());
-            return emitX(ps.parse(), c);
+            return emitX(expr, c);
         }
         default: return G.c(1.0);  // GS / Interp have no fixed-parameter factor in the reference
         }
@@ -1338,8 +1114,7 @@ GeneratedModel generateModel(const Model& m)
 
 void checkCustomExpr(const std::string& expr, const std::vector<std::string>& params)
 {
-    XParser p(expr, params);
-    p.parse();
+    parseLineshapeExpr(expr, params);
 }
 
 }  // namespace ctpwa

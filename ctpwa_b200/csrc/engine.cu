@@ -471,10 +471,15 @@ __global__ void __launch_bounds__(128) ag_group_kernel(AgGroup G, AgTables T, co
 // ============================================================================
 
 // v[a] = ratio[a] * p[chain[a]], params = [Re p (nc), Im p (nc), theta]
+// err (may be null): the evaluation's error flag, cleared here because this
+// kernel is the first of every evaluation, so a flag raised by one evaluation
+// (a staged table copy that did not arrive) does not stick to later ones.
 __global__ void ct_prepare_kernel(const double* __restrict__ params, const int* __restrict__ chain,
-                                  const double* __restrict__ ratio, int nA, int nc, double* __restrict__ v)
+                                  const double* __restrict__ ratio, int nA, int nc, double* __restrict__ v,
+                                  int* __restrict__ err)
 {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a == 0 && err) *err = 0;
     if (a >= nA) return;
     int c = chain[a];
     v[2 * a] = params[c] * ratio[a];
@@ -1682,7 +1687,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     const CtaLayout& lay = lay_[precision == kMixed ? 1 : 0];
     const Model& m = model_;
     int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, d_err_);
     CT_CUDA(cudaGetLastError());
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));
@@ -1809,7 +1814,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     const size_t off_c = off_v + up((size_t)2 * nA);
     const size_t off_p = off_c + up((size_t)std::max(1, gen_.nconst));
     const size_t off_parts = off_p + up((size_t)lay.grid * nacc);
-    const size_t off_err = off_parts + 8;  // one int (copy-timeout flag), zeroed by this call
+    const size_t off_err = off_parts + 8;  // one int (copy-timeout flag), cleared by ct_prepare_kernel
     const size_t off_k = up(off_err + 1);  // constant-bank image of this call
     const size_t need = off_k + up((k_sym_bytes_ + 7) / 8);
     const size_t cap = kStaticScratchBytes / sizeof(double);
@@ -1824,8 +1829,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     double* s_partials = base + off_p;
     double* s_parts = base + off_parts;
 
-    CT_CUDA(cudaMemsetAsync(base + off_err, 0, sizeof(int), stream));
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, s_v);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, s_v, (int*)(base + off_err));
     CT_CUDA(cudaGetLastError());
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));
@@ -1895,7 +1899,7 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
     const int nacc = 2 + 2 * nA + nT;
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, d_err_);
     CT_CUDA(cudaGetLastError());
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));
@@ -1948,7 +1952,7 @@ void Engine::finalizeSums(const double* d_params, const double* d_sums, double* 
 {
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, nullptr);
     CT_CUDA(cudaGetLastError());
     FinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
@@ -2218,7 +2222,7 @@ void Engine::hvpSums(const double* d_params, const double* d_dirs, int ndir, dou
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta(), nP = m.nParams();
     const int nacc = 2 + 2 * nA + nT;
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, nullptr);
     CT_CUDA(cudaGetLastError());
     CtHvpArgsH a;
     std::memset(&a, 0, sizeof(a));
@@ -2266,7 +2270,7 @@ void Engine::finalizeHvp(const double* d_params, const double* d_dirs, int ndir,
     if (ndir <= 0) return;
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, nullptr);
     CT_CUDA(cudaGetLastError());
     HvpFinalizeArgs f;
     std::memset(&f, 0, sizeof(f));
@@ -2369,7 +2373,7 @@ void Engine::partialIntegrals(const double* d_params, int kind, double* d_out, c
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nb = nBlocks();
     const DeviceSample& d = samples_[kind];
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, nullptr);
     CT_CUDA(cudaGetLastError());
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));
@@ -2407,7 +2411,7 @@ void Engine::exportWeights(const double* d_params, const std::vector<int>& mask,
     const int npair = nb * (nb + 1) / 2;
     if (!mask.empty() && (int)mask.size() != nb) throw std::runtime_error("export: wave mask must have one entry per block");
     const DeviceSample& d = samples_[0];
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, nullptr);
     CT_CUDA(cudaGetLastError());
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));
@@ -2445,7 +2449,7 @@ void Engine::intensity(const double* d_params, int kind, double* d_out, cudaStre
     if (kind < 0 || kind > 2 || samples_[kind].n == 0) throw std::runtime_error("intensity: empty or unknown sample");
     const Model& m = model_;
     int nA = m.nAmp(), nc = m.nVector();
-    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_);
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, nullptr);
     CT_CUDA(cudaGetLastError());
     CtArgsH a;
     std::memset(&a, 0, sizeof(a));

@@ -87,7 +87,9 @@ public:
     // constants, per-CTA partial rows, per-sample parts) in one fixed array
     // compiled into the library instead of the handle's buffers; allocates
     // nothing. Throws std::length_error when this model's scratch exceeds the
-    // array (kStaticScratchBytes). All handles on a device share the array.
+    // array (kStaticScratchBytes). All handles on a device share the array;
+    // the handle's module constant block (k_sym_) is written as by nllGrad,
+    // so calls on one handle must be ordered against its other evaluations.
     void nllGradStatic(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
     static constexpr size_t kStaticScratchBytes = size_t(2) << 20;
     // Event-sharded evaluation: the per-sample sums of this handle's events,

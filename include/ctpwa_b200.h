@@ -98,18 +98,23 @@ int ctpwa_nll_grad(ctpwa_handle* h, const double* d_params, double* d_nll, doubl
  * serving loop that admits jobs by memory). The evaluation scratch (coupling
  * vector, parameter-only constants, one partial-sum row per CTA) lives in one
  * fixed 2 MiB array compiled into libctpwa_b200.so, present on every GPU that
- * loads the library until the process exits; the call allocates nothing and
- * uses none of the handle's own scratch. Same arguments, results and stream
- * ordering as ctpwa_nll_grad.
+ * loads the library until the process exits; the call allocates nothing.
+ * Besides that array it writes one per-handle buffer that the regular entry
+ * point writes too: the handle's kernel-module constant block (the per-call
+ * constants and couplings the fused kernel reads), so a static call must be
+ * ordered (same stream, or an event) against the same handle's other
+ * evaluations. Same arguments, results (bit for bit) and stream ordering as
+ * ctpwa_nll_grad.
  *  - A model whose scratch does not fit (about 4 + 2 nA + nT doubles per CTA
  *    row, up to 8 rows per SM) is rejected with CTPWA_ERR_ARG and a message;
  *    use ctpwa_nll_grad for it.
  *  - The first call on a device looks the array's address up (once per
  *    device, with the handle's device current); make that first call before
  *    beginning any stream capture on the device.
- *  - Every call writes all the scratch it reads, so nothing needs clearing,
- *    but all handles on a device share the one array: calls whose GPU work
- *    can overlap (other streams, threads or handles without ordering between
+ *  - Every call writes all the scratch it reads (its error flag is cleared
+ *    by the call's first kernel), so nothing needs clearing beforehand, but
+ *    all handles on a device share the one array: calls whose GPU work can
+ *    overlap (other streams, threads or handles without ordering between
  *    them) race and give wrong results. ctpwa_last_parts does not see these
  *    calls. */
 int ctpwa_nll_grad_static(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision,

@@ -5,7 +5,7 @@
 // leg. The product (ctpwa_b200) never links or calls it.
 //
 // It takes the lowered model from the product's host layer (config.cpp,
-// model.cpp, dataio.cpp; pinned separately by tests/test_model.py) and
+// model.cpp, dataio.cpp; pinned separately by tests/test_config_model.py) and
 // restates the per-event numerics:
 //   angular tensors and chain contraction  src/AmpGen.cu:1034-1219 (+ Amplitude.cu)
 //   lineshape assembly, per-call blocks    src/AmpGen.cu:1593-1932 (computeCustomAmpsKernelT)

@@ -8,6 +8,7 @@ import pytest
 
 import ctpwa_b200
 from ctpwa_b200 import workloads
+from conftest import reference_root
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -88,10 +89,10 @@ def test_invalid_config_is_not_valid(tmp_path):
 def test_bad_custom_expression_is_rejected(tmp_path):
     p = tmp_path / "bad.yml"
     p.write_text(workloads.config_text("kkpi", "p.npy", "d.npy").replace("Bf(1, q, q0, 3.0)", "Bf(L, q, q0, 3.0)"))
-    with pytest.raises(RuntimeError, match="literal"):
+    with pytest.raises(RuntimeError, match="must be a number"):
         ctpwa_b200.describe(str(p))
     p.write_text(workloads.config_text("kkpi", "p.npy", "d.npy").replace("* Bf(", "* Foo("))
-    with pytest.raises(RuntimeError, match="unknown identifier"):
+    with pytest.raises(RuntimeError, match="is not a function"):
         ctpwa_b200.describe(str(p))
 
 
@@ -99,8 +100,45 @@ def test_reference_example_config_parses():
     """The reference's own example config (flow maps, complex keys, Plot
     section) parses; it lists particles absent from Data.order, which the
     reference's reader rejects too."""
-    ref = "/root/reference/example/config.yml"
-    if not os.path.exists(ref):
+    root = reference_root()
+    if root is None:
         pytest.skip("reference tree not present")
+    ref = os.path.join(root, "example", "config.yml")
     with pytest.raises(RuntimeError, match="Data.order"):
         ctpwa_b200.describe(ref)
+
+
+@pytest.mark.parametrize("expr,message", [
+    ("BWR(mass, gKK, L)", "must be a number"),
+    ("foo(m)", "is not a function"),
+    ("2m", "malformed number"),
+    ("1e", "exponent without digits"),
+    ("mass +", "operand is expected"),
+    ("(mass", "expected '\\)'"),
+    ("exp m", "after a complete expression"),
+    ("exp", "without an argument list"),
+    ("BW(mass)", "BW takes"),
+    ("Flatte(mass, gKK, 0.49)", "Flatte takes"),
+    ("mass $ 2", "not part of the language"),
+    ("mass * nope", "neither a parameter"),
+])
+def test_custom_expression_errors(tmp_path, expr, message):
+    """Syntax and name errors of the custom-lineshape language are reported
+    with the offending column, at model creation (no GPU needed)."""
+    text = workloads.config_text("kkpi", "p.npy", "d.npy")
+    old = 'expr: "Flatte(mass, gKK, gpipi, 0.493677, 0.493677, 0.13957, 0.13957) * Bf(1, q, q0, 3.0)"'
+    assert old in text
+    p = tmp_path / "bad.yml"
+    p.write_text(text.replace(old, f'expr: "{expr}"'))
+    with pytest.raises(RuntimeError, match=message):
+        ctpwa_b200.describe(str(p))
+
+
+@pytest.mark.parametrize("expr", ["-mass^2^0.5 + (m/gKK)^(1j*gKK) - -gpipi", "mass^-1^2 * 3*-m", ".5e+1*q0 + q0(m)",
+                                  "BWR(mass, gKK) + BWR(mass, gKK, 2) + BWR(mass, gKK, 1, 5.0)"])
+def test_custom_expression_accepted(tmp_path, expr):
+    text = workloads.config_text("kkpi", "p.npy", "d.npy")
+    old = 'expr: "Flatte(mass, gKK, gpipi, 0.493677, 0.493677, 0.13957, 0.13957) * Bf(1, q, q0, 3.0)"'
+    p = tmp_path / "ok.yml"
+    p.write_text(text.replace(old, f'expr: "{expr}"'))
+    assert len(ctpwa_b200.describe(str(p))["param_names"]) > 0

@@ -607,3 +607,39 @@ def test_builtin_lineshapes_parity(tmp_path, variant):
     assert np.max(np.abs(gmx.cpu().numpy() - og)) <= 1e-4 * np.max(np.abs(og))
     H = ana.getHessian(pt).cpu().numpy()
     assert np.max(np.abs(H - H.T)) <= 1e-9 * np.max(np.abs(H))
+
+
+_EXPRS = [
+    # signs, right-associative powers and the imaginary unit
+    "-mass^2^0.5 + (m/gKK)^(1j*gKK) - -gpipi + 2^-1^2*m + 3*-m/mass^2",
+    # builtin lineshapes inside an expression, q0 with and without arguments
+    "BWR(mass, gKK, 1, 3.0) * Bf(1, q, q0(m), 3.0) + gpipi*exp(1j*m) * q0",
+    # one-argument functions and nested parentheses
+    "mass^2/(mass^2 - m^2 - 1j*mass*gKK) * (1 + gpipi*Re(conj(1j*m)) + abs(gpipi - 1j)/sqrt(m) - Im(ln(m*gKK)))",
+]
+
+
+@pytest.mark.parametrize("expr", _EXPRS)
+def test_custom_expression_language_parity(tmp_path, expr):
+    """The custom-lineshape language through the code generator: precedence,
+    signs, the imaginary unit and builtin calls, FP64 NLL and gradient against
+    the oracle, whose evaluator is pinned to the reference's compiled one."""
+    import torch
+    import ctpwa_b200
+
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=8_000, n_data=2_000, n_bkg=0, accept_reject=False, seed=71,
+                         gpu_generator=False)
+    text = open(cfg).read()
+    old = 'expr: "Flatte(mass, gKK, gpipi, 0.493677, 0.493677, 0.13957, 0.13957) * Bf(1, q, q0, 3.0)"'
+    assert old in text
+    open(cfg, "w").write(text.replace(old, f'expr: "{expr}"'))
+    ana = ctpwa_b200.analysis(cfg)
+    assert ana.isValid()
+    orc = Oracle(cfg)
+    p = workloads.true_params(ana.getNVector(), ana.getFreeResParams()[0].numpy())
+    p[2 * ana.getNVector():] *= 1 + 0.01 * np.random.default_rng(5).standard_normal(ana.getNFreeTheta())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    onll, og, _ = orc.nll_grad(p)
+    nll, g = ana.getNLLAndGrad(pt, "fp64")
+    assert abs(float(nll) - onll) <= 1e-10 * max(1.0, abs(onll)), (float(nll), onll)
+    assert np.max(np.abs(g.cpu().numpy() - og)) <= 1e-9 * np.max(np.abs(og))
