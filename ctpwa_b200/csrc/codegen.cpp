@@ -250,7 +250,7 @@ struct Gen {
             if (f == "abs") return G.cr(G.sqrt(G.add(G.mul(a.re, a.re), G.mul(a.im, a.im))));
             if (f == "re") return G.cr(a.re);
             if (f == "im") return G.cr(a.im);
-            if (f == "conj") return {a.re, G.neg(a.im)};
+            if (f == "conj") return G.cconj(a);
             return a;
         }
         case XNode::Model: {

@@ -290,30 +290,153 @@ int Graph::deriv(int n, int j)
     return r;
 }
 
-Cx Graph::cmul(Cx a, Cx b)
+int Graph::negZero()
 {
-    return {sub(mul(a.re, b.re), mul(a.im, b.im)), add(mul(a.re, b.im), mul(a.im, b.re))};
+    Node n;
+    n.op = Const;
+    n.v = -0.0;
+    n.idx = 1;  // keeps it apart from +0.0 in the node memo
+    return make(n);
 }
 
+ZS Graph::zconst(bool negative) const
+{
+    auto z = std::make_shared<ZSign>();
+    z->k = negative ? ZSign::Neg : ZSign::Pos;
+    return z;
+}
+
+ZS Graph::zsign(const Cx& a) const
+{
+    if (a.zs) return a.zs;
+    return zconst(isConst(a.im) && std::signbit(val(a.im)));
+}
+
+ZS Graph::sgn(int x) const
+{
+    if (isConst(x)) return zconst(std::signbit(val(x)));
+    auto z = std::make_shared<ZSign>();
+    z->k = ZSign::SignOf;
+    z->node = x;
+    return z;
+}
+
+ZS Graph::zprod(const ZS& a, const ZS& b) const
+{
+    if (zisConst(a) && zisConst(b)) return zconst(zneg(a) != zneg(b));
+    auto z = std::make_shared<ZSign>();
+    z->k = ZSign::Prod;
+    z->a = a;
+    z->b = b;
+    return z;
+}
+
+ZS Graph::zflip(const ZS& a) const
+{
+    if (zisConst(a)) return zconst(!zneg(a));
+    auto z = std::make_shared<ZSign>();
+    z->k = ZSign::Flip;
+    z->a = a;
+    return z;
+}
+
+ZS Graph::zsum(const ZS& a, const ZS& b) const
+{
+    if (zisConst(a) && zisConst(b)) return zconst(zneg(a) && zneg(b));
+    if (zisConst(a) && !zneg(a)) return zconst(false);
+    if (zisConst(b) && !zneg(b)) return zconst(false);
+    auto z = std::make_shared<ZSign>();
+    z->k = ZSign::Both;
+    z->a = a;
+    z->b = b;
+    return z;
+}
+
+int Graph::zmaterialize(const ZS& a)
+{
+    if (!a || a->k == ZSign::Pos) return one_;
+    switch (a->k) {
+    case ZSign::Neg: return cnst(-1.0);
+    case ZSign::SignOf: return sel(LT0, a->node, cnst(-1.0), one_);
+    case ZSign::Prod: return mul(zmaterialize(a->a), zmaterialize(a->b));
+    case ZSign::Flip: return neg(zmaterialize(a->a));
+    case ZSign::Both: return sel(LT0, zmaterialize(a->a), zmaterialize(a->b), one_);
+    default: return one_;
+    }
+}
+
+Cx Graph::cadd(Cx a, Cx b)
+{
+    Cx r{add(a.re, b.re), add(a.im, b.im)};
+    if (zeroIm(a) && zeroIm(b)) r.zs = zsum(zsign(a), zsign(b));
+    return r;
+}
+
+Cx Graph::csub(Cx a, Cx b)
+{
+    Cx r{sub(a.re, b.re), sub(a.im, b.im)};
+    if (zeroIm(a) && zeroIm(b)) r.zs = zsum(zsign(a), zflip(zsign(b)));
+    return r;
+}
+
+Cx Graph::cneg(Cx a)
+{
+    Cx r{neg(a.re), neg(a.im)};
+    if (zeroIm(a)) r.zs = zflip(zsign(a));
+    return r;
+}
+
+Cx Graph::cconj(Cx a)
+{
+    Cx r{a.re, neg(a.im)};
+    if (zeroIm(a)) r.zs = zflip(zsign(a));
+    return r;
+}
+
+// im = a.re b.im + a.im b.re: for real a and b the two zero terms have the
+// signs sgn(a.re) zs(b) and zs(a) sgn(b.re)
+Cx Graph::cmul(Cx a, Cx b)
+{
+    Cx r{sub(mul(a.re, b.re), mul(a.im, b.im)), add(mul(a.re, b.im), mul(a.im, b.re))};
+    if (zeroIm(a) && zeroIm(b)) r.zs = zsum(zprod(sgn(a.re), zsign(b)), zprod(zsign(a), sgn(b.re)));
+    return r;
+}
+
+// im = (a.im b.re - a.re b.im) / |b|^2
 Cx Graph::cdivRef(Cx a, Cx b)
 {
     int s = add(mul(b.re, b.re), mul(b.im, b.im));
     s = sel(EQ0, s, cnst(1e-30), s);
     int is = recip(s);
-    return {mul(add(mul(a.re, b.re), mul(a.im, b.im)), is), mul(sub(mul(a.im, b.re), mul(a.re, b.im)), is)};
+    Cx r{mul(add(mul(a.re, b.re), mul(a.im, b.im)), is), mul(sub(mul(a.im, b.re), mul(a.re, b.im)), is)};
+    if (zeroIm(a) && zeroIm(b)) r.zs = zsum(zprod(zsign(a), sgn(b.re)), zflip(zprod(sgn(a.re), zsign(b))));
+    return r;
 }
 
+// im = e^re sin(im): sin(+-0) = +-0
 Cx Graph::cexp(Cx a)
 {
     int e = exp(a.re);
-    return {mul(e, cos(a.im)), mul(e, sin(a.im))};
+    Cx r{mul(e, cos(a.im)), mul(e, sin(a.im))};
+    if (zeroIm(a)) r.zs = zsign(a);
+    return r;
 }
 
+// im = atan2(a.im, a.re): +-pi on the negative real axis by the sign of a's
+// zero imaginary part
 Cx Graph::clogRef(Cx a)
 {
     int r = sqrt(add(mul(a.re, a.re), mul(a.im, a.im)));
     r = sel(EQ0, r, cnst(1e-30), r);
-    return {log(r), atan2(a.im, a.re)};
+    int y = a.im;
+    if (zeroIm(a)) {
+        ZS z = zsign(a);
+        y = zisConst(z) ? (zneg(z) ? negZero() : zero_) : sel(LT0, zmaterialize(z), negZero(), zero_);
+    }
+    Cx out{log(r), atan2(y, a.re)};
+    if (zeroIm(out))  // folded: y and a.re are constants
+        out.zs = zconst(std::signbit(std::atan2(val(y), val(a.re))));
+    return out;
 }
 
 Cx Graph::csqrt(Cx a)
@@ -324,16 +447,22 @@ Cx Graph::csqrt(Cx a)
     return {re, sel(LT0, a.im, neg(im), im)};
 }
 
+// im = cos(re) (e^im - e^-im) / 2: for real a, sgn(cos(re)) times +0
 Cx Graph::csin(Cx a)
 {
     int ep = exp(a.im), em = exp(neg(a.im));
-    return {mul(mul(sin(a.re), add(ep, em)), cnst(0.5)), mul(mul(cos(a.re), sub(ep, em)), cnst(0.5))};
+    Cx r{mul(mul(sin(a.re), add(ep, em)), cnst(0.5)), mul(mul(cos(a.re), sub(ep, em)), cnst(0.5))};
+    if (zeroIm(a)) r.zs = sgn(cos(a.re));  // the cos node exists already (memo)
+    return r;
 }
 
+// im = -sin(re) (e^im - e^-im) / 2: for real a, -sgn(sin(re)) times +0
 Cx Graph::ccos(Cx a)
 {
     int ep = exp(a.im), em = exp(neg(a.im));
-    return {mul(mul(cos(a.re), add(ep, em)), cnst(0.5)), neg(mul(mul(sin(a.re), sub(ep, em)), cnst(0.5)))};
+    Cx r{mul(mul(cos(a.re), add(ep, em)), cnst(0.5)), neg(mul(mul(sin(a.re), sub(ep, em)), cnst(0.5)))};
+    if (zeroIm(a)) r.zs = zflip(sgn(sin(a.re)));  // the sin node exists already (memo)
+    return r;
 }
 
 }  // namespace dag

@@ -14,6 +14,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <tuple>
 #include <unordered_map>
@@ -55,8 +56,24 @@ struct Node {
     int idx = 0;     // Theta / Kin index
 };
 
+// Sign (+1 / -1) of a zero imaginary part, kept as a small expression
+// outside the DAG and turned into nodes only where it is read.
+struct ZSign;
+using ZS = std::shared_ptr<const ZSign>;
+struct ZSign {
+    enum K { Pos, Neg, SignOf, Prod, Flip, Both } k = Pos;
+    int node = -1;  // SignOf: the real node whose sign is taken
+    ZS a, b;
+};
+
+// A complex value. When the imaginary part is a constant zero, `zs` carries
+// the sign that zero has under IEEE arithmetic with the formulas of the
+// custom-expression language (-x of a real x has imaginary part -0; null:
+// +0). The sign matters only where the value reaches the branch cut of
+// log / pow (atan2(+-0, re < 0) = +-pi), the one place it is read.
 struct Cx {
     int re, im;
+    ZS zs;
 };
 
 class Graph {
@@ -89,12 +106,13 @@ public:
     bool isConst(int n) const { return nodes[n].op == Const; }
     double val(int n) const { return nodes[n].v; }
 
-    // complex helpers
+    // complex helpers (formulas of the custom-expression language)
     Cx c(double re, double im = 0.0) { return {cnst(re), cnst(im)}; }
     Cx cr(int re) { return {re, zero_}; }
-    Cx cadd(Cx a, Cx b) { return {add(a.re, b.re), add(a.im, b.im)}; }
-    Cx csub(Cx a, Cx b) { return {sub(a.re, b.re), sub(a.im, b.im)}; }
-    Cx cneg(Cx a) { return {neg(a.re), neg(a.im)}; }
+    Cx cadd(Cx a, Cx b);
+    Cx csub(Cx a, Cx b);
+    Cx cneg(Cx a);
+    Cx cconj(Cx a);
     Cx cmul(Cx a, Cx b);
     Cx cscale(Cx a, int s) { return {mul(a.re, s), mul(a.im, s)}; }
     Cx cdivRef(Cx a, Cx b);  // |b|^2 == 0 uses 1e-30 (custom-expression convention)
@@ -108,6 +126,18 @@ public:
     std::vector<Node> nodes;
 
 private:
+    // signed zeros of imaginary parts (see Cx)
+    int negZero();                                     // the constant -0.0 (distinct from zero())
+    bool zeroIm(const Cx& a) const { return isConst(a.im) && val(a.im) == 0.0; }
+    ZS zsign(const Cx& a) const;                       // sign of a's zero imaginary part
+    ZS zconst(bool negative) const;
+    ZS sgn(int x) const;                               // sign of a real node
+    ZS zprod(const ZS& a, const ZS& b) const;
+    ZS zflip(const ZS& a) const;
+    ZS zsum(const ZS& a, const ZS& b) const;           // (+-0) + (+-0): negative iff both are
+    static bool zisConst(const ZS& a) { return !a || a->k == ZSign::Pos || a->k == ZSign::Neg; }
+    static bool zneg(const ZS& a) { return a && a->k == ZSign::Neg; }
+    int zmaterialize(const ZS& a);                     // +-1 as a node
     int make(Node n);
     int mulRaw(int a, int b);  // a * b as one node, no regrouping
     int zero_, one_;

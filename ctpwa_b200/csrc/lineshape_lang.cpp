@@ -8,6 +8,7 @@
 #include "lineshape_lang.hpp"
 
 #include <cctype>
+#include <cmath>
 #include <cstdlib>
 #include <stdexcept>
 
@@ -372,6 +373,61 @@ private:
     }
 };
 
+// ------------------------------------------------------------ folding
+// The language folds a resolved expression bottom-up before it is evaluated
+// (reference: simplify, src/CustomExpr.cu:785-835), and the folding is
+// observable: a constant power is the real pow ((-2)^0.5 is NaN), 0^x is 0,
+// a negated number literal is a negative number (imaginary part +0, not -0).
+// Rules, with "number" a Num node and 0 / 1 its value:
+//   0 + x, x + 0 -> x        x - 0 -> x          number op number -> number
+//   0 * x, x * 0 -> 0        1 * x, x * 1 -> x   0 / x -> 0, x / 1 -> x
+//   x ^ 1 -> x, 1 ^ x -> 1, 0 ^ x -> 0           -(-x) -> x, -number -> number
+bool isNum(const XP& x) { return x->k == XNode::Num; }
+bool isNum(const XP& x, double v) { return x->k == XNode::Num && x->v == v; }
+
+XP fold(const XP& x)
+{
+    if (x->kids.empty()) return x;
+    std::vector<XP> k;
+    for (const XP& c : x->kids) k.push_back(fold(c));
+    switch (x->k) {
+    case XNode::Add:
+        if (isNum(k[0], 0.0)) return k[1];
+        if (isNum(k[1], 0.0)) return k[0];
+        if (isNum(k[0]) && isNum(k[1])) return number(k[0]->v + k[1]->v);
+        break;
+    case XNode::Sub:
+        if (isNum(k[1], 0.0)) return k[0];
+        if (isNum(k[0]) && isNum(k[1])) return number(k[0]->v - k[1]->v);
+        break;
+    case XNode::Mul:
+        if (isNum(k[0], 0.0) || isNum(k[1], 0.0)) return number(0.0);
+        if (isNum(k[0], 1.0)) return k[1];
+        if (isNum(k[1], 1.0)) return k[0];
+        if (isNum(k[0]) && isNum(k[1])) return number(k[0]->v * k[1]->v);
+        break;
+    case XNode::Div:
+        if (isNum(k[0], 0.0)) return number(0.0);
+        if (isNum(k[1], 1.0)) return k[0];
+        if (isNum(k[0]) && isNum(k[1]) && k[1]->v != 0.0) return number(k[0]->v / k[1]->v);
+        break;
+    case XNode::Pow:
+        if (isNum(k[1], 1.0)) return k[0];
+        if (isNum(k[0], 1.0)) return number(1.0);
+        if (isNum(k[0], 0.0)) return number(0.0);
+        if (isNum(k[0]) && isNum(k[1])) return number(std::pow(k[0]->v, k[1]->v));
+        break;
+    case XNode::Neg:
+        if (k[0]->k == XNode::Neg) return k[0]->kids[0];
+        if (isNum(k[0])) return number(-k[0]->v);
+        break;
+    default: break;
+    }
+    XP n = std::make_shared<XNode>(*x);
+    n->kids = std::move(k);
+    return n;
+}
+
 }  // namespace
 
 XP parseLineshapeExpr(const std::string& text, const std::vector<std::string>& params)
@@ -379,7 +435,7 @@ XP parseLineshapeExpr(const std::string& text, const std::vector<std::string>& p
     Parser p(text);
     SynP tree = p.parseAll();
     Resolver r(text, params);
-    return r.resolve(*tree);
+    return fold(r.resolve(*tree));
 }
 
 }  // namespace ctpwa

@@ -40,7 +40,8 @@ struct XNode {
 };
 using XP = std::shared_ptr<XNode>;
 
-// Parses and resolves one expression against the resonance's parameter names.
+// Parses and resolves one expression against the resonance's parameter names,
+// then folds it by the language's constant rules (lineshape_lang.cpp, fold).
 // Throws std::runtime_error("custom lineshape: ...") with the column of the
 // offending token on any syntax or name error.
 XP parseLineshapeExpr(const std::string& text, const std::vector<std::string>& params);

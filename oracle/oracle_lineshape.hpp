@@ -227,6 +227,54 @@ inline ExprP mk(Expr::Kind k, std::vector<ExprP> kids = {}, double num = 0.0, in
     return e;
 }
 
+// The reference simplifies every parsed expression before it compiles or
+// evaluates it (simplify, src/CustomExpr.cu:785-835; called at :1281 and
+// src/ResModel.cu:569): bottom-up, 0+x / x+0 -> x, x-0 -> x, 0*x / x*0 -> 0,
+// 1*x / x*1 -> x, 0/x -> 0, x/1 -> x, x^1 -> x, 1^x -> 1, 0^x -> 0,
+// -(-x) -> x, -c -> (-c), and two numbers fold (a power by real std::pow).
+inline bool exprNum(const ExprP& e) { return e->kind == Expr::Num; }
+inline bool exprIs(const ExprP& e, double v) { return e->kind == Expr::Num && e->num == v; }
+inline ExprP simplifyRef(const ExprP& e)
+{
+    auto out = std::make_shared<Expr>(*e);
+    for (auto& k : out->kids) k = simplifyRef(k);
+    const auto& k = out->kids;
+    switch (out->kind) {
+    case Expr::Add:
+        if (exprIs(k[0], 0.0)) return k[1];
+        if (exprIs(k[1], 0.0)) return k[0];
+        if (exprNum(k[0]) && exprNum(k[1])) return mk(Expr::Num, {}, k[0]->num + k[1]->num);
+        break;
+    case Expr::Sub:
+        if (exprIs(k[1], 0.0)) return k[0];
+        if (exprNum(k[0]) && exprNum(k[1])) return mk(Expr::Num, {}, k[0]->num - k[1]->num);
+        break;
+    case Expr::Mul:
+        if (exprIs(k[0], 0.0) || exprIs(k[1], 0.0)) return mk(Expr::Num, {}, 0.0);
+        if (exprIs(k[0], 1.0)) return k[1];
+        if (exprIs(k[1], 1.0)) return k[0];
+        if (exprNum(k[0]) && exprNum(k[1])) return mk(Expr::Num, {}, k[0]->num * k[1]->num);
+        break;
+    case Expr::Div:
+        if (exprIs(k[0], 0.0)) return mk(Expr::Num, {}, 0.0);
+        if (exprIs(k[1], 1.0)) return k[0];
+        if (exprNum(k[0]) && exprNum(k[1]) && k[1]->num != 0.0) return mk(Expr::Num, {}, k[0]->num / k[1]->num);
+        break;
+    case Expr::Pow:
+        if (exprIs(k[1], 1.0)) return k[0];
+        if (exprIs(k[0], 1.0)) return mk(Expr::Num, {}, 1.0);
+        if (exprIs(k[0], 0.0)) return mk(Expr::Num, {}, 0.0);
+        if (exprNum(k[0]) && exprNum(k[1])) return mk(Expr::Num, {}, std::pow(k[0]->num, k[1]->num));
+        break;
+    case Expr::Neg:
+        if (k[0]->kind == Expr::Neg) return k[0]->kids[0];
+        if (exprNum(k[0])) return mk(Expr::Num, {}, -k[0]->num);
+        break;
+    default: break;
+    }
+    return out;
+}
+
 class ExprParser {
 public:
     ExprParser(const std::string& s, const std::vector<std::string>& params) : params_(params)
@@ -237,7 +285,7 @@ public:
     {
         ExprP e = expr();
         if (toks_[pos_].t != Tok::End) throw std::runtime_error("CustomExpr: trailing tokens");
-        return e;
+        return simplifyRef(e);
     }
 
 private:

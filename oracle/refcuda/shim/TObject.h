@@ -1,0 +1,3 @@
+// ORACLE BUILD SHIM (test infrastructure): see root_stub.h.
+#pragma once
+#include "root_stub.h"

@@ -616,6 +616,10 @@ _EXPRS = [
     "BWR(mass, gKK, 1, 3.0) * Bf(1, q, q0(m), 3.0) + gpipi*exp(1j*m) * q0",
     # one-argument functions and nested parentheses
     "mass^2/(mass^2 - m^2 - 1j*mass*gKK) * (1 + gpipi*Re(conj(1j*m)) + abs(gpipi - 1j)/sqrt(m) - Im(ln(m*gKK)))",
+    # constant folding and signed zeros on the branch cut of log / pow (the conjugate branch if either were lost)
+    "BWR(mass, gKK) * ((-m)^0.5 * (m*-2)^gpipi + log(-gKK*m) + exp(-m)*(-1)^gpipi)",
+    "BWR(mass, gKK) * ((-mass - m)^1.5 + conj(-m)^0.3 - (m/-1)^0.5 + (-1*m)^0.5 + sin(-mass)^2.5 * cos(mass)^0.5)",
+    "BWR(mass, gKK) * (0^(m-2) + mass^1*gpipi^1 + 1^m + (0-m)^0.5 - -(-m)^0.5 + (-(m^2-mass^2))^gpipi)",
 ]
 
 

@@ -106,7 +106,16 @@ EXPRS = [("Flatte(mass, gKK, gpipi, 0.493677, 0.493677, 0.13957, 0.13957) * Bf(1
          ("BWR(p0, p1, 1, 3.0) * Bf(1, q, q0(m), 3.0)", "p0,p1", [1.66, 0.125]),
          ("exp(1j*p2)*BW(p0,p1) + sqrt(m - p0) - log(m*p1) + sin(p2)*cos(m) + abs(p1-1j)/conj(p0+1j) + Re(p0*1j)"
           " - Im(p1) + csqrt(-m) + q0", "p0,p1,p2", [1.2, 0.2, 0.3]),
-         ("-p0^2^0.5 + (m/p1)^(1j*p1) - -p1", "p0,p1", [1.4, 0.3])]
+         ("-p0^2^0.5 + (m/p1)^(1j*p1) - -p1", "p0,p1", [1.4, 0.3]),
+         # the reference's constant folding and IEEE signed zeros on the branch cut of log / pow
+         ("(-m)^0.5 * (m*-2)^p2 + log(-p1*m) + exp(-m)*(-1)^p2", "p0,p1,p2", [1.68, 0.3, 0.1]),
+         ("(-p0 - m)^1.5 + conj(-m)^0.3 - (m/-1)^0.5 + (-1*m)^0.5 + sin(-p0)^2.5 * cos(p0)^0.5", "p0,p1",
+          [1.68, 0.3]),
+         ("0^(m-2) + p0^1*p1^1 + 1^m + (0-m)^0.5 - -(-m)^0.5 + 0*log(0*m) + (-(m^2-p0^2))^p1", "p0,p1",
+          [1.68, 0.3])]
+
+# folded constants that the reference evaluates to NaN (real pow of a negative number)
+NAN_EXPRS = ["(-2)^0.5 + p0", "(m*0-1)^0.5 * p0"]
 
 
 @pytest.mark.parametrize("case", EXPRS)
@@ -129,6 +138,23 @@ def test_custom_expressions_match_reference(ref, case):
         ref.ref_aux_eval(h, ptr(para), P, m, q, 1, 3.0, 0.493677, 0.493677, ptr(z8), ptr(o2))
         assert np.max(np.abs(o1[:2] - o2[:2])) <= 1e-13 * np.max(np.abs(o2[:2]))
         assert np.max(np.abs(o1[2:] - o2[2:2 + 2 * P])) <= 1e-12 * max(1e-300, np.max(np.abs(o2[2:2 + 2 * P])))
+    ref.ref_aux_free(h)
+
+
+@pytest.mark.parametrize("expr", NAN_EXPRS)
+def test_custom_expression_nan_folding_matches_reference(ref, expr):
+    orc = oracle_lib()
+    para = np.array([1.5])
+    h = ref.ref_custom_build(expr.encode(), b"p0")
+    assert h
+    o1, o2 = np.zeros(4), np.zeros(6)
+    err = ctypes.create_string_buffer(256)
+    m = 1.3
+    q = _q(m, 0.493677, 0.493677)
+    assert orc.orc_custom_eval(expr.encode(), b"p0", ptr(para), 1, m, q, 1, 3.0, 0.493677, 0.493677, ptr(o1),
+                               err, 256) == 0
+    ref.ref_aux_eval(h, ptr(para), 1, m, q, 1, 3.0, 0.493677, 0.493677, ptr(np.zeros(8)), ptr(o2))
+    assert np.isnan(o2[0]) and np.isnan(o1[0])
     ref.ref_aux_free(h)
 
 
