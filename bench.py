@@ -19,10 +19,12 @@ the same size (weak scaling); the per-step exchange is one NCCL all-reduce of
 the ranks' per-sample sums, after which every rank forms the loss and
 gradient of the union of the shards.
 
-`--impl reference`: the reference has no CPU path and its CUDA build needs
-yaml-cpp and ROOT, which are absent, so this arm times the FP64 OpenMP port of
-the reference's algorithm (oracle/) on all host cores, each step on a bounded
-sample of the same workload, scaled to full-size evaluations per second.
+`--impl reference`: the reference has no CPU path, so this arm times the
+FP64 OpenMP port of the reference's algorithm (oracle/) on all host cores, on
+the full workload, unscaled (each step one full-size NLL + gradient); the
+process imports nothing of the product (its events come from a child process,
+oracle.cpu_workload). The reference's own CUDA build is compared with this
+library in tests/test_reference_cuda.py.
 """
 from __future__ import annotations
 
@@ -162,107 +164,115 @@ def cpu_cores():
 
 
 # --------------------------------------------------------------------------- CPU port (oracle)
-def oracle_sample(data_dir, fraction, seed):
-    """Bounded CPU sample of the workload: same generator and accept-reject, intensities from the oracle."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    from binding import Oracle  # noqa: E402  (CPU baseline only)
-
-    from ctpwa_b200 import workloads
-
-    n_p, n_d, n_b, w_b = workloads.SIZES[WORKLOAD]
-    n_p, n_d, n_b = (max(100, int(round(x * fraction))) for x in (n_p, n_d, n_b))
-    out = Path(data_dir) / f"cpu_{WORKLOAD}_{n_p}_{n_d}_{n_b}_s{seed}"
-    cfg = out / "config.yml"
-    if not (out / "done").exists():
-
-        def intensity(cand_cfg, params):
-            o = Oracle(cand_cfg)
-            try:
-                return o.intensity(1, params)
-            finally:
-                o.close()
-
-        workloads.make(WORKLOAD, out, n_phsp=n_p, n_data=n_d, n_bkg=n_b, bkg_weight=w_b, seed=seed,
-                       gpu_generator=False, intensity=intensity)
-        (out / "done").write_text("ok")
-    return str(cfg), (n_p, n_d, n_b)
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
-def time_oracle(cfg, n_threads, min_seconds, min_evals=3, max_evals=None, seed=0):
-    sys.path.insert(0, str(ROOT / "oracle"))
-    from binding import Oracle  # noqa: E402
+def workload_config():
+    """The `config` of both arms' lines: the workload and the timing rules."""
+    sizes = {"phsp": 10_000_000, "data": 1_000_000, "bkg": 100_000}
+    return {"workload": WORKLOAD_TEXT, "events": sizes, "n_params": 23, "theta_perturbed_every_step": True,
+            "l2": f"inputs larger than L2 ({L2_BYTES // (1024 * 1024)} MiB): no flush"}
 
-    from ctpwa_b200 import workloads
 
-    o = Oracle(cfg)
-    p0 = workloads.true_params(o.nV, o.theta_init()[0])
+def time_oracle_evals(o, p0, n_evals, n_threads, seed):
+    """Wall time of each of n_evals FP64 NLL + gradient evaluations of the
+    oracle, the resonance parameters perturbed every evaluation."""
     rng = np.random.default_rng(seed + 17)
     nV = o.nV
     times = []
-    o.nll_grad(p0, n_threads)  # warm-up
-    t_start = time.perf_counter()
-    while True:
-        p = p0.copy()
+    for _ in range(n_evals):
+        p = np.array(p0, dtype=np.float64)
         p[2 * nV:] *= 1.0 + 1e-4 * rng.standard_normal(p.size - 2 * nV)
         t0 = time.perf_counter()
         o.nll_grad(p, n_threads)
         times.append(time.perf_counter() - t0)
-        if len(times) >= min_evals and time.perf_counter() - t_start >= min_seconds:
-            break
-        if max_evals and len(times) >= max_evals:
-            break
-    o.close()
     return times
 
 
-def full_size_events():
-    from ctpwa_b200 import workloads
+def cpu_baseline(cfg, p0, sizes):
+    """The oracle (FP64, OpenMP on all host threads) on the very events of the
+    GPU run, full size: the median of 3 NLL + gradient evaluations."""
+    from oracle.binding import Oracle  # CPU baseline only
 
-    n_p, n_d, n_b, _ = workloads.SIZES[WORKLOAD]
-    return n_p + n_d + n_b
-
-
-def cpu_baseline(data_dir, seed):
-    """Oracle on a 1 % sample of the workload, all host threads, >= 10 s of evaluations."""
-    fraction = 0.01
-    cfg, sizes = oracle_sample(data_dir, fraction, seed)
     cores = cpu_cores()
-    times = time_oracle(cfg, cores, min_seconds=10.0, seed=seed)
+    t0 = time.perf_counter()
+    o = Oracle(cfg)
+    t_open = time.perf_counter() - t0
+    try:
+        times = time_oracle_evals(o, p0, 3, cores, seed=1)
+    finally:
+        o.close()
     t = statistics.median(times)
-    scale = full_size_events() / float(sum(sizes))
-    return {"value": 1.0 / (t * scale), "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": (f"{sizes[0]} phsp / {sizes[1]} data / {sizes[2]} bkg events (1% of the workload), "
-                       f"median of {len(times)} FP64 NLL+grad evals ({t:.3f} s each), scaled x{scale:.1f} "
-                       f"by event count to full size")}
+    return {"value": 1.0 / t, "unit": UNIT, "cores": cores, "kind": "port", "cpu": cpu_model(),
+            "sample": (f"the full workload, the GPU run's own events ({sizes[0]} phsp / {sizes[1]} data / "
+                       f"{sizes[2]} bkg): median of {len(times)} FP64 NLL+grad evaluations "
+                       f"({', '.join(f'{x:.2f}' for x in times)} s), angular tensors computed once "
+                       f"at load ({t_open:.1f} s, not timed)")}
 
 
 def run_reference(args, rank, world):
+    """The reference's algorithm on the host cores, full size and unscaled:
+    the OpenMP FP64 oracle (the reference has no CPU path). This process
+    imports nothing of the product: the events are generated by a child
+    process (oracle.cpu_workload: numpy phase space and candidates), the data
+    drawn here by accept-reject against the oracle's intensities."""
     if rank != 0:
         return 0
+    from oracle.binding import Oracle
+
+    t_all = time.perf_counter()
     cores = cpu_cores()
-    # size the per-step sample so that warm-up + steps finish in about two minutes
-    pilot_cfg, pilot_sizes = oracle_sample(args.data_dir, 0.001, args.seed)
-    t_pilot = statistics.median(time_oracle(pilot_cfg, cores, min_seconds=1.0, max_evals=20, seed=args.seed))
-    per_event = t_pilot / sum(pilot_sizes)
-    budget = 120.0 / max(1, args.steps + args.warmup)
-    fraction = min(0.01, max(0.001, budget / (per_event * full_size_events())))
-    fraction = float(f"{fraction:.2g}")
-    cfg, sizes = oracle_sample(args.data_dir, fraction, args.seed)
-    times = time_oracle(cfg, cores, min_seconds=0.0, min_evals=args.steps + args.warmup,
-                        max_evals=args.steps + args.warmup, seed=args.seed)[args.warmup:]
+    out = Path(args.data_dir) / f"cpu_{WORKLOAD}_f{args.fraction:g}_s{args.seed}"
+    if not (out / "done").exists():
+        subprocess.run([sys.executable, "-m", "oracle.cpu_workload", str(out), "--name", WORKLOAD,
+                        "--seed", str(args.seed), "--fraction", str(args.fraction)], check=True, cwd=str(ROOT))
+    meta = json.loads((out / "params.json").read_text())
+    p0 = np.array(meta["true_params"])
+    t0 = time.perf_counter()
+    o = Oracle(out / "config.yml")
+    t_open = time.perf_counter() - t0
+    # accept-reject of the candidates against the model at the true parameters
+    I = o.intensity(1, p0)
+    rng = np.random.default_rng(6001 + args.seed)
+    keep = np.flatnonzero(rng.uniform(0.0, 1.2 * float(I.max()), I.size) < I)
+    n_d = int(meta["n_data"])
+    n_acc = int(keep.size)
+    if n_acc >= n_d:
+        idx = keep[:n_d]
+    else:  # top up by drawing accepted events again (the same distribution)
+        idx = np.concatenate([keep, rng.choice(keep, n_d - n_acc, replace=True)])
+    o.take(1, idx)
+    t_prep = time.perf_counter() - t_all
+    W, K = max(3, args.warmup), args.steps
+    time_oracle_evals(o, p0, W, cores, seed=args.seed)
+    times = time_oracle_evals(o, p0, K, cores, seed=args.seed + 1)
+    o.close()
     t = sum(times) / len(times)
-    scale = full_size_events() / float(sum(sizes))
-    value = 1.0 / (t * scale)
-    sample = (f"{sizes[0]} phsp / {sizes[1]} data / {sizes[2]} bkg events ({100 * fraction:.2g}% of the workload) "
-              f"per step, FP64 NLL+grad, mean step {t:.4f} s, scaled x{scale:.1f} by event count to full size")
+    value = 1.0 / t
+    sizes = meta["sizes"]
+    sample = ((f"the full workload, unscaled: " if args.fraction == 1.0 else f"fraction {args.fraction:g} of the workload: ") + f"{sizes[0]} phsp / {n_d} data / {sizes[2]} bkg events; data by "
+              f"accept-reject of {meta['n_cand']} phase-space candidates against the oracle's intensities "
+              f"({n_acc} accepted" + (f", topped up to {n_d} by drawing accepted events again)" if n_acc < n_d
+                                      else ")") +
+              f"; {K} timed FP64 NLL+grad evaluations after {W} untimed, mean {t:.2f} s; "
+              f"set-up {t_prep:.0f} s (generation, angular tensors {t_open:.0f} s)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t * scale, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, CPU generator)",
-        "config": {"workload": WORKLOAD_TEXT, "sample_fraction": fraction,
-                   "note": "reference has no CPU path and its CUDA build needs yaml-cpp/ROOT: timed the OpenMP FP64 "
-                           "port of its algorithm (oracle/) on the host cores"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "steps": K, "warmup": W, "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, CPU generator: same workload definition, own random draw)",
+        "config": workload_config() if args.fraction == 1.0 else dict(workload_config(), fraction=args.fraction),
+        "note": ("the reference has no CPU path (src/Analysis.cu:3939-3942): the OpenMP FP64 port of its algorithm "
+                 "(oracle/) on all host cores"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "cpu": cpu_model(),
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -361,6 +371,18 @@ def run_gpu(args, rank, world, local_rank):
     K = args.steps
     cfg, phsp, data, bkg, wts = gpu_workload(args, rank, local_rank)
     ana = ctpwa_b200.analysis.from_device(cfg, phsp, data, bkg, weights=wts, device=local_rank)
+    cpu_cfg = None
+    if world == 1 and not args.no_cpu_baseline:
+        # the same events for the CPU baseline (files the oracle reads)
+        from ctpwa_b200 import toymc, workloads as wl
+
+        d = Path(args.data_dir) / f"cpu_copy_{WORKLOAD}"
+        d.mkdir(parents=True, exist_ok=True)
+        for name, t in (("phsp", phsp), ("data", data), ("bkg", bkg)):
+            toymc.write_npy(d / f"{name}.npy", t.cpu().numpy())
+        cpu_cfg = d / "config.yml"
+        cpu_cfg.write_text(wl.config_text(WORKLOAD, str(d / "phsp.npy"), str(d / "data.npy"), str(d / "bkg.npy"),
+                                          wl.SIZES[WORKLOAD][3]))
     del phsp, data, bkg, wts
     nV, nT, nP = ana.getNVector(), ana.getNFreeTheta(), ana.getNParams()
     n_events = tuple(int(x) for x in ana.getNEvents())
@@ -504,14 +526,12 @@ def run_gpu(args, rank, world, local_rank):
         "dtype": "f32+f64 (mixed: FP32 angular tables, lineshapes and coherent sum; FP64 m0^2-m^2, log and sums)",
         "data": "synthetic, generated on the GPU (seeded phase space, accept-reject data, uniform background), "
                 "events resident in HBM",
-        "config": {"workload": WORKLOAD_TEXT, "events_per_rank": {"phsp": n_events[0], "data": n_events[1],
-                                                                  "bkg": n_events[2]},
-                   "n_params": nP, "theta_perturbed_every_step": True, "fraction": args.fraction,
-                   "launch": ana.launchShape(),
-                   "l2": f"inputs larger than L2: {streamed_bytes(layout, n_events, 'mixed', paired_mx) / 1e9:.2f} GB streamed "
-                         f"per step vs {L2_BYTES / 1e6:.0f} MB L2, no flush",
-                   "exchange": ("NCCL all-reduce of the per-sample sums per step (3*(2+2nA+nT)+4 doubles), "
-                                "then loss/gradient of the union on every rank") if world > 1 else "none (1 GPU)"},
+        "config": workload_config() if args.fraction == 1.0 else dict(workload_config(), fraction=args.fraction),
+        "run": {"events_per_rank": {"phsp": n_events[0], "data": n_events[1], "bkg": n_events[2]},
+                "n_params": nP, "launch": ana.launchShape(),
+                "streamed_gb_per_step": streamed_bytes(layout, n_events, "mixed", paired_mx) / 1e9,
+                "exchange": ("NCCL all-reduce of the per-sample sums per step (3*(2+2nA+nT)+4 doubles), "
+                             "then loss/gradient of the union on every rank") if world > 1 else "none (1 GPU)"},
         "fp64": {"value": world * 1e3 / res["fp64"]["ms"], "unit": UNIT, "ms_per_step": res["fp64"]["ms"],
                  "kernel_ms": res["fp64"]["kernel_ms"], "roofline_frac": ach64 / peak,
                  "traffic": ncu_traffic("fp64") if args.fraction == 1.0 else None,
@@ -533,8 +553,8 @@ def run_gpu(args, rank, world, local_rank):
         line["hessian"] = hess
     if world == 1 and not args.no_toy_fit:
         line["toy_fit"] = toy_fit(args, local_rank)
-    if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.data_dir, args.seed)
+    if cpu_cfg is not None:
+        line["cpu_baseline"] = cpu_baseline(str(cpu_cfg), p0, n_events)
     print(json.dumps(line), flush=True)
     return 0
 

@@ -200,7 +200,7 @@ def _gen(M, masses, n, seed, gpu, device):
 
 
 def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, seed=0, accept_reject=True,
-         device=0, gpu_generator=None, intensity=None):
+         device=0, gpu_generator=None, intensity=None, params_fn=None):
     """Write samples + config.yml for workload `name` into outdir; returns the config path.
 
     accept_reject=True draws the data sample against the model at the true
@@ -231,7 +231,7 @@ def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, se
         toymc.write_npy(out / "bkg.npy", _gen(M_JPSI, masses, n_bkg, 3001 + seed, gpu_generator, device))
         bkg_path = str(out / "bkg.npy")
     if accept_reject:
-        data = _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, intensity)
+        data = _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, intensity, params_fn)
     else:
         data = _gen(M_JPSI, masses, n_data, 2001 + seed, gpu_generator, device)
     toymc.write_npy(out / "data.npy", data)
@@ -255,9 +255,7 @@ def _gpu_intensity(device):
     return run
 
 
-def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, intensity=None):
-    from . import describe
-
+def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, intensity=None, params_fn=None):
     if intensity is None:
         intensity = _gpu_intensity(device)
     ncand = int(n_data * 12) + 10_000
@@ -267,7 +265,12 @@ def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, inten
     toymc.write_npy(out / "tiny.npy", tiny)
     cfg = out / "cand.yml"
     cfg.write_text(config_text(name, str(out / "tiny.npy"), str(out / "cand.npy")))
-    p = params_for(describe(str(cfg)))
+    if params_fn is None:
+        from . import describe
+
+        p = params_for(describe(str(cfg)))
+    else:
+        p = params_fn(str(cfg))
     I = intensity(cfg, p)
     sel = toymc.accept_reject(cand, I, seed=6001 + seed, safety=1.2)
     while sel.shape[0] < n_data:  # rare: top up from a fresh candidate batch

@@ -44,6 +44,7 @@ def oracle_lib():
                                        _I, _D, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                        ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]
         lib.orc_intensity.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D]
+        lib.orc_take.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long), ctypes.c_long]
         lib.orc_error.restype = ctypes.c_char_p
         lib.orc_error.argtypes = [ctypes.c_void_p]
         _orc = lib
@@ -135,6 +136,16 @@ class Oracle:
         out = np.zeros((self.nev[kind], self.npol, self.nA), dtype=np.complex128)
         self.lib.orc_columns(self.h, kind, ptr(t), out.ctypes.data_as(_D))
         return out
+
+    def take(self, kind, idx):
+        """Replace sample `kind` by its events idx (repeats allowed), keeping
+        their computed angular tensors."""
+        ix = np.ascontiguousarray(idx, dtype=np.int64)
+        if self.lib.orc_take(self.h, int(kind), ix.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), ix.size) != 0:
+            raise RuntimeError(self.lib.orc_error(self.h).decode())
+        nev = list(self.nev)
+        nev[kind] = int(ix.size)
+        self.nev = tuple(nev)
 
     def intensity(self, kind, params):
         p = np.ascontiguousarray(params, dtype=np.float64)

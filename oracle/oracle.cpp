@@ -23,6 +23,7 @@
 
 #include <omp.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -577,6 +578,51 @@ void* orc_open_shard(const char* config_path, int rank, int world, char* err, in
 }
 
 void orc_close(void* h) { delete static_cast<Oracle*>(h); }
+
+// Rebuilds sample k from its events idx[0..n) (repeats allowed), keeping the
+// angular tensors already computed: accept-reject selection of a candidate
+// sample, or a resample of it, without recomputing its events.
+int orc_take(void* h, int k, const long* idx, long n)
+{
+    auto* o = static_cast<Oracle*>(h);
+    try {
+        if (k < 0 || k > 2 || n < 0) throw std::runtime_error("orc_take: bad arguments");
+        OSample& S = o->smp[k];
+        const int nfin = S.s.n_final;
+        for (long i = 0; i < n; ++i)
+            if (idx[i] < 0 || idx[i] >= S.s.n) throw std::runtime_error("orc_take: index out of range");
+        OSample T;
+        T.s.n = n;
+        T.s.n_final = nfin;
+        T.s.p4.resize((size_t)n * nfin * 4);
+        if (!S.s.weights.empty()) T.s.weights.resize(n);
+        T.slamp.resize(S.slamp.size());
+        T.mom.resize(S.mom.size());
+        for (size_t gi = 0; gi < S.slamp.size(); ++gi) {
+            const size_t ps = S.s.n ? S.slamp[gi].size() / S.s.n : 0, pm = S.s.n ? S.mom[gi].size() / S.s.n : 0;
+            T.slamp[gi].resize((size_t)n * ps);
+            T.mom[gi].resize((size_t)n * pm);
+#pragma omp parallel for schedule(static)
+            for (long i = 0; i < n; ++i) {
+                std::copy_n(S.slamp[gi].begin() + (size_t)idx[i] * ps, ps, T.slamp[gi].begin() + (size_t)i * ps);
+                std::copy_n(S.mom[gi].begin() + (size_t)idx[i] * pm, pm, T.mom[gi].begin() + (size_t)i * pm);
+            }
+        }
+        for (long i = 0; i < n; ++i) {
+            std::copy_n(S.s.p4.begin() + (size_t)idx[i] * nfin * 4, nfin * 4, T.s.p4.begin() + (size_t)i * nfin * 4);
+            if (!S.s.weights.empty()) T.s.weights[i] = S.s.weights[idx[i]];
+        }
+        S = std::move(T);
+        double W = 0;
+        for (long e = 0; e < S.s.n; ++e) W += S.s.weights.empty() ? 1.0 : S.s.weights[e];
+        if (k == 1) o->W_data = W;
+        if (k == 2) o->W_bkg = W;
+        return 0;
+    } catch (const std::exception& e) {
+        o->err = e.what();
+        return -1;
+    }
+}
 
 // sizes: [nA, nTheta, nVector, npol, nGroups, n_phsp, n_data, n_bkg]
 int orc_sizes(void* h, long* out)
