@@ -26,7 +26,7 @@ import torch
 
 from . import _lib
 
-__all__ = ["analysis", "DecayInfo", "describe", "precompile", "version"]
+__all__ = ["analysis", "DecayInfo", "describe", "precompile", "spd_inverse", "version"]
 
 _PRECISIONS = {"fp64": 0, "double": 0, "plain": 0, "mixed": 1, "fp32": 1, "float": 1}
 
@@ -44,6 +44,25 @@ def precompile(config_file: str) -> float:
     if rc != 0:
         raise RuntimeError(err.value.decode("utf-8", "replace"))
     return sec.value
+
+
+def spd_inverse(a: torch.Tensor) -> torch.Tensor:
+    """Inverse of a symmetric positive definite float64 CUDA matrix, computed
+    on its device in FP64 (C ABI ctpwa_spd_inverse). Raises RuntimeError when
+    the matrix is not positive definite."""
+    if a.dim() != 2 or a.shape[0] != a.shape[1] or a.dtype != torch.float64 or not a.is_cuda:
+        raise RuntimeError("spd_inverse expects a square float64 CUDA matrix")
+    a = a.contiguous()
+    out = torch.empty_like(a)
+    info = torch.zeros(1, dtype=torch.int32, device=a.device)
+    stream = torch.cuda.current_stream(a.device).cuda_stream
+    lib = _lib.load()
+    if lib.ctpwa_spd_inverse(a.data_ptr(), a.shape[0], out.data_ptr(), info.data_ptr(), ctypes.c_void_p(stream)) != 0:
+        raise RuntimeError(_lib.error(None))
+    k = int(info.item())
+    if k:
+        raise RuntimeError(f"matrix is not positive definite (pivot {k})")
+    return out
 
 
 def describe(config_file: str) -> dict:
@@ -482,9 +501,14 @@ class analysis:
         errors = np.zeros_like(center)
         if free:
             H = hessian if hessian is not None else self.getHessian(p)
-            Hf = H[:2 * n, :2 * n].detach().to(torch.float64).cpu().numpy()[np.ix_(free, free)]
-            if np.linalg.eigvalsh(Hf)[0] > 1e-8:
-                cov = np.linalg.inv(Hf)
+            mask = torch.zeros(self.getNParams(), dtype=torch.bool)
+            mask[free] = True
+            try:
+                covd = self.getCovariance(p, free=mask, hessian=H)
+            except RuntimeError:
+                covd = None
+            if covd is not None:
+                cov = covd.cpu().numpy()[np.ix_(free, free)]
                 J = np.zeros((center.size, len(free)))
                 for c, j in enumerate(free):
                     eps = 5e-6 * max(abs(float(p[j])), 1.0)
@@ -627,6 +651,29 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return out
 
+    def getCovariance(self, params: torch.Tensor, free=None, hessian: torch.Tensor = None) -> torch.Tensor:
+        """Covariance of the fitted parameters: the inverse of the FP64 Hessian
+        over the free parameters, formed and inverted on the device (the
+        reference's fit driver inverts getHessian, example/fit.py:213,333).
+        free: boolean mask over the parameters (default: all but the fixed
+        first coupling, example/fit.py:48). float64 CUDA [nP, nP], zero in the
+        rows and columns of fixed parameters."""
+        p = self._check_params(params)
+        nP, n = self.getNParams(), self.getNVector()
+        if free is None:
+            mask = torch.ones(nP, dtype=torch.bool)
+            mask[0] = mask[n] = False
+        else:
+            mask = torch.as_tensor(free, dtype=torch.bool).reshape(-1)
+            if mask.numel() != nP:
+                raise RuntimeError(f"free mask must have {nP} entries")
+        H = hessian if hessian is not None else self.getHessian(p)
+        idx = torch.nonzero(mask).reshape(-1).to(p.device)
+        Hf = H.to(device=p.device, dtype=torch.float64).index_select(0, idx).index_select(1, idx)
+        C = torch.zeros((nP, nP), dtype=torch.float64, device=p.device)
+        C[idx.unsqueeze(1), idx.unsqueeze(0)] = spd_inverse(Hf)
+        return C
+
     def getHessian(self, params: torch.Tensor, method: str = "exact", rel_step: float = 1e-5) -> torch.Tensor:
         """Hessian [(2nV+nT), (2nV+nT)] (float64, CUDA), grouped [Re p, Im p, theta].
 
@@ -665,6 +712,19 @@ class analysis:
                                ctypes.c_void_p(stream)) != 0:
             raise RuntimeError(_lib.error(self._h))
         return out
+
+    def getGram(self, params: torch.Tensor) -> torch.Tensor:
+        """Phase-space normalisation matrix M_ab = (1/W) sum_e w_e sum_pol
+        A_a conj(A_b) at params (the reference's phase-space CGEMM matrix),
+        on the tensor cores from the mixed-form amplitudes: complex128 CUDA
+        [nA, nA]."""
+        p = self._check_params(params)
+        nA = len(self.getAmplitudeNames())
+        out = torch.empty((nA, nA, 2), dtype=torch.float64, device=p.device)
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        if self._lib.ctpwa_gram(self._h, p.data_ptr(), out.data_ptr(), ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return torch.view_as_complex(out)
 
     def getShardHvpSums(self, params: torch.Tensor, dirs: torch.Tensor) -> torch.Tensor:
         """This shard's tangent sums for the directions (float64 CUDA, to be

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SRCS = ["yaml_lite.cpp", "config.cpp", "model.cpp", "dataio.cpp", "exprdag.cpp", "lineshape_lang.cpp", "codegen.cpp", "fit.cpp",
              "capi.cpp"]
-CUDA_SRCS = ["engine.cu", "toymc.cu"]
+CUDA_SRCS = ["engine.cu", "toymc.cu", "linalg.cu"]
 
 
 def _newer(target: Path, deps) -> bool:

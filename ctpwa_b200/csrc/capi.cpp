@@ -208,6 +208,19 @@ int ctpwa_hessian_exact(ctpwa_handle* h, const double* d_params, double* d_hess,
     return CTPWA_OK;
 }
 
+int ctpwa_gram(ctpwa_handle* h, const double* d_params, double* d_out, void* stream)
+{
+    if (!h || !d_params || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    try {
+        h->eng->gram(d_params, d_out, (cudaStream_t)stream);
+    } catch (const std::length_error& e) {
+        return setErr(h, CTPWA_ERR_ARG, e.what());
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_hvp(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, double* d_out, void* stream)
 {
     if (!h || !d_params || !d_dirs || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");
@@ -423,6 +436,18 @@ int ctpwa_event_layout(const ctpwa_handle* h, int* out4)
     out4[1] = h->eng->model().npol;
     out4[2] = (int)g.slots.size();
     out4[3] = nmass;
+    return CTPWA_OK;
+}
+
+int ctpwa_spd_inverse(const double* d_a, int n, double* d_out, int* d_info, void* stream)
+{
+    if (!d_a || !d_out || !d_info) return setErr(nullptr, CTPWA_ERR_ARG, "null argument");
+    if (n <= 0 || n > 4096) return setErr(nullptr, CTPWA_ERR_ARG, "n must be in 1..4096");
+    try {
+        ctpwa::spdInverse(d_a, n, d_out, d_info, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(nullptr, CTPWA_ERR_CUDA, e.what());
+    }
     return CTPWA_OK;
 }
 

@@ -906,11 +906,13 @@ Engine::~Engine()
     devFree(d_hrows_);
     devFree(d_hvsums_);
     devFree(d_htsums_);
+    devFree(d_gpart_);
     if (mem_stream_) {
         cudaStreamSynchronize(mem_stream_);
         cudaStreamDestroy(mem_stream_);
     }
     if (hvp_lib_) cudaLibraryUnload((cudaLibrary_t)hvp_lib_);
+    if (gram_lib_) cudaLibraryUnload((cudaLibrary_t)gram_lib_);
     if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
 }
 
@@ -1597,6 +1599,20 @@ std::string jitHvpCubin(const GeneratedModel& gen, bool paired, bool* cache_hit)
                       optv, "Hessian kernel", cache_hit);
 }
 
+// The tensor-core Gram kernels of one generated model (kernels/gram.cuh).
+std::string jitGramCubin(const GeneratedModel& gen, bool paired, bool* cache_hit)
+{
+    std::string dir = kernelDir();
+    std::vector<std::string> optv = kNvrtcBase;
+    optv.push_back(std::string("-DCT_GRAM_PAIRED=") + (paired ? "1" : "0"));
+    return nvrtcCubin("#include \"gram.cuh\"\n",
+                      {{"device_helpers.cuh", readFile(dir + "/device_helpers.cuh")},
+                       {"fused_nll.cuh", readFile(dir + "/fused_nll.cuh")},
+                       {"gram.cuh", readFile(dir + "/gram.cuh")},
+                       {"model.cuh", gen.header}},
+                      optv, "Gram kernel", cache_hit);
+}
+
 void Engine::compileKernel()
 {
     auto t0 = std::chrono::steady_clock::now();
@@ -1651,6 +1667,10 @@ double precompileConfig(const std::string& config_path)
     bool hit = false;
     jitCubin(g, &hit);
     jitHvpCubin(g, false, &hit);
+    if (m.npol * 2 * m.nAmp() <= 128) {
+        jitGramCubin(g, false, &hit);
+        jitGramCubin(g, true, &hit);
+    }
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
@@ -2292,6 +2312,84 @@ void Engine::finalizeHvp(const double* d_params, const double* d_dirs, int ndir,
     f.out = d_out;
     ct_hvp_finalize_kernel<<<(ndir + 63) / 64, 64, 0, stream>>>(f);
     CT_CUDA(cudaGetLastError());
+}
+
+// argument block of ct_gram (must match CtGramArgs in kernels/gram.cuh)
+struct CtGramArgsH {
+    const void* slamp;
+    const float* evf;
+    const double* evd;
+    const double* w;
+    long long n, ld;
+    const void* K;
+    double* partials;
+    int* err;
+    int pad;
+};
+
+void Engine::compileGram()
+{
+    if (k_gram_) return;
+    const int rows = model_.npol * 2 * model_.nAmp();
+    if (rows > 128)
+        throw std::length_error("the tensor-core Gram supports npol * 2 * nA <= 128; this model has " +
+                                std::to_string(rows));
+    if (!samples_[0].slamp32) throw std::runtime_error("the Gram needs the mixed-precision tables");
+    bool hit = false;
+    std::string cubin = jitGramCubin(gen_, paired_[1], &hit);
+    cudaLibrary_t lib;
+    CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+    gram_lib_ = (void*)lib;
+    cudaKernel_t kg, kf;
+    CT_CUDA(cudaLibraryGetKernel(&kg, lib, "ct_gram"));
+    CT_CUDA(cudaLibraryGetKernel(&kf, lib, "ct_gram_finalize"));
+    gram_dsmem_ = 4 * (rows <= 64 ? 64 : 128) * 128 * 2;
+    CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributeMaxDynamicSharedMemorySize, gram_dsmem_));
+    int sms = 148;
+    CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    const int occ = std::max(1, std::min(2, residentCtas((void*)kg, 128, gram_dsmem_)));
+    const long long ntiles = (samples_[0].n + 127) / 128;
+    gram_grid_ = (int)std::max(1LL, std::min<long long>(ntiles, (long long)sms * occ));
+    alloc(d_gpart_, sizeof(double) * (size_t)gram_grid_ * rows * 2 * model_.nAmp());
+    k_gram_ = (void*)kg;
+    k_gram_fin_ = (void*)kf;
+}
+
+void Engine::gram(const double* d_params, double* d_out, cudaStream_t stream)
+{
+    compileGram();
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector();
+    // this call's couplings and parameter-only constants (the constant-bank image)
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, d_err_);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.consts = d_consts_;
+    a.err = d_err_;
+    a.kblock = d_kblock_;
+    void* args[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    const DeviceSample& d = samples_[0];
+    CtGramArgsH g;
+    std::memset(&g, 0, sizeof(g));
+    g.slamp = d.slamp32;
+    g.evf = d.evf;
+    g.evd = d.evd;
+    g.w = d.w;
+    g.n = d.n;
+    g.ld = d.ld;
+    g.K = d_kblock_;
+    g.partials = d_gpart_;
+    g.err = d_err_;
+    void* gargs[] = {&g};
+    CT_CUDA(cudaLaunchKernel(k_gram_, dim3(gram_grid_), dim3(128), gargs, (size_t)gram_dsmem_, stream));
+    int nb = gram_grid_;
+    double inv_w = 1.0 / (d.wsum > 0 ? d.wsum : 1.0);
+    void* fargs[] = {&d_gpart_, &nb, &inv_w, &d_out};
+    CT_CUDA(cudaLaunchKernel(k_gram_fin_, dim3(1), dim3(256), fargs, 0, stream));
 }
 
 void Engine::hessianVectorProducts(const double* d_params, const double* d_dirs, int ndir, double* d_out,

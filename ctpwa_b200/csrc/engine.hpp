@@ -70,6 +70,12 @@ double precompileConfig(const std::string& config_path);
 void phaseSpace(double M, const double* masses, long long n, unsigned long long seed, double* d_out,
                 cudaStream_t stream);
 
+// Inverse of the symmetric positive definite FP64 matrix a [n][n] (row-major,
+// device) into out (device), on the device in one CTA; *d_info (device) = 0,
+// or k + 1 when the k-th pivot is not positive (a not positive definite).
+// Stream-ordered, no host synchronisation (csrc/linalg.cu).
+void spdInverse(const double* d_a, int n, double* d_out, int* d_info, cudaStream_t stream);
+
 class Engine {
 public:
     Engine(const std::string& config_path, const EngineOptions& opt);
@@ -91,6 +97,10 @@ public:
     // the handle's module constant block (k_sym_) is written as by nllGrad,
     // so calls on one handle must be ordered against its other evaluations.
     void nllGradStatic(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
+    // Phase-space Gram matrix M_ab = (1/W) sum_e w_e sum_p A_a conj(A_b) of the
+    // mixed-form amplitudes at d_params, on the tensor cores; d_out [nA][nA]
+    // complex (re, im) FP64. The first call compiles the kernels.
+    void gram(const double* d_params, double* d_out, cudaStream_t stream);
     static constexpr size_t kStaticScratchBytes = size_t(2) << 20;
     // Event-sharded evaluation: the per-sample sums of this handle's events,
     // [3][nacc] + [n_phsp, W_phsp, W_data, W_bkg] (sumsSize() doubles), ready
@@ -193,6 +203,14 @@ private:
     void* k_exp_ = nullptr;
     int* d_mask_ = nullptr;  // [nBlocks] export wave mask
     void* k_pro_ = nullptr;
+    // tensor-core Gram (compiled on the first request)
+    void compileGram();
+    void* gram_lib_ = nullptr;
+    void* k_gram_ = nullptr;
+    void* k_gram_fin_ = nullptr;
+    int gram_grid_ = 0;
+    int gram_dsmem_ = 0;
+    double* d_gpart_ = nullptr;
     void* k_evc_ = nullptr;  // ct_event_cache
     double jit_seconds_ = 0.0;
     bool jit_cache_hit_ = false;

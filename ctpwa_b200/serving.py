@@ -215,7 +215,7 @@ class Server:
                 res.phase_ms = {"generate": 1e3 * (t2 - t1), "handle": 1e3 * (t3 - t2), "fit": 1e3 * (t4 - t3),
                                 "hessian": 1e3 * (t5 - t4)}
                 if spec.scan_param >= 0 and spec.scan_sigmas:
-                    res.scan = self._scan(ana, p.cpu().numpy(), nll, H.cpu().numpy(), spec, stream)
+                    res.scan = self._scan(ana, p, nll, H, spec, stream)
                     res.phase_ms["scan"] = 1e3 * (time.perf_counter() - t5)
                 res.phase_ms.update({"generate." + k: v for k, v in gen_ms.items()})
                 res.params = p.cpu().numpy()
@@ -251,16 +251,18 @@ class Server:
         """Profile-likelihood scan of parameter spec.scan_param around the
         fit: sigma from the inverse Hessian over the free parameters, one
         refit (parameter fixed) per point, started from the best fit."""
+        import torch
+
         nV = ana.getNVector()
-        n = best.size
+        n = best.numel()
         i = int(spec.scan_param)
         if not 0 <= i < n or i in (0, nV):
             raise ValueError(f"scan_param {i} is not a free parameter")
         free = np.ones(n, dtype=bool)
         free[0] = free[nV] = False
-        idx = np.flatnonzero(free)
-        cov = np.linalg.inv(H[np.ix_(idx, idx)])
-        sigma = float(np.sqrt(cov[np.searchsorted(idx, i), np.searchsorted(idx, i)]))
+        # covariance on the device (FP64 inverse of the Hessian over the free parameters)
+        sigma = float(torch.sqrt(ana.getCovariance(best, free=free, hessian=H)[i, i]))
+        best = best.cpu().numpy()
         res = ana.getFreeResParams().numpy()
         lo = np.concatenate([np.full(2 * nV, -np.inf), res[1]])
         hi = np.concatenate([np.full(2 * nV, np.inf), res[2]])

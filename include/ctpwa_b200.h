@@ -139,6 +139,21 @@ int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, doubl
  * later calls are queued on the stream without host synchronisation. */
 int ctpwa_hessian_exact(ctpwa_handle* h, const double* d_params, double* d_hess, void* stream);
 
+/* Replaces: the phase-space normalisation matrix of the reference, built by
+ * scalePhspAmpsKernel + CGEMM over its amplitude table
+ * (src/ComputeHessian.cu:1181-1197, src/Analysis.cu:729-805; used by its
+ * quadratic form, src/ComputeNLL.cu:414-597, and its Hessian).
+ * d_out [nA][nA] complex (re, im interleaved), FP64, device pointer:
+ *   M_ab = (1/W) sum_e w_e sum_pol A_a conj(A_b)
+ * over the phase-space sample at d_params, amplitudes in the mixed form
+ * (FP32), products on the tensor cores (BF16 hi + lo split operands, FP32
+ * accumulation in tensor memory, FP64 across chunks of 1024 events).
+ * Models with npol * 2 * nA > 128 are rejected with CTPWA_ERR_ARG. The first
+ * call compiles the kernels (or loads them from the kernel cache) and
+ * allocates their per-CTA partial buffer; later calls are stream-ordered
+ * without host synchronisation. */
+int ctpwa_gram(ctpwa_handle* h, const double* d_params, double* d_out, void* stream);
+
 /* Exact Hessian-vector products (no counterpart in the reference, which only
  * forms the full matrix): d_out[d] = H(d_params) d_dirs[d] for ndir directions
  * (device [ndir][n_params] in, [ndir][n_params] out). */
@@ -233,6 +248,16 @@ int ctpwa_last_parts(ctpwa_handle* h, double* out6, void* stream);
  * The reference computes the same quantity inside computeFactorNLL
  * (src/ComputeNLL.cu:21-84) and for its result export (ComputeResults.cu:22). */
 int ctpwa_intensity(ctpwa_handle* h, const double* d_params, int kind, double* d_out, void* stream);
+
+/* Replaces: the covariance step of the reference's fit driver, the inverse
+ * of the Hessian over the free parameters (example/fit.py:213,333,
+ * torch.linalg.inv on the Hessian). d_a [n][n] symmetric positive definite,
+ * row-major FP64 (device), d_out [n][n] its inverse (device, symmetrised),
+ * *d_info (device int) 0 or k + 1 when the k-th pivot of the elimination is
+ * not positive (not positive definite; d_out is then not an inverse).
+ * Gauss-Jordan elimination in FP64 in one CTA, n <= 4096; stream-ordered,
+ * no host synchronisation, no allocation. */
+int ctpwa_spd_inverse(const double* d_a, int n, double* d_out, int* d_info, void* stream);
 
 /* Toy-MC events on the device (no counterpart in the reference, whose toys
  * are generated outside the library): n events of uniform three-body phase

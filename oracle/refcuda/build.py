@@ -37,6 +37,11 @@ SOURCES = ["src/main.cu", "src/Amplitude.cu", "src/ComputeHessian.cu", "src/AmpG
 
 def build_one(ref: Path, precision: str, jobs: int) -> Path:
     os.environ.setdefault("TORCH_CUDA_ARCH_LIST", "10.0")
+    # the system compilers: the extension must use the process's shared
+    # libstdc++ (a statically linked copy breaks iostreams and exceptions
+    # across the pybind11 boundary)
+    os.environ["CC"] = os.environ.get("CTPWA_REF_CC", "/usr/bin/gcc")
+    os.environ["CXX"] = os.environ.get("CTPWA_REF_CXX", "/usr/bin/g++")
     os.environ.setdefault("MAX_JOBS", str(jobs))
     from setuptools import setup
     from torch.utils.cpp_extension import BuildExtension, CUDAExtension

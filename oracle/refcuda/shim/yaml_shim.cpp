@@ -9,11 +9,12 @@
 #include "yaml-cpp/yaml.h"
 
 #include <cerrno>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <fstream>
 #include <limits>
-#include <sstream>
+#include <iterator>
 
 namespace YAML {
 
@@ -84,36 +85,62 @@ void Node::insert(const Node& k, const Node& v) { d_->map.emplace_back(k, v); }
 
 namespace {
 
-Node readNode(std::istream& in, const std::string& path)
-{
-    std::string tag;
-    if (!(in >> tag)) throw Exception("truncated node tree " + path);
-    if (tag == "N") return Node::makeNull();
-    std::size_t k = 0;
-    if (!(in >> k)) throw Exception("malformed node tree " + path);
-    if (tag == "S") {
-        in.get();  // the newline after the length
-        std::string s(k, '\0');
-        in.read(&s[0], (std::streamsize)k);
-        if ((std::size_t)in.gcount() != k) throw Exception("truncated scalar in " + path);
-        return Node::makeScalar(s);
+// The tree file is parsed by hand (no iostream number extraction, whose
+// library implementation the host process may supply differently).
+struct TreeReader {
+    std::string buf;
+    size_t at = 0;
+    std::string path;
+
+    [[noreturn]] void bad(const char* what) { throw Exception(std::string(what) + " in node tree " + path); }
+    std::string word()
+    {
+        while (at < buf.size() && (buf[at] == ' ' || buf[at] == '\n')) ++at;
+        size_t s = at;
+        while (at < buf.size() && buf[at] != ' ' && buf[at] != '\n') ++at;
+        if (s == at) bad("truncated");
+        return buf.substr(s, at - s);
     }
-    if (tag == "Q") {
-        Node n = Node::makeSequence();
-        for (std::size_t i = 0; i < k; ++i) n.push(readNode(in, path));
-        return n;
-    }
-    if (tag == "M") {
-        Node n = Node::makeMap();
-        for (std::size_t i = 0; i < k; ++i) {
-            Node key = readNode(in, path);
-            Node val = readNode(in, path);
-            n.insert(key, val);
+    size_t count()
+    {
+        const std::string w = word();
+        size_t v = 0;
+        for (char c : w) {
+            if (c < '0' || c > '9') bad("malformed count");
+            v = v * 10 + (size_t)(c - '0');
         }
-        return n;
+        return v;
     }
-    throw Exception("unknown node tag '" + tag + "' in " + path);
-}
+    Node node()
+    {
+        const std::string tag = word();
+        if (tag == "N") return Node::makeNull();
+        const size_t k = count();
+        if (tag == "S") {
+            if (at >= buf.size() || buf[at] != '\n') bad("malformed scalar");
+            ++at;
+            if (at + k > buf.size()) bad("truncated scalar");
+            Node n = Node::makeScalar(buf.substr(at, k));
+            at += k;
+            return n;
+        }
+        if (tag == "Q") {
+            Node n = Node::makeSequence();
+            for (size_t i = 0; i < k; ++i) n.push(node());
+            return n;
+        }
+        if (tag == "M") {
+            Node n = Node::makeMap();
+            for (size_t i = 0; i < k; ++i) {
+                Node key = node();
+                Node val = node();
+                n.insert(key, val);
+            }
+            return n;
+        }
+        bad("unknown node tag");
+    }
+};
 
 }  // namespace
 
@@ -123,10 +150,12 @@ Node LoadFile(const std::string& path)
         std::ifstream src(path);
         if (!src) throw BadFile(path);
     }
-    const std::string tree = path + ".nodes";
-    std::ifstream in(tree, std::ios::binary);
-    if (!in) throw Exception("no composed node tree " + tree + " (write it with oracle/refcuda/yaml_nodes.py)");
-    return readNode(in, tree);
+    TreeReader r;
+    r.path = path + ".nodes";
+    std::ifstream in(r.path, std::ios::binary);
+    if (!in) throw Exception("no composed node tree " + r.path + " (write it with oracle/refcuda/yaml_nodes.py)");
+    r.buf.assign(std::istreambuf_iterator<char>(in), std::istreambuf_iterator<char>());
+    return r.node();
 }
 
 namespace detail {
@@ -150,12 +179,14 @@ bool toBool(const std::string& s, bool* out)
 
 bool toLong(const std::string& s, long long* out)
 {
-    std::istringstream is(s);
-    long long v = 0;
-    is >> v;
-    if (is.fail()) return false;
-    is >> std::ws;
-    if (!is.eof()) return false;
+    if (s.empty()) return false;
+    const char* b = s.c_str();
+    char* e = nullptr;
+    errno = 0;
+    const long long v = std::strtoll(b, &e, 10);
+    if (e == b || errno) return false;
+    while (*e == ' ' || *e == '\t') ++e;
+    if (*e) return false;
     *out = v;
     return true;
 }
@@ -166,12 +197,13 @@ bool toDouble(const std::string& s, double* out)
         return (*out = std::numeric_limits<double>::infinity()), true;
     if (s == "-.inf" || s == "-.Inf" || s == "-.INF") return (*out = -std::numeric_limits<double>::infinity()), true;
     if (s == ".nan" || s == ".NaN" || s == ".NAN") return (*out = std::numeric_limits<double>::quiet_NaN()), true;
-    std::istringstream is(s);
-    double v = 0;
-    is >> v;
-    if (is.fail()) return false;
-    is >> std::ws;
-    if (!is.eof()) return false;
+    if (s.empty()) return false;
+    const char* b = s.c_str();
+    char* e = nullptr;
+    const double v = std::strtod(b, &e);
+    if (e == b) return false;
+    while (*e == ' ' || *e == '\t') ++e;
+    if (*e) return false;
     *out = v;
     return true;
 }

@@ -647,3 +647,23 @@ def test_custom_expression_language_parity(tmp_path, expr):
     nll, g = ana.getNLLAndGrad(pt, "fp64")
     assert abs(float(nll) - onll) <= 1e-10 * max(1.0, abs(onll)), (float(nll), onll)
     assert np.max(np.abs(g.cpu().numpy() - og)) <= 1e-9 * np.max(np.abs(og))
+
+
+def test_device_covariance(setups):
+    """Covariance on the device: the FP64 inverse of the Hessian over the free
+    parameters equals the host inverse; a matrix that is not positive
+    definite is reported."""
+    import torch
+    import ctpwa_b200
+
+    ana, _, pt, _ = setups["kkpi"]
+    H = ana.getHessian(pt)
+    C = ana.getCovariance(pt, hessian=H).cpu().numpy()
+    n = ana.getNVector()
+    free = [j for j in range(ana.getNParams()) if j not in (0, n)]
+    Hf = H.cpu().numpy()[np.ix_(free, free)]
+    ref = np.linalg.inv(Hf)
+    assert np.max(np.abs(C[np.ix_(free, free)] - ref)) <= 1e-9 * np.max(np.abs(ref))
+    assert np.all(C[0] == 0) and np.all(C[:, n] == 0)
+    with pytest.raises(RuntimeError, match="not positive definite"):
+        ctpwa_b200.spd_inverse(-torch.eye(4, dtype=torch.float64, device="cuda"))
