@@ -62,8 +62,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-toy-fit", action="store_true", help="skip the toy-fit serving stream")
     ap.add_argument("--no-hessian", action="store_true", help="skip the full-size Hessian timing")
-    ap.add_argument("--toy-jobs", type=int, default=12)
-    ap.add_argument("--toy-rate", type=float, default=4.0)
+    ap.add_argument("--no-gram", action="store_true", help="skip the tensor-core Gram timing")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA build on a sample of the workload")
+    ap.add_argument("--no-fit-precision", action="store_true", help="skip the mixed-vs-FP64 fit comparison")
+    ap.add_argument("--toy-jobs", type=int, default=8, help="jobs per rate of the serving sweep")
+    ap.add_argument("--toy-rates", type=float, nargs="+", default=[1.0, 2.0, 5.0, 10.0, 20.0, 50.0])
     ap.add_argument("--data-dir", default=os.environ.get("CTPWA_BENCH_DIR", "/tmp/ctpwa_bench"))
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--fraction", type=float, default=1.0,
@@ -318,44 +322,190 @@ def streamed_bytes(layout, n_events, precision, paired=False):
     return per * (n_p + n_d + n_b) + 8 * n_b
 
 
+def gram_timing(ana, p0, device, reps=20):
+    """Tensor-core Gram of the phase-space sample (ctpwa_gram): device time per
+    call (CUDA events around `reps` back-to-back calls through the C ABI),
+    executed and useful tensor FLOPs."""
+    import ctypes
+
+    import torch
+
+    nA = len(ana.getAmplitudeNames())
+    npol = ana.getNPolarizations()
+    pt = torch.tensor(p0, dtype=torch.float64, device=device)
+    out = torch.empty((nA, nA, 2), dtype=torch.float64, device=device)
+    stream = torch.cuda.current_stream(device)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    for _ in range(3):
+        assert ana._lib.ctpwa_gram(ana._h, pt.data_ptr(), out.data_ptr(), sp) == 0
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ana._lib.ctpwa_gram(ana._h, pt.data_ptr(), out.data_ptr(), sp)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1) / reps
+    n_p = ana.getNEvents()[0]
+    rows = npol * 2 * nA
+    M, N = (64 if rows <= 64 else 128), (rows + 7) // 8 * 8
+    tiles = (n_p + 127) // 128
+    executed = tiles * 4 * (128 // 16) * 2.0 * M * N * 16
+    useful = 8.0 * nA * nA * npol * n_p
+    peaks = measured_peaks() or {}
+    peak = float(peaks.get("bf16_tflops") or 1590.0)
+    return {"ms": ms, "phsp_events": n_p, "n_amplitudes": nA, "npol": npol,
+            "tensor_tflops_executed": executed / (ms * 1e-3) / 1e12,
+            "tensor_frac_of_bf16_peak": executed / (ms * 1e-3) / 1e12 / peak,
+            "useful_gflop": useful / 1e9, "executed_gflop": executed / 1e9,
+            "operands": "BF16 hi + lo split (4 MMA passes), M=%d N=%d K=16, FP32 TMEM accumulation per 128-event tile, "
+                        "FP64 across tiles" % (M, N)}
+
+
+def reference_cuda_timing(args, device, reps=10):
+    """The reference's own CUDA build (FP64, complex<double>; oracle/_ref,
+    built from its sources) timed on a 1/10 sample of the workload (its .dat
+    reader limits the size), beside this library on the very same files:
+    getNLL + autograd per evaluation, resonance parameters moved every
+    evaluation, wall clock with a device synchronisation (both)."""
+    import torch
+
+    import ctpwa_b200
+    from ctpwa_b200 import workloads
+    from oracle import refcuda
+
+    if not refcuda.available("f64"):
+        return {"unavailable": "reference CUDA build not present (oracle/refcuda/build.py)"}
+    n_p, n_d, n_b, w_b = workloads.SIZES[WORKLOAD]
+    n_p, n_d, n_b = n_p // 10, n_d // 10, n_b // 10
+    out = Path(args.data_dir) / f"refcuda_{WORKLOAD}"
+    cfg = workloads.make(WORKLOAD, out, n_phsp=n_p, n_data=n_d, n_bkg=n_b, bkg_weight=w_b, seed=args.seed + 77,
+                         device=device)
+    dcfg = refcuda.dat_config(cfg)
+    ana = ctpwa_b200.analysis(dcfg, device=device)
+    nV = ana.getNVector()
+    p0 = workloads.true_params(nV, ana.getFreeResParams()[0].numpy())
+    try:
+        r = refcuda.run("f64", dcfg, [p0], timing=reps, timeout=1200)
+    except Exception as e:  # a failing reference run is reported, not fatal
+        return {"unavailable": f"reference CUDA build run failed: {str(e).splitlines()[0][:200]}"}
+    rng = np.random.default_rng(123)
+    times = {}
+    for prec in ("fp64", "mixed"):
+        ana._precision = ana._parse_precision(prec)  # the precision getNLL evaluates in
+        ts = []
+        for i in range(reps + 3):
+            q = p0.copy()
+            q[2 * nV:] *= 1 + 1e-4 * rng.standard_normal(q.size - 2 * nV)
+            pt = torch.tensor(q, dtype=torch.float64, device=device, requires_grad=True)
+            torch.cuda.synchronize(device)
+            t = time.perf_counter()
+            nll = ana.getNLL(pt)
+            (g,) = torch.autograd.grad(nll, pt)
+            torch.cuda.synchronize(device)
+            if i >= 3:
+                ts.append(time.perf_counter() - t)
+        times[prec] = statistics.median(ts)
+    ana._precision = ana._parse_precision("fp64")
+    ref_s = float(np.median(r["eval_s"]))
+    return {"sample": f"{n_p} phsp / {n_d} data / {n_b} bkg events (.dat files read by both)",
+            "reference_fp64_ms": 1e3 * ref_s, "ours_fp64_ms": 1e3 * times["fp64"],
+            "ours_mixed_ms": 1e3 * times["mixed"], "speedup_fp64": ref_s / times["fp64"],
+            "speedup_mixed": ref_s / times["mixed"], "reference_init_s": float(r["init_s"]),
+            "nll_rel_diff": abs(float(r["nll"][0]) - float(ana.getNLLAndGrad(
+                torch.tensor(p0, dtype=torch.float64, device=device), "fp64")[0])) / abs(float(r["nll"][0]))}
+
+
+def fit_precision(args, device, n_starts=5):
+    """Fitted parameters of the mixed form against the FP64 path (config 3:
+    three-chain rho model, 500k data / 5M phase space / 50k background), from
+    seeded starting points around the generating parameters; the
+    largest |difference| / sigma over the free parameters, sigma from the
+    device covariance at the FP64 minimum."""
+    import torch
+
+    import ctpwa_b200
+    from ctpwa_b200 import workloads
+
+    out_dir = Path(args.data_dir) / "fitprec_pipi_3rho"
+    cfg = workloads.make("pipi_3rho", out_dir, n_phsp=5_000_000, n_data=500_000, n_bkg=50_000, bkg_weight=0.8,
+                         seed=args.seed + 23, device=device)
+    ana = ctpwa_b200.analysis(cfg, device=device)
+    nV, nP = ana.getNVector(), ana.getNParams()
+    res = ana.getFreeResParams().numpy()
+    free = np.ones(nP, dtype=bool)
+    free[0] = free[nV] = False
+    worst, used, fits = 0.0, 0, []
+    p_true = workloads.true_params(nV, res[0])
+    for k in range(n_starts):
+        # starts around the generating parameters (couplings 20 %, resonance
+        # parameters 2 % of their range), in the basin of that minimum
+        rng = np.random.default_rng(1000 + k)
+        x0 = p_true.copy()
+        for i in range(1, nV):
+            x0[i] *= 1 + 0.2 * rng.standard_normal()
+            x0[nV + i] *= 1 + 0.2 * rng.standard_normal()
+        lo, hi = res[1], res[2]
+        x0[2 * nV:] = np.clip(x0[2 * nV:] + (rng.uniform(size=res.shape[1]) - 0.5) * 0.04 * (hi - lo),
+                              lo + 1e-7 * (hi - lo), hi - 1e-7 * (hi - lo))
+        x64, n64, e64, _, s64, _ = ana.fit(x0, max_evals=3000, ftol=1e-15, gtol=1e-8, precision="fp64")
+        xmx, nmx, emx, _, smx, _ = ana.fit(x0, max_evals=3000, ftol=1e-15, gtol=1e-8, precision="mixed")
+        fits.append({"status": [int(s64), int(smx)], "evals": [int(e64), int(emx)], "nll_fp64": n64,
+                     "dnll": nmx - n64})
+        try:
+            C = ana.getCovariance(torch.tensor(x64, dtype=torch.float64, device=device), free=free).cpu().numpy()
+        except RuntimeError:
+            continue
+        d = np.abs(xmx[free] - x64[free]) / np.sqrt(np.diag(C)[free])
+        worst = max(worst, float(d.max()))
+        used += 1
+    return {"model": "pipi_3rho 500k/5M/50k (config 3)", "starts": n_starts, "compared": used,
+            "max_abs_diff_over_sigma": worst, "fits": fits}
+
+
 def toy_fit(args, device):
-    """Toy-fit serving stream: Poisson arrivals of fit jobs (single-rho and
-    three-chain rho models, N_data log-uniform 10k-200k, 10x phase space),
-    events generated on the GPU, projected L-BFGS to convergence (<= 100
-    evaluations) + exact Hessian each, 4 concurrent slots; latency
-    percentiles per evaluation and per fit, mixed and FP64."""
+    """Serving stream of toy-MC fit jobs (the serving workload: Poisson
+    arrivals, rate swept over 1-50 jobs/s; single-rho and three-chain rho
+    models alternating; N_data log-uniform 10k-2M, 10x phase space; events
+    generated on the GPU, projected L-BFGS to convergence (<= 100
+    evaluations) + exact Hessian each, 4 concurrent slots): fits/hour and
+    latency percentiles per evaluation and per fit, mixed and FP64, per
+    rate."""
     from ctpwa_b200 import serving
 
-    out = {}
+    keys = ("jobs", "failed", "fits_per_hour", "evals", "eval_ms_p50", "eval_ms_p99", "fit_ms_p50", "fit_ms_p99",
+            "service_ms_p50", "service_ms_p99", "phase_ms_p50")
+    nd_range = (10_000, 2_000_000)
     # one untimed job per model and precision first, at the stream's largest
     # size: process-level one-time costs (library and kernel loading, growth
-    # of the memory pools to the largest job, first graph capture) are not
-    # part of a serving stream's latency
+    # of the memory pools to the largest job) are not part of a stream's latency
     warm = serving.Server(device=device, slots=4)
     try:
-        warm.run([serving.JobSpec(job_id=i, model=m, n_data=200_000, n_phsp=2_000_000, seed=90 + i, max_evals=5,
-                                  precision=p)
+        warm.run([serving.JobSpec(job_id=i, model=m, n_data=nd_range[1], n_phsp=10 * nd_range[1], seed=90 + i,
+                                  max_evals=5, precision=p)
                   for i, (m, p) in enumerate([(m, p) for m in ("pipi_rho", "pipi_3rho") for p in ("mixed", "fp64")])],
                  realtime=False)
     finally:
         warm.close()
-    for prec in ("mixed", "fp64"):
-        srv = serving.Server(device=device, slots=4)
-        try:
-            jobs = serving.poisson_stream(args.toy_rate, args.toy_jobs, nd_range=(10_000, 200_000), precision=prec,
-                                          seed=17 + args.seed)
-            t = time.perf_counter()
-            res = srv.run(jobs)
-            s = serving.summary(res, time.perf_counter() - t)
-        finally:
-            srv.close()
-        out[prec] = {k: s[k] for k in ("jobs", "failed", "fits_per_hour", "evals", "eval_ms_p50", "eval_ms_p99",
-                                        "fit_ms_p50", "fit_ms_p99", "service_ms_p50", "service_ms_p99",
-                                        "phase_ms_p50")}
-    out["config"] = {"rate_per_s": args.toy_rate, "jobs": args.toy_jobs, "slots": 4, "n_data": "log-uniform 10k-200k",
-                     "n_phsp": "10 x n_data", "models": ["pipi_rho", "pipi_3rho"],
-                     "fit": "native projected L-BFGS (ctpwa_fit), GIL released"}
-    return out
+    sweep = []
+    for rate in args.toy_rates:
+        row = {"rate_per_s": rate}
+        for prec in ("mixed", "fp64"):
+            srv = serving.Server(device=device, slots=4)
+            try:
+                jobs = serving.poisson_stream(rate, args.toy_jobs, nd_range=nd_range, precision=prec,
+                                              seed=17 + args.seed)
+                t = time.perf_counter()
+                res = srv.run(jobs)
+                s = serving.summary(res, time.perf_counter() - t)
+            finally:
+                srv.close()
+            row[prec] = {k: s[k] for k in keys}
+        sweep.append(row)
+    return {"sweep": sweep,
+            "config": {"rates_per_s": list(args.toy_rates), "jobs_per_rate": args.toy_jobs, "slots": 4,
+                       "n_data": "log-uniform 10k-2M", "n_phsp": "10 x n_data", "models": ["pipi_rho", "pipi_3rho"],
+                       "fit": "native projected L-BFGS (ctpwa_fit), GIL released"}}
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -551,8 +701,14 @@ def run_gpu(args, rank, world, local_rank):
     }
     if hess is not None:
         line["hessian"] = hess
+    if world == 1 and not args.no_gram:
+        line["gram"] = gram_timing(ana, p0, dev)
     if world == 1 and not args.no_toy_fit:
         line["toy_fit"] = toy_fit(args, local_rank)
+    if world == 1 and not args.no_fit_precision:
+        line["fit_precision"] = fit_precision(args, local_rank)
+    if world == 1 and not args.no_reference_cuda:
+        line["reference_cuda"] = reference_cuda_timing(args, local_rank)
     if cpu_cfg is not None:
         line["cpu_baseline"] = cpu_baseline(str(cpu_cfg), p0, n_events)
     print(json.dumps(line), flush=True)

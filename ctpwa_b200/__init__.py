@@ -26,7 +26,7 @@ import torch
 
 from . import _lib
 
-__all__ = ["analysis", "DecayInfo", "describe", "precompile", "spd_inverse", "version"]
+__all__ = ["analysis", "DecayInfo", "EvalBatch", "describe", "precompile", "spd_inverse", "version"]
 
 _PRECISIONS = {"fp64": 0, "double": 0, "plain": 0, "mixed": 1, "fp32": 1, "float": 1}
 
@@ -63,6 +63,49 @@ def spd_inverse(a: torch.Tensor) -> torch.Tensor:
     if k:
         raise RuntimeError(f"matrix is not positive definite (pivot {k})")
     return out
+
+
+class EvalBatch:
+    """Several analyses of one model evaluated in one launch (C ABI
+    ctpwa_batch_*): ``nll_grad`` for device parameters of several jobs at
+    once, and ``analysis.fit(..., batch=b)`` for fits on several threads whose
+    evaluations are gathered into shared launches (serving)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = _lib.load()
+        self._b = self._lib.ctpwa_batch_create(int(device))
+        if not self._b:
+            raise RuntimeError(_lib.error(None))
+        self.device = int(device)
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.ctpwa_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        self.close()
+
+    def nll_grad(self, analyses, params, precision="fp64"):
+        """[(nll, grad)] of each analysis at its float64 CUDA parameters, one launch per stage for all."""
+        n = len(analyses)
+        ps = [a._check_params(p) for a, p in zip(analyses, params)]
+        nll = [torch.empty((), dtype=torch.float64, device=p.device) for p in ps]
+        grad = [torch.empty_like(p) for p in ps]
+        VP = ctypes.c_void_p * n
+        hs = VP(*[a._h for a in analyses])
+        dp, dn, dg = VP(*[p.data_ptr() for p in ps]), VP(*[x.data_ptr() for x in nll]), VP(*[x.data_ptr() for x in grad])
+        stream = torch.cuda.current_stream(ps[0].device).cuda_stream if n else 0
+        prec = analysis._parse_precision(precision)
+        if self._lib.ctpwa_nll_grad_multi(self._b, hs, n, dp, dn, dg, prec, ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(None))
+        return list(zip(nll, grad))
+
+    def stats(self):
+        """(rounds, requests) of the gathered host evaluations so far."""
+        r, q = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        self._lib.ctpwa_batch_stats(self._b, ctypes.byref(r), ctypes.byref(q))
+        return r.value, q.value
 
 
 def describe(config_file: str) -> dict:
@@ -378,7 +421,7 @@ class analysis:
         return v.value, g
 
     def fit(self, start, lower=None, upper=None, free=None, max_evals=100, history=20, ftol=1e-13, gtol=1e-9,
-            precision=None, stream=None):
+            precision=None, stream=None, batch=None):
         """Minimise the NLL from `start` (host array of all parameters) by the
         library's projected limited-memory BFGS (``ctpwa_fit``), one
         host-buffer evaluation per function call, the whole loop in native
@@ -390,7 +433,9 @@ class analysis:
         (getFreeResParams). `lower` / `upper` / `free` (length n_params)
         replace those defaults. Returns (params, nll, evaluations, iterations,
         status, eval_ms); status 0: projected gradient <= gtol, 1: relative
-        decrease <= ftol, 2: max_evals spent, 3: no decrease found."""
+        decrease <= ftol, 2: max_evals spent, 3: no decrease found. With
+        `batch` (an EvalBatch), every evaluation is gathered with those of the
+        other fits running in the batch (one launch for all of them)."""
         self._check()
         import numpy as np
 
@@ -418,10 +463,17 @@ class analysis:
         dp = ctypes.POINTER(ctypes.c_double)
         prec = self._precision if precision is None else self._parse_precision(precision)
         sp = None if stream is None else ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
-        rc = self._lib.ctpwa_fit(self._h, x.ctypes.data_as(dp), fr.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
-                                 lo.ctypes.data_as(dp), hi.ctypes.data_as(dp), prec, int(max_evals), int(history),
-                                 float(ftol), float(gtol), out.ctypes.data_as(dp),
-                                 lat.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), sp)
+        if batch is not None:
+            rc = self._lib.ctpwa_fit_batched(batch._b, self._h, x.ctypes.data_as(dp),
+                                             fr.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), lo.ctypes.data_as(dp),
+                                             hi.ctypes.data_as(dp), prec, int(max_evals), int(history), float(ftol),
+                                             float(gtol), out.ctypes.data_as(dp),
+                                             lat.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        else:
+            rc = self._lib.ctpwa_fit(self._h, x.ctypes.data_as(dp), fr.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                     lo.ctypes.data_as(dp), hi.ctypes.data_as(dp), prec, int(max_evals), int(history),
+                                     float(ftol), float(gtol), out.ctypes.data_as(dp),
+                                     lat.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), sp)
         if rc != 0:
             raise RuntimeError(_lib.error(self._h))
         ne = int(out[1])
@@ -719,7 +771,8 @@ class analysis:
         on the tensor cores from the mixed-form amplitudes: complex128 CUDA
         [nA, nA]."""
         p = self._check_params(params)
-        nA = len(self.getAmplitudeNames())
+        nA = self._nA if getattr(self, "_nA", None) else len(self.getAmplitudeNames())
+        self._nA = nA
         out = torch.empty((nA, nA, 2), dtype=torch.float64, device=p.device)
         stream = torch.cuda.current_stream(p.device).cuda_stream
         if self._lib.ctpwa_gram(self._h, p.data_ptr(), out.data_ptr(), ctypes.c_void_p(stream)) != 0:

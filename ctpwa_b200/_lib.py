@@ -24,6 +24,18 @@ SIGNATURES = {
                                      ctypes.c_void_p]),
     "ctpwa_hessian_exact": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_gram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ctpwa_batch_create": (ctypes.c_void_p, [ctypes.c_int]),
+    "ctpwa_batch_destroy": (None, [ctypes.c_void_p]),
+    "ctpwa_nll_grad_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "ctpwa_batch_join": (ctypes.c_int, [ctypes.c_void_p]),
+    "ctpwa_batch_leave": (ctypes.c_int, [ctypes.c_void_p]),
+    "ctpwa_batch_eval_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int]),
+    "ctpwa_batch_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ctpwa_fit_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_spd_inverse": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p]),
     "ctpwa_hvp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,

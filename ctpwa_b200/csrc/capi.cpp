@@ -8,9 +8,12 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <vector>
 #include <stdexcept>
 #include <string>
 
@@ -345,6 +348,236 @@ int ctpwa_nll_grad_host(ctpwa_handle* h, const double* params, double* nll, doub
     } catch (const std::exception& e) {
         return setErr(h, CTPWA_ERR_CUDA, e.what());
     }
+    return CTPWA_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Evaluation batches: several handles of one model evaluated in one launch.
+// A batch also gathers blocking host-buffer evaluations from the fit threads
+// of a serving loop: each request waits until every fit that has joined the
+// batch has a request pending (or a short window has passed), and one of
+// the waiting threads then runs all pending requests, one multi-job launch
+// per model and precision, on the batch's stream.
+// ---------------------------------------------------------------------------
+struct ctpwa_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    ctpwa::MultiScratch scratch;
+    std::string err;
+    // request gathering
+    struct Request {
+        ctpwa_handle* h;
+        const double* params;
+        double* nll;
+        double* grad;
+        int precision;
+        int rc = CTPWA_OK;
+        bool done = false;
+    };
+    std::mutex mu;
+    std::condition_variable cv;
+    int members = 0;
+    bool running = false;
+    std::vector<Request*> pending;
+    int window_us = 200;
+    long long rounds = 0, requests = 0;
+};
+
+namespace {
+
+int batchErr(ctpwa_batch* b, int code, const std::string& m)
+{
+    if (b) b->err = m;
+    return setErr(nullptr, code, m);
+}
+
+// Runs requests (handles' host staging buffers, one multi-job launch per
+// model and precision); called by the leading thread with the lock released.
+void runRound(ctpwa_batch* b, std::vector<ctpwa_batch::Request*>& reqs)
+{
+    std::map<std::pair<const void*, int>, std::vector<ctpwa_batch::Request*>> groups;
+    for (auto* r : reqs) groups[{r->h->eng->kernelImageKey(), r->precision}].push_back(r);
+    for (auto& g : groups) {
+        auto& rs = g.second;
+        try {
+            std::vector<ctpwa::Engine*> es;
+            std::vector<const double*> dp;
+            std::vector<double*> dn, dg;
+            for (auto* r : rs) {
+                const int np = r->h->eng->nParams();
+                std::memcpy(r->h->h_pin, r->params, sizeof(double) * np);
+                if (cudaMemcpyAsync(r->h->d_params, r->h->h_pin, sizeof(double) * np, cudaMemcpyHostToDevice,
+                                    b->stream) != cudaSuccess)
+                    throw std::runtime_error("CUDA error: host-to-device copy failed");
+                es.push_back(r->h->eng.get());
+                dp.push_back(r->h->d_params);
+                dn.push_back(r->h->d_out);
+                dg.push_back(r->h->d_out + 1);
+            }
+            ctpwa::Engine::nllGradMulti(es, dp, dn, dg, g.first.second, b->scratch, b->stream);
+            for (auto* r : rs) {
+                const int np = r->h->eng->nParams();
+                if (cudaMemcpyAsync(r->h->h_pin + np, r->h->d_out, sizeof(double) * (1 + np), cudaMemcpyDeviceToHost,
+                                    b->stream) != cudaSuccess)
+                    throw std::runtime_error("CUDA error: device-to-host copy failed");
+            }
+            if (cudaStreamSynchronize(b->stream) != cudaSuccess)
+                throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
+            for (auto* r : rs) {
+                const int np = r->h->eng->nParams();
+                *r->nll = r->h->h_pin[np];
+                std::memcpy(r->grad, r->h->h_pin + np + 1, sizeof(double) * np);
+            }
+        } catch (const std::exception& e) {
+            for (auto* r : rs) r->rc = setErr(r->h, CTPWA_ERR_CUDA, e.what());
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+ctpwa_batch* ctpwa_batch_create(int device)
+{
+    auto b = std::make_unique<ctpwa_batch>();
+    b->device = device;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        batchErr(nullptr, CTPWA_ERR_CUDA, "batch: stream creation failed");
+        cudaSetDevice(prev);
+        return nullptr;
+    }
+    cudaSetDevice(prev);
+    return b.release();
+}
+
+void ctpwa_batch_destroy(ctpwa_batch* b)
+{
+    if (!b) return;
+    if (b->stream) {
+        cudaStreamSynchronize(b->stream);
+        cudaStreamDestroy(b->stream);
+    }
+    delete b;
+}
+
+int ctpwa_nll_grad_multi(ctpwa_batch* b, ctpwa_handle* const* hs, int n, const double* const* d_params,
+                         double* const* d_nll, double* const* d_grad, int precision, void* stream)
+{
+    if (!b || !hs || !d_params || !d_nll || !d_grad || n < 0) return batchErr(b, CTPWA_ERR_ARG, "null argument");
+    if (precision != CTPWA_FP64 && precision != CTPWA_MIXED) return batchErr(b, CTPWA_ERR_ARG, "precision must be 0 or 1");
+    try {
+        std::vector<ctpwa::Engine*> es;
+        std::vector<const double*> dp(d_params, d_params + n);
+        std::vector<double*> dn(d_nll, d_nll + n), dg(d_grad, d_grad + n);
+        for (int i = 0; i < n; ++i) {
+            if (!hs[i] || !d_params[i] || !d_nll[i] || !d_grad[i]) return batchErr(b, CTPWA_ERR_ARG, "null argument");
+            es.push_back(hs[i]->eng.get());
+        }
+        ctpwa::Engine::nllGradMulti(es, dp, dn, dg, precision, b->scratch, (cudaStream_t)stream);
+    } catch (const std::invalid_argument& e) {
+        return batchErr(b, CTPWA_ERR_ARG, e.what());
+    } catch (const std::exception& e) {
+        return batchErr(b, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_batch_join(ctpwa_batch* b)
+{
+    if (!b) return batchErr(nullptr, CTPWA_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(b->mu);
+    ++b->members;
+    return CTPWA_OK;
+}
+
+int ctpwa_batch_leave(ctpwa_batch* b)
+{
+    if (!b) return batchErr(nullptr, CTPWA_ERR_ARG, "null argument");
+    {
+        std::lock_guard<std::mutex> lk(b->mu);
+        if (b->members > 0) --b->members;
+    }
+    b->cv.notify_all();
+    return CTPWA_OK;
+}
+
+int ctpwa_batch_eval_host(ctpwa_batch* b, ctpwa_handle* h, const double* params, double* nll, double* grad,
+                          int precision)
+{
+    if (!b || !h || !params || !nll || !grad) return batchErr(b, CTPWA_ERR_ARG, "null argument");
+    if (precision != CTPWA_FP64 && precision != CTPWA_MIXED) return setErr(h, CTPWA_ERR_ARG, "precision must be 0 or 1");
+    ctpwa_batch::Request req{h, params, nll, grad, precision};
+    std::unique_lock<std::mutex> lk(b->mu);
+    b->pending.push_back(&req);
+    ++b->requests;
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds(b->window_us);
+    while (!req.done) {
+        const bool full = (int)b->pending.size() >= std::max(1, b->members);
+        if (!b->running && !b->pending.empty() && (full || std::chrono::steady_clock::now() >= deadline)) {
+            // this thread runs the round for everything pending
+            std::vector<ctpwa_batch::Request*> reqs;
+            reqs.swap(b->pending);
+            b->running = true;
+            ++b->rounds;
+            lk.unlock();
+            runRound(b, reqs);
+            lk.lock();
+            for (auto* r : reqs) r->done = true;
+            b->running = false;
+            b->cv.notify_all();
+            continue;
+        }
+        if (b->running || full) b->cv.wait(lk);
+        else b->cv.wait_until(lk, deadline);
+    }
+    return req.rc;
+}
+
+int ctpwa_batch_stats(const ctpwa_batch* b, long long* rounds, long long* requests)
+{
+    if (!b) return CTPWA_ERR_ARG;
+    if (rounds) *rounds = b->rounds;
+    if (requests) *requests = b->requests;
+    return CTPWA_OK;
+}
+
+int ctpwa_fit_batched(ctpwa_batch* b, ctpwa_handle* h, double* params, const unsigned char* free_mask, const double* lo,
+                      const double* hi, int precision, int max_evals, int history, double ftol, double gtol,
+                      double* out4, float* eval_ms)
+{
+    if (!b || !h || !params || !free_mask || !lo || !hi || !out4) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (max_evals < 1 || history < 1) return setErr(h, CTPWA_ERR_ARG, "max_evals and history must be >= 1");
+    const int np = h->eng->nParams();
+    for (int i = 0; i < np; ++i)
+        if (!(lo[i] <= hi[i])) return setErr(h, CTPWA_ERR_ARG, "lower bound above upper bound");
+    ctpwa::BoxLbfgsOptions opt;
+    opt.max_evals = max_evals;
+    opt.m = history;
+    opt.ftol = ftol;
+    opt.gtol = gtol;
+    int ne = 0;
+    auto fg = [&](const double* x, double* f, double* g) -> int {
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = ctpwa_batch_eval_host(b, h, x, f, g, precision);
+        if (eval_ms && ne < max_evals)
+            eval_ms[ne] = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        ++ne;
+        return rc;
+    };
+    ctpwa_batch_join(b);
+    ctpwa::BoxLbfgsResult r;
+    const int rc = ctpwa::boxLbfgs(fg, np, params, free_mask, lo, hi, opt, &r);
+    ctpwa_batch_leave(b);
+    if (rc != 0) return rc;
+    out4[0] = r.f;
+    out4[1] = r.evals;
+    out4[2] = r.iters;
+    out4[3] = r.status;
     return CTPWA_OK;
 }
 

@@ -486,6 +486,26 @@ __global__ void ct_prepare_kernel(const double* __restrict__ params, const int* 
     v[2 * a + 1] = params[nc + c] * ratio[a];
 }
 
+// one block per job of a multi-job evaluation: ct_prepare_kernel's work
+struct PrepareArgs {
+    const double* params;
+    const int* chain;
+    const double* ratio;
+    int nA, nc;
+    double* v;
+    int* err;
+};
+__global__ void ct_prepare_multi_kernel(const PrepareArgs* __restrict__ ps)
+{
+    const PrepareArgs& P = ps[blockIdx.x];
+    if (threadIdx.x == 0 && P.err) *P.err = 0;
+    for (int a = threadIdx.x; a < P.nA; a += blockDim.x) {
+        const int c = P.chain[a];
+        P.v[2 * a] = P.params[c] * P.ratio[a];
+        P.v[2 * a + 1] = P.params[P.nc + c] * P.ratio[a];
+    }
+}
+
 struct FinalizeArgs {
     const double* partials;
     int nacc, nA, nc, nT;
@@ -536,7 +556,7 @@ __global__ void __launch_bounds__(1024) ct_rowsum_kernel(const double* __restric
 // One CTA: deterministic column sums of the CTA partials, then loss/gradient
 // assembly (src/Analysis.cu:1134-1183) and the coupling-gradient transform
 // dL/dp_c = (1/p_c) sum_{a in c} conj(g_a) v_a (src/AmpGen.cu:3581-3637).
-__global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
+__device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
 {
     extern __shared__ double sh[];  // [3][nacc] sample sums, then gv [2 nA], gt [nT]
     double* sums = sh;
@@ -618,6 +638,14 @@ __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A)
         A.out_parts[4] = W_bkg;
         A.out_parts[5] = n_phsp;
     }
+}
+
+__global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A) { ct_finalize_body(A); }
+
+// one CTA per job of a multi-job evaluation (all jobs of one model: same shared-memory size)
+__global__ void __launch_bounds__(1024) ct_finalize_multi_kernel(const FinalizeArgs* __restrict__ fs)
+{
+    ct_finalize_body(fs[blockIdx.x]);
 }
 
 // ============================================================================
@@ -1642,11 +1670,30 @@ void Engine::compileKernel()
     k_exp_ = (void*)kexp;
     k_f64_ = (void*)k64;
     k_mixed_ = (void*)kmx;
+    // multi-job variants [precision][paired]
+    const char* multi_names[2][2] = {{"ct_fused_f64_multi", "ct_fused_f64_pc_multi"},
+                                     {"ct_fused_mixed_multi", "ct_fused_mixed_pc_multi"}};
+    for (int pr = 0; pr < 2; ++pr)
+        for (int pc = 0; pc < 2; ++pc) {
+            cudaKernel_t km;
+            CT_CUDA(cudaLibraryGetKernel(&km, lib, multi_names[pr][pc]));
+            k_multi_[pr][pc] = (void*)km;
+        }
+    cudaKernel_t kprom;
+    CT_CUDA(cudaLibraryGetKernel(&kprom, lib, "ct_prologue_multi"));
+    k_pro_multi_ = (void*)kprom;
     for (int pr = 0; pr < 2; ++pr)
         if (shape_.dsmem[pr] > 0)
-            for (void* k : {pr == 0 ? k_f64_ : k_mixed_, k_pc_[pr]})
+            for (void* k : {pr == 0 ? k_f64_ : k_mixed_, k_pc_[pr], k_multi_[pr][0], k_multi_[pr][1]})
                 CT_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, shape_.dsmem[pr]));
     k_int_ = (void*)kin;
+    {
+        std::string key = gen_.header;
+        for (int pr = 0; pr < 2; ++pr)
+            key += "|" + std::to_string(shape_.block[pr]) + "," + std::to_string(shape_.minb[pr]) + "," +
+                   std::to_string(shape_.dsmem[pr]);
+        image_key_ = (const void*)(uintptr_t)fnv1a(key);
+    }
     jit_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
@@ -1774,6 +1821,139 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     f.err = d_err_;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
+    CT_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Several jobs of one model in one evaluation (serving): one prepare, one
+// prologue, one fused and one finalize launch for all of them. Each job keeps
+// its own grid of CTAs, partial rows and finalize, so its results are those
+// of its own nllGrad, bit for bit; only the per-call constants come from the
+// job's image in global memory instead of the constant bank.
+// ---------------------------------------------------------------------------
+MultiScratch::~MultiScratch()
+{
+    if (host) cudaFreeHost(host);
+    if (dev) cudaFreeAsync(dev, 0);
+    if (copied) cudaEventDestroy(copied);
+}
+
+void Engine::nllGradMulti(const std::vector<Engine*>& es, const std::vector<const double*>& d_params,
+                          const std::vector<double*>& d_nll, const std::vector<double*>& d_grad, int precision,
+                          MultiScratch& sc, cudaStream_t stream)
+{
+    const int nj = (int)es.size();
+    if (nj == 0) return;
+    if (d_params.size() != es.size() || d_nll.size() != es.size() || d_grad.size() != es.size())
+        throw std::invalid_argument("multi evaluation: one parameter, NLL and gradient pointer per job");
+    Engine* e0 = es[0];
+    const int pr = precision == kMixed ? 1 : 0;
+    for (Engine* e : es) {
+        if (e->opt_.device != e0->opt_.device)
+            throw std::invalid_argument("multi evaluation: all jobs must be on one device");
+        if (e->kernelImageKey() != e0->kernelImageKey() ||
+            e->shape_.block[pr] != e0->shape_.block[pr] || e->shape_.dsmem[pr] != e0->shape_.dsmem[pr])
+            throw std::invalid_argument("multi evaluation: all jobs must share one model (generated kernel) and layout");
+        if (precision == kMixed && !e->samples_[0].slamp32)
+            throw std::runtime_error("mixed-precision tables were not built");
+    }
+    // staging: [CtArgsH x nj][PrepareArgs x nj][FinalizeArgs x nj][cta_off x (nj + 1)]
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t o_args = 0, o_prep = up(sizeof(CtArgsH) * nj), o_fin = o_prep + up(sizeof(PrepareArgs) * nj),
+                 o_off = o_fin + up(sizeof(FinalizeArgs) * nj), bytes = o_off + up(sizeof(int) * (nj + 1));
+    if (!sc.copied) CT_CUDA(cudaEventCreateWithFlags(&sc.copied, cudaEventDisableTiming));
+    CT_CUDA(cudaEventSynchronize(sc.copied));  // the previous call's copy has left the host buffer
+    if (bytes > sc.cap) {
+        if (sc.host) cudaFreeHost(sc.host);
+        if (sc.dev) cudaFreeAsync(sc.dev, stream);
+        sc.host = nullptr;
+        sc.dev = nullptr;
+        CT_CUDA(cudaMallocHost(&sc.host, bytes));
+        CT_CUDA(cudaMallocAsync(&sc.dev, bytes, stream));
+        sc.cap = bytes;
+    }
+    unsigned char* hb = (unsigned char*)sc.host;
+    unsigned char* db = (unsigned char*)sc.dev;
+    CtArgsH* ha = (CtArgsH*)(hb + o_args);
+    PrepareArgs* hp = (PrepareArgs*)(hb + o_prep);
+    FinalizeArgs* hf = (FinalizeArgs*)(hb + o_fin);
+    int* hoff = (int*)(hb + o_off);
+    int total = 0, shm_max = 0;
+    for (int j = 0; j < nj; ++j) {
+        Engine* e = es[j];
+        const CtaLayout& lay = e->lay_[pr];
+        const Model& m = e->model_;
+        const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+        hoff[j] = total;
+        CtArgsH& a = ha[j];
+        std::memset(&a, 0, sizeof(a));
+        int ns = 0;
+        for (int k = 0; k < 3; ++k) {
+            if (lay.cta[k][1] == 0) continue;
+            CtSampleH& smp = a.s[ns++];
+            const DeviceSample& d = e->samples_[k];
+            smp.slamp = pr ? (const void*)d.slamp32 : (e->paired_[0] ? (const void*)d.slamp64p : (const void*)d.slamp64);
+            smp.ev = pr ? (const void*)d.evf : (const void*)d.ev64;
+            smp.evd = pr ? d.evd : nullptr;
+            smp.w = d.w;
+            smp.n = d.n;
+            smp.ld = d.ld;
+            smp.kind = k;
+            smp.cta_begin = lay.cta[k][0];
+            smp.cta_count = lay.cta[k][1];
+            smp.vw_scale = 1.0 / (e->samples_[0].wsum > 0 ? e->samples_[0].wsum : 1.0);
+        }
+        a.nsamp = ns;
+        a.theta = d_params[j] + 2 * nc;
+        a.v = e->d_v_;
+        a.partials = e->d_partials_;
+        a.consts = e->d_consts_;
+        a.err = e->d_err_;
+        a.kblock = e->d_kblock_;
+        a.cta_base = -total;
+        hp[j] = PrepareArgs{d_params[j], e->d_amp_chain_, e->d_ratio_, nA, nc, e->d_v_, e->d_err_};
+        FinalizeArgs& f = hf[j];
+        std::memset(&f, 0, sizeof(f));
+        f.partials = e->d_partials_;
+        f.nacc = 2 + 2 * nA + nT;
+        f.nA = nA;
+        f.nc = nc;
+        f.nT = nT;
+        for (int k = 0; k < 3; ++k) {
+            f.cta[k][0] = lay.cta[k][0];
+            f.cta[k][1] = lay.cta[k][1];
+            f.has[k] = lay.cta[k][1] > 0;
+        }
+        f.n_phsp = (double)e->samples_[0].n;
+        f.W_data = e->samples_[1].wsum;
+        f.W_bkg = e->has_bkg_ ? e->samples_[2].wsum : 0.0;
+        f.params = d_params[j];
+        f.v = e->d_v_;
+        f.chain = e->d_amp_chain_;
+        f.gauss_idx = e->d_gauss_idx_;
+        f.gauss_ms = e->d_gauss_ms_;
+        f.ngauss = (int)m.gauss.size();
+        f.out_nll = d_nll[j];
+        f.out_grad = d_grad[j];
+        f.out_parts = e->d_parts_;
+        f.err = e->d_err_;
+        shm_max = std::max(shm_max, (int)(sizeof(double) * (3 * f.nacc + 2 * nA + 8)));
+        total += lay.grid;
+    }
+    hoff[nj] = total;
+    CT_CUDA(cudaMemcpyAsync(db, hb, bytes, cudaMemcpyHostToDevice, stream));
+    CT_CUDA(cudaEventRecord(sc.copied, stream));
+    ct_prepare_multi_kernel<<<nj, 128, 0, stream>>>((const PrepareArgs*)(db + o_prep));
+    CT_CUDA(cudaGetLastError());
+    const CtArgsH* dargs = (const CtArgsH*)(db + o_args);
+    void* pargs[] = {&dargs};
+    CT_CUDA(cudaLaunchKernel(e0->k_pro_multi_, dim3(nj), dim3(32), pargs, 0, stream));
+    const int* doff = (const int*)(db + o_off);
+    int njobs = nj;
+    void* fargs[] = {&dargs, &doff, &njobs};
+    CT_CUDA(cudaLaunchKernel(e0->k_multi_[pr][e0->paired_[pr] ? 1 : 0], dim3(total), dim3(e0->shape_.block[pr]), fargs,
+                             (size_t)e0->shape_.dsmem[pr], stream));
+    ct_finalize_multi_kernel<<<nj, 1024, shm_max, stream>>>((const FinalizeArgs*)(db + o_fin));
     CT_CUDA(cudaGetLastError());
 }
 

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <cstdint>
 #include <vector>
 
 namespace ctpwa {
@@ -43,6 +44,19 @@ struct DeviceSample {
     double* evd = nullptr;     // [nevd][ld] mixed form, FP64 frontier values
     double* w = nullptr;       // weights or nullptr
     double wsum = 0.0;         // sum of weights (or n)
+};
+
+// Host staging and device copy of the argument tables of a multi-job
+// evaluation (Engine::nllGradMulti); reused across calls, grown on demand.
+struct MultiScratch {
+    void* host = nullptr;  // pinned
+    void* dev = nullptr;
+    size_t cap = 0;
+    cudaEvent_t copied = nullptr;  // the last host -> device copy of the tables
+    MultiScratch() = default;
+    MultiScratch(const MultiScratch&) = delete;
+    MultiScratch& operator=(const MultiScratch&) = delete;
+    ~MultiScratch();
 };
 
 struct EngineOptions {
@@ -97,6 +111,18 @@ public:
     // the handle's module constant block (k_sym_) is written as by nllGrad,
     // so calls on one handle must be ordered against its other evaluations.
     void nllGradStatic(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
+    // The evaluations of several handles of one model (same generated kernel)
+    // in one prepare, prologue, fused and finalize launch on `stream`; each
+    // job's NLL and gradient equal its own nllGrad's. Device pointers per job.
+    // Identity of the compiled fused kernel image (generated model and
+    // launch layout): handles with equal keys can share a multi-job launch.
+    const void* kernelImageKey() const
+    {
+        return (const void*)((uintptr_t)image_key_ ^ (paired_[0] ? 1u : 0u) ^ (paired_[1] ? 2u : 0u));
+    }
+    static void nllGradMulti(const std::vector<Engine*>& es, const std::vector<const double*>& d_params,
+                             const std::vector<double*>& d_nll, const std::vector<double*>& d_grad, int precision,
+                             MultiScratch& sc, cudaStream_t stream);
     // Phase-space Gram matrix M_ab = (1/W) sum_e w_e sum_p A_a conj(A_b) of the
     // mixed-form amplitudes at d_params, on the tensor cores; d_out [nA][nA]
     // complex (re, im) FP64. The first call compiles the kernels.
@@ -203,6 +229,9 @@ private:
     void* k_exp_ = nullptr;
     int* d_mask_ = nullptr;  // [nBlocks] export wave mask
     void* k_pro_ = nullptr;
+    void* k_multi_[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [plain, mixed][paired]
+    void* k_pro_multi_ = nullptr;
+    const void* image_key_ = nullptr;
     // tensor-core Gram (compiled on the first request)
     void compileGram();
     void* gram_lib_ = nullptr;

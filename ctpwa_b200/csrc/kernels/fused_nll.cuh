@@ -125,9 +125,17 @@ __constant__ CtConsts ct_k;
 
 // The parameter-only part of every lineshape (prologue, one thread), then
 // the constant-bank image of this call (one warp).
+__device__ __forceinline__ void ct_prologue_body(const CtArgs& A);
 extern "C" __global__ void ct_prologue(CtArgs A)
 {
     if (blockIdx.x != 0) return;
+    ct_prologue_body(A);
+}
+// one block per job of a multi-job evaluation
+extern "C" __global__ void ct_prologue_multi(const CtArgs* __restrict__ jobs) { ct_prologue_body(jobs[blockIdx.x]); }
+
+__device__ __forceinline__ void ct_prologue_body(const CtArgs& A)
+{
     if (threadIdx.x == 0) model_prologue(A.theta, A.consts);
     __syncthreads();
     if (!A.kblock) return;
@@ -293,7 +301,10 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_event_cache(const doub
 // L: type of the lineshapes, their derivatives and the per-thread gradient
 //    sums
 // PH_ONLY: the launch serves phase-space events only
-template <typename R, typename L, bool PH_ONLY, int BLOCK, int STAGE, bool ACC_SMEM, bool PAIRED>
+// MULTI: one launch over several jobs of this model (ct_fused_*_multi): the
+// per-call constants are this job's image in global memory (A.kblock)
+// instead of the constant bank.
+template <typename R, typename L, bool PH_ONLY, int BLOCK, int STAGE, bool ACC_SMEM, bool PAIRED, bool MULTI = false>
 __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
 {
     typedef typename CtVec2<R>::type SL2;
@@ -321,13 +332,26 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     // parameter-only constants and couplings from the constant bank: FP64,
     // and FP32 hi + lo pairs for the FP32 form (a single FP32 rounding would
     // bias every event alike)
-    const double* sC = ct_k.c;
-    const float* sCfh = ct_k.ch;
-    const float* sCfl = ct_k.cl;
-    auto vr = [](int a) -> L { return sizeof(L) == 4 ? (L)ct_k.vh[2 * a] : (L)ct_k.v[2 * a]; };
-    auto vi = [](int a) -> L { return sizeof(L) == 4 ? (L)ct_k.vh[2 * a + 1] : (L)ct_k.v[2 * a + 1]; };
-    auto vrl = [](int a) -> L { return (L)ct_k.vl[2 * a]; };
-    auto vil = [](int a) -> L { return (L)ct_k.vl[2 * a + 1]; };
+    const CtConsts* __restrict__ Kg = MULTI ? (const CtConsts*)A.kblock : nullptr;
+    const double* sC = MULTI ? Kg->c : ct_k.c;
+    const float* sCfh = MULTI ? Kg->ch : ct_k.ch;
+    const float* sCfl = MULTI ? Kg->cl : ct_k.cl;
+    auto vr = [&](int a) -> L {
+        if constexpr (MULTI) return sizeof(L) == 4 ? (L)__ldg(Kg->vh + 2 * a) : (L)__ldg(Kg->v + 2 * a);
+        return sizeof(L) == 4 ? (L)ct_k.vh[2 * a] : (L)ct_k.v[2 * a];
+    };
+    auto vi = [&](int a) -> L {
+        if constexpr (MULTI) return sizeof(L) == 4 ? (L)__ldg(Kg->vh + 2 * a + 1) : (L)__ldg(Kg->v + 2 * a + 1);
+        return sizeof(L) == 4 ? (L)ct_k.vh[2 * a + 1] : (L)ct_k.v[2 * a + 1];
+    };
+    auto vrl = [&](int a) -> L {
+        if constexpr (MULTI) return (L)__ldg(Kg->vl + 2 * a);
+        return (L)ct_k.vl[2 * a];
+    };
+    auto vil = [&](int a) -> L {
+        if constexpr (MULTI) return (L)__ldg(Kg->vl + 2 * a + 1);
+        return (L)ct_k.vl[2 * a + 1];
+    };
 
     // all per-event work: ap / bp / slp point at this event's frontier values
     // (table type, FP64) and angular values, consecutive values `ks` / `ss`
@@ -649,6 +673,41 @@ extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_m
 extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB) ct_fused_mixed_pc(CtArgs a)
 {
     ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE, CT_MX_ACC != 0, true>(a);
+}
+
+// Several jobs of this model in one launch: the CTAs [cta_off[j],
+// cta_off[j+1]) serve job j, whose CtArgs (cta_base = -cta_off[j], kblock =
+// its constants image) hold its samples and partial rows; each job's
+// partial rows are exactly those of its own launch.
+__device__ __forceinline__ int ct_multi_job(const int* __restrict__ cta_off, int njobs)
+{
+    int j = 0;
+    while (j + 1 < njobs && (int)blockIdx.x >= __ldg(cta_off + j + 1)) ++j;
+    return j;
+}
+extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB)
+    ct_fused_f64_multi(const CtArgs* __restrict__ jobs, const int* __restrict__ cta_off, int njobs)
+{
+    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE, CT_F64_ACC != 0, false, true>(
+        jobs[ct_multi_job(cta_off, njobs)]);
+}
+extern "C" __global__ void __launch_bounds__(CT_F64_BLOCK, CT_F64_MINB)
+    ct_fused_f64_pc_multi(const CtArgs* __restrict__ jobs, const int* __restrict__ cta_off, int njobs)
+{
+    ct_fused_body<double, double, false, CT_F64_BLOCK, CT_F64_STAGE, CT_F64_ACC != 0, true, true>(
+        jobs[ct_multi_job(cta_off, njobs)]);
+}
+extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB)
+    ct_fused_mixed_multi(const CtArgs* __restrict__ jobs, const int* __restrict__ cta_off, int njobs)
+{
+    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE, CT_MX_ACC != 0, false, true>(
+        jobs[ct_multi_job(cta_off, njobs)]);
+}
+extern "C" __global__ void __launch_bounds__(CT_MX_BLOCK, CT_MX_MINB)
+    ct_fused_mixed_pc_multi(const CtArgs* __restrict__ jobs, const int* __restrict__ cta_off, int njobs)
+{
+    ct_fused_body<float, float, false, CT_MX_BLOCK, CT_MX_STAGE, CT_MX_ACC != 0, true, true>(
+        jobs[ct_multi_job(cta_off, njobs)]);
 }
 
 // Partial-wave integrals of sample s[0] (FP64): per resonance block i,

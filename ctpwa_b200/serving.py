@@ -109,10 +109,17 @@ class Server:
     """Runs fit jobs on one GPU with `slots` concurrent jobs and a device-memory budget."""
 
     def __init__(self, device: int = 0, slots: int = 4, budget_bytes: Optional[int] = None,
-                 workdir: Optional[str] = None):
+                 workdir: Optional[str] = None, batch: bool = False):
         import torch
 
         self.device = int(device)
+        # batch=True: the fits' evaluations are gathered across the running
+        # jobs into shared launches (one per model and precision and round)
+        self.batch = None
+        if batch:
+            import ctpwa_b200
+
+            self.batch = ctpwa_b200.EvalBatch(self.device)
         self.slots = int(slots)
         if budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
@@ -135,6 +142,9 @@ class Server:
 
     def close(self):
         shutil.rmtree(self.workdir, ignore_errors=True)
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
 
     # ----------------------------------------------------------- admission
     # resident device bytes per event of each model, shared by all servers of the process
@@ -243,7 +253,7 @@ class Server:
         import torch
 
         x, nll, n_evals, _, _, lat = ana.fit(start, max_evals=spec.max_evals, history=20, ftol=1e-13, gtol=1e-9,
-                                             stream=stream)
+                                             stream=stream, batch=self.batch)
         return torch.tensor(x, dtype=torch.float64, device=torch.device("cuda", self.device)), nll, n_evals, lat
 
     @staticmethod

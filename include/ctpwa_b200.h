@@ -233,6 +233,43 @@ int ctpwa_fit(ctpwa_handle* h, double* params, const unsigned char* free_mask, c
               int precision, int max_evals, int history, double ftol, double gtol, double* out4, float* eval_ms,
               void* stream);
 
+/* Evaluation batches (no counterpart in the reference, which serves one
+ * analysis per process): several handles of one model (equal configuration,
+ * hence one generated kernel) evaluated in one prepare, one prologue, one
+ * fused and one finalize launch. Each job keeps its own CTAs, partial rows
+ * and finalize, so its NLL and gradient equal those of ctpwa_nll_grad bit
+ * for bit. A batch owns a CUDA stream and a small argument table on `device`
+ * (grown on demand by the first calls); jobs of another model or device are
+ * rejected with CTPWA_ERR_ARG. */
+typedef struct ctpwa_batch ctpwa_batch;
+ctpwa_batch* ctpwa_batch_create(int device);
+void ctpwa_batch_destroy(ctpwa_batch* b);
+
+/* Device pointers per job; stream-ordered on `stream` (not the batch's own),
+ * no host synchronisation beyond the reuse of the batch's argument table. */
+int ctpwa_nll_grad_multi(ctpwa_batch* b, ctpwa_handle* const* hs, int n, const double* const* d_params,
+                         double* const* d_nll, double* const* d_grad, int precision, void* stream);
+
+/* Serving: blocking host-buffer evaluation gathered across threads. A fit
+ * that joined the batch (ctpwa_batch_join) submits each evaluation with
+ * ctpwa_batch_eval_host; the call returns when its result is in nll / grad.
+ * Requests wait until every joined fit has one pending, or at most 200
+ * microseconds, and one waiting thread then runs all pending requests (one
+ * multi-job launch per model and precision) on the batch's stream.
+ * ctpwa_batch_leave ends a fit's membership. */
+int ctpwa_batch_join(ctpwa_batch* b);
+int ctpwa_batch_leave(ctpwa_batch* b);
+int ctpwa_batch_eval_host(ctpwa_batch* b, ctpwa_handle* h, const double* params, double* nll, double* grad,
+                          int precision);
+/* rounds run and requests served so far (either pointer may be NULL) */
+int ctpwa_batch_stats(const ctpwa_batch* b, long long* rounds, long long* requests);
+
+/* ctpwa_fit with every evaluation gathered into the batch (joins the batch
+ * for the duration of the minimisation). Same arguments and results. */
+int ctpwa_fit_batched(ctpwa_batch* b, ctpwa_handle* h, double* params, const unsigned char* free_mask, const double* lo,
+                      const double* hi, int precision, int max_evals, int history, double ftol, double gtol,
+                      double* out4, float* eval_ms);
+
 /* The same minimiser over a host function (no GPU): fn(x, &f, g, user)
  * returns 0, or a nonzero code that ends the minimisation and is returned. */
 typedef int (*ctpwa_fg_fn)(const double* x, double* f, double* g, void* user);

@@ -3,9 +3,9 @@
 M_ab = (1/W) sum_e w_e sum_pol A_a conj(A_b) (the reference's normalisation
 matrix, src/ComputeHessian.cu:1181-1197 with src/Analysis.cu:729-805). The
 device forms the amplitudes in the mixed form (FP32) and the products on the
-tensor cores (BF16 hi + lo operands, FP32 accumulation per 1024 events, FP64
-beyond); the oracle's amplitudes and sums are FP64. Tolerance: 2e-6 of the
-largest |M_ab| elementwise, and 2e-6 relative on the phase-space mean
+tensor cores (BF16 hi + lo operands, FP32 accumulation per 128-event tile, FP64
+beyond); the oracle's amplitudes and sums are FP64. Tolerance: 1e-6 of the
+largest |M_ab| elementwise (measured 3.5e-7 to 4.5e-7), and 1e-6 relative on the phase-space mean
 intensity v^T M conj(v).
 """
 import numpy as np
@@ -36,18 +36,18 @@ def test_gram_matches_oracle(tmp_path, name):
     R = np.einsum("epa,epb->ab", A, np.conj(A)) / A.shape[0]
     scale = np.max(np.abs(R))
     err = np.max(np.abs(M - R)) / scale
-    assert err <= 2e-6, err
+    assert err <= 1e-6, err
     # a second call at other parameters: no state carried over
     q = p.copy()
     q[2 * nV:] *= 1.01
     M2 = ana.getGram(torch.tensor(q, dtype=torch.float64, device="cuda")).cpu().numpy()
     A2 = orc.columns(0, q[2 * nV:])
     R2 = np.einsum("epa,epb->ab", A2, np.conj(A2)) / A2.shape[0]
-    assert np.max(np.abs(M2 - R2)) <= 2e-6 * np.max(np.abs(R2))
+    assert np.max(np.abs(M2 - R2)) <= 1e-6 * np.max(np.abs(R2))
     # the phase-space mean intensity as the quadratic form of the couplings
     _, _, parts = orc.nll_grad(p)
     cp = ana.getModel()["coupling"]
     v = np.array([r * complex(p[c], p[nV + c]) for c, r in zip(cp["amp_chain"], cp["ratio"])])
     f = np.real(v @ M @ np.conj(v))
     mean = parts[2] / parts[5]
-    assert abs(f - mean) <= 2e-6 * abs(mean), (f, mean)
+    assert abs(f - mean) <= 1e-6 * abs(mean), (f, mean)

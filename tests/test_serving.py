@@ -138,3 +138,74 @@ def test_profile_scan_is_parabolic_near_the_minimum():
             assert dnll > -1e-6, (v, dnll)
             assert abs(dnll - 0.5 * s * s) <= 0.15 * s * s, (s, dnll)
         assert r.scan[0][0] < r.params[spec.scan_param] < r.scan[-1][0]
+
+
+@pytest.mark.gpu
+def test_multi_job_launch_equals_single_evaluations(tmp_path):
+    """Several handles of one model evaluated in one launch per stage
+    (ctpwa_nll_grad_multi): each job's NLL and gradient are those of its own
+    evaluation, bit for bit, in both precisions; a handle of another model
+    is rejected."""
+    import torch
+    import ctpwa_b200
+    from ctpwa_b200 import workloads
+
+    anas, params = [], []
+    for k, (nph, nda, nbk) in enumerate([(30_011, 3_001, 0), (80_003, 8_009, 1_001), (12_007, 1_201, 0)]):
+        cfg = workloads.make("pipi_3rho", tmp_path / f"j{k}", n_phsp=nph, n_data=nda, n_bkg=nbk,
+                             accept_reject=False, seed=40 + k)
+        a = ctpwa_b200.analysis(cfg)
+        p = workloads.true_params(a.getNVector(), a.getFreeResParams()[0].numpy())
+        p[2 * a.getNVector():] *= 1 + 0.01 * (k + 1)
+        anas.append(a)
+        params.append(torch.tensor(p, dtype=torch.float64, device="cuda"))
+    b = ctpwa_b200.EvalBatch(0)
+    try:
+        for prec in ("fp64", "mixed"):
+            for _ in range(2):  # the second call reuses the argument table
+                res = b.nll_grad(anas, params, prec)
+                torch.cuda.synchronize()
+                for a, p, (n_m, g_m) in zip(anas, params, res):
+                    n_s, g_s = a.getNLLAndGrad(p, prec)
+                    assert float(n_m) == float(n_s) and torch.equal(g_m, g_s), prec
+        other = ctpwa_b200.analysis(workloads.make("pipi_rho", tmp_path / "o", n_phsp=5_000, n_data=500, n_bkg=0,
+                                                   accept_reject=False, seed=1))
+        po = torch.tensor(workloads.true_params(other.getNVector(), other.getFreeResParams()[0].numpy()),
+                          dtype=torch.float64, device="cuda")
+        with pytest.raises(RuntimeError, match="one model"):
+            b.nll_grad([anas[0], other], [params[0], po], "fp64")
+    finally:
+        b.close()
+
+
+@pytest.mark.gpu
+def test_batched_serving_same_results_and_shared_launches():
+    """Serving with the fits' evaluations gathered into shared launches: each
+    job's fitted parameters, NLL and Hessian equal those of the job run alone
+    without batching, and the batch served several requests per round."""
+    jobs = [serving.JobSpec(job_id=0, model="pipi_rho", n_data=8_000, n_phsp=80_000, seed=11, max_evals=25),
+            serving.JobSpec(job_id=1, model="pipi_rho", n_data=12_000, n_phsp=120_000, seed=14, max_evals=25),
+            serving.JobSpec(job_id=2, model="pipi_3rho", n_data=5_000, n_phsp=50_000, seed=12, max_evals=25),
+            serving.JobSpec(job_id=3, model="pipi_3rho", n_data=6_000, n_phsp=60_000, seed=15, max_evals=25,
+                            precision="fp64")]
+    alone = []
+    srv = serving.Server(slots=1)
+    try:
+        for j in jobs:
+            alone += srv.run([j], realtime=False)
+    finally:
+        srv.close()
+    srv = serving.Server(slots=4, batch=True)
+    try:
+        mixed = srv.run(jobs, realtime=False)
+        rounds, requests = srv.batch.stats()
+    finally:
+        srv.close()
+    for a, m in zip(alone, mixed):
+        assert a.error is None and m.error is None, (a.error, m.error)
+        assert a.n_evals == m.n_evals > 0
+        assert a.nll == m.nll, (a.job_id, a.nll, m.nll)
+        assert np.array_equal(a.params, m.params)
+        assert np.allclose(a.hessian, m.hessian, rtol=1e-10, atol=1e-10 * np.max(np.abs(a.hessian)))
+    assert requests == sum(m.n_evals for m in mixed)
+    assert rounds < requests
