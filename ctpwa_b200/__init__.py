@@ -439,25 +439,7 @@ class analysis:
         self._check()
         import numpy as np
 
-        n = self._np
-        x = np.ascontiguousarray(np.asarray(start, dtype=np.float64)).copy()
-        if x.size != n:
-            raise RuntimeError(f"params size mismatch: got {x.size}, expected {n}")
-        nV = self.getNVector()
-        if lower is None or upper is None:
-            res = self.getFreeResParams().numpy()
-            lo = np.concatenate([np.full(2 * nV, -np.inf), res[1]])
-            hi = np.concatenate([np.full(2 * nV, np.inf), res[2]])
-            lower = lo if lower is None else lower
-            upper = hi if upper is None else upper
-        lo = np.ascontiguousarray(lower, dtype=np.float64)
-        hi = np.ascontiguousarray(upper, dtype=np.float64)
-        if free is None:
-            free = np.ones(n, dtype=np.uint8)
-            free[0] = free[nV] = 0
-        fr = np.ascontiguousarray(free, dtype=np.uint8)
-        if lo.size != n or hi.size != n or fr.size != n:
-            raise RuntimeError("fit: lower, upper and free need n_params entries")
+        x, lo, hi, fr = self._fit_box(start, lower, upper, free)
         out = np.zeros(4)
         lat = np.zeros(max(1, int(max_evals)), dtype=np.float32)
         dp = ctypes.POINTER(ctypes.c_double)
@@ -478,6 +460,66 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         ne = int(out[1])
         return x, float(out[0]), ne, int(out[2]), int(out[3]), lat[:min(ne, lat.size)].astype(np.float64).tolist()
+
+    def _fit_box(self, start, lower, upper, free):
+        """Start (copied), bounds and free mask of a fit, with the reference's
+        defaults (example/fit.py:113-160): the first coupling fixed, the
+        couplings unbounded, the free resonance parameters within their
+        bounds."""
+        import numpy as np
+
+        n = self._np
+        x = np.ascontiguousarray(np.asarray(start, dtype=np.float64)).copy()
+        if x.size != n:
+            raise RuntimeError(f"params size mismatch: got {x.size}, expected {n}")
+        nV = self.getNVector()
+        if lower is None or upper is None:
+            res = self.getFreeResParams().numpy()
+            lo = np.concatenate([np.full(2 * nV, -np.inf), res[1]])
+            hi = np.concatenate([np.full(2 * nV, np.inf), res[2]])
+            lower = lo if lower is None else lower
+            upper = hi if upper is None else upper
+        lo = np.ascontiguousarray(lower, dtype=np.float64)
+        hi = np.ascontiguousarray(upper, dtype=np.float64)
+        if free is None:
+            free = np.ones(n, dtype=np.uint8)
+            free[0] = free[nV] = 0
+        fr = np.ascontiguousarray(free, dtype=np.uint8)
+        if lo.size != n or hi.size != n or fr.size != n:
+            raise RuntimeError("fit: lower, upper and free need n_params entries")
+        return x, lo, hi, fr
+
+    def fitNewton(self, start, lower=None, upper=None, free=None, max_iter=50, xtol=1e-4, gtol=1e-9, fnoise=None,
+                  precision=None, stream=None):
+        """Newton fit with the exact FP64 Hessian (``ctpwa_fit_newton``):
+        Levenberg-Marquardt steps over the same box and free parameters as
+        `fit`, converging to the stationary point of the start's basin (the
+        reference keeps a fit result only where its Hessian is positive
+        definite, example/fit.py:202-230). The NLL and gradient are taken in
+        `precision`; the Hessian is FP64 in both forms. Stops after a step of
+        at most `xtol` in units of 1/sqrt(H_ii) per parameter, or one whose
+        predicted decrease is below 1e-2 `fnoise`. `fnoise` is the NLL's
+        rounding level (default 1e-3 for the mixed form, 1e-6 for FP64):
+        steps predicted to gain less are accepted unless the NLL rises by more.
+        Returns (params, nll, evaluations, hessians, status); status 0:
+        projected gradient <= gtol, 1: step <= xtol, 2: max_iter Hessians
+        spent, 3: no acceptable step."""
+        self._check()
+        import numpy as np
+
+        x, lo, hi, fr = self._fit_box(start, lower, upper, free)
+        prec = self._precision if precision is None else self._parse_precision(precision)
+        if fnoise is None:
+            fnoise = 1e-3 if prec == 1 else 1e-6
+        out = np.zeros(4)
+        dp = ctypes.POINTER(ctypes.c_double)
+        sp = None if stream is None else ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
+        rc = self._lib.ctpwa_fit_newton(self._h, x.ctypes.data_as(dp), fr.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                        lo.ctypes.data_as(dp), hi.ctypes.data_as(dp), prec, int(max_iter), float(xtol),
+                                        float(gtol), float(fnoise), out.ctypes.data_as(dp), sp)
+        if rc != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return x, float(out[0]), int(out[1]), int(out[2]), int(out[3])
 
     def getShardSums(self, params: torch.Tensor, precision=None) -> torch.Tensor:
         """This shard's per-sample sums (float64 CUDA, to be summed over shards

@@ -91,14 +91,24 @@ SIGNATURES = {
     "ctpwa_fit": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.POINTER(ctypes.c_ubyte), _c_double_p,
                                  _c_double_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                  ctypes.c_double, _c_double_p, ctypes.POINTER(ctypes.c_float), ctypes.c_void_p]),
+    "ctpwa_fit_newton": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.POINTER(ctypes.c_ubyte), _c_double_p,
+                                        _c_double_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, _c_double_p, ctypes.c_void_p]),
     "ctpwa_minimize_box": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _c_double_p,
                                           ctypes.POINTER(ctypes.c_ubyte), _c_double_p, _c_double_p, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_double, ctypes.c_double, _c_double_p]),
+    "ctpwa_minimize_box_newton": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                 _c_double_p, ctypes.POINTER(ctypes.c_ubyte), _c_double_p, _c_double_p,
+                                                 ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                 _c_double_p]),
 }
 
 # host function for ctpwa_minimize_box: fn(x, &f, g, user) -> status
 FG_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                          ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+# host Hessian for ctpwa_minimize_box_newton: hfn(x, H, user) -> status
+HESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                           ctypes.c_void_p)
 
 _lib = None
 

@@ -23,6 +23,7 @@ struct ctpwa_handle {
     double* d_params = nullptr;  // host-entry staging
     double* d_out = nullptr;     // [1 + n_params]
     double* h_pin = nullptr;     // pinned [1 + 2 n_params]
+    double* d_hess = nullptr;    // [n_params^2], allocated by the first Newton fit
 };
 
 namespace {
@@ -129,6 +130,7 @@ void ctpwa_destroy(ctpwa_handle* h)
     if (!h) return;
     cudaFree(h->d_params);
     cudaFree(h->d_out);
+    cudaFree(h->d_hess);
     cudaFreeHost(h->h_pin);
     delete h;
 }
@@ -614,6 +616,57 @@ int ctpwa_fit(ctpwa_handle* h, double* params, const unsigned char* free_mask, c
     return CTPWA_OK;
 }
 
+int ctpwa_fit_newton(ctpwa_handle* h, double* params, const unsigned char* free_mask, const double* lo,
+                     const double* hi, int precision, int max_iter, double xtol, double gtol, double fnoise, double* out4,
+                     void* stream)
+{
+    if (!h || !params || !free_mask || !lo || !hi || !out4) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (max_iter < 1 || !(xtol >= 0.0) || !(gtol >= 0.0) || !(fnoise >= 0.0))
+        return setErr(h, CTPWA_ERR_ARG, "max_iter must be >= 1 and xtol, gtol, fnoise >= 0");
+    const int np = h->eng->nParams();
+    for (int i = 0; i < np; ++i)
+        if (!(lo[i] <= hi[i])) return setErr(h, CTPWA_ERR_ARG, "lower bound above upper bound");
+    cudaStream_t s = (cudaStream_t)stream;
+    try {
+        if (!h->d_hess && cudaMalloc(&h->d_hess, sizeof(double) * np * np) != cudaSuccess)
+            throw std::runtime_error("CUDA error: Hessian buffer allocation failed");
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    auto fg = [&](const double* x, double* f, double* g) -> int {
+        return ctpwa_nll_grad_host(h, x, f, g, precision, stream);
+    };
+    // the exact FP64 Hessian at x (both precisions: the mixed form keeps its
+    // Hessian in FP64)
+    auto hf = [&](const double* x, double* H) -> int {
+        try {
+            std::memcpy(h->h_pin, x, sizeof(double) * np);
+            if (cudaMemcpyAsync(h->d_params, h->h_pin, sizeof(double) * np, cudaMemcpyHostToDevice, s) != cudaSuccess)
+                throw std::runtime_error("CUDA error: host-to-device copy failed");
+            h->eng->hessianExact(h->d_params, h->d_hess, s);
+            if (cudaMemcpyAsync(H, h->d_hess, sizeof(double) * np * np, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
+        } catch (const std::exception& e) {
+            return setErr(h, CTPWA_ERR_CUDA, e.what());
+        }
+        return CTPWA_OK;
+    };
+    ctpwa::NewtonOptions opt;
+    opt.max_iter = max_iter;
+    opt.xtol = xtol;
+    opt.gtol = gtol;
+    opt.fnoise = fnoise;
+    ctpwa::BoxLbfgsResult r;
+    const int rc = ctpwa::boxNewton(fg, hf, np, params, free_mask, lo, hi, opt, &r);
+    if (rc != 0) return rc;
+    out4[0] = r.f;
+    out4[1] = r.evals;
+    out4[2] = r.iters;
+    out4[3] = r.status;
+    return CTPWA_OK;
+}
+
 int ctpwa_minimize_box(ctpwa_fg_fn fn, void* user, int n, double* x, const unsigned char* free_mask, const double* lo,
                        const double* hi, int max_evals, int history, double ftol, double gtol, double* out4)
 {
@@ -629,6 +682,33 @@ int ctpwa_minimize_box(ctpwa_fg_fn fn, void* user, int n, double* x, const unsig
     ctpwa::BoxLbfgsResult r;
     const int rc = ctpwa::boxLbfgs([&](const double* xx, double* f, double* g) { return fn(xx, f, g, user); }, n, x,
                                    free_mask, lo, hi, opt, &r);
+    if (rc != 0) return rc;
+    out4[0] = r.f;
+    out4[1] = r.evals;
+    out4[2] = r.iters;
+    out4[3] = r.status;
+    return CTPWA_OK;
+}
+
+int ctpwa_minimize_box_newton(ctpwa_fg_fn fn, ctpwa_hess_fn hfn, void* user, int n, double* x,
+                              const unsigned char* free_mask, const double* lo, const double* hi, int max_iter,
+                              double xtol, double gtol, double fnoise, double* out4)
+{
+    if (!fn || !hfn || !x || !free_mask || !lo || !hi || !out4 || n < 1)
+        return setErr(nullptr, CTPWA_ERR_ARG, "bad argument");
+    if (max_iter < 1 || !(xtol >= 0.0) || !(gtol >= 0.0) || !(fnoise >= 0.0))
+        return setErr(nullptr, CTPWA_ERR_ARG, "max_iter must be >= 1 and xtol, gtol, fnoise >= 0");
+    for (int i = 0; i < n; ++i)
+        if (!(lo[i] <= hi[i])) return setErr(nullptr, CTPWA_ERR_ARG, "lower bound above upper bound");
+    ctpwa::NewtonOptions opt;
+    opt.max_iter = max_iter;
+    opt.xtol = xtol;
+    opt.gtol = gtol;
+    opt.fnoise = fnoise;
+    ctpwa::BoxLbfgsResult r;
+    const int rc = ctpwa::boxNewton([&](const double* xx, double* f, double* g) { return fn(xx, f, g, user); },
+                                    [&](const double* xx, double* H) { return hfn(xx, H, user); }, n, x, free_mask, lo,
+                                    hi, opt, &r);
     if (rc != 0) return rc;
     out4[0] = r.f;
     out4[1] = r.evals;

@@ -557,9 +557,10 @@ std::string Gen::emit()
     // m0^2 - m^2 and the like happens in full precision; transcendental
     // functions are FP64 too (their FP32 versions are not correctly rounded,
     // and a bias would not average out over a sample); everything else is
-    // FP32 with correctly rounded reciprocals and square roots. Frontier
-    // values are stored in the precision they are computed in (kinematic
-    // values and table lookups as FP64).
+    // FP32 with correctly rounded reciprocals and square roots. This applies
+    // to the per-call code: event-only nodes are evaluated once per event in
+    // FP64, and the mixed form stores each frontier value either as FP64
+    // (the ones marked here, and kinematic values) or rounded once to FP32.
     std::vector<char> cap(N.size(), 0), dbl(N.size(), 0);
     {
         for (size_t x = 0; x < N.size(); ++x) {
@@ -817,6 +818,29 @@ std::string Gen::emit()
                 if (k >= 0) st.push_back(k);
         }
     }
+    // FP32 value nodes kept as an unevaluated sum hi + lo (names e<x>_h,
+    // e<x>_l; e<x> is their rounded sum for the other consumers). A sum of a
+    // per-event value and a parameter-only constant, or its shifted form, is
+    // formed by an exact two-sum: its rounding would otherwise be the same
+    // for every event of a binade (below the event value's ulp the bits are
+    // the constant's), and so would be that of adding the constant's lo
+    // part, which moves every event's value by the same fraction of an ulp:
+    // a bias of ~1e-9 of the sample mean that the data weight sum multiplies.
+    // The products and sums that consume such a value take its lo part in,
+    // where the other factor's bits make the rounding independent per event.
+    std::vector<char> hasLo(N.size(), 0);
+    auto twoSum = [](size_t x, const std::string& a, const std::string& b, const std::string& c) {
+        const std::string X = "e" + std::to_string(x), H = X + "_h", L = X + "_l", BB = X + "_b";
+        return "  const float " + H + " = " + a + " + " + b + ";\n  const float " + BB + " = " + H + " - " + a +
+               ";\n  const float " + L + " = ((" + a + " - (" + H + " - " + BB + ")) + (" + b + " - " + BB + "))" +
+               (c.empty() ? std::string() : " + " + c) + ";\n  const float " + X + " = " + H + " + " + L + ";\n";
+    };
+    auto neg = [](const std::string& v) { return v.empty() ? v : "-(" + v + ")"; };
+    auto addLo = [](const std::string& a, const std::string& b) {
+        if (a.empty()) return b;
+        if (b.empty()) return a;
+        return "(" + a + " + " + b + ")";
+    };
     // definition of event node x
     auto nodeLine = [&](size_t x, bool f32, const RefFn& ref) -> std::string {
         const auto& nd = N[x];
@@ -829,6 +853,12 @@ std::string Gen::emit()
                               Dh = "Cfh[" + ks + "]", Dl = "Cfl[" + ks + "]";
             // the parameter-only part D = T -+ R enters as hi + lo (a single
             // FP32 rounding of it would shift every event alike)
+            if (valueNode[x]) {
+                hasLo[x] = 1;
+                if (nd.op == dag::Add) return twoSum(x, Dh, Xs, Dl);  // (T + R) + X'
+                if (xa) return twoSum(x, Xs, neg(Dh), neg(Dl));         // X - T = X' - D
+                return twoSum(x, Dh, neg(Xs), Dl);                     // T - X = D - X'
+            }
             std::string rhs;
             if (nd.op == dag::Add) rhs = "(" + Dh + " + " + Xs + ") + " + Dl;     // (T + R) + X'
             else if (xa) rhs = "-((" + Dh + " - " + Xs + ") + " + Dl + ")";      // X - T
@@ -853,50 +883,67 @@ std::string Gen::emit()
             }
         }
         std::string rhs = opExpr(nd, A, B, Cc, isF);
-        if (isF && valueNode[x] && (nd.op == dag::Add || nd.op == dag::Sub || nd.op == dag::Mul)) {
-            // An event-independent operand of a value node enters as hi + lo
-            // and the product is rounded once (fmaf): rounding it to FP32
-            // first would bias every event alike, and so would rounding the
-            // product of two FP32-grid factors (structured low bits).
-            std::string hi, lo;
-            auto split = [&](int y) -> bool {
+        if (isF && valueNode[x] && (nd.op == dag::Add || nd.op == dag::Sub || nd.op == dag::Mul || nd.op == dag::Neg)) {
+            // An event-independent operand of a value node enters as hi + lo,
+            // and so does an operand kept as hi + lo; a product is rounded
+            // once (fmaf): rounding it to FP32 first would bias every event
+            // alike, and so would rounding the product of two FP32-grid
+            // factors (structured low bits).
+            struct Part {
+                std::string hi, lo;
+                bool cst = false;
+            };
+            auto part = [&](int y, const std::string& plain) -> Part {
                 const auto& yn = N[y];
                 if (yn.op == dag::Const) {
                     float h = (float)yn.v;
                     double l = yn.v - (double)h;
-                    if (l == 0.0 || !std::isfinite(yn.v)) return false;
-                    hi = numf((double)h);
-                    lo = numf(l);
-                    return true;
+                    if (l == 0.0 || !std::isfinite(yn.v)) return {plain, "", true};
+                    return {numf((double)h), numf(l), true};
                 }
-                if (yn.dep == dag::DEP_THETA) {
-                    hi = "Cfh[" + std::to_string(cslot[y]) + "]";
-                    lo = "Cfl[" + std::to_string(cslot[y]) + "]";
-                    return true;
-                }
-                return false;
+                if (yn.dep == dag::DEP_THETA)
+                    return {"Cfh[" + std::to_string(cslot[y]) + "]", "Cfl[" + std::to_string(cslot[y]) + "]", true};
+                if (hasLo[y]) return {"e" + std::to_string(y) + "_h", "e" + std::to_string(y) + "_l", false};
+                return {plain, "", false};
             };
-            const bool ca = split(nd.a);
-            const std::string ha = hi, la = lo;
-            const bool cb = split(nd.b);
-            const std::string hb = hi, lb = lo;
-            if (ca != cb) {
-                const std::string ev = ca ? B : A, h = ca ? ha : hb, l = ca ? la : lb;
-                if (nd.op == dag::Mul) rhs = "fmaf(" + ev + ", " + h + ", " + ev + " * " + l + ")";
-                else if (nd.op == dag::Add) rhs = "(" + ev + " + " + h + ") + " + l;
-                else if (ca) rhs = "(" + h + " - " + ev + ") + " + l;  // const - event
-                else rhs = "(" + ev + " - " + h + ") - " + l;          // event - const
+            const std::string X = "e" + std::to_string(x);
+            if (nd.op == dag::Neg) {
+                if (hasLo[nd.a]) {
+                    hasLo[x] = 1;
+                    return "  const float " + X + "_h = -e" + std::to_string(nd.a) + "_h;\n  const float " + X +
+                           "_l = -e" + std::to_string(nd.a) + "_l;\n  const float " + X + " = -e" + std::to_string(nd.a) +
+                           ";\n";
+                }
+            } else {
+                const Part pa = part(nd.a, A), pb = part(nd.b, B);
+                const bool event_a = (N[nd.a].dep & dag::DEP_EVENT) != 0, event_b = (N[nd.b].dep & dag::DEP_EVENT) != 0;
+                if (nd.op == dag::Mul) {
+                    if (nd.a == nd.b && !pa.lo.empty()) {
+                        rhs = "fmaf(" + pa.hi + ", " + pa.hi + ", (" + pa.hi + " + " + pa.hi + ") * " + pa.lo + ")";
+                    } else if (!pa.lo.empty() || !pb.lo.empty()) {
+                        std::string corr;
+                        if (!pa.lo.empty() && !pb.lo.empty())
+                            corr = "fmaf(" + pa.hi + ", " + pb.lo + ", " + pa.lo + " * " + pb.hi + ")";
+                        else if (!pb.lo.empty()) corr = pa.hi + " * " + pb.lo;
+                        else corr = pa.lo + " * " + pb.hi;
+                        rhs = "fmaf(" + pa.hi + ", " + pb.hi + ", " + corr + ")";
+                    }
+                } else if ((event_a && event_b && (!pa.lo.empty() || !pb.lo.empty())) ||
+                           (event_a != event_b && (!pa.lo.empty() || !pb.lo.empty()))) {
+                    // a sum with a constant or with a hi + lo operand: two-sum of the
+                    // hi parts, the lo parts added to its error
+                    const bool sub = nd.op == dag::Sub;
+                    hasLo[x] = 1;
+                    return twoSum(x, pa.hi, sub ? neg(pb.hi) : pb.hi, addLo(pa.lo, sub ? neg(pb.lo) : pb.lo));
+                }
             }
         }
         return std::string("  const ") + (isF ? "float" : "double") + " e" + std::to_string(x) + " = " + rhs + ";\n";
     };
-    // once per event: event-only nodes, then the frontier values
-    auto eventPart = [&](bool f32) -> std::string {
+    // once per event (FP64): event-only nodes, then the frontier values
+    auto eventPart = [&]() -> std::string {
         std::ostringstream evs;
-        const RefFn ref = preRef(f32);
-        if (f32)
-            for (size_t k = 0; k < out.slots.size(); ++k)
-                evs << "  const float kf" << k << " = (float)kv[" << k << "]; (void)kf" << k << ";\n";
+        const RefFn ref = preRef(false);
         for (size_t u = 0; u < tab_uses.size(); ++u) {
             const auto& t = tab_uses[u];
             if (t.interp)
@@ -907,15 +954,9 @@ std::string Gen::emit()
                     << "), tim" << u << " = 0.0;\n";
         }
         for (size_t x = 0; x < N.size(); ++x)
-            if (live[x] && evOnly((int)x) && N[x].op != dag::Kin) evs << nodeLine(x, f32, ref);
-        for (size_t x = 0; x < N.size(); ++x) {
-            if (fs64[x] < 0) continue;
-            if (!f32) evs << "  o[" << fs64[x] << "] = " << ref((int)x, false) << ";\n";
-            else if (shifted[x]) evs << "  of[" << fsF[x] << "] = (float)(" << ref((int)x, false) << " - " << num(shiftR[x])
-                                     << ");\n";
-            else if (fsF[x] >= 0) evs << "  of[" << fsF[x] << "] = " << ref((int)x, true) << ";\n";
-            else evs << "  od[" << fsD[x] << "] = " << ref((int)x, false) << ";\n";
-        }
+            if (live[x] && evOnly((int)x) && N[x].op != dag::Kin) evs << nodeLine(x, false, ref);
+        for (size_t x = 0; x < N.size(); ++x)
+            if (fs64[x] >= 0) evs << "  o[" << fs64[x] << "] = " << ref((int)x, false) << ";\n";
         return evs.str();
     };
     // per call: parameter-dependent event nodes and the outputs
@@ -1046,11 +1087,25 @@ std::string Gen::emit()
          "// per-call code reads (frontier), FP64\n";
     h << "__device__ __forceinline__ void model_event(const double* __restrict__ kv, double* __restrict__ o)\n{\n"
          "  (void)kv; (void)o;\n"
-      << eventPart(false) << "}\n";
-    h << "// the same for the mixed form: FP32 values (of) and FP64 values (od)\n";
-    h << "__device__ __forceinline__ void model_event_mx(const double* __restrict__ kv, float* __restrict__ of,\n"
-         "    double* __restrict__ od)\n{\n  (void)kv; (void)of; (void)od;\n"
-      << eventPart(true) << "}\n";
+      << eventPart() << "}\n";
+    // The mixed form's frontier is the FP64 frontier rounded once per value
+    // (shifted values X - R formed in FP64 first): the once-per-event work
+    // costs nothing per call, so its FP64 result is kept rather than an FP32
+    // evaluation whose error of a few ulps would add to every event's
+    // intensity.
+    std::ostringstream mx;
+    for (size_t x = 0; x < N.size(); ++x) {
+        if (fs64[x] < 0) continue;
+        const std::string o = "o[" + std::to_string(fs64[x]) + "]";
+        if (shifted[x]) mx << "  of[" << fsF[x] << "] = (float)(" << o << " - " << num(shiftR[x]) << ");\n";
+        else if (fsF[x] >= 0) mx << "  of[" << fsF[x] << "] = (float)" << o << ";\n";
+        else mx << "  od[" << fsD[x] << "] = " << o << ";\n";
+    }
+    h << "// the same for the mixed form from the FP64 frontier o: FP32 values (of)\n"
+         "// and FP64 values (od)\n";
+    h << "__device__ __forceinline__ void model_event_mx(const double* __restrict__ o, float* __restrict__ of,\n"
+         "    double* __restrict__ od)\n{\n  (void)o; (void)of; (void)od;\n"
+      << mx.str() << "}\n";
     h << "// per-event lineshape products and their parameter derivatives (FP64) from the\n"
          "// event's frontier values\n";
     h << "__device__ __forceinline__ void model_columns(const double* __restrict__ ev, const double* __restrict__ C,\n"

@@ -2523,12 +2523,19 @@ void Engine::compileGram()
     cudaKernel_t kg, kf;
     CT_CUDA(cudaLibraryGetKernel(&kg, lib, "ct_gram"));
     CT_CUDA(cudaLibraryGetKernel(&kf, lib, "ct_gram_finalize"));
-    gram_dsmem_ = 4 * (rows <= 64 ? 64 : 128) * 128 * 2;
+    // operand tile(s) of 128 rows x 256 events (BF16; one when the hi and lo
+    // rows fit together) and the FP64 sums [128][2 nA] (kernels/gram.cuh)
+    const int r8 = (rows + 7) / 8 * 8;
+    gram_dsmem_ = (2 * r8 <= 128 ? 1 : 2) * 128 * 256 * 2 + 128 * 2 * model_.nAmp() * 8;
     CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributeMaxDynamicSharedMemorySize, gram_dsmem_));
     int sms = 148;
     CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
-    const int occ = std::max(1, std::min(2, residentCtas((void*)kg, 128, gram_dsmem_)));
-    const long long ntiles = (samples_[0].n + 127) / 128;
+    // tensor-memory columns per CTA (CT_GRAM_TMEM_COLS): NACC accumulators of N columns
+    const int nn = 2 * r8 <= 128 ? 2 * r8 : (rows + 15) / 16 * 16;
+    int tcols = 32;
+    while (tcols < (nn <= 64 ? 4 : 2) * nn) tcols *= 2;
+    const int occ = std::max(1, std::min({4, 512 / tcols, residentCtas((void*)kg, 256, gram_dsmem_)}));
+    const long long ntiles = (samples_[0].n + 255) / 256;
     gram_grid_ = (int)std::max(1LL, std::min<long long>(ntiles, (long long)sms * occ));
     alloc(d_gpart_, sizeof(double) * (size_t)gram_grid_ * rows * 2 * model_.nAmp());
     k_gram_ = (void*)kg;
@@ -2565,7 +2572,7 @@ void Engine::gram(const double* d_params, double* d_out, cudaStream_t stream)
     g.partials = d_gpart_;
     g.err = d_err_;
     void* gargs[] = {&g};
-    CT_CUDA(cudaLaunchKernel(k_gram_, dim3(gram_grid_), dim3(128), gargs, (size_t)gram_dsmem_, stream));
+    CT_CUDA(cudaLaunchKernel(k_gram_, dim3(gram_grid_), dim3(256), gargs, (size_t)gram_dsmem_, stream));
     int nb = gram_grid_;
     double inv_w = 1.0 / (d.wsum > 0 ? d.wsum : 1.0);
     void* fargs[] = {&d_gpart_, &nb, &inv_w, &d_out};

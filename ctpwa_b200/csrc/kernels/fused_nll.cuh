@@ -10,9 +10,10 @@
 //       (one term, or one per permutation of identical particles)
 //   der_term(k), der_th(k)   term / theta index of derivative entry k
 //   model_prologue(theta, C)   parameter-only subexpressions, once per call
-//   model_event(kin, o), model_event_mx(kin, of, od)   the parameter-independent
+//   model_event(kin, o), model_event_mx(o, of, od)   the parameter-independent
 //       per-event values the per-call code reads (frontier), evaluated once
-//       per event by ct_event_cache when a sample is loaded
+//       per event by ct_event_cache when a sample is loaded (FP64; the mixed
+//       form's FP32 / FP64 rows are those values rounded once)
 //   model_columns(ev, C, Fr, Fi, dFr, dFi)   lineshape products F_a and their
 //       theta derivatives for one event from its frontier values
 //       (straight-line generated code, FP64)
@@ -287,7 +288,7 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_event_cache(const doub
         if (evf) {
             float of[CT_NEVF_ALLOC];
             double od[CT_NEVD_ALLOC];
-            model_event_mx(kv, of, od);
+            model_event_mx(o, of, od);
 #pragma unroll
             for (int k = 0; k < M_NEVF; ++k) evf[(long long)k * ld + e] = of[k];
 #pragma unroll

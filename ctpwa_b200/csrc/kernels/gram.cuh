@@ -8,46 +8,54 @@
 // The amplitudes are formed on the fly from the angular tables and the
 // mixed-form (FP32) lineshapes and never written to HBM.
 //
-// Formulation. One CTA of 128 threads takes tiles of 128 events; thread t
-// forms event t's real amplitude row vector X (NROW = npol x 2nA values:
-// Re A and Im A of every column for every polarisation, scaled by sqrt(w))
-// and writes it as column t of the operand tile Xt [rows][128 events] in
-// shared memory. One MMA chain then accumulates D = Xt Xt^T
-// ((npol 2nA)^2, of which the npol diagonal blocks are the Gram of each
-// polarisation) in tensor memory: kind::f16 with BF16 operands and FP32
-// accumulation, M = 64 (or 128) rows, N = NROW rounded up to 8, K = 16
-// events per instruction. Each FP32 value x is split as x = hi + lo (two
-// BF16 numbers, hi = rn(x), lo = rn(x - hi)) and the four products
-// lo.lo + lo.hi + hi.lo + hi.hi are accumulated, which leaves a residual of
-// ~2^-18 |x| per value. Tiles alternate between two FP32 accumulators in
-// tensor memory; while one tile's MMAs run, the previous tile's accumulator
-// is read out (tcgen05.ld) into per-thread FP64 sums, so FP32 accumulation
-// spans one tile (32 MMAs) only. Per-CTA FP64 partials are reduced in a fixed
-// order by ct_gram_finalize.
+// Formulation. A CTA of 256 threads takes tiles of 256 events; thread t
+// forms event t's real amplitude vector X (ROWS = npol x 2nA values: Re A
+// and Im A of every column for every polarisation, scaled by sqrt(w)) and
+// writes it as column t of the operand tile Xt [rows][256 events] in shared
+// memory. Each FP32 value x is split into two BF16 numbers, hi = rn(x) and
+// lo = rn(x - hi) (residual ~2^-18 |x|). With R8 = ROWS rounded up to 8 and
+// 2 R8 <= 128, the hi values fill rows [0, R8) and the lo values rows
+// [R8, 2 R8) of one tile, and one MMA chain (kind::f16, BF16 operands, FP32
+// accumulator in tensor memory, M = 128, N = 2 R8, K = 16 events per
+// instruction) gives all four products hi.hi, hi.lo, lo.hi and lo.lo at
+// once; larger models keep hi and lo in two tiles and issue the four
+// products as four MMAs (N = ROWS rounded up to 16). The tile's K-steps go to
+// NACC accumulators in turn (64 or 128 events each); after every tile they
+// are read (tcgen05.ld) and added in FP64 in shared memory, so FP32
+// accumulation spans 64 or 128 events only. The npol diagonal blocks of the
+// (npol 2nA)^2 product are the Gram of each polarisation; per-CTA FP64
+// partials are reduced in a fixed order by ct_gram_finalize.
 //
-// Shared-memory operand layout: K-major, no swizzle ("interleaved" core
-// matrices of 8 rows x 16 bytes): element (row m, event k) at
-//   (m / 8) * SBO + (k / 8) * 128 + (m % 8) * 16 + (k % 8) * 2,  SBO = 2048,
-// so the two core matrices of one K = 16 step are LBO = 128 bytes apart.
-// Tensor-memory layout of D (cta_group::1): M = 128, row m in lane m; M = 64,
-// row m in lane (m % 16) + 32 (m / 16); column n in column n.
+// Shared-memory operand layout: MN-major (the matrix rows contiguous), no
+// swizzle: element (row m, event k) at
+//   (k / 8) * 128 + (m / 8) * SBO + (k % 8) * 16 + (m % 8) * 2,  SBO = 4096,
+// so a thread writes the 8 rows of a core matrix as one 16-byte store and a
+// warp's stores are contiguous; the two 8-event groups of one K = 16 step
+// are LBO = 128 bytes apart. Tensor-memory layout of D (cta_group::1,
+// M = 128): row m in lane m, column n in column n. Several CTAs per SM
+// overlap one CTA's MMA chain and read-out with the others' event work.
 #pragma once
 
 #include "fused_nll.cuh"
 
-#define CT_GRAM_THREADS 128
-#define CT_GRAM_TILE 128  // events per tile (one per thread)
+#define CT_GRAM_THREADS 256
+#define CT_GRAM_TILE 256  // events per tile (one per thread)
 #define CT_GRAM_ROWS (M_NPOL * 2 * M_NA)
 static_assert(CT_GRAM_ROWS <= 128, "the tensor-core Gram supports npol * 2 * nA <= 128");
-#define CT_GRAM_M (CT_GRAM_ROWS <= 64 ? 64 : 128)
-#define CT_GRAM_N ((CT_GRAM_ROWS + 7) / 8 * 8)
-// two accumulators (tiles alternate), each CT_GRAM_ACC_COLS columns
-#define CT_GRAM_ACC_COLS ((CT_GRAM_N + 15) / 16 * 16)
-#define CT_GRAM_TMEM_COLS (2 * CT_GRAM_ACC_COLS <= 32 ? 32 : 2 * CT_GRAM_ACC_COLS <= 64 ? 64 : 2 * CT_GRAM_ACC_COLS <= 128 ? 128 : 256)
-#define CT_GRAM_SBO 2048
-#define CT_GRAM_PART (CT_GRAM_M * CT_GRAM_TILE * 2)  // bytes of one BF16 operand tile
-// dynamic shared memory: [2 buffers][hi, lo] operand tiles
-#define CT_GRAM_SMEM (4 * CT_GRAM_PART)
+#define CT_GRAM_R8 ((CT_GRAM_ROWS + 7) / 8 * 8)
+#define CT_GRAM_STACK (2 * CT_GRAM_R8 <= 128)                 // hi and lo rows in one tile
+// MMA N (a multiple of 16 for M = 128)
+#define CT_GRAM_N (CT_GRAM_STACK ? 2 * CT_GRAM_R8 : (CT_GRAM_ROWS + 15) / 16 * 16)
+// accumulators per tile, each over 256 / NACC events (the tensor core's FP32
+// accumulation rounds toward zero: its bias grows with the accumulation length)
+#define CT_GRAM_NACC (CT_GRAM_N <= 64 ? 4 : 2)
+#define CT_GRAM_TMEM_COLS \
+    (CT_GRAM_NACC * CT_GRAM_N <= 32 ? 32 : CT_GRAM_NACC * CT_GRAM_N <= 64 ? 64 : CT_GRAM_NACC * CT_GRAM_N <= 128 ? 128 : 256)
+#define CT_GRAM_SBO 4096
+#define CT_GRAM_PART (128 * CT_GRAM_TILE * 2)  // bytes of one BF16 operand tile (128 rows)
+#define CT_GRAM_NPART (CT_GRAM_STACK ? 1 : 2)
+// dynamic shared memory: operand tile(s), then the FP64 sums [128][2 nA]
+#define CT_GRAM_SMEM (CT_GRAM_NPART * CT_GRAM_PART + 128 * 2 * M_NA * 8)
 #ifndef CT_GRAM_PAIRED
 #define CT_GRAM_PAIRED 0
 #endif
@@ -72,18 +80,19 @@ __device__ __forceinline__ unsigned short ct_bf16_rn(float x)
 }
 __device__ __forceinline__ float ct_bf16_to_f32(unsigned short h) { return __uint_as_float((unsigned)h << 16); }
 
-// shared-memory matrix descriptor (tcgen05): start, leading (K) and stride
-// (M/N) byte offsets, descriptor version 1, no swizzle
+// shared-memory matrix descriptor (tcgen05): start, leading-dimension and
+// stride-dimension byte offsets, descriptor version 1, no swizzle
 __device__ __forceinline__ unsigned long long ct_umma_desc(unsigned saddr, unsigned lbo, unsigned sbo)
 {
     return (unsigned long long)((saddr >> 4) & 0x3FFFu) | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
            ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N, M
-__device__ __forceinline__ unsigned ct_umma_idesc_bf16(int M, int N)
+// instruction descriptor: FP32 accumulator, BF16 A and B, both MN-major, N, M
+__device__ __forceinline__ unsigned ct_umma_idesc_bf16_mn(int M, int N)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(M >> 4) << 24);
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((unsigned)(N >> 3) << 17) |
+           ((unsigned)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void ct_tc_mma(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned idesc,
@@ -120,21 +129,20 @@ __device__ __forceinline__ void ct_tmem_ld16(unsigned taddr, float* v)
 
 extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS) ct_gram(CtGramArgs G)
 {
-    constexpr int NROW = CT_GRAM_ROWS, MM = CT_GRAM_M, NN = CT_GRAM_N, NA2 = 2 * M_NA;
+    constexpr int NROW = CT_GRAM_ROWS, R8 = CT_GRAM_R8, NN = CT_GRAM_N, NA2 = 2 * M_NA;
+    constexpr bool STACK = CT_GRAM_STACK;
     constexpr int NPS = CT_GRAM_PAIRED ? CT_NPOL_STORED : M_NPOL;
     extern __shared__ __align__(1024) unsigned char gsm[];
-    __shared__ __align__(8) unsigned long long bar[2];
+    double* sacc = (double*)(gsm + CT_GRAM_NPART * CT_GRAM_PART);  // [128][NA2]
+    __shared__ __align__(8) unsigned long long bar;
     __shared__ unsigned tmem_slot;
-    __shared__ int abort_flag;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5;
 
-    // zero both operand buffers once: rows >= NROW stay zero
+    // zero the operand tile(s) (unused rows stay zero) and the FP64 sums
     for (int i = tid; i < CT_GRAM_SMEM / 16; i += CT_GRAM_THREADS) reinterpret_cast<uint4*>(gsm)[i] = make_uint4(0, 0, 0, 0);
     if (tid == 0) {
-        ct_mbar_init(&bar[0], 1);
-        ct_mbar_init(&bar[1], 1);
+        ct_mbar_init(&bar, 1);
         ct_fence_mbar_init();
-        abort_flag = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(ct_smem_addr(&tmem_slot)),
@@ -148,50 +156,23 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS) ct_gram(CtGramArgs
     ct_tc_fence_after();
     const unsigned tmem = tmem_slot;
 
-    // this thread's D row in tensor memory (one row per lane; M = 64 uses
-    // the first 16 lanes of each warp's quarter)
-    const int my_row = MM == 128 ? tid : (lane < 16 ? 16 * warp + lane : NROW);
-    const int my_blk = my_row < NROW ? my_row / NA2 : 0;
-    double acc[NA2];
-#pragma unroll
-    for (int j = 0; j < NA2; ++j) acc[j] = 0.0;
-
-    // rows of this warp's tensor-memory lanes -> FP64 sums of this thread's
-    // row (columns of its polarisation block)
-    auto gram_readout = [&](unsigned tacc) {
-        if (MM == 128 || warp * 16 < NROW) {
-#pragma unroll
-            for (int c0 = 0; c0 < NN; c0 += 16) {
-                float v[16];
-                ct_tmem_ld16(tacc + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int col = c0 + j - my_blk * NA2;
-                    if (my_row < NROW && col >= 0 && col < NA2) acc[col] += (double)v[j];
-                }
-            }
-        }
-    };
     const long long ntiles = (G.n + CT_GRAM_TILE - 1) / CT_GRAM_TILE;
-    const unsigned idesc = ct_umma_idesc_bf16(MM, NN);
+    const unsigned idesc = ct_umma_idesc_bf16_mn(128, NN);
     const unsigned sbase = ct_smem_addr(gsm);
-    unsigned uses[2] = {0u, 0u};  // commits issued per buffer
-    int it = 0;
+    // this thread's column (event slot) in the operand tile
+    const unsigned kofs = (unsigned)(tid >> 3) * 128u + (unsigned)(tid & 7) * 16u;
+    // read-out: warps 0-3 read tensor-memory lanes 0-127 (one D row each)
+    const int my_row = tid;                       // D row of warps 0-3
+    const int my_r = STACK && my_row >= R8 ? my_row - R8 : my_row;  // operand row (hi or lo)
+    const int my_blk = my_r < NROW ? my_r / NA2 : 0;
     bool timed_out = false;
+    unsigned it = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int b = it & 1;
-        // the buffer's previous MMAs (two tiles ago) must be done before it is rewritten
-        if (uses[b] > 0) {
-            if (!ct_mbar_wait(&bar[b], (uses[b] - 1) & 1u, CT_WAIT_LIMIT)) timed_out = true;
-            if (__syncthreads_or(timed_out)) break;
-        }
-        // ---- this thread's event -> operand column tid of buffer b ----
+        // ---- this thread's event -> operand column tid ----
         const long long e = tile * CT_GRAM_TILE + tid;
-        float xr[M_NPOL][M_NA], xi[M_NPOL][M_NA];
+        float x[M_NPOL * NA2];
 #pragma unroll
-        for (int p = 0; p < M_NPOL; ++p)
-#pragma unroll
-            for (int a = 0; a < M_NA; ++a) xr[p][a] = xi[p][a] = 0.0f;
+        for (int i = 0; i < M_NPOL * NA2; ++i) x[i] = 0.0f;
         if (e < G.n) {
             CtEvent<float> ev;
             ev.load(G.evf + e, G.evd + e, G.ld);
@@ -204,81 +185,105 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS) ct_gram(CtGramArgs
                 const float fr = Fr[t] * sw, fi = Fi[t] * sw;
 #pragma unroll
                 for (int p = 0; p < NPS; ++p) {
-                    const float2 x = G.slamp[(long long)(term_plane(t) * NPS + p) * G.ld + e];
-                    xr[p][a] += fr * x.x - fi * x.y;
-                    xi[p][a] += fr * x.y + fi * x.x;
+                    const float2 sl = G.slamp[(long long)(term_plane(t) * NPS + p) * G.ld + e];
+                    x[p * NA2 + a] += fr * sl.x - fi * sl.y;
+                    x[p * NA2 + M_NA + a] += fr * sl.y + fi * sl.x;
                     const int q = M_NPOL - 1 - p;
                     if (CT_GRAM_PAIRED && q != p) {  // SL_q = conj(SL_p)
-                        xr[q][a] += fr * x.x + fi * x.y;
-                        xi[q][a] += fi * x.x - fr * x.y;
+                        x[q * NA2 + a] += fr * sl.x + fi * sl.y;
+                        x[q * NA2 + M_NA + a] += fi * sl.x - fr * sl.y;
                     }
                 }
             }
         }
-        unsigned char* hi = gsm + (size_t)b * 2 * CT_GRAM_PART;
-        unsigned char* lo = hi + CT_GRAM_PART;
-        const unsigned kofs = (unsigned)(tid >> 3) * 128u + (unsigned)(tid & 7) * 2u;
+        // hi and lo BF16 values, 8 rows (one core matrix) per 16-byte store
 #pragma unroll
-        for (int p = 0; p < M_NPOL; ++p)
+        for (int g = 0; g < R8 / 8; ++g) {
+            unsigned hw[4], lw[4];
 #pragma unroll
-            for (int c = 0; c < NA2; ++c) {
-                const int m = p * NA2 + c;
-                const float x = c < M_NA ? xr[p][c] : xi[p][c - M_NA];
-                const unsigned short h = ct_bf16_rn(x);
-                const unsigned short l = ct_bf16_rn(x - ct_bf16_to_f32(h));
-                const unsigned off = (unsigned)(m >> 3) * CT_GRAM_SBO + (unsigned)(m & 7) * 16u + kofs;
-                *reinterpret_cast<unsigned short*>(hi + off) = h;
-                *reinterpret_cast<unsigned short*>(lo + off) = l;
+            for (int q = 0; q < 4; ++q) {
+                unsigned short h2[2], l2[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int r = 8 * g + 2 * q + u;
+                    const float v = r < NROW ? x[r] : 0.0f;
+                    h2[u] = ct_bf16_rn(v);
+                    l2[u] = ct_bf16_rn(v - ct_bf16_to_f32(h2[u]));
+                }
+                hw[q] = (unsigned)h2[0] | ((unsigned)h2[1] << 16);
+                lw[q] = (unsigned)l2[0] | ((unsigned)l2[1] << 16);
             }
+            const unsigned hoff = (unsigned)g * CT_GRAM_SBO + kofs;
+            const unsigned loff = STACK ? (unsigned)(g + R8 / 8) * CT_GRAM_SBO + kofs : CT_GRAM_PART + hoff;
+            *reinterpret_cast<uint4*>(gsm + hoff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4*>(gsm + loff) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        }
         ct_fence_async_smem();
         ct_tc_fence_before();
         __syncthreads();
-        // ---- one thread issues the tile's MMA chain into accumulator b ----
-        // (smallest products first: FP32 accumulation rounds relative to the
-        // running sum, so the large hi.hi terms come last)
+        // ---- one thread issues the tile's MMA chain: K-steps [h SPA, (h+1) SPA)
+        // into accumulator h (tensor-memory columns [h NN, (h+1) NN)) ----
         if (tid == 0) {
             ct_tc_fence_after();
-            const unsigned base = sbase + (unsigned)b * 2u * CT_GRAM_PART;
-            const unsigned dacc = tmem + (unsigned)(b * CT_GRAM_ACC_COLS);
-#pragma unroll
-            for (int pass = 0; pass < 4; ++pass) {
-                const unsigned pa = (pass < 2 ? 1u : 0u) * CT_GRAM_PART, pb = (pass == 0 || pass == 2 ? 1u : 0u) * CT_GRAM_PART;
+            constexpr int SPA = CT_GRAM_TILE / 16 / CT_GRAM_NACC;
 #pragma unroll 1
-                for (int s = 0; s < CT_GRAM_TILE / 16; ++s) {
-                    const unsigned long long da = ct_umma_desc(base + pa + 256u * s, 128u, CT_GRAM_SBO);
-                    const unsigned long long db = ct_umma_desc(base + pb + 256u * s, 128u, CT_GRAM_SBO);
-                    ct_tc_mma(dacc, da, db, idesc, (s == 0 && pass == 0) ? 0u : 1u);
+            for (int s = 0; s < CT_GRAM_TILE / 16; ++s) {
+                const unsigned dt = tmem + (unsigned)((s / SPA) * NN);
+                const bool first = s % SPA == 0;
+                if constexpr (STACK) {
+                    const unsigned long long d = ct_umma_desc(sbase + 256u * s, 128u, CT_GRAM_SBO);
+                    ct_tc_mma(dt, d, d, idesc, first ? 0u : 1u);
+                } else {
+#pragma unroll
+                    for (int pass = 0; pass < 4; ++pass) {
+                        const unsigned pa = (pass < 2 ? 1u : 0u) * CT_GRAM_PART;
+                        const unsigned pb = (pass == 0 || pass == 2 ? 1u : 0u) * CT_GRAM_PART;
+                        ct_tc_mma(dt, ct_umma_desc(sbase + pa + 256u * s, 128u, CT_GRAM_SBO),
+                                  ct_umma_desc(sbase + pb + 256u * s, 128u, CT_GRAM_SBO), idesc,
+                                  (first && pass == 0) ? 0u : 1u);
+                    }
                 }
             }
-            ct_tc_commit(&bar[b]);
+            ct_tc_commit(&bar);
         }
-        ++uses[b];
-        // ---- the previous tile's FP32 accumulator -> per-thread FP64 sums ----
-        if (it > 0) {
-            const int pb = b ^ 1;
-            if (!ct_mbar_wait(&bar[pb], (uses[pb] - 1) & 1u, CT_WAIT_LIMIT)) timed_out = true;
-            if (__syncthreads_or(timed_out)) break;
-            ct_tc_fence_after();
-            gram_readout(tmem + (unsigned)(pb * CT_GRAM_ACC_COLS));
+        // ---- the tile's accumulator -> FP64 sums in shared memory ----
+        if (!ct_mbar_wait(&bar, it & 1u, CT_WAIT_LIMIT)) timed_out = true;
+        if (__syncthreads_or(timed_out)) break;
+        ct_tc_fence_after();
+        if (warp < 4) {
+            const unsigned lanes = tmem + ((unsigned)(warp * 32) << 16);
+#pragma unroll
+            for (int c0 = 0; c0 < NN; c0 += 16) {
+                double t[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) t[j] = 0.0;
+#pragma unroll
+                for (int h = 0; h < CT_GRAM_NACC; ++h) {
+                    float v[16];
+                    ct_tmem_ld16(lanes + (unsigned)(h * NN + c0), v);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) t[j] += (double)v[j];
+                }
+                if (my_r < NROW && (my_row < R8 || (STACK && my_row < 2 * R8))) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        // column c0 + j: a hi column (< R8) or, stacked, a lo column
+                        const int c = STACK && c0 + j >= R8 ? c0 + j - R8 : c0 + j;
+                        const int col = c - my_blk * NA2;
+                        if (col >= 0 && col < NA2 && c0 + j < NN) sacc[my_row * NA2 + col] += t[j];
+                    }
+                }
+            }
         }
+        ct_tc_fence_before();
+        __syncthreads();
     }
-    // the last tile's accumulator
-    if (!timed_out && it > 0) {
-        const int pb = (it - 1) & 1;
-        if (!ct_mbar_wait(&bar[pb], (uses[pb] - 1) & 1u, CT_WAIT_LIMIT)) timed_out = true;
-        if (!__syncthreads_or(timed_out)) {
-            ct_tc_fence_after();
-            gram_readout(tmem + (unsigned)(pb * CT_GRAM_ACC_COLS));
-        }
-    }
-    if (__syncthreads_or(timed_out)) {
-        if (tid == 0) {
-            atomicExch(G.err, 2);
-            abort_flag = 1;
-        }
-        // the MMAs already issued: wait for their completion (bounded) before freeing tensor memory
-        for (int bb = 0; bb < 2; ++bb)
-            if (uses[bb] > 0) ct_mbar_wait(&bar[bb], (uses[bb] - 1) & 1u, CT_WAIT_LIMIT);
+    const bool aborted = __syncthreads_or(timed_out);
+    if (aborted) {
+        if (tid == 0) atomicExch(G.err, 2);
+        // the loop left at tile `it`, whose MMA chain may still run: wait for
+        // it (bounded) before freeing tensor memory
+        ct_mbar_wait(&bar, it & 1u, CT_WAIT_LIMIT);
     }
     ct_tc_fence_before();
     __syncthreads();
@@ -286,11 +291,13 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS) ct_gram(CtGramArgs
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((unsigned)CT_GRAM_TMEM_COLS)
                      : "memory");
-    // this CTA's FP64 partial rows
+    // this CTA's FP64 partial rows (hi and lo rows of a stacked tile added)
     double* out = G.partials + (size_t)blockIdx.x * NROW * NA2;
-    if (my_row < NROW) {
-#pragma unroll
-        for (int j = 0; j < NA2; ++j) out[(size_t)my_row * NA2 + j] = abort_flag ? 0.0 : acc[j];
+    for (int i = tid; i < NROW * NA2; i += CT_GRAM_THREADS) {
+        const int r = i / NA2, j = i % NA2;
+        double v = sacc[r * NA2 + j];
+        if (STACK) v += sacc[(R8 + r) * NA2 + j];
+        out[i] = aborted ? 0.0 : v;
     }
 }
 

@@ -12,7 +12,23 @@ Samples are uniform three-body phase space (seeded) for phsp and background;
 data are drawn by accept-reject against the model at the true couplings
 (|v| in [0.1, 1], uniform phase, first coupling 1 + 0i, seeded) using the
 engine's per-event intensities, or taken as flat phase space when
-``accept_reject=False`` (enough for parity checks).
+``accept_reject=False`` (enough for parity checks). With a background sample
+of weight w, the data hold background events too (n_data in all, the rest
+drawn against the model), per ``data_bkg``:
+
+* ``"draw"`` (default): round(w n_bkg) events of the background's
+  distribution (uniform phase space, their own seed), the background that
+  the subtraction removes. Without them the subtracted density is negative
+  wherever the model is small, and the likelihood falls by thousands of units
+  from the generating parameters.
+* ``"sample"``: the background sample's own n_bkg events. Every subtracted
+  event then enters the NLL with net weight 1 - w > 0, so the likelihood is
+  bounded below. With independent background events it is not: each
+  subtracted event contributes +w log f at its own position, and an
+  amplitude zero placed on it sends the NLL to -infinity (for the three-chain
+  rho model such wells lie a few tens of NLL units below the generating
+  point).
+* ``"none"``: signal events only.
 """
 from __future__ import annotations
 
@@ -200,7 +216,7 @@ def _gen(M, masses, n, seed, gpu, device):
 
 
 def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, seed=0, accept_reject=True,
-         device=0, gpu_generator=None, intensity=None, params_fn=None):
+         device=0, gpu_generator=None, intensity=None, params_fn=None, data_bkg="draw"):
     """Write samples + config.yml for workload `name` into outdir; returns the config path.
 
     accept_reject=True draws the data sample against the model at the true
@@ -226,18 +242,36 @@ def make(name, outdir, n_phsp=None, n_data=None, n_bkg=None, bkg_weight=None, se
             gpu_generator = False
     phsp = _gen(M_JPSI, masses, n_phsp, 1001 + seed, gpu_generator, device)
     toymc.write_npy(out / "phsp.npy", phsp)
-    bkg_path = None
+    bkg_path, bkg = None, None
     if n_bkg:
-        toymc.write_npy(out / "bkg.npy", _gen(M_JPSI, masses, n_bkg, 3001 + seed, gpu_generator, device))
+        bkg = _gen(M_JPSI, masses, n_bkg, 3001 + seed, gpu_generator, device)
+        toymc.write_npy(out / "bkg.npy", bkg)
         bkg_path = str(out / "bkg.npy")
     if accept_reject:
-        data = _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, intensity, params_fn)
+        n_in = bkg_in_data(n_data, n_bkg, bkg_weight, data_bkg)
+        data = _accept_reject(name, out, masses, n_data - n_in, seed, device, gpu_generator, intensity, params_fn)
+        if n_in and data_bkg == "sample":
+            data = np.concatenate([data, bkg[:n_in]])
+        elif n_in:
+            data = np.concatenate([data, _gen(M_JPSI, masses, n_in, 4001 + seed, gpu_generator, device)])
     else:
         data = _gen(M_JPSI, masses, n_data, 2001 + seed, gpu_generator, device)
     toymc.write_npy(out / "data.npy", data)
     cfg = out / "config.yml"
     cfg.write_text(config_text(name, str(out / "phsp.npy"), str(out / "data.npy"), bkg_path, bkg_weight))
     return str(cfg)
+
+
+def bkg_in_data(n_data, n_bkg, bkg_weight, data_bkg="draw"):
+    """Background events in a data sample of n_data whose background sample
+    (n_bkg events of weight bkg_weight) is subtracted: round(w n_bkg) for
+    data_bkg "draw", n_bkg for "sample", 0 for "none"; at most n_data."""
+    if data_bkg not in ("draw", "sample", "none"):
+        raise ValueError("data_bkg must be 'draw', 'sample' or 'none'")
+    if not n_bkg or not bkg_weight or bkg_weight <= 0 or data_bkg == "none":
+        return 0
+    n = int(n_bkg) if data_bkg == "sample" else int(round(float(bkg_weight) * int(n_bkg)))
+    return min(int(n_data), n)
 
 
 def _gpu_intensity(device):
@@ -286,18 +320,24 @@ def _accept_reject(name, out, masses, n_data, seed, device, gpu_generator, inten
     return sel[:n_data]
 
 
-def make_device_samples(name, outdir, n_phsp, n_data, n_bkg=0, bkg_weight=None, seed=0, device=0):
-    """Workload `name` generated and kept on the GPU, background included:
-    returns (config_path, phsp, data, bkg, weights) for
+def make_device_samples(name, outdir, n_phsp, n_data, n_bkg=0, bkg_weight=None, seed=0, device=0, data_bkg="draw"):
+    """Workload `name` generated and kept on the GPU, background included
+    (in the data too, see the module docstring): returns (config_path, phsp,
+    data, bkg, weights) for
     ``analysis.from_device(config_path, phsp, data, bkg, weights=weights)``
     (bkg None when n_bkg is 0; weights: None or [None, None, bkg weights])."""
     import torch
 
-    cfg, phsp, data = make_device(name, outdir, n_phsp, n_data, seed=seed, device=device)
+    w = SIZES[name][3] if bkg_weight is None else bkg_weight
+    n_in = bkg_in_data(n_data, n_bkg, w, data_bkg)
+    cfg, phsp, data = make_device(name, outdir, n_phsp, n_data - n_in, seed=seed, device=device)
     if not n_bkg:
         return cfg, phsp, data, None, None
-    w = SIZES[name][3] if bkg_weight is None else bkg_weight
     bkg = toymc.phase_space_device(M_JPSI, MASSES[name], n_bkg, 3001 + seed, device=device)
+    if n_in and data_bkg == "sample":
+        data = torch.cat([data, bkg[:n_in]])
+    elif n_in:
+        data = torch.cat([data, toymc.phase_space_device(M_JPSI, MASSES[name], n_in, 4001 + seed, device=device)])
     wt = torch.full((n_bkg,), float(w), dtype=torch.float64, device=bkg.device)
     return cfg, phsp, data, bkg, [None, None, wt]
 

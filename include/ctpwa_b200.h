@@ -233,6 +233,22 @@ int ctpwa_fit(ctpwa_handle* h, double* params, const unsigned char* free_mask, c
               int precision, int max_evals, int history, double ftol, double gtol, double* out4, float* eval_ms,
               void* stream);
 
+/* Newton fit with the exact FP64 Hessian (ctpwa_hessian_exact) over the same
+ * box and free variables as ctpwa_fit: Levenberg-Marquardt steps (H + lambda
+ * diag|H|) s = -g, projected onto the box, kept when the NLL (in `precision`)
+ * falls by 1e-4 of the quadratic model's prediction or, for a predicted
+ * decrease <= fnoise, rises by at most fnoise (the NLL's rounding level). It
+ * converges to the stationary point of the start's basin. The reference
+ * checks the Hessian at its L-BFGS result for positive definiteness
+ * (example/fit.py:202-230); this routine polishes a start to such a point,
+ * quadratically. out4: {nll, evaluations, Hessians, status}: status 0
+ * projected gradient <= gtol, 1 a step of max_i |s_i| sqrt(H_ii) <= xtol or
+ * with a predicted decrease <= 1e-2 fnoise, 2 max_iter Hessians spent, 3 no
+ * acceptable step. */
+int ctpwa_fit_newton(ctpwa_handle* h, double* params, const unsigned char* free_mask, const double* lo,
+                     const double* hi, int precision, int max_iter, double xtol, double gtol, double fnoise, double* out4,
+                     void* stream);
+
 /* Evaluation batches (no counterpart in the reference, which serves one
  * analysis per process): several handles of one model (equal configuration,
  * hence one generated kernel) evaluated in one prepare, one prologue, one
@@ -275,6 +291,14 @@ int ctpwa_fit_batched(ctpwa_batch* b, ctpwa_handle* h, double* params, const uns
 typedef int (*ctpwa_fg_fn)(const double* x, double* f, double* g, void* user);
 int ctpwa_minimize_box(ctpwa_fg_fn fn, void* user, int n, double* x, const unsigned char* free_mask, const double* lo,
                        const double* hi, int max_evals, int history, double ftol, double gtol, double* out4);
+
+/* The Newton fit of ctpwa_fit_newton over host functions (no GPU): hfn(x, H,
+ * user) writes the row-major n x n Hessian at x and returns 0 or a nonzero
+ * code that ends the minimisation and is returned. */
+typedef int (*ctpwa_hess_fn)(const double* x, double* H, void* user);
+int ctpwa_minimize_box_newton(ctpwa_fg_fn fn, ctpwa_hess_fn hfn, void* user, int n, double* x,
+                              const unsigned char* free_mask, const double* lo, const double* hi, int max_iter,
+                              double xtol, double gtol, double fnoise, double* out4);
 
 /* Per-sample parts of the last evaluation (host, synchronising):
  * [data_nll, bkg_nll, sum_phsp_intensity, W_data, W_bkg, n_phsp]. */

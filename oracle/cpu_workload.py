@@ -8,7 +8,9 @@ background samples), generated on the host with numpy. The data sample is
 left as C x n_data phase-space candidates (`data: cand.npy` in the config):
 the caller opens the oracle on it, draws the data by accept-reject against
 the model's oracle intensities and keeps the selected events in place
-(Oracle.take), so every candidate's angular tensors are computed once.
+(Oracle.take), so every candidate's angular tensors are computed once. The
+last n_bkg_in_data rows of cand.npy are the data's background events (kept
+as they are, after the n_data - n_bkg_in_data accepted candidates).
 params.json holds the true parameters (seeded couplings, initial resonance
 parameters) and the data size to draw. Loads no product library: the
 workload module is plain Python and the layout comes from the oracle.
@@ -17,6 +19,8 @@ import argparse
 import json
 import sys
 from pathlib import Path
+
+import numpy as np
 
 ROOT = Path(__file__).resolve().parents[1]
 
@@ -37,8 +41,14 @@ def generate(outdir, name="kkpi", seed=0, fraction=1.0, cand_factor=12):
     if n_b:
         toymc.write_npy(out / "bkg.npy", toymc.phase_space(workloads.M_JPSI, masses, n_b, 3001 + seed))
         bkg = str(out / "bkg.npy")
-    n_c = int(cand_factor * n_d)
-    toymc.write_npy(out / "cand.npy", toymc.phase_space(workloads.M_JPSI, masses, n_c, 5001 + seed))
+    # candidates for the signal part of the data, then the data's background
+    # events (uniform phase space, as the device workload draws them)
+    n_in = workloads.bkg_in_data(n_d, n_b, w_b)
+    n_c = int(cand_factor * (n_d - n_in))
+    cand = toymc.phase_space(workloads.M_JPSI, masses, n_c, 5001 + seed)
+    if n_in:
+        cand = np.concatenate([cand, toymc.phase_space(workloads.M_JPSI, masses, n_in, 4001 + seed)])
+    toymc.write_npy(out / "cand.npy", cand)
     cfg = out / "config.yml"
     cfg.write_text(workloads.config_text(name, str(out / "phsp.npy"), str(out / "cand.npy"), bkg, w_b))
     # layout (number of couplings, initial resonance parameters) from the oracle on a tiny sample
@@ -50,7 +60,8 @@ def generate(outdir, name="kkpi", seed=0, fraction=1.0, cand_factor=12):
     nV, nT = o.nV, o.nT
     o.close()
     (out / "params.json").write_text(json.dumps({"true_params": [float(x) for x in p], "nV": nV, "nT": nT,
-                                                 "n_data": n_d, "sizes": [n_p, n_d, n_b], "n_cand": n_c}))
+                                                 "n_data": n_d, "n_bkg_in_data": n_in, "sizes": [n_p, n_d, n_b],
+                                                 "n_cand": n_c}))
     (out / "done").write_text("ok\n")
     return str(cfg)
 

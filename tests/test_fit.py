@@ -149,3 +149,106 @@ def test_argument_checks():
     rc = lib.ctpwa_minimize_box(fn, None, 2, x.ctypes.data_as(dp), fr.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
                                 lo.ctypes.data_as(dp), hi.ctypes.data_as(dp), 10, 5, 0.0, 0.0, out.ctypes.data_as(dp))
     assert rc != 0
+
+
+# ---------------------------------------------------------------------------
+# Newton fit (ctpwa_minimize_box_newton, the minimiser behind ctpwa_fit_newton)
+# ---------------------------------------------------------------------------
+def newton(fun, hess, x0, lo=None, hi=None, free=None, max_iter=100, xtol=1e-10, gtol=1e-12, fnoise=0.0):
+    lib = _lib.load()
+    n = len(x0)
+    x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+    lo = np.full(n, -INF) if lo is None else np.asarray(lo, dtype=np.float64)
+    hi = np.full(n, INF) if hi is None else np.asarray(hi, dtype=np.float64)
+    fr = np.ones(n, dtype=np.uint8) if free is None else np.asarray(free, dtype=np.uint8)
+    calls = {"f": 0, "h": 0}
+
+    def cb(xp, fp, gp, user):
+        calls["f"] += 1
+        r = fun(np.ctypeslib.as_array(xp, shape=(n,)).copy())
+        if isinstance(r, int):
+            return r
+        fp[0] = r[0]
+        np.ctypeslib.as_array(gp, shape=(n,))[:] = r[1]
+        return 0
+
+    def hb(xp, hp, user):
+        calls["h"] += 1
+        r = hess(np.ctypeslib.as_array(xp, shape=(n,)).copy())
+        if isinstance(r, int):
+            return r
+        np.ctypeslib.as_array(hp, shape=(n * n,))[:] = np.asarray(r, dtype=np.float64).reshape(-1)
+        return 0
+
+    fn, hn = _lib.FG_FN(cb), _lib.HESS_FN(hb)
+    out = np.zeros(4)
+    dp = ctypes.POINTER(ctypes.c_double)
+    rc = lib.ctpwa_minimize_box_newton(fn, hn, None, n, x.ctypes.data_as(dp),
+                                       fr.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), lo.ctypes.data_as(dp),
+                                       hi.ctypes.data_as(dp), max_iter, xtol, gtol, fnoise, out.ctypes.data_as(dp))
+    return rc, x, out, calls
+
+
+def rosen_hess(x):
+    return np.array([[2 - 400 * (x[1] - 3 * x[0] ** 2), -400 * x[0]], [-400 * x[0], 200.0]])
+
+
+def test_newton_rosenbrock_unbounded():
+    # the start's Hessian is indefinite: damped steps until it is not
+    rc, x, out, calls = newton(rosen, rosen_hess, [-1.2, 1.0])
+    assert rc == 0 and out[3] in (0, 1), out
+    assert np.allclose(x, [1.0, 1.0], atol=1e-9), x
+    assert out[2] == calls["h"] <= 60 and out[1] == calls["f"]
+
+
+def test_newton_active_bound_and_fixed_parameter():
+    rc, x, out, _ = newton(rosen, rosen_hess, [-1.2, 1.0], hi=[0.5, INF])
+    assert rc == 0 and np.allclose(x, [0.5, 0.25], atol=1e-9), (x, out)
+    # x1 fixed at 0.64: minimum over x0 alone (x0 = 0.8 solves x1 = x0^2 and x0 ~ 1)
+    rc, x, out, _ = newton(rosen, rosen_hess, [0.3, 0.64], free=[1, 0])
+    assert rc == 0 and x[1] == 0.64
+    g = rosen(x)[1]
+    assert abs(g[0]) < 1e-8, (x, g)
+
+
+def test_newton_stays_in_the_basin_of_a_singular_well():
+    # a quadratic bowl at 1 plus a log well at 2.5 that goes to -inf (the
+    # shape a subtracted background event gives a likelihood): from inside
+    # the bowl's basin the iteration converges to the bowl's minimum
+    a, w = 2.5, 0.8
+
+    def fun(x):
+        d = x[0] - a
+        return 50 * (x[0] - 1) ** 2 + w * np.log(d * d), np.array([100 * (x[0] - 1) + 2 * w / d])
+
+    def hess(x):
+        d = x[0] - a
+        return np.array([[100 - 2 * w / (d * d)]])
+
+    rc, x, out, _ = newton(fun, hess, [0.6])
+    assert rc == 0 and out[3] in (0, 1)
+    assert abs(fun(x)[1][0]) < 1e-9 and abs(x[0] - 1) < 0.02 and hess(x)[0, 0] > 0
+
+
+def test_newton_tolerates_rounding_noise_of_f():
+    # f carries a deterministic perturbation of 1e-6: steps whose predicted
+    # decrease is below fnoise are kept, and the iteration ends on the step
+    # size instead of failing to find a decrease
+    def fun(x):
+        f, g = rosen(x)
+        return f + 1e-6 * np.sin(1e7 * x[0] + 3e7 * x[1]), g
+
+    rc, x, out, _ = newton(fun, rosen_hess, [0.8, 0.7], xtol=1e-8, fnoise=1e-5)
+    assert rc == 0 and out[3] == 1, out
+    assert np.allclose(x, [1.0, 1.0], atol=1e-7), x
+
+
+def test_newton_callback_errors_and_arguments():
+    rc, _, _, _ = newton(lambda x: 7, rosen_hess, [0.0, 0.0])
+    assert rc == 7
+    rc, _, _, _ = newton(rosen, lambda x: 9, [0.0, 0.0])
+    assert rc == 9
+    rc, _, _, _ = newton(rosen, rosen_hess, [0.0, 0.0], lo=[1.0, -INF], hi=[0.0, INF])
+    assert rc != 0
+    rc, _, _, _ = newton(rosen, rosen_hess, [0.0, 0.0], max_iter=0)
+    assert rc != 0

@@ -1,14 +1,32 @@
 """Fit-level precision of the mixed form against the plain FP64 path.
 
 J/psi -> pi+ pi- pi0 with three rho chains (rho(770), rho(1450), rho(1700)
-each), 500k data events by accept-reject, 5M phase space and 50k background
-(weight 0.8). From 20 seeded starting points around the generating
-parameters
-the library's fit driver minimises the NLL once in FP64 and once in the
-mixed form. Both fits must reach the same minimum (NLL within 0.01) and
-every fitted parameter must agree within 0.01 sigma, sigma from
-the inverse of the exact FP64 Hessian at the FP64 minimum (example/fit.py:
-213, 333 form the errors the same way).
+each), 500k data events, 5M phase space and 50k uniform background events
+subtracted with weight 0.8; the data are the background sample's 50k events
+and 450k events drawn by accept-reject against the model
+(workloads data_bkg="sample"). From 20 seeded starting points
+around the generating parameters the library's Newton fit (exact FP64
+Hessian, Levenberg-Marquardt steps, `analysis.fitNewton`) minimises the NLL
+once in FP64 and once in the mixed form. Every FP64 minimum must have a
+positive-definite Hessian (the reference keeps a fit only then,
+example/fit.py:202-230), both fits of a start must reach the same minimum
+(NLL within 2e-3, the mixed form's rounding budget twice), and every fitted
+parameter must agree within 0.01 sigma, sigma from the inverse of the exact
+FP64 Hessian at the FP64 minimum (example/fit.py:213, 333 form the errors the
+same way).
+
+Why this data composition: a subtracted background event contributes
++w log f at its own position, so when it is not itself in the data, an
+amplitude zero placed on it sends the NLL to -infinity. With data drawn from
+the model alone the likelihood of this model falls by thousands of units from
+the generating point; with an independent background draw in the data it
+still reaches such a well a few tens of units below it (the Newton iteration
+from the generating point follows the descent until |g| ~ 1e11). With the
+background sample's own events in the data every subtracted event carries
+net weight 1 - w > 0, the likelihood is bounded below, its Hessian at the
+generating point is positive definite, and the Newton iteration converges
+quadratically to the minimum of each start's basin, so the comparison is
+between the two precisions' estimates of the same minimum.
 """
 import numpy as np
 import pytest
@@ -19,20 +37,25 @@ pytestmark = pytest.mark.gpu
 
 
 def start_point(p_true, nV, res, seed):
-    """The generating parameters moved at random: couplings by 20 % (the
-    first one stays fixed to 1 + 0i), resonance parameters by up to 2 % of
-    their allowed range, seeded, so that every start lies in the basin of
-    the generating minimum (the model has other local minima, which would
-    compare the optimiser's paths rather than the precision of the minimum)."""
+    """The generating parameters moved at random: couplings by 5 % (the first
+    one stays fixed to 1 + 0i), resonance parameters by up to 1 % of their
+    allowed range, seeded."""
     rng = np.random.default_rng(seed)
     p = p_true.copy()
     for i in range(1, nV):
-        p[i] *= 1 + 0.2 * rng.standard_normal()
-        p[nV + i] *= 1 + 0.2 * rng.standard_normal()
+        p[i] *= 1 + 0.05 * rng.standard_normal()
+        p[nV + i] *= 1 + 0.05 * rng.standard_normal()
     lo, hi = res[1], res[2]
-    th = p[2 * nV:] + (rng.uniform(size=res.shape[1]) - 0.5) * 0.04 * (hi - lo)
+    th = p[2 * nV:] + (rng.uniform(size=res.shape[1]) - 0.5) * 0.02 * (hi - lo)
     p[2 * nV:] = np.clip(th, lo + 1e-7 * (hi - lo), hi - 1e-7 * (hi - lo))
     return p
+
+
+def fit_pair(ana, x0):
+    """(FP64 result, mixed result): each (params, nll, evaluations, hessians, status)."""
+    r64 = ana.fitNewton(x0, max_iter=60, xtol=1e-5, precision="fp64")
+    rmx = ana.fitNewton(x0, max_iter=60, xtol=1e-5, precision="mixed")
+    return r64, rmx
 
 
 def test_mixed_fits_within_a_hundredth_of_sigma(tmp_path):
@@ -40,7 +63,7 @@ def test_mixed_fits_within_a_hundredth_of_sigma(tmp_path):
     import ctpwa_b200
 
     cfg = workloads.make("pipi_3rho", tmp_path, n_phsp=5_000_000, n_data=500_000, n_bkg=50_000, bkg_weight=0.8,
-                         seed=23)
+                         seed=23, data_bkg="sample")
     ana = ctpwa_b200.analysis(cfg)
     nV, nP = ana.getNVector(), ana.getNParams()
     res = ana.getFreeResParams().numpy()
@@ -50,15 +73,14 @@ def test_mixed_fits_within_a_hundredth_of_sigma(tmp_path):
     worst = 0.0
     for k in range(20):
         x0 = start_point(p_true, nV, res, 1000 + k)
-        x64, n64, _, _, s64, _ = ana.fit(x0, max_evals=3000, ftol=1e-15, gtol=1e-8, precision="fp64")
-        xmx, nmx, _, _, smx, _ = ana.fit(x0, max_evals=3000, ftol=1e-15, gtol=1e-8, precision="mixed")
-        # status 3 (no decrease along the search direction) ends a fit whose
-        # remaining decrease is below the NLL's rounding: it is converged
-        assert s64 in (0, 1, 3) and smx in (0, 1, 3), (k, s64, smx)
-        assert abs(nmx - n64) < 1e-2, (k, n64, nmx)
-        pt = torch.tensor(x64, dtype=torch.float64, device="cuda")
-        C = ana.getCovariance(pt, free=free).cpu().numpy()
-        sigma = np.sqrt(np.diag(C)[free])
+        (x64, n64, _, _, s64), (xmx, nmx, _, _, smx) = fit_pair(ana, x0)
+        assert s64 in (0, 1) and smx in (0, 1), (k, s64, smx)
+        H = ana.getHessian(torch.tensor(x64, dtype=torch.float64, device="cuda")).cpu().numpy()[np.ix_(free, free)]
+        ev = np.linalg.eigvalsh(H)
+        assert ev[0] > 0, (k, ev[0])
+        assert abs(nmx - n64) < 2e-3, (k, n64, nmx)
+        sigma = np.sqrt(np.diag(np.linalg.inv(H)))
         d = np.abs(xmx[free] - x64[free]) / sigma
         worst = max(worst, float(d.max()))
-        assert d.max() < 0.01, (k, d.max(), s64, smx, n64, nmx)
+        assert d.max() < 0.01, (k, d.max(), n64, nmx)
+    print(f"worst |mixed - fp64| / sigma over 20 starts: {worst:.2e}")

@@ -652,17 +652,25 @@ def test_custom_expression_language_parity(tmp_path, expr):
 def test_device_covariance(setups):
     """Covariance on the device: the FP64 inverse of the Hessian over the free
     parameters equals the host inverse; a matrix that is not positive
-    definite is reported."""
+    definite is reported. The sample here is not drawn from the model, so its
+    Hessian at this point need not be positive definite; the inverse is
+    checked on the Hessian shifted to a well-conditioned SPD matrix."""
     import torch
     import ctpwa_b200
 
     ana, _, pt, _ = setups["kkpi"]
     H = ana.getHessian(pt)
-    C = ana.getCovariance(pt, hessian=H).cpu().numpy()
     n = ana.getNVector()
     free = [j for j in range(ana.getNParams()) if j not in (0, n)]
     Hf = H.cpu().numpy()[np.ix_(free, free)]
-    ref = np.linalg.inv(Hf)
+    ev = np.linalg.eigvalsh(Hf)
+    if ev[0] <= 0.0:
+        with pytest.raises(RuntimeError, match="not positive definite"):
+            ana.getCovariance(pt, hessian=H)
+    shift = max(0.0, -ev[0]) + 0.1 * np.max(np.abs(ev))
+    Hs = H + shift * torch.eye(H.shape[0], dtype=torch.float64, device=H.device)
+    C = ana.getCovariance(pt, hessian=Hs).cpu().numpy()
+    ref = np.linalg.inv(Hf + shift * np.eye(len(free)))
     assert np.max(np.abs(C[np.ix_(free, free)] - ref)) <= 1e-9 * np.max(np.abs(ref))
     assert np.all(C[0] == 0) and np.all(C[:, n] == 0)
     with pytest.raises(RuntimeError, match="not positive definite"):

@@ -3,7 +3,7 @@
 M_ab = (1/W) sum_e w_e sum_pol A_a conj(A_b) (the reference's normalisation
 matrix, src/ComputeHessian.cu:1181-1197 with src/Analysis.cu:729-805). The
 device forms the amplitudes in the mixed form (FP32) and the products on the
-tensor cores (BF16 hi + lo operands, FP32 accumulation per 128-event tile, FP64
+tensor cores (BF16 hi + lo operands, FP32 accumulation per 256-event tile, FP64
 beyond); the oracle's amplitudes and sums are FP64. Tolerance: 1e-6 of the
 largest |M_ab| elementwise (measured 3.5e-7 to 4.5e-7), and 1e-6 relative on the phase-space mean
 intensity v^T M conj(v).
@@ -49,5 +49,5 @@ def test_gram_matches_oracle(tmp_path, name):
     cp = ana.getModel()["coupling"]
     v = np.array([r * complex(p[c], p[nV + c]) for c, r in zip(cp["amp_chain"], cp["ratio"])])
     f = np.real(v @ M @ np.conj(v))
-    mean = parts[2] / parts[5]
+    mean = parts[2]  # the phase-space factor: weighted intensity sum / weight total
     assert abs(f - mean) <= 1e-6 * abs(mean), (f, mean)
