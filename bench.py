@@ -493,7 +493,7 @@ def toy_fit(args, device):
     from ctpwa_b200 import serving
 
     keys = ("jobs", "failed", "fits_per_hour", "evals", "eval_ms_p50", "eval_ms_p99", "fit_ms_p50", "fit_ms_p99",
-            "service_ms_p50", "service_ms_p99", "phase_ms_p50")
+            "service_ms_p50", "service_ms_p99", "phase_ms_p50", "slowest")
     nd_range = (10_000, 2_000_000)
     # one untimed job per model and precision first, at the stream's largest
     # size: process-level one-time costs (library and kernel loading, growth
@@ -509,8 +509,10 @@ def toy_fit(args, device):
     sweep = []
     for rate in args.toy_rates:
         row = {"rate_per_s": rate}
-        for prec in ("mixed", "fp64"):
-            srv = serving.Server(device=device, slots=4)
+        # each precision with every fit evaluating on its own, and with the
+        # running fits' evaluations gathered into shared launches
+        for prec, batch in (("mixed", False), ("fp64", False), ("mixed", True), ("fp64", True)):
+            srv = serving.Server(device=device, slots=4, batch=batch)
             try:
                 jobs = serving.poisson_stream(rate, args.toy_jobs, nd_range=nd_range, precision=prec,
                                               seed=17 + args.seed)
@@ -519,12 +521,14 @@ def toy_fit(args, device):
                 s = serving.summary(res, time.perf_counter() - t)
             finally:
                 srv.close()
-            row[prec] = {k: s[k] for k in keys}
+            row[prec + ("_batched" if batch else "")] = {k: s[k] for k in keys}
         sweep.append(row)
     return {"sweep": sweep,
             "config": {"rates_per_s": list(args.toy_rates), "jobs_per_rate": args.toy_jobs, "slots": 4,
                        "n_data": "log-uniform 10k-2M", "n_phsp": "10 x n_data", "models": ["pipi_rho", "pipi_3rho"],
-                       "fit": "native projected L-BFGS (ctpwa_fit), GIL released"}}
+                       "fit": "native projected L-BFGS (ctpwa_fit), GIL released",
+                       "batched": "*_batched: the running fits' evaluations gathered into one launch per model and "
+                                  "precision (ctpwa_fit_batched, 200 us gather window)"}}
 
 
 def run_gpu(args, rank, world, local_rank):

@@ -2524,7 +2524,7 @@ void Engine::compileGram()
     CT_CUDA(cudaLibraryGetKernel(&kg, lib, "ct_gram"));
     CT_CUDA(cudaLibraryGetKernel(&kf, lib, "ct_gram_finalize"));
     // operand tile(s) of 128 rows x 256 events (BF16; one when the hi and lo
-    // rows fit together) and the FP64 sums [128][2 nA] (kernels/gram.cuh)
+    // rows fit together) and the FP64 sums [2 nA][128] (kernels/gram.cuh)
     const int r8 = (rows + 7) / 8 * 8;
     gram_dsmem_ = (2 * r8 <= 128 ? 1 : 2) * 128 * 256 * 2 + 128 * 2 * model_.nAmp() * 8;
     CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributeMaxDynamicSharedMemorySize, gram_dsmem_));

@@ -54,7 +54,7 @@ static_assert(CT_GRAM_ROWS <= 128, "the tensor-core Gram supports npol * 2 * nA 
 #define CT_GRAM_SBO 4096
 #define CT_GRAM_PART (128 * CT_GRAM_TILE * 2)  // bytes of one BF16 operand tile (128 rows)
 #define CT_GRAM_NPART (CT_GRAM_STACK ? 1 : 2)
-// dynamic shared memory: operand tile(s), then the FP64 sums [128][2 nA]
+// dynamic shared memory: operand tile(s), then the FP64 sums [2 nA][128]
 #define CT_GRAM_SMEM (CT_GRAM_NPART * CT_GRAM_PART + 128 * 2 * M_NA * 8)
 #ifndef CT_GRAM_PAIRED
 #define CT_GRAM_PAIRED 0
@@ -127,13 +127,15 @@ __device__ __forceinline__ void ct_tmem_ld16(unsigned taddr, float* v)
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS) ct_gram(CtGramArgs G)
+// two CTAs per SM (<= 128 registers): one CTA's MMA chain, barriers and
+// read-out overlap the other's event work
+extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS, 2) ct_gram(CtGramArgs G)
 {
     constexpr int NROW = CT_GRAM_ROWS, R8 = CT_GRAM_R8, NN = CT_GRAM_N, NA2 = 2 * M_NA;
     constexpr bool STACK = CT_GRAM_STACK;
     constexpr int NPS = CT_GRAM_PAIRED ? CT_NPOL_STORED : M_NPOL;
     extern __shared__ __align__(1024) unsigned char gsm[];
-    double* sacc = (double*)(gsm + CT_GRAM_NPART * CT_GRAM_PART);  // [128][NA2]
+    double* sacc = (double*)(gsm + CT_GRAM_NPART * CT_GRAM_PART);  // [NA2][128]: a warp's rows are consecutive
     __shared__ __align__(8) unsigned long long bar;
     __shared__ unsigned tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -270,7 +272,7 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS) ct_gram(CtGramArgs
                         // column c0 + j: a hi column (< R8) or, stacked, a lo column
                         const int c = STACK && c0 + j >= R8 ? c0 + j - R8 : c0 + j;
                         const int col = c - my_blk * NA2;
-                        if (col >= 0 && col < NA2 && c0 + j < NN) sacc[my_row * NA2 + col] += t[j];
+                        if (col >= 0 && col < NA2 && c0 + j < NN) sacc[col * 128 + my_row] += t[j];
                     }
                 }
             }
@@ -295,8 +297,8 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS) ct_gram(CtGramArgs
     double* out = G.partials + (size_t)blockIdx.x * NROW * NA2;
     for (int i = tid; i < NROW * NA2; i += CT_GRAM_THREADS) {
         const int r = i / NA2, j = i % NA2;
-        double v = sacc[r * NA2 + j];
-        if (STACK) v += sacc[(R8 + r) * NA2 + j];
+        double v = sacc[j * 128 + r];
+        if (STACK) v += sacc[j * 128 + R8 + r];
         out[i] = aborted ? 0.0 : v;
     }
 }

@@ -252,7 +252,13 @@ class Server:
         within their bounds, as the reference's fit clamps them."""
         import torch
 
-        x, nll, n_evals, _, _, lat = ana.fit(start, max_evals=spec.max_evals, history=20, ftol=1e-13, gtol=1e-9,
+        # relative decrease at which the fit stops: in the mixed form the NLL
+        # carries ~1e-4 to 1e-3 of rounding at these sizes, and a stop below it
+        # turns into line searches that cannot find a decrease (49 evaluations
+        # instead of 9 on a 2M-event job); 1e-10 of |NLL| is ~1e-4 at 1M
+        # events, far below the 0.5 of one standard deviation
+        ftol = 1e-10 if ana.getPrecision() == "mixed" else 1e-13
+        x, nll, n_evals, _, _, lat = ana.fit(start, max_evals=spec.max_evals, history=20, ftol=ftol, gtol=1e-9,
                                              stream=stream, batch=self.batch)
         return torch.tensor(x, dtype=torch.float64, device=torch.device("cuda", self.device)), nll, n_evals, lat
 
@@ -353,8 +359,18 @@ def summary(results: List[JobResult], wall_s: float) -> dict:
         "service_ms_p99": percentile(service, 99),
         "phase_ms_p50": {k: percentile([r.phase_ms[k] for r in ok if k in r.phase_ms], 50)
                          for k in sorted({k for r in ok for k in r.phase_ms})},
+        "slowest": _job_record(max(ok, key=lambda r: r.fit_latency)) if ok else None,
         "errors": [r.error for r in results if r.error][:5],
     }
+
+
+def _job_record(r: JobResult) -> dict:
+    """One job's size, evaluations and latency breakdown (ms): where a tail
+    latency comes from."""
+    return {"job": r.job_id, "model": r.model, "n_data": r.n_data, "n_phsp": r.n_phsp, "evals": r.n_evals,
+            "fit_ms": 1e3 * r.fit_latency, "queue_ms": 1e3 * (r.admitted - r.arrival),
+            "eval_ms_sum": float(np.sum(r.eval_ms)) if r.eval_ms else 0.0,
+            "phase_ms": {k: round(v, 3) for k, v in r.phase_ms.items()}}
 
 
 def main(argv=None):
