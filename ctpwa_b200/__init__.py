@@ -691,6 +691,25 @@ class analysis:
             raise RuntimeError(_lib.error(self._h))
         return out
 
+    def getSetupTimes(self) -> dict:
+        """Host milliseconds of this handle's set-up phases (model and
+        generated code, CUDA context, kernel modules, sample upload, angular
+        tables and kernels, the angular pass, polarisation pairing, buffers)."""
+        self._check()
+        buf = ctypes.create_string_buffer(1024)
+        n = self._lib.ctpwa_setup_times(self._h, buf, 1024)
+        if n < 0:
+            raise RuntimeError(_lib.error(self._h))
+        if n > 1024:
+            buf = ctypes.create_string_buffer(n)
+            self._lib.ctpwa_setup_times(self._h, buf, n)
+        out = {}
+        for item in buf.value.decode().split(";"):
+            if item:
+                k, v = item.split("=")
+                out[k] = float(v)
+        return out
+
     def eventLayout(self) -> dict:
         """Per-event cache layout: angular planes, polarisations, kinematic values,
         invariant masses, and the frontier values each evaluation reads (FP64

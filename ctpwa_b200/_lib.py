@@ -82,6 +82,7 @@ SIGNATURES = {
     "ctpwa_kernel_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "ctpwa_kernel_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "ctpwa_jit_seconds": (ctypes.c_double, [ctypes.c_void_p]),
+    "ctpwa_setup_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "ctpwa_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ctpwa_describe": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p,
                                       ctypes.c_size_t]),

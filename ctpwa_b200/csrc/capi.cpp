@@ -9,6 +9,7 @@
 
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -840,6 +841,18 @@ int ctpwa_model_json(const ctpwa_handle* h, char* buf, size_t cap)
 size_t ctpwa_device_bytes(const ctpwa_handle* h) { return h ? h->eng->deviceBytes() : 0; }
 
 double ctpwa_jit_seconds(const ctpwa_handle* h) { return h ? h->eng->jitSeconds() : -1.0; }
+
+int ctpwa_setup_times(const ctpwa_handle* h, char* buf, size_t cap)
+{
+    if (!h) return CTPWA_ERR_ARG;
+    std::string t;
+    for (const auto& p : h->eng->setupTimes()) {
+        char v[64];
+        std::snprintf(v, sizeof v, "%.4f", p.second);
+        t += (t.empty() ? "" : ";") + p.first + "=" + v;
+    }
+    return copyOut(t, buf, cap);
+}
 
 const char* ctpwa_last_error(const ctpwa_handle* h)
 {

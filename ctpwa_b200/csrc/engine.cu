@@ -821,6 +821,14 @@ void Engine::layoutCtas(int target, long long tot, int block, CtaLayout& lay) co
 
 Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(opt)
 {
+    // host time of each set-up phase (device work of the phase finished)
+    auto t_last = std::chrono::steady_clock::now();
+    auto mark = [&](const char* name) {
+        if (init_stream_) CT_CUDA(cudaStreamSynchronize(init_stream_));
+        const auto t = std::chrono::steady_clock::now();
+        setup_ms_.emplace_back(name, std::chrono::duration<double, std::milli>(t - t_last).count());
+        t_last = t;
+    };
     Config cfg = loadConfig(config_path);
     if (!cfg.valid()) {
         std::string w = cfg.warnings.empty() ? "" : (": " + cfg.warnings.front());
@@ -832,6 +840,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
         for (const auto& r : b.res)
             if (r.type == ModelType::Custom) checkCustomExpr(r.options.at("expr"), r.param_names);
     gen_ = cachedGenerate(model_, config_path);
+    mark("model");
     int ndev = 0;
     CT_CUDA(cudaGetDeviceCount(&ndev));
     if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
@@ -841,12 +850,29 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     // initialisation work goes to a private non-blocking stream, so a handle
     // being created does not serialise with other handles' evaluations
     CT_CUDA(cudaStreamCreateWithFlags(&init_stream_, cudaStreamNonBlocking));
+    mark("context");
     compileKernel();
+    mark("kernels");
     loadSamples();
+    mark("samples");
     buildTables();
+    mark("angular_tables");
+    {
+        // the generated kernels gather the pairing check's maxima as they
+        // write the tables (pairPolarisations reads them)
+        const int npair = model_.npol / 2, nplane = gen_.nplane;
+        bool all = !k_ang_.empty();
+        for (void* k : k_ang_) all = all && k;
+        if (all && npair > 0 && nplane * npair <= 32) {
+            alloc(d_pairmax_, sizeof(unsigned long long) * (2 * nplane * npair + 1));
+            CT_CUDA(cudaMemsetAsync(d_pairmax_, 0, sizeof(unsigned long long) * (2 * nplane * npair + 1), init_stream_));
+        }
+    }
     for (int k = 0; k < 3; ++k)
         if (samples_[k].n > 0 || k < 2) computeAngular(k);
+    mark("angular");
     pairPolarisations();
+    mark("pairing");
     // evaluation buffers
     int nA = model_.nAmp();
     alloc(d_v_, sizeof(double) * 2 * nA);
@@ -893,6 +919,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     alloc(d_mask_, sizeof(int) * std::max(1, (int)model_.blocks.size()));
     CT_CUDA(cudaMemsetAsync(d_err_, 0, sizeof(int), init_stream_));
     alloc(d_hscratch_, sizeof(double) * (3 * (size_t)std::max(1, model_.nParams()) + 1));
+    mark("buffers");
     CT_CUDA(cudaStreamSynchronize(init_stream_));
     cudaStreamDestroy(init_stream_);
     init_stream_ = nullptr;
@@ -912,6 +939,7 @@ Engine::~Engine()
         devFree(s.w);
     }
     devFree(d_ag_tables_);
+    devFree(d_pairmax_);
     devFree(d_v_);
     devFree(d_consts_);
     devFree(d_kblock_);
@@ -1028,63 +1056,38 @@ void Engine::loadSamples()
     }
 }
 
-void Engine::buildTables()
+std::string jitAngularCubin(const std::string& src, bool* cache_hit);
+bool angularInterpreted();
+
+// Host description of every angular group (AgGroup with its tables: the
+// (S, L) variant of each vertex per SL combination, the polarisation map,
+// the kinematic slots it fills), appending the vertex variants and their
+// Clebsch-Gordan products to vars / cg. Shared by the device tables of
+// Engine::buildTables and the generated angular kernels (angularSource),
+// so the offsets into cg agree.
+struct AgGroupHost {
+    AgGroup g;
+    std::vector<int> sl_var, pol_map, kin;
+};
+
+std::vector<AgGroupHost> angularGroups(const Model& model, const GeneratedModel& gen, std::vector<AgNodeVar>& vars,
+                                       std::vector<double>& cg)
 {
-    // Layout of one device allocation: vars | cg | ylm_norm | dcoef | doff | per-group (sl_var, pol_map, kin)
-    std::vector<AgNodeVar> vars;
-    std::vector<double> cg;
-    std::vector<double> ylm(AG_MAXD * AG_MAXD, 0.0);
-    for (int l = 0; l < AG_MAXD; ++l)
-        for (int am = 0; am <= l; ++am)
-            ylm[l * AG_MAXD + am] = (l == 0) ? 0.5 * std::sqrt(1.0 / M_PI)
-                                             : std::sqrt((2.0 * l + 1.0) * refFactorial((float)(l - am)) /
-                                                         (4.0 * M_PI * refFactorial((float)(l + am))));
-    std::vector<double> dcoef;
-    std::vector<int> doff((AG_MAXD + 1) * AG_MAXD * AG_MAXD, 0);
-    for (int dim = 1; dim <= AG_MAXD; ++dim) {
-        float j = (dim - 1) / 2.0f;
-        for (int i1 = 0; i1 < dim; ++i1)
-            for (int i2 = 0; i2 < dim; ++i2) {
-                float m1 = (dim - 1 - 2 * i1) / 2.0f, m2 = (dim - 1 - 2 * i2) / 2.0f;
-                doff[(dim * AG_MAXD + i1) * AG_MAXD + i2] = (int)dcoef.size();
-                size_t cnt_pos = dcoef.size();
-                dcoef.push_back(0.0);
-                int kmin = (m1 < m2) ? 0 : (int)(m1 - m2);
-                int kmax = (m1 > -m2) ? (int)(j - m2) : (int)(j + m1);
-                int cnt = 0;
-                for (int k = kmin; k <= kmax; ++k) {
-                    double num = refFactorial(j + m2) * refFactorial(j - m2) * refFactorial(j + m1) * refFactorial(j - m1);
-                    double den = refFactorial((float)k) * refFactorial(j - m2 - k) * refFactorial(j + m1 - k) *
-                                 refFactorial(k - m1 + m2);
-                    double c = std::pow(-1.0, k - m1 + m2) * std::sqrt(num) / den;
-                    dcoef.push_back(c);
-                    dcoef.push_back(2 * j + m1 - m2 - 2 * k);
-                    dcoef.push_back(2 * k - m1 + m2);
-                    ++cnt;
-                }
-                dcoef[cnt_pos] = cnt;
-            }
-    }
-    // per-group node variants and CG products
-    struct GroupHost {
-        AgGroup g;
-        std::vector<int> sl_var, pol_map, kin;
-    };
-    std::vector<GroupHost> gh(model_.groups.size());
-    for (size_t gi = 0; gi < model_.groups.size(); ++gi) {
-        const Group& G = model_.groups[gi];
-        GroupHost& H = gh[gi];
+    std::vector<AgGroupHost> gh(model.groups.size());
+    for (size_t gi = 0; gi < model.groups.size(); ++gi) {
+        const Group& G = model.groups[gi];
+        AgGroupHost& H = gh[gi];
         AgGroup& A = H.g;
         std::memset(&A, 0, sizeof(A));
         if ((int)G.particle_names.size() > AG_MAXP || (int)G.nodes.size() > AG_MAXN)
             throw std::runtime_error("decay chain too large for the angular kernel");
         A.np = (int)G.particle_names.size();
-        A.nfin = (int)model_.final_order.size();
+        A.nfin = (int)model.final_order.size();
         A.nnodes = (int)G.nodes.size();
         A.nsl = G.nSL();
-        A.npol = model_.npol;
+        A.npol = model.npol;
         A.tensor_size = G.tensor_size;
-        A.plane0 = gen_.group_plane0[gi];
+        A.plane0 = gen.group_plane0[gi];
         for (int i = 0; i < A.np; ++i) {
             A.input_slot[i] = G.input_slot[i];
             A.sum_a[i] = G.sum_of[i].first;
@@ -1144,13 +1147,234 @@ void Engine::buildTables()
         }
         for (int s = 0; s < G.nSL(); ++s)
             for (size_t ni = 0; ni < G.nodes.size(); ++ni) H.sl_var.push_back(G.sl_combs[s][ni]);
-        H.pol_map = model_.pol_map;
-        for (size_t k = 0; k < gen_.slots.size(); ++k) {
-            const KinSlot& ks = gen_.slots[k];
+        H.pol_map = model.pol_map;
+        for (size_t k = 0; k < gen.slots.size(); ++k) {
+            const KinSlot& ks = gen.slots[k];
             if (ks.group != (int)gi) continue;
             H.kin.insert(H.kin.end(), {ks.type, ks.a, ks.b, ks.c, (int)k});
         }
         A.nkin = (int)H.kin.size() / 5;
+    }
+    return gh;
+}
+
+// CUDA source of the generated angular kernels: one kernel ct_ang_<g> per
+// angular group, straight-line code over the group's particles, kinematic
+// slots, vertices and SL combinations with every tensor shape fixed
+// (kernels/angular_gen.cuh), the same values as ag_group_kernel's
+// interpretation of the group tables. Each vertex's frame and rotations are
+// computed once per event; each SL combination contracts its vertex tensors
+// along the chain in the interpreter's order and writes its planes.
+std::string angularSource(const std::vector<AgGroupHost>& gh, const std::vector<AgNodeVar>& vars, int nplane)
+{
+    std::ostringstream o;
+    o << "// generated by ctpwa_b200 (Engine angular kernels)\n#include \"angular_gen.cuh\"\n\n";
+    for (size_t gi = 0; gi < gh.size(); ++gi) {
+        const AgGroup& A = gh[gi].g;
+        const int npair = A.npol / 2;
+        // pairmax (may be null): maxima over events of
+        // |SL_{c,npol-1-q} -+ conj(SL_{c,q})| at [(c npair + q) 2 + 0 / 1] and
+        // of |SL| at [2 nplane npair] (the layout of ct_pair_check_kernel),
+        // accumulated by one atomic per warp and value
+        o << "extern \"C\" __global__ void __launch_bounds__(128) ct_ang_" << gi
+          << "(const double* __restrict__ p4, long long n, long long ld, AgTables T, double2* __restrict__ out64,\n"
+             "    float2* __restrict__ out32, double* __restrict__ kin, unsigned long long* __restrict__ pairmax)\n{\n"
+             "  const long long e = (long long)blockIdx.x * 128 + threadIdx.x;\n";
+        if (npair > 0) {
+            o << "  double pm[" << std::max(1, 2 * A.nsl * npair) << "] = {}, big = 0.0;\n";
+            o << "  if (e < n) {\n";
+        } else {
+            o << "  if (e >= n) return;\n  {\n";
+        }
+        for (int f = 0; f < A.nfin; ++f)
+            o << "  const V4 f" << f << " = {p4[" << 4 * f << " * n + e], p4[" << 4 * f + 1 << " * n + e], p4[" << 4 * f + 2
+              << " * n + e], p4[" << 4 * f + 3 << " * n + e]};\n";
+        o << "  V4 parent = {0, 0, 0, 0};\n";
+        for (int f = 0; f < A.nfin; ++f) o << "  parent = v4add(parent, f" << f << ");\n";
+        for (int k = 0; k < A.np; ++k) {
+            const int idx = A.build_order[k], sl = A.input_slot[idx];
+            o << "  const V4 m" << idx << " = ";
+            if (sl >= 0) o << "f" << sl;
+            else if (sl == -1) o << "parent";
+            else o << "v4add(m" << A.sum_a[idx] << ", m" << A.sum_b[idx] << ")";
+            o << ";\n";
+        }
+        const auto& K = gh[gi].kin;
+        for (size_t k = 0; k + 4 < K.size(); k += 5) {
+            const int type = K[k], a = K[k + 1], b = K[k + 2] >= 0 ? K[k + 2] : K[k + 1],
+                      c = K[k + 3] >= 0 ? K[k + 3] : K[k + 1];
+            o << "  kin[" << K[k + 4] << "LL * ld + e] = agKin<" << type << ">(m" << a << ", m" << b << ", m" << c
+              << ");\n";
+        }
+        for (int ni = 0; ni < A.nnodes; ++ni) {
+            const AgNode& nd = A.nodes[ni];
+            o << "  AgVertexFrame<" << nd.dj1 << ", " << nd.dj2 << "> F" << ni << ";\n  agVertexFrame<" << nd.dj1 << ", "
+              << nd.dj2 << ">(T, m" << nd.d1 << ", m" << nd.d2 << ", F" << ni << ");\n";
+        }
+        for (int s = 0; s < A.nsl; ++s) {
+            o << "  {  // SL combination " << s << "\n";
+            std::vector<int> shape, labels;
+            for (int ni = 0; ni < A.nnodes; ++ni) {
+                const AgNode& nd = A.nodes[ni];
+                const AgNodeVar& v = vars[nd.var_off + gh[gi].sl_var[s * A.nnodes + ni]];
+                const int size = nd.dj * nd.dj1 * nd.dj2;
+                o << "    double2 a" << ni << "[" << size << "];\n    agVertexAmp<" << nd.dj << ", " << nd.dj1 << ", "
+                  << nd.dj2 << ", " << v.L << ">(T, F" << ni << ", T.cg + " << v.cg_off << ", a" << ni << ");\n";
+                if (ni == 0) {
+                    shape = {nd.dj, nd.dj1, nd.dj2};
+                    labels = {nd.mother, nd.d1, nd.d2};
+                    o << "    const double2* c0 = a0;\n";
+                    continue;
+                }
+                const int rank = (int)shape.size();
+                int c = 0;
+                for (int j = 0; j < rank; ++j)
+                    if (labels[j] == nd.mother) {
+                        c = j;
+                        break;
+                    }
+                std::vector<int> st(rank);
+                st[rank - 1] = 1;
+                for (int j = rank - 2; j >= 0; --j) st[j] = st[j + 1] * shape[j + 1];
+                std::vector<int> oshape;
+                for (int j = 0; j < rank; ++j)
+                    if (j != c) oshape.push_back(shape[j]);
+                oshape.push_back(nd.dj1);
+                oshape.push_back(nd.dj2);
+                int total = 1;
+                for (int x : oshape) total *= x;
+                o << "    double2 c" << ni << "[" << total << "];\n";
+                const int ro = (int)oshape.size();
+                for (int idx = 0; idx < total; ++idx) {
+                    int t = idx;
+                    std::vector<int> ic(ro);
+                    for (int j = ro - 1; j >= 0; --j) {
+                        ic[j] = t % oshape[j];
+                        t /= oshape[j];
+                    }
+                    int base = 0, pos = 0;
+                    for (int j = 0; j < rank; ++j)
+                        if (j != c) base += ic[pos++] * st[j];
+                    o << "    c" << ni << "[" << idx << "] = agContract<" << shape[c] << ", " << nd.dj1 << ", " << nd.dj2
+                      << ">(c" << ni - 1 << ", " << base << ", " << st[c] << ", a" << ni << ", " << ic[ro - 2] << ", "
+                      << ic[ro - 1] << ");\n";
+                }
+                shape = oshape;
+                labels.erase(labels.begin() + c);
+                labels.push_back(nd.d1);
+                labels.push_back(nd.d2);
+            }
+            const int last = A.nnodes - 1;
+            const long long plane = (long long)(A.plane0 + s) * A.npol;
+            std::vector<int> srcs(A.npol);
+            for (int p = 0; p < A.npol; ++p) {
+                const int src = gh[gi].pol_map.empty() ? p : gh[gi].pol_map[p];
+                srcs[p] = src;
+                o << "    { const double2 v = c" << last << "[" << src << "]; out64[" << plane + p
+                  << "LL * ld + e] = v; if (out32) out32[" << plane + p
+                  << "LL * ld + e] = make_float2((float)v.x, (float)v.y); }\n";
+            }
+            if (npair > 0) {
+                for (int p = 0; p < A.npol; ++p)
+                    o << "    big = fmax(big, agDist(c" << last << "[" << srcs[p] << "].x, c" << last << "[" << srcs[p]
+                      << "].y));\n";
+                for (int q = 0; q < npair; ++q) {
+                    const std::string a = "c" + std::to_string(last) + "[" + std::to_string(srcs[q]) + "]",
+                                      b = "c" + std::to_string(last) + "[" + std::to_string(srcs[A.npol - 1 - q]) + "]";
+                    const int k = (s * npair + q) * 2;
+                    o << "    pm[" << k << "] = fmax(pm[" << k << "], agDist(" << b << ".x - " << a << ".x, " << b << ".y + "
+                      << a << ".y));\n";
+                    o << "    pm[" << k + 1 << "] = fmax(pm[" << k + 1 << "], agDist(" << b << ".x + " << a << ".x, " << b
+                      << ".y - " << a << ".y));\n";
+                }
+            }
+            o << "  }\n";
+        }
+        o << "  }\n";
+        if (npair > 0) {
+            o << "  if (pairmax) {\n    const int lane = threadIdx.x & 31;\n";
+            for (int s = 0; s < A.nsl; ++s)
+                for (int q = 0; q < npair; ++q)
+                    for (int w = 0; w < 2; ++w) {
+                        const int k = (s * npair + q) * 2 + w;
+                        const int out = ((A.plane0 + s) * npair + q) * 2 + w;
+                        o << "    { const double v = agWarpMax(pm[" << k << "]); if (lane == 0) atomicMax(pairmax + " << out
+                          << ", (unsigned long long)__double_as_longlong(v)); }\n";
+                    }
+            o << "    { const double v = agWarpMax(big); if (lane == 0) atomicMax(pairmax + " << 2 * nplane * npair
+              << ", (unsigned long long)__double_as_longlong(v)); }\n  }\n";
+        }
+        o << "}\n\n";
+    }
+    return o.str();
+}
+
+void Engine::buildTables()
+{
+    // Layout of one device allocation: vars | cg | ylm_norm | dcoef | doff | per-group (sl_var, pol_map, kin)
+    std::vector<AgNodeVar> vars;
+    std::vector<double> cg;
+    std::vector<double> ylm(AG_MAXD * AG_MAXD, 0.0);
+    for (int l = 0; l < AG_MAXD; ++l)
+        for (int am = 0; am <= l; ++am)
+            ylm[l * AG_MAXD + am] = (l == 0) ? 0.5 * std::sqrt(1.0 / M_PI)
+                                             : std::sqrt((2.0 * l + 1.0) * refFactorial((float)(l - am)) /
+                                                         (4.0 * M_PI * refFactorial((float)(l + am))));
+    std::vector<double> dcoef;
+    std::vector<int> doff((AG_MAXD + 1) * AG_MAXD * AG_MAXD, 0);
+    for (int dim = 1; dim <= AG_MAXD; ++dim) {
+        float j = (dim - 1) / 2.0f;
+        for (int i1 = 0; i1 < dim; ++i1)
+            for (int i2 = 0; i2 < dim; ++i2) {
+                float m1 = (dim - 1 - 2 * i1) / 2.0f, m2 = (dim - 1 - 2 * i2) / 2.0f;
+                doff[(dim * AG_MAXD + i1) * AG_MAXD + i2] = (int)dcoef.size();
+                size_t cnt_pos = dcoef.size();
+                dcoef.push_back(0.0);
+                int kmin = (m1 < m2) ? 0 : (int)(m1 - m2);
+                int kmax = (m1 > -m2) ? (int)(j - m2) : (int)(j + m1);
+                int cnt = 0;
+                for (int k = kmin; k <= kmax; ++k) {
+                    double num = refFactorial(j + m2) * refFactorial(j - m2) * refFactorial(j + m1) * refFactorial(j - m1);
+                    double den = refFactorial((float)k) * refFactorial(j - m2 - k) * refFactorial(j + m1 - k) *
+                                 refFactorial(k - m1 + m2);
+                    double c = std::pow(-1.0, k - m1 + m2) * std::sqrt(num) / den;
+                    dcoef.push_back(c);
+                    dcoef.push_back(2 * j + m1 - m2 - 2 * k);
+                    dcoef.push_back(2 * k - m1 + m2);
+                    ++cnt;
+                }
+                dcoef[cnt_pos] = cnt;
+            }
+    }
+    // per-group node variants and CG products
+    std::vector<AgGroupHost> gh = angularGroups(model_, gen_, vars, cg);
+    if (!angularInterpreted() && !gh.empty()) {
+        const std::string src = angularSource(gh, vars, gen_.nplane);
+        // the module has no per-handle state (unlike the fused kernels'
+        // constant bank): handles of one model share one loaded copy for the
+        // life of the process, found by the hash of the generated source, so
+        // creating a handle neither compiles, reads nor loads a module
+        static std::mutex lib_mu;
+        static std::map<uint64_t, cudaLibrary_t> libs;
+        cudaLibrary_t lib;
+        {
+            std::lock_guard<std::mutex> lk(lib_mu);
+            const uint64_t key = fnv1a(src);
+            auto it = libs.find(key);
+            if (it != libs.end()) lib = it->second;
+            else {
+                bool hit = false;
+                const std::string cubin = jitAngularCubin(src, &hit);
+                CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+                libs.emplace(key, lib);
+            }
+        }
+        k_ang_.assign(gh.size(), nullptr);
+        for (size_t g = 0; g < gh.size(); ++g) {
+            cudaKernel_t k;
+            CT_CUDA(cudaLibraryGetKernel(&k, lib, ("ct_ang_" + std::to_string(g)).c_str()));
+            k_ang_[g] = (void*)k;
+        }
     }
     // pack everything into one allocation
     auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
@@ -1278,11 +1502,20 @@ void Engine::pairPolarisations()
     const char* off = std::getenv("CTPWA_NO_POL_PAIRING");
     if (npair == 0 || nplane * npair > 32 || (off && *off && *off != '0')) return;
     const int nout = 2 * nplane * npair + 1;
-    unsigned long long* d_out = nullptr;
-    alloc(d_out, sizeof(unsigned long long) * nout);
     std::vector<double> worst(2 * nplane * npair, 0.0);
     double big = 0.0;
-    for (int k = 0; k < 3; ++k) {
+    if (d_pairmax_) {
+        // gathered by the generated angular kernels over all three samples
+        std::vector<unsigned long long> h(nout);
+        CT_CUDA(cudaMemcpyAsync(h.data(), d_pairmax_, sizeof(unsigned long long) * nout, cudaMemcpyDeviceToHost,
+                                init_stream_));
+        CT_CUDA(cudaStreamSynchronize(init_stream_));
+        for (int i = 0; i < 2 * nplane * npair; ++i) std::memcpy(&worst[i], &h[i], sizeof(double));
+        std::memcpy(&big, &h[2 * nplane * npair], sizeof(double));
+    }
+    unsigned long long* d_out = nullptr;
+    if (!d_pairmax_) alloc(d_out, sizeof(unsigned long long) * nout);
+    for (int k = 0; k < 3 && !d_pairmax_; ++k) {
         const DeviceSample& d = samples_[k];
         if (d.n <= 0) continue;
         CT_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * nout, init_stream_));
@@ -1374,6 +1607,18 @@ void Engine::computeAngular(int kind)
     AgTables T;
     std::memcpy(&T, ag_host_.data(), sizeof(T));
     for (size_t g = 0; g < group_desc_.size(); ++g) {
+        if (g < k_ang_.size() && k_ang_[g]) {
+            const double* p4 = d.p4;
+            double2* o64 = d.slamp64;
+            float2* o32 = d.slamp32;
+            double* kin = d.kin;
+            long long nn = n, lld = ld;
+            unsigned long long* pm = kind < 3 ? d_pairmax_ : nullptr;  // the phase-space truth sample is not checked
+            void* args[] = {(void*)&p4, (void*)&nn, (void*)&lld, (void*)&T, (void*)&o64, (void*)&o32, (void*)&kin,
+                            (void*)&pm};
+            CT_CUDA(cudaLaunchKernel(k_ang_[g], dim3((unsigned)((n + 127) / 128)), dim3(128), args, 0, init_stream_));
+            continue;
+        }
         AgGroup G;
         std::memcpy(&G, group_desc_[g].data(), sizeof(G));
         ag_group_kernel<<<(unsigned)((n + 127) / 128), 128, 0, init_stream_>>>(G, T, d.p4, n, ld, d.slamp64,
@@ -1493,8 +1738,8 @@ FusedShape fusedShape(const GeneratedModel& gen)
 }
 
 // NVRTC compile of one program (main source + named headers) for sm_100a, with
-// a disk cache keyed by the FNV-1a hash of the header texts, the options and
-// the NVRTC version.
+// a disk cache keyed by the FNV-1a hash of the main source, the header texts,
+// the options and the NVRTC version.
 std::string nvrtcCubin(const std::string& src, const std::vector<std::pair<std::string, std::string>>& headers,
                        const std::vector<std::string>& optv, const char* what, bool* cache_hit)
 {
@@ -1502,7 +1747,7 @@ std::string nvrtcCubin(const std::string& src, const std::vector<std::pair<std::
     for (const auto& o : optv) optp.push_back(o.c_str());
     const char* const* opts = optp.data();
     const int nopts = (int)optp.size();
-    std::string key_src;
+    std::string key_src = src;  // the main source too: the angular module's is the generated code
     for (const auto& h : headers) key_src += h.second;
     for (int i = 0; i < nopts; ++i) key_src += opts[i];
     int nvmaj = 0, nvmin = 0;
@@ -1641,6 +1886,22 @@ std::string jitGramCubin(const GeneratedModel& gen, bool paired, bool* cache_hit
                       optv, "Gram kernel", cache_hit);
 }
 
+// The generated angular kernels of one model (angularSource).
+std::string jitAngularCubin(const std::string& src, bool* cache_hit)
+{
+    std::string dir = kernelDir();
+    return nvrtcCubin(src, {{"angular_gen.cuh", readFile(dir + "/angular_gen.cuh")}}, kNvrtcBase, "angular kernel",
+                      cache_hit);
+}
+
+// CTPWA_ANGULAR_INTERP=1: the angular tables from the interpreter
+// (ag_group_kernel) instead of the generated kernels
+bool angularInterpreted()
+{
+    const char* e = std::getenv("CTPWA_ANGULAR_INTERP");
+    return e && *e && *e != '0';
+}
+
 void Engine::compileKernel()
 {
     auto t0 = std::chrono::steady_clock::now();
@@ -1714,6 +1975,19 @@ double precompileConfig(const std::string& config_path)
     bool hit = false;
     jitCubin(g, &hit);
     jitHvpCubin(g, false, &hit);
+    {
+        std::vector<AgNodeVar> vars;
+        std::vector<double> cg;
+        const std::vector<AgGroupHost> gh = angularGroups(m, g, vars, cg);
+        if (!gh.empty()) {
+            const std::string src = angularSource(gh, vars, g.nplane);
+            if (const char* out = std::getenv("CTPWA_MODEL_SOURCE_OUT"); out && *out) {
+                std::ofstream f(std::string(out) + ".angular.cu");
+                f << src;
+            }
+            jitAngularCubin(src, &hit);
+        }
+    }
     if (m.npol * 2 * m.nAmp() <= 128) {
         jitGramCubin(g, false, &hit);
         jitGramCubin(g, true, &hit);

@@ -190,6 +190,7 @@ public:
     int fusedGrid(int precision) const { return lay_[precision == kMixed ? 1 : 0].grid; }
     bool polPaired(int precision) const { return paired_[precision == kMixed ? 1 : 0]; }
     double jitSeconds() const { return jit_seconds_; }
+    const std::vector<std::pair<std::string, double>>& setupTimes() const { return setup_ms_; }
     bool jitCacheHit() const { return jit_cache_hit_; }
 
 private:
@@ -241,6 +242,14 @@ private:
     int gram_dsmem_ = 0;
     double* d_gpart_ = nullptr;
     void* k_evc_ = nullptr;  // ct_event_cache
+    std::vector<std::pair<std::string, double>> setup_ms_;  // set-up phases (host ms)
+    // generated angular kernels, one per angular group (empty: the
+    // interpreter ag_group_kernel runs instead); their module is shared
+    // process-wide
+    std::vector<void*> k_ang_;
+    // polarisation-pairing maxima accumulated by the generated angular
+    // kernels over the three samples (layout of ct_pair_check_kernel's output)
+    unsigned long long* d_pairmax_ = nullptr;
     double jit_seconds_ = 0.0;
     bool jit_cache_hit_ = false;
 

@@ -372,6 +372,12 @@ size_t ctpwa_device_bytes(const ctpwa_handle* h);
 /* Seconds spent compiling (or loading from the disk cache) the fused kernel. */
 double ctpwa_jit_seconds(const ctpwa_handle* h);
 
+/* Host milliseconds of the handle's set-up phases (model, context, kernels,
+ * samples, angular_tables, angular, pairing, buffers; each phase's device
+ * work finished), as "name=ms;name=ms" into buf (cap bytes, NUL-terminated).
+ * Returns the length the full text needs, including the NUL. */
+int ctpwa_setup_times(const ctpwa_handle* h, char* buf, size_t cap);
+
 /* Message of the last failure on this handle (or of the last failed create when h is NULL). */
 const char* ctpwa_last_error(const ctpwa_handle* h);
 
