@@ -37,6 +37,9 @@ def oracle_lib():
         lib.orc_pwa_amp.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
         lib.orc_clebsch.restype = ctypes.c_double
         lib.orc_clebsch.argtypes = [ctypes.c_int] * 6
+        lib.orc_small_d.restype = ctypes.c_double
+        lib.orc_small_d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        lib.orc_ylm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, _D]
         lib.orc_custom_eval.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _D, ctypes.c_char_p, ctypes.c_int]

@@ -885,6 +885,16 @@ void orc_pwa_amp(const double* p1, int dj1, const double* p2, int dj2, int dj, i
 
 double orc_clebsch(int dj1, int m1, int dj2, int m2, int dJ, int M) { return clebsch(dj1, m1, dj2, m2, dJ, M); }
 
+// Wigner small-d d^j_{m1 m2}(beta) (dim = 2j + 1, m doubled) and the
+// spherical harmonic Y_l^m(theta, phi) as (re, im) (pinning aids)
+double orc_small_d(int dim, int m1x2, int m2x2, double beta) { return smallD(dim, m1x2, m2x2, beta); }
+void orc_ylm(int l, int m, double theta, double phi, double* out2)
+{
+    const cplx y = sphericalY(l, m, theta, phi);
+    out2[0] = y.real();
+    out2[1] = y.imag();
+}
+
 // Custom expression: value and parameter derivatives (out = [Fr, Fi, dF0r, dF0i, ...]).
 int orc_custom_eval(const char* expr, const char* pnames_csv, const double* params, int P, double m, double q, int L,
                     double d, double md1, double md2, double* out, char* err, int errlen)

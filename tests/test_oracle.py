@@ -158,6 +158,41 @@ def test_custom_expression_nan_folding_matches_reference(ref, expr):
     ref.ref_aux_free(h)
 
 
+def test_wigner_small_d_is_orthogonal():
+    """d^j(beta) is a real orthogonal matrix for every j <= 3 (analytic
+    known answer): sum_m d^j_{m1 m}(b) d^j_{m2 m}(b) = delta_{m1 m2}, and
+    d^j(0) = 1."""
+    orc = oracle_lib()
+    for dim in range(1, 8):
+        ms = list(range(dim - 1, -dim, -2))
+        for beta in (0.0, 0.37, 1.2, 2.9):
+            d = np.array([[orc.orc_small_d(dim, a, b, beta) for b in ms] for a in ms])
+            assert np.max(np.abs(d @ d.T - np.eye(dim))) <= 1e-13, (dim, beta)
+            if beta == 0.0:
+                assert np.max(np.abs(d - np.eye(dim))) <= 1e-15
+
+
+def test_spherical_harmonics_are_orthonormal():
+    """Y_l^m orthonormal on the sphere for l <= 4 (analytic known answer),
+    by Gauss-Legendre quadrature in cos(theta) and the trapezoid rule in phi
+    (exact for these polynomials and trigonometric terms)."""
+    orc = oracle_lib()
+    x, wx = np.polynomial.legendre.leggauss(24)
+    nphi = 24
+    phis = 2 * np.pi * np.arange(nphi) / nphi
+    lm = [(l, m) for l in range(5) for m in range(-l, l + 1)]
+    Y = np.zeros((len(lm), x.size, nphi), dtype=complex)
+    out = np.zeros(2)
+    for i, (l, m) in enumerate(lm):
+        for a, c in enumerate(x):
+            for b, ph in enumerate(phis):
+                orc.orc_ylm(l, m, float(np.arccos(c)), float(ph), ptr(out))
+                Y[i, a, b] = out[0] + 1j * out[1]
+    w = wx[:, None] * (2 * np.pi / nphi)
+    G = np.einsum("iab,jab,ab->ij", np.conj(Y), Y, np.broadcast_to(w, Y.shape[1:]))
+    assert np.max(np.abs(G - np.eye(len(lm)))) <= 1e-12
+
+
 def test_barrier_and_breit_wigner_identities():
     """Bf(L, q0, q0) = 1 and |BWR(m0)| = 1/(m0 G0) (analytic known answers)."""
     orc = oracle_lib()
