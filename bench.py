@@ -658,7 +658,10 @@ def run_gpu(args, rank, world, local_rank):
 
         hess = {"n_params": nP}
         Hs = {}
-        for method in ("exact", "fd") if world == 1 else ("exact",):
+        # "gram": the coupling block from tensor-core Gram sums, the
+        # resonance rows exact (host-synchronising, so timed by the host
+        # clock around a device synchronisation as well as by events)
+        for method in ("exact", "fd", "gram") if world == 1 else ("exact",):
             hessian(method)
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -669,6 +672,12 @@ def run_gpu(args, rank, world, local_rank):
             hess[method + "_ms"] = max_over_ranks(e0.elapsed_time(e1))
         if "fd" in Hs:
             hess["fd_vs_exact_rel"] = float((Hs["fd"] - Hs["exact"]).abs().max() / Hs["exact"].abs().max())
+        if "gram" in Hs:
+            n2 = 2 * ana.getNVector()
+            He, Hg = Hs["exact"], Hs["gram"]
+            hess["gram_vs_exact_rel"] = float((Hg - He).abs().max() / He.abs().max())
+            hess["gram_vs_exact_coupling_block_rel"] = float((Hg[:n2, :n2] - He[:n2, :n2]).abs().max() /
+                                                             He[:n2, :n2].abs().max())
 
     if rank != 0:
         return 0

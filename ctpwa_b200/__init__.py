@@ -793,7 +793,11 @@ class analysis:
         method "exact" (default): forward-mode (dual-number) derivatives of the
         FP64 device gradient pass along every unit direction, symmetrised.
         method "fd": central differences of the exact FP64 device gradient with
-        steps rel_step * max(|p_i|, 1e-2)."""
+        steps rel_step * max(|p_i|, 1e-2).
+        method "gram": the coupling block from tensor-core Gram sums over the
+        samples (FP32 amplitudes, split-BF16 products, FP64 assembly; ~1e-6
+        relative to "exact"), the resonance-parameter rows exact; models with
+        (npol + 1) * 2 * nA <= 128."""
         p = self._check_params(params)
         H = torch.empty((self._np, self._np), dtype=torch.float64, device=p.device)
         stream = torch.cuda.current_stream(p.device).cuda_stream
@@ -801,8 +805,10 @@ class analysis:
             rc = self._lib.ctpwa_hessian_exact(self._h, p.data_ptr(), H.data_ptr(), ctypes.c_void_p(stream))
         elif method == "fd":
             rc = self._lib.ctpwa_hessian(self._h, p.data_ptr(), H.data_ptr(), float(rel_step), ctypes.c_void_p(stream))
+        elif method == "gram":
+            rc = self._lib.ctpwa_hessian_gram(self._h, p.data_ptr(), H.data_ptr(), ctypes.c_void_p(stream))
         else:
-            raise ValueError('method must be "exact" or "fd"')
+            raise ValueError('method must be "exact", "fd" or "gram"')
         if rc != 0:
             raise RuntimeError(_lib.error(self._h))
         return H

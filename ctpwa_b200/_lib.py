@@ -23,6 +23,7 @@ SIGNATURES = {
     "ctpwa_hessian": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                      ctypes.c_void_p]),
     "ctpwa_hessian_exact": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ctpwa_hessian_gram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_gram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_batch_create": (ctypes.c_void_p, [ctypes.c_int]),
     "ctpwa_batch_destroy": (None, [ctypes.c_void_p]),

@@ -940,6 +940,8 @@ Engine::~Engine()
     }
     devFree(d_ag_tables_);
     devFree(d_pairmax_);
+    devFree(d_ghpart_);
+    devFree(d_ghout_);
     devFree(d_v_);
     devFree(d_consts_);
     devFree(d_kblock_);
@@ -969,6 +971,7 @@ Engine::~Engine()
     }
     if (hvp_lib_) cudaLibraryUnload((cudaLibrary_t)hvp_lib_);
     if (gram_lib_) cudaLibraryUnload((cudaLibrary_t)gram_lib_);
+    if (gram_hess_lib_) cudaLibraryUnload((cudaLibrary_t)gram_hess_lib_);
     if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
 }
 
@@ -1873,11 +1876,12 @@ std::string jitHvpCubin(const GeneratedModel& gen, bool paired, bool* cache_hit)
 }
 
 // The tensor-core Gram kernels of one generated model (kernels/gram.cuh).
-std::string jitGramCubin(const GeneratedModel& gen, bool paired, bool* cache_hit)
+std::string jitGramCubin(const GeneratedModel& gen, bool paired, bool* cache_hit, bool hess = false)
 {
     std::string dir = kernelDir();
     std::vector<std::string> optv = kNvrtcBase;
     optv.push_back(std::string("-DCT_GRAM_PAIRED=") + (paired ? "1" : "0"));
+    if (hess) optv.push_back("-DCT_GRAM_HESS=1");
     return nvrtcCubin("#include \"gram.cuh\"\n",
                       {{"device_helpers.cuh", readFile(dir + "/device_helpers.cuh")},
                        {"fused_nll.cuh", readFile(dir + "/fused_nll.cuh")},
@@ -1991,6 +1995,10 @@ double precompileConfig(const std::string& config_path)
     if (m.npol * 2 * m.nAmp() <= 128) {
         jitGramCubin(g, false, &hit);
         jitGramCubin(g, true, &hit);
+    }
+    if ((m.npol + 1) * 2 * m.nAmp() <= 128) {
+        jitGramCubin(g, false, &hit, true);
+        jitGramCubin(g, true, &hit, true);
     }
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -2814,6 +2822,198 @@ void Engine::compileGram()
     alloc(d_gpart_, sizeof(double) * (size_t)gram_grid_ * rows * 2 * model_.nAmp());
     k_gram_ = (void*)kg;
     k_gram_fin_ = (void*)kf;
+}
+
+void Engine::compileGramHess()
+{
+    if (k_gramh_) return;
+    const int nA = model_.nAmp(), rows = (model_.npol + 1) * 2 * nA;
+    if (rows > 128)
+        throw std::length_error("the Gram-based Hessian supports (npol + 1) * 2 * nA <= 128; this model has " +
+                                std::to_string(rows));
+    if (!samples_[0].slamp32) throw std::runtime_error("the Gram needs the mixed-precision tables");
+    bool hit = false;
+    std::string cubin = jitGramCubin(gen_, paired_[1], &hit, true);
+    cudaLibrary_t lib;
+    CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+    gram_hess_lib_ = (void*)lib;
+    cudaKernel_t kg, kf;
+    CT_CUDA(cudaLibraryGetKernel(&kg, lib, "ct_gram"));
+    CT_CUDA(cudaLibraryGetKernel(&kf, lib, "ct_gram_hess_finalize"));
+    const int r8 = (rows + 7) / 8 * 8;
+    gramh_dsmem_ = (2 * r8 <= 128 ? 1 : 2) * 128 * 256 * 2 + 128 * 2 * nA * 8;
+    CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributeMaxDynamicSharedMemorySize, gramh_dsmem_));
+    int sms = 148;
+    CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    const int nn = 2 * r8 <= 128 ? 2 * r8 : (rows + 15) / 16 * 16;
+    int tcols = 32;
+    while (tcols < (nn <= 64 ? 4 : 2) * nn) tcols *= 2;
+    gramh_grid_ = sms * std::max(1, std::min({4, 512 / tcols, residentCtas((void*)kg, 256, gramh_dsmem_)}));
+    alloc(d_ghpart_, sizeof(double) * (size_t)gramh_grid_ * rows * 2 * nA);
+    alloc(d_ghout_, sizeof(double) * 2 * (2 * nA) * (2 * nA));
+    k_gramh_ = (void*)kg;
+    k_gramh_fin_ = (void*)kf;
+}
+
+// Hessian with the coupling block from tensor-core Gram sums (FP32
+// amplitudes, split-BF16 products, FP64 assembly): in the real couplings
+// z = [Re v; Im v], with per event f = z^T Q_e z, u_e = Q_e z,
+//   d2 (sum w log f) = 2 T1 - 4 T2,  T1 = sum (w / f) Q_e,  T2 = sum (w / f^2) u u^T,
+// over data (subtracted) and background (added), and for the normalisation
+// W_eff log pf with pf = z^T Qbar z (Qbar from the phase-space Gram),
+//   W_eff (2 Qbar / pf - 4 (Qbar z)(Qbar z)^T / pf^2);
+// mapped to the parameters by the linear coupling map v_a = r_a p_c(a).
+// The rows of the resonance parameters come from the exact FP64
+// Hessian-vector products along their unit directions. Host-synchronising.
+void Engine::hessianGram(const double* d_params, double* d_hess, cudaStream_t stream)
+{
+    compileGram();
+    compileGramHess();
+    compileHvp();
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta(), nP = m.nParams(), NA2 = 2 * nA;
+    std::vector<double> hp(nP);
+    CT_CUDA(cudaMemcpyAsync(hp.data(), d_params, sizeof(double) * nP, cudaMemcpyDeviceToHost, stream));
+    // the FP64 evaluation: phase-space factor and sample totals
+    nllGrad(d_params, d_hscratch_ + 3 * (size_t)nP, d_hscratch_, kFP64, stream);
+    double parts[6];
+    lastParts(parts, stream);
+    const double n_phsp = parts[5], pf_raw = n_phsp > 0 ? parts[2] / n_phsp : 0.0;
+    const double pf = (pf_raw <= 1e-30 || !std::isfinite(pf_raw)) ? 1e-30 : pf_raw;
+    const double weff = parts[3] - parts[4];
+    // phase-space Gram M = (1/W) sum w A conj(A)^T (complex [nA][nA])
+    double* d_M = d_ghout_;  // reused below for the weighted sums
+    std::vector<double> M(2 * nA * nA);
+    gram(d_params, d_M, stream);
+    CT_CUDA(cudaMemcpyAsync(M.data(), d_M, sizeof(double) * 2 * nA * nA, cudaMemcpyDeviceToHost, stream));
+    CT_CUDA(cudaStreamSynchronize(stream));
+    // weighted sums over data (kind 1) and background (kind 2); the constant
+    // block of this call is in place (gram() ran the prologue)
+    std::vector<double> S[3];
+    for (int kind = 1; kind <= 2; ++kind) {
+        const DeviceSample& d = samples_[kind];
+        S[kind].assign(2 * NA2 * NA2, 0.0);
+        if (d.n <= 0) continue;
+        CtGramArgsH g;
+        std::memset(&g, 0, sizeof(g));
+        g.slamp = d.slamp32;
+        g.evf = d.evf;
+        g.evd = d.evd;
+        g.w = d.w;
+        g.n = d.n;
+        g.ld = d.ld;
+        g.K = d_kblock_;
+        g.partials = d_ghpart_;
+        g.err = d_err_;
+        const int grid = (int)std::max(1LL, std::min<long long>((d.n + 255) / 256, gramh_grid_));
+        void* gargs[] = {&g};
+        CT_CUDA(cudaLaunchKernel(k_gramh_, dim3(grid), dim3(256), gargs, (size_t)gramh_dsmem_, stream));
+        int nb = grid;
+        void* fargs[] = {&d_ghpart_, &nb, &d_ghout_};
+        CT_CUDA(cudaLaunchKernel(k_gramh_fin_, dim3(1), dim3(256), fargs, 0, stream));
+        CT_CUDA(cudaMemcpyAsync(S[kind].data(), d_ghout_, sizeof(double) * 2 * NA2 * NA2, cudaMemcpyDeviceToHost,
+                                stream));
+        CT_CUDA(cudaStreamSynchronize(stream));
+    }
+    int herr = 0;
+    CT_CUDA(cudaMemcpy(&herr, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) throw std::runtime_error("the tensor-core Gram pipeline did not complete");
+    // couplings and z
+    std::vector<double> z(NA2);
+    for (int a = 0; a < nA; ++a) {
+        const int c = m.coupling.amp_chain[a];
+        const double r = m.coupling.ratio[a];
+        z[a] = r * hp[c];
+        z[nA + a] = r * hp[nc + c];
+    }
+    // the real symmetric form Q of a complex Hermitian K: [[Re K, Im K], [-Im K, Re K]]
+    auto Qof = [&](const std::vector<double>& reK, const std::vector<double>& imK) {
+        std::vector<double> Q(NA2 * NA2);
+        for (int a = 0; a < nA; ++a)
+            for (int b = 0; b < nA; ++b) {
+                Q[a * NA2 + b] = reK[a * nA + b];
+                Q[(nA + a) * NA2 + nA + b] = reK[a * nA + b];
+                Q[a * NA2 + nA + b] = imK[a * nA + b];
+                Q[(nA + a) * NA2 + b] = -imK[a * nA + b];
+            }
+        return Q;
+    };
+    std::vector<double> Hz(NA2 * NA2, 0.0);
+    for (int kind = 1; kind <= 2; ++kind) {
+        if (samples_[kind].n <= 0) continue;
+        const double* B = S[kind].data();           // sum of the amplitude blocks [Re; Im][Re; Im]^T
+        const double* C = S[kind].data() + NA2 * NA2;  // the c block
+        std::vector<double> reK(nA * nA), imK(nA * nA);
+        for (int a = 0; a < nA; ++a)
+            for (int b = 0; b < nA; ++b) {
+                reK[a * nA + b] = B[a * NA2 + b] + B[(nA + a) * NA2 + nA + b];
+                imK[a * nA + b] = B[(nA + a) * NA2 + b] - B[a * NA2 + nA + b];
+            }
+        const std::vector<double> T1 = Qof(reK, imK);
+        const double sgn = kind == 1 ? -1.0 : 1.0;  // NLL = -sum_data + sum_bkg
+        for (int i = 0; i < NA2; ++i)
+            for (int j = 0; j < NA2; ++j) {
+                // u u^T with u = [Re c; -Im c] from the [Re c; Im c] sums
+                const double flip = ((i < nA) != (j < nA)) ? -1.0 : 1.0;
+                const double T2 = flip * C[i * NA2 + j];
+                Hz[i * NA2 + j] += sgn * (2.0 * T1[i * NA2 + j] - 4.0 * T2);
+            }
+    }
+    {
+        const double wsum = samples_[0].wsum > 0 ? samples_[0].wsum : 1.0, scale = wsum / (n_phsp > 0 ? n_phsp : 1.0);
+        std::vector<double> reM(nA * nA), imM(nA * nA);
+        for (int i = 0; i < nA * nA; ++i) {
+            reM[i] = scale * M[2 * i];
+            imM[i] = scale * M[2 * i + 1];
+        }
+        const std::vector<double> Qb = Qof(reM, imM);
+        std::vector<double> qz(NA2, 0.0);
+        for (int i = 0; i < NA2; ++i)
+            for (int j = 0; j < NA2; ++j) qz[i] += Qb[i * NA2 + j] * z[j];
+        for (int i = 0; i < NA2; ++i)
+            for (int j = 0; j < NA2; ++j)
+                Hz[i * NA2 + j] += weff * (2.0 * Qb[i * NA2 + j] / pf - 4.0 * qz[i] * qz[j] / (pf * pf));
+    }
+    // symmetrised (the tensor-core sums of (i, j) and (j, i) round apart)
+    for (int i = 0; i < NA2; ++i)
+        for (int j = 0; j < i; ++j) {
+            const double v = 0.5 * (Hz[i * NA2 + j] + Hz[j * NA2 + i]);
+            Hz[i * NA2 + j] = Hz[j * NA2 + i] = v;
+        }
+    // the coupling block in the parameters, then the resonance rows
+    std::vector<double> H((size_t)nP * nP, 0.0);
+    auto zi = [&](int a, int part) { return part * nA + a; };
+    for (int a = 0; a < nA; ++a)
+        for (int b = 0; b < nA; ++b)
+            for (int pa = 0; pa < 2; ++pa)
+                for (int pb = 0; pb < 2; ++pb) {
+                    const int i = pa * nc + m.coupling.amp_chain[a], j = pb * nc + m.coupling.amp_chain[b];
+                    H[(size_t)i * nP + j] +=
+                        m.coupling.ratio[a] * m.coupling.ratio[b] * Hz[zi(a, pa) * NA2 + zi(b, pb)];
+                }
+    if (nT > 0) {
+        std::vector<double> dirs((size_t)nT * nP, 0.0);
+        for (int j = 0; j < nT; ++j) dirs[(size_t)j * nP + 2 * nc + j] = 1.0;
+        double* d_dirs = nullptr;
+        double* d_rows = nullptr;
+        CT_CUDA(cudaMallocAsync((void**)&d_dirs, sizeof(double) * dirs.size(), stream));
+        CT_CUDA(cudaMallocAsync((void**)&d_rows, sizeof(double) * dirs.size(), stream));
+        CT_CUDA(cudaMemcpyAsync(d_dirs, dirs.data(), sizeof(double) * dirs.size(), cudaMemcpyHostToDevice, stream));
+        hessianVectorProducts(d_params, d_dirs, nT, d_rows, stream);
+        std::vector<double> rows(dirs.size());
+        CT_CUDA(cudaMemcpyAsync(rows.data(), d_rows, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, stream));
+        CT_CUDA(cudaFreeAsync(d_dirs, stream));
+        CT_CUDA(cudaFreeAsync(d_rows, stream));
+        CT_CUDA(cudaStreamSynchronize(stream));
+        for (int j = 0; j < nT; ++j)
+            for (int i = 0; i < nP; ++i) {
+                const double v = rows[(size_t)j * nP + i];
+                H[(size_t)(2 * nc + j) * nP + i] = v;
+                H[(size_t)i * nP + 2 * nc + j] = v;
+            }
+    }
+    CT_CUDA(cudaMemcpyAsync(d_hess, H.data(), sizeof(double) * H.size(), cudaMemcpyHostToDevice, stream));
+    CT_CUDA(cudaStreamSynchronize(stream));
 }
 
 void Engine::gram(const double* d_params, double* d_out, cudaStream_t stream)

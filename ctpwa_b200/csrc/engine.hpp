@@ -127,6 +127,8 @@ public:
     // mixed-form amplitudes at d_params, on the tensor cores; d_out [nA][nA]
     // complex (re, im) FP64. The first call compiles the kernels.
     void gram(const double* d_params, double* d_out, cudaStream_t stream);
+    // Hessian with its coupling block from tensor-core Gram sums (host-synchronising)
+    void hessianGram(const double* d_params, double* d_hess, cudaStream_t stream);
     static constexpr size_t kStaticScratchBytes = size_t(2) << 20;
     // Event-sharded evaluation: the per-sample sums of this handle's events,
     // [3][nacc] + [n_phsp, W_phsp, W_data, W_bkg] (sumsSize() doubles), ready
@@ -235,6 +237,14 @@ private:
     const void* image_key_ = nullptr;
     // tensor-core Gram (compiled on the first request)
     void compileGram();
+    void compileGramHess();
+    void* gram_hess_lib_ = nullptr;
+    void* k_gramh_ = nullptr;
+    void* k_gramh_fin_ = nullptr;
+    int gramh_grid_ = 0;
+    int gramh_dsmem_ = 0;
+    double* d_ghpart_ = nullptr;
+    double* d_ghout_ = nullptr;
     void* gram_lib_ = nullptr;
     void* k_gram_ = nullptr;
     void* k_gram_fin_ = nullptr;

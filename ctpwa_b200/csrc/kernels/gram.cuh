@@ -40,8 +40,16 @@
 
 #define CT_GRAM_THREADS 256
 #define CT_GRAM_TILE 256  // events per tile (one per thread)
-#define CT_GRAM_ROWS (M_NPOL * 2 * M_NA)
-static_assert(CT_GRAM_ROWS <= 128, "the tensor-core Gram supports npol * 2 * nA <= 128");
+#ifndef CT_GRAM_HESS
+#define CT_GRAM_HESS 0
+#endif
+// CT_GRAM_HESS: the sums of the Hessian's coupling block over a data-like
+// sample instead of the normalisation matrix: the npol amplitude row blocks
+// scaled by sqrt(w / f_e), and one more block, c_a = sum_p A_pa conj(S_p)
+// (S_p = sum_a v_a A_pa, f_e = sum_p |S_p|^2), scaled by sqrt(w) / f_e
+#define CT_GRAM_BLOCKS (M_NPOL + CT_GRAM_HESS)
+#define CT_GRAM_ROWS (CT_GRAM_BLOCKS * 2 * M_NA)
+static_assert(CT_GRAM_ROWS <= 128, "the tensor-core Gram supports (npol + 1 for the Hessian sums) * 2 * nA <= 128");
 #define CT_GRAM_R8 ((CT_GRAM_ROWS + 7) / 8 * 8)
 #define CT_GRAM_STACK (2 * CT_GRAM_R8 <= 128)                 // hi and lo rows in one tile
 // MMA N (a multiple of 16 for M = 128)
@@ -172,15 +180,15 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS, 2) ct_gram(CtGramA
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         // ---- this thread's event -> operand column tid ----
         const long long e = tile * CT_GRAM_TILE + tid;
-        float x[M_NPOL * NA2];
+        float x[CT_GRAM_BLOCKS * NA2];
 #pragma unroll
-        for (int i = 0; i < M_NPOL * NA2; ++i) x[i] = 0.0f;
+        for (int i = 0; i < CT_GRAM_BLOCKS * NA2; ++i) x[i] = 0.0f;
         if (e < G.n) {
             CtEvent<float> ev;
             ev.load(G.evf + e, G.evd + e, G.ld);
             float Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
             ev.columns(G.K->c, G.K->ch, G.K->cl, Fr, Fi, dFr, dFi);
-            const float sw = G.w ? (float)sqrt(G.w[e]) : 1.0f;
+            const float sw = (G.w && !CT_GRAM_HESS) ? (float)sqrt(G.w[e]) : 1.0f;
 #pragma unroll
             for (int t = 0; t < M_NTERM; ++t) {
                 const int a = term_col(t);
@@ -197,6 +205,43 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS, 2) ct_gram(CtGramA
                     }
                 }
             }
+#if CT_GRAM_HESS
+            {
+                // S_p = sum_a v_a A_pa, f = sum_p |S_p|^2, c_a = sum_p A_pa conj(S_p)
+                float f = 0.0f, cr[M_NA], ci[M_NA];
+#pragma unroll
+                for (int a = 0; a < M_NA; ++a) cr[a] = ci[a] = 0.0f;
+#pragma unroll
+                for (int p = 0; p < M_NPOL; ++p) {
+                    float sr = 0.0f, si = 0.0f;
+#pragma unroll
+                    for (int a = 0; a < M_NA; ++a) {
+                        const float vr = G.K->vh[2 * a], vi = G.K->vh[2 * a + 1];
+                        const float ar = x[p * NA2 + a], ai = x[p * NA2 + M_NA + a];
+                        sr += vr * ar - vi * ai;
+                        si += vr * ai + vi * ar;
+                    }
+                    f += sr * sr + si * si;
+#pragma unroll
+                    for (int a = 0; a < M_NA; ++a) {
+                        const float ar = x[p * NA2 + a], ai = x[p * NA2 + M_NA + a];
+                        cr[a] += ar * sr + ai * si;
+                        ci[a] += ai * sr - ar * si;
+                    }
+                }
+                const double we = G.w ? G.w[e] : 1.0;
+                // an event with f = 0 (its log-likelihood is clamped) contributes no curvature
+                const float sa = f > 0.0f ? (float)sqrt(we / (double)f) : 0.0f;
+                const float sc = f > 0.0f ? (float)(sqrt(we) / (double)f) : 0.0f;
+#pragma unroll
+                for (int i = 0; i < M_NPOL * NA2; ++i) x[i] *= sa;
+#pragma unroll
+                for (int a = 0; a < M_NA; ++a) {
+                    x[M_NPOL * NA2 + a] = cr[a] * sc;
+                    x[M_NPOL * NA2 + M_NA + a] = ci[a] * sc;
+                }
+            }
+#endif
         }
         // hi and lo BF16 values, 8 rows (one core matrix) per 16-byte store
 #pragma unroll
@@ -302,6 +347,28 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS, 2) ct_gram(CtGramA
         out[i] = aborted ? 0.0 : v;
     }
 }
+
+#if CT_GRAM_HESS
+// Fixed-order sum of the CTA partials of the Hessian sums: out[0] = the
+// amplitude blocks summed over polarisations, out[1] = the c block, each the
+// real [2 nA][2 nA] matrix sum_e X X^T of its scaled rows [Re; Im].
+extern "C" __global__ void ct_gram_hess_finalize(const double* __restrict__ partials, int nblocks,
+                                                 double* __restrict__ out)
+{
+    constexpr int NA2 = 2 * M_NA;
+    for (int i = threadIdx.x; i < NA2 * NA2; i += blockDim.x) {
+        double g1 = 0.0, g2 = 0.0;
+        for (int c = 0; c < nblocks; ++c) {
+            const double* P = partials + (size_t)c * CT_GRAM_ROWS * NA2;
+#pragma unroll 1
+            for (int p = 0; p < M_NPOL; ++p) g1 += P[(size_t)p * NA2 * NA2 + i];
+            g2 += P[(size_t)M_NPOL * NA2 * NA2 + i];
+        }
+        out[i] = g1;
+        out[NA2 * NA2 + i] = g2;
+    }
+}
+#endif
 
 // Fixed-order sum of the CTA partials into the complex Gram (reference
 // orientation M_ab = sum A_a conj(A_b)), scaled by 1/W: out [nA][nA][2].

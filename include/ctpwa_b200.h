@@ -139,6 +139,18 @@ int ctpwa_hessian(ctpwa_handle* h, const double* d_params, double* d_hess, doubl
  * later calls are queued on the stream without host synchronisation. */
 int ctpwa_hessian_exact(ctpwa_handle* h, const double* d_params, double* d_hess, void* stream);
 
+/* The Hessian (same layout as ctpwa_hessian_exact) with its coupling block
+ * formed from tensor-core Gram sums: over data and background the sums
+ * sum (w/f) A_a conj(A_b) and sum (w/f^2) c_a conj(c_b) (c_a = sum_pol
+ * A_a conj(S)), over phase space the normalisation matrix, in FP32
+ * amplitudes with split-BF16 products and FP64 assembly (~1e-6 relative to
+ * the exact Hessian); the resonance-parameter rows from the exact FP64
+ * Hessian-vector products along their unit directions. The reference builds
+ * its Hessian from Gram products of the stored amplitudes
+ * (src/ComputeHessian.cu:149-1556). Host-synchronising; needs
+ * (npol + 1) * 2 * nA <= 128 (CTPWA_ERR_ARG otherwise). */
+int ctpwa_hessian_gram(ctpwa_handle* h, const double* d_params, double* d_hess, void* stream);
+
 /* Replaces: the phase-space normalisation matrix of the reference, built by
  * scalePhspAmpsKernel + CGEMM over its amplitude table
  * (src/ComputeHessian.cu:1181-1197, src/Analysis.cu:729-805; used by its
