@@ -364,7 +364,11 @@ def gram_timing(ana, p0, device, reps=20):
     useful = 8.0 * nA * nA * npol * n_p
     peaks = measured_peaks() or {}
     peak = float(peaks.get("bf16_tflops") or 1590.0)
-    return {"ms": ms, "phsp_events": n_p, "n_amplitudes": nA, "npol": npol,
+    shape = (ctypes.c_int * 4)()
+    launch = None
+    if ana._lib.ctpwa_gram_shape(ana._h, shape) == 0:
+        launch = {"grid": shape[0], "dyn_smem": shape[1], "resident_ctas_per_sm": shape[2], "block": shape[3]}
+    return {"ms": ms, "phsp_events": n_p, "n_amplitudes": nA, "npol": npol, "launch": launch,
             "tensor_tflops_executed": executed / (ms * 1e-3) / 1e12,
             "tensor_frac_of_bf16_peak": executed / (ms * 1e-3) / 1e12 / peak,
             "useful_gflop": useful / 1e9, "executed_gflop": executed / 1e9,

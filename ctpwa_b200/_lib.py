@@ -24,6 +24,7 @@ SIGNATURES = {
                                      ctypes.c_void_p]),
     "ctpwa_hessian_exact": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_hessian_gram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ctpwa_gram_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "ctpwa_gram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_batch_create": (ctypes.c_void_p, [ctypes.c_int]),
     "ctpwa_batch_destroy": (None, [ctypes.c_void_p]),

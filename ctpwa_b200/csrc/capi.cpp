@@ -227,6 +227,19 @@ int ctpwa_hessian_gram(ctpwa_handle* h, const double* d_params, double* d_hess, 
     return CTPWA_OK;
 }
 
+int ctpwa_gram_shape(ctpwa_handle* h, int* out4)
+{
+    if (!h || !out4) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    try {
+        h->eng->gramShape(out4);
+    } catch (const std::length_error& e) {
+        return setErr(h, CTPWA_ERR_ARG, e.what());
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_gram(ctpwa_handle* h, const double* d_params, double* d_out, void* stream)
 {
     if (!h || !d_params || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");

@@ -2810,13 +2810,18 @@ void Engine::compileGram()
     const int r8 = (rows + 7) / 8 * 8;
     gram_dsmem_ = (2 * r8 <= 128 ? 1 : 2) * 128 * 256 * 2 + 128 * 2 * model_.nAmp() * 8;
     CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributeMaxDynamicSharedMemorySize, gram_dsmem_));
+    // the whole unified L1 as shared memory: two CTAs of ~80 KB per SM (the
+    // occupancy query answered one with the default carveout)
+    CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
     int sms = 148;
     CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
     // tensor-memory columns per CTA (CT_GRAM_TMEM_COLS): NACC accumulators of N columns
     const int nn = 2 * r8 <= 128 ? 2 * r8 : (rows + 15) / 16 * 16;
     int tcols = 32;
     while (tcols < (nn <= 64 ? 4 : 2) * nn) tcols *= 2;
-    const int occ = std::max(1, std::min({4, 512 / tcols, residentCtas((void*)kg, 256, gram_dsmem_)}));
+    gram_resident_ = residentCtas((void*)kg, 256, gram_dsmem_);
+    const int occ = std::max(1, std::min({4, 512 / tcols, gram_resident_}));
     const long long ntiles = (samples_[0].n + 255) / 256;
     gram_grid_ = (int)std::max(1LL, std::min<long long>(ntiles, (long long)sms * occ));
     alloc(d_gpart_, sizeof(double) * (size_t)gram_grid_ * rows * 2 * model_.nAmp());
@@ -2843,6 +2848,8 @@ void Engine::compileGramHess()
     const int r8 = (rows + 7) / 8 * 8;
     gramh_dsmem_ = (2 * r8 <= 128 ? 1 : 2) * 128 * 256 * 2 + 128 * 2 * nA * 8;
     CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributeMaxDynamicSharedMemorySize, gramh_dsmem_));
+    CT_CUDA(cudaFuncSetAttribute((const void*)kg, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
     int sms = 148;
     CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
     const int nn = 2 * r8 <= 128 ? 2 * r8 : (rows + 15) / 16 * 16;
@@ -3014,6 +3021,15 @@ void Engine::hessianGram(const double* d_params, double* d_hess, cudaStream_t st
     }
     CT_CUDA(cudaMemcpyAsync(d_hess, H.data(), sizeof(double) * H.size(), cudaMemcpyHostToDevice, stream));
     CT_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Engine::gramShape(int* out4)
+{
+    compileGram();
+    out4[0] = gram_grid_;
+    out4[1] = gram_dsmem_;
+    out4[2] = gram_resident_;
+    out4[3] = 256;
 }
 
 void Engine::gram(const double* d_params, double* d_out, cudaStream_t stream)

@@ -127,6 +127,8 @@ public:
     // mixed-form amplitudes at d_params, on the tensor cores; d_out [nA][nA]
     // complex (re, im) FP64. The first call compiles the kernels.
     void gram(const double* d_params, double* d_out, cudaStream_t stream);
+    // Gram launch: grid, dynamic shared memory, resident CTAs per SM, block (compiles it if needed)
+    void gramShape(int* out4);
     // Hessian with its coupling block from tensor-core Gram sums (host-synchronising)
     void hessianGram(const double* d_params, double* d_hess, cudaStream_t stream);
     static constexpr size_t kStaticScratchBytes = size_t(2) << 20;
@@ -250,6 +252,7 @@ private:
     void* k_gram_fin_ = nullptr;
     int gram_grid_ = 0;
     int gram_dsmem_ = 0;
+    int gram_resident_ = 0;  // CTAs per SM from the occupancy query
     double* d_gpart_ = nullptr;
     void* k_evc_ = nullptr;  // ct_event_cache
     std::vector<std::pair<std::string, double>> setup_ms_;  // set-up phases (host ms)

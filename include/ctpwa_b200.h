@@ -151,6 +151,11 @@ int ctpwa_hessian_exact(ctpwa_handle* h, const double* d_params, double* d_hess,
  * (npol + 1) * 2 * nA <= 128 (CTPWA_ERR_ARG otherwise). */
 int ctpwa_hessian_gram(ctpwa_handle* h, const double* d_params, double* d_hess, void* stream);
 
+/* Launch shape of the tensor-core Gram kernel (compiled on first use):
+ * out4 = {grid, dynamic shared memory bytes, resident CTAs per SM from the
+ * occupancy query, threads per CTA}. No counterpart in the reference. */
+int ctpwa_gram_shape(ctpwa_handle* h, int* out4);
+
 /* Replaces: the phase-space normalisation matrix of the reference, built by
  * scalePhspAmpsKernel + CGEMM over its amplitude table
  * (src/ComputeHessian.cu:1181-1197, src/Analysis.cu:729-805; used by its
