@@ -2789,6 +2789,33 @@ struct CtGramArgsH {
     int pad;
 };
 
+// Resident CTAs per SM of a Gram kernel from the limits the hardware
+// applies: shared memory (dynamic + static + the per-CTA reservation, with
+// the whole unified L1 as shared memory), registers, threads. The occupancy
+// query on the library kernel handle answered 1 where these give 2 (ncu:
+// occupancy limits 2 by shared memory and 2 by registers at 79.9 KB and 127
+// registers).
+int gramResidentCtas(void* kernel, int block, int dsmem, int device)
+{
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, (const void*)kernel) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    int smem_sm = 0, reserved = 0, regs_sm = 65536, thr_sm = 2048;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device);
+    cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device);
+    cudaGetLastError();
+    const long long per_cta_smem = (long long)dsmem + (long long)fa.sharedSizeBytes + reserved;
+    const int by_smem = per_cta_smem > 0 ? (int)(smem_sm / per_cta_smem) : 32;
+    const int regs = (fa.numRegs + 7) / 8 * 8;  // per-thread allocation granularity
+    const int by_regs = regs > 0 ? regs_sm / (regs * block) : 32;
+    const int by_thr = thr_sm / block;
+    return std::max(1, std::min({by_smem, by_regs, by_thr}));
+}
+
 void Engine::compileGram()
 {
     if (k_gram_) return;
@@ -2820,7 +2847,7 @@ void Engine::compileGram()
     const int nn = 2 * r8 <= 128 ? 2 * r8 : (rows + 15) / 16 * 16;
     int tcols = 32;
     while (tcols < (nn <= 64 ? 4 : 2) * nn) tcols *= 2;
-    gram_resident_ = residentCtas((void*)kg, 256, gram_dsmem_);
+    gram_resident_ = gramResidentCtas((void*)kg, 256, gram_dsmem_, opt_.device);
     const int occ = std::max(1, std::min({4, 512 / tcols, gram_resident_}));
     const long long ntiles = (samples_[0].n + 255) / 256;
     gram_grid_ = (int)std::max(1LL, std::min<long long>(ntiles, (long long)sms * occ));
@@ -2855,7 +2882,7 @@ void Engine::compileGramHess()
     const int nn = 2 * r8 <= 128 ? 2 * r8 : (rows + 15) / 16 * 16;
     int tcols = 32;
     while (tcols < (nn <= 64 ? 4 : 2) * nn) tcols *= 2;
-    gramh_grid_ = sms * std::max(1, std::min({4, 512 / tcols, residentCtas((void*)kg, 256, gramh_dsmem_)}));
+    gramh_grid_ = sms * std::max(1, std::min({4, 512 / tcols, gramResidentCtas((void*)kg, 256, gramh_dsmem_, opt_.device)}));
     alloc(d_ghpart_, sizeof(double) * (size_t)gramh_grid_ * rows * 2 * nA);
     alloc(d_ghout_, sizeof(double) * 2 * (2 * nA) * (2 * nA));
     k_gramh_ = (void*)kg;
