@@ -528,6 +528,9 @@ struct FinalizeArgs {
     // set when a fused kernel's staged copy did not arrive: the evaluation is
     // invalid and reported like a non-finite NLL (loss 1e30, zero gradient)
     const int* err;
+    // 1 for sums of the mixed form, which evaluates at the couplings rounded
+    // to FP32 (v_h): the loss gets the first-order term of v - v_h
+    int vshift;
 };
 
 // Per-sample sums of the partial rows plus the sample totals (event-sharded
@@ -605,6 +608,16 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
         double i = Dd[3 + 2 * a] - B[3 + 2 * a] + (Weff / pf) * (P[3 + 2 * a] * gv_phsp_scale);
         gv[2 * a] = reset ? 0.0 : r;
         gv[2 * a + 1] = reset ? 0.0 : i;
+    }
+    if (A.vshift && !reset) {
+        // the mixed form's sums are at v_h = FP32(v): add dL/dRe v . (v - v_h)
+        // + dL/dIm v . (v - v_h) with dL/dRe v_a = 2 Re g_a, dL/dIm v_a = 2 Im g_a
+        double corr = 0.0;
+        for (int a = 0; a < A.nA; ++a) {
+            const double vr = A.v[2 * a], vi = A.v[2 * a + 1];
+            corr += 2.0 * (gv[2 * a] * (vr - (double)(float)vr) + gv[2 * a + 1] * (vi - (double)(float)vi));
+        }
+        loss += corr;
     }
     for (int c = 0; c < A.nc; ++c) {
         double sr = 0.0, si = 0.0;
@@ -2101,6 +2114,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     f.out_grad = d_grad;
     f.out_parts = d_parts_;
     f.err = d_err_;
+    f.vshift = precision == kMixed ? 1 : 0;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
@@ -2219,6 +2233,7 @@ void Engine::nllGradMulti(const std::vector<Engine*>& es, const std::vector<cons
         f.out_grad = d_grad[j];
         f.out_parts = e->d_parts_;
         f.err = e->d_err_;
+        f.vshift = pr;
         shm_max = std::max(shm_max, (int)(sizeof(double) * (3 * f.nacc + 2 * nA + 8)));
         total += lay.grid;
     }
@@ -2370,6 +2385,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     f.out_grad = d_grad;
     f.out_parts = s_parts;
     f.err = (const int*)(base + off_err);
+    f.vshift = precision == kMixed ? 1 : 0;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
@@ -2377,6 +2393,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
 
 void Engine::shardSums(const double* d_params, int precision, double* d_sums, cudaStream_t stream)
 {
+    sums_mixed_ = precision == kMixed;
     const CtaLayout& lay = lay_[precision == kMixed ? 1 : 0];
     const Model& m = model_;
     const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
@@ -2452,6 +2469,7 @@ void Engine::finalizeSums(const double* d_params, const double* d_sums, double* 
     f.out_grad = d_grad;
     f.out_parts = d_parts_;
     f.sums = d_sums;
+    f.vshift = sums_mixed_ ? 1 : 0;
     f.err = d_err_;
     size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);

@@ -276,6 +276,9 @@ private:
     double* d_parts_ = nullptr;     // [8]
     double* d_hscratch_ = nullptr;  // finite-difference Hessian: perturbed params, two gradients, nll [3 nP + 1]
     int* d_err_ = nullptr;          // set by a fused kernel whose staged copy did not arrive
+    // the precision of the last shardSums: finalizeSums applies the mixed
+    // form's first-order coupling term to sums of the mixed form
+    bool sums_mixed_ = false;
     int* d_amp_chain_ = nullptr;
     double* d_ratio_ = nullptr;
     int* d_gauss_idx_ = nullptr;

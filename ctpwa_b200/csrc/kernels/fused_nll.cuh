@@ -120,7 +120,7 @@ struct CtConsts {
     double c[CT_NCONST_ALLOC];
     double v[2 * M_NA];
     float ch[CT_NCONST_ALLOC], cl[CT_NCONST_ALLOC];
-    float vh[2 * M_NA], vl[2 * M_NA];
+    float vh[2 * M_NA];  // the couplings rounded to FP32 (the mixed form's; see ct_fused_body)
 };
 __constant__ CtConsts ct_k;
 
@@ -153,7 +153,6 @@ __device__ __forceinline__ void ct_prologue_body(const CtArgs& A)
         const float h = (float)v;
         K->v[i] = v;
         K->vh[i] = h;
-        K->vl[i] = (float)(v - (double)h);
     }
 }
 
@@ -345,14 +344,6 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         if constexpr (MULTI) return sizeof(L) == 4 ? (L)__ldg(Kg->vh + 2 * a + 1) : (L)__ldg(Kg->v + 2 * a + 1);
         return sizeof(L) == 4 ? (L)ct_k.vh[2 * a + 1] : (L)ct_k.v[2 * a + 1];
     };
-    auto vrl = [&](int a) -> L {
-        if constexpr (MULTI) return (L)__ldg(Kg->vl + 2 * a);
-        return (L)ct_k.vl[2 * a];
-    };
-    auto vil = [&](int a) -> L {
-        if constexpr (MULTI) return (L)__ldg(Kg->vl + 2 * a + 1);
-        return (L)ct_k.vl[2 * a + 1];
-    };
 
     // all per-event work: ap / bp / slp point at this event's frontier values
     // (table type, FP64) and angular values, consecutive values `ks` / `ss`
@@ -378,16 +369,15 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         for (int t = 0; t < M_NTERM; ++t) {
             const int a = term_col(t);
             if constexpr (sizeof(L) == 4) {
-                // Each product of a per-event value with a coupling is rounded
-                // once, from the full-precision coupling (hi + lo): rounding the
-                // product with the FP32 coupling alone would bias the sample
-                // mean by ~1e-9 (both factors on the FP32 grid), which the
-                // normalisation term multiplies by the data weight sum.
-                // (the lo products first, then each hi product fused into
-                // the running sum: every rounding is of a sum that holds the
-                // full-precision coupling's products)
-                cr[t] = fmaf(Fr[t], vr(a), fmaf(-Fi[t], vi(a), fmaf(Fr[t], vrl(a), -Fi[t] * vil(a))));
-                ci[t] = fmaf(Fi[t], vr(a), fmaf(Fr[t], vi(a), fmaf(Fi[t], vrl(a), Fr[t] * vil(a))));
+                // The mixed form evaluates the NLL at the couplings rounded
+                // to FP32, v_h; the finalize step adds the first-order term
+                // 2 sum_a Re(conj(g_a) (v_a - v_h,a)) (g = dNLL/d conj(v),
+                // which this pass sums), so the result is the NLL at v to
+                // second order (~|H| |v - v_h|^2, 1e-12). The products of the
+                // per-event values with the fixed v_h are rounded without
+                // bias (the per-event factor makes the low bits random).
+                cr[t] = fmaf(Fr[t], vr(a), -Fi[t] * vi(a));
+                ci[t] = fmaf(Fi[t], vr(a), Fr[t] * vi(a));
             } else {
                 cr[t] = (R)(vr(a) * Fr[t] - vi(a) * Fi[t]);
                 ci[t] = (R)(vr(a) * Fi[t] + vi(a) * Fr[t]);

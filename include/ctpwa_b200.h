@@ -224,7 +224,10 @@ int ctpwa_export_weights(ctpwa_handle* h, const double* d_params, const int* wav
  * then [n_phsp, W_phsp, W_data, W_bkg]); the caller sums these buffers over
  * the shards (one all-reduce) and ctpwa_finalize_sums turns the total into
  * the NLL and gradient of the union of the shards. Device pointers,
- * stream-ordered, no host synchronisation. */
+ * stream-ordered, no host synchronisation. ctpwa_finalize_sums takes the sums
+ * to be of the precision of this handle's last ctpwa_shard_sums call: sums
+ * of the mixed form, which is evaluated at the couplings rounded to FP32,
+ * get the first-order term of the rounding added to the NLL. */
 int ctpwa_sums_size(const ctpwa_handle* h);
 int ctpwa_shard_sums(ctpwa_handle* h, const double* d_params, int precision, double* d_sums, void* stream);
 int ctpwa_finalize_sums(ctpwa_handle* h, const double* d_params, const double* d_sums, double* d_nll, double* d_grad,
