@@ -378,9 +378,19 @@ def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2, timi
     lap("phsp")
     gen = torch.Generator(device=dev)
     gen.manual_seed(6001 + seed)
-    chunks, have, batch = [], 0, 0
+    # The first batch has 12 candidates per event; each later one is sized
+    # from the acceptance measured so far (15 % margin) but holds no more
+    # candidates than the first, so the device memory a caller reserves for
+    # the first batch bounds every batch. (A fixed 12x per missing event
+    # took ~15 batches, each with its own handle, on a model accepting 1/28.)
+    chunks, have, batch, tried = [], 0, 0, 0
+    cap = int(n_data * 12) + 10_000
     while have < n_data:
-        ncand = int((n_data - have) * 12) + 10_000
+        if batch == 0:
+            ncand = cap
+        else:
+            acc = max(have, 1) / tried
+            ncand = min(cap, int(1.15 * (n_data - have) / acc) + 10_000)
         cand = toymc.phase_space_device(M_JPSI, masses, ncand, 5001 + seed + 7919 * batch, device=device)
         lap("candidates")
         ana = analysis.from_device(str(cfg), tiny, cand, device=device)
@@ -392,6 +402,7 @@ def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2, timi
         lap("select")
         chunks.append(sel)
         have += sel.shape[0]
+        tried += ncand
         batch += 1
     data = torch.cat(chunks)[:n_data].contiguous()
     return str(cfg), phsp, data
