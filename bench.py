@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-toy-fit", action="store_true", help="skip the toy-fit serving stream")
     ap.add_argument("--no-hessian", action="store_true", help="skip the full-size Hessian timing")
     ap.add_argument("--no-gram", action="store_true", help="skip the tensor-core Gram timing")
+    ap.add_argument("--no-norm-cache", action="store_true",
+                    help="skip the timing of evaluations at fixed resonance parameters from the normalisation cache")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build on a sample of the workload")
     ap.add_argument("--no-fit-precision", action="store_true", help="skip the mixed-vs-FP64 fit comparison")
@@ -374,6 +376,57 @@ def gram_timing(ana, p0, device, reps=20):
             "useful_gflop": useful / 1e9, "executed_gflop": executed / 1e9,
             "operands": "BF16 hi + lo split (%s), M=128 N=%d K=16, FP32 TMEM accumulation per 256-event tile, "
                         "FP64 across tiles" % ("hi|lo rows stacked in one operand" if stacked else "4 MMA passes", N)}
+
+
+def norm_cache_timing(ana, p0, device, reps=50):
+    """Evaluations at fixed resonance parameters from the normalisation cache
+    (ctpwa_norm_cache_build, ctpwa_nll_grad_cached): device time of the
+    FP64 matrices' phase-space pass, device time per cached evaluation with
+    the couplings changed every call (FP64 and mixed; CUDA events around
+    `reps` back-to-back calls through the C ABI), and the cached FP64 result
+    against the full pass at one such point."""
+    import ctypes
+
+    import torch
+
+    nV, nP = ana.getNVector(), ana.getNParams()
+    pt = torch.tensor(p0, dtype=torch.float64, device=device)
+    ana.cacheNormalisation(pt)  # first call: loads or compiles the kernels
+    build_ms = ana.cacheNormalisation(pt)
+    rng = np.random.default_rng(7)
+    qs = []
+    for _ in range(reps):
+        q = np.array(p0, dtype=np.float64)
+        q[1:nV] *= 1 + 0.05 * rng.standard_normal(nV - 1)
+        q[nV + 1:2 * nV] += 0.05 * rng.standard_normal(nV - 1)
+        qs.append(torch.tensor(q, dtype=torch.float64, device=device))
+    nll = torch.empty((), dtype=torch.float64, device=device)
+    grad = torch.empty(nP, dtype=torch.float64, device=device)
+    stream = torch.cuda.current_stream(device)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    out = {"build_ms": build_ms, "phsp_events": ana.getNEvents()[0],
+           "evaluation": "data and background pass + quadratic forms of the FP64 matrices (no phase-space read)"}
+    for prec, code in (("fp64", 0), ("mixed", 1)):
+        for q in qs[:3]:
+            assert ana._lib.ctpwa_nll_grad_cached(ana._h, q.data_ptr(), nll.data_ptr(), grad.data_ptr(), code, sp) == 0
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for q in qs:
+            ana._lib.ctpwa_nll_grad_cached(ana._h, q.data_ptr(), nll.data_ptr(), grad.data_ptr(), code, sp)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1) / reps
+        out[prec + "_ms_per_eval"] = ms
+        out[prec + "_evals_per_s"] = 1e3 / ms
+    n1, g1 = ana.getNLLAndGrad(qs[0], "fp64", cached=True)
+    n0, g0 = ana.getNLLAndGrad(qs[0], "fp64")
+    out["fp64_cached_vs_full_rel_nll"] = abs(float(n1) - float(n0)) / abs(float(n0))
+    out["fp64_cached_vs_full_rel_grad"] = float((g1 - g0).abs().max() / g0.abs().max())
+    nm, _ = ana.getNLLAndGrad(qs[0], "mixed", cached=True)
+    out["mixed_cached_abs_dnll_vs_fp64"] = abs(float(nm) - float(n0))
+    ana.clearNormalisationCache()
+    return out
 
 
 def reference_cuda_timing(args, device, reps=10):
@@ -739,6 +792,8 @@ def run_gpu(args, rank, world, local_rank):
         line["hessian"] = hess
     if world == 1 and not args.no_gram:
         line["gram"] = gram_timing(ana, p0, dev)
+    if world == 1 and not args.no_norm_cache:
+        line["norm_cache"] = norm_cache_timing(ana, p0, dev)
     if world == 1 and not args.no_toy_fit:
         line["toy_fit"] = toy_fit(args, local_rank)
     if world == 1 and not args.no_fit_precision:

@@ -381,14 +381,14 @@ class analysis:
             raise RuntimeError(f"params size mismatch: got {params.numel()}, expected {self._np}")
         return params.detach().contiguous()
 
-    def _eval(self, params: torch.Tensor, precision=None):
+    def _eval(self, params: torch.Tensor, precision=None, cached=False):
         p = self._check_params(params)
         nll = torch.empty((), dtype=torch.float64, device=p.device)
         grad = torch.empty_like(p)
         stream = torch.cuda.current_stream(p.device).cuda_stream
         prec = self._precision if precision is None else self._parse_precision(precision)
-        rc = self._lib.ctpwa_nll_grad(self._h, p.data_ptr(), nll.data_ptr(), grad.data_ptr(), prec,
-                                      ctypes.c_void_p(stream))
+        fn = self._lib.ctpwa_nll_grad_cached if cached else self._lib.ctpwa_nll_grad
+        rc = fn(self._h, p.data_ptr(), nll.data_ptr(), grad.data_ptr(), prec, ctypes.c_void_p(stream))
         if rc != 0:
             raise RuntimeError(_lib.error(self._h))
         return nll, grad
@@ -398,9 +398,37 @@ class analysis:
         self._check_params(params)
         return _NLLFunction.apply(params, self)
 
-    def getNLLAndGrad(self, params: torch.Tensor, precision=None):
-        """(nll, grad) without autograd bookkeeping."""
-        return self._eval(params, precision)
+    def getNLLAndGrad(self, params: torch.Tensor, precision=None, cached=False):
+        """(nll, grad) without autograd bookkeeping. cached=True: from the
+        normalisation cache (cacheNormalisation), which must have been built
+        at the same resonance parameters; the phase-space sample is not read."""
+        return self._eval(params, precision, cached)
+
+    def cacheNormalisation(self, params: torch.Tensor) -> float:
+        """Build the normalisation cache at the resonance parameters of
+        `params`: the phase-space sums as FP64 quadratic forms in the
+        couplings, with the lineshape derivatives (the reference keeps its
+        phase-space matrix between evaluations when no resonance parameter is
+        free, src/Analysis.cu:748-829). Afterwards host-buffer evaluations
+        (getNLLHost, fit, fitNewton) at these resonance parameters, and
+        getNLLAndGrad(cached=True), read only the data and background samples.
+        The fits build the cache themselves when no resonance parameter is
+        free. Returns the device time of the phase-space pass in ms."""
+        p = self._check_params(params)
+        ms = ctypes.c_double()
+        stream = torch.cuda.current_stream(p.device).cuda_stream
+        if self._lib.ctpwa_norm_cache_build(self._h, p.data_ptr(), ctypes.byref(ms), ctypes.c_void_p(stream)) != 0:
+            raise RuntimeError(_lib.error(self._h))
+        return ms.value
+
+    def clearNormalisationCache(self):
+        """Drop the normalisation cache (every evaluation takes the full pass again)."""
+        self._check()
+        self._lib.ctpwa_norm_cache_clear(self._h)
+
+    def hasNormalisationCache(self) -> bool:
+        self._check()
+        return bool(self._lib.ctpwa_norm_cache_valid(self._h))
 
     def getNLLHost(self, params, precision=None):
         """Evaluate from host memory through the C ABI's host-buffer entry point."""

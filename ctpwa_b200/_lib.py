@@ -26,6 +26,12 @@ SIGNATURES = {
     "ctpwa_hessian_gram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ctpwa_gram_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "ctpwa_gram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ctpwa_norm_cache_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.c_void_p]),
+    "ctpwa_norm_cache_clear": (ctypes.c_int, [ctypes.c_void_p]),
+    "ctpwa_norm_cache_valid": (ctypes.c_int, [ctypes.c_void_p]),
+    "ctpwa_nll_grad_cached": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int, ctypes.c_void_p]),
     "ctpwa_batch_create": (ctypes.c_void_p, [ctypes.c_int]),
     "ctpwa_batch_destroy": (None, [ctypes.c_void_p]),
     "ctpwa_nll_grad_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,

@@ -41,6 +41,29 @@ int setErr(ctpwa_handle* h, int code, const std::string& m)
     return code;
 }
 
+// A fit none of whose resonance parameters can move (free[i] == 0 or
+// lo[i] == hi[i] for each): its evaluations can all use one normalisation cache.
+bool thetaFixed(const ctpwa_handle* h, const unsigned char* free_mask, const double* lo, const double* hi)
+{
+    const int np = h->eng->nParams(), off = 2 * h->eng->model().nVector();
+    for (int i = off; i < np; ++i)
+        if (free_mask[i] && lo[i] != hi[i]) return false;
+    return true;
+}
+
+// the normalisation cache at the resonance parameters of the host array x
+// (built unless it already matches them)
+void ensureNormCache(ctpwa_handle* h, const double* x, void* stream)
+{
+    if (h->eng->normCacheMatches(x)) return;
+    const int np = h->eng->nParams();
+    cudaStream_t s = (cudaStream_t)stream;
+    std::memcpy(h->h_pin, x, sizeof(double) * np);
+    if (cudaMemcpyAsync(h->d_params, h->h_pin, sizeof(double) * np, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        throw std::runtime_error("CUDA error: host-to-device copy failed");
+    h->eng->normCacheBuild(h->d_params, s);
+}
+
 int copyOut(const std::string& s, char* buf, size_t cap)
 {
     if (buf && cap > 0) {
@@ -253,6 +276,44 @@ int ctpwa_gram(ctpwa_handle* h, const double* d_params, double* d_out, void* str
     return CTPWA_OK;
 }
 
+int ctpwa_norm_cache_build(ctpwa_handle* h, const double* d_params, double* ms, void* stream)
+{
+    if (!h || !d_params) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    try {
+        const double t = h->eng->normCacheBuild(d_params, (cudaStream_t)stream);
+        if (ms) *ms = t;
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
+int ctpwa_norm_cache_clear(ctpwa_handle* h)
+{
+    if (!h) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    h->eng->normCacheClear();
+    return CTPWA_OK;
+}
+
+int ctpwa_norm_cache_valid(const ctpwa_handle* h)
+{
+    return h && h->eng->normCacheValid() ? 1 : 0;
+}
+
+int ctpwa_nll_grad_cached(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision,
+                          void* stream)
+{
+    if (!h || !d_params || !d_nll || !d_grad) return setErr(h, CTPWA_ERR_ARG, "null argument");
+    if (precision != CTPWA_FP64 && precision != CTPWA_MIXED) return setErr(h, CTPWA_ERR_ARG, "precision must be 0 or 1");
+    if (!h->eng->normCacheValid()) return setErr(h, CTPWA_ERR_ARG, "no normalisation cache: build it first");
+    try {
+        h->eng->nllGradCached(d_params, d_nll, d_grad, precision, (cudaStream_t)stream);
+    } catch (const std::exception& e) {
+        return setErr(h, CTPWA_ERR_CUDA, e.what());
+    }
+    return CTPWA_OK;
+}
+
 int ctpwa_hvp(ctpwa_handle* h, const double* d_params, const double* d_dirs, int ndir, double* d_out, void* stream)
 {
     if (!h || !d_params || !d_dirs || !d_out) return setErr(h, CTPWA_ERR_ARG, "null argument");
@@ -367,7 +428,9 @@ int ctpwa_nll_grad_host(ctpwa_handle* h, const double* params, double* nll, doub
         std::memcpy(h->h_pin, params, sizeof(double) * np);
         if (cudaMemcpyAsync(h->d_params, h->h_pin, sizeof(double) * np, cudaMemcpyHostToDevice, s) != cudaSuccess)
             throw std::runtime_error("CUDA error: host-to-device copy failed");
-        int rc = ctpwa_nll_grad(h, h->d_params, h->d_out, h->d_out + 1, precision, stream);
+        // points at the cached resonance parameters: from the normalisation cache
+        int rc = h->eng->normCacheMatches(params) ? ctpwa_nll_grad_cached(h, h->d_params, h->d_out, h->d_out + 1, precision, stream)
+                                                  : ctpwa_nll_grad(h, h->d_params, h->d_out, h->d_out + 1, precision, stream);
         if (rc != CTPWA_OK) return rc;
         if (cudaMemcpyAsync(h->h_pin + np, h->d_out, sizeof(double) * (1 + np), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
@@ -625,8 +688,16 @@ int ctpwa_fit(ctpwa_handle* h, double* params, const unsigned char* free_mask, c
     opt.ftol = ftol;
     opt.gtol = gtol;
     int ne = 0;
+    const bool fixed = thetaFixed(h, free_mask, lo, hi);
     auto fg = [&](const double* x, double* f, double* g) -> int {
         const auto t0 = std::chrono::steady_clock::now();
+        if (fixed) {
+            try {
+                ensureNormCache(h, x, stream);
+            } catch (const std::exception& e) {
+                return setErr(h, CTPWA_ERR_CUDA, e.what());
+            }
+        }
         const int rc = ctpwa_nll_grad_host(h, x, f, g, precision, stream);
         if (eval_ms && ne < max_evals)
             eval_ms[ne] = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -660,7 +731,15 @@ int ctpwa_fit_newton(ctpwa_handle* h, double* params, const unsigned char* free_
     } catch (const std::exception& e) {
         return setErr(h, CTPWA_ERR_CUDA, e.what());
     }
+    const bool fixed = thetaFixed(h, free_mask, lo, hi);
     auto fg = [&](const double* x, double* f, double* g) -> int {
+        if (fixed) {
+            try {
+                ensureNormCache(h, x, stream);
+            } catch (const std::exception& e) {
+                return setErr(h, CTPWA_ERR_CUDA, e.what());
+            }
+        }
         return ctpwa_nll_grad_host(h, x, f, g, precision, stream);
     };
     // the exact FP64 Hessian at x (both precisions: the mixed form keeps its

@@ -1043,6 +1043,7 @@ std::string Gen::emit()
         for (const auto& d : cols[a].der) der_entries.push_back({(int)a, d.first});
     const int k = (int)der_entries.size();
     out.nder = k;
+    out.nterm = (int)cols.size();
     out.nconst = ncon;
     std::ostringstream h;
     auto table = [&](const char* name, const std::vector<int>& v) {

@@ -31,6 +31,7 @@ struct GeneratedModel {
     int ngrad = 0;               // gradient sums per thread: 2 nA + nTheta
     std::vector<int> group_plane0;
     int nder = 0;
+    int nterm = 0;               // lineshape terms (one per amplitude column, more with identical particles)
     int nconst = 0;              // parameter-only subexpressions kept per call
     // per-event frontier tables (parameter-independent values the per-call
     // code reads): FP64 table rows; mixed form FP32 and FP64 rows

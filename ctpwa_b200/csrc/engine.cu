@@ -531,6 +531,9 @@ struct FinalizeArgs {
     // 1 for sums of the mixed form, which evaluates at the couplings rounded
     // to FP32 (v_h): the loss gets the first-order term of v - v_h
     int vshift;
+    // cached normalisation: the phase-space row of sums (ct_norm_row)
+    // replaces the phase-space CTAs' partial rows
+    const double* phsp_row;
 };
 
 // Per-sample sums of the partial rows plus the sample totals (event-sharded
@@ -561,8 +564,24 @@ __global__ void __launch_bounds__(1024) ct_rowsum_kernel(const double* __restric
 // dL/dp_c = (1/p_c) sum_{a in c} conj(g_a) v_a (src/AmpGen.cu:3581-3637).
 __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
 {
-    extern __shared__ double sh[];  // [3][nacc] sample sums, then gv [2 nA], gt [nT]
+    // [3][nacc] sample sums, gv [2 nA] (+ 8 spare), then the inputs of the
+    // serial assembly staged by all threads (thread 0 reads no global
+    // memory): couplings [2 nA], parameters [2 nc + nT], coupling chain
+    // [nA], Gaussian constraints [3 ngauss] (ct_finalize_shm)
+    extern __shared__ double sh[];
     double* sums = sh;
+    double* sv = sh + 3 * A.nacc + 2 * A.nA + 8;
+    double* sp = sv + 2 * A.nA;
+    double* sch = sp + 2 * A.nc + A.nT;
+    double* sg = sch + A.nA;
+    for (int i = threadIdx.x; i < 2 * A.nA; i += blockDim.x) sv[i] = A.v[i];
+    for (int i = threadIdx.x; i < 2 * A.nc + A.nT; i += blockDim.x) sp[i] = A.params[i];
+    for (int i = threadIdx.x; i < A.nA; i += blockDim.x) sch[i] = (double)A.chain[i];
+    for (int i = threadIdx.x; i < A.ngauss; i += blockDim.x) {
+        sg[3 * i] = (double)A.gauss_idx[i];
+        sg[3 * i + 1] = A.gauss_ms[2 * i];
+        sg[3 * i + 2] = A.gauss_ms[2 * i + 1];
+    }
     // one warp per (sample, column): lanes stride over the CTA rows, then a
     // fixed-order shuffle tree, so the sums are bit-reproducible
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
@@ -578,6 +597,10 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
         for (int i = warp; i < 3 * A.nacc; i += nwarp) {
             int k = i / A.nacc, j = i % A.nacc;
             double s = 0.0;
+            if (k == 0 && A.phsp_row) {
+                if (lane == 0) sums[i] = A.phsp_row[j];
+                continue;
+            }
             if (A.has[k])
                 for (int b = lane; b < A.cta[k][1]; b += 32) s += A.partials[(long long)(A.cta[k][0] + b) * A.nacc + j];
 #pragma unroll
@@ -595,10 +618,10 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
     double Weff = W_data - W_bkg;
     double loss = Dd[0] - B[0] + Weff * log(pf);
     if (A.err && *A.err) loss = nan("");
-    const double* theta = A.params + 2 * A.nc;
+    const double* theta = sp + 2 * A.nc;
     for (int g = 0; g < A.ngauss; ++g) {
-        double dl = theta[A.gauss_idx[g]] - A.gauss_ms[2 * g];
-        loss += dl * dl / (2.0 * A.gauss_ms[2 * g + 1] * A.gauss_ms[2 * g + 1]);
+        double dl = theta[(int)sg[3 * g]] - sg[3 * g + 1];
+        loss += dl * dl / (2.0 * sg[3 * g + 2] * sg[3 * g + 2]);
     }
     bool reset = isnan(loss) || isinf(loss);
     if (reset) loss = 1e30;
@@ -614,7 +637,7 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
         // + dL/dIm v . (v - v_h) with dL/dRe v_a = 2 Re g_a, dL/dIm v_a = 2 Im g_a
         double corr = 0.0;
         for (int a = 0; a < A.nA; ++a) {
-            const double vr = A.v[2 * a], vi = A.v[2 * a + 1];
+            const double vr = sv[2 * a], vi = sv[2 * a + 1];
             corr += 2.0 * (gv[2 * a] * (vr - (double)(float)vr) + gv[2 * a + 1] * (vi - (double)(float)vi));
         }
         loss += corr;
@@ -622,12 +645,12 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
     for (int c = 0; c < A.nc; ++c) {
         double sr = 0.0, si = 0.0;
         for (int a = 0; a < A.nA; ++a) {
-            if (A.chain[a] != c) continue;
-            double gr = gv[2 * a], gi = gv[2 * a + 1], vr = A.v[2 * a], vi = A.v[2 * a + 1];
+            if ((int)sch[a] != c) continue;
+            double gr = gv[2 * a], gi = gv[2 * a + 1], vr = sv[2 * a], vi = sv[2 * a + 1];
             sr += gr * vr + gi * vi;
             si += gr * vi - gi * vr;
         }
-        double pr = A.params[c], pi = A.params[A.nc + c];
+        double pr = sp[c], pi = sp[A.nc + c];
         double ps = pr * pr + pi * pi;
         if (ps < 1e-30) ps = 1e-30;
         A.out_grad[c] = 2.0 * (sr * pr + si * pi) / ps;
@@ -639,8 +662,8 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
     }
     if (!reset)
         for (int g = 0; g < A.ngauss; ++g) {
-            int j = A.gauss_idx[g];
-            A.out_grad[2 * A.nc + j] += (theta[j] - A.gauss_ms[2 * g]) / (A.gauss_ms[2 * g + 1] * A.gauss_ms[2 * g + 1]);
+            int j = (int)sg[3 * g];
+            A.out_grad[2 * A.nc + j] += (theta[j] - sg[3 * g + 1]) / (sg[3 * g + 2] * sg[3 * g + 2]);
         }
     *A.out_nll = loss;
     if (A.out_parts) {
@@ -654,6 +677,12 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
 }
 
 __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A) { ct_finalize_body(A); }
+
+// dynamic shared memory of a finalize launch (layout in ct_finalize_body)
+size_t ct_finalize_shm(const FinalizeArgs& f)
+{
+    return sizeof(double) * (3 * (size_t)f.nacc + 4 * (size_t)f.nA + 8 + 2 * (size_t)f.nc + f.nT + f.nA + 3 * (size_t)f.ngauss);
+}
 
 // one CTA per job of a multi-job evaluation (all jobs of one model: same shared-memory size)
 __global__ void __launch_bounds__(1024) ct_finalize_multi_kernel(const FinalizeArgs* __restrict__ fs)
@@ -799,13 +828,14 @@ int Engine::residentCtas(void* kernel, int block, int dsmem) const
 }
 
 // Split `target` CTAs over the samples in proportion to their event counts
-// (at least one CTA per non-empty sample, at most one per `block` events).
-void Engine::layoutCtas(int target, long long tot, int block, CtaLayout& lay) const
+// (at least one CTA per non-empty sample, at most one per `block` events);
+// no_phsp: over the data and background samples only.
+void Engine::layoutCtas(int target, long long tot, int block, CtaLayout& lay, bool no_phsp) const
 {
     long long want[3] = {0, 0, 0}, maxc[3] = {0, 0, 0};
     long long sum = 0;
     for (int k = 0; k < 3; ++k) {
-        if (samples_[k].n <= 0) continue;
+        if (samples_[k].n <= 0 || (no_phsp && k == 0)) continue;
         maxc[k] = (samples_[k].n + block - 1) / block;
         want[k] = std::max(1LL, std::min(maxc[k], (long long)std::floor((double)target * samples_[k].n / std::max(1LL, tot))));
         sum += want[k];
@@ -923,6 +953,8 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
         int occ = residentCtas(pr == 0 ? k_f64_ : k_mixed_, shape_.block[pr], shape_.dsmem[pr]);
         layoutCtas(sms * occ, tot, shape_.block[pr], lay_[pr]);
         maxgrid = std::max(maxgrid, lay_[pr].grid);
+        layoutCtas(sms * occ, samples_[1].n + samples_[2].n, shape_.block[pr], lay_data_[pr], true);
+        maxgrid = std::max(maxgrid, lay_data_[pr].grid);
     }
     grid_max_ = maxgrid;
     int nacc = 2 + 2 * nA + model_.nTheta();
@@ -978,6 +1010,10 @@ Engine::~Engine()
     devFree(d_hvsums_);
     devFree(d_htsums_);
     devFree(d_gpart_);
+    devFree(d_npart_);
+    devFree(d_nmat_);
+    devFree(d_ntheta_);
+    devFree(d_nrow_);
     if (mem_stream_) {
         cudaStreamSynchronize(mem_stream_);
         cudaStreamDestroy(mem_stream_);
@@ -985,6 +1021,7 @@ Engine::~Engine()
     if (hvp_lib_) cudaLibraryUnload((cudaLibrary_t)hvp_lib_);
     if (gram_lib_) cudaLibraryUnload((cudaLibrary_t)gram_lib_);
     if (gram_hess_lib_) cudaLibraryUnload((cudaLibrary_t)gram_hess_lib_);
+    if (norm_lib_) cudaLibraryUnload((cudaLibrary_t)norm_lib_);
     if (lib_) cudaLibraryUnload((cudaLibrary_t)lib_);
 }
 
@@ -1903,6 +1940,18 @@ std::string jitGramCubin(const GeneratedModel& gen, bool paired, bool* cache_hit
                       optv, "Gram kernel", cache_hit);
 }
 
+// The normalisation-cache kernels of one model (kernels/norm.cuh).
+std::string jitNormCubin(const GeneratedModel& gen, bool* cache_hit)
+{
+    std::string dir = kernelDir();
+    return nvrtcCubin("#include \"norm.cuh\"\n",
+                      {{"device_helpers.cuh", readFile(dir + "/device_helpers.cuh")},
+                       {"fused_nll.cuh", readFile(dir + "/fused_nll.cuh")},
+                       {"norm.cuh", readFile(dir + "/norm.cuh")},
+                       {"model.cuh", gen.header}},
+                      kNvrtcBase, "normalisation kernel", cache_hit);
+}
+
 // The generated angular kernels of one model (angularSource).
 std::string jitAngularCubin(const std::string& src, bool* cache_hit)
 {
@@ -1992,6 +2041,7 @@ double precompileConfig(const std::string& config_path)
     bool hit = false;
     jitCubin(g, &hit);
     jitHvpCubin(g, false, &hit);
+    jitNormCubin(g, &hit);
     {
         std::vector<AgNodeVar> vars;
         std::vector<double> cg;
@@ -2115,7 +2165,7 @@ void Engine::nllGrad(const double* d_params, double* d_nll, double* d_grad, int 
     f.out_parts = d_parts_;
     f.err = d_err_;
     f.vshift = precision == kMixed ? 1 : 0;
-    size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
+    size_t shm = ct_finalize_shm(f);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
 }
@@ -2234,7 +2284,7 @@ void Engine::nllGradMulti(const std::vector<Engine*>& es, const std::vector<cons
         f.out_parts = e->d_parts_;
         f.err = e->d_err_;
         f.vshift = pr;
-        shm_max = std::max(shm_max, (int)(sizeof(double) * (3 * f.nacc + 2 * nA + 8)));
+        shm_max = std::max(shm_max, (int)ct_finalize_shm(f));
         total += lay.grid;
     }
     hoff[nj] = total;
@@ -2386,7 +2436,7 @@ void Engine::nllGradStatic(const double* d_params, double* d_nll, double* d_grad
     f.out_parts = s_parts;
     f.err = (const int*)(base + off_err);
     f.vshift = precision == kMixed ? 1 : 0;
-    size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
+    size_t shm = ct_finalize_shm(f);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
 }
@@ -2471,7 +2521,7 @@ void Engine::finalizeSums(const double* d_params, const double* d_sums, double* 
     f.sums = d_sums;
     f.vshift = sums_mixed_ ? 1 : 0;
     f.err = d_err_;
-    size_t shm = sizeof(double) * (3 * f.nacc + 2 * nA + 8);
+    size_t shm = ct_finalize_shm(f);
     ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
     CT_CUDA(cudaGetLastError());
 }
@@ -3066,6 +3116,221 @@ void Engine::hessianGram(const double* d_params, double* d_hess, cudaStream_t st
     }
     CT_CUDA(cudaMemcpyAsync(d_hess, H.data(), sizeof(double) * H.size(), cudaMemcpyHostToDevice, stream));
     CT_CUDA(cudaStreamSynchronize(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Normalisation cache (kernels/norm.cuh): the phase-space sums as FP64
+// quadratic forms in the couplings at fixed resonance parameters.
+// ---------------------------------------------------------------------------
+// argument blocks of ct_norm_build and ct_norm_row (must match kernels/norm.cuh)
+struct CtNormArgsH {
+    const void* slamp;
+    const double* ev;
+    const double* w;
+    long long n, ld;
+    const double* consts;
+    double* partials;
+    int ne;
+    int pad;
+};
+struct CtNormRowArgsH {
+    const double* mat;
+    int weighted;
+    int use_vh;
+    const double* v;
+    double vw_scale;
+    const double* theta;
+    const double* theta_cached;
+    int* err;
+    int pad;
+    double* row;
+};
+
+void Engine::compileNorm()
+{
+    if (k_norm_build_) return;
+    const int nt = gen_.nterm, nd = gen_.nder, ng = gen_.nplane * (gen_.nplane + 1) / 2;
+    const int nu = nt * (nt + 1) / 2;
+    norm_ne_ = nu + nd * nt + (samples_[0].w ? nu : 0);
+    bool hit = false;
+    std::string cubin = jitNormCubin(gen_, &hit);
+    cudaLibrary_t lib;
+    CT_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+    norm_lib_ = (void*)lib;
+    cudaKernel_t kb, kr, kw;
+    CT_CUDA(cudaLibraryGetKernel(&kb, lib, "ct_norm_build"));
+    CT_CUDA(cudaLibraryGetKernel(&kr, lib, "ct_norm_reduce"));
+    CT_CUDA(cudaLibraryGetKernel(&kw, lib, "ct_norm_row"));
+    // one record of (terms + derivatives + plane pairs + weight) double2
+    // slots per event of a 128-event tile, the record length made odd
+    const int rec = (nt + nd + ng + 1) | 1;
+    norm_dsmem_ = 128 * rec * 16;
+    CT_CUDA(cudaFuncSetAttribute((const void*)kb, cudaFuncAttributeMaxDynamicSharedMemorySize, norm_dsmem_));
+    CT_CUDA(cudaFuncSetAttribute((const void*)kb, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
+    int sms = 148;
+    CT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    const int occ = gramResidentCtas((void*)kb, 128, norm_dsmem_, opt_.device);
+    const long long ntiles = (samples_[0].n + 127) / 128;
+    norm_grid_ = (int)std::max(1LL, std::min<long long>(ntiles, (long long)sms * occ));
+    alloc(d_npart_, sizeof(double) * 2 * (size_t)norm_grid_ * norm_ne_);
+    alloc(d_nmat_, sizeof(double) * 2 * (size_t)norm_ne_);
+    alloc(d_ntheta_, sizeof(double) * std::max(1, model_.nTheta()));
+    alloc(d_nrow_, sizeof(double) * (2 + 2 * model_.nAmp() + model_.nTheta()));
+    k_norm_build_ = (void*)kb;
+    k_norm_red_ = (void*)kr;
+    k_norm_row_ = (void*)kw;
+}
+
+double Engine::normCacheBuild(const double* d_params, cudaStream_t stream)
+{
+    compileNorm();
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    norm_valid_ = false;
+    // the parameter-only subexpressions at this theta
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, nullptr);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH pa;
+    std::memset(&pa, 0, sizeof(pa));
+    pa.theta = d_params + 2 * nc;
+    pa.v = d_v_;
+    pa.consts = d_consts_;
+    void* pargs[] = {&pa};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), pargs, 0, stream));
+    const DeviceSample& d = samples_[0];
+    CtNormArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    a.slamp = d.slamp64;
+    a.ev = d.ev64;
+    a.w = d.w;
+    a.n = d.n;
+    a.ld = d.ld;
+    a.consts = d_consts_;
+    a.partials = d_npart_;
+    a.ne = norm_ne_;
+    cudaEvent_t e0, e1;
+    CT_CUDA(cudaEventCreate(&e0));
+    CT_CUDA(cudaEventCreate(&e1));
+    CT_CUDA(cudaEventRecord(e0, stream));
+    void* args[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_norm_build_, dim3(norm_grid_), dim3(128), args, (size_t)norm_dsmem_, stream));
+    CT_CUDA(cudaEventRecord(e1, stream));
+    int rows = norm_grid_, ne = norm_ne_;
+    double* part = d_npart_;
+    double* mat = d_nmat_;
+    void* rargs[] = {&part, &rows, &ne, &mat};
+    CT_CUDA(cudaLaunchKernel(k_norm_red_, dim3(1), dim3(256), rargs, 0, stream));
+    if (nT > 0)
+        CT_CUDA(cudaMemcpyAsync(d_ntheta_, d_params + 2 * nc, sizeof(double) * nT, cudaMemcpyDeviceToDevice, stream));
+    norm_theta_.assign(nT, 0.0);
+    if (nT > 0)
+        CT_CUDA(cudaMemcpyAsync(norm_theta_.data(), d_params + 2 * nc, sizeof(double) * nT, cudaMemcpyDeviceToHost,
+                                stream));
+    CT_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0.0f;
+    CT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    norm_valid_ = true;
+    return (double)ms;
+}
+
+bool Engine::normCacheMatches(const double* params) const
+{
+    if (!norm_valid_) return false;
+    const int nT = model_.nTheta(), off = 2 * model_.nVector();
+    return nT == 0 || std::memcmp(params + off, norm_theta_.data(), sizeof(double) * nT) == 0;
+}
+
+// The evaluation at the cached resonance parameters: the fused pass over the
+// data and background samples (their own one-wave layout), the phase-space
+// row from the matrices, the usual finalize.
+void Engine::nllGradCached(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream)
+{
+    if (!norm_valid_) throw std::runtime_error("no normalisation cache: build it first");
+    const CtaLayout& lay = lay_data_[precision == kMixed ? 1 : 0];
+    const Model& m = model_;
+    const int nA = m.nAmp(), nc = m.nVector(), nT = m.nTheta();
+    ct_prepare_kernel<<<(nA + 127) / 128, 128, 0, stream>>>(d_params, d_amp_chain_, d_ratio_, nA, nc, d_v_, d_err_);
+    CT_CUDA(cudaGetLastError());
+    CtArgsH a;
+    std::memset(&a, 0, sizeof(a));
+    int ns = 0;
+    for (int k = 1; k < 3; ++k) {
+        if (lay.cta[k][1] == 0) continue;
+        CtSampleH& sm = a.s[ns++];
+        const DeviceSample& d = samples_[k];
+        sm.slamp = precision == kMixed ? (const void*)d.slamp32 : (paired_[0] ? (const void*)d.slamp64p : (const void*)d.slamp64);
+        sm.ev = precision == kMixed ? (const void*)d.evf : (const void*)d.ev64;
+        sm.evd = precision == kMixed ? d.evd : nullptr;
+        sm.w = d.w;
+        sm.n = d.n;
+        sm.ld = d.ld;
+        sm.kind = k;
+        sm.cta_begin = lay.cta[k][0];
+        sm.cta_count = lay.cta[k][1];
+        sm.vw_scale = 1.0;
+    }
+    a.nsamp = ns;
+    a.theta = d_params + 2 * nc;
+    a.v = d_v_;
+    a.partials = d_partials_;
+    a.consts = d_consts_;
+    a.err = d_err_;
+    a.kblock = d_kblock_;
+    if (precision == kMixed && !samples_[1].slamp32) throw std::runtime_error("mixed-precision tables were not built");
+    void* args[] = {&a};
+    CT_CUDA(cudaLaunchKernel(k_pro_, dim3(1), dim3(32), args, 0, stream));
+    CT_CUDA(cudaMemcpyAsync(k_sym_, d_kblock_, k_sym_bytes_, cudaMemcpyDeviceToDevice, stream));
+    a.cta_base = 0;
+    if (ns > 0)
+        CT_CUDA(cudaLaunchKernel(precision == kMixed ? k_mixed_ : k_f64_, dim3(lay.grid),
+                                 dim3(shape_.block[precision == kMixed]), args, (size_t)shape_.dsmem[precision == kMixed],
+                                 stream));
+    CtNormRowArgsH r;
+    std::memset(&r, 0, sizeof(r));
+    r.mat = d_nmat_;
+    r.weighted = samples_[0].w ? 1 : 0;
+    r.use_vh = precision == kMixed ? 1 : 0;
+    r.v = d_v_;
+    r.vw_scale = 1.0 / (samples_[0].wsum > 0 ? samples_[0].wsum : 1.0);
+    r.theta = d_params + 2 * nc;
+    r.theta_cached = d_ntheta_;
+    r.err = d_err_;
+    r.row = d_nrow_;
+    void* rargs[] = {&r};
+    CT_CUDA(cudaLaunchKernel(k_norm_row_, dim3(1), dim3(256), rargs, 0, stream));  // CT_NORM_ROW_THREADS
+    FinalizeArgs f;
+    std::memset(&f, 0, sizeof(f));
+    f.partials = d_partials_;
+    f.nacc = 2 + 2 * nA + nT;
+    f.nA = nA;
+    f.nc = nc;
+    f.nT = nT;
+    for (int k = 0; k < 3; ++k) {
+        f.cta[k][0] = lay.cta[k][0];
+        f.cta[k][1] = lay.cta[k][1];
+        f.has[k] = lay.cta[k][1] > 0;
+    }
+    f.n_phsp = (double)samples_[0].n;
+    f.W_data = samples_[1].wsum;
+    f.W_bkg = has_bkg_ ? samples_[2].wsum : 0.0;
+    f.params = d_params;
+    f.v = d_v_;
+    f.chain = d_amp_chain_;
+    f.gauss_idx = d_gauss_idx_;
+    f.gauss_ms = d_gauss_ms_;
+    f.ngauss = (int)m.gauss.size();
+    f.out_nll = d_nll;
+    f.out_grad = d_grad;
+    f.out_parts = d_parts_;
+    f.err = d_err_;
+    f.vshift = precision == kMixed ? 1 : 0;
+    f.phsp_row = d_nrow_;
+    size_t shm = ct_finalize_shm(f);
+    ct_finalize_kernel<<<1, 1024, shm, stream>>>(f);
+    CT_CUDA(cudaGetLastError());
 }
 
 void Engine::gramShape(int* out4)

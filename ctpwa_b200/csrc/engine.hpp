@@ -131,6 +131,20 @@ public:
     void gramShape(int* out4);
     // Hessian with its coupling block from tensor-core Gram sums (host-synchronising)
     void hessianGram(const double* d_params, double* d_hess, cudaStream_t stream);
+    // Normalisation cache (kernels/norm.cuh): the phase-space sums as FP64
+    // quadratic forms in the couplings at the resonance parameters of
+    // d_params. normCacheBuild computes them (one pass over the phase-space
+    // sample; host-synchronising; returns the pass's device time in ms);
+    // nllGradCached then evaluates at any couplings with those resonance
+    // parameters from the data and background samples and the matrices
+    // alone. Its resonance parameters must equal the cached ones bitwise; if
+    // not, the evaluation is flagged invalid (NLL 1e30, zero gradient).
+    double normCacheBuild(const double* d_params, cudaStream_t stream);
+    void normCacheClear() { norm_valid_ = false; }
+    bool normCacheValid() const { return norm_valid_; }
+    // true when the cache is valid for the resonance parameters of the host array params
+    bool normCacheMatches(const double* params) const;
+    void nllGradCached(const double* d_params, double* d_nll, double* d_grad, int precision, cudaStream_t stream);
     static constexpr size_t kStaticScratchBytes = size_t(2) << 20;
     // Event-sharded evaluation: the per-sample sums of this handle's events,
     // [3][nacc] + [n_phsp, W_phsp, W_data, W_bkg] (sumsSize() doubles), ready
@@ -254,6 +268,21 @@ private:
     int gram_dsmem_ = 0;
     int gram_resident_ = 0;  // CTAs per SM from the occupancy query
     double* d_gpart_ = nullptr;
+    // normalisation cache (compiled and allocated on the first build)
+    void compileNorm();
+    void* norm_lib_ = nullptr;
+    void* k_norm_build_ = nullptr;
+    void* k_norm_red_ = nullptr;
+    void* k_norm_row_ = nullptr;
+    int norm_grid_ = 0;
+    int norm_dsmem_ = 0;
+    int norm_ne_ = 0;                   // complex entries: Mu, D (and Mw for a weighted sample)
+    double* d_npart_ = nullptr;         // [norm_grid_][norm_ne_][2]
+    double* d_nmat_ = nullptr;          // [norm_ne_][2]
+    double* d_ntheta_ = nullptr;        // [nT] resonance parameters of the matrices
+    double* d_nrow_ = nullptr;          // [nacc] phase-space row of one cached evaluation
+    std::vector<double> norm_theta_;    // host copy of d_ntheta_
+    bool norm_valid_ = false;
     void* k_evc_ = nullptr;  // ct_event_cache
     std::vector<std::pair<std::string, double>> setup_ms_;  // set-up phases (host ms)
     // generated angular kernels, one per angular group (empty: the
@@ -288,10 +317,11 @@ private:
         int grid = 0;
     };
     CtaLayout lay_[2];   // fused-kernel grid of the plain [0] and mixed [1] forms
+    CtaLayout lay_data_[2];  // the same over the data and background samples only (cached normalisation)
     int grid_max_ = 0;   // rows of the partials table
     FusedShape shape_;
     int residentCtas(void* kernel, int block, int dsmem) const;
-    void layoutCtas(int target, long long tot, int block, CtaLayout& lay) const;
+    void layoutCtas(int target, long long tot, int block, CtaLayout& lay, bool no_phsp = false) const;
 
     // Hessian-vector products (compiled and allocated on first use)
     void* hvp_lib_ = nullptr;  // cudaLibrary_t

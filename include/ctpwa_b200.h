@@ -171,6 +171,32 @@ int ctpwa_gram_shape(ctpwa_handle* h, int* out4);
  * without host synchronisation. */
 int ctpwa_gram(ctpwa_handle* h, const double* d_params, double* d_out, void* stream);
 
+/* Normalisation cache. Replaces: the reference's phase-space matrix
+ * d_phsp_matrix_ = A^H diag(w/W) A, kept between its evaluations when no
+ * resonance parameter is free and used through its quadratic form
+ * (src/Analysis.cu:748-829, src/ComputeNLL.cu:575-597). Here the matrices
+ * are FP64 and carry the lineshape derivatives as well, so that the
+ * normalisation term, the coupling gradient and the resonance-parameter
+ * gradient at fixed resonance parameters all come from them:
+ * ctpwa_norm_cache_build sums them over the phase-space sample at the
+ * resonance parameters of d_params (FP64, one pass; host-synchronising;
+ * *ms, if not null, receives the pass's device time). While the cache is
+ * set, ctpwa_nll_grad_host, ctpwa_fit and ctpwa_fit_newton evaluate every
+ * point whose resonance parameters equal the cached ones bitwise from the
+ * data and background samples and the matrices alone (the phase-space
+ * sample is not read); other points take the full pass. ctpwa_fit and
+ * ctpwa_fit_newton build the cache themselves when no resonance parameter
+ * is free (free[i] == 0 or lo[i] == hi[i] for all of them).
+ * ctpwa_nll_grad_cached is the device-buffer evaluation from the cache; its
+ * resonance parameters must equal the cached ones, otherwise the result is
+ * flagged invalid (NLL 1e30, zero gradient). ctpwa_norm_cache_valid returns
+ * 1 while a cache is set, 0 otherwise. */
+int ctpwa_norm_cache_build(ctpwa_handle* h, const double* d_params, double* ms, void* stream);
+int ctpwa_norm_cache_clear(ctpwa_handle* h);
+int ctpwa_norm_cache_valid(const ctpwa_handle* h);
+int ctpwa_nll_grad_cached(ctpwa_handle* h, const double* d_params, double* d_nll, double* d_grad, int precision,
+                          void* stream);
+
 /* Exact Hessian-vector products (no counterpart in the reference, which only
  * forms the full matrix): d_out[d] = H(d_params) d_dirs[d] for ndir directions
  * (device [ndir][n_params] in, [ndir][n_params] out). */
