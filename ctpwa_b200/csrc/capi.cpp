@@ -282,6 +282,8 @@ int ctpwa_norm_cache_build(ctpwa_handle* h, const double* d_params, double* ms, 
     try {
         const double t = h->eng->normCacheBuild(d_params, (cudaStream_t)stream);
         if (ms) *ms = t;
+    } catch (const std::length_error& e) {
+        return setErr(h, CTPWA_ERR_ARG, e.what());
     } catch (const std::exception& e) {
         return setErr(h, CTPWA_ERR_CUDA, e.what());
     }
@@ -688,12 +690,14 @@ int ctpwa_fit(ctpwa_handle* h, double* params, const unsigned char* free_mask, c
     opt.ftol = ftol;
     opt.gtol = gtol;
     int ne = 0;
-    const bool fixed = thetaFixed(h, free_mask, lo, hi);
+    bool fixed = thetaFixed(h, free_mask, lo, hi);
     auto fg = [&](const double* x, double* f, double* g) -> int {
         const auto t0 = std::chrono::steady_clock::now();
         if (fixed) {
             try {
                 ensureNormCache(h, x, stream);
+            } catch (const std::length_error&) {
+                fixed = false;  // a model the cache does not support: full passes
             } catch (const std::exception& e) {
                 return setErr(h, CTPWA_ERR_CUDA, e.what());
             }
@@ -731,11 +735,13 @@ int ctpwa_fit_newton(ctpwa_handle* h, double* params, const unsigned char* free_
     } catch (const std::exception& e) {
         return setErr(h, CTPWA_ERR_CUDA, e.what());
     }
-    const bool fixed = thetaFixed(h, free_mask, lo, hi);
+    bool fixed = thetaFixed(h, free_mask, lo, hi);
     auto fg = [&](const double* x, double* f, double* g) -> int {
         if (fixed) {
             try {
                 ensureNormCache(h, x, stream);
+            } catch (const std::length_error&) {
+                fixed = false;  // a model the cache does not support: full passes
             } catch (const std::exception& e) {
                 return setErr(h, CTPWA_ERR_CUDA, e.what());
             }

@@ -2041,7 +2041,7 @@ double precompileConfig(const std::string& config_path)
     bool hit = false;
     jitCubin(g, &hit);
     jitHvpCubin(g, false, &hit);
-    jitNormCubin(g, &hit);
+    if (g.nterm + g.nder <= 256 && (size_t)(2 * g.nterm + g.nder) * g.nterm * 16 <= 40000) jitNormCubin(g, &hit);
     {
         std::vector<AgNodeVar> vars;
         std::vector<double> cg;
@@ -3130,7 +3130,7 @@ struct CtNormArgsH {
     long long n, ld;
     const double* consts;
     double* partials;
-    int ne;
+    int nrows;
     int pad;
 };
 struct CtNormRowArgsH {
@@ -3150,8 +3150,14 @@ void Engine::compileNorm()
 {
     if (k_norm_build_) return;
     const int nt = gen_.nterm, nd = gen_.nder, ng = gen_.nplane * (gen_.nplane + 1) / 2;
-    const int nu = nt * (nt + 1) / 2;
-    norm_ne_ = nu + nd * nt + (samples_[0].w ? nu : 0);
+    // output rows (terms, derivative entries, weighted terms) x nt columns;
+    // phase 2 of ct_norm_build: groups of rb rows, 128 / groups event slices
+    norm_rows_ = nt + nd + (samples_[0].w ? nt : 0);
+    norm_ne_ = norm_rows_ * nt;
+    const int rb = 2, groups = (norm_rows_ + rb - 1) / rb;  // CT_NORM_RB
+    if (groups > 128 || nt + nd > 256 || (size_t)(2 * nt + nd) * nt * 16 > 40000)
+        throw std::length_error("the normalisation cache supports models with up to 256 lineshape terms and "
+                                "derivative entries and (2 terms + entries) x terms <= 2500");
     bool hit = false;
     std::string cubin = jitNormCubin(gen_, &hit);
     cudaLibrary_t lib;
@@ -3164,7 +3170,8 @@ void Engine::compileNorm()
     // one record of (terms + derivatives + plane pairs + weight) double2
     // slots per event of a 128-event tile, the record length made odd
     const int rec = (nt + nd + ng + 1) | 1;
-    norm_dsmem_ = 128 * rec * 16;
+    const int slices = 128 / groups;
+    norm_dsmem_ = std::max(128 * rec * 16, slices * norm_ne_ * 16);  // records, then the slices' sums
     CT_CUDA(cudaFuncSetAttribute((const void*)kb, cudaFuncAttributeMaxDynamicSharedMemorySize, norm_dsmem_));
     CT_CUDA(cudaFuncSetAttribute((const void*)kb, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared));
@@ -3208,7 +3215,7 @@ double Engine::normCacheBuild(const double* d_params, cudaStream_t stream)
     a.ld = d.ld;
     a.consts = d_consts_;
     a.partials = d_npart_;
-    a.ne = norm_ne_;
+    a.nrows = norm_rows_;
     cudaEvent_t e0, e1;
     CT_CUDA(cudaEventCreate(&e0));
     CT_CUDA(cudaEventCreate(&e1));

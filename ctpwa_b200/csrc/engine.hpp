@@ -276,7 +276,8 @@ private:
     void* k_norm_row_ = nullptr;
     int norm_grid_ = 0;
     int norm_dsmem_ = 0;
-    int norm_ne_ = 0;                   // complex entries: Mu, D (and Mw for a weighted sample)
+    int norm_rows_ = 0;                 // rows of Mu, D (and Mw for a weighted sample), each of nterm entries
+    int norm_ne_ = 0;                   // complex entries: norm_rows_ x nterm
     double* d_npart_ = nullptr;         // [norm_grid_][norm_ne_][2]
     double* d_nmat_ = nullptr;          // [norm_ne_][2]
     double* d_ntheta_ = nullptr;        // [nT] resonance parameters of the matrices

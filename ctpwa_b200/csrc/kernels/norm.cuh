@@ -23,10 +23,15 @@
 // ct_norm_build: a CTA takes tiles of CT_NORM_TILE events. Phase 1: thread i
 // evaluates event i's lineshapes and derivatives (model_columns, FP64) and
 // plane products and writes them as one record to shared memory. Phase 2:
-// thread j owns entries j, j + CT_NORM_BLOCK, ... of the output and adds the
-// tile's events to them (three record reads and eight FP64 operations per
-// entry and event; the warp's lanes read one record at a time). Per-CTA
-// partial sums, reduced in a fixed order by ct_norm_reduce.
+// the output rows (terms, derivative entries, weighted terms), ordered by
+// angular plane, are cut into groups of CT_NORM_RB rows; thread (group,
+// slice) adds the tile's events slice, slice + slices, ... to its rows x all
+// columns, so per event it reads its rows' factors, the column factors and
+// the plane products of its rows' planes once and reuses them from
+// registers. At the end the slices' sums are added in a fixed order through
+// shared memory into one partial row per CTA, reduced over CTAs in a fixed
+// order by ct_norm_reduce. Output (complex, full matrices):
+//   Mu [M_NTERM][M_NTERM], D [M_NDER][M_NTERM], Mw [M_NTERM][M_NTERM] (weighted).
 #pragma once
 
 #include "fused_nll.cuh"
@@ -34,14 +39,14 @@
 #define CT_NORM_BLOCK 128
 #define CT_NORM_TILE 128  // events per tile (one per thread in phase 1)
 #define CT_NORM_NG (M_NPLANE * (M_NPLANE + 1) / 2)
-#define CT_NORM_NU (M_NTERM * (M_NTERM + 1) / 2)
-// entries: Mu, D, then Mw (weighted samples)
-#define CT_NORM_NE_MAX (2 * CT_NORM_NU + M_NDER * M_NTERM)
-#define CT_NORM_MAXJ ((CT_NORM_NE_MAX + CT_NORM_BLOCK - 1) / CT_NORM_BLOCK)
+// rows per phase-2 thread (rows x M_NTERM complex sums in registers; 4
+// spilled on K+K-pi0 next to the FP64 lineshapes of phase 1)
+#define CT_NORM_RB 2
 // record per event, in double2 slots: F_t, dF_k, G pairs, (w, 0); odd length
 // so the phase-1 stores of consecutive threads fall in different banks
 #define CT_NORM_REC0 (M_NTERM + M_NDER + CT_NORM_NG + 1)
 #define CT_NORM_REC (CT_NORM_REC0 | 1)
+#define CT_NORM_WSLOT (M_NTERM + M_NDER + CT_NORM_NG)
 
 struct CtNormArgs {
     const double2* slamp;  // FP64 angular table [M_NPLANE * M_NPOL][ld]
@@ -49,8 +54,8 @@ struct CtNormArgs {
     const double* w;       // per-event weights or nullptr
     long long n, ld;
     const double* consts;  // [M_NCONST] parameter-only subexpressions at the cached theta
-    double* partials;      // [grid][ne][2]
-    int ne;                // entries: CT_NORM_NU + M_NDER M_NTERM (+ CT_NORM_NU when weighted)
+    double* partials;      // [grid][nrows * M_NTERM][2]
+    int nrows;             // output rows: M_NTERM + M_NDER (+ M_NTERM when weighted)
     int pad;
 };
 
@@ -59,55 +64,79 @@ __device__ __forceinline__ int ct_norm_gpair(int c, int d)  // c <= d
     return c * M_NPLANE - c * (c - 1) / 2 + (d - c);
 }
 
-// upper-triangle index q -> (t, s), t <= s
-__device__ __forceinline__ void ct_norm_tri(int q, int& t, int& s)
+// record slot of the output row's first factor, its plane, weighting
+__device__ __forceinline__ void ct_norm_rowinfo(int r, int& slot, int& plane, bool& weighted)
 {
-    t = 0;
-    while (q >= M_NTERM - t) {
-        q -= M_NTERM - t;
-        ++t;
+    weighted = false;
+    if (r < M_NTERM) {
+        slot = r;
+        plane = term_plane(r);
+    } else if (r < M_NTERM + M_NDER) {
+        slot = r;
+        plane = term_plane(der_term(r - M_NTERM));
+    } else {
+        slot = r - M_NTERM - M_NDER;
+        plane = term_plane(slot);
+        weighted = true;
     }
-    s = t + q;
 }
 
 extern "C" __global__ void __launch_bounds__(CT_NORM_BLOCK) ct_norm_build(CtNormArgs A)
 {
-    extern __shared__ double2 nrec[];  // [CT_NORM_TILE][CT_NORM_REC]
+    extern __shared__ double2 nrec[];  // [CT_NORM_TILE][CT_NORM_REC]; at the end [slices][nrows][M_NTERM]
     __shared__ double sC[CT_NCONST_ALLOC];
     for (int i = threadIdx.x; i < M_NCONST; i += CT_NORM_BLOCK) sC[i] = A.consts[i];
 
-    // this thread's entries: record slots of the two factors and the plane
-    // pair, conjugation of the pair, weighting
-    short sa[CT_NORM_MAXJ], sb[CT_NORM_MAXJ], sg[CT_NORM_MAXJ];
-    bool cj[CT_NORM_MAXJ], wt[CT_NORM_MAXJ];
-    double accr[CT_NORM_MAXJ], acci[CT_NORM_MAXJ];
+    // ---- this thread's rows (plane-sorted order) and event slice ----
+    const int nrows = A.nrows;
+    const int groups = (nrows + CT_NORM_RB - 1) / CT_NORM_RB;
+    const int slices = CT_NORM_BLOCK / groups;  // >= 1 (host check)
+    const int grp = threadIdx.x % groups, sl = threadIdx.x / groups;
+    const bool active = sl < slices;
+    int rid[CT_NORM_RB], aslot[CT_NORM_RB];
+    unsigned cjm[CT_NORM_RB];           // bit d: plane pair (row plane, d) stored transposed
+    short gsl[CT_NORM_RB][M_NPLANE];    // record slot of G(row plane, d)
+    bool wrow[CT_NORM_RB];
+    {
+        // position grp * RB + j of the rows listed plane by plane
+        int pos = 0;
 #pragma unroll
-    for (int j = 0; j < CT_NORM_MAXJ; ++j) {
-        accr[j] = 0.0;
-        acci[j] = 0.0;
-        int q = threadIdx.x + j * CT_NORM_BLOCK, ra = 0, s = 0, pa = 0;
-        bool w = false;
-        if (q >= A.ne) q = 0;  // idle slot: computed, never stored
-        if (q < CT_NORM_NU) {
-            ct_norm_tri(q, ra, s);
-            pa = term_plane(ra);
-        } else if (q < CT_NORM_NU + M_NDER * M_NTERM) {
-            const int k = (q - CT_NORM_NU) / M_NTERM;
-            s = (q - CT_NORM_NU) % M_NTERM;
-            ra = M_NTERM + k;
-            pa = term_plane(der_term(k));
-        } else {
-            ct_norm_tri(q - CT_NORM_NU - M_NDER * M_NTERM, ra, s);
-            pa = term_plane(ra);
-            w = true;
+        for (int j = 0; j < CT_NORM_RB; ++j) rid[j] = -1;
+        for (int c = 0; c < M_NPLANE; ++c)
+            for (int r = 0; r < nrows; ++r) {
+                int sl_, pl;
+                bool wt_;
+                ct_norm_rowinfo(r, sl_, pl, wt_);
+                if (pl != c) continue;
+                const int j = pos - grp * CT_NORM_RB;
+#pragma unroll
+                for (int q = 0; q < CT_NORM_RB; ++q)
+                    if (q == j) rid[q] = r;
+                ++pos;
+            }
+#pragma unroll
+        for (int j = 0; j < CT_NORM_RB; ++j) {
+            int pl = 0;
+            bool wt_ = false;
+            aslot[j] = 0;
+            if (rid[j] >= 0) ct_norm_rowinfo(rid[j], aslot[j], pl, wt_);
+            wrow[j] = wt_;
+            cjm[j] = 0u;
+#pragma unroll
+            for (int d = 0; d < M_NPLANE; ++d) {
+                gsl[j][d] = (short)(M_NTERM + M_NDER + (pl <= d ? ct_norm_gpair(pl, d) : ct_norm_gpair(d, pl)));
+                if (pl > d) cjm[j] |= 1u << d;
+            }
         }
-        const int pb = term_plane(s);
-        sa[j] = (short)ra;
-        sb[j] = (short)s;
-        sg[j] = (short)(M_NTERM + M_NDER + (pa <= pb ? ct_norm_gpair(pa, pb) : ct_norm_gpair(pb, pa)));
-        cj[j] = pa > pb;
-        wt[j] = w;
     }
+    double accr[CT_NORM_RB][M_NTERM], acci[CT_NORM_RB][M_NTERM];
+#pragma unroll
+    for (int j = 0; j < CT_NORM_RB; ++j)
+#pragma unroll
+        for (int s = 0; s < M_NTERM; ++s) {
+            accr[j][s] = 0.0;
+            acci[j][s] = 0.0;
+        }
     __syncthreads();
 
     const long long ntiles = (A.n + CT_NORM_TILE - 1) / CT_NORM_TILE;
@@ -126,9 +155,9 @@ extern "C" __global__ void __launch_bounds__(CT_NORM_BLOCK) ct_norm_build(CtNorm
                 for (int t = 0; t < M_NTERM; ++t) r[t] = make_double2(Fr[t], Fi[t]);
 #pragma unroll
                 for (int k = 0; k < M_NDER; ++k) r[M_NTERM + k] = make_double2(dFr[k], dFi[k]);
-                double2 sl[M_NPLANE * M_NPOL];
+                double2 sl2[M_NPLANE * M_NPOL];
 #pragma unroll
-                for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl[c] = A.slamp[(long long)c * A.ld + e];
+                for (int c = 0; c < M_NPLANE * M_NPOL; ++c) sl2[c] = A.slamp[(long long)c * A.ld + e];
 #pragma unroll
                 for (int c = 0; c < M_NPLANE; ++c)
 #pragma unroll
@@ -136,53 +165,73 @@ extern "C" __global__ void __launch_bounds__(CT_NORM_BLOCK) ct_norm_build(CtNorm
                         double gr = 0.0, gi = 0.0;
 #pragma unroll
                         for (int p = 0; p < M_NPOL; ++p) {
-                            const double2 x = sl[c * M_NPOL + p], y = sl[d * M_NPOL + p];
+                            const double2 x = sl2[c * M_NPOL + p], y = sl2[d * M_NPOL + p];
                             gr += x.x * y.x + x.y * y.y;
                             gi += x.y * y.x - x.x * y.y;
                         }
                         r[M_NTERM + M_NDER + ct_norm_gpair(c, d)] = make_double2(gr, gi);
                     }
-                r[M_NTERM + M_NDER + CT_NORM_NG] = make_double2(A.w ? __ldg(A.w + e) : 1.0, 0.0);
+                r[CT_NORM_WSLOT] = make_double2(A.w ? __ldg(A.w + e) : 1.0, 0.0);
             } else {
                 // past the sample's end: zero factors contribute nothing
 #pragma unroll
-                for (int t = 0; t < M_NTERM; ++t) r[t] = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int k = 0; k < M_NDER; ++k) r[M_NTERM + k] = make_double2(0.0, 0.0);
-                r[M_NTERM + M_NDER + CT_NORM_NG] = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int g = 0; g < CT_NORM_NG; ++g) r[M_NTERM + M_NDER + g] = make_double2(0.0, 0.0);
+                for (int k = 0; k < CT_NORM_REC0; ++k) r[k] = make_double2(0.0, 0.0);
             }
         }
         __syncthreads();
-        // ---- phase 2: the tile's events into this thread's entries ----
-#pragma unroll 2
-        for (int i = 0; i < CT_NORM_TILE; ++i) {
-            const double2* r = nrec + (size_t)i * CT_NORM_REC;
-            const double we = r[M_NTERM + M_NDER + CT_NORM_NG].x;
+        // ---- phase 2: this slice's events into this thread's rows ----
+        if (active)
+            for (int i = sl; i < CT_NORM_TILE; i += slices) {
+                const double2* r = nrec + (size_t)i * CT_NORM_REC;
+                double2 b[M_NTERM];
 #pragma unroll
-            for (int j = 0; j < CT_NORM_MAXJ; ++j) {
-                const double2 a = r[sa[j]], b = r[sb[j]], g = r[sg[j]];
-                // x = a conj(b); accumulate x g (x conj(g) for a transposed plane pair)
-                double xr = a.x * b.x + a.y * b.y, xi = a.y * b.x - a.x * b.y;
-                if (wt[j]) {
-                    xr *= we;
-                    xi *= we;
+                for (int s = 0; s < M_NTERM; ++s) b[s] = r[s];
+                const double we = r[CT_NORM_WSLOT].x;
+#pragma unroll
+                for (int j = 0; j < CT_NORM_RB; ++j) {
+                    double2 a = r[aslot[j]];
+                    if (wrow[j]) {
+                        a.x *= we;
+                        a.y *= we;
+                    }
+                    double2 g[M_NPLANE];
+#pragma unroll
+                    for (int d = 0; d < M_NPLANE; ++d) {
+                        g[d] = r[gsl[j][d]];
+                        if (cjm[j] >> d & 1u) g[d].y = -g[d].y;
+                    }
+#pragma unroll
+                    for (int s = 0; s < M_NTERM; ++s) {
+                        // a conj(b_s) G(row plane, plane(s))
+                        const double xr = a.x * b[s].x + a.y * b[s].y, xi = a.y * b[s].x - a.x * b[s].y;
+                        const double2 gg = g[term_plane(s)];
+                        accr[j][s] = fma(xr, gg.x, fma(-xi, gg.y, accr[j][s]));
+                        acci[j][s] = fma(xr, gg.y, fma(xi, gg.x, acci[j][s]));
+                    }
                 }
-                const double gi = cj[j] ? -g.y : g.y;
-                accr[j] = fma(xr, g.x, fma(-xi, gi, accr[j]));
-                acci[j] = fma(xr, gi, fma(xi, g.x, acci[j]));
             }
-        }
         __syncthreads();
     }
+    // ---- the slices' sums, in slice order, into this CTA's partial row ----
+    double2* red = nrec;  // [slices][nrows][M_NTERM]
+    if (active)
 #pragma unroll
-    for (int j = 0; j < CT_NORM_MAXJ; ++j) {
-        const int q = threadIdx.x + j * CT_NORM_BLOCK;
-        if (q < A.ne) {
-            A.partials[((long long)blockIdx.x * A.ne + q) * 2] = accr[j];
-            A.partials[((long long)blockIdx.x * A.ne + q) * 2 + 1] = acci[j];
+        for (int j = 0; j < CT_NORM_RB; ++j)
+            if (rid[j] >= 0)
+#pragma unroll
+                for (int s = 0; s < M_NTERM; ++s)
+                    red[((size_t)sl * nrows + rid[j]) * M_NTERM + s] = make_double2(accr[j][s], acci[j][s]);
+    __syncthreads();
+    const int ne = nrows * M_NTERM;
+    for (int q = threadIdx.x; q < ne; q += CT_NORM_BLOCK) {
+        double xr = 0.0, xi = 0.0;
+        for (int k = 0; k < slices; ++k) {
+            const double2 x = red[(size_t)k * ne + q];
+            xr += x.x;
+            xi += x.y;
         }
+        A.partials[((long long)blockIdx.x * ne + q) * 2] = xr;
+        A.partials[((long long)blockIdx.x * ne + q) * 2 + 1] = xi;
     }
 }
 
@@ -201,7 +250,7 @@ extern "C" __global__ void __launch_bounds__(256) ct_norm_reduce(const double* _
 }
 
 struct CtNormRowArgs {
-    const double* mat;           // [ne][2]: Mu, D, Mw (ct_norm_reduce)
+    const double* mat;           // complex Mu [M_NTERM][M_NTERM], D [M_NDER][M_NTERM], Mw (ct_norm_reduce)
     int weighted;                // Mw present
     int use_vh;                  // mixed form: the couplings rounded to FP32, as its fused pass uses them
     const double* v;             // couplings (re, im) x M_NA
@@ -219,12 +268,12 @@ struct CtNormRowArgs {
 #define CT_NORM_ROW_THREADS 256
 extern "C" __global__ void __launch_bounds__(CT_NORM_ROW_THREADS) ct_norm_row(CtNormRowArgs A)
 {
-    constexpr int NE = CT_NORM_NE_MAX;
+    constexpr int NE = (2 * M_NTERM + M_NDER) * M_NTERM;
     __shared__ double sm[2 * NE];
     __shared__ double cr[M_NTERM], ci[M_NTERM];
     __shared__ double tr[M_NTERM], ti[M_NTERM], tf[M_NTERM];  // per term: r_t, Re(c_t u_t)
     __shared__ double dk[M_NDER > 0 ? M_NDER : 1];            // per derivative entry
-    const int ne = CT_NORM_NU + M_NDER * M_NTERM + (A.weighted ? CT_NORM_NU : 0);
+    const int ne = (M_NTERM + M_NDER + (A.weighted ? M_NTERM : 0)) * M_NTERM;
     for (int i = threadIdx.x; i < 2 * ne; i += blockDim.x) sm[i] = A.mat[i];
     for (int t = threadIdx.x; t < M_NTERM; t += blockDim.x) {
         const int a = term_col(t);
@@ -240,23 +289,15 @@ extern "C" __global__ void __launch_bounds__(CT_NORM_ROW_THREADS) ct_norm_row(Ct
         if (__double_as_longlong(A.theta[j]) != __double_as_longlong(A.theta_cached[j])) atomicExch(A.err, 1);
     __syncthreads();
     const double* Mu = sm;
-    const double* D = sm + 2 * CT_NORM_NU;
-    const double* Mw = A.weighted ? sm + 2 * (CT_NORM_NU + M_NDER * M_NTERM) : Mu;
-    // entry (t, s) of a Hermitian matrix stored as its upper triangle
-    auto herm = [&](const double* M, int t, int s, double& re, double& im) {
-        const int a = t <= s ? t : s, b = t <= s ? s : t;
-        const int q = a * M_NTERM - a * (a - 1) / 2 + (b - a);
-        re = M[2 * q];
-        im = t <= s ? M[2 * q + 1] : -M[2 * q + 1];
-    };
+    const double* D = sm + 2 * M_NTERM * M_NTERM;
+    const double* Mw = A.weighted ? sm + 2 * (M_NTERM + M_NDER) * M_NTERM : Mu;
     const int i = threadIdx.x;
     if (i < M_NTERM) {
         // r_t = sum_s c_s conj(Mw[t][s]);  u_t = sum_s conj(c_s) Mu[t][s]
         double rr = 0.0, ri = 0.0, ur = 0.0, ui = 0.0;
         for (int s = 0; s < M_NTERM; ++s) {
-            double mr, mi, wr, wi;
-            herm(Mu, i, s, mr, mi);
-            herm(Mw, i, s, wr, wi);
+            const double mr = Mu[2 * (i * M_NTERM + s)], mi = Mu[2 * (i * M_NTERM + s) + 1];
+            const double wr = Mw[2 * (i * M_NTERM + s)], wi = Mw[2 * (i * M_NTERM + s) + 1];
             rr += cr[s] * wr + ci[s] * wi;
             ri += ci[s] * wr - cr[s] * wi;
             ur += cr[s] * mr + ci[s] * mi;
