@@ -100,8 +100,16 @@ class Oracle:
     def __del__(self):
         self.close()
 
-    def nll_grad(self, params, nthreads=0):
+    def _params(self, params):
+        """The parameter array as the C side reads it: 2 nV + nT doubles
+        (a shorter array would be read past its end)."""
         p = np.ascontiguousarray(params, dtype=np.float64)
+        if p.ndim != 1 or p.size != 2 * self.nV + self.nT:
+            raise ValueError(f"params: expected {2 * self.nV + self.nT} values, got shape {p.shape}")
+        return p
+
+    def nll_grad(self, params, nthreads=0):
+        p = self._params(params)
         g = np.zeros_like(p)
         v = ctypes.c_double()
         parts = np.zeros(6)
@@ -112,7 +120,7 @@ class Oracle:
 
     def shard_sums(self, params, nthreads=0):
         """Per-sample sums of this oracle's events (layout of the engine's shard sums)."""
-        p = np.ascontiguousarray(params, dtype=np.float64)
+        p = self._params(params)
         out = np.zeros(3 * (2 + 2 * self.nA + self.nT) + 4)
         if self.lib.orc_shard_sums(self.h, ptr(p), ptr(out), nthreads) != 0:
             raise RuntimeError(self.lib.orc_error(self.h).decode())
@@ -120,7 +128,7 @@ class Oracle:
 
     def finalize_sums(self, params, sums):
         """(nll, grad) from summed shard sums."""
-        p = np.ascontiguousarray(params, dtype=np.float64)
+        p = self._params(params)
         s = np.ascontiguousarray(sums, dtype=np.float64)
         g = np.zeros_like(p)
         v = ctypes.c_double()
@@ -136,6 +144,8 @@ class Oracle:
 
     def columns(self, kind, theta):
         t = np.ascontiguousarray(theta, dtype=np.float64)
+        if t.ndim != 1 or t.size != self.nT:
+            raise ValueError(f"theta: expected {self.nT} values, got shape {t.shape}")
         out = np.zeros((self.nev[kind], self.npol, self.nA), dtype=np.complex128)
         self.lib.orc_columns(self.h, kind, ptr(t), out.ctypes.data_as(_D))
         return out
@@ -151,7 +161,7 @@ class Oracle:
         self.nev = tuple(nev)
 
     def intensity(self, kind, params):
-        p = np.ascontiguousarray(params, dtype=np.float64)
+        p = self._params(params)
         out = np.zeros(self.nev[kind])
         self.lib.orc_intensity(self.h, kind, ptr(p), ptr(out))
         return out
@@ -177,7 +187,7 @@ class Oracle:
 
     def hessian_fd(self, params, rel=1e-5):
         """[nP, nP] Hessian of the oracle NLL (symmetrised)."""
-        p = np.ascontiguousarray(params, dtype=np.float64)
+        p = self._params(params)
         n = p.size
         H = np.zeros((n, n))
         for i in range(n):
@@ -188,7 +198,7 @@ class Oracle:
 
     def hvp_sums_fd(self, params, dirs, rel=1e-5):
         """[ndir, 3 nacc] directional derivatives of shard_sums' per-sample sums."""
-        p = np.ascontiguousarray(params, dtype=np.float64)
+        p = self._params(params)
         nacc = 2 + 2 * self.nA + self.nT
         out = []
         for u in np.atleast_2d(dirs):
@@ -198,7 +208,7 @@ class Oracle:
     def finalize_hvp_fd(self, params, dirs, sums, tsums, rel=1e-5):
         """[ndir, nP] rows H u from value sums and tangent sums: the directional
         derivative of finalize_sums along (u, tangent sums)."""
-        p = np.ascontiguousarray(params, dtype=np.float64)
+        p = self._params(params)
         s = np.ascontiguousarray(sums, dtype=np.float64)
         nacc = 2 + 2 * self.nA + self.nT
         dirs = np.atleast_2d(dirs)

@@ -147,3 +147,33 @@ def test_fit_with_fixed_resonance_parameters(tmp_path):
     n0, g0 = ana.getNLLAndGrad(torch.tensor(x, dtype=torch.float64, device="cuda"), "fp64")
     assert abs(float(n0) - nll) <= 1e-10 * abs(nll)
     assert np.max(np.abs(g0.cpu().numpy()[free.astype(bool)])) < 1e-2
+
+
+def test_model_without_free_resonance_parameters(tmp_path):
+    """Every resonance parameter fixed in the configuration (no theta at
+    all): the cache holds for every evaluation, including the fit's."""
+    import torch
+    import ctpwa_b200
+
+    cfg = workloads.make("pipi_3rho", tmp_path, n_phsp=30_000, n_data=4_000, n_bkg=500, accept_reject=False, seed=9)
+    text = open(cfg).read()
+    assert ", free: [0, 1]" in text
+    open(cfg, "w").write(text.replace(", free: [0, 1]", ""))
+    ana = ctpwa_b200.analysis(cfg)
+    assert ana.getNFreeTheta() == 0
+    nV = ana.getNVector()
+    p = workloads.true_params(nV, [])
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    ana.cacheNormalisation(pt)
+    orc = Oracle(cfg)
+    for q in (p, _other_couplings(p, nV, 5)):
+        qt = torch.tensor(q, dtype=torch.float64, device="cuda")
+        n1, g1 = ana.getNLLAndGrad(qt, "fp64", cached=True)
+        _close(n1, g1, *ana.getNLLAndGrad(qt, "fp64"))
+        onll, og, _ = orc.nll_grad(q)
+        _close(n1, g1, onll, og)
+    ana.clearNormalisationCache()
+    x, nll, *_ = ana.fit(_other_couplings(p, nV, 6), max_evals=300, precision="fp64")
+    assert ana.hasNormalisationCache()
+    n0, _ = ana.getNLLAndGrad(torch.tensor(x, dtype=torch.float64, device="cuda"), "fp64")
+    assert abs(float(n0) - nll) <= 1e-10 * abs(nll)
