@@ -419,6 +419,25 @@ def norm_cache_timing(ana, p0, device, reps=50):
         ms = e0.elapsed_time(e1) / reps
         out[prec + "_ms_per_eval"] = ms
         out[prec + "_evals_per_s"] = 1e3 / ms
+    # through the host-buffer entry point, as a fit calls it (parameters in,
+    # NLL and gradient out, a synchronisation per call): host clock
+    qh = [q.cpu().numpy() for q in qs]
+    ana.getNLLHost(qh[0], "mixed")
+    t0 = time.perf_counter()
+    for q in qh:
+        ana.getNLLHost(q, "mixed")
+    out["mixed_host_ms_per_eval"] = 1e3 * (time.perf_counter() - t0) / len(qh)
+    # a fit of the couplings with the resonance parameters fixed (the fit
+    # builds the cache itself), against the same fit with them free
+    nV = ana.getNVector()
+    free = np.zeros(nP, dtype=np.uint8)
+    free[1:nV] = 1
+    free[nV + 1:2 * nV] = 1
+    ana.clearNormalisationCache()
+    t0 = time.perf_counter()
+    _, fnll, fev, _, fst, _ = ana.fit(qh[1], free=free, max_evals=200, precision="mixed")
+    out["fixed_theta_fit"] = {"ms": 1e3 * (time.perf_counter() - t0), "evaluations": fev, "status": fst,
+                              "includes": "cache build + evaluations (mixed, host buffers)"}
     n1, g1 = ana.getNLLAndGrad(qs[0], "fp64", cached=True)
     n0, g0 = ana.getNLLAndGrad(qs[0], "fp64")
     out["fp64_cached_vs_full_rel_nll"] = abs(float(n1) - float(n0)) / abs(float(n0))
