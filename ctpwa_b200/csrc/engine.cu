@@ -567,7 +567,8 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
     // [3][nacc] sample sums, gv [2 nA] (+ 8 spare), then the inputs of the
     // serial assembly staged by all threads (thread 0 reads no global
     // memory): couplings [2 nA], parameters [2 nc + nT], coupling chain
-    // [nA], Gaussian constraints [3 ngauss] (ct_finalize_shm)
+    // [nA], Gaussian constraints [3 ngauss]; then the per-warp sums of the
+    // row reduction [32][nacc] (ct_finalize_shm)
     extern __shared__ double sh[];
     double* sums = sh;
     double* sv = sh + 3 * A.nacc + 2 * A.nA + 8;
@@ -594,86 +595,121 @@ __device__ __forceinline__ void ct_finalize_body(const FinalizeArgs& A)
         W_data = A.sums[3 * A.nacc + 2];
         W_bkg = A.sums[3 * A.nacc + 3];
     } else {
-        for (int i = warp; i < 3 * A.nacc; i += nwarp) {
-            int k = i / A.nacc, j = i % A.nacc;
-            double s = 0.0;
+        // per sample: warp w sums rows w, w + nwarp, ... of the sample's CTA
+        // rows (each row read by one warp, lanes over its columns:
+        // coalesced), then one thread per column adds the warps' sums in
+        // warp order, so the sums are bit-reproducible
+        double* wsum = sg + 3 * A.ngauss;  // [nwarp][nacc]
+        for (int k = 0; k < 3; ++k) {
             if (k == 0 && A.phsp_row) {
-                if (lane == 0) sums[i] = A.phsp_row[j];
+                for (int j = threadIdx.x; j < A.nacc; j += blockDim.x) sums[j] = A.phsp_row[j];
                 continue;
             }
-            if (A.has[k])
-                for (int b = lane; b < A.cta[k][1]; b += 32) s += A.partials[(long long)(A.cta[k][0] + b) * A.nacc + j];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) sums[i] = s;
+            for (int j0 = 0; j0 < A.nacc; j0 += 32) {
+                const int j = j0 + lane;
+                if (j >= A.nacc) continue;
+                double s = 0.0;
+                if (A.has[k]) {
+                    const double* rows = A.partials + (long long)A.cta[k][0] * A.nacc + j;
+#pragma unroll 4
+                    for (int b = warp; b < A.cta[k][1]; b += nwarp) s += rows[(long long)b * A.nacc];
+                }
+                wsum[warp * A.nacc + j] = s;
+            }
+            __syncthreads();
+            for (int j = threadIdx.x; j < A.nacc; j += blockDim.x) {
+                double s = 0.0;
+                for (int w = 0; w < nwarp; ++w) s += wsum[w * A.nacc + j];
+                sums[k * A.nacc + j] = s;
+            }
+            __syncthreads();
         }
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;
+    // loss and gradient assembly, spread over threads: thread 0 the loss,
+    // threads a < nA the coupling sums g_a, then one thread per parameter
     const double* P = sums;               // phase space
     const double* Dd = sums + A.nacc;     // data
     const double* B = sums + 2 * A.nacc;  // background
-    double pf = n_phsp > 0 ? P[1] / n_phsp : 0.0;
-    if (pf <= 1e-30 || isnan(pf) || isinf(pf)) pf = 1e-30;
-    double Weff = W_data - W_bkg;
-    double loss = Dd[0] - B[0] + Weff * log(pf);
-    if (A.err && *A.err) loss = nan("");
-    const double* theta = sp + 2 * A.nc;
-    for (int g = 0; g < A.ngauss; ++g) {
-        double dl = theta[(int)sg[3 * g]] - sg[3 * g + 1];
-        loss += dl * dl / (2.0 * sg[3 * g + 2] * sg[3 * g + 2]);
-    }
-    bool reset = isnan(loss) || isinf(loss);
-    if (reset) loss = 1e30;
     double* gv = sums + 3 * A.nacc;
-    for (int a = 0; a < A.nA; ++a) {
+    double* scal = gv + 2 * A.nA;         // pf, W_eff, loss, reset (4 of the 8 spare)
+    const double* theta = sp + 2 * A.nc;
+    if (threadIdx.x == 0) {
+        double pf = n_phsp > 0 ? P[1] / n_phsp : 0.0;
+        if (pf <= 1e-30 || isnan(pf) || isinf(pf)) pf = 1e-30;
+        const double Weff = W_data - W_bkg;
+        double loss = Dd[0] - B[0] + Weff * log(pf);
+        if (A.err && *A.err) loss = nan("");
+        for (int g = 0; g < A.ngauss; ++g) {
+            double dl = theta[(int)sg[3 * g]] - sg[3 * g + 1];
+            loss += dl * dl / (2.0 * sg[3 * g + 2] * sg[3 * g + 2]);
+        }
+        const bool reset = isnan(loss) || isinf(loss);
+        scal[0] = pf;
+        scal[1] = Weff;
+        scal[2] = reset ? 1e30 : loss;
+        scal[3] = reset ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const double pf = scal[0], Weff = scal[1];
+    const bool reset = scal[3] != 0.0;
+    for (int a = threadIdx.x; a < A.nA; a += blockDim.x) {
         double r = Dd[2 + 2 * a] - B[2 + 2 * a] + (Weff / pf) * (P[2 + 2 * a] * gv_phsp_scale);
         double i = Dd[3 + 2 * a] - B[3 + 2 * a] + (Weff / pf) * (P[3 + 2 * a] * gv_phsp_scale);
         gv[2 * a] = reset ? 0.0 : r;
         gv[2 * a + 1] = reset ? 0.0 : i;
     }
-    if (A.vshift && !reset) {
-        // the mixed form's sums are at v_h = FP32(v): add dL/dRe v . (v - v_h)
-        // + dL/dIm v . (v - v_h) with dL/dRe v_a = 2 Re g_a, dL/dIm v_a = 2 Im g_a
-        double corr = 0.0;
-        for (int a = 0; a < A.nA; ++a) {
-            const double vr = sv[2 * a], vi = sv[2 * a + 1];
-            corr += 2.0 * (gv[2 * a] * (vr - (double)(float)vr) + gv[2 * a + 1] * (vi - (double)(float)vi));
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t == 0) {
+        double loss = scal[2];
+        if (A.vshift && !reset) {
+            // the mixed form's sums are at v_h = FP32(v): add dL/dRe v . (v - v_h)
+            // + dL/dIm v . (v - v_h) with dL/dRe v_a = 2 Re g_a, dL/dIm v_a = 2 Im g_a
+            double corr = 0.0;
+            for (int a = 0; a < A.nA; ++a) {
+                const double vr = sv[2 * a], vi = sv[2 * a + 1];
+                corr += 2.0 * (gv[2 * a] * (vr - (double)(float)vr) + gv[2 * a + 1] * (vi - (double)(float)vi));
+            }
+            loss += corr;
         }
-        loss += corr;
-    }
-    for (int c = 0; c < A.nc; ++c) {
-        double sr = 0.0, si = 0.0;
-        for (int a = 0; a < A.nA; ++a) {
-            if ((int)sch[a] != c) continue;
-            double gr = gv[2 * a], gi = gv[2 * a + 1], vr = sv[2 * a], vi = sv[2 * a + 1];
-            sr += gr * vr + gi * vi;
-            si += gr * vi - gi * vr;
+        *A.out_nll = loss;
+        if (A.out_parts) {
+            A.out_parts[0] = Dd[0];
+            A.out_parts[1] = B[0];
+            A.out_parts[2] = P[1];
+            A.out_parts[3] = W_data;
+            A.out_parts[4] = W_bkg;
+            A.out_parts[5] = n_phsp;
         }
-        double pr = sp[c], pi = sp[A.nc + c];
-        double ps = pr * pr + pi * pi;
-        if (ps < 1e-30) ps = 1e-30;
-        A.out_grad[c] = 2.0 * (sr * pr + si * pi) / ps;
-        A.out_grad[A.nc + c] = -2.0 * (si * pr - sr * pi) / ps;
     }
-    for (int j = 0; j < A.nT; ++j) {
-        double g = Dd[2 + 2 * A.nA + j] - B[2 + 2 * A.nA + j] + (Weff / (pf * n_phsp)) * P[2 + 2 * A.nA + j];
-        A.out_grad[2 * A.nc + j] = reset ? 0.0 : g;
-    }
-    if (!reset)
-        for (int g = 0; g < A.ngauss; ++g) {
-            int j = (int)sg[3 * g];
-            A.out_grad[2 * A.nc + j] += (theta[j] - sg[3 * g + 1]) / (sg[3 * g + 2] * sg[3 * g + 2]);
+    // the other warps: one parameter each (couplings, then resonance parameters)
+    if (t >= 32)
+        for (int u = t - 32; u < A.nc + A.nT; u += (int)blockDim.x - 32) {
+            if (u < A.nc) {
+                const int c = u;
+                double sr = 0.0, si = 0.0;
+                for (int a = 0; a < A.nA; ++a) {
+                    if ((int)sch[a] != c) continue;
+                    double gr = gv[2 * a], gi = gv[2 * a + 1], vr = sv[2 * a], vi = sv[2 * a + 1];
+                    sr += gr * vr + gi * vi;
+                    si += gr * vi - gi * vr;
+                }
+                double pr = sp[c], pi = sp[A.nc + c];
+                double ps = pr * pr + pi * pi;
+                if (ps < 1e-30) ps = 1e-30;
+                A.out_grad[c] = 2.0 * (sr * pr + si * pi) / ps;
+                A.out_grad[A.nc + c] = -2.0 * (si * pr - sr * pi) / ps;
+            } else {
+                const int j = u - A.nc;
+                double g = Dd[2 + 2 * A.nA + j] - B[2 + 2 * A.nA + j] + (Weff / (pf * n_phsp)) * P[2 + 2 * A.nA + j];
+                if (reset) g = 0.0;
+                else
+                    for (int q = 0; q < A.ngauss; ++q)
+                        if ((int)sg[3 * q] == j) g += (theta[j] - sg[3 * q + 1]) / (sg[3 * q + 2] * sg[3 * q + 2]);
+                A.out_grad[2 * A.nc + j] = g;
+            }
         }
-    *A.out_nll = loss;
-    if (A.out_parts) {
-        A.out_parts[0] = Dd[0];
-        A.out_parts[1] = B[0];
-        A.out_parts[2] = P[1];
-        A.out_parts[3] = W_data;
-        A.out_parts[4] = W_bkg;
-        A.out_parts[5] = n_phsp;
-    }
 }
 
 __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A) { ct_finalize_body(A); }
@@ -681,7 +717,8 @@ __global__ void __launch_bounds__(1024) ct_finalize_kernel(FinalizeArgs A) { ct_
 // dynamic shared memory of a finalize launch (layout in ct_finalize_body)
 size_t ct_finalize_shm(const FinalizeArgs& f)
 {
-    return sizeof(double) * (3 * (size_t)f.nacc + 4 * (size_t)f.nA + 8 + 2 * (size_t)f.nc + f.nT + f.nA + 3 * (size_t)f.ngauss);
+    return sizeof(double) * (3 * (size_t)f.nacc + 4 * (size_t)f.nA + 8 + 2 * (size_t)f.nc + f.nT + f.nA +
+                             3 * (size_t)f.ngauss + 32 * (size_t)f.nacc);
 }
 
 // one CTA per job of a multi-job evaluation (all jobs of one model: same shared-memory size)
@@ -889,6 +926,12 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     if (ndev == 0) throw std::runtime_error("no CUDA devices available (this engine has no CPU path)");
     CT_CUDA(cudaSetDevice(opt_.device));
     CT_CUDA(cudaStreamCreateWithFlags(&mem_stream_, cudaStreamNonBlocking));
+    // the finalize kernels' shared memory grows with the gradient length
+    // (per-warp row sums, ct_finalize_shm): allow up to 200 KB
+    CT_CUDA(cudaFuncSetAttribute((const void*)ct_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 200 * 1024));
+    CT_CUDA(cudaFuncSetAttribute((const void*)ct_finalize_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 200 * 1024));
     shape_ = fusedShape(gen_);
     // initialisation work goes to a private non-blocking stream, so a handle
     // being created does not serialise with other handles' evaluations
