@@ -40,3 +40,16 @@ def test_precompile_without_gpu(tmp_path):
     p = tmp_path / "c.yml"
     p.write_text(workloads.config_text("pipi_rho", "p.npy", "d.npy"))
     assert ctpwa_b200.precompile(str(p)) >= 0.0
+
+
+def test_null_handle_arguments_are_rejected():
+    """Entry points given no handle or no buffers return CTPWA_ERR_ARG (or 0
+    for the queries) without touching a device."""
+    lib = _lib.load()
+    ERR_ARG = -3  # CTPWA_ERR_ARG
+    dp = ctypes.c_void_p(0)
+    assert lib.ctpwa_norm_cache_valid(None) == 0
+    assert lib.ctpwa_norm_cache_clear(None) == ERR_ARG
+    assert lib.ctpwa_norm_cache_build(None, dp, None, None) == ERR_ARG
+    assert lib.ctpwa_nll_grad_cached(None, dp, dp, dp, 0, None) == ERR_ARG
+    assert lib.ctpwa_nll_grad(None, dp, dp, dp, 0, None) == ERR_ARG
