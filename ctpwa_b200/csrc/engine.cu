@@ -1728,6 +1728,12 @@ void Engine::computeAngular(int kind)
     buildEventCache(kind);
 }
 
+// floats per event of the event-major FP32 frontier table (CT_EVF_STRIDE)
+int evfStride(const GeneratedModel& gen)
+{
+    return 4 * (gen.nevf > 0 ? (gen.nevf + 3) / 4 : 1);
+}
+
 // The per-event frontier tables (parameter-independent values the per-call
 // code reads) from the kinematic cache, once per sample; the kinematic cache
 // is released afterwards.
@@ -1739,7 +1745,8 @@ void Engine::buildEventCache(int kind)
     alloc(d.ev64, b64);
     device_bytes_ += b64;
     if (opt_.mixed_tables) {
-        const size_t bf = sizeof(float) * std::max(1, gen_.nevf) * ld, bd = sizeof(double) * std::max(1, gen_.nevd) * ld;
+        // FP32 frontier table event-major, 16-byte records (CT_EVF_STRIDE floats per event)
+        const size_t bf = sizeof(float) * evfStride(gen_) * ld, bd = sizeof(double) * std::max(1, gen_.nevd) * ld;
         alloc(d.evf, bf);
         alloc(d.evd, bd);
         device_bytes_ += bf + bd;
@@ -1819,12 +1826,12 @@ FusedShape fusedShape(const GeneratedModel& gen)
             acc_bytes = 0;
         }
         const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
-        const long long evb = i == 0 ? 8LL * gen.nev64 : 4LL * gen.nevf + 8LL * gen.nevd;  // frontier bytes per event
+        const long long evb = i == 0 ? 8LL * gen.nev64 : 4LL * evfStride(gen) + 8LL * gen.nevd;  // frontier bytes per event
         const int stage_on = stage_req[i];
         long long stage_bytes = 2LL * ((stage_on == 2 ? npl * rowb[i] : 0) + evb) * sh.block[i];
         if (stage_on == 3) {
             // [2][NA][block] values of the table's type (16-byte rounded), then [2][NB][block] FP64
-            const long long na = i == 0 ? gen.nev64 : gen.nevf, nb = i == 0 ? 0 : gen.nevd, sz = i == 0 ? 8 : 4;
+            const long long na = i == 0 ? gen.nev64 : evfStride(gen), nb = i == 0 ? 0 : gen.nevd, sz = i == 0 ? 8 : 4;
             stage_bytes = (2LL * std::max(1LL, na) * sh.block[i] * sz + 15) / 16 * 16 + 2LL * nb * sh.block[i] * 8;
         }
         if (stage_on && fits(i, acc_bytes + stage_bytes)) sh.stage[i] = stage_on;

@@ -234,12 +234,20 @@ __device__ __forceinline__ void ct_block_reduce_store(const double* accd, const 
 #define CT_NEV_ALLOC (M_NEV > 0 ? M_NEV : 1)
 #define CT_NEVF_ALLOC (M_NEVF > 0 ? M_NEVF : 1)
 #define CT_NEVD_ALLOC (M_NEVD > 0 ? M_NEVD : 1)
+// The FP32 frontier table is event-major: each event's values in one record
+// of CT_EVF_STRIDE floats (padded to 16 bytes), read and copied as float4;
+// the FP64 tables are row-major [value][ld].
+#define CT_NEVF4 (M_NEVF > 0 ? (M_NEVF + 3) / 4 : 1)
+#define CT_EVF_STRIDE (4 * CT_NEVF4)
 template <typename L>
 struct CtEvent;
 template <>
 struct CtEvent<double> {
-    static constexpr int NA = M_NEV, NB = 0;  // rows of the table's type, FP64 rows
+    static constexpr int NA = M_NEV, NB = 0;  // values of the table's type per event, FP64 rows
+    static constexpr bool EVMAJ = false;      // table layout [value][ld]
     double v[CT_NEV_ALLOC];
+    // this event's first value in the table (consecutive values `ld` apart)
+    static __device__ __forceinline__ const double* at(const double* table, long long e) { return table + e; }
     __device__ __forceinline__ void load(const double* a, const double*, long long stride)
     {
 #pragma unroll
@@ -253,13 +261,28 @@ struct CtEvent<double> {
 };
 template <>
 struct CtEvent<float> {
-    static constexpr int NA = M_NEVF, NB = M_NEVD;
+    static constexpr int NA = CT_EVF_STRIDE, NB = M_NEVD;  // floats per event record, FP64 rows
+    static constexpr bool EVMAJ = true;                    // FP32 table event-major
     float f[CT_NEVF_ALLOC];
     double d[CT_NEVD_ALLOC];
+    // this event's record in the table
+    static __device__ __forceinline__ const float* at(const float* table, long long e)
+    {
+        return table + e * CT_EVF_STRIDE;
+    }
+    // a: the event's 16-byte aligned record; b: its first FP64 value
+    // (consecutive values `stride` apart)
     __device__ __forceinline__ void load(const float* a, const double* b, long long stride)
     {
+        const float4* r = reinterpret_cast<const float4*>(a);
 #pragma unroll
-        for (int k = 0; k < M_NEVF; ++k) f[k] = a[(long long)k * stride];
+        for (int q = 0; q < CT_NEVF4; ++q) {
+            const float4 x = r[q];
+            if (4 * q + 0 < M_NEVF) f[4 * q + 0] = x.x;
+            if (4 * q + 1 < M_NEVF) f[4 * q + 1] = x.y;
+            if (4 * q + 2 < M_NEVF) f[4 * q + 2] = x.z;
+            if (4 * q + 3 < M_NEVF) f[4 * q + 3] = x.w;
+        }
 #pragma unroll
         for (int k = 0; k < M_NEVD; ++k) d[k] = b[(long long)k * stride];
     }
@@ -288,8 +311,9 @@ extern "C" __global__ void __launch_bounds__(CT_BLOCK) ct_event_cache(const doub
             float of[CT_NEVF_ALLOC];
             double od[CT_NEVD_ALLOC];
             model_event_mx(o, of, od);
+            float* r = evf + (long long)e * CT_EVF_STRIDE;
 #pragma unroll
-            for (int k = 0; k < M_NEVF; ++k) evf[(long long)k * ld + e] = of[k];
+            for (int k = 0; k < CT_EVF_STRIDE; ++k) r[k] = k < M_NEVF ? of[k] : 0.0f;
 #pragma unroll
             for (int k = 0; k < M_NEVD; ++k) evd[(long long)k * ld + e] = od[k];
         }
@@ -529,9 +553,17 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         double* bbuf = (double*)(ct_dyn + ACC_BYTES + ABYTES);  // [2][NB][BLOCK]
         const int tid = threadIdx.x;
         auto fetch = [&](long long e, int b) {
+            if constexpr (CtEvent<L>::EVMAJ) {
+                // the event's record: [2][BLOCK][NA] floats, 16-byte copies
+                float4* dst = reinterpret_cast<float4*>(abuf + ((size_t)b * BLOCK + tid) * NA);
+                const float4* src = reinterpret_cast<const float4*>(eva + e * NA);
 #pragma unroll
-            for (int k = 0; k < NA; ++k)
-                ct_cp_async<sizeof(L)>(abuf + ((size_t)b * NA + k) * BLOCK + tid, eva + (long long)k * S.ld + e);
+                for (int q = 0; q < NA / 4; ++q) ct_cp_async<16>(dst + q, src + q);
+            } else {
+#pragma unroll
+                for (int k = 0; k < NA; ++k)
+                    ct_cp_async<sizeof(L)>(abuf + ((size_t)b * NA + k) * BLOCK + tid, eva + (long long)k * S.ld + e);
+            }
 #pragma unroll
             for (int k = 0; k < NB; ++k)
                 ct_cp_async<8>(bbuf + ((size_t)b * NB + k) * BLOCK + tid, evb + (long long)k * S.ld + e);
@@ -545,7 +577,8 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             if (e + stride < n) fetch(e + stride, b ^ 1);
             else ct_cp_async_commit();  // empty group: the wait below covers buffer b alike
             ct_cp_async_wait<1>();
-            event(e, abuf + (size_t)b * NA * BLOCK + tid, bbuf + (size_t)b * NB * BLOCK + tid, BLOCK, slamp + e, S.ld);
+            const L* ap = CtEvent<L>::EVMAJ ? abuf + ((size_t)b * BLOCK + tid) * NA : abuf + (size_t)b * NA * BLOCK + tid;
+            event(e, ap, bbuf + (size_t)b * NB * BLOCK + tid, BLOCK, slamp + e, S.ld);
         }
         ct_cp_async_wait<0>();
     } else if constexpr (STAGE > 0) {
@@ -573,8 +606,13 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             unsigned char* buf = wbuf + (size_t)b * BUF;
             unsigned long long* bar = &ct_wbar[warp][b];
             ct_mbar_expect_tx(bar, BUF);
+            if constexpr (CtEvent<L>::EVMAJ) {
+                // the tile's 32 records in one copy
+                ct_bulk_g2s(buf, eva + e0 * NA, NA * AR, bar);
+            } else {
 #pragma unroll 1
-            for (int r = 0; r < NA; ++r) ct_bulk_g2s(buf + (size_t)r * AR, eva + (long long)r * S.ld + e0, AR, bar);
+                for (int r = 0; r < NA; ++r) ct_bulk_g2s(buf + (size_t)r * AR, eva + (long long)r * S.ld + e0, AR, bar);
+            }
 #pragma unroll 1
             for (int r = 0; r < NB; ++r)
                 ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)r * BR, evb + (long long)r * S.ld + e0, BR, bar);
@@ -603,7 +641,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             const long long e = (first + k * tstep) * 32 + lane;
             if (e < n) {
                 const unsigned char* buf = wbuf + (size_t)b * BUF;
-                const L* ap = (const L*)buf + lane;
+                const L* ap = (const L*)buf + (CtEvent<L>::EVMAJ ? lane * NA : lane);
                 const double* bp = (const double*)(buf + (size_t)NA * AR) + lane;
                 if constexpr (STAGE > 1)
                     event(e, ap, bp, 32, (const SL2*)(buf + (size_t)NA * AR + (size_t)NB * BR) + lane, 32);
@@ -628,7 +666,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     } else {
         const long long stride = (long long)S.cta_count * BLOCK;
         for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride)
-            event(e, eva + e, evb ? evb + e : nullptr, S.ld, slamp + e, S.ld);
+            event(e, CtEvent<L>::at(eva, e), evb ? evb + e : nullptr, S.ld, slamp + e, S.ld);
     }
     ct_block_reduce_store<BLOCK>(accd, accg, A.partials + (long long)cta * CT_NACC, kind == 0 ? S.vw_scale : -1.0,
                                  kind == 0 ? 2.0 : -2.0);

@@ -185,7 +185,7 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS, 2) ct_gram(CtGramA
         for (int i = 0; i < CT_GRAM_BLOCKS * NA2; ++i) x[i] = 0.0f;
         if (e < G.n) {
             CtEvent<float> ev;
-            ev.load(G.evf + e, G.evd + e, G.ld);
+            ev.load(CtEvent<float>::at(G.evf, e), G.evd + e, G.ld);
             float Fr[M_NTERM], Fi[M_NTERM], dFr[M_NDER > 0 ? M_NDER : 1], dFi[M_NDER > 0 ? M_NDER : 1];
             ev.columns(G.K->c, G.K->ch, G.K->cl, Fr, Fi, dFr, dFi);
             const float sw = (G.w && !CT_GRAM_HESS) ? (float)sqrt(G.w[e]) : 1.0f;
