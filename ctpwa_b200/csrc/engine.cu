@@ -958,6 +958,7 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
         if (samples_[k].n > 0 || k < 2) computeAngular(k);
     mark("angular");
     pairPolarisations();
+    eventMajorMixedAngular();
     mark("pairing");
     // evaluation buffers
     int nA = model_.nAmp();
@@ -1676,6 +1677,39 @@ void Engine::pairPolarisations()
     CT_CUDA(cudaStreamSynchronize(init_stream_));
 }
 
+// old [row][ld] FP32 angular rows -> event-major records of sls float2
+// (the rows' values, then zeros; zeros for the padding events past n)
+__global__ void ct_sl32_event_major_kernel(const float2* __restrict__ rows, long long n, long long ld, int nrow, int sls,
+                                           float2* __restrict__ out)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ld; e += (long long)gridDim.x * blockDim.x)
+        for (int r = 0; r < sls; ++r)
+            out[e * sls + r] = (r < nrow && e < n) ? rows[(long long)r * ld + e] : make_float2(0.0f, 0.0f);
+}
+
+// The FP32 angular tables of the evaluated samples event-major: each event's
+// values (planes x stored polarisations) in one record of an even number of
+// float2 (CT_SL32_STRIDE in kernels/fused_nll.cuh), so the mixed kernels
+// read them with 16-byte loads. The FP64 tables stay [row][ld].
+void Engine::eventMajorMixedAngular()
+{
+    const int npol = model_.npol, ns = paired_[1] ? (npol + 1) / 2 : npol;
+    const int rows = gen_.nplane * ns, sls = (rows + 1) / 2 * 2;
+    for (int k = 0; k < 3; ++k) {
+        DeviceSample& d = samples_[k];
+        if (!d.slamp32) continue;
+        float2* em = nullptr;
+        alloc(em, sizeof(float2) * (size_t)sls * d.ld);
+        const unsigned grid = (unsigned)std::min<long long>((d.ld + 255) / 256, 148LL * 16);
+        ct_sl32_event_major_kernel<<<grid, 256, 0, init_stream_>>>(d.slamp32, d.n, d.ld, rows, sls, em);
+        CT_CUDA(cudaGetLastError());
+        CT_CUDA(cudaStreamSynchronize(init_stream_));
+        devFree(d.slamp32);
+        device_bytes_ += sizeof(float2) * (size_t)(sls - rows) * d.ld;
+        d.slamp32 = em;
+    }
+}
+
 void Engine::computeAngular(int kind)
 {
     DeviceSample& d = samples_[kind];
@@ -1825,7 +1859,8 @@ FusedShape fusedShape(const GeneratedModel& gen)
             sh.acc[i] = 0;
             acc_bytes = 0;
         }
-        const long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
+        long long npl = (long long)std::max(1, gen.nplane) * std::max(1, gen.npol);
+        if (i == 1) npl = (npl + 1) / 2 * 2;  // FP32 angular records of an even number of values
         const long long evb = i == 0 ? 8LL * gen.nev64 : 4LL * evfStride(gen) + 8LL * gen.nevd;  // frontier bytes per event
         const int stage_on = stage_req[i];
         long long stage_bytes = 2LL * ((stage_on == 2 ? npl * rowb[i] : 0) + evb) * sh.block[i];

@@ -217,6 +217,7 @@ private:
     void computeAngular(int kind);
     void buildEventCache(int kind);
     void pairPolarisations();
+    void eventMajorMixedAngular();
     // SL_{npol-1-q} = conj(SL_q) on every event of every sample: the fused
     // kernels' tables keep the first (npol + 1) / 2 polarisations
     bool paired_[2] = {false, false};  // plain, mixed fused kernels use the paired tables

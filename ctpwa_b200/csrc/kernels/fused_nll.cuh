@@ -74,7 +74,7 @@
 #endif
 
 struct CtSample {
-    const void* slamp;  // [M_NPLANE * M_NPOL planes][ld] of SL2
+    const void* slamp;  // FP64: [M_NPLANE * M_NPOL planes][ld] of SL2; FP32: event-major records (CT_SL32_STRIDE)
     const void* ev;     // frontier rows [M_NEV][ld] FP64 (plain), [M_NEVF][ld] FP32 (mixed)
     const double* evd;  // mixed form: FP64 frontier rows [M_NEVD][ld]
     const double* w;    // per-event weights or nullptr (unit weights)
@@ -109,6 +109,10 @@ struct CtArgs {
 // CT_NPOL_STORED polarisations only, [plane][q][ld], and the *_pc kernels
 // rebuild the others as conjugates (the negation folds into the FMAs).
 #define CT_NPOL_STORED ((M_NPOL + 1) / 2)
+// The FP32 angular table is event-major: each event's NPL complex values
+// (NPL = M_NPLANE x the stored polarisations) in one record of an even
+// number of float2, read as float4; the FP64 tables are [row][ld].
+#define CT_SL32_STRIDE(NPL) (((NPL) + 1) / 2 * 2)
 
 // Per-call constants of the fused kernels in the constant bank: the
 // parameter-only subexpressions (FP64, and FP32 hi + lo pairs) and the
@@ -342,6 +346,11 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     const int kind = PH_ONLY ? 0 : S.kind;
     const long long n = S.n;
     const SL2* __restrict__ slamp = (const SL2*)S.slamp;
+    // this event's angular values: its record of the event-major FP32 table,
+    // or its first value of the [row][ld] FP64 table
+    constexpr int SL_NPL = M_NPLANE * (PAIRED ? CT_NPOL_STORED : M_NPOL);
+    constexpr int SL_SLS = CT_SL32_STRIDE(SL_NPL);
+    auto slat = [&](long long e) -> const SL2* { return sizeof(R) == 4 ? slamp + e * SL_SLS : slamp + e; };
     const L* __restrict__ eva = (const L*)S.ev;
     const double* __restrict__ evb = S.evd;
     const double* __restrict__ wts = S.w;
@@ -385,8 +394,19 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         // CT_NPOL_STORED polarisations are stored and read)
         constexpr int NPS = PAIRED ? CT_NPOL_STORED : M_NPOL;
         SL2 sl[M_NPLANE * NPS];
+        if constexpr (sizeof(R) == 4) {
+            // event-major FP32 record (16-byte aligned): two values per load
+            const float4* q4 = reinterpret_cast<const float4*>(slp);
 #pragma unroll
-        for (int c = 0; c < M_NPLANE * NPS; ++c) sl[c] = slp[(long long)c * ss];
+            for (int c = 0; c < M_NPLANE * NPS; c += 2) {
+                const float4 x = q4[c / 2];
+                sl[c] = make_float2(x.x, x.y);
+                if (c + 1 < M_NPLANE * NPS) sl[c + 1] = make_float2(x.z, x.w);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < M_NPLANE * NPS; ++c) sl[c] = slp[(long long)c * ss];
+        }
         // c_t = v_col(t) F_t per term (one per column, more with identical particles)
         R cr[M_NTERM], ci[M_NTERM];
 #pragma unroll
@@ -578,7 +598,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             else ct_cp_async_commit();  // empty group: the wait below covers buffer b alike
             ct_cp_async_wait<1>();
             const L* ap = CtEvent<L>::EVMAJ ? abuf + ((size_t)b * BLOCK + tid) * NA : abuf + (size_t)b * NA * BLOCK + tid;
-            event(e, ap, bbuf + (size_t)b * NB * BLOCK + tid, BLOCK, slamp + e, S.ld);
+            event(e, ap, bbuf + (size_t)b * NB * BLOCK + tid, BLOCK, slat(e), S.ld);
         }
         ct_cp_async_wait<0>();
     } else if constexpr (STAGE > 0) {
@@ -594,7 +614,9 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         constexpr int W = BLOCK / 32;
         constexpr int NA = CtEvent<L>::NA, NB = CtEvent<L>::NB;
         constexpr unsigned AR = 32 * sizeof(L), BR = 32 * sizeof(double), SR = 32 * sizeof(SL2);
-        constexpr unsigned BUF = NA * AR + NB * BR + (STAGE > 1 ? NPL * SR : 0);
+        // angular part of a tile: NPL rows of 32 values (FP64), or 32 records of SL_SLS values (FP32)
+        constexpr unsigned SLB = (sizeof(R) == 4 ? SL_SLS : NPL) * SR;
+        constexpr unsigned BUF = NA * AR + NB * BR + (STAGE > 1 ? SLB : 0);
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         unsigned char* wbuf = ct_dyn + ACC_BYTES + (size_t)warp * 2 * BUF;
         __shared__ __align__(8) unsigned long long ct_wbar[W][2];
@@ -617,10 +639,15 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             for (int r = 0; r < NB; ++r)
                 ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)r * BR, evb + (long long)r * S.ld + e0, BR, bar);
             if constexpr (STAGE > 1) {
+                if constexpr (sizeof(R) == 4) {
+                    // the tile's 32 records in one copy
+                    ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)NB * BR, slamp + e0 * SL_SLS, SLB, bar);
+                } else {
 #pragma unroll 1
-                for (int c = 0; c < NPL; ++c)
-                    ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)NB * BR + (size_t)c * SR, slamp + (long long)c * S.ld + e0,
-                                SR, bar);
+                    for (int c = 0; c < NPL; ++c)
+                        ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)NB * BR + (size_t)c * SR,
+                                    slamp + (long long)c * S.ld + e0, SR, bar);
+                }
             }
         };
         if (lane == 0) {
@@ -644,9 +671,10 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 const L* ap = (const L*)buf + (CtEvent<L>::EVMAJ ? lane * NA : lane);
                 const double* bp = (const double*)(buf + (size_t)NA * AR) + lane;
                 if constexpr (STAGE > 1)
-                    event(e, ap, bp, 32, (const SL2*)(buf + (size_t)NA * AR + (size_t)NB * BR) + lane, 32);
+                    event(e, ap, bp, 32,
+                          (const SL2*)(buf + (size_t)NA * AR + (size_t)NB * BR) + (sizeof(R) == 4 ? lane * SL_SLS : lane), 32);
                 else
-                    event(e, ap, bp, 32, slamp + e, S.ld);
+                    event(e, ap, bp, 32, slat(e), S.ld);
             }
             // every lane is done with buffer b before it is refilled
             __syncwarp();
@@ -666,7 +694,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     } else {
         const long long stride = (long long)S.cta_count * BLOCK;
         for (long long e = (long long)(cta - S.cta_begin) * BLOCK + threadIdx.x; e < n; e += stride)
-            event(e, CtEvent<L>::at(eva, e), evb ? evb + e : nullptr, S.ld, slamp + e, S.ld);
+            event(e, CtEvent<L>::at(eva, e), evb ? evb + e : nullptr, S.ld, slat(e), S.ld);
     }
     ct_block_reduce_store<BLOCK>(accd, accg, A.partials + (long long)cta * CT_NACC, kind == 0 ? S.vw_scale : -1.0,
                                  kind == 0 ? 2.0 : -2.0);

@@ -69,7 +69,7 @@ static_assert(CT_GRAM_ROWS <= 128, "the tensor-core Gram supports (npol + 1 for 
 #endif
 
 struct CtGramArgs {
-    const float2* slamp;     // mixed angular table of the phase-space sample
+    const float2* slamp;     // mixed angular table of the phase-space sample (event-major records)
     const float* evf;        // FP32 frontier rows
     const double* evd;       // FP64 frontier rows
     const double* w;         // per-event weights or nullptr
@@ -195,7 +195,7 @@ extern "C" __global__ void __launch_bounds__(CT_GRAM_THREADS, 2) ct_gram(CtGramA
                 const float fr = Fr[t] * sw, fi = Fi[t] * sw;
 #pragma unroll
                 for (int p = 0; p < NPS; ++p) {
-                    const float2 sl = G.slamp[(long long)(term_plane(t) * NPS + p) * G.ld + e];
+                    const float2 sl = G.slamp[e * CT_SL32_STRIDE(M_NPLANE * NPS) + term_plane(t) * NPS + p];
                     x[p * NA2 + a] += fr * sl.x - fi * sl.y;
                     x[p * NA2 + M_NA + a] += fr * sl.y + fi * sl.x;
                     const int q = M_NPOL - 1 - p;
