@@ -1593,6 +1593,19 @@ __global__ void ct_pair_check_kernel(const double2* __restrict__ sl, long long n
 // FP64 copy (the other kernels keep the full FP64 table). The check also
 // measures the minus-sign relation, which the paired kernels do not use.
 // Runs on the constructor's initialisation stream.
+// the compact table of paired polarisations, event-major:
+// out[e][c ns + q] = rows[c npol + q][e] (q < ns stored polarisations; zeros
+// for the padding events past n)
+__global__ void ct_compact_event_major_kernel(const double2* __restrict__ rows, long long n, long long ld, int nplane,
+                                              int npol, int ns, double2* __restrict__ out)
+{
+    const int nr = nplane * ns;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ld; e += (long long)gridDim.x * blockDim.x)
+        for (int c = 0; c < nplane; ++c)
+            for (int q = 0; q < ns; ++q)
+                out[e * nr + c * ns + q] = e < n ? rows[(long long)(c * npol + q) * ld + e] : make_double2(0.0, 0.0);
+}
+
 void Engine::pairPolarisations()
 {
     const int npol = model_.npol, nplane = gen_.nplane, npair = npol / 2;
@@ -1654,12 +1667,13 @@ void Engine::pairPolarisations()
         if (!d.slamp64) continue;
         const size_t rows = (size_t)nplane * ns;
         if (paired_[0]) {
+            // the compact FP64 table event-major: [ld][plane x stored polarisation]
             alloc(d.slamp64p, sizeof(double2) * rows * d.ld);
             device_bytes_ += sizeof(double2) * rows * d.ld;
-            for (int c = 0; c < nplane; ++c)
-                for (int q = 0; q < ns; ++q)
-                    CT_CUDA(cudaMemcpyAsync(d.slamp64p + (size_t)(c * ns + q) * d.ld, d.slamp64 + (size_t)(c * npol + q) * d.ld,
-                                            sizeof(double2) * d.ld, cudaMemcpyDeviceToDevice, init_stream_));
+            const unsigned grid = (unsigned)std::min<long long>((d.ld + 255) / 256, 148LL * 16);
+            ct_compact_event_major_kernel<<<grid, 256, 0, init_stream_>>>(d.slamp64, d.n, d.ld, nplane, npol, ns,
+                                                                           d.slamp64p);
+            CT_CUDA(cudaGetLastError());
         }
         if (paired_[1] && d.slamp32) {
             float2* compact = nullptr;

@@ -74,7 +74,7 @@
 #endif
 
 struct CtSample {
-    const void* slamp;  // FP64: [M_NPLANE * M_NPOL planes][ld] of SL2; FP32: event-major records (CT_SL32_STRIDE)
+    const void* slamp;  // full FP64: [M_NPLANE * M_NPOL planes][ld] of SL2; FP32 and paired FP64: event-major records
     const void* ev;     // frontier rows [M_NEV][ld] FP64 (plain), [M_NEVF][ld] FP32 (mixed)
     const double* evd;  // mixed form: FP64 frontier rows [M_NEVD][ld]
     const double* w;    // per-event weights or nullptr (unit weights)
@@ -348,9 +348,12 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
     const SL2* __restrict__ slamp = (const SL2*)S.slamp;
     // this event's angular values: its record of the event-major FP32 table,
     // or its first value of the [row][ld] FP64 table
+    // (event-major: the FP32 table, and the compact FP64 table of paired
+    // polarisations; the full FP64 table is [row][ld])
     constexpr int SL_NPL = M_NPLANE * (PAIRED ? CT_NPOL_STORED : M_NPOL);
-    constexpr int SL_SLS = CT_SL32_STRIDE(SL_NPL);
-    auto slat = [&](long long e) -> const SL2* { return sizeof(R) == 4 ? slamp + e * SL_SLS : slamp + e; };
+    constexpr bool SL_EM = sizeof(R) == 4 || PAIRED;
+    constexpr int SL_SLS = sizeof(R) == 4 ? CT_SL32_STRIDE(SL_NPL) : SL_NPL;
+    auto slat = [&](long long e) -> const SL2* { return SL_EM ? slamp + e * SL_SLS : slamp + e; };
     const L* __restrict__ eva = (const L*)S.ev;
     const double* __restrict__ evb = S.evd;
     const double* __restrict__ wts = S.w;
@@ -403,6 +406,10 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 sl[c] = make_float2(x.x, x.y);
                 if (c + 1 < M_NPLANE * NPS) sl[c + 1] = make_float2(x.z, x.w);
             }
+        } else if constexpr (SL_EM) {
+            // event-major FP64 record: consecutive 16-byte values
+#pragma unroll
+            for (int c = 0; c < M_NPLANE * NPS; ++c) sl[c] = slp[c];
         } else {
 #pragma unroll
             for (int c = 0; c < M_NPLANE * NPS; ++c) sl[c] = slp[(long long)c * ss];
@@ -615,7 +622,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
         constexpr int NA = CtEvent<L>::NA, NB = CtEvent<L>::NB;
         constexpr unsigned AR = 32 * sizeof(L), BR = 32 * sizeof(double), SR = 32 * sizeof(SL2);
         // angular part of a tile: NPL rows of 32 values (FP64), or 32 records of SL_SLS values (FP32)
-        constexpr unsigned SLB = (sizeof(R) == 4 ? SL_SLS : NPL) * SR;
+        constexpr unsigned SLB = (SL_EM ? SL_SLS : NPL) * SR;
         constexpr unsigned BUF = NA * AR + NB * BR + (STAGE > 1 ? SLB : 0);
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         unsigned char* wbuf = ct_dyn + ACC_BYTES + (size_t)warp * 2 * BUF;
@@ -639,7 +646,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
             for (int r = 0; r < NB; ++r)
                 ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)r * BR, evb + (long long)r * S.ld + e0, BR, bar);
             if constexpr (STAGE > 1) {
-                if constexpr (sizeof(R) == 4) {
+                if constexpr (SL_EM) {
                     // the tile's 32 records in one copy
                     ct_bulk_g2s(buf + (size_t)NA * AR + (size_t)NB * BR, slamp + e0 * SL_SLS, SLB, bar);
                 } else {
@@ -672,7 +679,7 @@ __device__ __forceinline__ void ct_fused_body(const CtArgs& A)
                 const double* bp = (const double*)(buf + (size_t)NA * AR) + lane;
                 if constexpr (STAGE > 1)
                     event(e, ap, bp, 32,
-                          (const SL2*)(buf + (size_t)NA * AR + (size_t)NB * BR) + (sizeof(R) == 4 ? lane * SL_SLS : lane), 32);
+                          (const SL2*)(buf + (size_t)NA * AR + (size_t)NB * BR) + (SL_EM ? lane * SL_SLS : lane), 32);
                 else
                     event(e, ap, bp, 32, slat(e), S.ld);
             }

@@ -112,7 +112,7 @@ __device__ __forceinline__ double ct_value(CtDual x) { return x.v; }
 #define CT_HCONST_ALLOC (M_NCONST > 0 ? M_NCONST : 1)
 
 struct CtHvpSample {
-    const double2* slamp;  // [M_NPLANE * M_NPOL][ld] angular values
+    const double2* slamp;  // [M_NPLANE * M_NPOL][ld] angular values; paired: event-major [ld][M_NPLANE * stored]
     const double* ev;      // [M_NEV][ld] FP64 frontier values
     const double* w;       // per-event weights or nullptr
     long long n;
@@ -221,7 +221,9 @@ extern "C" __global__ void __launch_bounds__(CT_HVP_BLOCK) ct_hvp_f64(CtHvpArgs 
             constexpr int NPS = CT_HVP_PAIRED ? (M_NPOL + 1) / 2 : M_NPOL;
             double2 sl[M_NPLANE * NPS];
 #pragma unroll
-            for (int c = 0; c < M_NPLANE * NPS; ++c) sl[c] = __ldg(S.slamp + (long long)c * ld + e);
+            for (int c = 0; c < M_NPLANE * NPS; ++c)
+                sl[c] = CT_HVP_PAIRED ? __ldg(S.slamp + e * (M_NPLANE * NPS) + c)  // compact table: event-major
+                                      : __ldg(S.slamp + (long long)c * ld + e);
             CtDual cr[M_NTERM], ci[M_NTERM];
 #pragma unroll
             for (int t = 0; t < M_NTERM; ++t) {
