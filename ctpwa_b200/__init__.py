@@ -217,13 +217,15 @@ class analysis:
 
     @classmethod
     def from_device(cls, config_file: str, phsp, data, bkg=None, weights=None, device=None,
-                    precision: str = "fp64") -> "analysis":
+                    precision: str = "fp64", fp64_only: bool = False) -> "analysis":
         """Analysis over in-memory samples: the model from config_file, the
         events from float64 CUDA tensors [n, n_final, 4] (E, px, py, pz in the
         config's Data.order) instead of the config's Data files. weights: None
         or three per-event float64 CUDA tensors / None (phase space, data,
         background). The tensors are copied; pending work on the current
-        stream is waited for first."""
+        stream is waited for first. fp64_only: build neither the mixed-form
+        tables nor the polarisation pairing (FP64 evaluations and intensities
+        only; cheaper to build)."""
         self = cls.__new__(cls)
         self._h = None
         self._lib = _lib.load()
@@ -259,8 +261,8 @@ class analysis:
         torch.cuda.current_stream(self._device).synchronize()
         status = ctypes.c_int(0)
         err = ctypes.create_string_buffer(4096)
-        h = self._lib.ctpwa_create_from_device(str(config_file).encode(), self._device, p4, n, w,
-                                               ctypes.byref(status), err, 4096)
+        h = self._lib.ctpwa_create_from_device_flags(str(config_file).encode(), self._device, p4, n, w,
+                                                     1 if fp64_only else 0, ctypes.byref(status), err, 4096)
         if not h:
             raise RuntimeError(err.value.decode("utf-8", "replace"))
         self._h = ctypes.c_void_p(h)

@@ -17,6 +17,12 @@ SIGNATURES = {
     "ctpwa_create_from_device": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                                    ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_void_p),
                                                    ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_size_t]),
+    "ctpwa_create_from_device_flags": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.c_int,
+                                                         ctypes.POINTER(ctypes.c_void_p),
+                                                         ctypes.POINTER(ctypes.c_longlong),
+                                                         ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                                         ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                                         ctypes.c_size_t]),
     "ctpwa_create_shard": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_size_t]),
     "ctpwa_destroy": (None, [ctypes.c_void_p]),

@@ -131,8 +131,15 @@ ctpwa_handle* ctpwa_create_from_device(const char* config_path, int device, cons
                                        const long long* n, const double* const* w, int* status, char* err,
                                        size_t errlen)
 {
-    if (!p4 || !n) {
-        const std::string msg = "null argument";
+    return ctpwa_create_from_device_flags(config_path, device, p4, n, w, 0, status, err, errlen);
+}
+
+ctpwa_handle* ctpwa_create_from_device_flags(const char* config_path, int device, const double* const* p4,
+                                             const long long* n, const double* const* w, int flags, int* status,
+                                             char* err, size_t errlen)
+{
+    if (!p4 || !n || (flags & ~CTPWA_CREATE_FP64_ONLY)) {
+        const std::string msg = (!p4 || !n) ? "null argument" : "unknown creation flags";
         if (status) *status = CTPWA_ERR_ARG;
         setErr(nullptr, CTPWA_ERR_ARG, msg);
         if (err && errlen) copyOut(msg, err, errlen);
@@ -141,6 +148,10 @@ ctpwa_handle* ctpwa_create_from_device(const char* config_path, int device, cons
     ctpwa::EngineOptions opt;
     opt.device = device;
     opt.device_samples = true;
+    if (flags & CTPWA_CREATE_FP64_ONLY) {
+        opt.mixed_tables = false;
+        opt.pair_polarisations = false;
+    }
     for (int k = 0; k < 3; ++k) {
         opt.dev_p4[k] = p4[k];
         opt.dev_n[k] = n[k];

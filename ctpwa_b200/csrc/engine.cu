@@ -1610,7 +1610,7 @@ void Engine::pairPolarisations()
 {
     const int npol = model_.npol, nplane = gen_.nplane, npair = npol / 2;
     const char* off = std::getenv("CTPWA_NO_POL_PAIRING");
-    if (npair == 0 || nplane * npair > 32 || (off && *off && *off != '0')) return;
+    if (!opt_.pair_polarisations || npair == 0 || nplane * npair > 32 || (off && *off && *off != '0')) return;
     const int nout = 2 * nplane * npair + 1;
     std::vector<double> worst(2 * nplane * npair, 0.0);
     double big = 0.0;

@@ -63,6 +63,7 @@ struct EngineOptions {
     int device = 0;
     bool keep_momenta = false;
     bool mixed_tables = true;  // build the FP32 angular table for the mixed path
+    bool pair_polarisations = true;  // check the conjugate pairing and build the compact tables
     int shard_rank = 0;        // keep event block shard_rank of shard_world of every sample
     int shard_world = 1;
     // In-memory samples: when set, the events come from these device arrays

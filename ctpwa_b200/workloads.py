@@ -393,7 +393,7 @@ def make_device(name, outdir, n_phsp, n_data, seed=0, device=0, safety=1.2, timi
             ncand = min(cap, int(1.15 * (n_data - have) / acc) + 10_000)
         cand = toymc.phase_space_device(M_JPSI, masses, ncand, 5001 + seed + 7919 * batch, device=device)
         lap("candidates")
-        ana = analysis.from_device(str(cfg), tiny, cand, device=device)
+        ana = analysis.from_device(str(cfg), tiny, cand, device=device, fp64_only=True)
         lap("cand_handle")
         I = ana.getIntensity(p, kind=1)
         del ana

@@ -61,6 +61,17 @@ ctpwa_handle* ctpwa_create_from_device(const char* config_path, int device, cons
                                        const long long* n, const double* const* w, int* status, char* err,
                                        size_t errlen);
 
+/* The same with creation flags. CTPWA_CREATE_FP64_ONLY: no mixed-form
+ * tables and no polarisation pairing (nor its compact tables): a handle
+ * for FP64 evaluations and intensities only, cheaper to build (a toy
+ * generator's accept-reject candidates); a mixed-form evaluation on it fails
+ * with CTPWA_ERR_CUDA ("mixed-precision tables were not built"). Unknown
+ * flags: CTPWA_ERR_ARG. No counterpart in the reference. */
+#define CTPWA_CREATE_FP64_ONLY 1
+ctpwa_handle* ctpwa_create_from_device_flags(const char* config_path, int device, const double* const* p4,
+                                             const long long* n, const double* const* w, int flags, int* status,
+                                             char* err, size_t errlen);
+
 /* Releases device memory of the handle (the reference never frees;
  * src/Analysis.cu:1284-1290) into this library's per-device memory pool,
  * where later handles reuse it. It does not wait for work on the caller's

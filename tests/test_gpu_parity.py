@@ -696,3 +696,28 @@ def test_dat_momenta_match_npy(tmp_path):
         na, ga = a.getNLLAndGrad(pt, prec)
         nb, gb = b.getNLLAndGrad(pt, prec)
         assert float(na) == float(nb) and torch.equal(ga, gb)
+
+
+def test_fp64_only_handles(tmp_path):
+    """Handles created without the mixed-form tables and the polarisation
+    pairing (ctpwa_create_from_device_flags, CTPWA_CREATE_FP64_ONLY; the toy
+    generator's accept-reject candidates): the same intensities bit for bit,
+    FP64 NLL and gradient within 1e-12, and a clear error for the mixed form."""
+    import torch
+    import ctpwa_b200
+
+    cfg = workloads.make("kkpi", tmp_path, n_phsp=30_001, n_data=4_001, n_bkg=999, accept_reject=False, seed=22)
+    dev = [torch.from_numpy(np.load(tmp_path / f)).cuda() for f in ("phsp.npy", "data.npy", "bkg.npy")]
+    full = ctpwa_b200.analysis.from_device(cfg, dev[0], dev[1], dev[2])
+    lean = ctpwa_b200.analysis.from_device(cfg, dev[0], dev[1], dev[2], fp64_only=True)
+    assert full.launchShape()["fp64"]["pol_paired"] == 1 and lean.launchShape()["fp64"]["pol_paired"] == 0
+    assert lean.deviceBytes() < full.deviceBytes()
+    p = workloads.true_params(full.getNVector(), full.getFreeResParams()[0].numpy())
+    pt = torch.tensor(p, dtype=torch.float64, device="cuda")
+    assert torch.equal(full.getIntensity(pt, kind=1), lean.getIntensity(pt, kind=1))
+    n0, g0 = full.getNLLAndGrad(pt, "fp64")
+    n1, g1 = lean.getNLLAndGrad(pt, "fp64")
+    assert abs(float(n1) - float(n0)) <= 1e-12 * abs(float(n0))
+    assert float((g1 - g0).abs().max()) <= 1e-11 * float(g0.abs().max())
+    with pytest.raises(RuntimeError, match="mixed-precision tables"):
+        lean.getNLLAndGrad(pt, "mixed")
