@@ -537,19 +537,34 @@ struct FinalizeArgs {
 };
 
 // Per-sample sums of the partial rows plus the sample totals (event-sharded
-// evaluation); same fixed-order reduction as ct_finalize_kernel.
+// evaluation); the same fixed-order reduction as ct_finalize_kernel (each
+// row read by one warp, the warps' sums added in warp order; launched with
+// 1024 threads and [32][nacc] doubles of dynamic shared memory), so a
+// sharded evaluation on one shard reproduces the unsharded sums bit for bit.
 __global__ void __launch_bounds__(1024) ct_rowsum_kernel(const double* __restrict__ partials, int nacc, FinalizeArgs A,
                                                          double W_phsp, double* __restrict__ out)
 {
+    extern __shared__ double wsum[];  // [nwarp][nacc]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int i = warp; i < 3 * nacc; i += nwarp) {
-        int k = i / nacc, j = i % nacc;
-        double s = 0.0;
-        if (A.has[k])
-            for (int b = lane; b < A.cta[k][1]; b += 32) s += partials[(long long)(A.cta[k][0] + b) * nacc + j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) out[i] = s;
+    for (int k = 0; k < 3; ++k) {
+        for (int j0 = 0; j0 < nacc; j0 += 32) {
+            const int j = j0 + lane;
+            if (j >= nacc) continue;
+            double s = 0.0;
+            if (A.has[k]) {
+                const double* rows = partials + (long long)A.cta[k][0] * nacc + j;
+#pragma unroll 4
+                for (int b = warp; b < A.cta[k][1]; b += nwarp) s += rows[(long long)b * nacc];
+            }
+            wsum[warp * nacc + j] = s;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < nacc; j += blockDim.x) {
+            double s = 0.0;
+            for (int w = 0; w < nwarp; ++w) s += wsum[w * nacc + j];
+            out[k * nacc + j] = s;
+        }
+        __syncthreads();
     }
     if (threadIdx.x == 0) {
         out[3 * nacc + 0] = A.n_phsp;
@@ -931,6 +946,8 @@ Engine::Engine(const std::string& config_path, const EngineOptions& opt) : opt_(
     CT_CUDA(cudaFuncSetAttribute((const void*)ct_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  200 * 1024));
     CT_CUDA(cudaFuncSetAttribute((const void*)ct_finalize_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 200 * 1024));
+    CT_CUDA(cudaFuncSetAttribute((const void*)ct_rowsum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  200 * 1024));
     shape_ = fusedShape(gen_);
     // initialisation work goes to a private non-blocking stream, so a handle
@@ -2591,7 +2608,8 @@ void Engine::shardSums(const double* d_params, int precision, double* d_sums, cu
     f.n_phsp = (double)samples_[0].n;
     f.W_data = samples_[1].wsum;
     f.W_bkg = has_bkg_ ? samples_[2].wsum : 0.0;
-    ct_rowsum_kernel<<<1, 1024, 0, stream>>>(d_partials_, nacc, f, samples_[0].wsum, d_sums);
+    ct_rowsum_kernel<<<1, 1024, sizeof(double) * 32 * (size_t)nacc, stream>>>(d_partials_, nacc, f, samples_[0].wsum,
+                                                                               d_sums);
     CT_CUDA(cudaGetLastError());
 }
 
