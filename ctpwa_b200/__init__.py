@@ -465,10 +465,11 @@ class analysis:
         status, eval_ms); status 0: projected gradient <= gtol, 1: relative
         decrease <= ftol, 2: max_evals spent, 3: no decrease found. With
         `batch` (an EvalBatch), every evaluation is gathered with those of the
-        other fits running in the batch (one launch for all of them). When no
-        resonance parameter can move (free 0 or lower == upper for all of
-        them), the fit builds the normalisation cache (cacheNormalisation)
-        and its evaluations read only the data and background samples."""
+        other fits running in the batch (one launch for all of them). Without
+        `batch`, when no resonance parameter can move (free 0 or lower ==
+        upper for all of them), the fit builds the normalisation cache
+        (cacheNormalisation) and its evaluations read only the data and
+        background samples."""
         self._check()
         import numpy as np
 
