@@ -16,7 +16,12 @@ front end, what the reference builds from it:
     the parameters listed in `free` (all for `[-1]` and for custom
     lineshapes), named "<resonance>_<parameter>" (src/Info.cu:86-98), with
     `free_range` bounds or the default +-50 % of the value;
-  - one free complex coupling per amplitude (no coupling matrix).
+  - one free complex coupling per amplitude (no coupling matrix);
+  - `Constraints: var_equal` groups of resonance parameters: the later
+    members share the first one's slot and are not free parameters of their
+    own;
+  - the parent's `polarization` list of m values: the polarisation states
+    kept, as indices into m = +J .. -J (src/Analysis.cu:4249-4322).
 Supported lineshapes: BWR (mass, width) and Custom (paramNames). Anything
 else raises NotImplementedError, so a test cannot pass by omission.
 """
@@ -93,9 +98,12 @@ def lower(config_path):
     identical = set()
     for pair in (cfg.get("Constraints") or {}).get("identical", []) or []:
         identical.add(frozenset(pair))
-    for key in ("CouplingMatrix", "coupling_matrix", "var_equal"):
+    for key in ("CouplingMatrix", "coupling_matrix"):
         if key in cfg:
             raise NotImplementedError(f"{key} is outside the restated subset")
+    tied = set()
+    for group in (cfg.get("Constraints") or {}).get("var_equal", []) or []:
+        tied.update(group[1:])
 
     names, slots, seen = [], [], set()
     for chain_name, chain in cfg["DecayChains"].items():
@@ -145,5 +153,25 @@ def lower(config_path):
                         lo, hi = (float(x) for x in ranges[n_i])
                     else:
                         lo, hi = v - 0.5 * abs(v), v + 0.5 * abs(v)
-                    slots.append((f"{rname}_{pnames[i]}", v, lo, hi))
-    return {"amplitude_names": names, "slots": slots, "n_free": len(names)}
+                    if f"{rname}_{pnames[i]}" not in tied:
+                        slots.append((f"{rname}_{pnames[i]}", v, lo, hi))
+    # polarisation states: the parent's m = +J .. -J times the spin states of
+    # the (massive) final-state particles; a parent's `polarization` list
+    # keeps some of its m values
+    parent = particles[mother]
+    two_j = _twice(parent["J"])
+    n_final = 1
+    for name in cfg["Data"]["order"]:
+        fp = particles[name]
+        if _twice(fp["J"]) and not float(fp.get("mass", 0.0)) > 0.0:
+            raise NotImplementedError("massless final-state particles with spin are outside the restated subset")
+        n_final *= _twice(fp["J"]) + 1
+    pols = parent.get("polarization")
+    if pols is None:
+        pol_map = list(range((two_j + 1) * n_final))
+    elif n_final == 1:
+        pol_map = [int((two_j - _twice(m)) // 2) for m in pols]
+    else:
+        raise NotImplementedError("a polarisation list with spinning final-state particles is outside the subset")
+    return {"amplitude_names": names, "slots": slots, "n_free": len(names), "npol": len(pol_map),
+            "npol_total": (two_j + 1) * n_final, "pol_map": pol_map}

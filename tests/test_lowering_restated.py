@@ -21,6 +21,9 @@ def _check(cfg):
         np.testing.assert_allclose([v, lo, hi], [s["init"], s["lower"], s["upper"]], rtol=1e-12)
     assert r["n_free"] == d["coupling"]["n_free"]
     assert d["param_names"] == r["amplitude_names"] + [s[0] for s in r["slots"]]
+    assert (r["npol"], r["npol_total"]) == (d["npol"], d["npol_total"])
+    # the library lists the kept polarisations only when some are dropped
+    assert r["pol_map"] == (list(d["pol_map"]) or list(range(d["npol_total"])))
     return r
 
 
@@ -47,6 +50,20 @@ def test_lowering_variants_match_restatement(tmp_path):
     r = _check(p)
     assert [s[0] for s in r["slots"]] == ["rho770_mass", "rho770_width", "rho1450_width"]
     np.testing.assert_allclose(r["slots"][2][2:], [0.3, 0.5])
+
+
+def test_polarisation_mask_and_shared_parameters_match_restatement(tmp_path):
+    """The layout case of the reference-build comparison: J/psi with m = +-1
+    only and a var_equal group tying K*(1410)'s width to K*(892)'s."""
+    text = workloads.config_text("kkpi", "p.npy", "d.npy")
+    text = text.replace("Jpsi: {J: 1, P: -1, mass: 3.0969}",
+                        "Jpsi: {J: 1, P: -1, mass: 3.0969, polarization: [1, -1]}")
+    text = text.replace("Resonances:", "Constraints:\n  var_equal:\n    - [Kst892_width, Kst1410_width]\nResonances:", 1)
+    p = tmp_path / "m.yml"
+    p.write_text(text)
+    r = _check(p)
+    assert r["npol"] == 2 and r["pol_map"] == [0, 2]
+    assert "Kst1410_width" not in [s[0] for s in r["slots"]]
 
 
 def test_vertices_with_several_waves_match_restatement(tmp_path):
